@@ -1,0 +1,216 @@
+/*
+ * seldon_b200.h -- C ABI of libseldon_b200.so, the B200 (sm_100a) engine
+ * behind Seldon's sparse Krylov path.
+ *
+ * Every entry point replaces one routine of the reference (Seldon, a
+ * header-only C++ template library).  The reference "interface" is a set of
+ * free-function overloads resolved by argument-dependent lookup; the citation
+ * beside each declaration names the overload it stands in for (file:line in
+ * the Seldon tree).  include/SeldonB200.hxx maps Seldon's C++ templates onto
+ * these functions, so a Seldon user changes only an allocator argument.
+ *
+ * Conventions
+ *   - Sizes and CSR indices are int32, as in Seldon (Matrix_Sparse.hxx:60-64).
+ *   - Vector arguments are DEVICE pointers unless the name says _host.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *   - Every function returns an int status: SB2_OK (0) or a negative SB2_ERR_*
+ *     code.  Nothing throws, nothing aborts.  Solver convergence/breakdown is
+ *     NOT a status: it is reported in sb2_iter_result.error_code exactly as
+ *     Seldon's Iteration::ErrorCode() (Iterative.cxx:344-354).
+ *   - Device-side waits (grid barriers of the fused solvers) are bounded; a
+ *     wait that runs out ends the kernel and the call returns SB2_ERR_TIMEOUT.
+ */
+#ifndef SELDON_B200_H
+#define SELDON_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define SB2_OK 0
+#define SB2_ERR_INVALID_VALUE -1 /* bad sizes / null pointers / aliasing */
+#define SB2_ERR_NO_MEMORY -2     /* a device allocation failed */
+#define SB2_ERR_CUDA -3          /* any other CUDA runtime error */
+#define SB2_ERR_TIMEOUT -4       /* a bounded device-side wait ran out */
+#define SB2_ERR_INVALID_CSR -5   /* CSR invariants violated (validator) */
+#define SB2_ERR_NOT_SUPPORTED -6 /* option combination not implemented */
+
+/* Human-readable text for a status code (static storage). */
+const char* sb2_status_string(int status);
+
+/* Library version, e.g. 10000 for 1.0.0. */
+int sb2_version(void);
+
+/* ------------------------------------------------------------ CSR handle */
+
+/* Opaque device CSR matrix (device copies of ptr_/ind_/data_ plus the
+ * row-block partition the SpMV kernels use). */
+typedef struct sb2_csr sb2_csr;
+
+/* Create a device matrix from HOST arrays in Seldon's layout.
+ *   m, n, nnz          sizes (nnz = ptr[m])
+ *   ptr[m+1], ind[nnz], val[nnz]   Seldon's ptr_, ind_, data_
+ *   symmetric_upper    0: Matrix<double, General, RowSparse>
+ *                      1: Matrix<double, Symmetric, RowSymSparse>: only the
+ *                         upper triangle (diagonal included) is given
+ *                         (Matrix_SymSparse.cxx:1031-1032)
+ *   validate           1: check ptr monotone, ptr[0]=0, ptr[m]=nnz,
+ *                         0<=ind<n (and ind>=row for symmetric_upper), as
+ *                         SELDON_CHECK_DIMENSIONS does (Matrix_Sparse.cxx:118-170)
+ * The host arrays are copied; the caller keeps ownership.
+ * Replaces the constructor Matrix_Sparse(i, j, values, ptr, ind)
+ * (Matrix_Sparse.cxx:105-180) and SetData (Matrix_Sparse.cxx:305-415). */
+int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
+                   const double* val, int symmetric_upper, int validate,
+                   sb2_csr** out);
+
+/* Release a matrix (Matrix_Sparse::~Matrix_Sparse, Matrix_Sparse.cxx:206). */
+int sb2_csr_destroy(sb2_csr* A);
+
+/* Sizes: rows, columns, stored nonzeros (upper part for symmetric) and the
+ * nonzeros of the full operator.  (GetM/GetN/GetNonZeros, Matrix_Sparse.hxx:101-106) */
+int sb2_csr_info(const sb2_csr* A, int* m, int* n, int* nnz_stored,
+                 int* nnz_full);
+
+/* Copy the stored arrays back to host buffers (ptr[m+1], ind[nnz_stored],
+ * val[nnz_stored]); any pointer may be NULL. */
+int sb2_csr_download(const sb2_csr* A, int* ptr, int* ind, double* val);
+
+/* ------------------------------------------------------------ SpMV */
+
+/* y = beta*y + alpha*op(A)*x  with op = A (trans=0) or A^T (trans=1).
+ * Seldon semantics: y is scaled by beta even when beta == 0, so a NaN in y
+ * stays NaN.  x and y must not overlap.
+ * Replaces MltAdd(alpha, M, X, beta, Y) for RowSparse
+ * (Functions_MatVect.cxx:398-431), RowSymSparse (:526-564), and
+ * MltAdd(alpha, SeldonTrans, M, X, beta, Y) (:729-758; symmetric :915-927). */
+int sb2_spmv(const sb2_csr* A, int trans, double alpha, const double* x,
+             double beta, double* y, void* stream);
+
+/* y = alpha*op(A)*x, y overwritten (not read).
+ * Replaces Mlt(M, X, Y) / Mlt(alpha, M, X, Y) / Mlt(Trans, M, X, Y)
+ * (Functions_MatVect.cxx:72-130: Y.Fill(0) then MltAdd(alpha, M, X, 0, Y)). */
+int sb2_mlt(const sb2_csr* A, int trans, double alpha, const double* x,
+            double* y, void* stream);
+
+/* MltAdd with HOST vectors: x is copied in, y is copied in (beta != 0) and
+ * back out, on `stream`; returns after y is back on the host.  For callers
+ * whose vectors live in host memory (Seldon's default MallocAlloc). */
+int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
+                  const double* x_host, double beta, double* y_host,
+                  void* stream);
+
+/* Mlt with HOST vectors: y_host = alpha*op(A)*x_host (y not read).
+ * Same reference routine as sb2_mlt (Functions_MatVect.cxx:72-130). */
+int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
+                 const double* x_host, double* y_host, void* stream);
+
+/* ------------------------------------------------------------ BLAS-1 (FP64) */
+/* All reductions are deterministic: the same n gives the same summation tree
+ * on every call and every run. */
+
+/* *result (host) = sum_i x_i*y_i.  DotProd / DotProdConj (real)
+ * (Functions_Vector.cxx:330-346, :391-397; cblas_ddot Blas_1.cxx:428-438). */
+int sb2_dot(int n, const double* x, const double* y, double* result,
+            void* stream);
+
+/* *result (host) = sqrt(sum_i x_i^2).  Norm2 (Functions_Vector.cxx:540-549;
+ * cblas_dnrm2 Blas_1.cxx:611-615). */
+int sb2_nrm2(int n, const double* x, double* result, void* stream);
+
+/* Device-result forms: write the scalar to device memory, do not synchronize. */
+int sb2_dot_device(int n, const double* x, const double* y, double* d_result,
+                   void* stream);
+int sb2_nrm2_device(int n, const double* x, double* d_result, void* stream);
+
+/* y += alpha*x; no-op when alpha == 0.  Add (Functions_Vector.cxx:85-105;
+ * cblas_daxpy Blas_1.cxx:353-365). */
+int sb2_axpy(int n, double alpha, const double* x, double* y, void* stream);
+
+/* x *= alpha.  Mlt(alpha, X) (Functions_Vector.cxx:69-74; cblas_dscal
+ * Blas_1.cxx:212-216). */
+int sb2_scal(int n, double alpha, double* x, void* stream);
+
+/* y = x.  Copy (Functions_Vector.cxx:240-246; cblas_dcopy Blas_1.cxx:282-293). */
+int sb2_copy(int n, const double* x, double* y, void* stream);
+
+/* x_i = value.  Vector::Fill / Zero (vector/Vector.cxx:687). */
+int sb2_fill(int n, double value, double* x, void* stream);
+
+/* ------------------------------------------------------------ preconditioners */
+
+#define SB2_PRECOND_IDENTITY 0 /* Preconditioner_Base (Iterative.cxx:50-77) */
+#define SB2_PRECOND_JACOBI 1   /* z_i = r_i / A(i,i); absent from the reference */
+#define SB2_PRECOND_SOR 2      /* SorPreconditioner (Precond_Ssor.cxx:24-90) */
+
+typedef struct sb2_precond sb2_precond;
+
+/* kind: SB2_PRECOND_*.  omega, nb_iter, symmetric: SorPreconditioner's
+ * SetParameterRelaxation / SetNumberIterations / Init(Un)SymmetricPreconditioning
+ * (Precond_Ssor.cxx:36-39; defaults omega=1, nb_iter=1, symmetric=1). */
+int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
+                       int symmetric, sb2_precond** out);
+int sb2_precond_destroy(sb2_precond* M);
+
+/* z = M^{-1} r (Solve) / M^{-T} r (TransSolve).  z and r must not overlap.
+ * Precond_Ssor.cxx:62-90: z is zeroed, then SOR type 0 (symmetric), 2
+ * (forward, Solve) or 3 (backward, TransSolve). */
+int sb2_precond_solve(const sb2_precond* M, const double* r, double* z,
+                      void* stream);
+int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z,
+                            void* stream);
+
+/* In-place relaxation on x: SOR(A, X, B, omega, iter, type_ssor) with
+ * type_ssor 2 (forward), 3 (backward) or 0 (both), reproducing the
+ * sequential sweep order exactly by level scheduling.
+ * Relaxation_MatVect.cxx:41-95 (RowSparse), :176-298 (RowSymSparse). */
+int sb2_sor(const sb2_csr* A, double* x, const double* b, double omega,
+            int iter, int type_ssor, void* stream);
+
+/* ------------------------------------------------------------ iterative solvers */
+
+/* Iteration<double> parameters (Iterative.hxx:47-108). */
+typedef struct {
+  double tol;          /* SetTolerance; Seldon default 1e-6 */
+  int max_iter;        /* SetMaxNumberIteration; default 100 */
+  int restart;         /* SetRestart (GMRES m); default 10 */
+  int print_level;     /* 0 silent, 1 every 100 iterations, 6 every iteration */
+  int init_guess_null; /* SetInitGuess: 1 -> x is zeroed, 0 -> x is used */
+} sb2_iter_params;
+
+/* What the solve reports back. */
+typedef struct {
+  int nb_iter;          /* Iteration::GetNumberIteration() at exit */
+  int error_code;       /* Iteration::ErrorCode(): 0, -2 (max_iter), 1/2/3 */
+  int init_failed;      /* 1 when Init() found a zero right-hand side */
+  int hist_len;         /* entries written to the caller's history buffer */
+  double facteur_reste; /* 1/||r_init|| (Iteration::GetFactor) */
+  double last_residual; /* relative residual of the last Finished() test */
+} sb2_iter_result;
+
+/* Seldon's drivers.  M == NULL means the identity (Preconditioner_Base).
+ * hist/hist_it (host, may be NULL) receive, for every Finished() test, the
+ * relative residual and the iteration number it was tested at (hist_cap
+ * entries at most) -- the lines Seldon prints at print_level 6.
+ * Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183. */
+int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+           const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+           int* hist_it, int hist_cap, void* stream);
+int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x,
+                 const double* b, const sb2_iter_params* params,
+                 sb2_iter_result* result, double* hist, int* hist_it,
+                 int hist_cap, void* stream);
+int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
+              const double* b, const sb2_iter_params* params,
+              sb2_iter_result* result, double* hist, int* hist_it,
+              int hist_cap, void* stream);
+
+/* Device-side wait limit for the fused solvers' grid barriers, in
+ * milliseconds (default 2000).  Returns the previous value. */
+int sb2_set_wait_limit_ms(int ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SELDON_B200_H */

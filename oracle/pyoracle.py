@@ -1,0 +1,189 @@
+"""ctypes access to the checkers -- TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``: the plain-C restatement (oracle/liboracle.so).
+* ``Reference``: the reference itself (oracle/_ref/libseldon_ref.so, built
+  from the Seldon headers by oracle/Makefile), present only where it was
+  built; ``Reference.available()`` says so.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+bench.py use this module; the product path never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libseldon_ref.so")
+REF_FAST_SO = os.path.join(HERE, "_ref", "libseldon_ref_fast.so")
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _csr_args(ptr, ind, val):
+    ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+    ind = np.ascontiguousarray(ind, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    return ptr, ind, val
+
+
+class _Base:
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing: run `make -C oracle`")
+        self.lib = ctypes.CDLL(path)
+
+
+class Oracle(_Base):
+    """The plain-C restatement of Seldon's path (seldon_oracle.c)."""
+
+    def __init__(self, path=ORACLE_SO):
+        super().__init__(path)
+        L = self.lib
+        L.orc_mltadd.argtypes = [_i, _i, _vp, _vp, _vp, _i, _i, _d, _vp, _d, _vp]
+        L.orc_mltadd.restype = None
+        L.orc_dot.argtypes = [_i, _vp, _vp]
+        L.orc_dot.restype = _d
+        L.orc_nrm2.argtypes = [_i, _vp]
+        L.orc_nrm2.restype = _d
+        L.orc_genrot.argtypes = [_vp, _vp, _vp, _vp]
+        L.orc_genrot.restype = None
+        L.orc_trsv_upper.argtypes = [_i, _vp, _i, _vp]
+        L.orc_trsv_upper.restype = None
+        L.orc_sor.argtypes = [_i, _vp, _vp, _vp, _i, _vp, _vp, _d, _i, _i]
+        L.orc_sor.restype = None
+        L.orc_solve.argtypes = [_i, _i, _i, _vp, _vp, _vp, _i, _i, _d, _i, _i, _vp, _vp,
+                                _d, _i, _i, _i, _vp, _vp, _vp, _i, _vp]
+        L.orc_solve.restype = _i
+
+    def mltadd(self, m, n, ptr, ind, val, alpha, x, beta, y, sym=False, trans=False):
+        """Returns a new y = beta*y + alpha*op(A)*x (MltAdd)."""
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.array(y, dtype=np.float64, copy=True)
+        self.lib.orc_mltadd(m, n, _p(ptr), _p(ind), _p(val), int(sym), int(trans),
+                            float(alpha), _p(x), float(beta), _p(y))
+        return y
+
+    def dot(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        return self.lib.orc_dot(x.size, _p(x), _p(y))
+
+    def nrm2(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.orc_nrm2(x.size, _p(x))
+
+    def genrot(self, a, b):
+        v = np.array([a, b, 0.0, 0.0])
+        base = v.ctypes.data
+        self.lib.orc_genrot(base, base + 8, base + 16, base + 24)
+        return tuple(v)  # (r, z, c, s)
+
+    def sor(self, ptr, ind, val, x, b, omega, it, type_ssor, sym=False):
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        x = np.array(x, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.lib.orc_sor(ptr.size - 1, _p(ptr), _p(ind), _p(val), int(sym), _p(x), _p(b),
+                         float(omega), int(it), int(type_ssor))
+        return x
+
+    def solve(self, which, ptr, ind, val, b, x0=None, sym=False, precond=0, omega=1.0,
+              sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
+              hist_cap=0):
+        """which: 'cg' | 'bicgstab' | 'gmres'.  precond: 0 identity, 1 Jacobi, 2 SOR.
+        Returns (x, error_code, nb_iter, hist, hist_it)."""
+        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        m = ptr.size - 1
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        nb = ctypes.c_int(0)
+        hl = ctypes.c_int(0)
+        hist = np.zeros(max(hist_cap, 1))
+        hist_it = np.zeros(max(hist_cap, 1), dtype=np.int32)
+        code = self.lib.orc_solve(
+            w, m, ind.size, _p(ptr), _p(ind), _p(val), int(sym), int(precond), float(omega),
+            int(sor_iter), int(sor_sym), _p(x), _p(b), float(tol), int(max_iter), int(restart),
+            int(x0 is None), ctypes.byref(nb), _p(hist) if hist_cap else None,
+            _p(hist_it) if hist_cap else None, int(hist_cap), ctypes.byref(hl))
+        return x, code, nb.value, hist[:hl.value].copy(), hist_it[:hl.value].copy()
+
+
+class Reference(_Base):
+    """The reference compiled from its own headers (oracle/_ref)."""
+
+    @staticmethod
+    def available(path=REF_SO):
+        return os.path.exists(path)
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+        L = self.lib
+        L.ref_mltadd.argtypes = [_i, _i, _i, _vp, _vp, _vp, _i, _i, _d, _vp, _d, _vp]
+        L.ref_mltadd.restype = _i
+        L.ref_sor.argtypes = [_i, _i, _vp, _vp, _vp, _i, _vp, _vp, _d, _i, _i]
+        L.ref_sor.restype = _i
+        L.ref_solve.argtypes = [_i, _i, _i, _vp, _vp, _vp, _i, _i, _d, _i, _i, _vp, _vp, _d,
+                                _i, _i, _i, _i, _vp]
+        L.ref_solve.restype = _i
+        L.ref_dot.argtypes = [_i, _vp, _vp]
+        L.ref_dot.restype = _d
+        L.ref_norm2.argtypes = [_i, _vp]
+        L.ref_norm2.restype = _d
+        L.ref_genrot.argtypes = [_vp, _vp, _vp, _vp]
+        L.ref_genrot.restype = None
+
+    def mltadd(self, m, n, ptr, ind, val, alpha, x, beta, y, sym=False, trans=False):
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.array(y, dtype=np.float64, copy=True)
+        self.lib.ref_mltadd(m, n, ind.size, _p(ptr), _p(ind), _p(val), int(sym), int(trans),
+                            float(alpha), _p(x), float(beta), _p(y))
+        return y
+
+    def dot(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        return self.lib.ref_dot(x.size, _p(x), _p(y))
+
+    def nrm2(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.ref_norm2(x.size, _p(x))
+
+    def genrot(self, a, b):
+        v = np.array([a, b, 0.0, 0.0])
+        base = v.ctypes.data
+        self.lib.ref_genrot(base, base + 8, base + 16, base + 24)
+        return tuple(v)
+
+    def sor(self, ptr, ind, val, x, b, omega, it, type_ssor, sym=False):
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        x = np.array(x, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.lib.ref_sor(ptr.size - 1, ind.size, _p(ptr), _p(ind), _p(val), int(sym), _p(x),
+                         _p(b), float(omega), int(it), int(type_ssor))
+        return x
+
+    def solve(self, which, ptr, ind, val, b, x0=None, sym=False, precond=0, omega=1.0,
+              sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
+              print_level=0):
+        """Returns (x, error_code, nb_iter)."""
+        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        m = ptr.size - 1
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        nb = ctypes.c_int(0)
+        code = self.lib.ref_solve(w, m, ind.size, _p(ptr), _p(ind), _p(val), int(sym),
+                                  int(precond), float(omega), int(sor_iter), int(sor_sym),
+                                  _p(x), _p(b), float(tol), int(max_iter), int(restart),
+                                  int(x0 is None), int(print_level), ctypes.byref(nb))
+        return x, code, nb.value

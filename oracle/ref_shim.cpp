@@ -1,0 +1,236 @@
+// Thin C entry points over the UNMODIFIED reference (Seldon) templates.
+//
+// This file is test infrastructure: it is compiled, by oracle/Makefile, against
+// the Seldon headers where they lie in the reference tree, into
+// oracle/_ref/libseldon_ref*.so.  Only the test-suite and the CPU-baseline leg
+// of bench.py load it.  Every arithmetic step it runs is Seldon's own:
+//   MltAdd RowSparse        computation/basic_functions/Functions_MatVect.cxx:398-431
+//   MltAdd RowSymSparse     computation/basic_functions/Functions_MatVect.cxx:526-564
+//   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
+//   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
+//   SOR                     matrix_sparse/Relaxation_MatVect.cxx:41-95, 176-298
+//   SorPreconditioner       computation/solver/preconditioner/Precond_Ssor.cxx:24-90
+//
+// Two pieces are not in the reference and are supplied here:
+//   * Solve(ColUpTriang) - Gmres.cxx:166 needs it and Seldon only provides it
+//     through cblas (computation/interfaces/Blas_2.cxx:3226-3238).  The
+//     overload below is the netlib DTRSV column sweep (UPLO=U, TRANS=N,
+//     DIAG=N), the published reference-BLAS order.
+//   * JacobiPreconditioner - z_i = r_i / A(i,i), with A(i,i) read through
+//     Seldon's own Matrix_Sparse::operator() (Matrix_Sparse.cxx:1051-1083).
+//
+// Matrices and vectors wrap the caller's buffers through SetData/Nullify
+// (Matrix_Sparse.cxx:397-412), so nothing is copied.
+
+#include "Seldon.hxx"
+
+namespace Seldon
+{
+  // Back-substitution for the (i x i) upper-triangular GMRES Hessenberg.
+  template <class Prop0, class Allocator0, class Allocator1>
+  void Solve(const Matrix<double, Prop0, ColUpTriang, Allocator0>& A,
+             Vector<double, VectFull, Allocator1>& X)
+  {
+    int n = A.GetN();
+    for (int j = n - 1; j >= 0; j--)
+      if (X(j) != 0.0)
+        {
+          X(j) = X(j) / A(j, j);
+          double t = X(j);
+          for (int i = j - 1; i >= 0; i--)
+            X(i) = X(i) - t * A(i, j);
+        }
+  }
+}
+
+#include "SeldonSolver.hxx"
+
+using namespace Seldon;
+
+namespace
+{
+  typedef Matrix<double, General, RowSparse> GenMat;
+  typedef Matrix<double, Symmetric, RowSymSparse> SymMat;
+  typedef Vector<double> Vec;
+
+  struct Wrap
+  {
+    GenMat G;
+    SymMat S;
+    bool sym;
+    Wrap(int m, int n, int nnz, const int* ptr, const int* ind,
+         const double* val, int sym_)
+      : sym(sym_ != 0)
+    {
+      if (sym)
+        S.SetData(m, n, nnz, const_cast<double*>(val),
+                  const_cast<int*>(ptr), const_cast<int*>(ind));
+      else
+        G.SetData(m, n, nnz, const_cast<double*>(val),
+                  const_cast<int*>(ptr), const_cast<int*>(ind));
+    }
+    ~Wrap() { G.Nullify(); S.Nullify(); }
+  };
+
+  struct VWrap
+  {
+    Vec v;
+    VWrap(int n, const double* p) { v.SetData(n, const_cast<double*>(p)); }
+    ~VWrap() { v.Nullify(); }
+  };
+
+  // Jacobi preconditioner: the reference has none; it is written here in the
+  // shape of Preconditioner_Base (Iterative.hxx:24-39).
+  class JacobiPreconditioner
+  {
+  public:
+    Vec diag;
+    template <class Mat>
+    void Init(const Mat& A)
+    {
+      diag.Reallocate(A.GetM());
+      for (int i = 0; i < A.GetM(); i++)
+        diag(i) = A(i, i);
+    }
+    template <class Mat, class V>
+    void Solve(const Mat&, const V& r, V& z)
+    {
+      for (int i = 0; i < r.GetM(); i++)
+        z(i) = r(i) / diag(i);
+    }
+    template <class Mat, class V>
+    void TransSolve(const Mat& A, const V& r, V& z) { Solve(A, r, z); }
+  };
+
+  template <class Mat, class Prec>
+  int run_solver(int which, Mat& A, Vec& x, const Vec& b, Prec& M,
+                 Iteration<double>& it)
+  {
+    switch (which)
+      {
+      case 0: return Cg(A, x, b, M, it);
+      case 1: return BiCgStab(A, x, b, M, it);
+      case 2: return Gmres(A, x, b, M, it);
+      default: return -100;
+      }
+  }
+
+  template <class Mat>
+  int solve_mat(int which, Mat& A, int precond, double omega, int sor_iter,
+                int sor_sym, Vec& x, const Vec& b, double tol, int max_iter,
+                int restart, int init_guess_null, int print_level,
+                int* nb_iter)
+  {
+    Iteration<double> it(max_iter, tol);
+    it.SetRestart(restart);
+    it.SetInitGuess(init_guess_null != 0);
+    if (print_level <= 0)
+      it.HideMessages();
+    else if (print_level >= 6)
+      it.ShowFullHistory();
+    else
+      it.ShowMessages();
+    int code;
+    if (precond == 0)
+      {
+        Preconditioner_Base M;
+        code = run_solver(which, A, x, b, M, it);
+      }
+    else if (precond == 1)
+      {
+        JacobiPreconditioner M;
+        M.Init(A);
+        code = run_solver(which, A, x, b, M, it);
+      }
+    else
+      {
+        SorPreconditioner<double> M;
+        M.SetParameterRelaxation(omega);
+        M.SetNumberIterations(sor_iter);
+        if (sor_sym)
+          M.InitSymmetricPreconditioning();
+        else
+          M.InitUnSymmetricPreconditioning();
+        code = run_solver(which, A, x, b, M, it);
+      }
+    *nb_iter = it.GetNumberIteration();
+    return code;
+  }
+}
+
+extern "C"
+{
+  // Y = beta*Y + alpha*op(A)*X through Seldon's MltAdd.
+  int ref_mltadd(int m, int n, int nnz, const int* ptr, const int* ind,
+                 const double* val, int sym, int trans, double alpha,
+                 const double* x, double beta, double* y)
+  {
+    Wrap A(m, n, nnz, ptr, ind, val, sym);
+    int nx = trans ? m : n, ny = trans ? n : m;
+    VWrap X(nx, x), Y(ny, y);
+    if (sym)
+      {
+        if (trans)
+          MltAdd(alpha, SeldonTrans, A.S, X.v, beta, Y.v);
+        else
+          MltAdd(alpha, A.S, X.v, beta, Y.v);
+      }
+    else
+      {
+        if (trans)
+          MltAdd(alpha, SeldonTrans, A.G, X.v, beta, Y.v);
+        else
+          MltAdd(alpha, A.G, X.v, beta, Y.v);
+      }
+    return 0;
+  }
+
+  // Seldon's SOR sweeps (type 2 forward, 3 backward, 0 both).
+  int ref_sor(int m, int nnz, const int* ptr, const int* ind, const double* val,
+              int sym, double* x, const double* b, double omega, int iter,
+              int type_ssor)
+  {
+    Wrap A(m, m, nnz, ptr, ind, val, sym);
+    VWrap X(m, x), B(m, b);
+    if (sym)
+      SOR(A.S, X.v, B.v, omega, iter, type_ssor);
+    else
+      SOR(A.G, X.v, B.v, omega, iter, type_ssor);
+    return 0;
+  }
+
+  // which: 0 Cg, 1 BiCgStab, 2 Gmres.  precond: 0 identity, 1 Jacobi, 2 SOR.
+  // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
+  int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
+                const double* val, int sym, int precond, double omega,
+                int sor_iter, int sor_sym, double* x, const double* b,
+                double tol, int max_iter, int restart, int init_guess_null,
+                int print_level, int* nb_iter)
+  {
+    Wrap A(m, m, nnz, ptr, ind, val, sym);
+    VWrap X(m, x), B(m, b);
+    if (sym)
+      return solve_mat(which, A.S, precond, omega, sor_iter, sor_sym, X.v,
+                       B.v, tol, max_iter, restart, init_guess_null,
+                       print_level, nb_iter);
+    return solve_mat(which, A.G, precond, omega, sor_iter, sor_sym, X.v, B.v,
+                     tol, max_iter, restart, init_guess_null, print_level,
+                     nb_iter);
+  }
+
+  // Seldon's generic BLAS-1 loops (Functions_Vector.cxx), for pinning.
+  double ref_dot(int n, const double* x, const double* y)
+  {
+    VWrap X(n, x), Y(n, y);
+    return DotProd(X.v, Y.v);
+  }
+  double ref_norm2(int n, const double* x)
+  {
+    VWrap X(n, x);
+    return Norm2(X.v);
+  }
+  void ref_genrot(double* a, double* b, double* c, double* s)
+  {
+    GenRot(*a, *b, *c, *s);
+  }
+}

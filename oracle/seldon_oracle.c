@@ -1,0 +1,579 @@
+/*
+ * CPU restatement of Seldon's sparse Krylov path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * This is the oracle the GPU path is checked against.  Only tests/,
+ * __graft_entry__.smoke() and the CPU-baseline leg of bench.py load it; the
+ * product library never links or calls it.  It is pinned bit-for-bit against
+ * the reference itself (oracle/_ref/libseldon_ref.so, built from the Seldon
+ * headers by oracle/Makefile) and against golden vectors generated from the
+ * reference (tests/golden/).
+ *
+ * Each function restates one reference routine in plain C, keeping its exact
+ * floating-point operation order (compile with -ffp-contract=off so products
+ * and sums are rounded separately, as in the reference loops).  Citations are
+ * file:line within the Seldon tree.
+ *
+ * Conventions: CSR arrays are 0-based int32 (ptr[m+1], ind[nnz]); values and
+ * vectors are double.  A "sym" matrix stores only the upper triangle,
+ * diagonal included (matrix_sparse/Matrix_SymSparse.cxx:1031-1032).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  int m, n, nnz;
+  const int* ptr;
+  const int* ind;
+  const double* val;
+  int sym;
+} orc_csr;
+
+/* ---------------------------------------------------------------- BLAS-1 */
+
+/* Functions_Vector.cxx:69-74 -> Vector::operator*= : X(i) *= alpha. */
+void orc_scal(int n, double alpha, double* x) {
+  for (int i = 0; i < n; i++) x[i] *= alpha;
+}
+
+/* Functions_Vector.cxx:85-105: no-op when alpha == 0, else Y(i) += alpha*X(i). */
+void orc_axpy(int n, double alpha, const double* x, double* y) {
+  if (alpha == 0.0) return;
+  for (int i = 0; i < n; i++) y[i] += alpha * x[i];
+}
+
+/* Functions_Vector.cxx:240-246 (Y.Copy(X), vector/Vector.cxx:581-586). */
+void orc_copy(int n, const double* x, double* y) {
+  memcpy(y, x, (size_t)n * sizeof(double));
+}
+
+/* Functions_Vector.cxx:330-346: sequential sum from i = 0. */
+double orc_dot(int n, const double* x, const double* y) {
+  double v = 0.0;
+  for (int i = 0; i < n; i++) v += x[i] * y[i];
+  return v;
+}
+
+/* Functions_Vector.cxx:540-549: unscaled sqrt(sum x_i^2). */
+double orc_nrm2(int n, const double* x) {
+  double v = 0.0;
+  for (int i = 0; i < n; i++) v += x[i] * x[i];
+  return sqrt(v);
+}
+
+/* Functions_Vector.cxx:612-649: old-BLAS drotg semantics.  On exit *a = r,
+ * *b = z; r takes the sign of the larger-magnitude input. */
+void orc_genrot(double* a_in, double* b_in, double* c_, double* s_) {
+  double a = *a_in, b = *b_in;
+  double roe = (fabs(a) > fabs(b)) ? a : b;
+  double scal = fabs(a) + fabs(b);
+  double r, z;
+  if (scal != 0.0) {
+    double a_scl = a / scal;
+    double b_scl = b / scal;
+    r = scal * sqrt(a_scl * a_scl + b_scl * b_scl);
+    if (roe < 0.0) r *= -1.0;
+    *c_ = a / r;
+    *s_ = b / r;
+    z = 1.0;
+    if (fabs(a) > fabs(b))
+      z = *s_;
+    else if (fabs(b) >= fabs(a) && *c_ != 0.0)
+      z = 1.0 / *c_;
+  } else {
+    *c_ = 1.0;
+    *s_ = 0.0;
+    r = 0.0;
+    z = 0.0;
+  }
+  *a_in = r;
+  *b_in = z;
+}
+
+/* Functions_Vector.cxx:681-687. */
+void orc_applyrot(double* x, double* y, double c, double s) {
+  double temp = c * *x + s * *y;
+  *y = c * *y - s * *x;
+  *x = temp;
+}
+
+/* Upper-triangular back-substitution H y = s, H column-major with leading
+ * dimension ld.  Gmres.cxx:166 calls Solve(ColUpTriang), which Seldon routes
+ * to cblas_dtrsv (computation/interfaces/Blas_2.cxx:3226-3238); this is the
+ * netlib DTRSV column sweep (UPLO=U, TRANS=N, DIAG=N). */
+void orc_trsv_upper(int n, const double* H, int ld, double* s) {
+  for (int j = n - 1; j >= 0; j--)
+    if (s[j] != 0.0) {
+      s[j] = s[j] / H[j + (size_t)j * ld];
+      double t = s[j];
+      for (int i = j - 1; i >= 0; i--) s[i] = s[i] - t * H[i + (size_t)j * ld];
+    }
+}
+
+/* ---------------------------------------------------------------- SpMV */
+
+/* MltAdd on RowSparse, Functions_MatVect.cxx:398-431:
+ * Y *= beta (always, even for beta == 0), then Y(i) += alpha * sum_j. */
+void orc_mltadd_rowsparse(int m, const int* ptr, const int* ind,
+                          const double* val, double alpha, const double* x,
+                          double beta, double* y) {
+  orc_scal(m, beta, y);
+  for (int i = 0; i < m; i++) {
+    double temp = 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) temp += val[j] * x[ind[j]];
+    y[i] += alpha * temp;
+  }
+}
+
+/* MltAdd on RowSymSparse (upper stored), Functions_MatVect.cxx:526-564:
+ * row pass over the stored part, then a scatter of the strict upper part
+ * for rows i < m-1. */
+void orc_mltadd_rowsymsparse(int m, const int* ptr, const int* ind,
+                             const double* val, double alpha, const double* x,
+                             double beta, double* y) {
+  orc_scal(m, beta, y);
+  for (int i = 0; i < m; i++) {
+    double temp = 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) temp += val[j] * x[ind[j]];
+    y[i] += alpha * temp;
+  }
+  for (int i = 0; i < m - 1; i++)
+    for (int j = ptr[i]; j < ptr[i + 1]; j++)
+      if (ind[j] != i) y[ind[j]] += alpha * val[j] * x[i];
+}
+
+/* MltAdd(SeldonTrans) on RowSparse, Functions_MatVect.cxx:729-758:
+ * Y *= beta, then Y(ind[j]) += alpha * data[j] * X(i) row by row. */
+void orc_mltadd_rowsparse_trans(int m, int n, const int* ptr, const int* ind,
+                                const double* val, double alpha,
+                                const double* x, double beta, double* y) {
+  orc_scal(n, beta, y);
+  for (int i = 0; i < m; i++)
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) y[ind[j]] += alpha * val[j] * x[i];
+}
+
+/* C entry used by tests: sym/trans dispatch as in Functions_MatVect.cxx
+ * (RowSymSparse Trans reduces to NoTrans, :915-927). */
+void orc_mltadd(int m, int n, const int* ptr, const int* ind, const double* val,
+                int sym, int trans, double alpha, const double* x, double beta,
+                double* y) {
+  if (sym)
+    orc_mltadd_rowsymsparse(m, ptr, ind, val, alpha, x, beta, y);
+  else if (trans)
+    orc_mltadd_rowsparse_trans(m, n, ptr, ind, val, alpha, x, beta, y);
+  else
+    orc_mltadd_rowsparse(m, ptr, ind, val, alpha, x, beta, y);
+}
+
+static void csr_mlt(const orc_csr* A, const double* x, double* y) {
+  /* Mlt(M, X, Y): Y.Fill(0); MltAdd(1, M, X, 0, Y) -- Functions_MatVect.cxx:72-81 */
+  memset(y, 0, (size_t)A->m * sizeof(double));
+  orc_mltadd(A->m, A->n, A->ptr, A->ind, A->val, A->sym, 0, 1.0, x, 0.0, y);
+}
+
+static void csr_residual(const orc_csr* A, const double* x, double* r) {
+  /* MltAdd(-1, A, x, 1, r) */
+  orc_mltadd(A->m, A->n, A->ptr, A->ind, A->val, A->sym, 0, -1.0, x, 1.0, r);
+}
+
+/* Matrix_Sparse::operator()(i, i) lookup, Matrix_Sparse.cxx:1051-1083:
+ * advance while k < b-1 and ind[k] < i, then test ind[k] == i. */
+double orc_diag_entry(const int* ptr, const int* ind, const double* val, int i) {
+  int a = ptr[i], b = ptr[i + 1];
+  if (a == b) return 0.0;
+  int k = a;
+  while (k < b - 1 && ind[k] < i) k++;
+  return ind[k] == i ? val[k] : 0.0;
+}
+
+/* ---------------------------------------------------------------- SOR */
+
+/* SOR on RowSparse, Relaxation_MatVect.cxx:41-95. */
+void orc_sor_rowsparse(int m, const int* ptr, const int* ind, const double* val,
+                       double* x, const double* b, double omega, int iter,
+                       int type_ssor) {
+  if (type_ssor % 2 == 0)
+    for (int it = 0; it < iter; it++)
+      for (int j = 0; j < m; j++) {
+        double temp = 0.0;
+        double ajj = orc_diag_entry(ptr, ind, val, j);
+        for (int k = ptr[j]; k < ptr[j + 1]; k++) temp += val[k] * x[ind[k]];
+        temp = b[j] - temp + ajj * x[j];
+        x[j] = (1.0 - omega) * x[j] + omega * temp / ajj;
+      }
+  if (type_ssor % 3 == 0)
+    for (int it = 0; it < iter; it++)
+      for (int j = m - 1; j >= 0; j--) {
+        double temp = 0.0;
+        double ajj = orc_diag_entry(ptr, ind, val, j);
+        for (int k = ptr[j]; k < ptr[j + 1]; k++) temp += val[k] * x[ind[k]];
+        temp = b[j] - temp + ajj * x[j];
+        x[j] = (1.0 - omega) * x[j] + omega * temp / ajj;
+      }
+}
+
+/* SOR on RowSymSparse (upper stored), Relaxation_MatVect.cxx:176-298. */
+void orc_sor_rowsymsparse(int m, const int* ptr, const int* ind,
+                          const double* val, double* x, const double* b,
+                          double omega, int iter, int type_ssor) {
+  double* y = (double*)calloc((size_t)(m > 0 ? m : 1), sizeof(double));
+  if (type_ssor % 2 == 0)
+    for (int it = 0; it < iter; it++) {
+      for (int j = 0; j < m; j++) {
+        double temp = 0.0, ajj = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+          int p = ind[k];
+          double v = val[k];
+          if (p == j)
+            ajj += v;
+          else
+            temp += v * x[p];
+        }
+        temp = b[j] - temp;
+        x[j] = (1.0 - omega) / omega * ajj * x[j] + temp;
+      }
+      for (int j = 0; j < m; j++) {
+        double ajj = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; k++)
+          if (ind[k] == j) ajj += val[k];
+        x[j] *= omega / ajj;
+        for (int k = ptr[j]; k < ptr[j + 1]; k++)
+          if (ind[k] != j) x[ind[k]] -= val[k] * x[j];
+      }
+    }
+  if (type_ssor % 3 == 0)
+    for (int it = 0; it < iter; it++) {
+      memset(y, 0, (size_t)m * sizeof(double));
+      for (int j = 0; j < m; j++) {
+        double ajj = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+          int p = ind[k];
+          double v = val[k];
+          if (p == j)
+            ajj += v;
+          else
+            y[p] += v * x[j];
+        }
+        x[j] = (1.0 - omega) / omega * ajj * x[j] + b[j] - y[j];
+      }
+      for (int j = m - 1; j >= 0; j--) {
+        double temp = 0.0, ajj = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+          int p = ind[k];
+          double v = val[k];
+          if (p == j)
+            ajj += v;
+          else
+            temp += v * x[p];
+        }
+        x[j] = (x[j] - temp) * omega / ajj;
+      }
+    }
+  free(y);
+}
+
+void orc_sor(int m, const int* ptr, const int* ind, const double* val, int sym,
+             double* x, const double* b, double omega, int iter, int type_ssor) {
+  if (sym)
+    orc_sor_rowsymsparse(m, ptr, ind, val, x, b, omega, iter, type_ssor);
+  else
+    orc_sor_rowsparse(m, ptr, ind, val, x, b, omega, iter, type_ssor);
+}
+
+/* ---------------------------------------------------------------- Iteration */
+
+/* Iteration<Titer>, Iterative.hxx:47-108 / Iterative.cxx:80-354. */
+typedef struct {
+  double tolerance, facteur_reste;
+  int max_iter, nb_iter, error_code, fail_convergence, init_guess_null;
+  /* residual log: every Finished() call appends (nb_iter, relative residual). */
+  double* hist;
+  int* hist_it;
+  int hist_cap, hist_len;
+} orc_iter;
+
+static int it_init(orc_iter* it, int n, const double* r) {
+  /* Iterative.cxx:235-249 */
+  double nr = orc_nrm2(n, r);
+  if (nr == 0.0) return -1;
+  it->facteur_reste = 1.0 / nr;
+  it->nb_iter = 0;
+  return 0;
+}
+
+static int it_finished(orc_iter* it, double res) {
+  /* Iterative.cxx:299-319 (the vector form :272-295 is Norm2 then this). */
+  double reste = it->facteur_reste * res;
+  if (it->hist && it->hist_len < it->hist_cap) {
+    it->hist[it->hist_len] = reste;
+    it->hist_it[it->hist_len] = it->nb_iter;
+    it->hist_len++;
+  }
+  return (reste < it->tolerance) || (it->nb_iter >= it->max_iter);
+}
+
+static void it_fail(orc_iter* it, int code) {
+  /* Iterative.cxx:324-331 */
+  it->fail_convergence = 1;
+  it->error_code = code;
+}
+
+static int it_error_code(const orc_iter* it) {
+  /* Iterative.cxx:344-354 */
+  if (it->nb_iter >= it->max_iter) return -2;
+  if (it->fail_convergence) return it->error_code;
+  return 0;
+}
+
+/* ---------------------------------------------------------------- preconditioners */
+
+typedef struct {
+  int kind; /* 0 identity, 1 Jacobi, 2 SOR */
+  double omega;
+  int nb_iter, symmetric;
+  double* diag;
+} orc_prec;
+
+/* Preconditioner_Base::Solve = Copy (Iterative.cxx:60-65); Jacobi
+ * z_i = r_i / A(i,i) (not in the reference); SorPreconditioner::Solve zeros z
+ * then runs SOR type 0 (symmetric) or 2 (Precond_Ssor.cxx:62-74). */
+static void prec_solve(const orc_prec* M, const orc_csr* A, const double* r,
+                       double* z) {
+  int n = A->m;
+  if (M->kind == 0) {
+    orc_copy(n, r, z);
+  } else if (M->kind == 1) {
+    for (int i = 0; i < n; i++) z[i] = r[i] / M->diag[i];
+  } else {
+    memset(z, 0, (size_t)n * sizeof(double));
+    orc_sor(n, A->ptr, A->ind, A->val, A->sym, z, r, M->omega, M->nb_iter,
+            M->symmetric ? 0 : 2);
+  }
+}
+
+/* ---------------------------------------------------------------- solvers */
+
+/* Cg, computation/solver/iterative/Cg.cxx:45-116. */
+static int orc_cg_impl(const orc_csr* A, double* x, const double* b,
+                       const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  double rho = 1.0, rho_1 = 1.0, alpha, beta, delta;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *p = malloc(bytes), *q = malloc(bytes), *r = malloc(bytes),
+         *z = malloc(bytes);
+  memcpy(p, b, bytes); memcpy(q, b, bytes); memcpy(r, b, bytes); memcpy(z, b, bytes);
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r))) {
+    prec_solve(M, A, r, z);
+    rho = orc_dot(N, r, z);
+    if (rho == 0.0) { it_fail(it, 1); break; }
+    if (it->nb_iter == 0)
+      orc_copy(N, z, p);
+    else {
+      beta = rho / rho_1;
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, z, p);
+    }
+    csr_mlt(A, p, q);
+    delta = orc_dot(N, p, q);
+    if (delta == 0.0) { it_fail(it, 2); break; }
+    alpha = rho / delta;
+    orc_axpy(N, alpha, p, x);
+    orc_axpy(N, -alpha, q, r);
+    rho_1 = rho;
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  free(p); free(q); free(r); free(z);
+  return code;
+}
+
+/* BiCgStab, computation/solver/iterative/BiCgStab.cxx:43-145. */
+static int orc_bicgstab_impl(const orc_csr* A, double* x, const double* b,
+                             const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  double rho_1, rho_2 = 0.0, alpha = 0.0, beta, omega = 0.0, sigma;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *p = malloc(bytes), *phat = malloc(bytes), *s = malloc(bytes),
+         *shat = malloc(bytes), *t = malloc(bytes), *v = malloc(bytes),
+         *r = malloc(bytes), *rtilde = malloc(bytes);
+  double* all[8] = {p, phat, s, shat, t, v, r, rtilde};
+  for (int k = 0; k < 8; k++) memcpy(all[k], b, bytes);
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  orc_copy(N, r, rtilde);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r))) {
+    rho_1 = orc_dot(N, rtilde, r);
+    if (rho_1 == 0.0) { it_fail(it, 1); break; }
+    if (it->nb_iter == 0)
+      orc_copy(N, r, p);
+    else {
+      if (omega == 0.0) { it_fail(it, 2); break; }
+      beta = (rho_1 / rho_2) * (alpha / omega);
+      orc_axpy(N, -omega, v, p);
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, r, p);
+    }
+    prec_solve(M, A, p, phat);
+    csr_mlt(A, phat, v);
+    sigma = orc_dot(N, rtilde, v);
+    if (sigma == 0.0) { it_fail(it, 3); break; }
+    alpha = rho_1 / sigma;
+    orc_copy(N, r, s);
+    orc_axpy(N, -alpha, v, s);
+    it->nb_iter++;
+    if (it_finished(it, orc_nrm2(N, s))) {
+      orc_axpy(N, alpha, phat, x);
+      break;
+    }
+    prec_solve(M, A, s, shat);
+    csr_mlt(A, shat, t);
+    omega = orc_dot(N, t, s) / orc_dot(N, t, t);
+    orc_axpy(N, alpha, phat, x);
+    orc_axpy(N, omega, shat, x);
+    orc_copy(N, s, r);
+    orc_axpy(N, -omega, t, r);
+    rho_2 = rho_1;
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 8; k++) free(all[k]);
+  return code;
+}
+
+/* Gmres(m), computation/solver/iterative/Gmres.cxx:44-183.  Left
+ * preconditioning, modified Gram-Schmidt, Givens rotations; the Hessenberg is
+ * kept column-major in an (m+1)x(m+1) array. */
+static int orc_gmres_impl(const orc_csr* A, double* x, const double* b,
+                          const orc_prec* M, orc_iter* outer, int m) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  if (m < 1) m = 1;
+  size_t bytes = (size_t)N * sizeof(double);
+  int ld = m + 1;
+  double* V = calloc((size_t)(m + 1) * N, sizeof(double));
+  double* H = calloc((size_t)ld * ld, sizeof(double));
+  double *w = calloc(N, sizeof(double)), *r = calloc(N, sizeof(double)),
+         *u = calloc(N, sizeof(double));
+  double* s = calloc(m + 1, sizeof(double));
+  double* rc = calloc(m + 1, sizeof(double));
+  double* rs = calloc(m + 1, sizeof(double));
+  int code;
+
+  orc_copy(N, b, w);
+  if (!outer->init_guess_null)
+    csr_residual(A, x, w);
+  else
+    memset(x, 0, bytes);
+  prec_solve(M, A, w, r);
+  double beta = orc_nrm2(N, r);
+  if (it_init(outer, N, r) != 0) { code = it_error_code(outer); goto out; }
+
+  outer->nb_iter = 0;
+  while (!it_finished(outer, beta)) {
+    double* V0 = V;
+    orc_copy(N, r, V0);
+    orc_scal(N, 1.0 / beta, V0);
+    memset(s, 0, (size_t)(m + 1) * sizeof(double));
+    s[0] = beta;
+    int i = 0;
+    /* Iteration inner(outer): copies tolerance and facteur_reste; its
+     * max_iter is outer's count + m (Gmres.cxx:114-116). */
+    orc_iter inner = *outer;
+    inner.max_iter = outer->nb_iter + m;
+    int stop;
+    do {
+      double* Vi = V + (size_t)i * N;
+      csr_mlt(A, Vi, u);
+      prec_solve(M, A, u, w);
+      for (int k = 0; k <= i; k++) {
+        double h = orc_dot(N, V + (size_t)k * N, w);
+        H[k + (size_t)i * ld] = h;
+        orc_axpy(N, -h, V + (size_t)k * N, w);
+      }
+      double hi_ip1 = orc_nrm2(N, w);
+      double* Vn = V + (size_t)(i + 1) * N;
+      orc_copy(N, w, Vn);
+      if (hi_ip1 != 0.0) orc_scal(N, 1.0 / hi_ip1, Vn);
+      for (int k = 0; k < i; k++)
+        orc_applyrot(&H[k + (size_t)i * ld], &H[k + 1 + (size_t)i * ld], rc[k],
+                     rs[k]);
+      if (hi_ip1 != 0.0) {
+        orc_genrot(&H[i + (size_t)i * ld], &hi_ip1, &rc[i], &rs[i]);
+        orc_applyrot(&s[i], &s[i + 1], rc[i], rs[i]);
+      }
+      inner.nb_iter++;
+      outer->nb_iter++;
+      i++;
+      stop = it_finished(&inner, fabs(s[i]));
+    } while (!stop);
+    /* the inner log entries belong to the caller's history */
+    outer->hist_len = inner.hist_len;
+
+    orc_trsv_upper(i, H, ld, s);
+    for (int k = 0; k < i; k++) orc_axpy(N, s[k], V + (size_t)k * N, x);
+
+    orc_copy(N, b, w);
+    csr_residual(A, x, w);
+    prec_solve(M, A, w, r);
+    beta = orc_nrm2(N, r);
+  }
+  code = it_error_code(outer);
+out:
+  free(V); free(H); free(w); free(r); free(u); free(s); free(rc); free(rs);
+  return code;
+}
+
+/* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres.
+ * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
+ * hist/hist_it (may be NULL) receive the relative residual and iteration
+ * number of every Finished() test, hist_len their count.
+ * Returns Iteration::ErrorCode(); *nb_iter the final iteration count. */
+int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
+              const double* val, int sym, int precond, double omega,
+              int sor_iter, int sor_sym, double* x, const double* b, double tol,
+              int max_iter, int restart, int init_guess_null, int* nb_iter,
+              double* hist, int* hist_it, int hist_cap, int* hist_len) {
+  orc_csr A = {m, m, nnz, ptr, ind, val, sym};
+  orc_iter it;
+  memset(&it, 0, sizeof(it));
+  it.tolerance = tol;
+  it.max_iter = max_iter;
+  it.init_guess_null = init_guess_null;
+  it.hist = hist;
+  it.hist_it = hist_it;
+  it.hist_cap = hist ? hist_cap : 0;
+  orc_prec M = {precond, omega, sor_iter, sor_sym, NULL};
+  if (precond == 1) {
+    M.diag = malloc((size_t)(m > 0 ? m : 1) * sizeof(double));
+    for (int i = 0; i < m; i++) M.diag[i] = orc_diag_entry(ptr, ind, val, i);
+  }
+  int code;
+  if (which == 0)
+    code = orc_cg_impl(&A, x, b, &M, &it);
+  else if (which == 1)
+    code = orc_bicgstab_impl(&A, x, b, &M, &it);
+  else
+    code = orc_gmres_impl(&A, x, b, &M, &it, restart);
+  free(M.diag);
+  if (nb_iter) *nb_iter = it.nb_iter;
+  if (hist_len) *hist_len = it.hist_len;
+  return code;
+}

@@ -1,0 +1,131 @@
+"""ctypes binding of libseldon_b200.so (the C ABI in include/seldon_b200.h).
+
+The shared library is built in-tree (seldon_b200/libseldon_b200.so) by
+``seldon_b200.build.build_library()``.  There is no fallback: if the library
+is missing or fails to load, importing this module raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libseldon_b200.so")
+
+SB2_OK = 0
+SB2_ERR_INVALID_VALUE = -1
+SB2_ERR_NO_MEMORY = -2
+SB2_ERR_CUDA = -3
+SB2_ERR_TIMEOUT = -4
+SB2_ERR_INVALID_CSR = -5
+SB2_ERR_NOT_SUPPORTED = -6
+
+PRECOND_IDENTITY = 0
+PRECOND_JACOBI = 1
+PRECOND_SOR = 2
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_void_p = ctypes.c_void_p
+
+
+class IterParams(ctypes.Structure):
+    """sb2_iter_params: Seldon's Iteration<double> settings."""
+
+    _fields_ = [
+        ("tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
+        ("restart", ctypes.c_int),
+        ("print_level", ctypes.c_int),
+        ("init_guess_null", ctypes.c_int),
+    ]
+
+
+class IterResult(ctypes.Structure):
+    """sb2_iter_result: what a Krylov driver reports back."""
+
+    _fields_ = [
+        ("nb_iter", ctypes.c_int),
+        ("error_code", ctypes.c_int),
+        ("init_failed", ctypes.c_int),
+        ("hist_len", ctypes.c_int),
+        ("facteur_reste", ctypes.c_double),
+        ("last_residual", ctypes.c_double),
+    ]
+
+
+class SeldonB200Error(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = _lib.sb2_status_string(status).decode() if _lib else str(status)
+        super().__init__(f"{where}: status {status} ({msg})")
+
+
+# (name, restype, argtypes) of every exported entry point
+_PROTOS = [
+    ("sb2_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("sb2_version", ctypes.c_int, []),
+    ("sb2_set_wait_limit_ms", ctypes.c_int, [ctypes.c_int]),
+    ("sb2_csr_create", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p,
+      ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_void_p)]),
+    ("sb2_csr_destroy", ctypes.c_int, [c_void_p]),
+    ("sb2_csr_info", ctypes.c_int, [c_void_p, c_int_p, c_int_p, c_int_p, c_int_p]),
+    ("sb2_csr_download", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_spmv", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, ctypes.c_double, c_void_p, c_void_p]),
+    ("sb2_mlt", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    ("sb2_spmv_host", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, ctypes.c_double, c_void_p, c_void_p]),
+    ("sb2_mlt_host", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    ("sb2_dot", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_double_p, c_void_p]),
+    ("sb2_nrm2", ctypes.c_int, [ctypes.c_int, c_void_p, c_double_p, c_void_p]),
+    ("sb2_dot_device", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_nrm2_device", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_void_p]),
+    ("sb2_axpy", ctypes.c_int, [ctypes.c_int, ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    ("sb2_scal", ctypes.c_int, [ctypes.c_int, ctypes.c_double, c_void_p, c_void_p]),
+    ("sb2_copy", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_void_p]),
+    ("sb2_fill", ctypes.c_int, [ctypes.c_int, ctypes.c_double, c_void_p, c_void_p]),
+    ("sb2_precond_create", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+      ctypes.POINTER(c_void_p)]),
+    ("sb2_precond_destroy", ctypes.c_int, [c_void_p]),
+    ("sb2_precond_solve", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_precond_trans_solve", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_sor", ctypes.c_int,
+     [c_void_p, c_void_p, c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, c_void_p]),
+]
+
+_SOLVER_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParams),
+                ctypes.POINTER(IterResult), c_void_p, c_void_p, ctypes.c_int, c_void_p]
+for _name in ("sb2_cg", "sb2_bicgstab", "sb2_gmres"):
+    _PROTOS.append((_name, ctypes.c_int, _SOLVER_ARGS))
+
+_lib = None
+
+
+def load():
+    """Load the library (once) and attach prototypes.  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with seldon_b200.build.build_library() "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in _PROTOS:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_names():
+    return [p[0] for p in _PROTOS]
+
+
+def check(status, where):
+    if status != SB2_OK:
+        raise SeldonB200Error(status, where)

@@ -1,0 +1,354 @@
+"""Python mirror of Seldon's interface for the sparse Krylov path.
+
+Names, argument order and error behaviour follow the reference's free
+functions, so code written against Seldon reads the same here:
+
+    A = RowSparse(m, n, ptr, ind, val)            # Matrix<double, General, RowSparse>
+    S = RowSymSparse(m, ptr, ind, val)            # Matrix<double, Symmetric, RowSymSparse>
+    MltAdd(alpha, A, X, beta, Y)                  # Functions_MatVect.cxx:398-431
+    Mlt(A, X, Y); Mlt(alpha, X)                   # :72-130; Functions_Vector.cxx:69-74
+    DotProd(X, Y); Norm2(X); Add(alpha, X, Y); Copy(X, Y)
+    it = Iteration(max_iter, tol); Cg(A, x, b, M, it)   # Cg.cxx:45-116
+
+Vectors are device tensors (torch, float64, contiguous) -- torch is used only
+for device memory and streams; every operation runs in libseldon_b200.so.
+"""
+import ctypes
+
+from . import _lib
+from ._lib import IterParams, IterResult, check
+
+_L = _lib.load()
+
+
+def _stream(stream=None):
+    if stream is not None:
+        return ctypes.c_void_p(int(stream))
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev_ptr(t, n=None, name="vector"):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float64:
+        raise TypeError(f"{name}: expected a CUDA float64 tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: expected a contiguous tensor")
+    if n is not None and t.numel() != n:
+        raise ValueError(f"{name}: length {t.numel()} != {n} (WrongDim)")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RowSparse:
+    """Matrix<double, General, RowSparse> held on the device.
+
+    ptr/ind/val are host arrays in Seldon's layout (ptr_, ind_, data_); they
+    are copied, the caller keeps them."""
+
+    symmetric = False
+
+    def __init__(self, m, n, ptr, ind, val, validate=True):
+        import numpy as np
+        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+        ind = np.ascontiguousarray(ind, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        if ptr.size != m + 1 or ind.size != val.size:
+            raise ValueError("WrongDim: ptr must hold m+1 entries and ind/val nnz entries")
+        h = ctypes.c_void_p()
+        st = _L.sb2_csr_create(int(m), int(n), int(ind.size), _np_ptr(ptr), _np_ptr(ind),
+                               _np_ptr(val), int(self.symmetric), int(validate), ctypes.byref(h))
+        check(st, "sb2_csr_create")
+        self._h = h
+        self.m, self.n = int(m), int(n)
+        self.nnz_stored = int(ind.size)
+        full = ctypes.c_int()
+        _L.sb2_csr_info(h, None, None, None, ctypes.byref(full))
+        self.nnz_full = full.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def GetM(self):
+        return self.m
+
+    def GetN(self):
+        return self.n
+
+    def GetNonZeros(self):
+        return self.nnz_stored
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _L.sb2_csr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RowSymSparse(RowSparse):
+    """Matrix<double, Symmetric, RowSymSparse>: only the upper triangle
+    (diagonal included) is given (Matrix_SymSparse.cxx:1031-1032)."""
+
+    symmetric = True
+
+    def __init__(self, m, ptr, ind, val, validate=True):
+        super().__init__(m, m, ptr, ind, val, validate)
+
+
+SeldonNoTrans = 0
+SeldonTrans = 1
+
+
+def MltAdd(alpha, A, X, beta, Y, trans=SeldonNoTrans, stream=None):
+    """Y = beta*Y + alpha*op(A)*X (Y scaled by beta even when beta == 0)."""
+    nx, ny = (A.m, A.n) if trans else (A.n, A.m)
+    check(_L.sb2_spmv(A.handle, int(trans), float(alpha), _dev_ptr(X, nx, "X"), float(beta),
+                      _dev_ptr(Y, ny, "Y"), _stream(stream)), "MltAdd")
+
+
+def Mlt(*args, trans=SeldonNoTrans, stream=None):
+    """Mlt(A, X, Y): Y = A*X;  Mlt(alpha, A, X, Y): Y = alpha*A*X;
+    Mlt(alpha, X): X *= alpha."""
+    if len(args) == 2:
+        alpha, X = args
+        check(_L.sb2_scal(X.numel(), float(alpha), _dev_ptr(X), _stream(stream)), "Mlt")
+        return
+    if len(args) == 3:
+        alpha, (A, X, Y) = 1.0, args
+    else:
+        alpha, A, X, Y = args
+    nx, ny = (A.m, A.n) if trans else (A.n, A.m)
+    check(_L.sb2_mlt(A.handle, int(trans), float(alpha), _dev_ptr(X, nx, "X"),
+                     _dev_ptr(Y, ny, "Y"), _stream(stream)), "Mlt")
+
+
+def DotProd(X, Y, stream=None):
+    out = ctypes.c_double()
+    check(_L.sb2_dot(X.numel(), _dev_ptr(X), _dev_ptr(Y, X.numel(), "Y"), ctypes.byref(out),
+                     _stream(stream)), "DotProd")
+    return out.value
+
+
+DotProdConj = DotProd
+
+
+def Norm2(X, stream=None):
+    out = ctypes.c_double()
+    check(_L.sb2_nrm2(X.numel(), _dev_ptr(X), ctypes.byref(out), _stream(stream)), "Norm2")
+    return out.value
+
+
+def Add(alpha, X, Y, stream=None):
+    """Y += alpha*X (no-op when alpha == 0)."""
+    check(_L.sb2_axpy(X.numel(), float(alpha), _dev_ptr(X), _dev_ptr(Y, X.numel(), "Y"),
+                      _stream(stream)), "Add")
+
+
+def Copy(X, Y, stream=None):
+    check(_L.sb2_copy(X.numel(), _dev_ptr(X), _dev_ptr(Y, X.numel(), "Y"), _stream(stream)),
+          "Copy")
+
+
+def Fill(X, value, stream=None):
+    check(_L.sb2_fill(X.numel(), float(value), _dev_ptr(X), _stream(stream)), "Fill")
+
+
+# ------------------------------------------------------------------ preconditioners
+
+class Preconditioner_Base:
+    """Identity preconditioner (Iterative.cxx:50-77)."""
+
+    kind = _lib.PRECOND_IDENTITY
+
+    def handle_for(self, A):
+        return None
+
+
+class _DevicePrecond:
+    kind = None
+
+    def __init__(self):
+        self._cache = {}
+
+    def _params(self):
+        return 1.0, 1, 1
+
+    def handle_for(self, A):
+        key = id(A)
+        ent = self._cache.get(key)
+        if ent is None or ent[0] is not A or ent[2] != self._params():
+            omega, nb, sym = self._params()
+            h = ctypes.c_void_p()
+            check(_L.sb2_precond_create(A.handle, self.kind, float(omega), int(nb), int(sym),
+                                        ctypes.byref(h)), "sb2_precond_create")
+            if ent is not None:
+                _L.sb2_precond_destroy(ent[1])
+            ent = (A, h, self._params())
+            self._cache[key] = ent
+        return ent[1]
+
+    def Solve(self, A, r, z, stream=None):
+        check(_L.sb2_precond_solve(self.handle_for(A), _dev_ptr(r, A.m, "r"),
+                                   _dev_ptr(z, A.m, "z"), _stream(stream)), "Solve")
+
+    def TransSolve(self, A, r, z, stream=None):
+        check(_L.sb2_precond_trans_solve(self.handle_for(A), _dev_ptr(r, A.m, "r"),
+                                         _dev_ptr(z, A.m, "z"), _stream(stream)), "TransSolve")
+
+    def __del__(self):
+        try:
+            for _, h, _p in self._cache.values():
+                _L.sb2_precond_destroy(h)
+        except Exception:
+            pass
+
+
+class JacobiPreconditioner(_DevicePrecond):
+    """z_i = r_i / A(i,i).  The reference has no Jacobi preconditioner; this
+    one has the shape of Preconditioner_Base (Iterative.hxx:24-39)."""
+
+    kind = _lib.PRECOND_JACOBI
+
+
+class SorPreconditioner(_DevicePrecond):
+    """SorPreconditioner<double> (Precond_Ssor.cxx:24-90): omega 1, one
+    sweep, symmetric by default."""
+
+    kind = _lib.PRECOND_SOR
+
+    def __init__(self):
+        super().__init__()
+        self.omega, self.nb_iter, self.symmetric = 1.0, 1, True
+
+    def InitSymmetricPreconditioning(self):
+        self.symmetric = True
+
+    def InitUnSymmetricPreconditioning(self):
+        self.symmetric = False
+
+    def SetParameterRelaxation(self, omega):
+        self.omega = float(omega)
+
+    def SetNumberIterations(self, n):
+        self.nb_iter = int(n)
+
+    def _params(self):
+        return self.omega, self.nb_iter, int(self.symmetric)
+
+
+def SOR(A, X, B, omega, iter, type_ssor=2, stream=None):
+    """In-place relaxation (Relaxation_MatVect.cxx:41-95, :176-298)."""
+    check(_L.sb2_sor(A.handle, _dev_ptr(X, A.m, "X"), _dev_ptr(B, A.m, "B"), float(omega),
+                     int(iter), int(type_ssor), _stream(stream)), "SOR")
+
+
+# ------------------------------------------------------------------ Iteration
+
+class Iteration:
+    """Iteration<double> (Iterative.hxx:47-108): defaults tol 1e-6,
+    max_iter 100, restart 10, print level 1, null initial guess."""
+
+    def __init__(self, max_iteration=100, tol=1e-6):
+        self.tolerance = float(tol)
+        self.max_iter = int(max_iteration)
+        self.parameter_restart = 10
+        self.print_level = 1
+        self.init_guess_null = True
+        self.nb_iter = 0
+        self.error_code = 0
+        self.facteur_reste = 0.0
+        self.history = []      # (iteration, relative residual) of each Finished() test
+        self.init_failed = False
+
+    def SetRestart(self, m):
+        self.parameter_restart = int(m)
+
+    def GetRestart(self):
+        return self.parameter_restart
+
+    def SetTolerance(self, tol):
+        self.tolerance = float(tol)
+
+    def GetTolerance(self):
+        return self.tolerance
+
+    def SetMaxNumberIteration(self, n):
+        self.max_iter = int(n)
+
+    def GetNumberIteration(self):
+        return self.nb_iter
+
+    def SetNumberIteration(self, n):
+        self.nb_iter = int(n)
+
+    def GetFactor(self):
+        return self.facteur_reste
+
+    def ShowMessages(self):
+        self.print_level = 1
+
+    def ShowFullHistory(self):
+        self.print_level = 6
+
+    def HideMessages(self):
+        self.print_level = 0
+
+    def SetInitGuess(self, null):
+        self.init_guess_null = bool(null)
+
+    def IsInitGuess_Null(self):
+        return self.init_guess_null
+
+    def ErrorCode(self):
+        return self.error_code
+
+    def _replay(self):
+        # the lines Iteration::Finished prints (Iterative.cxx:282-287)
+        for it, res in self.history:
+            if (self.print_level >= 1 and it % 100 == 0) or self.print_level >= 6:
+                print(f"Residu at iteration number {it}  {res:g}")
+
+
+def _solve(fn, A, x, b, M, iteration, hist_cap, stream):
+    import numpy as np
+    params = IterParams(iteration.tolerance, iteration.max_iter, iteration.parameter_restart,
+                        iteration.print_level, int(iteration.init_guess_null))
+    res = IterResult()
+    cap = int(hist_cap if hist_cap is not None else max(iteration.max_iter * 2 + 8, 16))
+    hist = np.zeros(cap)
+    hist_it = np.zeros(cap, dtype=np.int32)
+    Mh = None if M is None else M.handle_for(A)
+    st = fn(A.handle, Mh, _dev_ptr(x, A.m, "x"), _dev_ptr(b, A.m, "b"), ctypes.byref(params),
+            ctypes.byref(res), _np_ptr(hist), _np_ptr(hist_it), cap, _stream(stream))
+    check(st, fn.__name__)
+    iteration.nb_iter = res.nb_iter
+    iteration.error_code = res.error_code
+    iteration.facteur_reste = res.facteur_reste
+    iteration.init_failed = bool(res.init_failed)
+    iteration.history = list(zip(hist_it[:res.hist_len].tolist(), hist[:res.hist_len].tolist()))
+    iteration._replay()
+    return res.error_code
+
+
+def Cg(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Preconditioned CG (Cg.cxx:45-116); returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_cg, A, x, b, M, iteration, hist_cap, stream)
+
+
+def BiCgStab(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """BiCGSTAB (BiCgStab.cxx:43-145); returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_bicgstab, A, x, b, M, iteration, hist_cap, stream)
+
+
+def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183)."""
+    return _solve(_L.sb2_gmres, A, x, b, M, iteration, hist_cap, stream)

@@ -1,0 +1,263 @@
+// Device CSR handle: upload, validation, symmetric expansion, row-block
+// partition, lazy transpose and diagonal.
+#include <algorithm>
+#include <cstring>
+
+#include "sb2_internal.cuh"
+
+namespace sb2 {
+
+static int validate_csr(int m, int n, int nnz, const int* ptr, const int* ind,
+                        int upper) {
+  // Matrix_Sparse.cxx:118-170 (SELDON_CHECK_DIMENSIONS) plus the index checks
+  // a device kernel needs to stay in bounds.
+  if (ptr[0] != 0 || ptr[m] != nnz) return SB2_ERR_INVALID_CSR;
+  for (int i = 0; i < m; i++) {
+    if (ptr[i + 1] < ptr[i]) return SB2_ERR_INVALID_CSR;
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      const int j = ind[k];
+      if (j < 0 || j >= n) return SB2_ERR_INVALID_CSR;
+      if (upper && j < i) return SB2_ERR_INVALID_CSR;
+    }
+  }
+  return SB2_OK;
+}
+
+// Full operator from the stored upper triangle.  Row i lists first the
+// mirrored strict-upper entries of rows k < i (increasing k), then row i's
+// stored entries in stored order.
+static void expand_symmetric(int m, const int* ptr, const int* ind,
+                             const double* val, std::vector<int>& fptr,
+                             std::vector<int>& find, std::vector<double>& fval) {
+  std::vector<int> lower_cnt(m + 1, 0);
+  for (int i = 0; i < m; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++)
+      if (ind[k] != i) lower_cnt[ind[k]]++;
+  fptr.assign(m + 1, 0);
+  for (int i = 0; i < m; i++) fptr[i + 1] = fptr[i] + lower_cnt[i] + (ptr[i + 1] - ptr[i]);
+  const long long total = fptr[m];
+  find.resize(total);
+  fval.resize(total);
+  std::vector<int> fill(m);
+  for (int i = 0; i < m; i++) fill[i] = fptr[i];
+  // mirrored entries, visited in increasing source row -> increasing k per row
+  for (int i = 0; i < m; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      const int j = ind[k];
+      if (j != i) {
+        find[fill[j]] = i;
+        fval[fill[j]] = val[k];
+        fill[j]++;
+      }
+    }
+  for (int i = 0; i < m; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      find[fill[i]] = ind[k];
+      fval[fill[i]] = val[k];
+      fill[i]++;
+    }
+}
+
+int build_partition_host(const int* ptr, int rows, Partition* out) {
+  std::vector<int> blk;
+  std::vector<unsigned char> kind;
+  blk.reserve(rows / 64 + 16);
+  int r = 0;
+  while (r < rows) {
+    const int len0 = ptr[r + 1] - ptr[r];
+    if (len0 > kLongRow) {
+      blk.push_back(r);
+      kind.push_back(kBlkLong);
+      r++;
+      continue;
+    }
+    const int start = r;
+    int nnz = 0, maxlen = 0;
+    while (r < rows && r - start < kRowCap) {
+      const int len = ptr[r + 1] - ptr[r];
+      if (len > kLongRow || nnz + len > kNnzCap) break;
+      nnz += len;
+      maxlen = std::max(maxlen, len);
+      r++;
+    }
+    blk.push_back(start);
+    kind.push_back(maxlen <= kThreadRowMax ? kBlkThread : kBlkWarp);
+  }
+  blk.push_back(rows);
+  out->nblk = (int)kind.size();
+  SB2_CUDA_TRY(cudaMalloc(&out->d_blk, sizeof(int) * blk.size()));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_blk, blk.data(), sizeof(int) * blk.size(), cudaMemcpyHostToDevice));
+  if (out->nblk > 0) {
+    SB2_CUDA_TRY(cudaMalloc(&out->d_kind, kind.size()));
+    SB2_CUDA_TRY(cudaMemcpy(out->d_kind, kind.data(), kind.size(), cudaMemcpyHostToDevice));
+  }
+  return SB2_OK;
+}
+
+int upload_csr(int rows, int cols, const int* ptr, const int* ind,
+               const double* val, CsrArrays* out) {
+  out->rows = rows;
+  out->cols = cols;
+  out->nnz = ptr[rows];
+  const long long cap = padded_nnz(out->nnz);
+  SB2_CUDA_TRY(cudaMalloc(&out->d_ptr, sizeof(int) * (rows + 1)));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_ind, sizeof(int) * cap));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_val, sizeof(double) * cap));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_ptr, ptr, sizeof(int) * (rows + 1), cudaMemcpyHostToDevice));
+  // padding: column 0 with value 0 keeps every speculative vector load valid
+  SB2_CUDA_TRY(cudaMemset(out->d_ind, 0, sizeof(int) * cap));
+  SB2_CUDA_TRY(cudaMemset(out->d_val, 0, sizeof(double) * cap));
+  if (out->nnz > 0) {
+    SB2_CUDA_TRY(cudaMemcpy(out->d_ind, ind, sizeof(int) * out->nnz, cudaMemcpyHostToDevice));
+    SB2_CUDA_TRY(cudaMemcpy(out->d_val, val, sizeof(double) * out->nnz, cudaMemcpyHostToDevice));
+  }
+  return build_partition_host(ptr, rows, &out->part);
+}
+
+void free_csr(CsrArrays* a) {
+  cudaFree(a->d_ptr);
+  cudaFree(a->d_ind);
+  cudaFree(a->d_val);
+  cudaFree(a->part.d_blk);
+  cudaFree(a->part.d_kind);
+  *a = CsrArrays();
+}
+
+// A^T as a CSR (= CSC of A), entries of each column in increasing row order.
+int ensure_transpose(const sb2_csr* cA) {
+  sb2_csr* A = const_cast<sb2_csr*>(cA);
+  std::lock_guard<std::mutex> g(A->mu);
+  if (A->trans.d_ptr) return SB2_OK;
+  const CsrArrays& f = A->full;
+  std::vector<int> ptr(f.rows + 1), ind(f.nnz);
+  std::vector<double> val(f.nnz);
+  SB2_CUDA_TRY(cudaMemcpy(ptr.data(), f.d_ptr, sizeof(int) * (f.rows + 1), cudaMemcpyDeviceToHost));
+  if (f.nnz) {
+    SB2_CUDA_TRY(cudaMemcpy(ind.data(), f.d_ind, sizeof(int) * f.nnz, cudaMemcpyDeviceToHost));
+    SB2_CUDA_TRY(cudaMemcpy(val.data(), f.d_val, sizeof(double) * f.nnz, cudaMemcpyDeviceToHost));
+  }
+  std::vector<int> tptr(f.cols + 1, 0), tind(f.nnz);
+  std::vector<double> tval(f.nnz);
+  for (long long k = 0; k < f.nnz; k++) tptr[ind[k] + 1]++;
+  for (int c = 0; c < f.cols; c++) tptr[c + 1] += tptr[c];
+  std::vector<int> fill(tptr.begin(), tptr.end() - 1);
+  for (int i = 0; i < f.rows; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      const int p = fill[ind[k]]++;
+      tind[p] = i;
+      tval[p] = val[k];
+    }
+  return upload_csr(f.cols, f.rows, tptr.data(), tind.data(), tval.data(), &A->trans);
+}
+
+__global__ void diag_kernel(int m, const int* __restrict__ ptr,
+                            const int* __restrict__ ind,
+                            const double* __restrict__ val, double* d) {
+  // Matrix_Sparse::operator()(i, i) (Matrix_Sparse.cxx:1051-1083): advance
+  // while k < b-1 and ind[k] < i, then test ind[k] == i.
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  int a = ptr[i], b = ptr[i + 1];
+  double v = 0.0;
+  if (a != b) {
+    int k = a;
+    while (k < b - 1 && ind[k] < i) k++;
+    if (ind[k] == i) v = val[k];
+  }
+  d[i] = v;
+}
+
+int ensure_diag(const sb2_csr* cA) {
+  sb2_csr* A = const_cast<sb2_csr*>(cA);
+  std::lock_guard<std::mutex> g(A->mu);
+  if (A->d_diag) return SB2_OK;
+  double* d = nullptr;
+  SB2_CUDA_TRY(cudaMalloc(&d, sizeof(double) * std::max(A->m, 1)));
+  // The symmetric lookup scans the stored (upper) row, whose first entry is
+  // the diagonal when present; the general lookup scans the full row.
+  const CsrArrays& src = A->sym ? A->upper : A->full;
+  if (A->m > 0)
+    diag_kernel<<<(A->m + 255) / 256, 256>>>(A->m, src.d_ptr, src.d_ind, src.d_val, d);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return map_cuda_error(e);
+  }
+  A->d_diag = d;
+  return SB2_OK;
+}
+
+}  // namespace sb2
+
+using namespace sb2;
+
+extern "C" {
+
+int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
+                   const double* val, int symmetric_upper, int validate,
+                   sb2_csr** out) {
+  if (!out || m < 0 || n < 0 || nnz < 0 || !ptr) return SB2_ERR_INVALID_VALUE;
+  if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
+  if (symmetric_upper && m != n) return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  if (validate) SB2_TRY(validate_csr(m, n, nnz, ptr, ind, symmetric_upper));
+  else if (ptr[m] != nnz) return SB2_ERR_INVALID_CSR;
+
+  sb2_csr* A = new sb2_csr();
+  A->device = current_device();
+  A->m = m;
+  A->n = n;
+  A->nnz_stored = nnz;
+  A->sym = symmetric_upper ? 1 : 0;
+  int st;
+  if (A->sym) {
+    std::vector<int> fptr, find;
+    std::vector<double> fval;
+    expand_symmetric(m, ptr, ind, val, fptr, find, fval);
+    st = upload_csr(m, n, fptr.data(), find.data(), fval.data(), &A->full);
+    if (st == SB2_OK) st = upload_csr(m, n, ptr, ind, val, &A->upper);
+  } else {
+    st = upload_csr(m, n, ptr, ind, val, &A->full);
+  }
+  if (st != SB2_OK) {
+    sb2_csr_destroy(A);
+    return st;
+  }
+  A->nnz = A->full.nnz;
+  *out = A;
+  return SB2_OK;
+}
+
+int sb2_csr_destroy(sb2_csr* A) {
+  if (!A) return SB2_OK;
+  int prev = current_device();
+  cudaSetDevice(A->device);
+  free_csr(&A->full);
+  free_csr(&A->upper);
+  free_csr(&A->trans);
+  cudaFree(A->d_diag);
+  cudaFree(A->d_val32);
+  cudaSetDevice(prev);
+  delete A;
+  return SB2_OK;
+}
+
+int sb2_csr_info(const sb2_csr* A, int* m, int* n, int* nnz_stored, int* nnz_full) {
+  if (!A) return SB2_ERR_INVALID_VALUE;
+  if (m) *m = A->m;
+  if (n) *n = A->n;
+  if (nnz_stored) *nnz_stored = A->nnz_stored;
+  if (nnz_full) *nnz_full = (int)A->nnz;
+  return SB2_OK;
+}
+
+int sb2_csr_download(const sb2_csr* A, int* ptr, int* ind, double* val) {
+  if (!A) return SB2_ERR_INVALID_VALUE;
+  const CsrArrays& s = A->sym ? A->upper : A->full;
+  if (ptr) SB2_CUDA_TRY(cudaMemcpy(ptr, s.d_ptr, sizeof(int) * (A->m + 1), cudaMemcpyDeviceToHost));
+  if (ind && s.nnz) SB2_CUDA_TRY(cudaMemcpy(ind, s.d_ind, sizeof(int) * s.nnz, cudaMemcpyDeviceToHost));
+  if (val && s.nnz) SB2_CUDA_TRY(cudaMemcpy(val, s.d_val, sizeof(double) * s.nnz, cudaMemcpyDeviceToHost));
+  return SB2_OK;
+}
+
+}  // extern "C"

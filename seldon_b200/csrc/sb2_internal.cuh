@@ -1,0 +1,187 @@
+// Internal declarations shared by the libseldon_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "seldon_b200.h"
+
+namespace sb2 {
+
+// ----------------------------------------------------------------- status
+
+#define SB2_CUDA_TRY(expr)                                   \
+  do {                                                       \
+    cudaError_t e_ = (expr);                                 \
+    if (e_ != cudaSuccess) return ::sb2::map_cuda_error(e_); \
+  } while (0)
+
+#define SB2_TRY(expr)          \
+  do {                         \
+    int s_ = (expr);           \
+    if (s_ != SB2_OK) return s_; \
+  } while (0)
+
+int map_cuda_error(cudaError_t e);
+
+// ----------------------------------------------------------------- tuning
+
+// SpMV row-block partition.  A block is either a run of consecutive rows whose
+// nonzeros (<= kNnzCap) are streamed once through shared memory, or a single
+// long row handled by the whole CTA.
+constexpr int kSpmvThreads = 256;
+constexpr int kNnzCap = 2048;      // nonzeros staged per stream block
+constexpr int kRowCap = 1024;      // rows per stream block
+constexpr int kLongRow = 512;      // rows longer than this get a CTA each
+constexpr int kThreadRowMax = 24;  // longest row for thread-per-row reduction
+
+enum BlockKind : unsigned char { kBlkThread = 0, kBlkWarp = 1, kBlkLong = 2 };
+
+// Device arrays are padded so 16-byte vector loads of ind/val never leave
+// the allocation: capacity rounded up to 4 plus one spare group.
+inline long long padded_nnz(long long nnz) { return ((nnz + 3) / 4) * 4 + 4; }
+
+// ----------------------------------------------------------------- matrix
+
+struct Partition {
+  int nblk = 0;
+  int* d_blk = nullptr;             // [nblk+1] first row of each block
+  unsigned char* d_kind = nullptr;  // [nblk]
+};
+
+struct CsrArrays {
+  int rows = 0, cols = 0;
+  long long nnz = 0;
+  int* d_ptr = nullptr;     // [rows+1]
+  int* d_ind = nullptr;     // [padded_nnz]
+  double* d_val = nullptr;  // [padded_nnz]
+  Partition part;
+};
+
+}  // namespace sb2
+
+struct sb2_csr {
+  int device = 0;
+  int m = 0, n = 0;
+  int nnz_stored = 0;  // as given (upper part for symmetric)
+  long long nnz = 0;   // nonzeros of the full operator
+  int sym = 0;
+  sb2::CsrArrays full;    // the operator (symmetric input expanded)
+  sb2::CsrArrays upper;   // stored upper part (symmetric only; SOR semantics)
+  sb2::CsrArrays trans;   // A^T (built on first transposed product)
+  double* d_diag = nullptr;  // A(i,i) by Seldon's lookup rule (lazy)
+  float* d_val32 = nullptr;  // FP32 copy of full.d_val (lazy)
+  std::mutex mu;             // guards the lazy members
+};
+
+namespace sb2 {
+
+// ----------------------------------------------------------------- helpers
+
+int upload_csr(int rows, int cols, const int* ptr, const int* ind,
+               const double* val, CsrArrays* out);
+void free_csr(CsrArrays* a);
+int build_partition_host(const int* ptr, int rows, Partition* out);
+int ensure_transpose(const sb2_csr* A);
+int ensure_diag(const sb2_csr* A);
+
+// Per-(device, stream) scratch for reductions: kRedSlots partial sums and a
+// completion counter that the last CTA resets to zero.
+constexpr int kRedMaxBlocks = 1184;
+struct RedScratch {
+  double* partials = nullptr;  // [kRedMaxBlocks * 4]
+  unsigned* counter = nullptr;
+  double* result = nullptr;    // [8] device results of host-returning calls
+};
+int get_red_scratch(cudaStream_t s, RedScratch** out);
+
+int current_device();
+int num_sms(int device);
+
+// Launch y = beta*y + alpha*A*x (overwrite: y = alpha*A*x) on a CSR operator.
+int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
+                double* y, bool overwrite, cudaStream_t s);
+
+extern int g_wait_limit_ms;
+
+// ----------------------------------------------------------------- device code
+
+#ifdef __CUDACC__
+
+// Products and sums rounded separately (no FMA contraction), matching the
+// reference loops compiled without contraction.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+  // Fixed tree: lane 0 ends with ((v0+v16)+(v8+v24))... for every call.
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = add_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Deterministic block sum; the result is valid in thread 0 only.  `red` must
+// hold NT/32 elements of shared memory.
+template <int NT, typename T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < NT / 32) ? red[lane] : T(0);
+    v = warp_sum(v);
+  }
+  __syncthreads();
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;"
+               : "=r"(old)
+               : "l"(p), "r"(v)
+               : "memory");
+  return old;
+}
+
+// Streaming loads of the matrix (read once per product: evict first).
+__device__ __forceinline__ int4 ld_stream_int4(const int* p) {
+  return __ldcs(reinterpret_cast<const int4*>(p));
+}
+__device__ __forceinline__ void ld_stream_val4(const double* p, double v[4]) {
+  double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+  double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld_stream_val4(const float* p, float v[4]) {
+  float4 a = __ldcs(reinterpret_cast<const float4*>(p));
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace sb2

@@ -1,0 +1,125 @@
+// Standalone SpMV: MltAdd / Mlt on device and host vectors.
+#include "spmv_core.cuh"
+
+namespace sb2 {
+
+// y = beta*y + alpha*t (MltAdd: Mlt(beta, Y) then Y(i) += alpha*temp,
+// Functions_MatVect.cxx:414, :428) or y = alpha*t (Mlt: Y.Fill(0) first,
+// Functions_MatVect.cxx:72-81).
+struct EpiAxpby {
+  double alpha, beta;
+  double* __restrict__ y;
+  bool overwrite;
+  __device__ __forceinline__ void operator()(int r, double t) const {
+    double v = mul_rn(alpha, t);
+    if (!overwrite) v = add_rn(mul_rn(beta, y[r]), v);
+    y[r] = v;
+  }
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT) spmv_kernel(
+    const int* __restrict__ ptr, const int* __restrict__ ind,
+    const double* __restrict__ val, const int* __restrict__ blk,
+    const unsigned char* __restrict__ kind, double alpha,
+    const double* __restrict__ x, double beta, double* __restrict__ y,
+    bool overwrite) {
+  __shared__ double s_prod[kNnzCap];
+  __shared__ double s_red[NT / 32];
+  const int b = blockIdx.x;
+  EpiAxpby epi{alpha, beta, y, overwrite};
+  XLoadLdg<double> xl{x};
+  spmv_row_block<NT, double, double>(ptr, ind, val, blk[b], blk[b + 1], kind[b],
+                                     xl, epi, s_prod, s_red);
+}
+
+int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
+                double* y, bool overwrite, cudaStream_t s) {
+  if (a.rows == 0) return SB2_OK;
+  spmv_kernel<kSpmvThreads><<<a.part.nblk, kSpmvThreads, 0, s>>>(
+      a.d_ptr, a.d_ind, a.d_val, a.part.d_blk, a.part.d_kind, alpha, x, beta,
+      y, overwrite);
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const char* pa = static_cast<const char*>(a);
+  const char* pb = static_cast<const char*>(b);
+  return pa < pb + nb && pb < pa + na;
+}
+
+static int spmv_common(const sb2_csr* A, int trans, double alpha,
+                       const double* x, double beta, double* y, bool overwrite,
+                       cudaStream_t s) {
+  if (!A || (!x && (trans ? A->m : A->n) > 0) || (!y && (trans ? A->n : A->m) > 0))
+    return SB2_ERR_INVALID_VALUE;
+  const int nx = trans ? A->m : A->n, ny = trans ? A->n : A->m;
+  if (nx > 0 && ny > 0 && overlaps(x, sizeof(double) * nx, y, sizeof(double) * ny))
+    return SB2_ERR_INVALID_VALUE;
+  // A symmetric operator is its own transpose (Functions_MatVect.cxx:915-927).
+  if (trans && !A->sym) {
+    SB2_TRY(ensure_transpose(A));
+    return launch_spmv(A->trans, alpha, x, beta, y, overwrite, s);
+  }
+  return launch_spmv(A->full, alpha, x, beta, y, overwrite, s);
+}
+
+}  // namespace sb2
+
+using namespace sb2;
+
+extern "C" {
+
+int sb2_spmv(const sb2_csr* A, int trans, double alpha, const double* x,
+             double beta, double* y, void* stream) {
+  return spmv_common(A, trans, alpha, x, beta, y, false, (cudaStream_t)stream);
+}
+
+int sb2_mlt(const sb2_csr* A, int trans, double alpha, const double* x,
+            double* y, void* stream) {
+  return spmv_common(A, trans, alpha, x, 0.0, y, true, (cudaStream_t)stream);
+}
+
+static int spmv_host_common(const sb2_csr* A, int trans, double alpha,
+                            const double* x_host, double beta, double* y_host,
+                            bool overwrite, cudaStream_t s) {
+  if (!A) return SB2_ERR_INVALID_VALUE;
+  const int nx = trans ? A->m : A->n, ny = trans ? A->n : A->m;
+  if ((nx > 0 && !x_host) || (ny > 0 && !y_host)) return SB2_ERR_INVALID_VALUE;
+  double *dx = nullptr, *dy = nullptr;
+  int st = SB2_OK;
+  cudaError_t e = cudaMallocAsync(&dx, sizeof(double) * (nx > 0 ? nx : 1), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&dy, sizeof(double) * (ny > 0 ? ny : 1), s);
+  if (e == cudaSuccess && nx > 0)
+    e = cudaMemcpyAsync(dx, x_host, sizeof(double) * nx, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && ny > 0 && !overwrite)
+    e = cudaMemcpyAsync(dy, y_host, sizeof(double) * ny, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) st = map_cuda_error(e);
+  if (st == SB2_OK) st = spmv_common(A, trans, alpha, dx, beta, dy, overwrite, s);
+  if (st == SB2_OK && ny > 0) {
+    e = cudaMemcpyAsync(y_host, dy, sizeof(double) * ny, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) st = map_cuda_error(e);
+  }
+  cudaFreeAsync(dx, s);
+  cudaFreeAsync(dy, s);
+  e = cudaStreamSynchronize(s);
+  if (st == SB2_OK && e != cudaSuccess) st = map_cuda_error(e);
+  return st;
+}
+
+int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
+                  const double* x_host, double beta, double* y_host,
+                  void* stream) {
+  // y is copied in too: MltAdd scales it by beta even when beta == 0.
+  return spmv_host_common(A, trans, alpha, x_host, beta, y_host, false,
+                          (cudaStream_t)stream);
+}
+
+int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
+                 const double* x_host, double* y_host, void* stream) {
+  return spmv_host_common(A, trans, alpha, x_host, 0.0, y_host, true,
+                          (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// Status codes, device queries and per-stream reduction scratch.
+#include <cstdio>
+
+#include "sb2_internal.cuh"
+
+namespace sb2 {
+
+int g_wait_limit_ms = 2000;
+
+int map_cuda_error(cudaError_t e) {
+  if (e == cudaSuccess) return SB2_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // clear the sticky-free allocation error
+    return SB2_ERR_NO_MEMORY;
+  }
+  return SB2_ERR_CUDA;
+}
+
+int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+int num_sms(int device) {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(device);
+  if (it != cache.end()) return it->second;
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0)
+    v = 148;
+  cache[device] = v;
+  return v;
+}
+
+int get_red_scratch(cudaStream_t s, RedScratch** out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, cudaStream_t>, RedScratch*> table;
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(dev, s);
+  auto it = table.find(key);
+  if (it != table.end()) {
+    *out = it->second;
+    return SB2_OK;
+  }
+  RedScratch* r = new RedScratch();
+  cudaError_t e = cudaMalloc(&r->partials, sizeof(double) * kRedMaxBlocks * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&r->counter, sizeof(unsigned) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&r->result, sizeof(double) * 8);
+  if (e == cudaSuccess) e = cudaMemset(r->counter, 0, sizeof(unsigned) * 4);
+  if (e != cudaSuccess) {
+    cudaFree(r->partials);
+    cudaFree(r->counter);
+    cudaFree(r->result);
+    delete r;
+    return map_cuda_error(e);
+  }
+  table[key] = r;
+  *out = r;
+  return SB2_OK;
+}
+
+}  // namespace sb2
+
+extern "C" {
+
+const char* sb2_status_string(int status) {
+  switch (status) {
+    case SB2_OK: return "ok";
+    case SB2_ERR_INVALID_VALUE: return "invalid value (sizes, null or overlapping pointers)";
+    case SB2_ERR_NO_MEMORY: return "device allocation failed";
+    case SB2_ERR_CUDA: return "CUDA runtime error";
+    case SB2_ERR_TIMEOUT: return "a bounded device-side wait ran out";
+    case SB2_ERR_INVALID_CSR: return "CSR invariants violated";
+    case SB2_ERR_NOT_SUPPORTED: return "option combination not supported";
+    default: return "unknown status";
+  }
+}
+
+int sb2_version(void) { return 10000; }
+
+int sb2_set_wait_limit_ms(int ms) {
+  int old = sb2::g_wait_limit_ms;
+  if (ms > 0) sb2::g_wait_limit_ms = ms;
+  return old;
+}
+
+}  // extern "C"

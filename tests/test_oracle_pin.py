@@ -1,0 +1,139 @@
+"""The oracle (oracle/seldon_oracle.c) is pinned before it is trusted:
+bit-for-bit against golden vectors produced by the reference itself, and
+against the live reference build where oracle/_ref exists."""
+import os
+
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "seldon_golden.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+def _mat(g, name):
+    return (g[f"mat/{name}/ptr"], g[f"mat/{name}/ind"], g[f"mat/{name}/val"],
+            int(g[f"mat/{name}/m"]), int(g[f"mat/{name}/n"]))
+
+
+@pytest.mark.parametrize("name", ["lap2d_9", "conv_4", "rand_37x29"])
+def test_mltadd_golden(golden, oracle, name):
+    ptr, ind, val, m, n = _mat(golden, name)
+    k = f"mltadd/{name}"
+    out = oracle.mltadd(m, n, ptr, ind, val, float(golden[k + "/alpha"]), golden[k + "/x"],
+                        float(golden[k + "/beta"]), golden[k + "/y"])
+    assert np.array_equal(out, golden[k + "/out"])
+    k = f"mltadd_t/{name}"
+    out = oracle.mltadd(m, n, ptr, ind, val, float(golden[k + "/alpha"]), golden[k + "/x"],
+                        float(golden[k + "/beta"]), golden[k + "/y"], trans=True)
+    assert np.array_equal(out, golden[k + "/out"])
+
+
+def test_mltadd_sym_golden(golden, oracle):
+    ptr, ind, val, m, n = _mat(golden, "lap2d_9_upper")
+    k = "mltadd_sym/lap2d_9"
+    out = oracle.mltadd(m, n, ptr, ind, val, float(golden[k + "/alpha"]), golden[k + "/x"],
+                        float(golden[k + "/beta"]), golden[k + "/y"], sym=True)
+    assert np.array_equal(out, golden[k + "/out"])
+
+
+@pytest.mark.parametrize("t", [0, 2, 3])
+@pytest.mark.parametrize("sym", [0, 1])
+def test_sor_golden(golden, oracle, t, sym):
+    name = "lap2d_9_upper" if sym else "lap2d_9"
+    ptr, ind, val, m, n = _mat(golden, name)
+    k = f"sor/t{t}_s{sym}"
+    out = oracle.sor(ptr, ind, val, golden[k + "/x0"], golden[k + "/b"], float(golden[k + "/omega"]),
+                     int(golden[k + "/it"]), t, sym=bool(sym))
+    assert np.array_equal(out, golden[k + "/out"])
+
+
+def _solve_keys(g):
+    return sorted({k.split("/")[1] for k in g.files if k.startswith("solve/")})
+
+
+def test_solvers_golden(golden, oracle):
+    keys = _solve_keys(golden)
+    assert len(keys) >= 12
+    for key in keys:
+        which, rest = key.split("_", 1)
+        mname, pc, sym = rest.rsplit("_", 2)
+        pc, sym = int(pc[1:]), int(sym[1:])
+        ptr, ind, val, m, n = _mat(golden, mname)
+        A = matgen.upper(ptr, ind, val) if sym else (ptr, ind, val)
+        k = f"solve/{key}"
+        x, code, nb, _, _ = oracle.solve(which, *A, golden[k + "/b"], sym=bool(sym), precond=pc,
+                                         omega=float(golden[k + "/omega"]),
+                                         tol=float(golden[k + "/tol"]),
+                                         max_iter=int(golden[k + "/max_iter"]),
+                                         restart=int(golden[k + "/restart"]))
+        assert code == int(golden[k + "/code"]), key
+        assert nb == int(golden[k + "/nb"]), key
+        assert np.array_equal(x, golden[k + "/x"]), key
+
+
+def test_genrot_golden(golden, oracle):
+    for a, b, r, z, c, s in golden["genrot/table"]:
+        assert oracle.genrot(a, b) == (r, z, c, s)
+
+
+# ---------------------------------------------------------------- live reference
+
+@pytest.mark.parametrize("seed", range(6))
+def test_mltadd_live(reference, oracle, seed):
+    rng = np.random.default_rng(seed)
+    m, n = int(rng.integers(1, 80)), int(rng.integers(1, 80))
+    ptr, ind, val = matgen.random_csr(m, n, float(rng.uniform(0.02, 0.4)), seed=seed,
+                                      empty_rows=0.2)
+    x, y = rng.standard_normal(n), rng.standard_normal(m)
+    a, b = float(rng.standard_normal()), float(rng.standard_normal())
+    assert np.array_equal(oracle.mltadd(m, n, ptr, ind, val, a, x, b, y),
+                          reference.mltadd(m, n, ptr, ind, val, a, x, b, y))
+    xt, yt = rng.standard_normal(m), rng.standard_normal(n)
+    assert np.array_equal(oracle.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True),
+                          reference.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True))
+
+
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres"])
+@pytest.mark.parametrize("pc", [0, 1, 2])
+def test_solvers_live(reference, oracle, which, pc):
+    ptr, ind, val = matgen.convdiff3d(5) if which != "cg" else matgen.lap2d(15)
+    m = ptr.size - 1
+    rng = np.random.default_rng(7)
+    b = matgen.matvec(ptr, ind, val, rng.uniform(-1, 1, m))
+    xo, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, precond=pc, tol=1e-10,
+                                    max_iter=500, restart=8, omega=1.1)
+    xr, cr, nr = reference.solve(which, ptr, ind, val, b, precond=pc, tol=1e-10,
+                                 max_iter=500, restart=8, omega=1.1)
+    assert (co, no) == (cr, nr)
+    assert np.array_equal(xo, xr)
+
+
+def test_breakdown_and_edge_codes(reference, oracle):
+    # zero right-hand side: Init fails, x untouched, code 0 (Iterative.cxx:240-241)
+    ptr, ind, val = matgen.lap2d(4)
+    b = np.zeros(16)
+    x0 = np.arange(16.0)
+    for which in ("cg", "bicgstab", "gmres"):
+        xo, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, x0=x0)
+        xr, cr, nr = reference.solve(which, ptr, ind, val, b, x0=x0)
+        assert co == cr
+        assert np.array_equal(xo, xr)
+    # max_iter reached -> -2
+    b = np.ones(16)
+    xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b, tol=1e-30, max_iter=3)
+    xr, cr, nr = reference.solve("cg", ptr, ind, val, b, tol=1e-30, max_iter=3)
+    assert co == cr == -2 and no == nr == 3
+    # CG on an indefinite matrix with a vanishing p.q -> breakdown #2
+    ptr = np.array([0, 1, 2], dtype=np.int32)
+    ind = np.array([0, 1], dtype=np.int32)
+    val = np.array([1.0, -1.0])
+    b = np.array([1.0, 1.0])
+    xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b)
+    xr, cr, nr = reference.solve("cg", ptr, ind, val, b)
+    assert co == cr == 2
