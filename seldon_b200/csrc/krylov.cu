@@ -1,8 +1,1052 @@
-// Krylov drivers (placeholder entry points).
-#include "sb2_internal.cuh"
+// Seldon's Krylov drivers on the device.
+//
+// Identity and Jacobi preconditioning run as ONE cooperative persistent
+// kernel per solve: the whole iteration loop, the Iteration<double> stopping
+// rule, the breakdown tests and (GMRES) the Givens rotations and Hessenberg
+// back-solve stay on the GPU; the only host round trip is the final result.
+// Each iteration fuses the SpMV with the dot product that follows it and the
+// vector updates with the next residual norm; grid-wide reductions are
+// deterministic (fixed CTA order).
+//
+// SOR preconditioning (level-scheduled sweeps, many dependent launches) goes
+// through a host-driven driver over the same device kernels, one operation at
+// a time, in the reference's order.
+//
+// References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
+// Iterative.cxx:235-354.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "persist.cuh"
+
+namespace sb2 {
+
+int precond_apply(const sb2_precond* M, bool trans, const double* r, double* z,
+                  cudaStream_t s);
+
+constexpr int NT = kSpmvThreads;
+
+// ----------------------------------------------------------------- common
+
+struct OpArgs {
+  const int* ptr;
+  const int* ind;
+  const double* val;
+  const int* blk;
+  const unsigned char* kind;
+  int nblk;
+  int n;
+  const double* diag;  // nullptr: identity preconditioner, else Jacobi
+};
+
+struct IterArgs {
+  double tol;
+  int max_iter;
+  int restart;
+  int init_guess_null;
+};
+
+#define SB2_SHARED_DECL                     \
+  __shared__ double s_prod[kNnzCap];        \
+  __shared__ double s_red[NT / 32];         \
+  __shared__ double s_vals[kMaxRed]
+
+__device__ __forceinline__ double precond_val(const double* diag, int i, double r) {
+  return diag ? __ddiv_rn(r, diag[i]) : r;  // Jacobi z_i = r_i / A(i,i)
+}
+
+__device__ __forceinline__ void hist_push(const History& h, int* len, int it, double res) {
+  if (*len < h.cap) {
+    h.res[*len] = res;
+    h.it[*len] = it;
+  }
+  (*len)++;
+}
+
+__device__ __forceinline__ void write_out(SolveOut* out, int nb_iter, int max_iter, int fail,
+                                          double facteur, double last, int hist_len) {
+  out->nb_iter = nb_iter;
+  // Iteration::ErrorCode (Iterative.cxx:344-354)
+  out->error_code = (nb_iter >= max_iter) ? -2 : fail;
+  out->init_failed = 0;
+  out->facteur_reste = facteur;
+  out->last_residual = last;
+  out->hist_len = hist_len;
+}
+
+// epilogue: y_r = t; acc += w_r * t   (SpMV fused with the dot that follows)
+struct EpiStoreDot {
+  double* y;
+  const double* w;
+  double acc;
+  __device__ __forceinline__ void operator()(int r, double t) {
+    y[r] = t;
+    acc = add_rn(acc, mul_rn(__ldcg(w + r), t));
+  }
+};
+
+// epilogue: r_r = b_r - t (MltAdd(-1, A, x, 1, r) after Copy(b, r)), then the
+// preconditioned z_r; accumulate r.r and r.z.
+struct EpiResidual {
+  const double* b;
+  double* r;
+  const double* diag;
+  double rr, rz;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double v = add_rn(__ldg(b + i), -t);
+    r[i] = v;
+    const double z = precond_val(diag, i, v);
+    rr = add_rn(rr, mul_rn(v, v));
+    rz = add_rn(rz, mul_rn(v, z));
+  }
+};
+
+template <class Epi>
+__device__ __forceinline__ void spmv_phase(const OpArgs& A, const double* x, Epi& epi,
+                                           double* s_prod, double* s_red) {
+  XLoadCg<double> xl{x};
+  for (int b = blockIdx.x; b < A.nblk; b += gridDim.x)
+    spmv_row_block<NT, double, double>(A.ptr, A.ind, A.val, A.blk[b], A.blk[b + 1], A.kind[b],
+                                       xl, epi, s_prod, s_red);
+}
+
+// ----------------------------------------------------------------- CG
+
+struct CgVecs {
+  const double* b;
+  double *x, *r, *p, *q;
+};
+
+__global__ void __launch_bounds__(NT) cg_fused_kernel(OpArgs A, CgVecs v, IterArgs it,
+                                                      Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  // iter.Init(b): facteur_reste = 1/||b|| (Iterative.cxx:235-249)
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b), with ||r||^2 and r.z
+  double rr = 0.0, rz = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      v.x[i] = 0.0;
+      v.r[i] = bi;
+      const double z = precond_val(A.diag, (int)i, bi);
+      rr = add_rn(rr, mul_rn(bi, bi));
+      rz = add_rn(rz, mul_rn(bi, z));
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, A.diag, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+    rz = epi.rz;
+  }
+  rr = block_sum<NT>(rr, s_red);
+  rz = block_sum<NT>(rz, s_red);
+  if (tid == 0) { s_vals[0] = rr; s_vals[1] = rz; }
+  if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double rho = s_vals[1], rho_1 = 1.0;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    // while (!iter.Finished(r))
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    // z = M^{-1} r; rho = (r, z): already reduced with the norm
+    if (rho == 0.0) { fail = 1; break; }
+    // p = z (first) | p = beta*p + z: Mlt(beta, p); Add(1, z, p)
+    if (nb_iter == 0) {
+      for (long long i = gt; i < n; i += gs)
+        v.p[i] = precond_val(A.diag, (int)i, __ldcg(v.r + i));
+    } else {
+      const double beta = rho / rho_1;
+      for (long long i = gt; i < n; i += gs) {
+        const double z = precond_val(A.diag, (int)i, __ldcg(v.r + i));
+        v.p[i] = add_rn(mul_rn(__ldcg(v.p + i), beta), z);
+      }
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // q = A p fused with delta = (p, q)
+    EpiStoreDot epi{v.q, v.p, 0.0};
+    spmv_phase(A, v.p, epi, s_prod, s_red);
+    double d = block_sum<NT>(epi.acc, s_red);
+    if (tid == 0) s_vals[0] = d;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    const double delta = s_vals[0];
+    if (delta == 0.0) { fail = 2; break; }
+    const double alpha = rho / delta;
+    // Add(alpha, p, x); Add(-alpha, q, r); then ||r||^2 and (r, z) for the next test
+    rr = 0.0;
+    rz = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      if (alpha != 0.0) v.x[i] = add_rn(__ldcg(v.x + i), mul_rn(alpha, __ldcg(v.p + i)));
+      double ri = __ldcg(v.r + i);
+      if (-alpha != 0.0) {
+        ri = add_rn(ri, mul_rn(-alpha, __ldcg(v.q + i)));
+        v.r[i] = ri;
+      }
+      const double z = precond_val(A.diag, (int)i, ri);
+      rr = add_rn(rr, mul_rn(ri, ri));
+      rz = add_rn(rz, mul_rn(ri, z));
+    }
+    rr = block_sum<NT>(rr, s_red);
+    rz = block_sum<NT>(rz, s_red);
+    if (tid == 0) { s_vals[0] = rr; s_vals[1] = rz; }
+    if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    rr = s_vals[0];
+    rho_1 = rho;
+    rho = s_vals[1];
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
+// ----------------------------------------------------------------- BiCGSTAB
+
+struct BicgVecs {
+  const double* b;
+  double *x, *r, *rt, *p, *ph, *v, *s, *sh, *t;
+};
+
+// epilogue: y_r = t; acc0 += w0_r t; acc1 += w1_r t
+struct EpiStoreDot2 {
+  double* y;
+  const double* w0;
+  const double* w1;
+  double acc0, acc1;
+  __device__ __forceinline__ void operator()(int r, double t) {
+    y[r] = t;
+    acc0 = add_rn(acc0, mul_rn(__ldcg(w0 + r), t));
+    if (w1) acc1 = add_rn(acc1, mul_rn(__ldcg(w1 + r), t));
+  }
+};
+
+__global__ void __launch_bounds__(NT) bicgstab_fused_kernel(OpArgs A, BicgVecs v, IterArgs it,
+                                                            Persist P, History H,
+                                                            SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0); rtilde = r; ||r||^2 and (rtilde, r)
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      v.x[i] = 0.0;
+      v.r[i] = bi;
+      v.rt[i] = bi;
+      rr = add_rn(rr, mul_rn(bi, bi));
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    for (long long i = gt; i < n; i += gs) v.rt[i] = __ldcg(v.r + i);
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) { s_vals[0] = rr; s_vals[1] = rr; }
+  if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double rho_1 = s_vals[1];  // (rtilde, r) with rtilde = r
+  double rho_2 = 0.0, alpha = 0.0, omega = 0.0;
+  const bool jac = (A.diag != nullptr);
+  double* ph = jac ? v.ph : v.p;  // identity: phat aliases p, shat aliases s
+  double* sh = jac ? v.sh : v.s;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho_1 == 0.0) { fail = 1; break; }
+    if (nb_iter == 0) {
+      // Copy(r, p); phat = M^{-1} p
+      for (long long i = gt; i < n; i += gs) {
+        const double pi = __ldcg(v.r + i);
+        v.p[i] = pi;
+        if (jac) ph[i] = precond_val(A.diag, (int)i, pi);
+      }
+    } else {
+      if (omega == 0.0) { fail = 2; break; }
+      const double beta = (rho_1 / rho_2) * (alpha / omega);
+      // Add(-omega, v, p); Mlt(beta, p); Add(1, r, p); phat = M^{-1} p
+      for (long long i = gt; i < n; i += gs) {
+        double pi = add_rn(__ldcg(v.p + i), mul_rn(-omega, __ldcg(v.v + i)));
+        pi = add_rn(mul_rn(pi, beta), __ldcg(v.r + i));
+        v.p[i] = pi;
+        if (jac) ph[i] = precond_val(A.diag, (int)i, pi);
+      }
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // v = A phat, sigma = (rtilde, v)
+    EpiStoreDot2 e1{v.v, v.rt, nullptr, 0.0, 0.0};
+    spmv_phase(A, ph, e1, s_prod, s_red);
+    double d = block_sum<NT>(e1.acc0, s_red);
+    if (tid == 0) s_vals[0] = d;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    const double sigma = s_vals[0];
+    if (sigma == 0.0) { fail = 3; break; }
+    alpha = rho_1 / sigma;
+    // Copy(r, s); Add(-alpha, v, s); shat = M^{-1} s; ||s||^2
+    double ss = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      double si = __ldcg(v.r + i);
+      if (-alpha != 0.0) si = add_rn(si, mul_rn(-alpha, __ldcg(v.v + i)));
+      v.s[i] = si;
+      if (jac) sh[i] = precond_val(A.diag, (int)i, si);
+      ss = add_rn(ss, mul_rn(si, si));
+    }
+    ss = block_sum<NT>(ss, s_red);
+    if (tid == 0) s_vals[0] = ss;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    nb_iter++;
+    reste = facteur * sqrt(s_vals[0]);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) {
+      // Add(alpha, phat, x)
+      if (alpha != 0.0)
+        for (long long i = gt; i < n; i += gs)
+          v.x[i] = add_rn(__ldcg(v.x + i), mul_rn(alpha, __ldcg(ph + i)));
+      break;
+    }
+    // t = A shat; omega = (t, s) / (t, t)
+    EpiStoreDot2 e2{v.t, v.s, nullptr, 0.0, 0.0};
+    spmv_phase(A, sh, e2, s_prod, s_red);
+    // (t, t) needs t itself: accumulate from the epilogue's stored values
+    double ts = block_sum<NT>(e2.acc0, s_red);
+    if (tid == 0) s_vals[0] = ts;
+    __syncthreads();
+    double tt = 0.0;
+    for (int b = blockIdx.x; b < A.nblk; b += gridDim.x)
+      for (int r = A.blk[b] + tid; r < A.blk[b + 1]; r += NT) {
+        const double tr = __ldcg(v.t + r);
+        tt = add_rn(tt, mul_rn(tr, tr));
+      }
+    tt = block_sum<NT>(tt, s_red);
+    if (tid == 0) s_vals[1] = tt;
+    if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    omega = s_vals[0] / s_vals[1];
+    // Add(alpha, phat, x); Add(omega, shat, x); Copy(s, r); Add(-omega, t, r)
+    rr = 0.0;
+    double rtr = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      double xi = __ldcg(v.x + i);
+      if (alpha != 0.0) xi = add_rn(xi, mul_rn(alpha, __ldcg(ph + i)));
+      if (omega != 0.0) xi = add_rn(xi, mul_rn(omega, __ldcg(sh + i)));
+      v.x[i] = xi;
+      double ri = __ldcg(v.s + i);
+      if (-omega != 0.0) ri = add_rn(ri, mul_rn(-omega, __ldcg(v.t + i)));
+      v.r[i] = ri;
+      rr = add_rn(rr, mul_rn(ri, ri));
+      rtr = add_rn(rtr, mul_rn(__ldcg(v.rt + i), ri));
+    }
+    rr = block_sum<NT>(rr, s_red);
+    rtr = block_sum<NT>(rtr, s_red);
+    if (tid == 0) { s_vals[0] = rr; s_vals[1] = rtr; }
+    if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    rr = s_vals[0];
+    rho_2 = rho_1;
+    rho_1 = s_vals[1];
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
+// ----------------------------------------------------------------- GMRES
+
+struct GmresVecs {
+  const double* b;
+  double *x, *r, *w, *V;  // V: (m+1) vectors of length n, contiguous
+};
+
+// Givens rotation, Functions_Vector.cxx:612-649 (old BLAS drotg semantics).
+__device__ void gen_rot(double& a_in, double& b_in, double& c_, double& s_) {
+  const double a = a_in, b = b_in;
+  const double roe = (fabs(a) > fabs(b)) ? a : b;
+  const double scal = fabs(a) + fabs(b);
+  double r, z;
+  if (scal != 0.0) {
+    const double a_scl = a / scal, b_scl = b / scal;
+    r = mul_rn(scal, sqrt(add_rn(mul_rn(a_scl, a_scl), mul_rn(b_scl, b_scl))));
+    if (roe < 0.0) r = mul_rn(r, -1.0);
+    c_ = a / r;
+    s_ = b / r;
+    z = 1.0;
+    if (fabs(a) > fabs(b)) z = s_;
+    else if (fabs(b) >= fabs(a) && c_ != 0.0) z = 1.0 / c_;
+  } else {
+    c_ = 1.0;
+    s_ = 0.0;
+    r = 0.0;
+    z = 0.0;
+  }
+  a_in = r;
+  b_in = z;
+}
+
+// Functions_Vector.cxx:681-687
+__device__ __forceinline__ void apply_rot(double& x, double& y, double c, double s) {
+  const double temp = add_rn(mul_rn(c, x), mul_rn(s, y));
+  y = __dsub_rn(mul_rn(c, y), mul_rn(s, x));
+  x = temp;
+}
+
+// epilogue of u = A V_i: w_r = M^{-1} u_r, acc += V0_r * w_r (first MGS dot)
+struct EpiPrecDot {
+  double* w;
+  const double* v0;
+  const double* diag;
+  double acc;
+  __device__ __forceinline__ void operator()(int r, double t) {
+    const double wr = precond_val(diag, r, t);
+    w[r] = wr;
+    acc = add_rn(acc, mul_rn(__ldcg(v0 + r), wr));
+  }
+};
+
+__global__ void __launch_bounds__(NT) gmres_fused_kernel(OpArgs A, GmresVecs v, IterArgs it,
+                                                         Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  extern __shared__ double s_dyn[];
+  const int m = it.restart;
+  const int ld = m + 1;
+  double* Hm = s_dyn;            // (m+1) x (m+1), column-major
+  double* sv = Hm + ld * ld;     // s(0..m)
+  double* cs = sv + ld;          // rotations_cos
+  double* sn = cs + ld;          // rotations_sin
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const size_t nn = (size_t)n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  for (int k = tid; k < ld * ld + 3 * ld; k += NT) s_dyn[k] = 0.0;
+
+  // w = b (- A x); r = M^{-1} w; beta = ||r|| (Gmres.cxx:82-90)
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      v.x[i] = 0.0;
+      const double ri = precond_val(A.diag, (int)i, bi);
+      v.r[i] = ri;
+      rr = add_rn(rr, mul_rn(ri, ri));
+    }
+  } else {
+    EpiResidual epi{v.b, v.w, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    for (long long i = gt; i < n; i += gs) {
+      const double ri = precond_val(A.diag, (int)i, __ldcg(v.w + i));
+      v.r[i] = ri;
+      rr = add_rn(rr, mul_rn(ri, ri));
+    }
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  double beta = sqrt(s_vals[0]);
+  // outer.Init(r)
+  if (beta == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / beta;
+
+  int nb_iter = 0;
+  double reste;
+  for (;;) {
+    // while (!outer.Finished(beta))
+    reste = facteur * beta;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    // V0 = r * (1/beta); s = beta e0
+    const double inv_beta = 1.0 / beta;
+    for (long long i = gt; i < n; i += gs) v.V[i] = mul_rn(__ldcg(v.r + i), inv_beta);
+    if (tid == 0) {
+      for (int k = 0; k < ld; k++) sv[k] = 0.0;
+      sv[0] = beta;
+    }
+    const int inner_max = nb_iter + m;
+    int i = 0;
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    for (;;) {
+      double* Vi = v.V + (size_t)i * nn;
+      // u = A V_i; w = M^{-1} u; h_{0,i} = (V_0, w)
+      EpiPrecDot epi{v.w, v.V, A.diag, 0.0};
+      spmv_phase(A, Vi, epi, s_prod, s_red);
+      double d = block_sum<NT>(epi.acc, s_red);
+      if (tid == 0) s_vals[0] = d;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+      // modified Gram-Schmidt: H(k,i) = (V_k, w); Add(-H(k,i), V_k, w)
+      for (int k = 0; k <= i; k++) {
+        const double h = s_vals[0];
+        if (tid == 0) Hm[k + i * ld] = h;
+        const double* Vk = v.V + (size_t)k * nn;
+        const double* Vn = (k < i) ? v.V + (size_t)(k + 1) * nn : nullptr;
+        double acc = 0.0;
+        for (long long e = gt; e < n; e += gs) {
+          double we = __ldcg(v.w + e);
+          if (-h != 0.0) {
+            we = add_rn(we, mul_rn(-h, __ldcg(Vk + e)));
+            v.w[e] = we;
+          }
+          acc = Vn ? add_rn(acc, mul_rn(__ldcg(Vn + e), we)) : add_rn(acc, mul_rn(we, we));
+        }
+        acc = block_sum<NT>(acc, s_red);
+        if (tid == 0) s_vals[0] = acc;
+        if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+      }
+      // h_{i+1,i} = ||w||; V_{i+1} = w / h
+      double hi_ip1 = sqrt(s_vals[0]);
+      double* Vn = v.V + (size_t)(i + 1) * nn;
+      const double inv_h = (hi_ip1 != 0.0) ? 1.0 / hi_ip1 : 1.0;
+      for (long long e = gt; e < n; e += gs) {
+        const double we = __ldcg(v.w + e);
+        Vn[e] = (hi_ip1 != 0.0) ? mul_rn(we, inv_h) : we;
+      }
+      // rotations (every CTA computes the same scalars)
+      if (tid == 0) {
+        for (int k = 0; k < i; k++) apply_rot(Hm[k + i * ld], Hm[k + 1 + i * ld], cs[k], sn[k]);
+        if (hi_ip1 != 0.0) {
+          gen_rot(Hm[i + i * ld], hi_ip1, cs[i], sn[i]);
+          apply_rot(sv[i], sv[i + 1], cs[i], sn[i]);
+        }
+      }
+      i++;
+      nb_iter++;
+      __syncthreads();
+      // inner.Finished(|s(i)|): inner counts alongside outer, max = start + m
+      const double rin = facteur * fabs(sv[i]);
+      if (lead) hist_push(H, &hlen, nb_iter, rin);
+      reste = rin;
+      const bool stop = (rin < it.tol) || (nb_iter >= inner_max);
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;  // V_{i} complete
+      if (stop) break;
+    }
+    // Solve(H, s): netlib DTRSV column sweep on the leading i x i block
+    if (tid == 0) {
+      for (int j = i - 1; j >= 0; j--)
+        if (sv[j] != 0.0) {
+          sv[j] = sv[j] / Hm[j + j * ld];
+          const double t = sv[j];
+          for (int r = j - 1; r >= 0; r--) sv[r] = __dsub_rn(sv[r], mul_rn(t, Hm[r + j * ld]));
+        }
+    }
+    __syncthreads();
+    // x += sum_k s(k) V_k (Add skipped when s(k) == 0)
+    for (long long e = gt; e < n; e += gs) {
+      double xe = __ldcg(v.x + e);
+      for (int k = 0; k < i; k++)
+        if (sv[k] != 0.0) xe = add_rn(xe, mul_rn(sv[k], __ldcg(v.V + (size_t)k * nn + e)));
+      v.x[e] = xe;
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // w = b - A x; r = M^{-1} w; beta = ||r||
+    EpiResidual epi{v.b, v.w, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    rr = 0.0;
+    for (long long e = gt; e < n; e += gs) {
+      const double re = precond_val(A.diag, (int)e, __ldcg(v.w + e));
+      v.r[e] = re;
+      rr = add_rn(rr, mul_rn(re, re));
+    }
+    rr = block_sum<NT>(rr, s_red);
+    if (tid == 0) s_vals[0] = rr;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    beta = sqrt(s_vals[0]);
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, 0, facteur, reste, hlen);
+}
+
+// ----------------------------------------------------------------- launch glue
+
+struct DeviceBuf {
+  void* p = nullptr;
+  cudaStream_t s = nullptr;
+  ~DeviceBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
+
+struct SolveScratch {
+  DeviceBuf vecs, state;
+  double* vec = nullptr;
+  GridSync* sync = nullptr;
+  double* partials = nullptr;
+  SolveOut* out = nullptr;
+  double* hist = nullptr;
+  int* hist_it = nullptr;
+  int hist_cap = 0;
+};
+
+static int alloc_scratch(cudaStream_t s, int n, int nvec, int grid, int hist_cap,
+                         SolveScratch* S) {
+  S->vecs.s = S->state.s = s;
+  const size_t vbytes = sizeof(double) * (size_t)std::max(n, 1) * nvec;
+  SB2_CUDA_TRY(cudaMallocAsync(&S->vecs.p, vbytes, s));
+  S->vec = (double*)S->vecs.p;
+  S->hist_cap = std::max(hist_cap, 1);
+  const size_t sync_b = 256, part_b = sizeof(double) * kMaxRed * grid, out_b = 256;
+  const size_t hist_b = sizeof(double) * S->hist_cap, hit_b = sizeof(int) * S->hist_cap;
+  const size_t total = sync_b + ((part_b + 255) / 256) * 256 + out_b + ((hist_b + 255) / 256) * 256 + hit_b;
+  SB2_CUDA_TRY(cudaMallocAsync(&S->state.p, total, s));
+  char* c = (char*)S->state.p;
+  S->sync = (GridSync*)c;
+  c += sync_b;
+  S->partials = (double*)c;
+  c += ((part_b + 255) / 256) * 256;
+  S->out = (SolveOut*)c;
+  c += out_b;
+  S->hist = (double*)c;
+  c += ((hist_b + 255) / 256) * 256;
+  S->hist_it = (int*)c;
+  SB2_CUDA_TRY(cudaMemsetAsync(S->state.p, 0, sync_b + ((part_b + 255) / 256) * 256 + out_b, s));
+  return SB2_OK;
+}
+
+static int coop_grid(const void* kernel, size_t smem, const sb2_csr* A) {
+  const int dev = current_device();
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, smem) != cudaSuccess ||
+      per_sm < 1)
+    return 0;
+  const int cap = per_sm * num_sms(dev);
+  const int n = A->m;
+  // enough CTAs to cover the work, no more: a small grid makes the barriers cheap
+  const int want = std::max((n + NT * 4 - 1) / (NT * 4), (A->full.part.nblk + 1) / 2);
+  return std::max(1, std::min(cap, want));
+}
+
+static int finish_solve(SolveScratch& S, cudaStream_t s, sb2_iter_result* res, double* hist,
+                        int* hist_it, int hist_cap, int max_iter) {
+  SolveOut o;
+  GridSync gsync;
+  SB2_CUDA_TRY(cudaMemcpyAsync(&o, S.out, sizeof(o), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaMemcpyAsync(&gsync, S.sync, sizeof(gsync), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  if (gsync.status != 0) return SB2_ERR_TIMEOUT;
+  const int nh = std::min(o.hist_len, hist_cap);
+  if (hist && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist, S.hist, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+  if (hist_it && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist_it, S.hist_it, sizeof(int) * nh, cudaMemcpyDeviceToHost));
+  res->nb_iter = o.nb_iter;
+  // a zero right-hand side returns ErrorCode() of an untouched Iteration
+  res->error_code = o.init_failed ? (max_iter <= 0 ? -2 : 0) : o.error_code;
+  res->init_failed = o.init_failed;
+  res->hist_len = nh;
+  res->facteur_reste = o.facteur_reste;
+  res->last_residual = o.last_residual;
+  return SB2_OK;
+}
+
+static OpArgs op_args(const sb2_csr* A, const double* diag) {
+  const CsrArrays& f = A->full;
+  return OpArgs{f.d_ptr, f.d_ind, f.d_val, f.part.d_blk, f.part.d_kind, f.part.nblk, A->m, diag};
+}
+
+enum Solver { kCg = 0, kBicg = 1, kGmres = 2 };
+
+static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
+                       const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
+                       double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
+  const int n = A->m;
+  const int m = std::max(prm->restart, 1);
+  const void* kern = nullptr;
+  size_t smem = 0;
+  int nvec = 0;
+  if (which == kCg) { kern = (const void*)cg_fused_kernel; nvec = 3; }
+  if (which == kBicg) { kern = (const void*)bicgstab_fused_kernel; nvec = 9; }
+  if (which == kGmres) {
+    kern = (const void*)gmres_fused_kernel;
+    nvec = 2 + (m + 1);
+    smem = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (m + 1));
+    if (smem > 160 * 1024) return SB2_ERR_NOT_SUPPORTED;
+    SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+  }
+  const int grid = coop_grid(kern, smem, A);
+  if (grid < 1) return SB2_ERR_CUDA;
+  SolveScratch S;
+  // history: every Finished() test; GMRES tests once per inner step and once
+  // per restart
+  const int hcap = std::max(hist_cap, 0) + 1;
+  SB2_TRY(alloc_scratch(s, n, nvec, grid, hcap, &S));
+  Persist P{S.sync, S.partials, (unsigned long long)g_wait_limit_ms * 1000000ull};
+  History H{S.hist, S.hist_it, hcap};
+  IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null};
+  OpArgs op = op_args(A, diag);
+  const size_t nn = (size_t)std::max(n, 1);
+  double* V = S.vec;
+  void* args[6];
+  CgVecs cv;
+  BicgVecs bv;
+  GmresVecs gv;
+  args[0] = &op;
+  args[2] = &it;
+  args[3] = &P;
+  args[4] = &H;
+  args[5] = &S.out;
+  if (which == kCg) {
+    cv = CgVecs{b, x, V, V + nn, V + 2 * nn};
+    args[1] = &cv;
+  } else if (which == kBicg) {
+    bv = BicgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                  V + 7 * nn};
+    args[1] = &bv;
+  } else {
+    gv = GmresVecs{b, x, V, V + nn, V + 2 * nn};
+    args[1] = &gv;
+  }
+  SB2_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(NT), args, smem, s));
+  return finish_solve(S, s, res, hist, hist_it, hcap - 1 > 0 ? hcap - 1 : 0, prm->max_iter);
+}
+
+// ----------------------------------------------------------------- host-driven drivers (SOR)
+
+struct HostIter {
+  double tol, facteur = 0.0;
+  int max_iter, nb_iter = 0, fail = 0;
+  std::vector<std::pair<int, double>> hist;
+  bool finished(double res) {
+    const double reste = facteur * res;
+    hist.emplace_back(nb_iter, reste);
+    return reste < tol || nb_iter >= max_iter;
+  }
+  int code() const { return nb_iter >= max_iter ? -2 : fail; }
+};
+
+struct Ops {
+  const sb2_csr* A;
+  const sb2_precond* M;
+  cudaStream_t s;
+  int n;
+  RedScratch* rs = nullptr;
+  int dot(const double* x, const double* y, double* out) { return sb2_dot(n, x, y, out, s); }
+  int nrm(const double* x, double* out) { return sb2_nrm2(n, x, out, s); }
+  int axpy(double a, const double* x, double* y) { return sb2_axpy(n, a, x, y, s); }
+  int scal(double a, double* x) { return sb2_scal(n, a, x, s); }
+  int copy(const double* x, double* y) { return sb2_copy(n, x, y, s); }
+  int mlt(const double* x, double* y) { return sb2_mlt(A, 0, 1.0, x, y, s); }
+  int residual(const double* b, const double* x, double* r) {
+    SB2_TRY(copy(b, r));
+    return sb2_spmv(A, 0, -1.0, x, 1.0, r, s);
+  }
+  int prec(const double* r, double* z) { return precond_apply(M, false, r, z, s); }
+};
+
+static int host_cg(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                   HostIter& it, double* V, int* init_failed) {
+  const int n = o.n;
+  double *p = V, *q = V + n, *r = V + 2 * (size_t)n, *z = V + 3 * (size_t)n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(n, 0.0, x, o.s)); }
+  double rho = 1.0, rho_1 = 1.0, res;
+  for (;;) {
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    SB2_TRY(o.prec(r, z));
+    SB2_TRY(o.dot(r, z, &rho));
+    if (rho == 0.0) { it.fail = 1; break; }
+    if (it.nb_iter == 0) SB2_TRY(o.copy(z, p));
+    else {
+      SB2_TRY(o.scal(rho / rho_1, p));
+      SB2_TRY(o.axpy(1.0, z, p));
+    }
+    SB2_TRY(o.mlt(p, q));
+    double delta;
+    SB2_TRY(o.dot(p, q, &delta));
+    if (delta == 0.0) { it.fail = 2; break; }
+    const double alpha = rho / delta;
+    SB2_TRY(o.axpy(alpha, p, x));
+    SB2_TRY(o.axpy(-alpha, q, r));
+    rho_1 = rho;
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
+static int host_bicgstab(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                         HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *p = V, *phat = V + n, *s = V + 2 * n, *shat = V + 3 * n, *t = V + 4 * n,
+         *v = V + 5 * n, *r = V + 6 * n, *rt = V + 7 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.copy(r, rt));
+  double rho_1, rho_2 = 0.0, alpha = 0.0, omega = 0.0, res;
+  for (;;) {
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    SB2_TRY(o.dot(rt, r, &rho_1));
+    if (rho_1 == 0.0) { it.fail = 1; break; }
+    if (it.nb_iter == 0) SB2_TRY(o.copy(r, p));
+    else {
+      if (omega == 0.0) { it.fail = 2; break; }
+      const double beta = (rho_1 / rho_2) * (alpha / omega);
+      SB2_TRY(o.axpy(-omega, v, p));
+      SB2_TRY(o.scal(beta, p));
+      SB2_TRY(o.axpy(1.0, r, p));
+    }
+    SB2_TRY(o.prec(p, phat));
+    SB2_TRY(o.mlt(phat, v));
+    double sigma;
+    SB2_TRY(o.dot(rt, v, &sigma));
+    if (sigma == 0.0) { it.fail = 3; break; }
+    alpha = rho_1 / sigma;
+    SB2_TRY(o.copy(r, s));
+    SB2_TRY(o.axpy(-alpha, v, s));
+    it.nb_iter++;
+    SB2_TRY(o.nrm(s, &res));
+    if (it.finished(res)) {
+      SB2_TRY(o.axpy(alpha, phat, x));
+      break;
+    }
+    SB2_TRY(o.prec(s, shat));
+    SB2_TRY(o.mlt(shat, t));
+    double ts, tt;
+    SB2_TRY(o.dot(t, s, &ts));
+    SB2_TRY(o.dot(t, t, &tt));
+    omega = ts / tt;
+    SB2_TRY(o.axpy(alpha, phat, x));
+    SB2_TRY(o.axpy(omega, shat, x));
+    SB2_TRY(o.copy(s, r));
+    SB2_TRY(o.axpy(-omega, t, r));
+    rho_2 = rho_1;
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
+static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
+  const double a = a_in, b = b_in;
+  const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
+  const double scal = std::fabs(a) + std::fabs(b);
+  double r, z;
+  if (scal != 0.0) {
+    volatile double a_scl = a / scal, b_scl = b / scal;
+    volatile double aa = a_scl * a_scl, bb = b_scl * b_scl;
+    r = scal * std::sqrt(aa + bb);
+    if (roe < 0.0) r *= -1.0;
+    c_ = a / r;
+    s_ = b / r;
+    z = 1.0;
+    if (std::fabs(a) > std::fabs(b)) z = s_;
+    else if (std::fabs(b) >= std::fabs(a) && c_ != 0.0) z = 1.0 / c_;
+  } else {
+    c_ = 1.0; s_ = 0.0; r = 0.0; z = 0.0;
+  }
+  a_in = r;
+  b_in = z;
+}
+
+static void host_applyrot(double& x, double& y, double c, double s) {
+  volatile double cx = c * x, sy = s * y, cy = c * y, sx = s * x;
+  const double temp = cx + sy;
+  y = cy - sx;
+  x = temp;
+}
+
+static int host_gmres(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                      HostIter& it, double* Vbuf, int* init_failed) {
+  const size_t n = o.n;
+  const int m = std::max(prm->restart, 1);
+  const int ld = m + 1;
+  double *w = Vbuf, *r = Vbuf + n, *u = Vbuf + 2 * n, *V = Vbuf + 3 * n;
+  std::vector<double> Hm((size_t)ld * ld, 0.0), s(ld, 0.0), cs(ld, 0.0), sn(ld, 0.0);
+  SB2_TRY(o.copy(b, w));
+  if (!prm->init_guess_null) SB2_TRY(sb2_spmv(o.A, 0, -1.0, x, 1.0, w, o.s));
+  else SB2_TRY(sb2_fill(o.n, 0.0, x, o.s));
+  SB2_TRY(o.prec(w, r));
+  double beta;
+  SB2_TRY(o.nrm(r, &beta));
+  if (beta == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / beta;
+  it.nb_iter = 0;
+  while (!it.finished(beta)) {
+    SB2_TRY(o.copy(r, V));
+    SB2_TRY(o.scal(1.0 / beta, V));
+    std::fill(s.begin(), s.end(), 0.0);
+    s[0] = beta;
+    int i = 0;
+    HostIter inner = it;
+    inner.max_iter = it.nb_iter + m;
+    bool stop;
+    do {
+      SB2_TRY(o.mlt(V + i * n, u));
+      SB2_TRY(o.prec(u, w));
+      for (int k = 0; k <= i; k++) {
+        double h;
+        SB2_TRY(o.dot(V + k * n, w, &h));
+        Hm[k + (size_t)i * ld] = h;
+        SB2_TRY(o.axpy(-h, V + k * n, w));
+      }
+      double hi;
+      SB2_TRY(o.nrm(w, &hi));
+      SB2_TRY(o.copy(w, V + (i + 1) * n));
+      if (hi != 0.0) SB2_TRY(o.scal(1.0 / hi, V + (i + 1) * n));
+      for (int k = 0; k < i; k++) host_applyrot(Hm[k + (size_t)i * ld], Hm[k + 1 + (size_t)i * ld], cs[k], sn[k]);
+      if (hi != 0.0) {
+        host_genrot(Hm[i + (size_t)i * ld], hi, cs[i], sn[i]);
+        host_applyrot(s[i], s[i + 1], cs[i], sn[i]);
+      }
+      inner.nb_iter++;
+      it.nb_iter++;
+      i++;
+      stop = inner.finished(std::fabs(s[i]));
+    } while (!stop);
+    it.hist = inner.hist;
+    for (int j = i - 1; j >= 0; j--)
+      if (s[j] != 0.0) {
+        s[j] = s[j] / Hm[j + (size_t)j * ld];
+        const double t = s[j];
+        for (int q = j - 1; q >= 0; q--) {
+          volatile double tq = t * Hm[q + (size_t)j * ld];
+          s[q] = s[q] - tq;
+        }
+      }
+    for (int k = 0; k < i; k++) SB2_TRY(o.axpy(s[k], V + k * n, x));
+    SB2_TRY(o.copy(b, w));
+    SB2_TRY(sb2_spmv(o.A, 0, -1.0, x, 1.0, w, o.s));
+    SB2_TRY(o.prec(w, r));
+    SB2_TRY(o.nrm(r, &beta));
+  }
+  return SB2_OK;
+}
+
+static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double* x,
+                      const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
+                      double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
+  const int n = A->m;
+  const int m = std::max(prm->restart, 1);
+  const int nvec = which == kCg ? 4 : (which == kBicg ? 8 : 3 + m + 1);
+  DeviceBuf buf;
+  buf.s = s;
+  SB2_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (size_t)std::max(n, 1) * nvec, s));
+  Ops o{A, M, s, n};
+  HostIter it;
+  it.tol = prm->tol;
+  it.max_iter = prm->max_iter;
+  int init_failed = 0;
+  double* V = (double*)buf.p;
+  if (which == kCg) SB2_TRY(host_cg(o, x, b, prm, it, V, &init_failed));
+  else if (which == kBicg) SB2_TRY(host_bicgstab(o, x, b, prm, it, V, &init_failed));
+  else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  res->init_failed = init_failed;
+  res->nb_iter = init_failed ? 0 : it.nb_iter;
+  res->error_code = init_failed ? (prm->max_iter <= 0 ? -2 : 0) : it.code();
+  res->facteur_reste = it.facteur;
+  res->last_residual = it.hist.empty() ? 0.0 : it.hist.back().second;
+  const int nh = std::min((int)it.hist.size(), std::max(hist_cap, 0));
+  for (int k = 0; k < nh; k++) {
+    if (hist) hist[k] = it.hist[k].second;
+    if (hist_it) hist_it[k] = it.hist[k].first;
+  }
+  res->hist_len = nh;
+  return SB2_OK;
+}
+
+static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double* x,
+                       const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
+                       double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
+  if (!A || !prm || !res || A->m != A->n) return SB2_ERR_INVALID_VALUE;
+  if (A->m > 0 && (!x || !b || x == b)) return SB2_ERR_INVALID_VALUE;
+  *res = sb2_iter_result{};
+  // Solvers return 0 for an empty system before touching anything (Cg.cxx:50-51)
+  if (A->m <= 0) return SB2_OK;
+  const int kind = M ? precond_kind(M) : SB2_PRECOND_IDENTITY;
+  if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
+  if (kind == SB2_PRECOND_SOR)
+    return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
+  const double* diag = nullptr;
+  if (kind == SB2_PRECOND_JACOBI) {
+    SB2_TRY(ensure_diag(A));
+    diag = A->d_diag;
+  }
+  return fused_solve(which, A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
+}
+
+}  // namespace sb2
+
+using namespace sb2;
 
 extern "C" {
-int sb2_cg(const sb2_csr*, const sb2_precond*, double*, const double*, const sb2_iter_params*, sb2_iter_result*, double*, int*, int, void*) { return SB2_ERR_NOT_SUPPORTED; }
-int sb2_bicgstab(const sb2_csr*, const sb2_precond*, double*, const double*, const sb2_iter_params*, sb2_iter_result*, double*, int*, int, void*) { return SB2_ERR_NOT_SUPPORTED; }
-int sb2_gmres(const sb2_csr*, const sb2_precond*, double*, const double*, const sb2_iter_params*, sb2_iter_result*, double*, int*, int, void*) { return SB2_ERR_NOT_SUPPORTED; }
+
+int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+           const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,
+           int hist_cap, void* stream) {
+  return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
 }
+
+int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+                 const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+                 int* hist_it, int hist_cap, void* stream) {
+  return solve_entry(kBicg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+}
+
+int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+              int* hist_it, int hist_cap, void* stream) {
+  return solve_entry(kGmres, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Persistent-kernel plumbing: a bounded grid barrier that also performs the
+// deterministic cross-CTA reduction, and the per-solve device state.
+//
+// The kernels using it are launched cooperatively (all CTAs co-resident).
+// Every wait is bounded by a wall-clock limit read from %globaltimer: a CTA
+// that waits too long sets `status` and the whole grid unwinds, so a solve can
+// never hang the GPU.
+#pragma once
+
+#include "spmv_core.cuh"
+
+namespace sb2 {
+
+constexpr int kMaxRed = 4;  // scalars reduced by one barrier at most
+
+struct GridSync {
+  unsigned count;  // arrivals at the current barrier
+  unsigned gen;    // barrier generation
+  int status;      // 0 ok, 1 a wait ran out
+  int pad;
+  double res[kMaxRed];
+};
+
+struct SolveOut {
+  int nb_iter;
+  int error_code;
+  int init_failed;
+  int hist_len;
+  double facteur_reste;
+  double last_residual;
+};
+
+struct Persist {
+  GridSync* sync;
+  double* partials;  // [kMaxRed * gridDim.x]
+  unsigned long long wait_ns;
+};
+
+// Record of the relative residual of one Finished() test.
+struct History {
+  double* res;
+  int* it;
+  int cap;
+};
+
+#ifdef __CUDACC__
+
+// Grid barrier.  Thread 0 of each CTA deposits K block sums (s_vals[0..K)),
+// the last CTA to arrive sums the deposits in CTA order (the same tree on
+// every run), publishes them and releases the grid; on return s_vals holds
+// the K grid sums in every CTA.  Returns false when a wait ran out or another
+// CTA reported so.
+template <int NT>
+__device__ __forceinline__ bool grid_sync(const Persist& P, unsigned& epoch, int K,
+                                          double* s_vals, double* s_red) {
+  __shared__ int s_last, s_ok;  // separate: a lagging warp may still read s_last
+  const int tid = threadIdx.x;
+  const unsigned G = gridDim.x;
+  if (tid == 0)
+    for (int k = 0; k < K; k++) P.partials[k * G + blockIdx.x] = s_vals[k];
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&P.sync->count, 1u);
+    s_last = (prev == G - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    for (int k = 0; k < K; k++) {
+      double v = 0.0;
+      for (unsigned i = tid; i < G; i += NT) v = add_rn(v, __ldcg(P.partials + k * G + i));
+      v = block_sum<NT>(v, s_red);
+      if (tid == 0) P.sync->res[k] = v;
+    }
+    if (tid == 0) {
+      P.sync->count = 0u;
+      __threadfence();
+      st_release_u32(&P.sync->gen, epoch + 1u);
+    }
+  } else if (tid == 0) {
+    const unsigned long long t0 = global_timer_ns();
+    while (ld_acquire_u32(&P.sync->gen) == epoch) {
+      if (global_timer_ns() - t0 > P.wait_ns) {
+        atomicExch(&P.sync->status, 1);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  if (tid == 0) {
+    for (int k = 0; k < K; k++) s_vals[k] = __ldcg(P.sync->res + k);
+    s_ok = (*((volatile int*)&P.sync->status) == 0) ? 1 : 0;
+  }
+  __syncthreads();
+  epoch++;
+  return s_ok != 0;
+}
+
+// Loads of vectors written inside the same persistent kernel go to L2
+// (the coherence point); the read-only matrix uses the streaming path.
+template <typename T>
+struct XLoadCg {
+  const T* x;
+  __device__ __forceinline__ T operator()(int j) const { return __ldcg(x + j); }
+};
+
+#endif  // __CUDACC__
+
+}  // namespace sb2

@@ -1,17 +1,411 @@
-// Preconditioners (placeholder entry points; filled in by the solver work).
+// Preconditioners: identity, Jacobi and level-scheduled SOR.
+//
+// SOR reproduces the reference's strictly sequential sweeps
+// (Relaxation_MatVect.cxx:41-95 RowSparse, :176-298 RowSymSparse) bit for
+// bit: rows are grouped into wavefront levels such that every value a row
+// reads is the one the sequential order would have read (true dependencies on
+// already-updated rows AND anti-dependencies on rows that must still hold
+// their old value), and each row repeats the reference's own operation order
+// with separately rounded products.
+#include <algorithm>
+#include <vector>
+
 #include "sb2_internal.cuh"
 
-struct sb2_precond {
-  int kind;
+namespace sb2 {
+
+struct LevelPlan {
+  int nlev = 0;
+  std::vector<int> h_lvl;      // [nlev+1] offsets into rows
+  int* d_rows = nullptr;       // rows ordered by level
+  int* d_lvl = nullptr;        // device copy of h_lvl
+  void release() {
+    cudaFree(d_rows);
+    cudaFree(d_lvl);
+    d_rows = d_lvl = nullptr;
+    h_lvl.clear();
+    nlev = 0;
+  }
 };
 
+static int upload_plan(const std::vector<int>& level, int n, LevelPlan* P) {
+  int nlev = 0;
+  for (int i = 0; i < n; i++) nlev = std::max(nlev, level[i] + 1);
+  P->nlev = nlev;
+  P->h_lvl.assign(nlev + 1, 0);
+  for (int i = 0; i < n; i++) P->h_lvl[level[i] + 1]++;
+  for (int l = 0; l < nlev; l++) P->h_lvl[l + 1] += P->h_lvl[l];
+  std::vector<int> rows(std::max(n, 1)), fill(P->h_lvl.begin(), P->h_lvl.end() - 1);
+  for (int i = 0; i < n; i++) rows[fill[level[i]]++] = i;  // increasing row in a level
+  SB2_CUDA_TRY(cudaMalloc(&P->d_rows, sizeof(int) * std::max(n, 1)));
+  SB2_CUDA_TRY(cudaMalloc(&P->d_lvl, sizeof(int) * (nlev + 1)));
+  SB2_CUDA_TRY(cudaMemcpy(P->d_rows, rows.data(), sizeof(int) * std::max(n, 1), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMemcpy(P->d_lvl, P->h_lvl.data(), sizeof(int) * (nlev + 1), cudaMemcpyHostToDevice));
+  return SB2_OK;
+}
+
+// Levels of a sequential sweep over rows in `order` (forward: increasing,
+// backward: decreasing).  Row j reads x(k) for every stored k: it must come
+// after k when k precedes j in the sweep (k is read updated) and before k
+// when k follows j (k is read old).
+static void sweep_levels(int n, const int* ptr, const int* ind, bool forward,
+                         std::vector<int>& level) {
+  level.assign(n, 0);
+  std::vector<int> req(n, 0);
+  for (int s = 0; s < n; s++) {
+    const int j = forward ? s : n - 1 - s;
+    int lev = req[j];
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+      const int c = ind[k];
+      const bool before = forward ? (c < j) : (c > j);
+      if (before) lev = std::max(lev, level[c] + 1);
+    }
+    level[j] = lev;
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+      const int c = ind[k];
+      const bool after = forward ? (c > j) : (c < j);
+      if (after) req[c] = std::max(req[c], lev + 1);
+    }
+  }
+}
+
+// Levels of a triangular solve: row j depends on the entries of `ptr/ind`
+// on the solved side (lower: c < j, upper: c > j).
+static void tri_levels(int n, const int* ptr, const int* ind, bool lower,
+                       std::vector<int>& level) {
+  level.assign(n, 0);
+  for (int s = 0; s < n; s++) {
+    const int j = lower ? s : n - 1 - s;
+    int lev = 0;
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) {
+      const int c = ind[k];
+      if (lower ? (c < j) : (c > j)) lev = std::max(lev, level[c] + 1);
+    }
+    level[j] = lev;
+  }
+}
+
+// ------------------------------------------------------------------ row ops
+
+#ifdef __CUDACC__
+// Plain loads: within one CTA (all levels in one launch) the SM's L1 holds
+// the CTA's own stores, and across launches every write is visible.
+__device__ __forceinline__ double ldx(const double* p) { return *p; }
+
+// RowSparse sweep, one row (Relaxation_MatVect.cxx:69-77 / :83-91).
+struct RowSparseSor {
+  const int* ptr; const int* ind; const double* val; const double* diag;
+  const double* b; double* x; double omega;
+  __device__ void operator()(int j) const {
+    double temp = 0.0;
+    const double ajj = diag[j];
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) temp = add_rn(temp, mul_rn(val[k], ldx(x + ind[k])));
+    const double xj = ldx(x + j);
+    temp = add_rn(__dsub_rn(b[j], temp), mul_rn(ajj, xj));
+    x[j] = add_rn(mul_rn(__dsub_rn(1.0, omega), xj), __ddiv_rn(mul_rn(omega, temp), ajj));
+  }
+};
+
+__device__ __forceinline__ double sym_diag(const int* uptr, const int* uind, const double* uval, int j) {
+  double ajj = 0.0;
+  for (int k = uptr[j]; k < uptr[j + 1]; k++)
+    if (uind[k] == j) ajj = add_rn(ajj, uval[k]);
+  return ajj;
+}
+
+// RowSymSparse forward, first loop (Relaxation_MatVect.cxx:214-230):
+// t_j = ((1-w)/w * ajj) * x_j + (b_j - sum_{p != j} a_jp x_p), x read old.
+struct SymFwd1 {
+  const int* uptr; const int* uind; const double* uval;
+  const double* b; const double* x; double* t; double omega;
+  __device__ void operator()(int j) const {
+    double temp = 0.0, ajj = 0.0;
+    for (int k = uptr[j]; k < uptr[j + 1]; k++) {
+      const int p = uind[k];
+      if (p == j) ajj = add_rn(ajj, uval[k]);
+      else temp = add_rn(temp, mul_rn(uval[k], ldx(x + p)));
+    }
+    temp = __dsub_rn(b[j], temp);
+    const double c = __ddiv_rn(__dsub_rn(1.0, omega), omega);
+    t[j] = add_rn(mul_rn(mul_rn(c, ajj), ldx(x + j)), temp);
+  }
+};
+
+// RowSymSparse forward, second loop as a gather (:232-249): x_j =
+// (t_j - a_{k1 j} x_{k1} - a_{k2 j} x_{k2} ...) * (w / ajj), k increasing.
+// fptr/find/fval: the full row, whose entries with column < j come first in
+// increasing column order (they mirror the strict upper part).
+struct SymFwd2 {
+  const int* fptr; const int* find; const double* fval;
+  const int* uptr; const int* uind; const double* uval;
+  const double* t; double* x; double omega;
+  __device__ void operator()(int j) const {
+    double v = t[j];
+    for (int k = fptr[j]; k < fptr[j + 1]; k++) {
+      const int c = find[k];
+      if (c >= j) break;
+      v = __dsub_rn(v, mul_rn(fval[k], ldx(x + c)));
+    }
+    const double ajj = sym_diag(uptr, uind, uval, j);
+    x[j] = mul_rn(v, __ddiv_rn(omega, ajj));
+  }
+};
+
+// RowSymSparse backward, first loop (:257-276): y_j = sum_{k<j} a_kj x_k (old x,
+// increasing k); t_j = (((1-w)/w * ajj) * x_j + b_j) - y_j.
+struct SymBwd1 {
+  const int* fptr; const int* find; const double* fval;
+  const int* uptr; const int* uind; const double* uval;
+  const double* b; const double* x; double* t; double omega;
+  __device__ void operator()(int j) const {
+    double y = 0.0;
+    for (int k = fptr[j]; k < fptr[j + 1]; k++) {
+      const int c = find[k];
+      if (c >= j) break;
+      y = add_rn(y, mul_rn(fval[k], ldx(x + c)));
+    }
+    const double ajj = sym_diag(uptr, uind, uval, j);
+    const double c0 = __ddiv_rn(__dsub_rn(1.0, omega), omega);
+    t[j] = __dsub_rn(add_rn(mul_rn(mul_rn(c0, ajj), ldx(x + j)), b[j]), y);
+  }
+};
+
+// RowSymSparse backward, second loop (:278-294): x_j = ((t_j - sum_{p != j}
+// a_jp x_p) * w) / ajj, rows decreasing, stored order.
+struct SymBwd2 {
+  const int* uptr; const int* uind; const double* uval;
+  const double* t; double* x; double omega;
+  __device__ void operator()(int j) const {
+    double temp = 0.0, ajj = 0.0;
+    for (int k = uptr[j]; k < uptr[j + 1]; k++) {
+      const int p = uind[k];
+      if (p == j) ajj = add_rn(ajj, uval[k]);
+      else temp = add_rn(temp, mul_rn(uval[k], ldx(x + p)));
+    }
+    x[j] = __ddiv_rn(mul_rn(__dsub_rn(t[j], temp), omega), ajj);
+  }
+};
+
+template <class Op>
+__global__ void rows_kernel(int n, Op op) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) op(j);
+}
+
+template <class Op>
+__global__ void level_kernel(int begin, int end, const int* __restrict__ rows, Op op) {
+  int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < end) op(rows[i]);
+}
+
+// All levels in one CTA, separated by __syncthreads (small systems).
+template <class Op>
+__global__ void __launch_bounds__(1024) level_single_cta(int nlev, const int* __restrict__ lvl,
+                                                         const int* __restrict__ rows, Op op) {
+  for (int l = 0; l < nlev; l++) {
+    for (int i = lvl[l] + threadIdx.x; i < lvl[l + 1]; i += blockDim.x) op(rows[i]);
+    __syncthreads();
+  }
+}
+
+__global__ void jacobi_kernel(int n, const double* __restrict__ r,
+                              const double* __restrict__ d, double* __restrict__ z) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    z[i] = __ddiv_rn(r[i], d[i]);
+}
+#endif
+
+constexpr int kSorSingleCtaMaxN = 65536;
+
+template <class Op>
+static int run_levels(const LevelPlan& P, int n, const Op& op, cudaStream_t s) {
+  if (n == 0 || P.nlev == 0) return SB2_OK;
+  if (n <= kSorSingleCtaMaxN) {
+    level_single_cta<Op><<<1, 1024, 0, s>>>(P.nlev, P.d_lvl, P.d_rows, op);
+  } else {
+    for (int l = 0; l < P.nlev; l++) {
+      const int cnt = P.h_lvl[l + 1] - P.h_lvl[l];
+      level_kernel<Op><<<(cnt + 255) / 256, 256, 0, s>>>(P.h_lvl[l], P.h_lvl[l + 1], P.d_rows, op);
+    }
+  }
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+template <class Op>
+static int run_rows(int n, const Op& op, cudaStream_t s) {
+  if (n == 0) return SB2_OK;
+  rows_kernel<Op><<<(n + 255) / 256, 256, 0, s>>>(n, op);
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+}  // namespace sb2
+
+struct sb2_precond {
+  const sb2_csr* A = nullptr;
+  int kind = 0;
+  double omega = 1.0;
+  int nb_iter = 1;
+  int symmetric = 1;
+  // SOR schedules: general forward/backward sweeps, or for symmetric storage
+  // the lower (forward) and upper (backward) triangular solves.
+  sb2::LevelPlan fwd, bwd;
+  double* d_t = nullptr;  // scratch of the symmetric sweeps
+  std::mutex mu;
+  bool planned = false;
+};
+
+namespace sb2 {
+
+static int plan_sor(sb2_precond* M) {
+  std::lock_guard<std::mutex> g(M->mu);
+  if (M->planned) return SB2_OK;
+  const sb2_csr* A = M->A;
+  const int n = A->m;
+  const CsrArrays& src = A->sym ? A->upper : A->full;
+  std::vector<int> ptr(n + 1), ind(src.nnz);
+  SB2_CUDA_TRY(cudaMemcpy(ptr.data(), src.d_ptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+  if (src.nnz) SB2_CUDA_TRY(cudaMemcpy(ind.data(), src.d_ind, sizeof(int) * src.nnz, cudaMemcpyDeviceToHost));
+  std::vector<int> level;
+  if (!A->sym) {
+    sweep_levels(n, ptr.data(), ind.data(), true, level);
+    SB2_TRY(upload_plan(level, n, &M->fwd));
+    sweep_levels(n, ptr.data(), ind.data(), false, level);
+    SB2_TRY(upload_plan(level, n, &M->bwd));
+  } else {
+    // forward second loop = lower solve (dependencies c < j of the full
+    // pattern); backward second loop = upper solve on the stored rows.
+    const CsrArrays& f = A->full;
+    std::vector<int> fptr(n + 1), find(f.nnz);
+    SB2_CUDA_TRY(cudaMemcpy(fptr.data(), f.d_ptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    if (f.nnz) SB2_CUDA_TRY(cudaMemcpy(find.data(), f.d_ind, sizeof(int) * f.nnz, cudaMemcpyDeviceToHost));
+    tri_levels(n, fptr.data(), find.data(), true, level);
+    SB2_TRY(upload_plan(level, n, &M->fwd));
+    tri_levels(n, ptr.data(), ind.data(), false, level);
+    SB2_TRY(upload_plan(level, n, &M->bwd));
+    SB2_CUDA_TRY(cudaMalloc(&M->d_t, sizeof(double) * std::max(n, 1)));
+  }
+  M->planned = true;
+  return SB2_OK;
+}
+
+// SOR(A, X, B, omega, iter, type_ssor) on device, in place on x.
+static int sor_apply(sb2_precond* M, double* x, const double* b, double omega,
+                     int iter, int type_ssor, cudaStream_t s) {
+  SB2_TRY(plan_sor(M));
+  const sb2_csr* A = M->A;
+  const int n = A->m;
+  if (!A->sym) {
+    SB2_TRY(ensure_diag(A));
+    RowSparseSor op{A->full.d_ptr, A->full.d_ind, A->full.d_val, A->d_diag, b, x, omega};
+    if (type_ssor % 2 == 0)
+      for (int i = 0; i < iter; i++) SB2_TRY(run_levels(M->fwd, n, op, s));
+    if (type_ssor % 3 == 0)
+      for (int i = 0; i < iter; i++) SB2_TRY(run_levels(M->bwd, n, op, s));
+    return SB2_OK;
+  }
+  const CsrArrays& u = A->upper;
+  const CsrArrays& f = A->full;
+  if (type_ssor % 2 == 0)
+    for (int i = 0; i < iter; i++) {
+      SB2_TRY(run_rows(n, SymFwd1{u.d_ptr, u.d_ind, u.d_val, b, x, M->d_t, omega}, s));
+      SB2_TRY(run_levels(M->fwd, n,
+                         SymFwd2{f.d_ptr, f.d_ind, f.d_val, u.d_ptr, u.d_ind, u.d_val, M->d_t, x, omega}, s));
+    }
+  if (type_ssor % 3 == 0)
+    for (int i = 0; i < iter; i++) {
+      SB2_TRY(run_rows(n, SymBwd1{f.d_ptr, f.d_ind, f.d_val, u.d_ptr, u.d_ind, u.d_val, b, x, M->d_t, omega}, s));
+      SB2_TRY(run_levels(M->bwd, n, SymBwd2{u.d_ptr, u.d_ind, u.d_val, M->d_t, x, omega}, s));
+    }
+  return SB2_OK;
+}
+
+int precond_kind(const sb2_precond* M) { return M->kind; }
+const sb2_csr* precond_matrix(const sb2_precond* M) { return M->A; }
+
+int precond_apply(const sb2_precond* cM, bool trans, const double* r, double* z,
+                  cudaStream_t s) {
+  sb2_precond* M = const_cast<sb2_precond*>(cM);
+  const int n = M->A->m;
+  if (n == 0) return SB2_OK;
+  if (M->kind == SB2_PRECOND_IDENTITY) {
+    SB2_CUDA_TRY(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return SB2_OK;
+  }
+  if (M->kind == SB2_PRECOND_JACOBI) {
+    SB2_TRY(ensure_diag(M->A));
+    int g = std::min((n + 255) / 256, num_sms(current_device()) * 8);
+    jacobi_kernel<<<g, 256, 0, s>>>(n, r, M->A->d_diag, z);
+    SB2_CUDA_TRY(cudaGetLastError());
+    return SB2_OK;
+  }
+  // SorPreconditioner::Solve / TransSolve (Precond_Ssor.cxx:62-90)
+  SB2_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(double) * n, s));
+  const int type = M->symmetric ? 0 : (trans ? 3 : 2);
+  return sor_apply(M, z, r, M->omega, M->nb_iter, type, s);
+}
+
+}  // namespace sb2
+
+using namespace sb2;
+
 extern "C" {
-int sb2_precond_create(const sb2_csr*, int, double, int, int, sb2_precond** out) {
-  if (out) *out = nullptr;
-  return SB2_ERR_NOT_SUPPORTED;
+
+int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
+                       int symmetric, sb2_precond** out) {
+  if (!out || !A) return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  if (kind < SB2_PRECOND_IDENTITY || kind > SB2_PRECOND_SOR) return SB2_ERR_INVALID_VALUE;
+  if (A->m != A->n) return SB2_ERR_INVALID_VALUE;
+  sb2_precond* M = new sb2_precond();
+  M->A = A;
+  M->kind = kind;
+  M->omega = omega;
+  M->nb_iter = nb_iter;
+  M->symmetric = symmetric ? 1 : 0;
+  if (kind == SB2_PRECOND_JACOBI) {
+    int st = ensure_diag(A);
+    if (st != SB2_OK) { delete M; return st; }
+  }
+  *out = M;
+  return SB2_OK;
 }
-int sb2_precond_destroy(sb2_precond* M) { delete M; return SB2_OK; }
-int sb2_precond_solve(const sb2_precond*, const double*, double*, void*) { return SB2_ERR_NOT_SUPPORTED; }
-int sb2_precond_trans_solve(const sb2_precond*, const double*, double*, void*) { return SB2_ERR_NOT_SUPPORTED; }
-int sb2_sor(const sb2_csr*, double*, const double*, double, int, int, void*) { return SB2_ERR_NOT_SUPPORTED; }
+
+int sb2_precond_destroy(sb2_precond* M) {
+  if (!M) return SB2_OK;
+  M->fwd.release();
+  M->bwd.release();
+  cudaFree(M->d_t);
+  delete M;
+  return SB2_OK;
 }
+
+int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+  if (!M || (M->A->m > 0 && (!r || !z)) || (r == z && M->A->m > 0)) return SB2_ERR_INVALID_VALUE;
+  return precond_apply(M, false, r, z, (cudaStream_t)stream);
+}
+
+int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+  if (!M || (M->A->m > 0 && (!r || !z)) || (r == z && M->A->m > 0)) return SB2_ERR_INVALID_VALUE;
+  return precond_apply(M, true, r, z, (cudaStream_t)stream);
+}
+
+int sb2_sor(const sb2_csr* A, double* x, const double* b, double omega, int iter,
+            int type_ssor, void* stream) {
+  if (!A || A->m != A->n || (A->m > 0 && (!x || !b)) || x == b) return SB2_ERR_INVALID_VALUE;
+  sb2_precond tmp;
+  tmp.A = A;
+  tmp.kind = SB2_PRECOND_SOR;
+  int st = sor_apply(&tmp, x, b, omega, iter, type_ssor, (cudaStream_t)stream);
+  // the plan is released after the stream has consumed it
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  tmp.fwd.release();
+  tmp.bwd.release();
+  cudaFree(tmp.d_t);
+  if (st == SB2_OK && e != cudaSuccess) st = map_cuda_error(e);
+  return st;
+}
+
+}  // extern "C"

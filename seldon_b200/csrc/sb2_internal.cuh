@@ -88,6 +88,8 @@ void free_csr(CsrArrays* a);
 int build_partition_host(const int* ptr, int rows, Partition* out);
 int ensure_transpose(const sb2_csr* A);
 int ensure_diag(const sb2_csr* A);
+int precond_kind(const sb2_precond* M);
+const sb2_csr* precond_matrix(const sb2_precond* M);
 
 // Per-(device, stream) scratch for reductions: kRedSlots partial sums and a
 // completion counter that the last CTA resets to zero.

@@ -1,0 +1,235 @@
+"""GPU parity of the preconditioners and Krylov drivers against the oracle.
+
+SOR must be bit-exact (level scheduling reproduces the sequential sweep).
+Solvers: same error code, iteration count within a few percent of the
+oracle's (reductions are summed in a different order), both solutions meet
+the stopping rule, and they agree to the accuracy the tolerance implies."""
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+from tests.helpers import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api(cuda):
+    from seldon_b200 import api
+    return api
+
+
+def _mats():
+    lp = matgen.lap2d(24)
+    up = matgen.upper(*lp)
+    cd = matgen.convdiff3d(7)
+    return {"lap": lp, "lap_up": up, "conv": cd}
+
+
+# ------------------------------------------------------------------ SOR
+
+@pytest.mark.parametrize("g", [12, 310])  # single-CTA path and per-level launches
+@pytest.mark.parametrize("sym", [False, True])
+@pytest.mark.parametrize("t", [0, 2, 3])
+def test_sor_bit_exact(api, oracle, g, sym, t):
+    full = matgen.lap2d(g) if sym else matgen.convdiff3d(max(4, g // 15))
+    A = matgen.upper(*full) if sym else full
+    n = A[0].size - 1
+    rng = np.random.default_rng(g + t)
+    x0, b = rng.standard_normal(n), rng.standard_normal(n)
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+    X = to_dev(x0)
+    api.SOR(M, X, to_dev(b), 1.37, 2, t)
+    ref = oracle.sor(*A, x0, b, 1.37, 2, t, sym=sym)
+    assert np.array_equal(to_host(X), ref)
+
+
+def test_precond_solve(api, oracle):
+    ptr, ind, val = matgen.convdiff3d(6)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    r = np.random.default_rng(2).standard_normal(n)
+    J = api.JacobiPreconditioner()
+    Z = to_dev(np.zeros(n))
+    J.Solve(A, to_dev(r), Z)
+    diag = np.array([val[ptr[i]:ptr[i + 1]][ind[ptr[i]:ptr[i + 1]] == i][0] for i in range(n)])
+    assert np.array_equal(to_host(Z), r / diag)
+    S = api.SorPreconditioner()
+    S.SetParameterRelaxation(1.2)
+    S.InitUnSymmetricPreconditioning()
+    S.Solve(A, to_dev(r), Z)
+    assert np.array_equal(to_host(Z), oracle.sor(ptr, ind, val, np.zeros(n), r, 1.2, 1, 2))
+    S.TransSolve(A, to_dev(r), Z)
+    assert np.array_equal(to_host(Z), oracle.sor(ptr, ind, val, np.zeros(n), r, 1.2, 1, 3))
+    S.InitSymmetricPreconditioning()
+    S.Solve(A, to_dev(r), Z)
+    assert np.array_equal(to_host(Z), oracle.sor(ptr, ind, val, np.zeros(n), r, 1.2, 1, 0))
+
+
+# ------------------------------------------------------------------ drivers
+
+def _precond(api, pc):
+    if pc == 0:
+        return api.Preconditioner_Base()
+    if pc == 1:
+        return api.JacobiPreconditioner()
+    S = api.SorPreconditioner()
+    S.SetParameterRelaxation(1.2)
+    return S
+
+
+SOLVER_CASES = [
+    ("cg", "lap", 0), ("cg", "lap", 1), ("cg", "lap", 2),
+    ("cg", "lap_up", 0), ("cg", "lap_up", 1), ("cg", "lap_up", 2),
+    ("bicgstab", "conv", 0), ("bicgstab", "conv", 1), ("bicgstab", "conv", 2),
+    ("gmres", "conv", 0), ("gmres", "conv", 1), ("gmres", "conv", 2),
+    ("gmres", "lap_up", 1),
+]
+
+
+@pytest.mark.parametrize("which,mname,pc", SOLVER_CASES)
+def test_solver_parity(api, oracle, which, mname, pc):
+    mats = _mats()
+    sym = mname.endswith("_up")
+    A = mats[mname]
+    full = mats["lap"] if sym else A
+    n = A[0].size - 1
+    rng = np.random.default_rng(3)
+    b = matgen.matvec(*full, rng.uniform(-1, 1, n))
+    tol, restart = 1e-10, 8
+    xo, co, no, ho, hio = oracle.solve(which, *A, b, sym=sym, precond=pc, omega=1.2, tol=tol,
+                                       max_iter=2000, restart=restart, hist_cap=10000)
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(2000, tol)
+    it.SetRestart(restart)
+    it.HideMessages()
+    fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
+    code = fn(M, X, to_dev(b), _precond(api, pc), it)
+    x = to_host(X)
+    assert code == co == 0
+    nb = it.GetNumberIteration()
+    assert abs(nb - no) <= max(2, int(0.05 * no)), (nb, no)
+    # both meet the rule on the true residual to within the recurrence drift
+    for xx in (x, xo):
+        r = b - matgen.matvec(*full, xx)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 50 * tol
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+    # residual history: same length as the oracle's within the iteration slack,
+    # same first entry, decreasing to below tol
+    h = np.array([r for _, r in it.history])
+    assert h[0] == pytest.approx(ho[0], rel=1e-12)
+    assert h[-1] < tol
+
+
+def test_cg_deterministic(api):
+    ptr, ind, val = matgen.lap2d(40)
+    n = ptr.size - 1
+    b = matgen.matvec(ptr, ind, val, np.random.default_rng(1).uniform(-1, 1, n))
+    A = api.RowSparse(n, n, ptr, ind, val)
+    outs = []
+    for _ in range(2):
+        X = to_dev(np.zeros(n))
+        it = api.Iteration(5000, 1e-10)
+        it.HideMessages()
+        api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it)
+        outs.append((to_host(X), it.GetNumberIteration()))
+    assert outs[0][1] == outs[1][1]
+    assert np.array_equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres"])
+def test_zero_rhs_and_max_iter(api, oracle, which):
+    ptr, ind, val = matgen.lap2d(6)
+    n = 36
+    A = api.RowSparse(n, n, ptr, ind, val)
+    fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
+    # zero right-hand side.  Cg/BiCgStab test Init(b): it fails, x is left
+    # untouched and ErrorCode() is 0.  Gmres tests Init(M^{-1}(b - A x0))
+    # (Gmres.cxx:82-93), so with x0 != 0 it solves A x = 0 like the oracle.
+    x0 = np.arange(n, dtype=float)
+    X = to_dev(x0)
+    it = api.Iteration(100, 1e-10)
+    it.HideMessages()
+    it.SetInitGuess(False)
+    assert fn(A, X, to_dev(np.zeros(n)), api.Preconditioner_Base(), it) == 0
+    if which == "gmres":
+        xo, co, no, _, _ = oracle.solve(which, ptr, ind, val, np.zeros(n), x0=x0, tol=1e-10,
+                                        max_iter=100)
+        assert co == 0 and abs(it.GetNumberIteration() - no) <= 2
+        assert np.abs(to_host(X)).max() < 1e-7 * np.abs(x0).max()
+    else:
+        assert np.array_equal(to_host(X), x0)
+    X = to_dev(x0)
+    it.SetInitGuess(True)
+    assert fn(A, X, to_dev(np.zeros(n)), api.Preconditioner_Base(), it) == 0
+    assert np.array_equal(to_host(X), np.zeros(n))  # null guess: x zeroed, then Init fails
+    # max_iter reached -> -2 with exactly max_iter iterations (GMRES: a multiple
+    # of the restart length may overshoot exactly like the reference)
+    b = np.ones(n)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(3, 1e-30)
+    it.HideMessages()
+    it.SetRestart(2)
+    code = fn(A, X, to_dev(b), api.Preconditioner_Base(), it)
+    _, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, tol=1e-30, max_iter=3, restart=2)
+    assert code == co == -2
+    assert it.GetNumberIteration() == no
+
+
+def test_warm_start(api, oracle):
+    ptr, ind, val = matgen.lap2d(20)
+    n = ptr.size - 1
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(n)
+    x0 = rng.standard_normal(n)
+    A = api.RowSparse(n, n, ptr, ind, val)
+    for which, fn in (("cg", api.Cg), ("bicgstab", api.BiCgStab), ("gmres", api.Gmres)):
+        X = to_dev(x0)
+        it = api.Iteration(1000, 1e-9)
+        it.HideMessages()
+        it.SetInitGuess(False)
+        it.SetRestart(15)
+        assert fn(A, X, to_dev(b), api.Preconditioner_Base(), it) == 0
+        xo, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, x0=x0, tol=1e-9, max_iter=1000,
+                                        restart=15)
+        assert abs(it.GetNumberIteration() - no) <= max(2, no // 20)
+        assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-6
+
+
+def test_breakdowns(api, oracle):
+    # CG breakdown #2: (p, Ap) == 0 on diag(1, -1)
+    A = api.RowSparse(2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, -1.0]))
+    it = api.Iteration(10, 1e-12)
+    it.HideMessages()
+    X = to_dev(np.zeros(2))
+    assert api.Cg(A, X, to_dev(np.array([1.0, 1.0])), api.Preconditioner_Base(), it) == 2
+    # BiCGSTAB breakdown #3: (rtilde, A p) == 0 for the swap matrix
+    P = api.RowSparse(2, 2, np.array([0, 1, 2]), np.array([1, 0]), np.array([1.0, 1.0]))
+    it = api.Iteration(10, 1e-12)
+    it.HideMessages()
+    X = to_dev(np.zeros(2))
+    code = api.BiCgStab(P, X, to_dev(np.array([1.0, 0.0])), api.Preconditioner_Base(), it)
+    _, co, _, _, _ = oracle.solve("bicgstab", np.array([0, 1, 2]), np.array([1, 0]),
+                                  np.array([1.0, 1.0]), np.array([1.0, 0.0]), tol=1e-12,
+                                  max_iter=10)
+    assert code == co == 3
+
+
+def test_history_matches_oracle(api, oracle):
+    ptr, ind, val = matgen.convdiff3d(6)
+    n = ptr.size - 1
+    b = np.random.default_rng(4).standard_normal(n)
+    A = api.RowSparse(n, n, ptr, ind, val)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(500, 1e-10)
+    it.HideMessages()
+    it.SetRestart(5)
+    api.Gmres(A, X, to_dev(b), api.JacobiPreconditioner(), it)
+    _, _, _, ho, hio = oracle.solve("gmres", ptr, ind, val, b, precond=1, tol=1e-10, max_iter=500,
+                                    restart=5, hist_cap=5000)
+    its = [i for i, _ in it.history]
+    res = np.array([r for _, r in it.history])
+    k = min(len(res), len(ho)) - 2
+    assert its[:k] == hio[:k].tolist()
+    np.testing.assert_allclose(res[:k], ho[:k], rtol=1e-6)

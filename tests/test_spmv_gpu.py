@@ -167,7 +167,8 @@ def test_blas1(api, oracle, n):
     assert abs(d - oracle.dot(x, y)) <= 1e-13 * np.abs(x * y).sum()
     assert api.DotProd(X, Y) == d  # deterministic
     nr = api.Norm2(X)
-    assert abs(nr - oracle.nrm2(x)) <= 1e-14 * nr
+    # the oracle sums sequentially: its own error grows like n*eps
+    assert abs(nr - oracle.nrm2(x)) <= 1e-12 * nr
     api.Add(0.75, X, Y)
     assert np.array_equal(to_host(Y), y + 0.75 * x)
     api.Mlt(-2.0, X)
