@@ -1,0 +1,439 @@
+"""Benchmark of the Seldon sparse Krylov path on B200.
+
+One step = one FP64 CSR SpMV y = A*x (Seldon's Mlt on Matrix<double,
+General, RowSparse>) on the 3D 7-point upwind convection-diffusion matrix of
+a 128^3 grid (n = 2,097,152, nnz = 14,581,760).  `value` is whole-job HBM
+throughput in algorithmic GB/s (nnz*(8+4) + 4*(n+1) + 8*n + 8*n bytes per
+SpMV); the inputs (217 MB) exceed the 126 MB L2.
+
+The same JSON line carries the time-to-solution figures of the path (CG on
+the 100^2 Laplacian, FP64 CG on the 192^3 Poisson problem, GMRES(30)+Jacobi
+on the 128^3 convection-diffusion problem, the Zipf SpMV) and the roofline,
+e2e, cpu_baseline and clock records.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: replicas only (the path does not shard, one system per GPU); under
+torchrun every rank runs the same step and `value` is the sum over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("ms to 1e-10 rel. residual: mixed/batched vs plain FP64 GPU CG; SpMV HBM GB/s")
+WORKLOAD = "fp64 CSR SpMV, 3D 7-pt upwind convection-diffusion 128^3 (n=2097152, nnz=14581760)"
+GRID = 128
+
+
+def spmv_bytes(n, m, nnz, vbytes=8, wbytes=8):
+    return nnz * (vbytes + 4) + 4 * (m + 1) + n * wbytes + m * wbytes
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-extras", action="store_true", help="skip the solver/Zipf extras")
+    p.add_argument("--cpu-seconds", type=float, default=8.0,
+                   help="bounded CPU-baseline sample (seconds of work)")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference CPU arm
+
+def cpu_reference_spmv(ptr, ind, val, seconds, threads):
+    """The reference's own MltAdd (oracle/_ref, Seldon's templates compiled
+    from its headers) on the host cores: `threads` independent products of
+    the same matrix (one output vector each), repeated until ~`seconds`.
+    Returns (GB/s aggregate, spmv count, threads, wall seconds)."""
+    from oracle.pyoracle import REF_FAST_SO, Reference, Oracle
+    if Reference.available(REF_FAST_SO):
+        lib, kind = Reference(REF_FAST_SO), "reference"
+    else:
+        lib, kind = Oracle(), "port"
+    m = ptr.size - 1
+    x = np.random.default_rng(0).standard_normal(m)
+    one = time.perf_counter()
+    lib.mltadd(m, m, ptr, ind, val, 1.0, x, 0.0, np.zeros(m))
+    one = time.perf_counter() - one
+    reps = max(1, int(seconds / max(one, 1e-6) / 1.0))
+    counts = [0] * threads
+
+    p_ = np.ascontiguousarray(ptr, dtype=np.int32)
+    i_ = np.ascontiguousarray(ind, dtype=np.int32)
+    v_ = np.ascontiguousarray(val, dtype=np.float64)
+
+    def work(t):
+        y = np.zeros(m)
+        fn = lib.lib.ref_mltadd if kind == "reference" else None
+        for _ in range(reps):
+            if fn is not None:
+                fn(m, m, i_.size, p_.ctypes.data, i_.ctypes.data, v_.ctypes.data, 0, 0,
+                   ctypes.c_double(1.0), x.ctypes.data, ctypes.c_double(0.0), y.ctypes.data)
+            else:
+                lib.lib.orc_mltadd(m, m, p_.ctypes.data, i_.ctypes.data, v_.ctypes.data, 0, 0,
+                                   ctypes.c_double(1.0), x.ctypes.data, ctypes.c_double(0.0),
+                                   y.ctypes.data)
+            counts[t] += 1
+
+    ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    t0 = time.perf_counter()
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    wall = time.perf_counter() - t0
+    total = sum(counts)
+    gbs = total * spmv_bytes(m, m, ind.size) / wall / 1e9
+    return gbs, total, threads, wall, kind
+
+
+def host_threads():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from seldon_b200 import matgen
+    ptr, ind, val = matgen.convdiff3d(GRID)
+    n = ptr.size - 1
+    threads = min(host_threads(), 64)
+    # each step: a bounded sample (threads concurrent products)
+    per_step = []
+    kind = "reference"
+    for s in range(args.warmup + args.steps):
+        gbs, cnt, th, wall, kind = cpu_reference_spmv(ptr, ind, val, 0.0, threads)
+        if s >= args.warmup:
+            per_step.append((gbs, cnt, wall))
+    tot_bytes = sum(c for _, c, _ in per_step) * spmv_bytes(n, n, ind.size)
+    tot_wall = sum(w for _, _, w in per_step)
+    value = tot_bytes / tot_wall / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot_wall / len(per_step) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads, one product each"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
+                         "kind": kind,
+                         "sample": f"{threads} concurrent Seldon MltAdd products per step"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+
+def read_traffic():
+    """dram bytes per SpMV launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "spmv_csr_fp64_convdiff128.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_bytes_per_launch:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+
+    from seldon_b200 import api, matgen
+    from seldon_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    L = _lib.load()
+
+    ptr, ind, val = matgen.convdiff3d(GRID)
+    n = ptr.size - 1
+    nnz = ind.size
+    A = api.RowSparse(n, n, ptr, ind, val)
+    B = spmv_bytes(n, n, nnz)
+    x = torch.rand(n, dtype=torch.float64, device=dev)
+    y = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        api.Mlt(A, x, y)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            api.Mlt(A, x, y)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * B / (ms_max * 1e-3) / 1e9
+    kernel_gbs = B / (ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # e2e: host (pinned) x in, y out, through the C ABI host entry point
+    xh = torch.empty(n, dtype=torch.float64).pin_memory()
+    yh = torch.empty(n, dtype=torch.float64).pin_memory()
+    xh.copy_(x.cpu())
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    for _ in range(max(2, args.warmup)):
+        _lib.check(L.sb2_mlt_host(A.handle, 0, 1.0, ctypes.c_void_p(xh.data_ptr()),
+                                  ctypes.c_void_p(yh.data_ptr()), sp), "sb2_mlt_host")
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        L.sb2_mlt_host(A.handle, 0, 1.0, ctypes.c_void_p(xh.data_ptr()),
+                       ctypes.c_void_p(yh.data_ptr()), sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * B / (e2e_ms * 1e-3) / 1e9
+    ok = np.allclose(yh.numpy(), y.cpu().numpy(), rtol=0, atol=0)
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras = run_extras(api, matgen, torch, dev)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        gbs, cnt, th, wall, kind = cpu_reference_spmv(ptr, ind, val, args.cpu_seconds,
+                                                      min(host_threads(), 64))
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": th, "kind": kind,
+               "sample": f"{cnt} Seldon MltAdd products of the same 128^3 matrix on {th} "
+                         f"threads in {wall:.1f} s"}
+
+    if rank == 0:
+        traffic = read_traffic()
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, seldon_b200/matgen.py)",
+            "config": {"workload": WORKLOAD, "nnz": int(nnz), "n": int(n),
+                       "bytes_per_step": int(B), "l2": "inputs 217 MB > 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(kernel_gbs / peak, 4),
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "sb2::spmv_kernel<256>"},
+            "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": 8 * n, "ms_per_step": round(e2e_ms, 4),
+                    "matches_device_result": bool(ok)},
+            "gpu_launches": args.steps * 2,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_extras(api, matgen, torch, dev):
+    """Time-to-solution figures on the other configurations (device-timed)."""
+    out = {}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    rng = np.random.default_rng(2024)
+    # C1: CG, identity, 100^2 Laplacian stored RowSymSparse
+    ptr, ind, val = matgen.lap2d(100)
+    n = ptr.size - 1
+    xs = rng.uniform(-1, 1, n)
+    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
+    S = api.RowSymSparse(n, *matgen.upper(ptr, ind, val))
+
+    def cg_c1():
+        X = torch.zeros(n, dtype=torch.float64, device=dev)
+        it = api.Iteration(10000, 1e-10)
+        it.HideMessages()
+        api.Cg(S, X, b, api.Preconditioner_Base(), it)
+        return it
+    cg_c1()
+    ms, it = timed(cg_c1)
+    out["cg_lap2d_100"] = {"ms": round(ms, 3), "iterations": it.GetNumberIteration(),
+                           "rel_residual": it.history[-1][1]}
+    # C3 FP64 CG, 192^3 Poisson
+    ptr, ind, val = matgen.poisson3d(192)
+    n = ptr.size - 1
+    xs = rng.uniform(-1, 1, n)
+    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
+    A = api.RowSparse(n, n, ptr, ind, val)
+
+    def cg_c3():
+        X = torch.zeros(n, dtype=torch.float64, device=dev)
+        it = api.Iteration(20000, 1e-10)
+        it.HideMessages()
+        api.Cg(A, X, b, api.Preconditioner_Base(), it)
+        return it, X
+    ms, (it, X) = timed(cg_c3)
+    fe = float(np.linalg.norm(X.cpu().numpy() - xs) / np.linalg.norm(xs))
+    per_it = (spmv_bytes(n, n, ind.size) + 10 * 8 * n)
+    out["cg_fp64_poisson192"] = {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
+                                 "rel_residual": it.history[-1][1], "forward_error": fe,
+                                 "gbs_per_iteration_model": round(
+                                     per_it * it.GetNumberIteration() / (ms * 1e-3) / 1e9, 1)}
+    del A
+    # C2a GMRES(30) + Jacobi
+    ptr, ind, val = matgen.convdiff3d(GRID)
+    n = ptr.size - 1
+    xs = rng.uniform(-1, 1, n)
+    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
+    A = api.RowSparse(n, n, ptr, ind, val)
+
+    def gm():
+        X = torch.zeros(n, dtype=torch.float64, device=dev)
+        it = api.Iteration(20000, 1e-10)
+        it.HideMessages()
+        it.SetRestart(30)
+        api.Gmres(A, X, b, api.JacobiPreconditioner(), it)
+        return it
+    ms, it = timed(gm)
+    out["gmres30_jacobi_convdiff128"] = {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
+                                         "rel_residual": it.history[-1][1]}
+    del A
+    # C2b Zipf SpMV
+    ptr, ind, val = matgen.zipf_csr(1_000_000, seed=1)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    x = torch.rand(n, dtype=torch.float64, device=dev)
+    y = torch.zeros(n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        api.Mlt(A, x, y)
+    ms, _ = timed(lambda: [api.Mlt(A, x, y) for _ in range(20)])
+    Bz = spmv_bytes(n, n, ind.size)
+    out["spmv_zipf_1e6"] = {"gbs": round(Bz / (ms / 20 * 1e-3) / 1e9, 1), "nnz": int(ind.size),
+                            "us": round(ms / 20 * 1e3, 1)}
+    return out
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -106,6 +106,17 @@ int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
 int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
                  const double* x_host, double* y_host, void* stream);
 
+/* Product algorithm and launch configuration, chosen by the autotuner; no
+ * counterpart in the reference (tuning knobs of this engine).
+ *   algo     SB2_SPMV_SELL   binned SELL-32 (thread/warp/CTA per row), default
+ *            SB2_SPMV_STREAM row blocks streamed through shared memory
+ *            SB2_SPMV_TMA    row blocks in a TMA bulk-copy ring
+ *   threads  256 or 512 (TMA kernel), stages 3 or 4 (TMA ring depth) */
+#define SB2_SPMV_SELL 0
+#define SB2_SPMV_STREAM 1
+#define SB2_SPMV_TMA 2
+int sb2_spmv_set_config(int algo, int threads, int stages);
+
 /* ------------------------------------------------------------ BLAS-1 (FP64) */
 /* All reductions are deterministic: the same n gives the same summation tree
  * on every call and every run. */

@@ -18,6 +18,10 @@ SB2_ERR_TIMEOUT = -4
 SB2_ERR_INVALID_CSR = -5
 SB2_ERR_NOT_SUPPORTED = -6
 
+SPMV_SELL = 0
+SPMV_STREAM = 1
+SPMV_TMA = 2
+
 PRECOND_IDENTITY = 0
 PRECOND_JACOBI = 1
 PRECOND_SOR = 2
@@ -78,6 +82,7 @@ _PROTOS = [
      [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, ctypes.c_double, c_void_p, c_void_p]),
     ("sb2_mlt_host", ctypes.c_int,
      [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    ("sb2_spmv_set_config", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("sb2_dot", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_double_p, c_void_p]),
     ("sb2_nrm2", ctypes.c_int, [ctypes.c_int, c_void_p, c_double_p, c_void_p]),
     ("sb2_dot_device", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p]),

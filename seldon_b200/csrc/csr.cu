@@ -94,13 +94,153 @@ int build_partition_host(const int* ptr, int rows, Partition* out) {
   return SB2_OK;
 }
 
+// Partition for the TMA-pipelined kernel: blocks of <= 2048 nonzeros and
+// <= 512 rows; a row longer than 256 is a block of its own, summed by the
+// whole CTA.  Not applicable (nblk = -1) when a row exceeds one stage.
+int build_tma_partition_host(const int* ptr, int rows, Partition* out) {
+  constexpr int kCap = 2048, kRowCapT = 512, kCtaRow = 256;
+  std::vector<int> blk;
+  std::vector<unsigned char> kind;
+  int r = 0;
+  while (r < rows) {
+    const int len0 = ptr[r + 1] - ptr[r];
+    if (len0 > kCap) {
+      out->nblk = -1;
+      return SB2_OK;
+    }
+    if (len0 > kCtaRow) {
+      blk.push_back(r);
+      kind.push_back(2);
+      r++;
+      continue;
+    }
+    const int start = r;
+    int nnz = 0, maxlen = 0;
+    while (r < rows && r - start < kRowCapT) {
+      const int len = ptr[r + 1] - ptr[r];
+      if (len > kCtaRow || nnz + len > kCap) break;
+      nnz += len;
+      maxlen = std::max(maxlen, len);
+      r++;
+    }
+    blk.push_back(start);
+    kind.push_back(maxlen <= kThreadRowMax ? 0 : 1);
+  }
+  blk.push_back(rows);
+  out->nblk = (int)kind.size();
+  SB2_CUDA_TRY(cudaMalloc(&out->d_blk, sizeof(int) * blk.size()));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_blk, blk.data(), sizeof(int) * blk.size(), cudaMemcpyHostToDevice));
+  if (out->nblk > 0) {
+    SB2_CUDA_TRY(cudaMalloc(&out->d_kind, kind.size()));
+    SB2_CUDA_TRY(cudaMemcpy(out->d_kind, kind.data(), kind.size(), cudaMemcpyHostToDevice));
+    std::vector<int4> desc(out->nblk);
+    for (int b = 0; b < out->nblk; b++)
+      desc[b] = make_int4(blk[b], blk[b + 1] | ((int)kind[b] << 30), ptr[blk[b]], ptr[blk[b + 1]]);
+    SB2_CUDA_TRY(cudaMalloc(&out->d_desc, sizeof(int4) * desc.size()));
+    SB2_CUDA_TRY(cudaMemcpy(out->d_desc, desc.data(), sizeof(int4) * desc.size(), cudaMemcpyHostToDevice));
+  }
+  return SB2_OK;
+}
+
+// Binned SELL-32: short rows in slices of 32 (sorted by length when the
+// lengths are irregular), longer rows listed for the warp and CTA bins.
+int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
+                    SellArrays* out) {
+  constexpr int kMax = 32, kCta = 1024;
+  if (rows >= (1 << 26)) {
+    out->nslice = -1;
+    return SB2_OK;
+  }
+  std::vector<int> shortr, wr, cr;
+  int lmin = kMax, lmax = 0;
+  for (int i = 0; i < rows; i++) {
+    const int len = ptr[i + 1] - ptr[i];
+    if (len <= kMax) {
+      shortr.push_back(i);
+      lmin = std::min(lmin, len);
+      lmax = std::max(lmax, len);
+    } else if (len <= kCta) {
+      wr.push_back(i);
+    } else {
+      cr.push_back(i);
+    }
+  }
+  // sort only when the slices would otherwise carry much padding
+  out->sorted = (lmax - lmin) > 8;
+  if (out->sorted)
+    std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
+      return (ptr[a + 1] - ptr[a]) > (ptr[b + 1] - ptr[b]);
+    });
+  const int ns = (int)((shortr.size() + 31) / 32);
+  std::vector<long long> sptr(ns + 1, 0);
+  std::vector<unsigned> rinfo((size_t)ns * 32, (1u << 26) - 1u);
+  for (int sl = 0; sl < ns; sl++) {
+    int w = 0;
+    for (int l = 0; l < 32; l++) {
+      const size_t q = (size_t)sl * 32 + l;
+      if (q < shortr.size()) {
+        const int r = shortr[q], len = ptr[r + 1] - ptr[r];
+        w = std::max(w, len);
+        rinfo[q] = (unsigned)r | ((unsigned)len << 26);
+      }
+    }
+    sptr[sl + 1] = sptr[sl] + 32ll * w;
+  }
+  const long long tot = sptr[ns];
+  std::vector<int> scol(std::max(tot, 1ll), 0);
+  std::vector<double> sval(std::max(tot, 1ll), 0.0);
+  for (int sl = 0; sl < ns; sl++)
+    for (int l = 0; l < 32; l++) {
+      const size_t q = (size_t)sl * 32 + l;
+      if (q >= shortr.size()) continue;
+      const int r = shortr[q];
+      for (int j = 0; j < ptr[r + 1] - ptr[r]; j++) {
+        const long long e = sptr[sl] + (long long)j * 32 + l;
+        scol[e] = ind[ptr[r] + j];
+        sval[e] = val[ptr[r] + j];
+      }
+    }
+  out->nslice = ns;
+  out->padded = tot;
+  out->nwarp = (int)wr.size();
+  out->ncta = (int)cr.size();
+  SB2_CUDA_TRY(cudaMalloc(&out->d_sptr, sizeof(long long) * (ns + 1)));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_sptr, sptr.data(), sizeof(long long) * (ns + 1), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_rinfo, sizeof(unsigned) * std::max<size_t>(rinfo.size(), 1)));
+  if (!rinfo.empty())
+    SB2_CUDA_TRY(cudaMemcpy(out->d_rinfo, rinfo.data(), sizeof(unsigned) * rinfo.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_scol, sizeof(int) * scol.size()));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_scol, scol.data(), sizeof(int) * scol.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_sval, sizeof(double) * sval.size()));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_sval, sval.data(), sizeof(double) * sval.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_wrows, sizeof(int) * std::max<size_t>(wr.size(), 1)));
+  if (!wr.empty()) SB2_CUDA_TRY(cudaMemcpy(out->d_wrows, wr.data(), sizeof(int) * wr.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_crows, sizeof(int) * std::max<size_t>(cr.size(), 1)));
+  if (!cr.empty()) SB2_CUDA_TRY(cudaMemcpy(out->d_crows, cr.data(), sizeof(int) * cr.size(), cudaMemcpyHostToDevice));
+  return SB2_OK;
+}
+
+void free_sell(SellArrays* s) {
+  cudaFree(s->d_sptr);
+  cudaFree(s->d_rinfo);
+  cudaFree(s->d_scol);
+  cudaFree(s->d_sval);
+  cudaFree(s->d_sval32);
+  cudaFree(s->d_wrows);
+  cudaFree(s->d_crows);
+  *s = SellArrays();
+}
+
 int upload_csr(int rows, int cols, const int* ptr, const int* ind,
                const double* val, CsrArrays* out) {
   out->rows = rows;
   out->cols = cols;
   out->nnz = ptr[rows];
   const long long cap = padded_nnz(out->nnz);
-  SB2_CUDA_TRY(cudaMalloc(&out->d_ptr, sizeof(int) * (rows + 1)));
+  const long long pcap = padded_rows(rows);
+  for (int i = 0; i < rows; i++) out->max_row = std::max(out->max_row, ptr[i + 1] - ptr[i]);
+  SB2_CUDA_TRY(cudaMalloc(&out->d_ptr, sizeof(int) * pcap));
+  SB2_CUDA_TRY(cudaMemset(out->d_ptr, 0, sizeof(int) * pcap));
   SB2_CUDA_TRY(cudaMalloc(&out->d_ind, sizeof(int) * cap));
   SB2_CUDA_TRY(cudaMalloc(&out->d_val, sizeof(double) * cap));
   SB2_CUDA_TRY(cudaMemcpy(out->d_ptr, ptr, sizeof(int) * (rows + 1), cudaMemcpyHostToDevice));
@@ -111,7 +251,9 @@ int upload_csr(int rows, int cols, const int* ptr, const int* ind,
     SB2_CUDA_TRY(cudaMemcpy(out->d_ind, ind, sizeof(int) * out->nnz, cudaMemcpyHostToDevice));
     SB2_CUDA_TRY(cudaMemcpy(out->d_val, val, sizeof(double) * out->nnz, cudaMemcpyHostToDevice));
   }
-  return build_partition_host(ptr, rows, &out->part);
+  SB2_TRY(build_partition_host(ptr, rows, &out->part));
+  SB2_TRY(build_sell_host(ptr, ind, val, rows, &out->sell));
+  return build_tma_partition_host(ptr, rows, &out->tma);
 }
 
 void free_csr(CsrArrays* a) {
@@ -120,6 +262,10 @@ void free_csr(CsrArrays* a) {
   cudaFree(a->d_val);
   cudaFree(a->part.d_blk);
   cudaFree(a->part.d_kind);
+  cudaFree(a->tma.d_blk);
+  cudaFree(a->tma.d_kind);
+  cudaFree(a->tma.d_desc);
+  free_sell(&a->sell);
   *a = CsrArrays();
 }
 

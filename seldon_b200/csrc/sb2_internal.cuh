@@ -51,15 +51,39 @@ struct Partition {
   int nblk = 0;
   int* d_blk = nullptr;             // [nblk+1] first row of each block
   unsigned char* d_kind = nullptr;  // [nblk]
+  int4* d_desc = nullptr;           // [nblk] {r0, r1 | kind << 30, k0, k1} (TMA partition)
+};
+
+// Row pointers are padded the same way: the bulk copies of a block's row
+// pointers start and end on 16-byte boundaries.
+inline long long padded_rows(long long rows) { return ((rows + 1 + 3) / 4) * 4 + 4; }
+
+// Binned sliced-ELLPACK copy of an operator (see sell.cuh).  nslice < 0:
+// not applicable (more than 2^26 rows).
+struct SellArrays {
+  int nslice = -1;
+  long long* d_sptr = nullptr;
+  unsigned* d_rinfo = nullptr;
+  int* d_scol = nullptr;
+  double* d_sval = nullptr;
+  float* d_sval32 = nullptr;  // FP32 copy (lazy, mixed precision)
+  int nwarp = 0, ncta = 0;
+  int* d_wrows = nullptr;
+  int* d_crows = nullptr;
+  long long padded = 0;       // stored entries incl. padding
+  bool sorted = false;
 };
 
 struct CsrArrays {
   int rows = 0, cols = 0;
   long long nnz = 0;
-  int* d_ptr = nullptr;     // [rows+1]
+  int* d_ptr = nullptr;     // [padded_rows]
   int* d_ind = nullptr;     // [padded_nnz]
   double* d_val = nullptr;  // [padded_nnz]
-  Partition part;
+  Partition part;           // plain kernel: row blocks incl. long rows
+  Partition tma;            // pipelined kernel (nblk == -1: not applicable)
+  SellArrays sell;          // binned SELL-32 (default product)
+  int max_row = 0;          // longest row
 };
 
 }  // namespace sb2
@@ -86,6 +110,9 @@ int upload_csr(int rows, int cols, const int* ptr, const int* ind,
                const double* val, CsrArrays* out);
 void free_csr(CsrArrays* a);
 int build_partition_host(const int* ptr, int rows, Partition* out);
+int build_tma_partition_host(const int* ptr, int rows, Partition* out);
+int build_sell_host(const int* ptr, const int* ind, const double* val, int rows, SellArrays* out);
+void free_sell(SellArrays* s);
 int ensure_transpose(const sb2_csr* A);
 int ensure_diag(const sb2_csr* A);
 int precond_kind(const sb2_precond* M);
@@ -98,6 +125,7 @@ struct RedScratch {
   double* partials = nullptr;  // [kRedMaxBlocks * 4]
   unsigned* counter = nullptr;
   double* result = nullptr;    // [8] device results of host-returning calls
+  int* status = nullptr;       // bounded-wait status of kernels on this stream
 };
 int get_red_scratch(cudaStream_t s, RedScratch** out);
 

@@ -1,5 +1,9 @@
 // Standalone SpMV: MltAdd / Mlt on device and host vectors.
+#include <algorithm>
+
+#include "sell.cuh"
 #include "spmv_core.cuh"
+#include "spmv_tma.cuh"
 
 namespace sb2 {
 
@@ -33,9 +37,87 @@ __global__ void __launch_bounds__(NT) spmv_kernel(
                                      xl, epi, s_prod, s_red);
 }
 
+// One product through the TMA-pipelined engine: each CTA streams its
+// contiguous share of row blocks once.
+template <int NT, int S>
+__global__ void __launch_bounds__(NT, 2) spmv_tma_kernel(
+    TmaOp<double> op, double alpha, const double* __restrict__ x, double beta,
+    double* __restrict__ y, bool overwrite, int* status, unsigned long long limit_ns) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double s_red[NT / 32];
+  TmaRing<S, double, double> R;
+  R.carve(smem);
+  R.init(op);
+  EpiAxpby epi{alpha, beta, y, overwrite};
+  XLoadLdg<double> xl{x};
+  if (!tma_spmv_pass<NT, S>(R, op, xl, epi, s_red, (unsigned)R.nb, limit_ns, status))
+    R.drain(limit_ns);
+}
+
+// Product algorithm (set by the autotuner): binned SELL-32 by default, the
+// row-block stream kernel or the TMA-pipelined kernel; and the TMA launch
+// configuration (threads per CTA, ring stages).
+static int g_spmv_algo = SB2_SPMV_SELL, g_spmv_threads = 256, g_spmv_stages = 4;
+
+template <int NT>
+__global__ void __launch_bounds__(NT) sell_kernel(SellOp<double> S, double alpha,
+                                                  const double* __restrict__ x, double beta,
+                                                  double* __restrict__ y, bool overwrite) {
+  __shared__ double s_red[NT / 32];
+  EpiAxpby epi{alpha, beta, y, overwrite};
+  XLoadLdg<double> xl{x};
+  sell_spmv<NT, double, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+}
+
+SellOp<double> sell_op(const CsrArrays& a) {
+  const SellArrays& s = a.sell;
+  return SellOp<double>{s.nslice, s.d_sptr, s.d_rinfo, s.d_scol, s.d_sval, s.nwarp, s.d_wrows,
+                        s.ncta, s.d_crows, a.d_ptr, a.d_ind, a.d_val};
+}
+
+template <int NT, int S>
+static int launch_tma(const CsrArrays& a, double alpha, const double* x, double beta, double* y,
+                      bool overwrite, cudaStream_t s, int* status) {
+  static int per_sm = -1;
+  const size_t smem = TmaRing<S, double, double>::smem_bytes();
+  if (per_sm < 0) {
+    cudaFuncSetAttribute(spmv_tma_kernel<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, spmv_tma_kernel<NT, S>, NT, smem) !=
+        cudaSuccess)
+      v = 1;
+    per_sm = v < 1 ? 1 : v;
+  }
+  const int g = std::min(a.tma.nblk, per_sm * num_sms(current_device()));
+  TmaOp<double> op{a.d_ptr, a.d_ind, a.d_val, a.tma.d_desc, a.tma.nblk, a.rows};
+  spmv_tma_kernel<NT, S><<<g, NT, smem, s>>>(op, alpha, x, beta, y, overwrite, status,
+                                             (unsigned long long)g_wait_limit_ms * 1000000ull);
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
 int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
                 double* y, bool overwrite, cudaStream_t s) {
   if (a.rows == 0) return SB2_OK;
+  if (g_spmv_algo == SB2_SPMV_SELL && a.sell.nslice >= 0) {
+    const long long warps = (long long)a.sell.nslice + a.sell.nwarp;
+    long long g = std::max<long long>((warps + 7) / 8, a.sell.ncta);
+    g = std::max<long long>(g, 1);
+    sell_kernel<256><<<(unsigned)std::min<long long>(g, 1 << 30), 256, 0, s>>>(
+        sell_op(a), alpha, x, beta, y, overwrite);
+    SB2_CUDA_TRY(cudaGetLastError());
+    return SB2_OK;
+  }
+  if (g_spmv_algo == SB2_SPMV_TMA && a.tma.nblk > 0) {
+    RedScratch* rs = nullptr;
+    SB2_TRY(get_red_scratch(s, &rs));
+    if (g_spmv_threads == 512)
+      return g_spmv_stages == 3 ? launch_tma<512, 3>(a, alpha, x, beta, y, overwrite, s, rs->status)
+                                : launch_tma<512, 4>(a, alpha, x, beta, y, overwrite, s, rs->status);
+    return g_spmv_stages == 3 ? launch_tma<256, 3>(a, alpha, x, beta, y, overwrite, s, rs->status)
+                              : launch_tma<256, 4>(a, alpha, x, beta, y, overwrite, s, rs->status);
+  }
   spmv_kernel<kSpmvThreads><<<a.part.nblk, kSpmvThreads, 0, s>>>(
       a.d_ptr, a.d_ind, a.d_val, a.part.d_blk, a.part.d_kind, alpha, x, beta,
       y, overwrite);
@@ -114,6 +196,16 @@ int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
   // y is copied in too: MltAdd scales it by beta even when beta == 0.
   return spmv_host_common(A, trans, alpha, x_host, beta, y_host, false,
                           (cudaStream_t)stream);
+}
+
+int sb2_spmv_set_config(int algo, int threads, int stages) {
+  if (algo < SB2_SPMV_SELL || algo > SB2_SPMV_TMA) return SB2_ERR_INVALID_VALUE;
+  if ((threads != 256 && threads != 512) || (stages != 3 && stages != 4))
+    return SB2_ERR_INVALID_VALUE;
+  g_spmv_algo = algo;
+  g_spmv_threads = threads;
+  g_spmv_stages = stages;
+  return SB2_OK;
 }
 
 int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,

@@ -58,10 +58,15 @@ __device__ __forceinline__ void spmv_row_block(
     int4 c = ld_stream_int4(ind + k);
     VT v[4];
     ld_stream_val4(val + k, v);
-    if (k >= k0 && k < k1) s_prod[k - k0] = mul_rn(AT(v[0]), AT(xl(c.x)));
-    if (k + 1 >= k0 && k + 1 < k1) s_prod[k + 1 - k0] = mul_rn(AT(v[1]), AT(xl(c.y)));
-    if (k + 2 >= k0 && k + 2 < k1) s_prod[k + 2 - k0] = mul_rn(AT(v[2]), AT(xl(c.z)));
-    if (k + 3 >= k0 && k + 3 < k1) s_prod[k + 3 - k0] = mul_rn(AT(v[3]), AT(xl(c.w)));
+    // all four gathers issue before the first product is stored
+    AT xv[4];
+    xv[0] = (k >= k0 && k < k1) ? AT(xl(c.x)) : AT(0);
+    xv[1] = (k + 1 >= k0 && k + 1 < k1) ? AT(xl(c.y)) : AT(0);
+    xv[2] = (k + 2 >= k0 && k + 2 < k1) ? AT(xl(c.z)) : AT(0);
+    xv[3] = (k + 3 >= k0 && k + 3 < k1) ? AT(xl(c.w)) : AT(0);
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (k + e >= k0 && k + e < k1) s_prod[k + e - k0] = mul_rn(AT(v[e]), xv[e]);
   }
   __syncthreads();
   if (kind == kBlkThread) {

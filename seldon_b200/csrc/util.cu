@@ -50,11 +50,14 @@ int get_red_scratch(cudaStream_t s, RedScratch** out) {
   cudaError_t e = cudaMalloc(&r->partials, sizeof(double) * kRedMaxBlocks * 4);
   if (e == cudaSuccess) e = cudaMalloc(&r->counter, sizeof(unsigned) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&r->result, sizeof(double) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&r->status, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMemset(r->status, 0, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMemset(r->counter, 0, sizeof(unsigned) * 4);
   if (e != cudaSuccess) {
     cudaFree(r->partials);
     cudaFree(r->counter);
     cudaFree(r->result);
+    cudaFree(r->status);
     delete r;
     return map_cuda_error(e);
   }
