@@ -217,6 +217,25 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
               sb2_iter_result* result, double* hist, int* hist_it,
               int hist_cap, void* stream);
 
+/* Cg with the identity preconditioner that allocates no memory at all.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- code whose device memory is entirely owned by another
+ * allocator (a framework that reserves the whole GPU up front), latency-bound
+ * loops that must not pay cudaMalloc's implicit device synchronization, and
+ * plugin hosts that forbid libraries to allocate.  Such a caller creates the
+ * matrix beforehand and passes x and b (device memory it owns).
+ * The work vectors live in a fixed array inside this library, sized for
+ * n <= 131072 rows (about 3.2 MB, held on every GPU that loads the library
+ * until the process exits); larger systems are rejected with
+ * SB2_ERR_INVALID_VALUE.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture.  All calls on a
+ * device share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialized by the caller.  Iteration
+ * count, error code and last residual are reported; no residual history.
+ * Same arithmetic and results as sb2_cg with M == NULL. */
+int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
+                   const sb2_iter_params* params, sb2_iter_result* result, void* stream);
+
 /* Device-side wait limit for the fused solvers' grid barriers, in
  * milliseconds (default 2000).  Returns the previous value. */
 int sb2_set_wait_limit_ms(int ms);

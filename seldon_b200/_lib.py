@@ -105,6 +105,9 @@ _SOLVER_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParam
                 ctypes.POINTER(IterResult), c_void_p, c_void_p, ctypes.c_int, c_void_p]
 for _name in ("sb2_cg", "sb2_bicgstab", "sb2_gmres"):
     _PROTOS.append((_name, ctypes.c_int, _SOLVER_ARGS))
+_PROTOS.append(("sb2_cg_noalloc", ctypes.c_int,
+                [c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParams),
+                 ctypes.POINTER(IterResult), c_void_p]))
 
 _lib = None
 

@@ -1050,3 +1050,90 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------- no-allocation CG
+
+namespace sb2 {
+
+// Scratch of sb2_cg_noalloc: the three work vectors, the reduction slots, the
+// barrier word and the result record, for systems of up to kNoAllocMaxN
+// rows.  It is a file-scope device array, so it exists on every GPU that
+// loads this library (about 3.2 MB each) until the process exits, and every
+// call on a GPU reuses the same array.
+constexpr int kNoAllocMaxN = 131072;
+constexpr int kNoAllocMaxGrid = 2048;
+constexpr size_t kNoAllocVec = 3 * (size_t)kNoAllocMaxN;
+constexpr size_t kNoAllocPart = (size_t)kMaxRed * kNoAllocMaxGrid;
+constexpr size_t kNoAllocDoubles = kNoAllocVec + kNoAllocPart + 64 + 64 + 16;
+static __device__ __align__(256) double g_cg_noalloc_scratch[kNoAllocDoubles];
+
+// Device address of the scratch on the current device.  Host code cannot use
+// the array's name as a device address, so the address is looked up once per
+// device (with that device current) and remembered.
+static int cg_noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static double* addr[128] = {};
+  const int dev = current_device();
+  if (dev < 0 || dev >= 128) return SB2_ERR_INVALID_VALUE;
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_cg_noalloc_scratch);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    addr[dev] = static_cast<double*>(p);
+  }
+  *out = addr[dev];
+  return SB2_OK;
+}
+
+static int cg_noalloc(const sb2_csr* A, double* x, const double* b, const sb2_iter_params* prm,
+                      sb2_iter_result* res, cudaStream_t s) {
+  if (!A || !prm || !res || A->m != A->n) return SB2_ERR_INVALID_VALUE;
+  if (A->m > kNoAllocMaxN) return SB2_ERR_INVALID_VALUE;  // beyond the scratch
+  if (A->m > 0 && (!x || !b || x == b)) return SB2_ERR_INVALID_VALUE;
+  *res = sb2_iter_result{};
+  if (A->m <= 0) return SB2_OK;
+  const int grid = coop_grid((const void*)cg_fused_kernel, 0, A);
+  if (grid < 1) return SB2_ERR_CUDA;
+  if (grid > kNoAllocMaxGrid) return SB2_ERR_NOT_SUPPORTED;
+  double* base = nullptr;
+  SB2_TRY(cg_noalloc_scratch(&base));
+  const size_t n = (size_t)A->m;
+  double* vec = base;
+  double* partials = base + kNoAllocVec;
+  GridSync* sync = reinterpret_cast<GridSync*>(partials + kNoAllocPart);
+  SolveOut* out = reinterpret_cast<SolveOut*>(partials + kNoAllocPart + 64);
+  double* hist = partials + kNoAllocPart + 128;
+  int* hist_it = reinterpret_cast<int*>(hist + 8);
+  // the barrier word and the result record must start at zero on every call
+  SB2_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(double) * 128, s));
+  Persist P{sync, partials, (unsigned long long)g_wait_limit_ms * 1000000ull};
+  History H{hist, hist_it, 1};
+  IterArgs it{prm->tol, prm->max_iter, std::max(prm->restart, 1), prm->init_guess_null};
+  OpArgs op = op_args(A, nullptr);
+  CgVecs cv{b, x, vec, vec + n, vec + 2 * n};
+  void* args[6] = {&op, &cv, &it, &P, &H, &out};
+  SB2_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)cg_fused_kernel, dim3(grid), dim3(NT),
+                                           args, 0, s));
+  SolveOut o;
+  GridSync gs;
+  SB2_CUDA_TRY(cudaMemcpyAsync(&o, out, sizeof(o), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaMemcpyAsync(&gs, sync, sizeof(gs), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  if (gs.status != 0) return SB2_ERR_TIMEOUT;
+  res->nb_iter = o.nb_iter;
+  res->error_code = o.init_failed ? (prm->max_iter <= 0 ? -2 : 0) : o.error_code;
+  res->init_failed = o.init_failed;
+  res->hist_len = 0;
+  res->facteur_reste = o.facteur_reste;
+  res->last_residual = o.last_residual;
+  return SB2_OK;
+}
+
+}  // namespace sb2
+
+extern "C" int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
+                              const sb2_iter_params* params, sb2_iter_result* result,
+                              void* stream) {
+  return sb2::cg_noalloc(A, x, b, params, result, (cudaStream_t)stream);
+}
