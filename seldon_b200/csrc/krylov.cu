@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "persist.cuh"
+#include "sell.cuh"
 
 namespace sb2 {
 
@@ -38,6 +39,7 @@ struct OpArgs {
   int nblk;
   int n;
   const double* diag;  // nullptr: identity preconditioner, else Jacobi
+  SellOp<double> sell; // binned SELL-32 (nslice < 0: use the row blocks)
 };
 
 struct IterArgs {
@@ -106,6 +108,10 @@ template <class Epi>
 __device__ __forceinline__ void spmv_phase(const OpArgs& A, const double* x, Epi& epi,
                                            double* s_prod, double* s_red) {
   XLoadCg<double> xl{x};
+  if (A.sell.nslice >= 0) {
+    sell_spmv<NT, double, double>(A.sell, xl, epi, s_red, blockIdx.x, gridDim.x);
+    return;
+  }
   for (int b = blockIdx.x; b < A.nblk; b += gridDim.x)
     spmv_row_block<NT, double, double>(A.ptr, A.ind, A.val, A.blk[b], A.blk[b + 1], A.kind[b],
                                        xl, epi, s_prod, s_red);
@@ -118,7 +124,7 @@ struct CgVecs {
   double *x, *r, *p, *q;
 };
 
-__global__ void __launch_bounds__(NT) cg_fused_kernel(OpArgs A, CgVecs v, IterArgs it,
+__global__ void __launch_bounds__(NT, 4) cg_fused_kernel(OpArgs A, CgVecs v, IterArgs it,
                                                       Persist P, History H, SolveOut* out) {
   SB2_SHARED_DECL;
   const int tid = threadIdx.x;
@@ -178,14 +184,19 @@ __global__ void __launch_bounds__(NT) cg_fused_kernel(OpArgs A, CgVecs v, IterAr
     // z = M^{-1} r; rho = (r, z): already reduced with the norm
     if (rho == 0.0) { fail = 1; break; }
     // p = z (first) | p = beta*p + z: Mlt(beta, p); Add(1, z, p)
-    if (nb_iter == 0) {
-      for (long long i = gt; i < n; i += gs)
-        v.p[i] = precond_val(A.diag, (int)i, __ldcg(v.r + i));
-    } else {
-      const double beta = rho / rho_1;
-      for (long long i = gt; i < n; i += gs) {
-        const double z = precond_val(A.diag, (int)i, __ldcg(v.r + i));
-        v.p[i] = add_rn(mul_rn(__ldcg(v.p + i), beta), z);
+    {
+      double* __restrict__ pp = v.p;
+      const double* __restrict__ rp = v.r;
+      if (nb_iter == 0) {
+#pragma unroll 4
+        for (long long i = gt; i < n; i += gs) pp[i] = precond_val(A.diag, (int)i, __ldcg(rp + i));
+      } else {
+        const double beta = rho / rho_1;
+#pragma unroll 4
+        for (long long i = gt; i < n; i += gs) {
+          const double z = precond_val(A.diag, (int)i, __ldcg(rp + i));
+          pp[i] = add_rn(mul_rn(__ldcg(pp + i), beta), z);
+        }
       }
     }
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
@@ -201,16 +212,23 @@ __global__ void __launch_bounds__(NT) cg_fused_kernel(OpArgs A, CgVecs v, IterAr
     // Add(alpha, p, x); Add(-alpha, q, r); then ||r||^2 and (r, z) for the next test
     rr = 0.0;
     rz = 0.0;
-    for (long long i = gt; i < n; i += gs) {
-      if (alpha != 0.0) v.x[i] = add_rn(__ldcg(v.x + i), mul_rn(alpha, __ldcg(v.p + i)));
-      double ri = __ldcg(v.r + i);
-      if (-alpha != 0.0) {
-        ri = add_rn(ri, mul_rn(-alpha, __ldcg(v.q + i)));
-        v.r[i] = ri;
+    {
+      double* __restrict__ xp = v.x;
+      double* __restrict__ rp = v.r;
+      const double* __restrict__ pp = v.p;
+      const double* __restrict__ qp = v.q;
+#pragma unroll 4
+      for (long long i = gt; i < n; i += gs) {
+        if (alpha != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(alpha, __ldcg(pp + i)));
+        double ri = __ldcg(rp + i);
+        if (-alpha != 0.0) {
+          ri = add_rn(ri, mul_rn(-alpha, __ldcg(qp + i)));
+          rp[i] = ri;
+        }
+        const double z = precond_val(A.diag, (int)i, ri);
+        rr = add_rn(rr, mul_rn(ri, ri));
+        rz = add_rn(rz, mul_rn(ri, z));
       }
-      const double z = precond_val(A.diag, (int)i, ri);
-      rr = add_rn(rr, mul_rn(ri, ri));
-      rz = add_rn(rz, mul_rn(ri, z));
     }
     rr = block_sum<NT>(rr, s_red);
     rz = block_sum<NT>(rz, s_red);
@@ -231,20 +249,20 @@ struct BicgVecs {
   double *x, *r, *rt, *p, *ph, *v, *s, *sh, *t;
 };
 
-// epilogue: y_r = t; acc0 += w0_r t; acc1 += w1_r t
+// epilogue: y_r = t; acc0 += w0_r t; with `self`, acc1 += t t
 struct EpiStoreDot2 {
   double* y;
   const double* w0;
-  const double* w1;
+  bool self;
   double acc0, acc1;
   __device__ __forceinline__ void operator()(int r, double t) {
     y[r] = t;
     acc0 = add_rn(acc0, mul_rn(__ldcg(w0 + r), t));
-    if (w1) acc1 = add_rn(acc1, mul_rn(__ldcg(w1 + r), t));
+    if (self) acc1 = add_rn(acc1, mul_rn(t, t));
   }
 };
 
-__global__ void __launch_bounds__(NT) bicgstab_fused_kernel(OpArgs A, BicgVecs v, IterArgs it,
+__global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVecs v, IterArgs it,
                                                             Persist P, History H,
                                                             SolveOut* out) {
   SB2_SHARED_DECL;
@@ -324,7 +342,7 @@ __global__ void __launch_bounds__(NT) bicgstab_fused_kernel(OpArgs A, BicgVecs v
     }
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // v = A phat, sigma = (rtilde, v)
-    EpiStoreDot2 e1{v.v, v.rt, nullptr, 0.0, 0.0};
+    EpiStoreDot2 e1{v.v, v.rt, false, 0.0, 0.0};
     spmv_phase(A, ph, e1, s_prod, s_red);
     double d = block_sum<NT>(e1.acc0, s_red);
     if (tid == 0) s_vals[0] = d;
@@ -355,20 +373,11 @@ __global__ void __launch_bounds__(NT) bicgstab_fused_kernel(OpArgs A, BicgVecs v
       break;
     }
     // t = A shat; omega = (t, s) / (t, t)
-    EpiStoreDot2 e2{v.t, v.s, nullptr, 0.0, 0.0};
+    EpiStoreDot2 e2{v.t, v.s, true, 0.0, 0.0};
     spmv_phase(A, sh, e2, s_prod, s_red);
-    // (t, t) needs t itself: accumulate from the epilogue's stored values
-    double ts = block_sum<NT>(e2.acc0, s_red);
-    if (tid == 0) s_vals[0] = ts;
-    __syncthreads();
-    double tt = 0.0;
-    for (int b = blockIdx.x; b < A.nblk; b += gridDim.x)
-      for (int r = A.blk[b] + tid; r < A.blk[b + 1]; r += NT) {
-        const double tr = __ldcg(v.t + r);
-        tt = add_rn(tt, mul_rn(tr, tr));
-      }
-    tt = block_sum<NT>(tt, s_red);
-    if (tid == 0) s_vals[1] = tt;
+    const double ts = block_sum<NT>(e2.acc0, s_red);
+    const double tt = block_sum<NT>(e2.acc1, s_red);
+    if (tid == 0) { s_vals[0] = ts; s_vals[1] = tt; }
     if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
     omega = s_vals[0] / s_vals[1];
     // Add(alpha, phat, x); Add(omega, shat, x); Copy(s, r); Add(-omega, t, r)
@@ -449,7 +458,7 @@ struct EpiPrecDot {
   }
 };
 
-__global__ void __launch_bounds__(NT) gmres_fused_kernel(OpArgs A, GmresVecs v, IterArgs it,
+__global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs v, IterArgs it,
                                                          Persist P, History H, SolveOut* out) {
   SB2_SHARED_DECL;
   extern __shared__ double s_dyn[];
@@ -532,13 +541,29 @@ __global__ void __launch_bounds__(NT) gmres_fused_kernel(OpArgs A, GmresVecs v, 
         const double* Vk = v.V + (size_t)k * nn;
         const double* Vn = (k < i) ? v.V + (size_t)(k + 1) * nn : nullptr;
         double acc = 0.0;
-        for (long long e = gt; e < n; e += gs) {
-          double we = __ldcg(v.w + e);
-          if (-h != 0.0) {
-            we = add_rn(we, mul_rn(-h, __ldcg(Vk + e)));
-            v.w[e] = we;
+        double* __restrict__ wp = v.w;
+        const double* __restrict__ vk = Vk;
+        const double* __restrict__ vn = Vn;
+        if (vn) {
+#pragma unroll 4
+          for (long long e = gt; e < n; e += gs) {
+            double we = __ldcg(wp + e);
+            if (-h != 0.0) {
+              we = add_rn(we, mul_rn(-h, __ldcg(vk + e)));
+              wp[e] = we;
+            }
+            acc = add_rn(acc, mul_rn(__ldcg(vn + e), we));
           }
-          acc = Vn ? add_rn(acc, mul_rn(__ldcg(Vn + e), we)) : add_rn(acc, mul_rn(we, we));
+        } else {
+#pragma unroll 4
+          for (long long e = gt; e < n; e += gs) {
+            double we = __ldcg(wp + e);
+            if (-h != 0.0) {
+              we = add_rn(we, mul_rn(-h, __ldcg(vk + e)));
+              wp[e] = we;
+            }
+            acc = add_rn(acc, mul_rn(we, we));
+          }
         }
         acc = block_sum<NT>(acc, s_red);
         if (tid == 0) s_vals[0] = acc;
@@ -687,9 +712,12 @@ static int finish_solve(SolveScratch& S, cudaStream_t s, sb2_iter_result* res, d
   return SB2_OK;
 }
 
+SellOp<double> sell_op(const CsrArrays& a);
+
 static OpArgs op_args(const sb2_csr* A, const double* diag) {
   const CsrArrays& f = A->full;
-  return OpArgs{f.d_ptr, f.d_ind, f.d_val, f.part.d_blk, f.part.d_kind, f.part.nblk, A->m, diag};
+  return OpArgs{f.d_ptr, f.d_ind, f.d_val, f.part.d_blk, f.part.d_kind, f.part.nblk, A->m, diag,
+                sell_op(f)};
 }
 
 enum Solver { kCg = 0, kBicg = 1, kGmres = 2 };

@@ -100,6 +100,10 @@ struct sb2_csr {
   double* d_diag = nullptr;  // A(i,i) by Seldon's lookup rule (lazy)
   float* d_val32 = nullptr;  // FP32 copy of full.d_val (lazy)
   std::mutex mu;             // guards the lazy members
+  // staging vectors of the host-buffer entry points (lazy, reused)
+  double* d_hx = nullptr;
+  double* d_hy = nullptr;
+  std::mutex host_mu;        // one host-buffer product at a time per matrix
 };
 
 namespace sb2 {

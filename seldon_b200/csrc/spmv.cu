@@ -163,31 +163,30 @@ int sb2_mlt(const sb2_csr* A, int trans, double alpha, const double* x,
   return spmv_common(A, trans, alpha, x, 0.0, y, true, (cudaStream_t)stream);
 }
 
-static int spmv_host_common(const sb2_csr* A, int trans, double alpha,
+static int spmv_host_common(const sb2_csr* cA, int trans, double alpha,
                             const double* x_host, double beta, double* y_host,
                             bool overwrite, cudaStream_t s) {
-  if (!A) return SB2_ERR_INVALID_VALUE;
+  if (!cA) return SB2_ERR_INVALID_VALUE;
+  sb2_csr* A = const_cast<sb2_csr*>(cA);
   const int nx = trans ? A->m : A->n, ny = trans ? A->n : A->m;
   if ((nx > 0 && !x_host) || (ny > 0 && !y_host)) return SB2_ERR_INVALID_VALUE;
-  double *dx = nullptr, *dy = nullptr;
-  int st = SB2_OK;
-  cudaError_t e = cudaMallocAsync(&dx, sizeof(double) * (nx > 0 ? nx : 1), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&dy, sizeof(double) * (ny > 0 ? ny : 1), s);
-  if (e == cudaSuccess && nx > 0)
-    e = cudaMemcpyAsync(dx, x_host, sizeof(double) * nx, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && ny > 0 && !overwrite)
-    e = cudaMemcpyAsync(dy, y_host, sizeof(double) * ny, cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) st = map_cuda_error(e);
-  if (st == SB2_OK) st = spmv_common(A, trans, alpha, dx, beta, dy, overwrite, s);
-  if (st == SB2_OK && ny > 0) {
-    e = cudaMemcpyAsync(y_host, dy, sizeof(double) * ny, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) st = map_cuda_error(e);
+  std::lock_guard<std::mutex> g(A->host_mu);
+  // staging vectors sized for both orientations, allocated on first use
+  if (!A->d_hx) {
+    const size_t len = (size_t)std::max(std::max(A->m, A->n), 1);
+    SB2_CUDA_TRY(cudaMalloc(&A->d_hx, sizeof(double) * len));
+    SB2_CUDA_TRY(cudaMalloc(&A->d_hy, sizeof(double) * len));
   }
-  cudaFreeAsync(dx, s);
-  cudaFreeAsync(dy, s);
-  e = cudaStreamSynchronize(s);
-  if (st == SB2_OK && e != cudaSuccess) st = map_cuda_error(e);
-  return st;
+  double *dx = A->d_hx, *dy = A->d_hy;
+  if (nx > 0)
+    SB2_CUDA_TRY(cudaMemcpyAsync(dx, x_host, sizeof(double) * nx, cudaMemcpyHostToDevice, s));
+  if (ny > 0 && !overwrite)
+    SB2_CUDA_TRY(cudaMemcpyAsync(dy, y_host, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
+  SB2_TRY(spmv_common(A, trans, alpha, dx, beta, dy, overwrite, s));
+  if (ny > 0)
+    SB2_CUDA_TRY(cudaMemcpyAsync(y_host, dy, sizeof(double) * ny, cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  return SB2_OK;
 }
 
 int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
