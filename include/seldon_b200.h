@@ -236,6 +236,12 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
 int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
                    const sb2_iter_params* params, sb2_iter_result* result, void* stream);
 
+/* Size from which Cg runs as a chain of full-occupancy kernels (one per
+ * pass, scalars in device memory) instead of one persistent kernel; chosen
+ * by the autotuner, default 200000 rows.  Returns the previous value.  No
+ * counterpart in the reference (a tuning knob of this engine). */
+int sb2_krylov_set_config(int chain_min_n);
+
 /* Device-side wait limit for the fused solvers' grid barriers, in
  * milliseconds (default 2000).  Returns the previous value. */
 int sb2_set_wait_limit_ms(int ms);

@@ -1,0 +1,319 @@
+// Conjugate gradients as a chain of full-occupancy kernels (see chain.cuh).
+//
+// Same iteration as the reference's Cg (Cg.cxx:45-116) and as the persistent
+// kernel of krylov.cu:
+//   while (!Finished(r)) { z = M^{-1} r; rho = (r, z); [rho == 0: fail 1]
+//     p = z | p = beta*p + z;  q = A p;  delta = (p, q); [delta == 0: fail 2]
+//     alpha = rho/delta;  x += alpha p;  r -= alpha q;  ++iter }
+// with one kernel per pass:  K_p (p update), K_q (q = A p fused with (p, q)),
+// K_x (x and r updates fused with ||r||^2 and (r, z) and the stopping test).
+// Templated on the vector/scalar type T and the matrix value type VT, so the
+// same chain runs the FP64 drop-in and the FP32 inner solves of iterative
+// refinement.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "chain.cuh"
+#include "spmv_core.cuh"
+
+namespace sb2 {
+
+constexpr int CT = 256;
+
+template <typename T>
+__device__ __forceinline__ bool chain_done(const ChainState<T>* st) {
+  return *((volatile const int*)&st->done) != 0;
+}
+
+// Finished() at the current nb_iter (Iterative.cxx:299-319), run by one thread.
+template <typename T>
+__device__ __forceinline__ bool chain_finished(ChainArgs<T>& a, T rr) {
+  ChainState<T>* st = a.st;
+  const T res = (T)sqrt(rr);
+  const double reste = (double)((T)st->facteur * res);
+  st->reste = reste;
+  if (st->hist_len < st->hist_cap) {
+    a.hist[st->hist_len] = reste;
+    a.hist_it[st->hist_len] = st->nb_iter;
+  }
+  st->hist_len++;
+  return (reste < st->tol) || (st->nb_iter >= st->max_iter);
+}
+
+// ||b||: Init(b) (Iterative.cxx:235-249).
+template <typename T>
+__global__ void __launch_bounds__(CT, 8) k_norm_b(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[1];
+  T acc = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const T bi = __ldg(a.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  T v[1] = {block_sum<CT>(acc, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    const T nb = (T)sqrt(s_out[0]);
+    if (nb == T(0)) {
+      a.st->init_failed = 1;
+      a.st->done = 1;
+    } else {
+      a.st->facteur = (double)(T(1) / nb);
+    }
+  }
+}
+
+// Start of the loop once r is known: Finished(r) at iteration 0, then rho.
+template <typename T>
+__device__ __forceinline__ void chain_start(ChainArgs<T>& a, T rr, T rz) {
+  if (chain_finished(a, rr)) {
+    a.st->done = 1;
+    return;
+  }
+  a.st->rho = rz;
+  if (rz == T(0)) {
+    a.st->fail = 1;
+    a.st->done = 1;
+  }
+}
+
+// Null initial guess: x = 0, r = b, with ||r||^2 and (r, z).
+template <typename T>
+__global__ void __launch_bounds__(CT, 8) k_init_null(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  if (chain_done(a.st)) return;
+  T rr = T(0), rz = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const T bi = __ldg(a.b + i);
+    a.x[i] = T(0);
+    a.r[i] = bi;
+    rr = add_rn(rr, mul_rn(bi, bi));
+    rz = add_rn(rz, mul_rn(bi, zval(a.diag, i, bi)));
+  }
+  T v[2] = {block_sum<CT>(rr, s_red), block_sum<CT>(rz, s_red)};
+  if (deposit_and_finish<CT, 2>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0)
+    chain_start(a, s_out[0], s_out[1]);
+}
+
+// r = b - A x (Copy(b, r); MltAdd(-1, A, x, 1, r)) with ||r||^2 and (r, z).
+template <typename T>
+struct EpiChainResidual {
+  ChainArgs<T> a;
+  T rr, rz;
+  __device__ __forceinline__ void operator()(int i, T t) {
+    const T v = add_rn(__ldg(a.b + i), -t);
+    a.r[i] = v;
+    rr = add_rn(rr, mul_rn(v, v));
+    rz = add_rn(rz, mul_rn(v, zval(a.diag, i, v)));
+  }
+};
+
+// q = A p with (p, q).
+template <typename T>
+struct EpiChainDot {
+  T* q;
+  const T* p;
+  T acc;
+  __device__ __forceinline__ void operator()(int i, T t) {
+    q[i] = t;
+    acc = add_rn(acc, mul_rn(__ldg(p + i), t));
+  }
+};
+
+// After the (p, q) reduction: alpha = rho / delta, or breakdown #2.
+template <typename T>
+__device__ __forceinline__ void chain_after_delta(ChainArgs<T>& a, T delta) {
+  if (delta == T(0)) {
+    a.st->fail = 2;
+    a.st->done = 1;
+    return;
+  }
+  a.st->alpha = a.st->rho / delta;
+}
+
+// One SELL product fused with a reduction; MODE 0: q = A p and (p, q);
+// MODE 1: r = b - A x with ||r||^2, (r, z).  PART 0: slices, PART 1: long
+// rows (deposit slots after the slices').
+template <typename T, typename VT, int MODE, int PART>
+__global__ void __launch_bounds__(CT, PART == 0 ? 8 : 1)
+    k_spmv(ChainArgs<T> a, SellOp<VT> S, int slot0, int tot) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  if (chain_done(a.st)) return;
+  if (MODE == 0) {
+    EpiChainDot<T> epi{a.q, a.p, T(0)};
+    XLoadLdg<T> xl{a.p};
+    if (PART == 0)
+      sell_spmv_slices<CT, VT, T>(S, xl, epi, blockIdx.x, gridDim.x);
+    else
+      sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+    T v[1] = {block_sum<CT>(epi.acc, s_red)};
+    if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, slot0 + blockIdx.x, tot, s_red, s_out) &&
+        threadIdx.x == 0)
+      chain_after_delta(a, s_out[0]);
+  } else {
+    EpiChainResidual<T> epi{a, T(0), T(0)};
+    XLoadLdg<T> xl{a.x};
+    if (PART == 0)
+      sell_spmv_slices<CT, VT, T>(S, xl, epi, blockIdx.x, gridDim.x);
+    else
+      sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+    T v[2] = {block_sum<CT>(epi.rr, s_red), block_sum<CT>(epi.rz, s_red)};
+    if (deposit_and_finish<CT, 2>(v, a.part, &a.st->cnt, slot0 + blockIdx.x, tot, s_red, s_out) &&
+        threadIdx.x == 0)
+      chain_start(a, s_out[0], s_out[1]);
+  }
+}
+
+// p = z (first iteration) | p = beta*p + z: Mlt(beta, p); Add(1, z, p).
+template <typename T>
+__global__ void __launch_bounds__(CT, 8) k_p(ChainArgs<T> a) {
+  if (chain_done(a.st)) return;
+  const bool first = (a.st->nb_iter == 0);
+  const T beta = a.st->beta;
+  T* __restrict__ p = a.p;
+  const T* __restrict__ r = a.r;
+#pragma unroll 4
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const T z = zval(a.diag, i, r[i]);
+    p[i] = first ? z : add_rn(mul_rn(p[i], beta), z);
+  }
+}
+
+// Add(alpha, p, x); Add(-alpha, q, r); ||r||^2, (r, z); ++iter; the test.
+template <typename T>
+__global__ void __launch_bounds__(CT, 8) k_x(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  if (chain_done(a.st)) return;
+  const T alpha = a.st->alpha;
+  T* __restrict__ x = a.x;
+  T* __restrict__ r = a.r;
+  const T* __restrict__ p = a.p;
+  const T* __restrict__ q = a.q;
+  T rr = T(0), rz = T(0);
+#pragma unroll 4
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    if (alpha != T(0)) x[i] = add_rn(x[i], mul_rn(alpha, __ldg(p + i)));
+    T ri = r[i];
+    if (-alpha != T(0)) {
+      ri = add_rn(ri, mul_rn(-alpha, __ldg(q + i)));
+      r[i] = ri;
+    }
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rz = add_rn(rz, mul_rn(ri, zval(a.diag, i, ri)));
+  }
+  T v[2] = {block_sum<CT>(rr, s_red), block_sum<CT>(rz, s_red)};
+  if (deposit_and_finish<CT, 2>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->nb_iter++;
+    if (chain_finished(a, s_out[0])) {
+      st->done = 1;
+      return;
+    }
+    st->rho_1 = st->rho;
+    st->rho = s_out[1];
+    if (st->rho == T(0)) {
+      st->fail = 1;
+      st->done = 1;
+      return;
+    }
+    st->beta = st->rho / st->rho_1;
+  }
+}
+
+// ----------------------------------------------------------------- host driver
+
+static int chain_elem_grid(int n) {
+  const int cap = num_sms(current_device()) * 8;
+  return std::max(1, std::min((n + CT * 4 - 1) / (CT * 4), cap));
+}
+
+// CTAs of a reducing product: one slice per warp up to four resident waves,
+// beyond that warps loop over slices (fewer deposits to sum at the end).
+template <typename VT>
+static int reducing_slice_grid(const SellOp<VT>& S) {
+  if (S.nslice <= 0) return 0;
+  const int cap = num_sms(current_device()) * 8 * 4;
+  return std::min((S.nslice + 7) / 8, cap);
+}
+
+template <typename T, typename VT>
+static int launch_spmv_pair(int mode, const ChainArgs<T>& a, const SellOp<VT>& S,
+                            cudaStream_t s) {
+  const int g1 = reducing_slice_grid(S);
+  const int g2 = (S.nwarp_rows + S.ncta_rows) > 0 ? std::max((S.nwarp_rows + 7) / 8, S.ncta_rows) : 0;
+  const int tot = g1 + g2;
+  if (tot == 0) return SB2_ERR_NOT_SUPPORTED;
+  if (mode == 0) {
+    if (g1) k_spmv<T, VT, 0, 0><<<g1, CT, 0, s>>>(a, S, 0, tot);
+    if (g2) k_spmv<T, VT, 0, 1><<<g2, CT, 0, s>>>(a, S, g1, tot);
+  } else {
+    if (g1) k_spmv<T, VT, 1, 0><<<g1, CT, 0, s>>>(a, S, 0, tot);
+    if (g2) k_spmv<T, VT, 1, 1><<<g2, CT, 0, s>>>(a, S, g1, tot);
+  }
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+// Deposit slots one solve needs (two values per CTA of the widest kernel).
+template <typename VT>
+long long chain_part_slots(const SellOp<VT>& S, int n) {
+  const long long g1 = reducing_slice_grid(S);
+  const long long g2 = std::max<long long>((S.nwarp_rows + 7) / 8, S.ncta_rows);
+  return 2 * std::max<long long>(g1 + g2, chain_elem_grid(n)) + 16;
+}
+
+template <typename T, typename VT>
+int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* work,
+             ChainState<T>* st, T* part, double* hist, int* hist_it, int hist_cap, double tol,
+             int max_iter, int init_guess_null, cudaStream_t s, ChainState<T>* out) {
+  ChainState<T> init{};
+  init.max_iter = max_iter;
+  init.tol = tol;
+  init.hist_cap = hist_cap;
+  SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  ChainArgs<T> a{n, b, x, work, work + n, work + 2 * (size_t)n, diag, st, part, hist, hist_it};
+  const int ge = chain_elem_grid(n);
+  k_norm_b<T><<<ge, CT, 0, s>>>(a);
+  if (init_guess_null)
+    k_init_null<T><<<ge, CT, 0, s>>>(a);
+  else
+    SB2_TRY((launch_spmv_pair<T, VT>(1, a, S, s)));
+  SB2_CUDA_TRY(cudaGetLastError());
+  // iterations in chunks; the stop flag is read back once per chunk
+  int launched = 0, chunk = 8;
+  ChainState<T> h{};
+  for (;;) {
+    for (int c = 0; c < chunk; c++) {
+      k_p<T><<<ge, CT, 0, s>>>(a);
+      SB2_TRY((launch_spmv_pair<T, VT>(0, a, S, s)));
+      k_x<T><<<ge, CT, 0, s>>>(a);
+    }
+    SB2_CUDA_TRY(cudaGetLastError());
+    launched += chunk;
+    SB2_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s));
+    SB2_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h.done || launched > max_iter + 1) break;
+    chunk = std::min(chunk * 2, 32);
+  }
+  *out = h;
+  return SB2_OK;
+}
+
+template long long chain_part_slots<double>(const SellOp<double>&, int);
+template long long chain_part_slots<float>(const SellOp<float>&, int);
+template int chain_cg<double, double>(const SellOp<double>&, int, const double*, double*,
+                                      const double*, double*, ChainState<double>*, double*,
+                                      double*, int*, int, double, int, int, cudaStream_t,
+                                      ChainState<double>*);
+template int chain_cg<float, float>(const SellOp<float>&, int, const float*, float*,
+                                    const float*, float*, ChainState<float>*, float*, double*,
+                                    int*, int, double, int, int, cudaStream_t,
+                                    ChainState<float>*);
+
+}  // namespace sb2

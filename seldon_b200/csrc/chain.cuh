@@ -1,0 +1,95 @@
+// Krylov loops as chains of full-occupancy kernels (large systems).
+//
+// For large n the cost of an iteration is the HBM traffic of its passes, and
+// each pass runs best at the occupancy its own kernel allows (the SpMV at 8
+// CTAs per SM).  The chain keeps every scalar of the iteration (rho, alpha,
+// beta, the residual, the counters and the stop flag) in device memory:
+// kernels read them, the last CTA of each reducing kernel updates them, and a
+// kernel launched after the solve has stopped returns at once.  The host
+// enqueues iterations in chunks and reads the stop flag once per chunk, so
+// the device never waits for the host.
+//
+// Reductions are deterministic: every CTA deposits its partial sum, and the
+// CTA that completes the deposits sums them in CTA order.  A reduction may
+// span two kernels (SELL slices + long rows): both deposit into one array
+// and the last depositor of the pair finishes it.
+#pragma once
+
+#include "sell.cuh"
+
+namespace sb2 {
+
+// Device-resident state of one chained solve, in the vector precision T.
+template <typename T>
+struct ChainState {
+  T rho, rho_1, alpha, beta;
+  double facteur;  // 1 / ||b||
+  double reste;    // relative residual of the last Finished() test
+  int nb_iter, max_iter, done, fail, init_failed, hist_len, hist_cap;
+  double tol;
+  unsigned cnt;  // deposits of the reduction in progress
+};
+
+template <typename T>
+struct ChainArgs {
+  int n;
+  const T* b;
+  T* x;
+  T* r;
+  T* p;
+  T* q;
+  const T* diag;  // Jacobi: z = r / diag; nullptr: identity
+  ChainState<T>* st;
+  T* part;        // deposits (2 per CTA at most)
+  double* hist;   // relative residual of each Finished() test
+  int* hist_it;
+};
+
+#ifdef __CUDACC__
+
+template <typename T>
+__device__ __forceinline__ T zval(const T* diag, long long i, T r) {
+  return diag ? r / __ldg(diag + i) : r;  // IEEE division, as the reference's Jacobi
+}
+
+// Deposit K block sums (valid in thread 0) at slots [off, off+K*tot) with
+// stride tot; the CTA completing `tot` deposits sums them in order and
+// returns true (all its threads), with the totals in out[0..K).
+template <int NT, int K, typename T>
+__device__ __forceinline__ bool deposit_and_finish(const T (&v)[K], T* part, unsigned* cnt,
+                                                   int slot, int tot, T* s_red, T* out) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) part[(size_t)k * tot + slot] = v[k];
+    __threadfence();
+    s_last = (atomicAdd(cnt, 1u) == (unsigned)tot - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    // four independent chains keep several loads in flight; the order of
+    // every addition is fixed by (slot, thread), so the total is too
+    const T* pv = part + (size_t)k * tot;
+    T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+    int i = threadIdx.x;
+    for (; i + 3 * NT < tot; i += 4 * NT) {
+      a0 = add_rn(a0, __ldcg(pv + i));
+      a1 = add_rn(a1, __ldcg(pv + i + NT));
+      a2 = add_rn(a2, __ldcg(pv + i + 2 * NT));
+      a3 = add_rn(a3, __ldcg(pv + i + 3 * NT));
+    }
+    for (; i < tot; i += NT) a0 = add_rn(a0, __ldcg(pv + i));
+    T a = block_sum<NT>(add_rn(add_rn(a0, a1), add_rn(a2, a3)), s_red);
+    if (threadIdx.x == 0) out[k] = a;
+  }
+  if (threadIdx.x == 0) *cnt = 0u;
+  __syncthreads();
+  return true;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace sb2

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <vector>
 
+#include "chain.cuh"
 #include "persist.cuh"
 #include "sell.cuh"
 
@@ -1030,6 +1031,52 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   return SB2_OK;
 }
 
+template <typename VT>
+long long chain_part_slots(const SellOp<VT>& S, int n);
+template <typename T, typename VT>
+int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* work,
+             ChainState<T>* st, T* part, double* hist, int* hist_it, int hist_cap, double tol,
+             int max_iter, int init_guess_null, cudaStream_t s, ChainState<T>* out);
+
+// Systems at least this large run CG as a chain of full-occupancy kernels;
+// smaller ones as one persistent kernel (latency-bound, barriers are cheap).
+// Set by the autotuner (sb2_krylov_set_config).
+static int g_chain_min_n = 200000;
+
+static int chain_cg_solve(const sb2_csr* A, const double* diag, double* x, const double* b,
+                          const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
+                          int* hist_it, int hist_cap, cudaStream_t s) {
+  const SellOp<double> S = sell_op(A->full);
+  const int n = A->m;
+  const long long slots = chain_part_slots(S, n);
+  const int hcap = std::max(hist_cap, 1);
+  const size_t vb = sizeof(double) * 3 * (size_t)n;
+  const size_t sb = 256, pb = sizeof(double) * slots, hb = sizeof(double) * hcap, ib = sizeof(int) * hcap;
+  DeviceBuf buf;
+  buf.s = s;
+  SB2_CUDA_TRY(cudaMallocAsync(&buf.p, vb + sb + pb + hb + ib + 64, s));
+  char* c = (char*)buf.p;
+  double* work = (double*)c;
+  ChainState<double>* st = (ChainState<double>*)(c + vb);
+  double* part = (double*)(c + vb + sb);
+  double* dh = (double*)(c + vb + sb + pb);
+  int* dhi = (int*)(c + vb + sb + pb + hb);
+  ChainState<double> o;
+  SB2_TRY((chain_cg<double, double>(S, n, diag, x, b, work, st, part, dh, dhi, hcap, prm->tol,
+                                    prm->max_iter, prm->init_guess_null, s, &o)));
+  const int nh = std::min(o.hist_len, std::max(hist_cap, 0));
+  if (hist && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist, dh, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+  if (hist_it && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist_it, dhi, sizeof(int) * nh, cudaMemcpyDeviceToHost));
+  res->init_failed = o.init_failed;
+  res->nb_iter = o.init_failed ? 0 : o.nb_iter;
+  res->error_code = o.init_failed ? (prm->max_iter <= 0 ? -2 : 0)
+                                  : (o.nb_iter >= prm->max_iter ? -2 : o.fail);
+  res->hist_len = nh;
+  res->facteur_reste = o.facteur;
+  res->last_residual = o.reste;
+  return SB2_OK;
+}
+
 static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
                        double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
@@ -1047,6 +1094,8 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
     SB2_TRY(ensure_diag(A));
     diag = A->d_diag;
   }
+  if (which == kCg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
+    return chain_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
   return fused_solve(which, A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
 }
 
@@ -1055,6 +1104,13 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
 using namespace sb2;
 
 extern "C" {
+
+int sb2_krylov_set_config(int chain_min_n) {
+  if (chain_min_n < 0) return SB2_ERR_INVALID_VALUE;
+  const int old = g_chain_min_n;
+  g_chain_min_n = chain_min_n;
+  return old;
+}
 
 int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
            const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,

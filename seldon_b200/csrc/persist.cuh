@@ -68,9 +68,15 @@ __device__ __forceinline__ bool grid_sync(const Persist& P, unsigned& epoch, int
   if (s_last) {
     __threadfence();
     for (int k = 0; k < K; k++) {
-      double v = 0.0;
-      for (unsigned i = tid; i < G; i += NT) v = add_rn(v, __ldcg(P.partials + k * G + i));
-      v = block_sum<NT>(v, s_red);
+      const double* pv = P.partials + k * G;
+      double v0 = 0.0, v1 = 0.0;
+      unsigned i = tid;
+      for (; i + NT < G; i += 2 * NT) {
+        v0 = add_rn(v0, __ldcg(pv + i));
+        v1 = add_rn(v1, __ldcg(pv + i + NT));
+      }
+      if (i < G) v0 = add_rn(v0, __ldcg(pv + i));
+      const double v = block_sum<NT>(add_rn(v0, v1), s_red);
       if (tid == 0) P.sync->res[k] = v;
     }
     if (tid == 0) {

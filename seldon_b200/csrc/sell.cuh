@@ -111,17 +111,37 @@ __device__ __forceinline__ void sell_cta_row(const SellOp<VT>& S, int row, const
 // All bins of one product, work spread over the grid: warps take slices and
 // warp-bin rows, CTAs take CTA-bin rows.  `cta`/`ncta` let a persistent
 // kernel pass its own CTA index and grid size.
+// The thread bin (slices), warps grid-strided from (cta, ncta).
 template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 4>
-__device__ __forceinline__ void sell_spmv(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
-                                          AT* s_red, int cta, int ncta) {
+__device__ __forceinline__ void sell_spmv_slices(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
+                                                 int cta, int ncta) {
   constexpr int W = NT / 32;
   const int lane = threadIdx.x & 31;
   const long long gw = (long long)cta * W + (threadIdx.x >> 5), nw = (long long)ncta * W;
   for (long long s = gw; s < S.nslice; s += nw) sell_slice<VT, AT, XLoad, Epi, U>(S, (int)s, lane, xl, epi);
+}
+
+// The warp and CTA bins.
+template <int NT, typename VT, typename AT, class XLoad, class Epi>
+__device__ __forceinline__ void sell_spmv_long(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
+                                               AT* s_red, int cta, int ncta) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31;
+  const long long gw = (long long)cta * W + (threadIdx.x >> 5), nw = (long long)ncta * W;
   for (long long r = gw; r < S.nwarp_rows; r += nw)
     sell_warp_row<VT, AT>(S, __ldg(S.wrows + r), lane, xl, epi);
   for (int r = cta; r < S.ncta_rows; r += ncta)
     sell_cta_row<NT, VT, AT>(S, __ldg(S.crows + r), xl, epi, s_red);
+}
+
+// All bins of one product, work spread over the grid: warps take slices and
+// warp-bin rows, CTAs take CTA-bin rows.  `cta`/`ncta` let a persistent
+// kernel pass its own CTA index and grid size.
+template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 4>
+__device__ __forceinline__ void sell_spmv(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
+                                          AT* s_red, int cta, int ncta) {
+  sell_spmv_slices<NT, VT, AT, XLoad, Epi, U>(S, xl, epi, cta, ncta);
+  sell_spmv_long<NT, VT, AT>(S, xl, epi, s_red, cta, ncta);
 }
 
 #endif  // __CUDACC__

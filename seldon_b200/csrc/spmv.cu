@@ -59,14 +59,38 @@ __global__ void __launch_bounds__(NT, 2) spmv_tma_kernel(
 // configuration (threads per CTA, ring stages).
 static int g_spmv_algo = SB2_SPMV_SELL, g_spmv_threads = 256, g_spmv_stages = 4;
 
-template <int NT>
-__global__ void __launch_bounds__(NT) sell_kernel(SellOp<double> S, double alpha,
-                                                  const double* __restrict__ x, double beta,
-                                                  double* __restrict__ y, bool overwrite) {
-  __shared__ double s_red[NT / 32];
-  EpiAxpby epi{alpha, beta, y, overwrite};
+// y = beta*y + alpha*t, or y = alpha*t when OVERWRITE (Mlt)
+template <bool OVERWRITE>
+struct EpiAxpbyT {
+  double alpha, beta;
+  double* __restrict__ y;
+  __device__ __forceinline__ void operator()(int r, double t) const {
+    double v = mul_rn(alpha, t);
+    if (!OVERWRITE) v = add_rn(mul_rn(beta, y[r]), v);
+    y[r] = v;
+  }
+};
+
+// Thread bin: one warp per slice, 8 CTAs of 256 threads per SM (32
+// registers); the occupancy is what hides the latency of the x gathers.
+template <int NT, bool OVERWRITE>
+__global__ void __launch_bounds__(NT, 8) sell_slices_kernel(SellOp<double> S, double alpha,
+                                                            const double* __restrict__ x,
+                                                            double beta, double* __restrict__ y) {
+  EpiAxpbyT<OVERWRITE> epi{alpha, beta, y};
   XLoadLdg<double> xl{x};
-  sell_spmv<NT, double, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+  sell_spmv_slices<NT, double, double>(S, xl, epi, blockIdx.x, gridDim.x);
+}
+
+// Warp and CTA bins (rows longer than 32), launched only when present.
+template <int NT, bool OVERWRITE>
+__global__ void __launch_bounds__(NT) sell_long_kernel(SellOp<double> S, double alpha,
+                                                       const double* __restrict__ x, double beta,
+                                                       double* __restrict__ y) {
+  __shared__ double s_red[NT / 32];
+  EpiAxpbyT<OVERWRITE> epi{alpha, beta, y};
+  XLoadLdg<double> xl{x};
+  sell_spmv_long<NT, double, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
 }
 
 SellOp<double> sell_op(const CsrArrays& a) {
@@ -101,11 +125,21 @@ int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
                 double* y, bool overwrite, cudaStream_t s) {
   if (a.rows == 0) return SB2_OK;
   if (g_spmv_algo == SB2_SPMV_SELL && a.sell.nslice >= 0) {
-    const long long warps = (long long)a.sell.nslice + a.sell.nwarp;
-    long long g = std::max<long long>((warps + 7) / 8, a.sell.ncta);
-    g = std::max<long long>(g, 1);
-    sell_kernel<256><<<(unsigned)std::min<long long>(g, 1 << 30), 256, 0, s>>>(
-        sell_op(a), alpha, x, beta, y, overwrite);
+    const SellOp<double> op = sell_op(a);
+    if (a.sell.nslice > 0) {
+      const unsigned g = (unsigned)std::min<long long>(((long long)a.sell.nslice + 7) / 8, 1 << 30);
+      if (overwrite)
+        sell_slices_kernel<256, true><<<g, 256, 0, s>>>(op, alpha, x, beta, y);
+      else
+        sell_slices_kernel<256, false><<<g, 256, 0, s>>>(op, alpha, x, beta, y);
+    }
+    if (a.sell.nwarp + a.sell.ncta > 0) {
+      const unsigned g = (unsigned)std::max<long long>(((long long)a.sell.nwarp + 7) / 8, a.sell.ncta);
+      if (overwrite)
+        sell_long_kernel<256, true><<<g, 256, 0, s>>>(op, alpha, x, beta, y);
+      else
+        sell_long_kernel<256, false><<<g, 256, 0, s>>>(op, alpha, x, beta, y);
+    }
     SB2_CUDA_TRY(cudaGetLastError());
     return SB2_OK;
   }

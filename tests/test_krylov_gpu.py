@@ -235,3 +235,85 @@ def test_history_matches_oracle(api, oracle):
     k = min(len(res), len(ho)) - 2
     assert its[:k] == hio[:k].tolist()
     np.testing.assert_allclose(res[:k], ho[:k], rtol=1e-6)
+
+
+# ------------------------------------------------------------------ chained CG
+
+@pytest.fixture
+def chain_everywhere(api):
+    """Run Cg through the kernel chain at every size, then restore."""
+    from seldon_b200 import _lib
+    L = _lib.load()
+    old = L.sb2_krylov_set_config(0)
+    yield
+    L.sb2_krylov_set_config(old)
+
+
+@pytest.mark.parametrize("mname,pc", [("lap", 0), ("lap", 1), ("lap_up", 0), ("conv_spd", 1)])
+def test_chain_cg_parity(api, oracle, chain_everywhere, mname, pc):
+    mats = _mats()
+    if mname == "conv_spd":
+        A = matgen.poisson3d(14)
+    else:
+        A = mats[mname]
+    sym = mname.endswith("_up")
+    full = mats["lap"] if sym else A
+    n = A[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(6).uniform(-1, 1, n))
+    xo, co, no, ho, hio = oracle.solve("cg", *A, b, sym=sym, precond=pc, tol=1e-10, max_iter=3000,
+                                       hist_cap=4000)
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(3000, 1e-10)
+    it.HideMessages()
+    code = api.Cg(M, X, to_dev(b), api.JacobiPreconditioner() if pc else api.Preconditioner_Base(), it)
+    assert code == co == 0
+    assert abs(it.GetNumberIteration() - no) <= max(2, no // 20)
+    assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-7
+    assert len(it.history) == it.GetNumberIteration() + 1
+    assert it.history[0][1] == pytest.approx(ho[0], rel=1e-12)
+
+
+def test_chain_cg_edges(api, oracle, chain_everywhere):
+    # zero right-hand side, max_iter, breakdown #2, warm start -- through the chain
+    ptr, ind, val = matgen.lap2d(6)
+    A = api.RowSparse(36, 36, ptr, ind, val)
+    x0 = np.arange(36.0)
+    X = to_dev(x0)
+    it = api.Iteration(100, 1e-10)
+    it.HideMessages()
+    assert api.Cg(A, X, to_dev(np.zeros(36)), api.Preconditioner_Base(), it) == 0
+    assert np.array_equal(to_host(X), x0)
+    it = api.Iteration(3, 1e-30)
+    it.HideMessages()
+    assert api.Cg(A, to_dev(np.zeros(36)), to_dev(np.ones(36)), api.Preconditioner_Base(), it) == -2
+    assert it.GetNumberIteration() == 3
+    D = api.RowSparse(2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, -1.0]))
+    it = api.Iteration(10, 1e-12)
+    it.HideMessages()
+    assert api.Cg(D, to_dev(np.zeros(2)), to_dev(np.ones(2)), api.Preconditioner_Base(), it) == 2
+    rng = np.random.default_rng(3)
+    b, x0 = rng.standard_normal(36), rng.standard_normal(36)
+    X = to_dev(x0)
+    it = api.Iteration(1000, 1e-9)
+    it.HideMessages()
+    it.SetInitGuess(False)
+    assert api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it) == 0
+    xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b, x0=x0, tol=1e-9, max_iter=1000)
+    assert abs(it.GetNumberIteration() - no) <= 2
+    assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-6
+
+
+def test_chain_cg_large_vs_oracle(api, oracle):
+    """Default dispatch at n = 250000 (chain path) against the oracle."""
+    ptr, ind, val = matgen.lap2d(500)
+    n = ptr.size - 1
+    b = matgen.matvec(ptr, ind, val, np.random.default_rng(9).uniform(-1, 1, n))
+    xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b, tol=1e-8, max_iter=5000)
+    A = api.RowSparse(n, n, ptr, ind, val)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(5000, 1e-8)
+    it.HideMessages()
+    assert api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it) == co == 0
+    assert abs(it.GetNumberIteration() - no) <= max(2, no // 50)
+    assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-5
