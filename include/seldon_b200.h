@@ -236,6 +236,45 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
 int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
                    const sb2_iter_params* params, sb2_iter_result* result, void* stream);
 
+/* ------------------------------------------------------------ mixed precision */
+
+/* Iterative refinement with FP32 inner Krylov solves (FP32 values, vectors
+ * and accumulation) inside an FP64 outer loop: the residual r = b - A x, the
+ * solution update and the stopping test stay in FP64.  New form beside the
+ * reference's drivers (no counterpart in Seldon); the inner solver follows
+ * Cg.cxx:45-116 and the stopping rule Iterative.cxx:272-319. */
+typedef struct {
+  double tol;          /* outer target: ||b - A x|| / ||b|| < tol (FP64) */
+  double inner_tol;    /* relative residual reduction of each inner solve */
+  int max_outer;       /* refinement steps at most */
+  int max_inner;       /* iterations of one inner solve at most */
+  int solver;          /* inner solver: 0 = CG (the only one implemented) */
+  int restart;         /* reserved (GMRES restart) */
+  int init_guess_null; /* 1: x = 0; 0: start from x */
+  int mode;            /* 0: reliable updates -- one FP32 CG run whose residual
+                          is replaced by the FP64 true residual each time it has
+                          dropped by inner_tol (the search direction carries
+                          on, so the iteration count stays near FP64 CG's);
+                          1: restarted refinement -- a fresh FP32 CG solve of
+                          A d = r to inner_tol per outer step */
+} sb2_ir_params;
+
+typedef struct {
+  int outer_iter;      /* FP64 corrections applied */
+  int inner_iter;      /* FP32 iterations in all */
+  int error_code;      /* 0 converged, -2 stopped at max_outer */
+  int init_failed;     /* zero right-hand side (x untouched) */
+  int hist_len;        /* entries written to hist */
+  double rel_residual; /* final FP64 ||b - A x|| / ||b|| */
+} sb2_ir_result;
+
+/* M: NULL (identity) or a Jacobi preconditioner of A (applied in FP32 inside
+ * the inner solves).  hist (host, may be NULL) receives the FP64 relative
+ * residual before each refinement step and at the end. */
+int sb2_ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+                 const sb2_ir_params* params, sb2_ir_result* result, double* hist,
+                 int hist_cap, void* stream);
+
 /* Size from which Cg runs as a chain of full-occupancy kernels (one per
  * pass, scalars in device memory) instead of one persistent kernel; chosen
  * by the autotuner, default 200000 rows.  Returns the previous value.  No

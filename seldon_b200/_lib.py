@@ -56,6 +56,34 @@ class IterResult(ctypes.Structure):
     ]
 
 
+class IrParams(ctypes.Structure):
+    """sb2_ir_params: mixed-precision iterative refinement settings."""
+
+    _fields_ = [
+        ("tol", ctypes.c_double),
+        ("inner_tol", ctypes.c_double),
+        ("max_outer", ctypes.c_int),
+        ("max_inner", ctypes.c_int),
+        ("solver", ctypes.c_int),
+        ("restart", ctypes.c_int),
+        ("init_guess_null", ctypes.c_int),
+        ("mode", ctypes.c_int),
+    ]
+
+
+class IrResult(ctypes.Structure):
+    """sb2_ir_result."""
+
+    _fields_ = [
+        ("outer_iter", ctypes.c_int),
+        ("inner_iter", ctypes.c_int),
+        ("error_code", ctypes.c_int),
+        ("init_failed", ctypes.c_int),
+        ("hist_len", ctypes.c_int),
+        ("rel_residual", ctypes.c_double),
+    ]
+
+
 class SeldonB200Error(RuntimeError):
     def __init__(self, status, where):
         self.status = status
@@ -106,6 +134,9 @@ _SOLVER_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParam
                 ctypes.POINTER(IterResult), c_void_p, c_void_p, ctypes.c_int, c_void_p]
 for _name in ("sb2_cg", "sb2_bicgstab", "sb2_gmres"):
     _PROTOS.append((_name, ctypes.c_int, _SOLVER_ARGS))
+_PROTOS.append(("sb2_ir_solve", ctypes.c_int,
+                [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IrParams),
+                 ctypes.POINTER(IrResult), c_void_p, ctypes.c_int, c_void_p]))
 _PROTOS.append(("sb2_cg_noalloc", ctypes.c_int,
                 [c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParams),
                  ctypes.POINTER(IterResult), c_void_p]))

@@ -16,7 +16,7 @@ for device memory and streams; every operation runs in libseldon_b200.so.
 import ctypes
 
 from . import _lib
-from ._lib import IterParams, IterResult, check
+from ._lib import IrParams, IrResult, IterParams, IterResult, check
 
 _L = _lib.load()
 
@@ -352,3 +352,32 @@ def BiCgStab(A, x, b, M, iteration, hist_cap=None, stream=None):
 def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None):
     """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183)."""
     return _solve(_L.sb2_gmres, A, x, b, M, iteration, hist_cap, stream)
+
+
+# ------------------------------------------------------------------ mixed precision
+
+def IterativeRefinement(A, x, b, M=None, tol=1e-10, inner_tol=None, max_outer=50,
+                        max_inner=20000, init_guess_null=True, restarted=False, stream=None):
+    """FP32-inner / FP64-outer iterative refinement with CG.
+
+    restarted=False: reliable updates -- one FP32 CG run whose residual is
+    replaced by the FP64 true residual each time it has dropped by inner_tol
+    (default 1e-2); True: a fresh FP32 CG solve of A d = r to inner_tol
+    (default 1e-5) per outer step.  Returns (error_code, info) with the FP64
+    corrections, FP32 iterations, final FP64 relative residual and the
+    residual history."""
+    import numpy as np
+    if inner_tol is None:
+        inner_tol = 1e-5 if restarted else 1e-2
+    prm = IrParams(tol, inner_tol, max_outer, max_inner, 0, 0, int(init_guess_null),
+                   1 if restarted else 0)
+    res = IrResult()
+    hist = np.zeros(max_outer + 2)
+    Mh = None if (M is None or M.kind == _lib.PRECOND_IDENTITY) else M.handle_for(A)
+    check(_L.sb2_ir_solve(A.handle, Mh, _dev_ptr(x, A.m, "x"), _dev_ptr(b, A.m, "b"),
+                          ctypes.byref(prm), ctypes.byref(res), _np_ptr(hist), hist.size,
+                          _stream(stream)), "sb2_ir_solve")
+    info = {"outer_iter": res.outer_iter, "inner_iter": res.inner_iter,
+            "rel_residual": res.rel_residual, "init_failed": bool(res.init_failed),
+            "history": hist[:res.hist_len].tolist()}
+    return res.error_code, info

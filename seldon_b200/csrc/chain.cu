@@ -23,7 +23,7 @@ constexpr int CT = 256;
 
 template <typename T>
 __device__ __forceinline__ bool chain_done(const ChainState<T>* st) {
-  return *((volatile const int*)&st->done) != 0;
+  return (*((volatile const int*)&st->done) | *((volatile const int*)&st->pending)) != 0;
 }
 
 // Finished() at the current nb_iter (Iterative.cxx:299-319), run by one thread.
@@ -147,7 +147,8 @@ __global__ void __launch_bounds__(CT, PART == 0 ? 8 : 1)
     EpiChainDot<T> epi{a.q, a.p, T(0)};
     XLoadLdg<T> xl{a.p};
     if (PART == 0)
-      sell_spmv_slices<CT, VT, T>(S, xl, epi, blockIdx.x, gridDim.x);
+      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainDot<T>, 4>(
+          S, xl, epi, blockIdx.x, gridDim.x);
     else
       sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
     T v[1] = {block_sum<CT>(epi.acc, s_red)};
@@ -168,24 +169,80 @@ __global__ void __launch_bounds__(CT, PART == 0 ? 8 : 1)
   }
 }
 
+// Elementwise passes work on groups of 4 consecutive entries loaded with
+// 16-byte accesses (the work vectors come from one 256-byte-aligned block;
+// a caller's x or b that is not 16-byte aligned takes the scalar path).
+template <typename T>
+struct Quad {
+  T v[4];
+};
+template <typename T>
+__device__ __forceinline__ Quad<T> ld4(const T* p) {
+  Quad<T> q;
+  if (sizeof(T) == 8) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *(reinterpret_cast<const double2*>(p) + 1);
+    q.v[0] = (T)a.x; q.v[1] = (T)a.y; q.v[2] = (T)b.x; q.v[3] = (T)b.y;
+  } else {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    q.v[0] = (T)a.x; q.v[1] = (T)a.y; q.v[2] = (T)a.z; q.v[3] = (T)a.w;
+  }
+  return q;
+}
+template <typename T>
+__device__ __forceinline__ void st4(T* p, const Quad<T>& q) {
+  if (sizeof(T) == 8) {
+    *reinterpret_cast<double2*>(p) = make_double2((double)q.v[0], (double)q.v[1]);
+    *(reinterpret_cast<double2*>(p) + 1) = make_double2((double)q.v[2], (double)q.v[3]);
+  } else {
+    *reinterpret_cast<float4*>(p) = make_float4((float)q.v[0], (float)q.v[1], (float)q.v[2], (float)q.v[3]);
+  }
+}
+
+__device__ __forceinline__ bool aligned16(const void* p) {
+  return (reinterpret_cast<unsigned long long>(p) & 15ull) == 0;
+}
+
 // p = z (first iteration) | p = beta*p + z: Mlt(beta, p); Add(1, z, p).
 template <typename T>
-__global__ void __launch_bounds__(CT, 8) k_p(ChainArgs<T> a) {
+__global__ void __launch_bounds__(CT, 4) k_p(ChainArgs<T> a) {
   if (chain_done(a.st)) return;
   const bool first = (a.st->nb_iter == 0);
   const T beta = a.st->beta;
+  const T zc = a.st->zc;  // 1 in the reference's recurrence: 1*z == z exactly
   T* __restrict__ p = a.p;
   const T* __restrict__ r = a.r;
-#pragma unroll 4
-  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+  constexpr int H = sizeof(T) == 8 ? 1 : 2;  // quads per stream: 32 bytes in flight each
+  const long long n8 = (aligned16(p) && aligned16(r) && (!a.diag || aligned16(a.diag))) ? a.n / (4 * H) : 0;
+  const long long t0 = (long long)blockIdx.x * CT + threadIdx.x, ts = (long long)gridDim.x * CT;
+  for (long long g = t0; g < n8; g += ts) {
+    const long long i = 4 * H * g;
+    Quad<T> rq[H], dq[H], pq[H];
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+      rq[h] = ld4(r + i + 4 * h);
+      if (a.diag) dq[h] = ld4(a.diag + i + 4 * h);
+      if (!first) pq[h] = ld4(p + i + 4 * h);
+    }
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const T z = a.diag ? rq[h].v[k] / dq[h].v[k] : rq[h].v[k];
+        pq[h].v[k] = first ? z : add_rn(mul_rn(pq[h].v[k], beta), mul_rn(zc, z));
+      }
+      st4(p + i + 4 * h, pq[h]);
+    }
+  }
+  for (long long i = 4 * H * n8 + t0; i < a.n; i += ts) {
     const T z = zval(a.diag, i, r[i]);
-    p[i] = first ? z : add_rn(mul_rn(p[i], beta), z);
+    p[i] = first ? z : add_rn(mul_rn(p[i], beta), mul_rn(zc, z));
   }
 }
 
 // Add(alpha, p, x); Add(-alpha, q, r); ||r||^2, (r, z); ++iter; the test.
 template <typename T>
-__global__ void __launch_bounds__(CT, 8) k_x(ChainArgs<T> a) {
+__global__ void __launch_bounds__(CT, 4) k_x(ChainArgs<T> a) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
   if (chain_done(a.st)) return;
@@ -195,8 +252,37 @@ __global__ void __launch_bounds__(CT, 8) k_x(ChainArgs<T> a) {
   const T* __restrict__ p = a.p;
   const T* __restrict__ q = a.q;
   T rr = T(0), rz = T(0);
-#pragma unroll 4
-  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+  const bool vec = aligned16(x) && aligned16(r) && aligned16(p) && aligned16(q) &&
+                   (!a.diag || aligned16(a.diag));
+  constexpr int H = sizeof(T) == 8 ? 1 : 2;  // quads per stream: 32 bytes in flight each
+  const long long n8 = vec ? a.n / (4 * H) : 0;
+  const long long t0 = (long long)blockIdx.x * CT + threadIdx.x, ts = (long long)gridDim.x * CT;
+  for (long long g = t0; g < n8; g += ts) {
+    const long long i = 4 * H * g;
+    Quad<T> xq[H], rq[H], pq[H], qq[H], dq[H];
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+      xq[h] = ld4(x + i + 4 * h);
+      rq[h] = ld4(r + i + 4 * h);
+      pq[h] = ld4(p + i + 4 * h);
+      qq[h] = ld4(q + i + 4 * h);
+      if (a.diag) dq[h] = ld4(a.diag + i + 4 * h);
+    }
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (alpha != T(0)) xq[h].v[k] = add_rn(xq[h].v[k], mul_rn(alpha, pq[h].v[k]));
+        if (-alpha != T(0)) rq[h].v[k] = add_rn(rq[h].v[k], mul_rn(-alpha, qq[h].v[k]));
+        const T ri = rq[h].v[k];
+        rr = add_rn(rr, mul_rn(ri, ri));
+        rz = add_rn(rz, mul_rn(ri, a.diag ? ri / dq[h].v[k] : ri));
+      }
+      if (alpha != T(0)) st4(x + i + 4 * h, xq[h]);
+      if (-alpha != T(0)) st4(r + i + 4 * h, rq[h]);
+    }
+  }
+  for (long long i = 4 * H * n8 + t0; i < a.n; i += ts) {
     if (alpha != T(0)) x[i] = add_rn(x[i], mul_rn(alpha, __ldg(p + i)));
     T ri = r[i];
     if (-alpha != T(0)) {
@@ -226,11 +312,128 @@ __global__ void __launch_bounds__(CT, 8) k_x(ChainArgs<T> a) {
   }
 }
 
+// Reliable-update form of k_x (mixed precision): x here is the low-precision
+// correction accumulated since the last high-precision update.  The test uses
+// ||r|| / ||b|| as the estimate of the true residual; a drop by `delta` since
+// the last correction, or a predicted convergence, halts with `pending`.
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_x_ru(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  if (chain_done(a.st)) return;
+  const T alpha = a.st->alpha;
+  T* __restrict__ x = a.x;
+  T* __restrict__ r = a.r;
+  const T* __restrict__ p = a.p;
+  const T* __restrict__ q = a.q;
+  T rr = T(0), rz = T(0);
+  const bool vec = aligned16(x) && aligned16(r) && aligned16(p) && aligned16(q) &&
+                   (!a.diag || aligned16(a.diag));
+  constexpr int H = sizeof(T) == 8 ? 1 : 2;  // quads per stream: 32 bytes in flight each
+  const long long n8 = vec ? a.n / (4 * H) : 0;
+  const long long t0 = (long long)blockIdx.x * CT + threadIdx.x, ts = (long long)gridDim.x * CT;
+  for (long long g = t0; g < n8; g += ts) {
+    const long long i = 4 * H * g;
+    Quad<T> xq[H], rq[H], pq[H], qq[H], dq[H];
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+      xq[h] = ld4(x + i + 4 * h);
+      rq[h] = ld4(r + i + 4 * h);
+      pq[h] = ld4(p + i + 4 * h);
+      qq[h] = ld4(q + i + 4 * h);
+      if (a.diag) dq[h] = ld4(a.diag + i + 4 * h);
+    }
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        xq[h].v[k] = add_rn(xq[h].v[k], mul_rn(alpha, pq[h].v[k]));
+        rq[h].v[k] = add_rn(rq[h].v[k], mul_rn(-alpha, qq[h].v[k]));
+        const T ri = rq[h].v[k];
+        rr = add_rn(rr, mul_rn(ri, ri));
+        rz = add_rn(rz, mul_rn(ri, a.diag ? ri / dq[h].v[k] : ri));
+      }
+      st4(x + i + 4 * h, xq[h]);
+      st4(r + i + 4 * h, rq[h]);
+    }
+  }
+  for (long long i = 4 * H * n8 + t0; i < a.n; i += ts) {
+    x[i] = add_rn(x[i], mul_rn(alpha, __ldg(p + i)));
+    const T ri = add_rn(r[i], mul_rn(-alpha, __ldg(q + i)));
+    r[i] = ri;
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rz = add_rn(rz, mul_rn(ri, zval(a.diag, i, ri)));
+  }
+  T v[2] = {block_sum<CT>(rr, s_red), block_sum<CT>(rz, s_red)};
+  if (deposit_and_finish<CT, 2>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->nb_iter++;
+    st->zc = T(1);
+    const double res = sqrt((double)s_out[0]);
+    st->reste = st->facteur * res;
+    st->rho_1 = st->rho;
+    st->rho = s_out[1];
+    if (st->nb_iter >= st->max_iter) {
+      st->pending = 1;  // correct once more, then stop
+      return;
+    }
+    if (st->reste < st->tol || res < st->delta * st->rmax) {
+      st->pending = 1;
+      return;
+    }
+    if (st->rho == T(0)) {
+      st->fail = 1;
+      st->pending = 1;
+      return;
+    }
+    st->beta = st->rho / st->rho_1;
+  }
+}
+
+// After a high-precision correction replaced r: rho = (r, z) of the new
+// residual, beta against the previous iteration's rho, new ||r|| reference.
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_rho_ru(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[3];
+  T rr = T(0), rz = T(0), rp = T(0);
+  const bool have_p = (a.st->nb_iter > 0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const T ri = a.r[i];
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rz = add_rn(rz, mul_rn(ri, zval(a.diag, i, ri)));
+    if (have_p) rp = add_rn(rp, mul_rn(ri, a.p[i]));
+  }
+  T v[3] = {block_sum<CT>(rr, s_red), block_sum<CT>(rz, s_red), block_sum<CT>(rp, s_red)};
+  if (deposit_and_finish<CT, 3>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->rmax = sqrt((double)s_out[0]);
+    st->rho = s_out[1];
+    st->zc = T(1);
+    if (!have_p) {
+      st->pending = 0;  // first direction: p = z
+      return;
+    }
+    if (st->rho == T(0)) {
+      st->fail = 1;
+      st->done = 1;
+      return;
+    }
+    st->beta = st->rho / st->rho_1;
+    // p <- z + beta (p - ((r, p) / (r, z)) z): the previous direction loses
+    // its component along the replaced residual, restoring r orthogonal to p
+    st->zc = T(1) - st->beta * (s_out[2] / st->rho);
+    st->pending = 0;
+  }
+}
+
 // ----------------------------------------------------------------- host driver
 
 static int chain_elem_grid(int n) {
   const int cap = num_sms(current_device()) * 8;
-  return std::max(1, std::min((n + CT * 4 - 1) / (CT * 4), cap));
+  return std::max(1, std::min((n + CT * 32 - 1) / (CT * 32), cap));
 }
 
 // CTAs of a reducing product: one slice per warp up to four resident waves,
@@ -238,7 +441,7 @@ static int chain_elem_grid(int n) {
 template <typename VT>
 static int reducing_slice_grid(const SellOp<VT>& S) {
   if (S.nslice <= 0) return 0;
-  const int cap = num_sms(current_device()) * 8 * 4;
+  const int cap = num_sms(current_device()) * 24;
   return std::min((S.nslice + 7) / 8, cap);
 }
 
@@ -276,6 +479,7 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
   init.max_iter = max_iter;
   init.tol = tol;
   init.hist_cap = hist_cap;
+  init.zc = T(1);
   SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   ChainArgs<T> a{n, b, x, work, work + n, work + 2 * (size_t)n, diag, st, part, hist, hist_it};
   const int ge = chain_elem_grid(n);
@@ -304,6 +508,64 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
   *out = h;
   return SB2_OK;
 }
+
+template <typename T, typename VT>
+int chain_ru_resume(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                    ChainState<T>* st, T* part, cudaStream_t s);
+
+// Reliable-update CG iterations: the caller's loop applies the corrections.
+// ru_start: state for an initial residual r already in place (x = 0);
+// ru_iterate: enqueue up to `chunk` iterations, return the state after them.
+template <typename T, typename VT>
+int chain_ru_start(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                   ChainState<T>* st, T* part, double facteur, double tol, double delta,
+                   int max_iter, cudaStream_t s) {
+  ChainState<T> init{};
+  init.max_iter = max_iter;
+  init.tol = tol;
+  init.delta = delta;
+  init.facteur = facteur;
+  init.pending = 1;
+  init.zc = T(1);
+  SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  SB2_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(T) * (size_t)n, s));
+  return chain_ru_resume<T, VT>(S, n, diag, x, r, work, st, part, s);
+}
+
+template <typename T, typename VT>
+int chain_ru_resume(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                    ChainState<T>* st, T* part, cudaStream_t s) {
+  ChainArgs<T> a{n, nullptr, x, r, work, work + n, diag, st, part, nullptr, nullptr};
+  k_rho_ru<T><<<chain_elem_grid(n), CT, 0, s>>>(a);
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+template <typename T, typename VT>
+int chain_ru_iterate(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                     ChainState<T>* st, T* part, int chunk, cudaStream_t s, ChainState<T>* out) {
+  ChainArgs<T> a{n, nullptr, x, r, work, work + n, diag, st, part, nullptr, nullptr};
+  const int ge = chain_elem_grid(n);
+  for (int c = 0; c < chunk; c++) {
+    k_p<T><<<ge, CT, 0, s>>>(a);
+    SB2_TRY((launch_spmv_pair<T, VT>(0, a, S, s)));
+    k_x_ru<T><<<ge, CT, 0, s>>>(a);
+  }
+  SB2_CUDA_TRY(cudaGetLastError());
+  SB2_CUDA_TRY(cudaMemcpyAsync(out, st, sizeof(*out), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  return SB2_OK;
+}
+
+template int chain_ru_start<float, float>(const SellOp<float>&, int, const float*, float*, float*,
+                                          float*, ChainState<float>*, float*, double, double,
+                                          double, int, cudaStream_t);
+template int chain_ru_resume<float, float>(const SellOp<float>&, int, const float*, float*,
+                                           float*, float*, ChainState<float>*, float*,
+                                           cudaStream_t);
+template int chain_ru_iterate<float, float>(const SellOp<float>&, int, const float*, float*,
+                                            float*, float*, ChainState<float>*, float*, int,
+                                            cudaStream_t, ChainState<float>*);
 
 template long long chain_part_slots<double>(const SellOp<double>&, int);
 template long long chain_part_slots<float>(const SellOp<float>&, int);

@@ -28,6 +28,16 @@ struct ChainState {
   int nb_iter, max_iter, done, fail, init_failed, hist_len, hist_cap;
   double tol;
   unsigned cnt;  // deposits of the reduction in progress
+  // reliable updates (mixed precision): when the low-precision residual has
+  // dropped by `delta` since the last correction, or predicts convergence,
+  // the iteration halts with `pending` set and the host applies the
+  // high-precision correction before resuming
+  int pending;
+  double delta;
+  double rmax;   // ||r|| at the last correction
+  T zc;          // coefficient of z in the next p update (1 except right
+                 // after a correction, where it also removes from p its
+                 // component along the replaced residual)
 };
 
 template <typename T>

@@ -383,6 +383,7 @@ int sb2_csr_destroy(sb2_csr* A) {
   free_csr(&A->trans);
   cudaFree(A->d_diag);
   cudaFree(A->d_val32);
+  cudaFree(A->d_diag32);
   cudaFree(A->d_hx);
   cudaFree(A->d_hy);
   cudaSetDevice(prev);

@@ -99,6 +99,7 @@ struct sb2_csr {
   sb2::CsrArrays trans;   // A^T (built on first transposed product)
   double* d_diag = nullptr;  // A(i,i) by Seldon's lookup rule (lazy)
   float* d_val32 = nullptr;  // FP32 copy of full.d_val (lazy)
+  float* d_diag32 = nullptr; // FP32 copy of d_diag (lazy)
   std::mutex mu;             // guards the lazy members
   // staging vectors of the host-buffer entry points (lazy, reused)
   double* d_hx = nullptr;
