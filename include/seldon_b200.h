@@ -275,6 +275,53 @@ int sb2_ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double
                  const sb2_ir_params* params, sb2_ir_result* result, double* hist,
                  int hist_cap, void* stream);
 
+/* ------------------------------------------------------------ batched solves */
+
+/* A batch of independent square systems, held as one block-diagonal CSR
+ * operator: system s owns rows [sys_row[s], sys_row[s+1]) and its entries may
+ * only reference columns in that range (checked).  New form beside the
+ * reference's drivers (no counterpart in Seldon): each system is solved as
+ * Cg.cxx:45-116 would, with the Iterative.cxx:272-319 stopping rule. */
+typedef struct sb2_batch sb2_batch;
+
+typedef struct {
+  double tol;          /* per system: stop when ||b - A x|| / ||b|| < tol (FP64) */
+  double update_ratio; /* mode 0: FP64 correction when the FP32 residual has
+                          dropped by this factor (e.g. 1e-2) */
+  int max_iter;        /* iterations per system at most */
+  int mode;            /* 0: FP32 CG with FP64 reliable updates; 1: FP64 CG */
+  int init_guess_null; /* 1: x = 0; 0: start from x */
+} sb2_batch_params;
+
+typedef struct {
+  int converged;           /* systems that met tol */
+  int max_iter;            /* largest iteration count of a system */
+  long long total_iter;    /* iterations summed over the systems */
+  double max_rel_residual; /* worst final FP64 relative residual */
+} sb2_batch_result;
+
+/* HOST arrays: sys_row[nsys+1], ptr[m+1], ind[nnz] (global columns), val[nnz]. */
+int sb2_batch_create(int nsys, const int* sys_row, const int* ptr, const int* ind,
+                     const double* val, sb2_batch** out);
+int sb2_batch_destroy(sb2_batch* B);
+
+/* Solve every system in ONE persistent launch (CTAs take systems from a
+ * queue, largest first).  x, b: device vectors of all rows.  d_iters /
+ * d_relres (device, may be NULL): per-system iteration count and final
+ * relative residual.  With result == NULL the call only enqueues work on
+ * `stream` (no host synchronization, so it can be captured in a CUDA graph);
+ * with result != NULL it waits and summarizes (d_iters and d_relres needed). */
+int sb2_batch_solve(const sb2_batch* B, double* x, const double* b,
+                    const sb2_batch_params* params, int* d_iters, double* d_relres,
+                    sb2_batch_result* result, void* stream);
+
+/* Autotuner: times the solve of this batch (x is overwritten) with CTAs of
+ * 128, 256 and 512 threads and keeps the fastest for later solves. */
+int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
+                       const sb2_batch_params* params, void* stream);
+int sb2_batch_set_threads(sb2_batch* B, int threads);
+int sb2_batch_get_threads(const sb2_batch* B);
+
 /* Size from which Cg runs as a chain of full-occupancy kernels (one per
  * pass, scalars in device memory) instead of one persistent kernel; chosen
  * by the autotuner, default 200000 rows.  Returns the previous value.  No

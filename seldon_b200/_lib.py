@@ -84,6 +84,29 @@ class IrResult(ctypes.Structure):
     ]
 
 
+class BatchParams(ctypes.Structure):
+    """sb2_batch_params."""
+
+    _fields_ = [
+        ("tol", ctypes.c_double),
+        ("update_ratio", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
+        ("mode", ctypes.c_int),
+        ("init_guess_null", ctypes.c_int),
+    ]
+
+
+class BatchResult(ctypes.Structure):
+    """sb2_batch_result."""
+
+    _fields_ = [
+        ("converged", ctypes.c_int),
+        ("max_iter", ctypes.c_int),
+        ("total_iter", ctypes.c_longlong),
+        ("max_rel_residual", ctypes.c_double),
+    ]
+
+
 class SeldonB200Error(RuntimeError):
     def __init__(self, status, where):
         self.status = status
@@ -137,6 +160,18 @@ for _name in ("sb2_cg", "sb2_bicgstab", "sb2_gmres"):
 _PROTOS.append(("sb2_ir_solve", ctypes.c_int,
                 [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IrParams),
                  ctypes.POINTER(IrResult), c_void_p, ctypes.c_int, c_void_p]))
+_PROTOS += [
+    ("sb2_batch_create", ctypes.c_int,
+     [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_void_p)]),
+    ("sb2_batch_destroy", ctypes.c_int, [c_void_p]),
+    ("sb2_batch_solve", ctypes.c_int,
+     [c_void_p, c_void_p, c_void_p, ctypes.POINTER(BatchParams), c_void_p, c_void_p,
+      ctypes.POINTER(BatchResult), c_void_p]),
+    ("sb2_batch_autotune", ctypes.c_int,
+     [c_void_p, c_void_p, c_void_p, ctypes.POINTER(BatchParams), c_void_p]),
+    ("sb2_batch_set_threads", ctypes.c_int, [c_void_p, ctypes.c_int]),
+    ("sb2_batch_get_threads", ctypes.c_int, [c_void_p]),
+]
 _PROTOS.append(("sb2_cg_noalloc", ctypes.c_int,
                 [c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParams),
                  ctypes.POINTER(IterResult), c_void_p]))

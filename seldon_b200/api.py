@@ -381,3 +381,74 @@ def IterativeRefinement(A, x, b, M=None, tol=1e-10, inner_tol=None, max_outer=50
             "rel_residual": res.rel_residual, "init_failed": bool(res.init_failed),
             "history": hist[:res.hist_len].tolist()}
     return res.error_code, info
+
+
+# ------------------------------------------------------------------ batched solves
+
+class Batch:
+    """Independent systems solved together (block-diagonal CSR + row ranges).
+
+    systems: list of (ptr, ind, val) CSR triples with local indices."""
+
+    def __init__(self, systems):
+        import numpy as np
+        sizes = [len(p) - 1 for p, _, _ in systems]
+        sys_row = np.zeros(len(systems) + 1, dtype=np.int32)
+        np.cumsum(sizes, out=sys_row[1:])
+        ptrs, inds, vals, off, base = [], [], [], 0, 0
+        for (p, i, v), r0 in zip(systems, sys_row[:-1]):
+            p = np.asarray(p, dtype=np.int64)
+            ptrs.append(p[:-1] + base)
+            inds.append(np.asarray(i, dtype=np.int64) + r0)
+            vals.append(np.asarray(v, dtype=np.float64))
+            base += int(p[-1])
+        ptr = np.concatenate(ptrs + [np.array([base])]).astype(np.int32)
+        ind = np.ascontiguousarray(np.concatenate(inds).astype(np.int32))
+        val = np.ascontiguousarray(np.concatenate(vals))
+        self.sys_row = sys_row
+        self.m = int(sys_row[-1])
+        self.nsys = len(systems)
+        h = ctypes.c_void_p()
+        check(_L.sb2_batch_create(self.nsys, _np_ptr(sys_row), _np_ptr(ptr), _np_ptr(ind),
+                                  _np_ptr(val), ctypes.byref(h)), "sb2_batch_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def params(self, tol=1e-9, update_ratio=1e-2, max_iter=10000, mixed=True, init_guess_null=True):
+        return _lib.BatchParams(tol, update_ratio, max_iter, 0 if mixed else 1, int(init_guess_null))
+
+    def solve(self, x, b, iters=None, relres=None, summary=True, stream=None, **kw):
+        """Solve all systems; iters/relres: optional device tensors (int32/float64)."""
+        import torch
+        prm = self.params(**kw)
+        if summary and (iters is None or relres is None):
+            iters = torch.zeros(self.nsys, dtype=torch.int32, device=x.device)
+            relres = torch.zeros(self.nsys, dtype=torch.float64, device=x.device)
+        res = _lib.BatchResult()
+        check(_L.sb2_batch_solve(self._h, _dev_ptr(x, self.m, "x"), _dev_ptr(b, self.m, "b"),
+                                 ctypes.byref(prm),
+                                 ctypes.c_void_p(iters.data_ptr()) if iters is not None else None,
+                                 ctypes.c_void_p(relres.data_ptr()) if relres is not None else None,
+                                 ctypes.byref(res) if summary else None, _stream(stream)),
+              "sb2_batch_solve")
+        return res if summary else None
+
+    def autotune(self, x, b, stream=None, **kw):
+        prm = self.params(**kw)
+        check(_L.sb2_batch_autotune(self._h, _dev_ptr(x, self.m, "x"), _dev_ptr(b, self.m, "b"),
+                                    ctypes.byref(prm), _stream(stream)), "sb2_batch_autotune")
+        return _L.sb2_batch_get_threads(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _L.sb2_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

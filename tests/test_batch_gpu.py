@@ -1,0 +1,100 @@
+"""Batched solves: many independent uneven SPD systems in one persistent
+launch, checked system by system against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+from tests.helpers import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api(cuda):
+    from seldon_b200 import api
+    return api
+
+
+def _systems(seed, k, lo, hi, zero=()):
+    rng = np.random.default_rng(seed)
+    systems, rhs, xs = [], [], []
+    for s in range(k):
+        g = int(rng.integers(lo, hi + 1))
+        ptr, ind, val = matgen.lap2d(g, shift=0.01)
+        x = rng.uniform(-1, 1, g * g)
+        systems.append((ptr, ind, val))
+        xs.append(x)
+        rhs.append(np.zeros(g * g) if s in zero else matgen.matvec(ptr, ind, val, x))
+    return systems, rhs, xs
+
+
+@pytest.mark.parametrize("mixed", [True, False])
+def test_batch_matches_oracle(api, oracle, mixed):
+    systems, rhs, xs = _systems(1, 40, 4, 30)
+    B = api.Batch(systems)
+    import torch
+    X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    res = B.solve(X, to_dev(np.concatenate(rhs)), it, rr, tol=1e-9, mixed=mixed)
+    assert res.converged == B.nsys and res.max_rel_residual < 1e-9
+    x = to_host(X)
+    its = to_host(it)
+    for s, ((ptr, ind, val), b) in enumerate(zip(systems, rhs)):
+        xsys = x[B.sys_row[s]:B.sys_row[s + 1]]
+        rel = np.linalg.norm(b - matgen.matvec(ptr, ind, val, xsys)) / np.linalg.norm(b)
+        assert rel < 1e-9, (s, rel)
+        xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b, tol=1e-9, max_iter=2000)
+        assert np.linalg.norm(xsys - xo) / np.linalg.norm(xo) < 1e-6
+        if not mixed:
+            assert abs(int(its[s]) - no) <= max(2, no // 20), (s, its[s], no)
+
+
+def test_batch_edges(api):
+    import torch
+    systems, rhs, xs = _systems(2, 6, 3, 12, zero=(2,))
+    B = api.Batch(systems)
+    x0 = np.arange(B.m, dtype=float)
+    X = to_dev(x0)
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    res = B.solve(X, to_dev(np.concatenate(rhs)), it, rr, tol=1e-9, init_guess_null=False)
+    x = to_host(X)
+    # the system with a zero right-hand side is left as it was
+    a, e = B.sys_row[2], B.sys_row[3]
+    assert np.array_equal(x[a:e], x0[a:e]) and int(to_host(it)[2]) == 0
+    assert res.converged == B.nsys
+    # entries may not cross systems
+    from seldon_b200._lib import SeldonB200Error
+    bad = [(np.array([0, 1, 2]), np.array([0, 2]), np.array([1.0, 1.0])),
+           (np.array([0, 1]), np.array([0]), np.array([1.0]))]
+    with pytest.raises(SeldonB200Error):
+        api.Batch(bad)
+
+
+def test_batch_autotune_and_graph(api):
+    import torch
+    systems, rhs, xs = _systems(3, 64, 6, 40)
+    B = api.Batch(systems)
+    b = to_dev(np.concatenate(rhs))
+    X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
+    assert B.autotune(X, b, tol=1e-9) in (128, 256, 512)
+    # the solve enqueues only device work: capture it once, replay it
+    X.zero_()
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    B.solve(X, b, it, rr, tol=1e-9)
+    ref = to_host(X).copy()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        B.solve(X, b, it, rr, summary=False, tol=1e-9)
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        B.solve(X, b, it, rr, summary=False, tol=1e-9)
+    X.fill_(7.0)
+    g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(X), ref)  # deterministic: same result bit for bit
+    assert float(to_host(rr).max()) < 1e-9
