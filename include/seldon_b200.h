@@ -275,6 +275,28 @@ int sb2_ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double
                  const sb2_ir_params* params, sb2_ir_result* result, double* hist,
                  int hist_cap, void* stream);
 
+/* ------------------------------------------------------------ differentiation */
+/* Pieces of the hand-written adjoint of x = A^{-1} b for a loss L(x): solve
+ * A^T lambda = dL/dx with sb2_cg (symmetric A) or sb2_bicgstab / sb2_gmres
+ * (general A: pass the transpose), then dL/db = lambda and the kernels below.
+ * No counterpart in the reference (new form beside its drivers). */
+
+/* New values on the same pattern (general RowSparse matrices only): val[nnz]
+ * in the stored order, on the device (on_device = 1) or the host.  Derived
+ * copies (diagonal, FP32 values, transpose) are rebuilt on their next use. */
+int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* stream);
+
+/* grad_val[k] = alpha * lambda[row(k)] * x[ind[k]] for every stored entry k:
+ * with alpha = -1, dL/dA_ij restricted to the pattern. */
+int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const double* x,
+                     double* grad_val, void* stream);
+
+/* grad[e] = -(lambda[i] - lambda[j]) * (x[i] - x[j]) for edges e = (ei[e], ej[e]):
+ * dL/dtheta_e of a weighted graph Laplacian (A_ii, A_jj += theta_e,
+ * A_ij = A_ji -= theta_e). */
+int sb2_grad_edges(int nedges, const int* ei, const int* ej, const double* lambda,
+                   const double* x, double* grad, void* stream);
+
 /* ------------------------------------------------------------ batched solves */
 
 /* A batch of independent square systems, held as one block-diagonal CSR

@@ -172,6 +172,13 @@ _PROTOS += [
     ("sb2_batch_set_threads", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("sb2_batch_get_threads", ctypes.c_int, [c_void_p]),
 ]
+_PROTOS += [
+    ("sb2_csr_set_values", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p]),
+    ("sb2_grad_pattern", ctypes.c_int,
+     [c_void_p, ctypes.c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_grad_edges", ctypes.c_int,
+     [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+]
 _PROTOS.append(("sb2_cg_noalloc", ctypes.c_int,
                 [c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParams),
                  ctypes.POINTER(IterResult), c_void_p]))

@@ -189,6 +189,7 @@ int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
   const long long tot = sptr[ns];
   std::vector<int> scol(std::max(tot, 1ll), 0);
   std::vector<double> sval(std::max(tot, 1ll), 0.0);
+  std::vector<long long> pos(std::max<long long>(ptr[rows], 1), -1);
   for (int sl = 0; sl < ns; sl++)
     for (int l = 0; l < 32; l++) {
       const size_t q = (size_t)sl * 32 + l;
@@ -198,6 +199,7 @@ int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
         const long long e = sptr[sl] + (long long)j * 32 + l;
         scol[e] = ind[ptr[r] + j];
         sval[e] = val[ptr[r] + j];
+        pos[ptr[r] + j] = e;
       }
     }
   out->nslice = ns;
@@ -213,6 +215,8 @@ int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
   SB2_CUDA_TRY(cudaMemcpy(out->d_scol, scol.data(), sizeof(int) * scol.size(), cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMalloc(&out->d_sval, sizeof(double) * sval.size()));
   SB2_CUDA_TRY(cudaMemcpy(out->d_sval, sval.data(), sizeof(double) * sval.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_pos, sizeof(long long) * pos.size()));
+  SB2_CUDA_TRY(cudaMemcpy(out->d_pos, pos.data(), sizeof(long long) * pos.size(), cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMalloc(&out->d_wrows, sizeof(int) * std::max<size_t>(wr.size(), 1)));
   if (!wr.empty()) SB2_CUDA_TRY(cudaMemcpy(out->d_wrows, wr.data(), sizeof(int) * wr.size(), cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMalloc(&out->d_crows, sizeof(int) * std::max<size_t>(cr.size(), 1)));
@@ -228,6 +232,7 @@ void free_sell(SellArrays* s) {
   cudaFree(s->d_sval32);
   cudaFree(s->d_wrows);
   cudaFree(s->d_crows);
+  cudaFree(s->d_pos);
   *s = SellArrays();
 }
 

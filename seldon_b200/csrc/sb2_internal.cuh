@@ -72,6 +72,8 @@ struct SellArrays {
   int* d_crows = nullptr;
   long long padded = 0;       // stored entries incl. padding
   bool sorted = false;
+  long long* d_pos = nullptr; // SELL position of each CSR entry of the thread
+                              // bin, -1 for entries of the warp/CTA bins
 };
 
 struct CsrArrays {
