@@ -7,9 +7,11 @@ throughput in algorithmic GB/s (nnz*(8+4) + 4*(n+1) + 8*n + 8*n bytes per
 SpMV); the inputs (217 MB) exceed the 126 MB L2.
 
 The same JSON line carries the time-to-solution figures of the path (CG on
-the 100^2 Laplacian, FP64 CG on the 192^3 Poisson problem, GMRES(30)+Jacobi
-on the 128^3 convection-diffusion problem, the Zipf SpMV) and the roofline,
-e2e, cpu_baseline and clock records.
+the 100^2 Laplacian; FP64 CG and FP32/FP64 iterative refinement on the 192^3
+Poisson problem; GMRES(30)+Jacobi on the 128^3 convection-diffusion problem;
+the Zipf SpMV; 4096 batched shifted Laplacians against a loop of FP64 CG
+calls; the adjoint solve on the 512^2 anisotropic graph Laplacian with its
+gradient checks) and the roofline, e2e, cpu_baseline and clock records.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -249,6 +251,9 @@ def run_ours(args, rank, world, local):
     nnz = ind.size
     A = api.RowSparse(n, n, ptr, ind, val)
     B = spmv_bytes(n, n, nnz)
+    # rows of at most 32 entries go to the SELL slice kernel, longer ones to
+    # the long-row kernel (a second launch)
+    launches_per_spmv = 1 + int(np.diff(ptr).max() > 32)
     x = torch.rand(n, dtype=torch.float64, device=dev)
     y = torch.zeros(n, dtype=torch.float64, device=dev)
 
@@ -347,11 +352,11 @@ def run_ours(args, rank, world, local):
             "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(kernel_gbs / peak, 4),
                          "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "sb2::spmv_kernel<256>"},
+                         "kernel": "sb2::sell_slices_kernel<256, true>"},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n, "ms_per_step": round(e2e_ms, 4),
                     "matches_device_result": bool(ok)},
-            "gpu_launches": args.steps * 2,
+            "gpu_launches": args.steps * launches_per_spmv,
             "timing": "K products captured in one CUDA graph, CUDA events around one replay",
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
@@ -406,14 +411,33 @@ def run_extras(api, matgen, torch, dev):
         it.HideMessages()
         api.Cg(A, X, b, api.Preconditioner_Base(), it)
         return it, X
+    cg_c3()  # warm: first call sets up the chained solver's state
     ms, (it, X) = timed(cg_c3)
-    fe = float(np.linalg.norm(X.cpu().numpy() - xs) / np.linalg.norm(xs))
+    X64 = X.cpu().numpy()
+    fe = float(np.linalg.norm(X64 - xs) / np.linalg.norm(xs))
     per_it = (spmv_bytes(n, n, ind.size) + 10 * 8 * n)
     out["cg_fp64_poisson192"] = {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
                                  "rel_residual": it.history[-1][1], "forward_error": fe,
                                  "gbs_per_iteration_model": round(
                                      per_it * it.GetNumberIteration() / (ms * 1e-3) / 1e9, 1)}
-    del A
+    # C3 mixed precision: FP32 inner CG, FP64 outer residual/update to 1e-10
+    for key, restarted, inner in (("ir_reliable_poisson192", False, 1e-2),
+                                  ("ir_restarted_poisson192", True, 1e-5)):
+        def ir():
+            Xi = torch.zeros(n, dtype=torch.float64, device=dev)
+            code, info = api.IterativeRefinement(A, Xi, b, tol=1e-10, inner_tol=inner,
+                                                 restarted=restarted)
+            return code, info, Xi
+        ir()
+        ms_ir, (code, info, Xi) = timed(ir)
+        Xi = Xi.cpu().numpy()
+        out[key] = {"ms": round(ms_ir, 2), "inner_tol": inner, "error_code": code,
+                    "outer_iter": info["outer_iter"], "inner_iter": info["inner_iter"],
+                    "rel_residual_fp64": info["rel_residual"],
+                    "forward_error_vs_fp64_cg": float(np.linalg.norm(Xi - X64) / np.linalg.norm(X64)),
+                    "forward_error_vs_xstar": float(np.linalg.norm(Xi - xs) / np.linalg.norm(xs)),
+                    "speedup_vs_fp64_cg": round(ms / ms_ir, 3)}
+    del A, X, X64
     # C2a GMRES(30) + Jacobi
     ptr, ind, val = matgen.convdiff3d(GRID)
     n = ptr.size - 1
@@ -444,6 +468,137 @@ def run_extras(api, matgen, torch, dev):
     Bz = spmv_bytes(n, n, ind.size)
     out["spmv_zipf_1e6"] = {"gbs": round(Bz / (ms / 20 * 1e-3) / 1e9, 1), "nnz": int(ind.size),
                             "us": round(ms / 20 * 1e3, 1)}
+    del A
+    out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed)
+    out["adjoint_aniso512"] = run_adjoint(matgen, torch, dev, timed)
+    return out
+
+
+def run_batch(api, matgen, torch, dev, timed, nsys=4096, sample_every=8):
+    """4096 shifted 2D Laplacians (side uniform in [8,140]) in one persistent
+    launch, against a loop of plain FP64 CG calls over every 8th system."""
+    from seldon_b200 import _lib
+    rng = np.random.default_rng(7)
+    gs = rng.integers(8, 141, nsys)
+    cache, systems, rhs = {}, [], []
+    for g in gs:
+        g = int(g)
+        if g not in cache:
+            cache[g] = matgen.lap2d(g, shift=0.01)
+        p, i, v = cache[g]
+        systems.append(cache[g])
+        rhs.append(matgen.matvec(p, i, v, rng.uniform(-1, 1, g * g)))
+    Bt = api.Batch(systems)
+    b = torch.as_tensor(np.concatenate(rhs), device=dev)
+    X = torch.zeros(Bt.m, dtype=torch.float64, device=dev)
+    its = torch.zeros(Bt.nsys, dtype=torch.int32, device=dev)
+    rr = torch.zeros(Bt.nsys, dtype=torch.float64, device=dev)
+    out = {"systems": nsys, "rows": Bt.m, "nnz": int(sum(s[1].size for s in systems)),
+           "tol": 1e-9, "autotuned_threads": Bt.autotune(X, b, tol=1e-9)}
+    for key, mixed in (("mixed", True), ("fp64", False)):
+        Bt.solve(X, b, its, rr, tol=1e-9, mixed=mixed)
+        ms, res = timed(lambda: Bt.solve(X, b, its, rr, tol=1e-9, mixed=mixed))
+        out[key] = {"ms": round(ms, 2), "systems_per_s": round(nsys / ms * 1e3, 1),
+                    "converged": res.converged, "max_iter": res.max_iter,
+                    "total_iter": res.total_iter, "max_rel_residual": res.max_rel_residual}
+    # graph-captured launch (no host synchronisation inside)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        Bt.solve(X, b, its, rr, summary=False, tol=1e-9, mixed=True)
+    g.replay()
+    ms, _ = timed(g.replay)
+    out["mixed_graph_ms"] = round(ms, 2)
+    tot, n_loop = 0.0, 0
+    for s in range(0, nsys, sample_every):
+        p, i, v = systems[s]
+        n = p.size - 1
+        A = api.RowSparse(n, n, p, i, v)
+        bs = torch.as_tensor(rhs[s], device=dev)
+        Xs = torch.zeros(n, dtype=torch.float64, device=dev)
+
+        def cg():
+            Xs.zero_()
+            itr = api.Iteration(10000, 1e-9)
+            itr.HideMessages()
+            api.Cg(A, Xs, bs, api.Preconditioner_Base(), itr)
+        cg()
+        ms, _ = timed(cg)
+        tot += ms
+        n_loop += 1
+    per = tot / n_loop
+    out["loop_fp64_cg"] = {"ms_per_system": round(per, 4), "systems_per_s": round(1e3 / per, 1),
+                           "sample": f"every {sample_every}th system ({n_loop} calls)",
+                           "est_ms_all": round(per * nsys, 1)}
+    out["speedup_mixed_vs_loop"] = round(out["loop_fp64_cg"]["est_ms_all"] / out["mixed"]["ms"], 1)
+    Bt.close()
+    return out
+
+
+def run_adjoint(matgen, torch, dev, timed, g=512, n_fd=64, h=1e-6):
+    """Adjoint CG on the 512^2 anisotropic graph Laplacian + 1e-3 I with
+    theta ~ LogNormal(0,1): forward and backward times, and the gradient
+    against an FP64 direct-solve gradient (all edges) and central differences
+    (h = 1e-6) on 64 random edges."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sl
+    from seldon_b200 import autograd as ag
+    rng = np.random.default_rng(11)
+    n = g * g
+    edges = matgen.grid_edges(g)
+    E = edges.shape[0]
+    theta0 = rng.lognormal(0.0, 1.0, E)
+    bh = rng.normal(size=n)
+    xt = rng.normal(size=n)
+    lap = ag.GraphLaplacian(n, edges, 1e-3)
+    XT = torch.as_tensor(xt, device=dev)
+    b = torch.as_tensor(bh, device=dev)
+    tol = 1e-12
+
+    def fwd_bwd():
+        th = torch.tensor(theta0, device=dev, requires_grad=True)
+        bb = b.clone().requires_grad_(True)
+        x = ag.graph_laplacian_solve(th, bb, lap, tol)
+        loss = 0.5 * ((x - XT) ** 2).sum()
+        return th, bb, x, loss
+    th, bb, x, loss = fwd_bwd()
+    loss.backward()
+    ms_f, (th, bb, x, loss) = timed(fwd_bwd)
+    ms_b, _ = timed(loss.backward)
+    gt = th.grad.cpu().numpy()
+    gb = bb.grad.cpu().numpy()
+    xg = x.detach()
+    # FP64 reference: sparse direct factorisation
+    p, i, v, _ = matgen.aniso2d(g, theta0, 1e-3)
+    lu = sl.splu(sp.csr_matrix((v, i, p), shape=(n, n)).tocsc())
+    xr = lu.solve(bh)
+    lr = lu.solve(xr - xt)
+    gr = -(lr[edges[:, 0]] - lr[edges[:, 1]]) * (xr[edges[:, 0]] - xr[edges[:, 1]])
+    out = {"n": n, "edges": E, "tol": tol, "ms_forward": round(ms_f, 2),
+           "ms_backward": round(ms_b, 2),
+           "grad_theta_err_vs_fp64_direct": float(np.abs(gt - gr).max() / np.abs(gr).max()),
+           "grad_b_err_vs_fp64_direct": float(np.abs(gb - lr).max() / np.abs(lr).max()),
+           "x_err_vs_fp64_direct": float(np.abs(xg.cpu().numpy() - xr).max() / np.abs(xr).max())}
+    # central differences: L(theta +- h e) - L(theta) from the perturbation
+    # dx, which solves (A +- h E_e) dx = -+ h E_e x (no cancellation in L)
+    res = xg - XT
+    worst = 0.0
+    for e in rng.choice(E, n_fd, replace=False):
+        a, c = (int(t) for t in edges[e])
+        d = float(xg[a] - xg[c])
+        dl = []
+        for sgn in (1.0, -1.0):
+            tp = torch.tensor(theta0, device=dev)
+            tp[e] += sgn * h
+            rhs = torch.zeros(n, dtype=torch.float64, device=dev)
+            rhs[a], rhs[c] = -sgn * h * d, sgn * h * d
+            with torch.no_grad():
+                dx = ag.graph_laplacian_solve(tp, rhs, lap, 1e-13)
+            dl.append(float(dx @ res) + 0.5 * float(dx @ dx))
+        fd = (dl[0] - dl[1]) / (2 * h)
+        worst = max(worst, abs(fd - gt[e]) / max(abs(gt[e]), 1e-300))
+    out["fd_edges"] = n_fd
+    out["fd_h"] = h
+    out["grad_theta_max_rel_err_vs_fd"] = worst
     return out
 
 
