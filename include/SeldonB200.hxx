@@ -1,0 +1,1290 @@
+// SeldonB200.hxx -- Seldon's sparse Krylov path on one B200 GPU.
+//
+// Include this header after Seldon's own (SeldonSolver.hxx, or Seldon.hxx
+// with the iterative solvers) and link libseldon_b200.so.  A Seldon program
+// moves its sparse system to the GPU by changing one template argument, the
+// allocator, to CudaAlloc<double>:
+//
+//   typedef Matrix<double, General, RowSparse, CudaAlloc<double> > GpuMatrix;
+//   typedef Vector<double, VectFull, CudaAlloc<double> > GpuVector;
+//   GpuMatrix A;  A.Copy(A_host);          // upload a Seldon host matrix
+//   GpuVector x(n), b;  Copy(b_host, b);   // host -> device
+//   Iteration<double> iter(1000, 1e-10);
+//   Preconditioner_Base M;
+//   Cg(A, x, b, M, iter);                  // fused persistent CG on the GPU
+//   Copy(x, x_host);                       // device -> host
+//
+// Everything below is an overload, a class specialisation or an allocator in
+// namespace Seldon that C++ partial ordering prefers over Seldon's generic
+// templates whenever the arguments are device types:
+//
+//   CudaAlloc<T>                              allocator concept of
+//                                             share/Allocator.hxx:31-48
+//   Vector<T, VectFull, CudaAlloc<T> >        vector/Vector.hxx:38-176
+//   Matrix<double, Prop, RowSparse, CudaAlloc<double> >
+//                                             matrix_sparse/Matrix_Sparse.hxx:42-195
+//   Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >
+//                                             matrix_sparse/Matrix_SymSparse.hxx:45-195
+//   Mlt / MltAdd (NoTrans and SeldonTrans)    Functions_MatVect.cxx:72-130,
+//                                             398-431, 526-564, 729-758, 915-927
+//   Mlt(alpha, X), Add, Copy, DotProd, DotProdConj, Norm2
+//                                             Functions_Vector.cxx:69-105,
+//                                             240-246, 330-397, 540-549
+//   SOR                                       Relaxation_MatVect.cxx:41-95, 176-298
+//   Cg / BiCgStab / Gmres                     Cg.cxx:45-116, BiCgStab.cxx:43-145,
+//                                             Gmres.cxx:44-183
+//   JacobiPreconditioner<T>                   (absent from Seldon) z_i = r_i / A(i,i)
+//
+// The solver overloads run the library's fused kernels when the
+// preconditioner is Preconditioner_Base, JacobiPreconditioner or
+// SorPreconditioner; with any other preconditioner class Seldon's own
+// generic driver runs on the device types, every vector operation of it on
+// the GPU.  The Iteration object is left in the state Seldon's driver leaves
+// it in (iteration count, factor, error code) and the residual lines it
+// prints are printed, from the device-side history, after the solve.
+//
+// Errors: a status from the library is thrown as a Seldon exception
+// (share/Errors.hxx): NoMemory for a failed device allocation, WrongDim for
+// inconsistent sizes or CSR arrays, WrongArgument for invalid arguments,
+// Error otherwise.
+//
+// Work is queued on the stream set by Seldon::b200::SetStream (default: the
+// legacy default stream); the scalar results (DotProd, Norm2, a solver's
+// return) and every copy that touches host memory wait for it.
+#ifndef SELDON_FILE_SELDON_B200_HXX
+#define SELDON_FILE_SELDON_B200_HXX
+
+#include <atomic>
+#include <cstdlib>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "seldon_b200.h"
+
+namespace Seldon
+{
+
+  namespace b200
+  {
+    inline void*& StreamSlot()
+    {
+      static thread_local void* s = 0;
+      return s;
+    }
+
+    //! Stream (a cudaStream_t) on which this thread's device work is queued.
+    inline void SetStream(void* stream) { StreamSlot() = stream; }
+    inline void* GetStream() { return StreamSlot(); }
+
+    //! Throws the Seldon exception matching a library status.
+    inline void Check(int status, const std::string& function)
+    {
+      if (status == SB2_OK)
+        return;
+      std::string what = sb2_status_string(status);
+      switch (status)
+        {
+        case SB2_ERR_NO_MEMORY:
+          throw NoMemory(function, what);
+        case SB2_ERR_INVALID_CSR:
+          throw WrongDim(function, what);
+        case SB2_ERR_INVALID_VALUE:
+          throw WrongArgument(function, what);
+        default:
+          throw Error(function, what);
+        }
+    }
+
+    inline unsigned long long NextSerial()
+    {
+      static std::atomic<unsigned long long> counter(0);
+      return ++counter;
+    }
+  }
+
+
+  /////////////////
+  // CUDA MEMORY //
+  /////////////////
+
+
+  //! Allocator of device memory (the allocator concept of Allocator.hxx).
+  /*! Device memory cannot be dereferenced on the host: the vector and matrix
+    specialisations below are the only containers meant to use it. */
+  template <class T>
+  class CudaAlloc
+  {
+  public:
+    typedef T value_type;
+    typedef T* pointer;
+    typedef const T* const_pointer;
+    typedef T& reference;
+    typedef const T& const_reference;
+
+    pointer allocate(int num, void* h = 0)
+    {
+      void* p = 0;
+      if (num > 0)
+        b200::Check(sb2_device_alloc(sizeof(T) * size_t(num), &p),
+                    "CudaAlloc::allocate");
+      return static_cast<pointer>(p);
+    }
+
+    void deallocate(pointer data, int num, void* h = 0)
+    {
+      sb2_device_free(data);
+    }
+
+    //! New buffer of num entries; the old contents are not kept.
+    void* reallocate(pointer data, int num, void* h = 0)
+    {
+      deallocate(data, num, h);
+      return allocate(num, h);
+    }
+
+    //! Sets num bytes to c.
+    void memoryset(pointer data, char c, size_t num)
+    {
+      if (num == 0)
+        return;
+      std::vector<char> buf(num, c);
+      b200::Check(sb2_memcpy(data, &buf[0], num, b200::GetStream()),
+                  "CudaAlloc::memoryset");
+    }
+
+    //! Copies num entries (device to device).
+    void memorycpy(pointer datat, pointer datas, size_t num)
+    {
+      b200::Check(sb2_memcpy(datat, datas, num * sizeof(T), b200::GetStream()),
+                  "CudaAlloc::memorycpy");
+    }
+  };
+
+
+  namespace b200
+  {
+    template <class T>
+    inline void FillValue(T* data, int n, const T& x)
+    {
+      if (n <= 0)
+        return;
+      std::vector<T> h(n, x);
+      Check(sb2_memcpy(data, &h[0], sizeof(T) * size_t(n), GetStream()),
+            "Vector::Fill");
+    }
+
+    inline void FillValue(double* data, int n, const double& x)
+    {
+      if (n > 0)
+        Check(sb2_fill(n, x, data, GetStream()), "Vector::Fill");
+    }
+  }
+
+
+  //////////////////////////
+  // VECTOR ON THE DEVICE //
+  //////////////////////////
+
+
+  //! Dense vector whose entries live in device memory.
+  /*! Same interface as Vector<T, VectFull, Allocator> (Vector.hxx:38-176)
+    except element references: operator() returns the value, read from the
+    device (one synchronous copy per call). */
+  template <class T>
+  class Vector<T, VectFull, CudaAlloc<T> >: public Vector_Base<T, CudaAlloc<T> >
+  {
+  public:
+    typedef T value_type;
+    typedef T* pointer;
+    typedef const T* const_pointer;
+    typedef T& reference;
+    typedef const T& const_reference;
+    typedef VectFull storage;
+
+  private:
+    typedef Vector_Base<T, CudaAlloc<T> > base;
+
+  public:
+    explicit Vector(): base() {}
+
+    //! Allocates i entries (not initialised), as Seldon does.
+    explicit Vector(int i): base(i)
+    {
+      this->data_ = this->vect_allocator_.allocate(i, this);
+    }
+
+    //! Takes ownership of a device buffer of i entries.
+    Vector(int i, pointer data): base()
+    {
+      this->m_ = i;
+      this->data_ = data;
+    }
+
+    Vector(const Vector<T, VectFull, CudaAlloc<T> >& X): base()
+    {
+      Copy(X);
+    }
+
+    ~Vector() {}
+
+    void Clear()
+    {
+      if (this->data_ != NULL)
+        this->vect_allocator_.deallocate(this->data_, this->m_);
+      this->data_ = NULL;
+      this->m_ = 0;
+    }
+
+    void Reallocate(int i)
+    {
+      if (i == this->m_)
+        return;
+      Clear();
+      this->data_ = this->vect_allocator_.allocate(i, this);
+      this->m_ = i;
+    }
+
+    //! Changes the length and keeps the first min(old, new) entries.
+    void Resize(int i)
+    {
+      if (i == this->m_)
+        return;
+      pointer d = this->vect_allocator_.allocate(i, this);
+      int keep = i < this->m_ ? i : this->m_;
+      if (keep > 0)
+        b200::Check(sb2_memcpy(d, this->data_, sizeof(T) * size_t(keep),
+                               b200::GetStream()), "Vector::Resize");
+      Clear();
+      this->data_ = d;
+      this->m_ = i;
+    }
+
+    //! Takes ownership of a device buffer of i entries.
+    void SetData(int i, pointer data)
+    {
+      Clear();
+      this->m_ = i;
+      this->data_ = data;
+    }
+
+    //! Shares the buffer of V (call Nullify before either is destroyed).
+    void SetData(const Vector<T, VectFull, CudaAlloc<T> >& V)
+    {
+      SetData(V.GetM(), V.GetData());
+    }
+
+    void Nullify()
+    {
+      this->m_ = 0;
+      this->data_ = NULL;
+    }
+
+    //! Entry i, read from the device.
+    value_type operator() (int i) const
+    {
+      T v;
+      b200::Check(sb2_memcpy(&v, this->data_ + i, sizeof(T), b200::GetStream()),
+                  "Vector::operator()");
+      return v;
+    }
+
+    value_type Get(int i) const
+    {
+      return (*this)(i);
+    }
+
+    Vector<T, VectFull, CudaAlloc<T> >&
+    operator= (const Vector<T, VectFull, CudaAlloc<T> >& X)
+    {
+      Copy(X);
+      return *this;
+    }
+
+    void Copy(const Vector<T, VectFull, CudaAlloc<T> >& X)
+    {
+      if (&X == this)
+        return;
+      Reallocate(X.GetM());
+      if (this->m_ > 0)
+        b200::Check(sb2_memcpy(this->data_, X.GetData(),
+                               sizeof(T) * size_t(this->m_), b200::GetStream()),
+                    "Vector::Copy");
+    }
+
+    Vector<T, VectFull, CudaAlloc<T> > Copy() const
+    {
+      return Vector<T, VectFull, CudaAlloc<T> >(*this);
+    }
+
+    int GetDataSize() const
+    {
+      return this->m_;
+    }
+
+    void Zero()
+    {
+      b200::FillValue(this->data_, this->m_, T(0));
+    }
+
+    //! Entry i set to i (Vector.cxx Fill()).
+    void Fill()
+    {
+      if (this->m_ <= 0)
+        return;
+      std::vector<T> h(this->m_);
+      for (int i = 0; i < this->m_; i++)
+        h[i] = T(i);
+      b200::Check(sb2_memcpy(this->data_, &h[0], sizeof(T) * size_t(this->m_),
+                             b200::GetStream()), "Vector::Fill");
+    }
+
+    template <class T0>
+    void Fill(const T0& x)
+    {
+      b200::FillValue(this->data_, this->m_, T(x));
+    }
+
+    template <class T0>
+    Vector<T, VectFull, CudaAlloc<T> >& operator= (const T0& x)
+    {
+      Fill(x);
+      return *this;
+    }
+
+    template <class T0>
+    Vector<T, VectFull, CudaAlloc<T> >& operator*= (const T0& alpha)
+    {
+      Mlt(alpha, *this);
+      return *this;
+    }
+
+    //! Prints the entries (read back from the device) as Vector::Print does.
+    void Print() const
+    {
+      std::vector<T> h(this->m_);
+      if (this->m_ > 0)
+        b200::Check(sb2_memcpy(&h[0], this->data_, sizeof(T) * size_t(this->m_),
+                               b200::GetStream()), "Vector::Print");
+      for (int i = 0; i < this->m_; i++)
+        std::cout << h[i] << '\t';
+      std::cout << std::endl;
+    }
+  };
+
+
+  ////////////////////////////
+  // MATRICES ON THE DEVICE //
+  ////////////////////////////
+
+
+  namespace b200
+  {
+    //! Device CSR matrix behind the RowSparse and RowSymSparse
+    //! specialisations: an opaque library handle that owns device copies
+    //! of ptr_/ind_/data_ (and the SpMV layouts built from them).
+    template <int Symmetric>
+    class DeviceCsr: public Matrix_Base<double, CudaAlloc<double> >
+    {
+    protected:
+      sb2_csr* h_;
+      int nz_;
+      unsigned long long serial_;
+
+    public:
+      DeviceCsr(): h_(0), nz_(0), serial_(0)
+      {
+        this->m_ = 0;
+        this->n_ = 0;
+        this->data_ = NULL;
+      }
+
+      DeviceCsr(const DeviceCsr& A): h_(0), nz_(0), serial_(0)
+      {
+        this->m_ = 0;
+        this->n_ = 0;
+        this->data_ = NULL;
+        CopyDevice(A);
+      }
+
+      ~DeviceCsr()
+      {
+        if (h_)
+          sb2_csr_destroy(h_);
+      }
+
+      DeviceCsr& operator= (const DeviceCsr& A)
+      {
+        CopyDevice(A);
+        return *this;
+      }
+
+      //! Builds the device matrix from host CSR arrays (copied, not kept).
+      void Create(int i, int j, int nz, const int* ptr, const int* ind,
+                  const double* val)
+      {
+        std::vector<int> zero_ptr;
+        if (ptr == NULL)
+          {
+            zero_ptr.assign(i + 1, 0);
+            ptr = &zero_ptr[0];
+          }
+        sb2_csr* h = 0;
+        Check(sb2_csr_create(i, j, nz, ptr, ind, val, Symmetric, 1, &h),
+              "Matrix::SetData");
+        if (h_)
+          sb2_csr_destroy(h_);
+        h_ = h;
+        this->m_ = i;
+        this->n_ = j;
+        nz_ = nz;
+        serial_ = NextSerial();
+      }
+
+      //! i x j matrix without entries (Matrix_Sparse(i, j)).
+      void Reallocate(int i, int j)
+      {
+        Create(i, j, 0, NULL, NULL, NULL);
+      }
+
+      //! Takes the host vectors' contents and leaves them empty, as
+      //! Matrix_Sparse::SetData does (Matrix_Sparse.cxx:305-415).
+      template <class Storage0, class Allocator0, class Storage1,
+                class Allocator1, class Storage2, class Allocator2>
+      void SetData(int i, int j, Vector<double, Storage0, Allocator0>& values,
+                   Vector<int, Storage1, Allocator1>& ptr,
+                   Vector<int, Storage2, Allocator2>& ind)
+      {
+        if (ptr.GetM() != i + 1)
+          throw WrongDim("Matrix::SetData", "ptr must have i+1 entries");
+        if (ind.GetM() != values.GetM())
+          throw WrongDim("Matrix::SetData", "ind and values sizes differ");
+        Create(i, j, values.GetM(), ptr.GetData(), ind.GetData(),
+               values.GetData());
+        values.Clear();
+        ptr.Clear();
+        ind.Clear();
+      }
+
+      //! Takes host arrays allocated with malloc/calloc (Seldon's default
+      //! allocators): they are copied to the device and freed.
+      void SetData(int i, int j, int nz, double* values, int* ptr, int* ind)
+      {
+        Create(i, j, nz, ptr, ind, values);
+        free(values);
+        free(ptr);
+        free(ind);
+      }
+
+      void Clear()
+      {
+        if (h_)
+          sb2_csr_destroy(h_);
+        h_ = 0;
+        nz_ = 0;
+        this->m_ = 0;
+        this->n_ = 0;
+        serial_ = NextSerial();
+      }
+
+      //! Stored entries (the upper triangle for RowSymSparse).
+      int GetNonZeros() const { return nz_; }
+      int GetDataSize() const { return nz_; }
+
+      //! Library handle (for the C ABI of seldon_b200.h).
+      sb2_csr* GetHandle() const
+      {
+        if (!h_)
+          throw WrongArgument("Matrix::GetHandle", "matrix not initialised");
+        return h_;
+      }
+
+      //! Changes every time the device matrix is rebuilt.
+      unsigned long long GetSerial() const { return serial_; }
+
+      //! Host copies of the stored arrays.
+      void Download(std::vector<int>& ptr, std::vector<int>& ind,
+                    std::vector<double>& val) const
+      {
+        ptr.assign(this->m_ + 1, 0);
+        ind.resize(nz_);
+        val.resize(nz_);
+        if (!h_)
+          return;
+        Check(sb2_csr_download(h_, &ptr[0], nz_ ? &ind[0] : NULL,
+                               nz_ ? &val[0] : NULL), "Matrix::Download");
+      }
+
+    protected:
+      void CopyDevice(const DeviceCsr& A)
+      {
+        if (&A == this)
+          return;
+        if (!A.h_)
+          {
+            Clear();
+            return;
+          }
+        std::vector<int> p, i;
+        std::vector<double> v;
+        A.Download(p, i, v);
+        Create(A.GetM(), A.GetN(), A.nz_, &p[0], i.empty() ? NULL : &i[0],
+               v.empty() ? NULL : &v[0]);
+      }
+
+      template <class MatrixHost>
+      void UploadFrom(const MatrixHost& A)
+      {
+        Create(A.GetM(), A.GetN(), A.GetNonZeros(), A.GetPtr(), A.GetInd(),
+               A.GetData());
+      }
+
+      template <class MatrixHost>
+      void DownloadTo(MatrixHost& A) const
+      {
+        std::vector<int> p, i;
+        std::vector<double> v;
+        Download(p, i, v);
+        Vector<double> values(nz_);
+        Vector<int> ptr(this->m_ + 1), ind(nz_);
+        for (int k = 0; k < nz_; k++)
+          {
+            values(k) = v[k];
+            ind(k) = i[k];
+          }
+        for (int k = 0; k <= this->m_; k++)
+          ptr(k) = p[k];
+        A.SetData(this->m_, this->n_, values, ptr, ind);
+      }
+    };
+  }
+
+
+  //! General CSR matrix in device memory (Matrix<T, Prop, RowSparse>).
+  template <class Prop>
+  class Matrix<double, Prop, RowSparse, CudaAlloc<double> >:
+    public b200::DeviceCsr<0>
+  {
+  public:
+    typedef double value_type;
+    typedef Prop property;
+    typedef RowSparse storage;
+    typedef CudaAlloc<double> allocator;
+
+    Matrix() {}
+
+    Matrix(int i, int j)
+    {
+      this->Reallocate(i, j);
+    }
+
+    template <class Storage0, class Allocator0, class Storage1,
+              class Allocator1, class Storage2, class Allocator2>
+    Matrix(int i, int j, Vector<double, Storage0, Allocator0>& values,
+           Vector<int, Storage1, Allocator1>& ptr,
+           Vector<int, Storage2, Allocator2>& ind)
+    {
+      this->SetData(i, j, values, ptr, ind);
+    }
+
+    //! Device-to-device copy.
+    void Copy(const Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A)
+    {
+      this->CopyDevice(A);
+    }
+
+    //! Upload of a Seldon host matrix (its arrays are left as they are).
+    template <class Prop0, class Allocator0>
+    void Copy(const Matrix<double, Prop0, RowSparse, Allocator0>& A)
+    {
+      this->UploadFrom(A);
+    }
+
+    //! Download into a Seldon host matrix.
+    template <class Prop0, class Allocator0>
+    void CopyToHost(Matrix<double, Prop0, RowSparse, Allocator0>& A) const
+    {
+      this->DownloadTo(A);
+    }
+  };
+
+
+  //! Symmetric matrix in device memory, upper triangle stored
+  //! (Matrix<T, Prop, RowSymSparse>).
+  template <class Prop>
+  class Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >:
+    public b200::DeviceCsr<1>
+  {
+  public:
+    typedef double value_type;
+    typedef Prop property;
+    typedef RowSymSparse storage;
+    typedef CudaAlloc<double> allocator;
+
+    Matrix() {}
+
+    Matrix(int i, int j)
+    {
+      this->Reallocate(i, j);
+    }
+
+    template <class Storage0, class Allocator0, class Storage1,
+              class Allocator1, class Storage2, class Allocator2>
+    Matrix(int i, int j, Vector<double, Storage0, Allocator0>& values,
+           Vector<int, Storage1, Allocator1>& ptr,
+           Vector<int, Storage2, Allocator2>& ind)
+    {
+      this->SetData(i, j, values, ptr, ind);
+    }
+
+    void Copy(const Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A)
+    {
+      this->CopyDevice(A);
+    }
+
+    template <class Prop0, class Allocator0>
+    void Copy(const Matrix<double, Prop0, RowSymSparse, Allocator0>& A)
+    {
+      this->UploadFrom(A);
+    }
+
+    template <class Prop0, class Allocator0>
+    void CopyToHost(Matrix<double, Prop0, RowSymSparse, Allocator0>& A) const
+    {
+      this->DownloadTo(A);
+    }
+  };
+
+
+  ////////////
+  // BLAS-1 //
+  ////////////
+
+
+  //! X = alpha X (Functions_Vector.cxx:69-74).
+  template <class T0>
+  void Mlt(const T0& alpha, Vector<double, VectFull, CudaAlloc<double> >& X)
+  {
+    b200::Check(sb2_scal(X.GetM(), double(alpha), X.GetData(), b200::GetStream()),
+                "Mlt(alpha, X)");
+  }
+
+  //! Y = Y + alpha X; nothing when alpha is zero (Functions_Vector.cxx:85-105).
+  template <class T0>
+  void Add(const T0& alpha, const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    if (double(alpha) == 0.0)
+      return;
+    if (X.GetM() != Y.GetM())
+      throw WrongDim("Add(alpha, X, Y)", "X and Y sizes differ");
+    b200::Check(sb2_axpy(X.GetM(), double(alpha), X.GetData(), Y.GetData(),
+                         b200::GetStream()), "Add(alpha, X, Y)");
+  }
+
+  //! Y = X, Y resized (Functions_Vector.cxx:240-246).
+  inline void Copy(const Vector<double, VectFull, CudaAlloc<double> >& X,
+                   Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    Y.Copy(X);
+  }
+
+  //! Host vector to device vector.
+  template <class Allocator0>
+  void Copy(const Vector<double, VectFull, Allocator0>& X,
+            Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    Y.Reallocate(X.GetM());
+    if (X.GetM() > 0)
+      b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(double) * size_t(X.GetM()),
+                             b200::GetStream()), "Copy(host, device)");
+  }
+
+  //! Device vector to host vector.
+  template <class Allocator0>
+  void Copy(const Vector<double, VectFull, CudaAlloc<double> >& X,
+            Vector<double, VectFull, Allocator0>& Y)
+  {
+    Y.Reallocate(X.GetM());
+    if (X.GetM() > 0)
+      b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(double) * size_t(X.GetM()),
+                             b200::GetStream()), "Copy(device, host)");
+  }
+
+  //! Sum of X_i Y_i (Functions_Vector.cxx:330-346), deterministic order.
+  inline double DotProd(const Vector<double, VectFull, CudaAlloc<double> >& X,
+                        const Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    if (X.GetM() != Y.GetM())
+      throw WrongDim("DotProd(X, Y)", "X and Y sizes differ");
+    double r = 0.0;
+    b200::Check(sb2_dot(X.GetM(), X.GetData(), Y.GetData(), &r, b200::GetStream()),
+                "DotProd(X, Y)");
+    return r;
+  }
+
+  //! Real vectors: DotProdConj is DotProd (Functions_Vector.cxx:391-397).
+  inline double DotProdConj(const Vector<double, VectFull, CudaAlloc<double> >& X,
+                            const Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    return DotProd(X, Y);
+  }
+
+  //! Unscaled 2-norm sqrt(sum X_i^2) (Functions_Vector.cxx:540-549).
+  inline double Norm2(const Vector<double, VectFull, CudaAlloc<double> >& X)
+  {
+    double r = 0.0;
+    b200::Check(sb2_nrm2(X.GetM(), X.GetData(), &r, b200::GetStream()), "Norm2(X)");
+    return r;
+  }
+
+
+  ////////////
+  // SPMV   //
+  ////////////
+
+
+  namespace b200
+  {
+    template <class MatrixD>
+    void SpMV(const MatrixD& M, int trans, double alpha,
+              const Vector<double, VectFull, CudaAlloc<double> >& X, double beta,
+              Vector<double, VectFull, CudaAlloc<double> >& Y, bool overwrite)
+    {
+      const int nx = trans ? M.GetM() : M.GetN();
+      const int ny = trans ? M.GetN() : M.GetM();
+      if (X.GetM() != nx || Y.GetM() != ny)
+        throw WrongDim("MltAdd(alpha, M, X, beta, Y)",
+                       "vector sizes do not match the matrix");
+      if (overwrite)
+        Check(sb2_mlt(M.GetHandle(), trans, alpha, X.GetData(), Y.GetData(),
+                      GetStream()), "Mlt(M, X, Y)");
+      else
+        Check(sb2_spmv(M.GetHandle(), trans, alpha, X.GetData(), beta,
+                       Y.GetData(), GetStream()), "MltAdd(alpha, M, X, beta, Y)");
+    }
+  }
+
+
+  //! Y = beta Y + alpha M X (Functions_MatVect.cxx:398-431).
+  template <class T0, class Prop1, class T3>
+  void MltAdd(const T0 alpha,
+              const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& M,
+              const Vector<double, VectFull, CudaAlloc<double> >& X,
+              const T3 beta, Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, double(alpha), X, double(beta), Y, false);
+  }
+
+  //! Symmetric, upper triangle stored (Functions_MatVect.cxx:526-564).
+  template <class T0, class Prop1, class T3>
+  void MltAdd(const T0 alpha,
+              const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& M,
+              const Vector<double, VectFull, CudaAlloc<double> >& X,
+              const T3 beta, Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, double(alpha), X, double(beta), Y, false);
+  }
+
+  //! Y = beta Y + alpha op(M) X (Functions_MatVect.cxx:729-758, 915-927).
+  //! One overload per transposition flag class, as Seldon declares them
+  //! (Functions_MatVect.hxx:230-350), so that these are the exact matches.
+#define SELDON_B200_MLTADD_TRANS(FLAG, STORAGE)                                \
+  template <class T0, class Prop1, class T3>                                    \
+  void MltAdd(const T0 alpha, const FLAG& Trans,                                \
+              const Matrix<double, Prop1, STORAGE, CudaAlloc<double> >& M,      \
+              const Vector<double, VectFull, CudaAlloc<double> >& X,            \
+              const T3 beta, Vector<double, VectFull, CudaAlloc<double> >& Y)   \
+  {                                                                             \
+    b200::SpMV(M, Trans.NoTrans() ? 0 : 1, double(alpha), X, double(beta), Y,  \
+               false);                                                          \
+  }
+
+  SELDON_B200_MLTADD_TRANS(SeldonTranspose, RowSparse)
+  SELDON_B200_MLTADD_TRANS(SeldonTranspose, RowSymSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonNoTrans, RowSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonNoTrans, RowSymSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonTrans, RowSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonTrans, RowSymSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonConjTrans, RowSparse)
+  SELDON_B200_MLTADD_TRANS(class_SeldonConjTrans, RowSymSparse)
+
+#undef SELDON_B200_MLTADD_TRANS
+
+  //! Y = M X (Functions_MatVect.cxx:72-83: Y.Fill(0), then MltAdd).
+  template <class Prop1>
+  void Mlt(const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, 1.0, X, 0.0, Y, true);
+  }
+
+  template <class Prop1>
+  void Mlt(const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, 1.0, X, 0.0, Y, true);
+  }
+
+  //! Y = alpha M X (Functions_MatVect.cxx:98-109).
+  template <class Prop1>
+  void Mlt(const double& alpha,
+           const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, alpha, X, 0.0, Y, true);
+  }
+
+  template <class Prop1>
+  void Mlt(const double& alpha,
+           const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, 0, alpha, X, 0.0, Y, true);
+  }
+
+  //! Y = op(M) X (Functions_MatVect.cxx:121-130).
+  template <class Prop1>
+  void Mlt(const SeldonTranspose& Trans,
+           const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, Trans.NoTrans() ? 0 : 1, 1.0, X, 0.0, Y, true);
+  }
+
+  template <class Prop1>
+  void Mlt(const SeldonTranspose& Trans,
+           const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& M,
+           const Vector<double, VectFull, CudaAlloc<double> >& X,
+           Vector<double, VectFull, CudaAlloc<double> >& Y)
+  {
+    b200::SpMV(M, Trans.NoTrans() ? 0 : 1, 1.0, X, 0.0, Y, true);
+  }
+
+
+  /////////
+  // SOR //
+  /////////
+
+
+  //! Sweeps of (S)SOR on A X = B, bit-identical to the sequential sweeps
+  //! (Relaxation_MatVect.cxx:41-95).  type_ssor: 0 symmetric, 2 forward,
+  //! 3 backward.
+  template <class Prop0, class T3>
+  void SOR(const Matrix<double, Prop0, RowSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& X,
+           const Vector<double, VectFull, CudaAlloc<double> >& B,
+           const T3& omega, int iter, int type_ssor = 2)
+  {
+    b200::Check(sb2_sor(A.GetHandle(), X.GetData(), B.GetData(), double(omega), iter,
+                        type_ssor, b200::GetStream()), "SOR");
+  }
+
+  //! Symmetric storage (Relaxation_MatVect.cxx:176-298).
+  template <class Prop0, class T3>
+  void SOR(const Matrix<double, Prop0, RowSymSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& X,
+           const Vector<double, VectFull, CudaAlloc<double> >& B,
+           const T3& omega, int iter, int type_ssor = 2)
+  {
+    b200::Check(sb2_sor(A.GetHandle(), X.GetData(), B.GetData(), double(omega), iter,
+                        type_ssor, b200::GetStream()), "SOR");
+  }
+
+
+  ////////////////////
+  // PRECONDITIONERS //
+  ////////////////////
+
+
+  //! Jacobi preconditioner z_i = r_i / A(i,i) (absent from Seldon; same
+  //! Solve/TransSolve interface as Preconditioner_Base, Iterative.hxx:24-39).
+  /*! The diagonal is looked up as Matrix_Sparse::operator()(i, i) does: the
+    first stored entry of row i with column i; a row without one gives a
+    division by zero.  Usable with host matrices (Seldon's element access)
+    and with device matrices (library kernel, diagonal cached per matrix). */
+  template <class T>
+  class JacobiPreconditioner
+  {
+    sb2_precond* h_;
+    unsigned long long serial_;
+
+  public:
+    JacobiPreconditioner(): h_(0), serial_(0) {}
+    JacobiPreconditioner(const JacobiPreconditioner&): h_(0), serial_(0) {}
+    JacobiPreconditioner& operator= (const JacobiPreconditioner&)
+    {
+      Release();
+      return *this;
+    }
+    ~JacobiPreconditioner() { Release(); }
+
+    void Release()
+    {
+      if (h_)
+        sb2_precond_destroy(h_);
+      h_ = 0;
+      serial_ = 0;
+    }
+
+    //! Library handle for device matrix A (created once per matrix).
+    template <class MatrixD>
+    const sb2_precond* GetHandle(const MatrixD& A)
+    {
+      if (!h_ || serial_ != A.GetSerial())
+        {
+          Release();
+          b200::Check(sb2_precond_create(A.GetHandle(), SB2_PRECOND_JACOBI, 1.0, 1,
+                                         1, &h_), "JacobiPreconditioner");
+          serial_ = A.GetSerial();
+        }
+      return h_;
+    }
+
+    //! Host matrices and vectors: z_i = r_i / A(i,i).
+    template <class Matrix1, class Vector1>
+    void Solve(const Matrix1& A, const Vector1& r, Vector1& z)
+    {
+      for (int i = 0; i < r.GetM(); i++)
+        z(i) = r(i) / A(i, i);
+    }
+
+    template <class Matrix1, class Vector1>
+    void TransSolve(const Matrix1& A, const Vector1& r, Vector1& z)
+    {
+      Solve(A, r, z);
+    }
+
+    template <class Prop1>
+    void Solve(const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& A,
+               const Vector<double, VectFull, CudaAlloc<double> >& r,
+               Vector<double, VectFull, CudaAlloc<double> >& z)
+    {
+      DeviceSolve(A, r, z);
+    }
+
+    template <class Prop1>
+    void Solve(const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& A,
+               const Vector<double, VectFull, CudaAlloc<double> >& r,
+               Vector<double, VectFull, CudaAlloc<double> >& z)
+    {
+      DeviceSolve(A, r, z);
+    }
+
+    template <class Prop1>
+    void TransSolve(const Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& A,
+                    const Vector<double, VectFull, CudaAlloc<double> >& r,
+                    Vector<double, VectFull, CudaAlloc<double> >& z)
+    {
+      DeviceSolve(A, r, z);
+    }
+
+    template <class Prop1>
+    void TransSolve(const Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& A,
+                    const Vector<double, VectFull, CudaAlloc<double> >& r,
+                    Vector<double, VectFull, CudaAlloc<double> >& z)
+    {
+      DeviceSolve(A, r, z);
+    }
+
+  private:
+    template <class MatrixD>
+    void DeviceSolve(const MatrixD& A,
+                     const Vector<double, VectFull, CudaAlloc<double> >& r,
+                     Vector<double, VectFull, CudaAlloc<double> >& z)
+    {
+      b200::Check(sb2_precond_solve(GetHandle(A), r.GetData(), z.GetData(),
+                                    b200::GetStream()), "JacobiPreconditioner::Solve");
+    }
+  };
+
+
+  /////////////
+  // SOLVERS //
+  /////////////
+
+
+  namespace b200
+  {
+    //! Reads and writes the protected state of Iteration<Titer>
+    //! (Iterative.hxx:47-108) that its public interface does not expose.
+    template <class Titer>
+    struct IterationState: public Iteration<Titer>
+    {
+      static int MaxIter(const Iteration<Titer>& it)
+      {
+        return it.*(&IterationState::max_iter);
+      }
+      static int PrintLevel(const Iteration<Titer>& it)
+      {
+        return it.*(&IterationState::print_level);
+      }
+      static void SetFactor(Iteration<Titer>& it, Titer f)
+      {
+        it.*(&IterationState::facteur_reste) = f;
+      }
+    };
+
+    //! Reads the parameters of Seldon's SorPreconditioner (Precond_Ssor.cxx:24-90).
+    template <class T>
+    struct SorState: public SorPreconditioner<T>
+    {
+      static bool Symmetric(const SorPreconditioner<T>& M)
+      {
+        return M.*(&SorState::symmetric_precond);
+      }
+      static int NbIter(const SorPreconditioner<T>& M)
+      {
+        return M.*(&SorState::nb_iter);
+      }
+      static T Omega(const SorPreconditioner<T>& M)
+      {
+        return M.*(&SorState::omega);
+      }
+    };
+
+    //! Device handle of a preconditioner, released at scope exit.
+    struct PrecondHandle
+    {
+      sb2_precond* owned;
+      const sb2_precond* use;
+      PrecondHandle(): owned(0), use(0) {}
+      ~PrecondHandle()
+      {
+        if (owned)
+          sb2_precond_destroy(owned);
+      }
+    };
+
+    //! Preconditioners the fused solvers run natively.
+    template <class P>
+    struct PrecondTraits
+    {
+      static const bool native = false;
+      template <class MatrixD>
+      static void Acquire(P&, const MatrixD&, PrecondHandle&) {}
+    };
+
+    template <>
+    struct PrecondTraits<Preconditioner_Base>
+    {
+      static const bool native = true;
+      template <class MatrixD>
+      static void Acquire(Preconditioner_Base&, const MatrixD&, PrecondHandle&) {}
+    };
+
+    template <class T>
+    struct PrecondTraits<JacobiPreconditioner<T> >
+    {
+      static const bool native = true;
+      template <class MatrixD>
+      static void Acquire(JacobiPreconditioner<T>& M, const MatrixD& A,
+                          PrecondHandle& h)
+      {
+        h.use = M.GetHandle(A);
+      }
+    };
+
+    template <class T>
+    struct PrecondTraits<SorPreconditioner<T> >
+    {
+      static const bool native = true;
+      template <class MatrixD>
+      static void Acquire(SorPreconditioner<T>& M, const MatrixD& A,
+                          PrecondHandle& h)
+      {
+        Check(sb2_precond_create(A.GetHandle(), SB2_PRECOND_SOR,
+                                 double(SorState<T>::Omega(M)),
+                                 SorState<T>::NbIter(M),
+                                 SorState<T>::Symmetric(M) ? 1 : 0, &h.owned),
+              "SorPreconditioner");
+        h.use = h.owned;
+      }
+    };
+
+    enum SolverKind { kCg, kBiCgStab, kGmres };
+
+    inline const char* BreakdownMessage(SolverKind kind, int code)
+    {
+      // the strings Cg.cxx:82,101 and BiCgStab.cxx:77,87,107 pass to Fail
+      if (kind == kCg)
+        return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
+      if (code == 1)
+        return "Bicgstab breakdown #1";
+      return code == 2 ? "Bicgstab breakdown #2" : "Bicgstab breakdown #3";
+    }
+
+    //! Runs one fused solver and leaves `iter` as Seldon's driver would.
+    template <class Titer, class MatrixD, class P>
+    int RunSolver(SolverKind kind, MatrixD& A,
+                  Vector<double, VectFull, CudaAlloc<double> >& x,
+                  const Vector<double, VectFull, CudaAlloc<double> >& b,
+                  P& M, Iteration<Titer>& iter)
+    {
+      const int N = A.GetM();
+      if (N <= 0)
+        return 0;
+      if (x.GetM() != N || b.GetM() != N)
+        throw WrongDim("Iterative solver", "x and b must have A.GetM() entries");
+      PrecondHandle ph;
+      PrecondTraits<P>::Acquire(M, A, ph);
+      sb2_iter_params prm;
+      prm.tol = double(iter.GetTolerance());
+      prm.max_iter = IterationState<Titer>::MaxIter(iter);
+      prm.restart = iter.GetRestart();
+      prm.print_level = IterationState<Titer>::PrintLevel(iter);
+      prm.init_guess_null = iter.IsInitGuess_Null() ? 1 : 0;
+      int cap = 0;
+      std::vector<double> hist;
+      std::vector<int> hist_it;
+      if (prm.print_level >= 1)
+        {
+          cap = 2 * (prm.max_iter > 0 ? prm.max_iter : 0) + 8;
+          hist.resize(cap);
+          hist_it.resize(cap);
+        }
+      sb2_iter_result res;
+      int st;
+      if (kind == kCg)
+        st = sb2_cg(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                    cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kBiCgStab)
+        st = sb2_bicgstab(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                          cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
+                          GetStream());
+      else
+        st = sb2_gmres(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                       cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
+                       GetStream());
+      Check(st, kind == kCg ? "Cg" : (kind == kBiCgStab ? "BiCgStab" : "Gmres"));
+      // Init() found a zero right-hand side: Seldon returns at once
+      if (res.init_failed)
+        return iter.ErrorCode();
+      IterationState<Titer>::SetFactor(iter, Titer(res.facteur_reste));
+      // the lines Iteration::Finished prints (Iterative.cxx:282-287)
+      for (int k = 0; k < res.hist_len && k < cap; k++)
+        {
+          const int it = hist_it[k];
+          if ((prm.print_level >= 1 && it % 100 == 0) || prm.print_level >= 6)
+            std::cout << "Residu at iteration number " << it << "  "
+                      << Titer(hist[k]) << std::endl;
+        }
+      iter.SetNumberIteration(res.nb_iter);
+      if (res.error_code > 0)
+        iter.Fail(res.error_code, BreakdownMessage(kind, res.error_code));
+      return iter.ErrorCode();
+    }
+  }
+
+
+  namespace b200
+  {
+    //! Fused kernels for the preconditioners of PrecondTraits; Seldon's
+    //! generic driver (on the device types) for any other class.
+    template <bool native>
+    struct Dispatch
+    {
+      template <class Titer, class MatrixD, class P>
+      static int Run(SolverKind kind, MatrixD& A,
+                     Vector<double, VectFull, CudaAlloc<double> >& x,
+                     const Vector<double, VectFull, CudaAlloc<double> >& b,
+                     P& M, Iteration<Titer>& iter)
+      {
+        return RunSolver(kind, A, x, b, M, iter);
+      }
+    };
+
+    template <>
+    struct Dispatch<false>
+    {
+      template <class Titer, class MatrixD, class P>
+      static int Run(SolverKind kind, MatrixD& A,
+                     Vector<double, VectFull, CudaAlloc<double> >& x,
+                     const Vector<double, VectFull, CudaAlloc<double> >& b,
+                     P& M, Iteration<Titer>& iter)
+      {
+        typedef Vector<double, VectFull, CudaAlloc<double> > VectorD;
+        if (kind == kCg)
+          return Seldon::Cg<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kBiCgStab)
+          return Seldon::BiCgStab<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+      }
+    };
+
+    template <class Titer, class MatrixD, class P>
+    int Solve(SolverKind kind, MatrixD& A,
+              Vector<double, VectFull, CudaAlloc<double> >& x,
+              const Vector<double, VectFull, CudaAlloc<double> >& b,
+              P& M, Iteration<Titer>& iter)
+    {
+      return Dispatch<PrecondTraits<P>::native>::Run(kind, A, x, b, M, iter);
+    }
+  }
+
+
+  //! Preconditioned CG on the GPU (Cg.cxx:45-116).
+  template <class Titer, class Prop, class Preconditioner>
+  int Cg(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+         Vector<double, VectFull, CudaAlloc<double> >& x,
+         const Vector<double, VectFull, CudaAlloc<double> >& b,
+         Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCg, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int Cg(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+         Vector<double, VectFull, CudaAlloc<double> >& x,
+         const Vector<double, VectFull, CudaAlloc<double> >& b,
+         Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCg, A, x, b, M, iter);
+  }
+
+  //! BiCGSTAB on the GPU (BiCgStab.cxx:43-145).
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCgStab(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+               Vector<double, VectFull, CudaAlloc<double> >& x,
+               const Vector<double, VectFull, CudaAlloc<double> >& b,
+               Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCgStab, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCgStab(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+               Vector<double, VectFull, CudaAlloc<double> >& x,
+               const Vector<double, VectFull, CudaAlloc<double> >& b,
+               Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCgStab, A, x, b, M, iter);
+  }
+
+  //! Restarted left-preconditioned GMRES(m) on the GPU (Gmres.cxx:44-183).
+  template <class Titer, class Prop, class Preconditioner>
+  int Gmres(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+            Vector<double, VectFull, CudaAlloc<double> >& x,
+            const Vector<double, VectFull, CudaAlloc<double> >& b,
+            Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGmres, A, x, b, M, outer);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int Gmres(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+            Vector<double, VectFull, CudaAlloc<double> >& x,
+            const Vector<double, VectFull, CudaAlloc<double> >& b,
+            Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGmres, A, x, b, M, outer);
+  }
+
+} // namespace Seldon.
+
+#endif

@@ -23,6 +23,8 @@
 #ifndef SELDON_B200_H
 #define SELDON_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -41,6 +43,23 @@ const char* sb2_status_string(int status);
 
 /* Library version, e.g. 10000 for 1.0.0. */
 int sb2_version(void);
+
+/* ------------------------------------------------------------ device memory */
+
+/* Device buffers for callers that do not link the CUDA runtime themselves
+ * (the CudaAlloc allocator of SeldonB200.hxx).  They stand in for the
+ * allocator concept's allocate/deallocate/memorycpy (share/Allocator.hxx:
+ * 31-48, share/Allocator.cxx:33-65) on device memory.
+ *   sb2_device_alloc  cudaMalloc of `bytes` (bytes == 0 gives NULL)
+ *   sb2_device_free   cudaFree (NULL is a no-op)
+ *   sb2_memcpy        copy `bytes` between host and/or device memory
+ *                     (unified addressing decides the direction), on
+ *                     `stream`; returns after the copy has completed
+ *   sb2_stream_sync   wait for all work queued on `stream` */
+int sb2_device_alloc(size_t bytes, void** out);
+int sb2_device_free(void* p);
+int sb2_memcpy(void* dst, const void* src, size_t bytes, void* stream);
+int sb2_stream_sync(void* stream);
 
 /* ------------------------------------------------------------ CSR handle */
 

@@ -118,6 +118,10 @@ class SeldonB200Error(RuntimeError):
 _PROTOS = [
     ("sb2_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("sb2_version", ctypes.c_int, []),
+    ("sb2_device_alloc", ctypes.c_int, [ctypes.c_size_t, c_void_p]),
+    ("sb2_device_free", ctypes.c_int, [c_void_p]),
+    ("sb2_memcpy", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_size_t, c_void_p]),
+    ("sb2_stream_sync", ctypes.c_int, [c_void_p]),
     ("sb2_set_wait_limit_ms", ctypes.c_int, [ctypes.c_int]),
     ("sb2_csr_create", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p,

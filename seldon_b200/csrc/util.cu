@@ -85,6 +85,31 @@ const char* sb2_status_string(int status) {
 
 int sb2_version(void) { return 10000; }
 
+int sb2_device_alloc(size_t bytes, void** out) {
+  if (!out) return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  if (bytes == 0) return SB2_OK;
+  return sb2::map_cuda_error(cudaMalloc(out, bytes));
+}
+
+int sb2_device_free(void* p) {
+  if (!p) return SB2_OK;
+  return sb2::map_cuda_error(cudaFree(p));
+}
+
+int sb2_memcpy(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return SB2_OK;
+  if (!dst || !src) return SB2_ERR_INVALID_VALUE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return sb2::map_cuda_error(e);
+}
+
+int sb2_stream_sync(void* stream) {
+  return sb2::map_cuda_error(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+}
+
 int sb2_set_wait_limit_ms(int ms) {
   int old = sb2::g_wait_limit_ms;
   if (ms > 0) sb2::g_wait_limit_ms = ms;

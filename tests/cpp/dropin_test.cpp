@@ -1,0 +1,494 @@
+// Drop-in test of SeldonB200.hxx: the same templated user code runs on
+// Seldon's host types (the reference library itself, compiled from its
+// headers) and on the CudaAlloc device types, and the results are compared.
+//
+// Checked: SpMV (MltAdd, Mlt, transposed) bit for bit; DotProd/Norm2/Add/Mlt;
+// Cg (identity, Jacobi, SSOR), BiCgStab, Gmres(m)+Jacobi: return codes,
+// iteration counts, solutions and the residual lines Iteration prints;
+// a user-defined preconditioner (Seldon's generic driver on device types);
+// zero right-hand side; exceptions for invalid input.
+//
+// Output: one "PASS name ..." or "FAIL name ..." line per check; the exit
+// status is the number of failures.
+
+#include <cmath>
+#include <cstdio>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "Seldon.hxx"
+
+namespace Seldon
+{
+  // Upper-triangular back-substitution for the GMRES Hessenberg system
+  // (Gmres.cxx:166).  Seldon provides this only through cblas.
+  template <class Prop0, class Allocator0, class Allocator1>
+  void Solve(const Matrix<double, Prop0, ColUpTriang, Allocator0>& A,
+             Vector<double, VectFull, Allocator1>& X)
+  {
+    for (int j = A.GetN() - 1; j >= 0; j--)
+      if (X(j) != 0.0)
+        {
+          X(j) /= A(j, j);
+          for (int i = j - 1; i >= 0; i--)
+            X(i) -= X(j) * A(i, j);
+        }
+  }
+}
+
+#include "SeldonSolver.hxx"
+#include "SeldonB200.hxx"
+
+using namespace Seldon;
+
+typedef Matrix<double, General, RowSparse> HostGen;
+typedef Matrix<double, Symmetric, RowSymSparse> HostSym;
+typedef Vector<double> HostVec;
+typedef Matrix<double, General, RowSparse, CudaAlloc<double> > DevGen;
+typedef Matrix<double, Symmetric, RowSymSparse, CudaAlloc<double> > DevSym;
+typedef Vector<double, VectFull, CudaAlloc<double> > DevVec;
+
+static int failures = 0;
+
+static void report(bool ok, const std::string& name, const std::string& detail)
+{
+  std::printf("%s %s %s\n", ok ? "PASS" : "FAIL", name.c_str(), detail.c_str());
+  if (!ok)
+    failures++;
+}
+
+// ---------------------------------------------------------------- problems
+
+struct Csr
+{
+  int m, n;
+  std::vector<int> ptr, ind;
+  std::vector<double> val;
+};
+
+// 2D 5-point Laplacian of a g x g grid, upper triangle (RowSymSparse).
+static Csr laplacian_upper(int g)
+{
+  Csr A;
+  A.m = A.n = g * g;
+  A.ptr.push_back(0);
+  for (int y = 0; y < g; y++)
+    for (int x = 0; x < g; x++)
+      {
+        int i = y * g + x;
+        A.ind.push_back(i);
+        A.val.push_back(4.0);
+        if (x + 1 < g)
+          {
+            A.ind.push_back(i + 1);
+            A.val.push_back(-1.0);
+          }
+        if (y + 1 < g)
+          {
+            A.ind.push_back(i + g);
+            A.val.push_back(-1.0);
+          }
+        A.ptr.push_back(int(A.ind.size()));
+      }
+  return A;
+}
+
+// 2D upwind convection-diffusion of a g x g grid (nonsymmetric, RowSparse).
+static Csr convdiff(int g, double cx, double cy)
+{
+  Csr A;
+  A.m = A.n = g * g;
+  A.ptr.push_back(0);
+  for (int y = 0; y < g; y++)
+    for (int x = 0; x < g; x++)
+      {
+        int i = y * g + x;
+        if (y > 0)
+          {
+            A.ind.push_back(i - g);
+            A.val.push_back(-1.0 - cy);
+          }
+        if (x > 0)
+          {
+            A.ind.push_back(i - 1);
+            A.val.push_back(-1.0 - cx);
+          }
+        A.ind.push_back(i);
+        A.val.push_back(4.0 + cx + cy);
+        if (x + 1 < g)
+          {
+            A.ind.push_back(i + 1);
+            A.val.push_back(-1.0);
+          }
+        if (y + 1 < g)
+          {
+            A.ind.push_back(i + g);
+            A.val.push_back(-1.0);
+          }
+        A.ptr.push_back(int(A.ind.size()));
+      }
+  return A;
+}
+
+template <class MatrixH>
+static void to_host(const Csr& c, MatrixH& A)
+{
+  Vector<double> v(int(c.val.size()));
+  Vector<int> p(c.m + 1), ind(int(c.ind.size()));
+  for (size_t k = 0; k < c.val.size(); k++)
+    {
+      v(int(k)) = c.val[k];
+      ind(int(k)) = c.ind[k];
+    }
+  for (int k = 0; k <= c.m; k++)
+    p(k) = c.ptr[k];
+  A.SetData(c.m, c.n, v, p, ind);
+}
+
+static HostVec random_vector(int n, unsigned seed)
+{
+  HostVec v(n);
+  unsigned long long s = 0x9E3779B97F4A7C15ULL * (seed + 1);
+  for (int i = 0; i < n; i++)
+    {
+      s ^= s << 13;
+      s ^= s >> 7;
+      s ^= s << 17;
+      v(i) = double(s >> 11) / double(1ULL << 53) * 2.0 - 1.0;
+    }
+  return v;
+}
+
+static HostVec download(const DevVec& d)
+{
+  HostVec h;
+  Copy(d, h);
+  return h;
+}
+
+static double max_rel_diff(const HostVec& a, const HostVec& b)
+{
+  double num = 0.0, den = 0.0;
+  for (int i = 0; i < a.GetM(); i++)
+    {
+      num = std::max(num, std::fabs(a(i) - b(i)));
+      den = std::max(den, std::fabs(a(i)));
+    }
+  return den > 0.0 ? num / den : num;
+}
+
+static bool identical(const HostVec& a, const HostVec& b)
+{
+  if (a.GetM() != b.GetM())
+    return false;
+  for (int i = 0; i < a.GetM(); i++)
+    if (a(i) != b(i))
+      return false;
+  return true;
+}
+
+static std::string fmt(const char* f, double a, double b = 0, double c = 0)
+{
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), f, a, b, c);
+  return buf;
+}
+
+// ---------------------------------------------------------------- user code
+// Written once against Seldon's interface; instantiated for host and device.
+
+template <class MatrixT, class VectorT>
+void user_spmv(const MatrixT& A, const VectorT& x, VectorT& y, VectorT& z)
+{
+  MltAdd(1.5, A, x, -0.5, y);  // y = 1.5 A x - 0.5 y
+  Mlt(A, x, z);                // z = A x
+}
+
+template <class MatrixT, class VectorT>
+void user_spmv_trans(const MatrixT& A, const VectorT& x, VectorT& y)
+{
+  MltAdd(2.0, SeldonTrans, A, x, 1.0, y);
+}
+
+template <class MatrixT, class VectorT, class Precond>
+int user_solve(const std::string& solver, MatrixT& A, VectorT& x, const VectorT& b,
+               Precond& M, Iteration<double>& iter)
+{
+  if (solver == "cg")
+    return Cg(A, x, b, M, iter);
+  if (solver == "bicgstab")
+    return BiCgStab(A, x, b, M, iter);
+  return Gmres(A, x, b, M, iter);
+}
+
+// A preconditioner the library does not know: Seldon's generic driver runs
+// with the device types (z = r / 4 through Copy and Mlt).
+class QuarterPreconditioner
+{
+public:
+  template <class MatrixT, class VectorT>
+  void Solve(const MatrixT&, const VectorT& r, VectorT& z)
+  {
+    Copy(r, z);
+    Mlt(0.25, z);
+  }
+  template <class MatrixT, class VectorT>
+  void TransSolve(const MatrixT& A, const VectorT& r, VectorT& z)
+  {
+    Solve(A, r, z);
+  }
+};
+
+struct SolveOutcome
+{
+  int code, nb_iter;
+  HostVec x;
+  std::vector<int> printed_iters;
+};
+
+static std::vector<int> printed_iterations(const std::string& out)
+{
+  std::vector<int> its;
+  std::istringstream in(out);
+  std::string line;
+  const std::string key = "Residu at iteration number ";
+  while (std::getline(in, line))
+    if (line.compare(0, key.size(), key) == 0)
+      its.push_back(std::atoi(line.c_str() + key.size()));
+  return its;
+}
+
+template <class MatrixT, class VectorT, class Precond>
+SolveOutcome run_solve(const std::string& solver, MatrixT& A, VectorT& x,
+                       const VectorT& b, Precond& M, int max_iter, double tol,
+                       int restart, bool show)
+{
+  Iteration<double> iter(max_iter, tol);
+  iter.SetRestart(restart);
+  if (show)
+    iter.ShowMessages();
+  else
+    iter.HideMessages();
+  std::ostringstream captured;
+  std::streambuf* old = std::cout.rdbuf(captured.rdbuf());
+  SolveOutcome r;
+  r.code = user_solve(solver, A, x, b, M, iter);
+  std::cout.rdbuf(old);
+  r.nb_iter = iter.GetNumberIteration();
+  r.printed_iters = printed_iterations(captured.str());
+  return r;
+}
+
+template <class HM, class DM, class HP, class DP>
+void compare_solve(const std::string& name, const std::string& solver, HM& Ah, DM& Ad,
+                   const HostVec& bh, HP& Mh, DP& Md, int max_iter, double tol,
+                   int restart, double xtol, int iter_slack)
+{
+  HostVec xh(bh.GetM());
+  xh.Zero();
+  DevVec bd, xd;
+  Copy(bh, bd);
+  Copy(xh, xd);
+  SolveOutcome h = run_solve(solver, Ah, xh, bh, Mh, max_iter, tol, restart, true);
+  SolveOutcome d = run_solve(solver, Ad, xd, bd, Md, max_iter, tol, restart, true);
+  d.x = download(xd);
+  double dx = max_rel_diff(xh, d.x);
+  bool ok = h.code == d.code && std::abs(h.nb_iter - d.nb_iter) <= iter_slack
+    && dx <= xtol && h.printed_iters == d.printed_iters;
+  if (iter_slack > 0)
+    ok = h.code == d.code && std::abs(h.nb_iter - d.nb_iter) <= iter_slack && dx <= xtol;
+  char buf[256];
+  std::snprintf(buf, sizeof(buf),
+                "code %d/%d iterations %d/%d printed %d/%d lines max|dx|/max|x| %.2e",
+                h.code, d.code, h.nb_iter, d.nb_iter, int(h.printed_iters.size()),
+                int(d.printed_iters.size()), dx);
+  report(ok, name, buf);
+}
+
+int main()
+{
+  // ------------------------------------------------ matrices
+  Csr lap = laplacian_upper(40);     // n = 1600, SPD
+  Csr cd = convdiff(48, 0.8, 0.3);   // n = 2304, nonsymmetric
+  HostSym Sh;
+  HostGen Gh;
+  to_host(lap, Sh);
+  to_host(cd, Gh);
+  DevSym Sd;
+  DevGen Gd;
+  Sd.Copy(Sh);
+  Gd.Copy(Gh);
+  report(Sd.GetM() == Sh.GetM() && Sd.GetNonZeros() == Sh.GetNonZeros()
+         && Gd.GetN() == Gh.GetN() && Gd.GetNonZeros() == Gh.GetNonZeros(),
+         "upload", fmt("sym nnz %g general nnz %g", Sd.GetNonZeros(), Gd.GetNonZeros()));
+
+  // round trip through the device
+  {
+    HostGen back;
+    Gd.CopyToHost(back);
+    bool same = back.GetM() == Gh.GetM() && back.GetNonZeros() == Gh.GetNonZeros();
+    for (int k = 0; same && k <= Gh.GetM(); k++)
+      same = back.GetPtr()[k] == Gh.GetPtr()[k];
+    for (int k = 0; same && k < Gh.GetNonZeros(); k++)
+      same = back.GetInd()[k] == Gh.GetInd()[k] && back.GetData()[k] == Gh.GetData()[k];
+    report(same, "download", "CopyToHost reproduces ptr/ind/data");
+  }
+
+  // ------------------------------------------------ SpMV, bit for bit
+  {
+    const int n = Gh.GetM();
+    HostVec xh = random_vector(n, 1), yh = random_vector(n, 2), zh(n);
+    DevVec xd, yd, zd(n);
+    Copy(xh, xd);
+    Copy(yh, yd);
+    user_spmv(Gh, xh, yh, zh);
+    user_spmv(Gd, xd, yd, zd);
+    report(identical(yh, download(yd)) && identical(zh, download(zd)), "spmv_general",
+           "MltAdd(1.5, A, x, -0.5, y) and Mlt(A, x, z) identical to Seldon");
+    HostVec th = random_vector(n, 3);
+    DevVec td;
+    Copy(th, td);
+    user_spmv_trans(Gh, xh, th);
+    user_spmv_trans(Gd, xd, td);
+    double d = max_rel_diff(th, download(td));
+    report(d <= 1e-15, "spmv_general_trans",
+           fmt("MltAdd(2, SeldonTrans, A, x, 1, y): max rel diff %.2e (scatter order)", d));
+  }
+  {
+    const int n = Sh.GetM();
+    HostVec xh = random_vector(n, 4), yh = random_vector(n, 5), zh(n);
+    DevVec xd, yd, zd(n);
+    Copy(xh, xd);
+    Copy(yh, yd);
+    user_spmv(Sh, xh, yh, zh);
+    user_spmv(Sd, xd, yd, zd);
+    // Seldon adds the lower-triangle terms of a row in a second (scatter)
+    // pass; the device sums the expanded row, so the additions associate
+    // differently and agree to rounding, not bit for bit
+    double d = std::max(max_rel_diff(yh, download(yd)), max_rel_diff(zh, download(zd)));
+    report(d <= 1e-14, "spmv_symmetric",
+           fmt("RowSymSparse MltAdd and Mlt: max rel diff %.2e", d));
+  }
+
+  // ------------------------------------------------ BLAS-1
+  {
+    const int n = 100003;
+    HostVec xh = random_vector(n, 6), yh = random_vector(n, 7);
+    DevVec xd, yd;
+    Copy(xh, xd);
+    Copy(yh, yd);
+    double dh = DotProd(xh, yh), dd = DotProd(xd, yd);
+    double nh = Norm2(xh), nd = Norm2(xd);
+    Add(-0.75, xh, yh);
+    Add(-0.75, xd, yd);
+    Mlt(3.0, xh);
+    Mlt(3.0, xd);
+    double sh = 0;
+    for (int i = 0; i < n; i++)
+      sh += std::fabs(xh(i) * yh(i));
+    bool ok = std::fabs(dh - dd) <= 1e-12 * sh && std::fabs(nh - nd) <= 1e-14 * nh
+      && identical(yh, download(yd)) && identical(xh, download(xd));
+    report(ok, "blas1", fmt("dot diff %.2e norm2 rel diff %.2e", std::fabs(dh - dd),
+                            std::fabs(nh - nd) / nh));
+  }
+
+  // ------------------------------------------------ solvers
+  HostVec b_sym = random_vector(Sh.GetM(), 8), b_gen = random_vector(Gh.GetM(), 9);
+  {
+    Preconditioner_Base Mh, Md;
+    compare_solve("cg_identity", "cg", Sh, Sd, b_sym, Mh, Md, 2000, 1e-10, 10, 1e-8, 0);
+  }
+  {
+    JacobiPreconditioner<double> Mh, Md;
+    compare_solve("cg_jacobi", "cg", Sh, Sd, b_sym, Mh, Md, 2000, 1e-10, 10, 1e-8, 0);
+  }
+  {
+    SorPreconditioner<double> Mh, Md;
+    Mh.SetParameterRelaxation(1.2);
+    Md.SetParameterRelaxation(1.2);
+    compare_solve("cg_ssor", "cg", Sh, Sd, b_sym, Mh, Md, 2000, 1e-10, 10, 1e-8, 0);
+  }
+  {
+    Preconditioner_Base Mh, Md;
+    compare_solve("bicgstab_identity", "bicgstab", Gh, Gd, b_gen, Mh, Md, 4000, 1e-10, 10,
+                  1e-7, 2);
+  }
+  {
+    JacobiPreconditioner<double> Mh, Md;
+    compare_solve("gmres20_jacobi", "gmres", Gh, Gd, b_gen, Mh, Md, 4000, 1e-10, 20, 1e-8, 0);
+  }
+  {
+    SorPreconditioner<double> Mh, Md;
+    Mh.InitUnSymmetricPreconditioning();
+    Md.InitUnSymmetricPreconditioning();
+    compare_solve("gmres10_sor_forward", "gmres", Gh, Gd, b_gen, Mh, Md, 4000, 1e-10, 10,
+                  1e-8, 0);
+  }
+  {
+    QuarterPreconditioner Mh, Md;
+    compare_solve("cg_user_preconditioner", "cg", Sh, Sd, b_sym, Mh, Md, 2000, 1e-10, 10,
+                  1e-8, 0);
+  }
+  {
+    Preconditioner_Base Mh, Md;
+    compare_solve("cg_max_iter", "cg", Sh, Sd, b_sym, Mh, Md, 25, 1e-10, 10, 1e-9, 0);
+  }
+  {
+    // zero right-hand side: Init fails, the code is returned, x is untouched
+    HostVec zero(Sh.GetM());
+    zero.Zero();
+    HostVec xh = random_vector(Sh.GetM(), 10);
+    DevVec xd, bd;
+    Copy(xh, xd);
+    Copy(zero, bd);
+    Preconditioner_Base Mh, Md;
+    Iteration<double> ih(100, 1e-10), id(100, 1e-10);
+    ih.HideMessages();
+    id.HideMessages();
+    int ch = Cg(Sh, xh, zero, Mh, ih);
+    int cd2 = Cg(Sd, xd, bd, Md, id);
+    report(ch == cd2 && identical(xh, download(xd)), "cg_zero_rhs",
+           fmt("codes %g/%g, x untouched", ch, cd2));
+  }
+
+  // ------------------------------------------------ errors
+  {
+    bool thrown = false;
+    try
+      {
+        Vector<double> v(2);
+        Vector<int> p(3), ind(2);
+        p(0) = 0;
+        p(1) = 1;
+        p(2) = 2;
+        ind(0) = 0;
+        ind(1) = 5;  // column out of range
+        v.Fill(1.0);
+        DevGen bad(2, 2, v, p, ind);
+      }
+    catch (WrongDim&)
+      {
+        thrown = true;
+      }
+    report(thrown, "invalid_csr_throws", "column index out of range -> WrongDim");
+  }
+  {
+    bool thrown = false;
+    try
+      {
+        DevVec a(10), c(11);
+        a.Zero();
+        c.Zero();
+        Add(1.0, a, c);
+      }
+    catch (WrongDim&)
+      {
+        thrown = true;
+      }
+    report(thrown, "size_mismatch_throws", "Add with different sizes -> WrongDim");
+  }
+
+  std::printf("%d failure(s)\n", failures);
+  return failures;
+}
