@@ -121,6 +121,18 @@ struct EpiChainDot {
     q[i] = t;
     acc = add_rn(acc, mul_rn(__ldg(p + i), t));
   }
+  __device__ __forceinline__ void quad(int i, const T* t) {
+    if (!is_aligned16(q + i) || !is_aligned16(p + i)) {
+      for (int j = 0; j < 4; j++) (*this)(i + j, t[j]);
+      return;
+    }
+    T pv[4];
+    const T tv[4] = {t[0], t[1], t[2], t[3]};
+    vld4_ldg(p + i, pv);
+    vst4(q + i, tv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc = add_rn(acc, mul_rn(pv[j], t[j]));
+  }
 };
 
 // After the (p, q) reduction: alpha = rho / delta, or breakdown #2.
@@ -138,7 +150,7 @@ __device__ __forceinline__ void chain_after_delta(ChainArgs<T>& a, T delta) {
 // MODE 1: r = b - A x with ||r||^2, (r, z).  PART 0: slices, PART 1: long
 // rows (deposit slots after the slices').
 template <typename T, typename VT, int MODE, int PART>
-__global__ void __launch_bounds__(CT, PART == 0 ? 8 : 1)
+__global__ void __launch_bounds__(CT, PART == 1 ? 1 : (sizeof(VT) == 8 ? 4 : 6))
     k_spmv(ChainArgs<T> a, SellOp<VT> S, int slot0, int tot) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
@@ -147,7 +159,7 @@ __global__ void __launch_bounds__(CT, PART == 0 ? 8 : 1)
     EpiChainDot<T> epi{a.q, a.p, T(0)};
     XLoadLdg<T> xl{a.p};
     if (PART == 0)
-      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainDot<T>, 4>(
+      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainDot<T>, 1>(
           S, xl, epi, blockIdx.x, gridDim.x);
     else
       sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);

@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "sb2_internal.cuh"
+#include "sell.cuh"
 
 namespace sb2 {
 
@@ -146,11 +147,7 @@ int build_tma_partition_host(const int* ptr, int rows, Partition* out) {
 // lengths are irregular), longer rows listed for the warp and CTA bins.
 int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
                     SellArrays* out) {
-  constexpr int kMax = 32, kCta = 1024;
-  if (rows >= (1 << 26)) {
-    out->nslice = -1;
-    return SB2_OK;
-  }
+  constexpr int kMax = 32, kCta = 1024, kRows = 128;
   std::vector<int> shortr, wr, cr;
   int lmin = kMax, lmax = 0;
   for (int i = 0; i < rows; i++) {
@@ -171,46 +168,74 @@ int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
     std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
       return (ptr[a + 1] - ptr[a]) > (ptr[b + 1] - ptr[b]);
     });
-  const int ns = (int)((shortr.size() + 31) / 32);
+  const long long nshort = (long long)shortr.size();
+  const int ns = (int)((nshort + kRows - 1) / kRows);
+  auto row_at = [&](long long q) { return q < nshort ? shortr[q] : -1; };
+  auto len_of = [&](int r) { return r < 0 ? 0 : ptr[r + 1] - ptr[r]; };
+  // slice offsets in groups (a group = entry k of the 4 rows of one lane)
   std::vector<long long> sptr(ns + 1, 0);
-  std::vector<unsigned> rinfo((size_t)ns * 32, (1u << 26) - 1u);
+  std::vector<uint2> qinfo((size_t)ns * 32);
+  std::vector<int4> qrows((size_t)ns * 32);
+  bool scattered = false;
   for (int sl = 0; sl < ns; sl++) {
     int w = 0;
     for (int l = 0; l < 32; l++) {
-      const size_t q = (size_t)sl * 32 + l;
-      if (q < shortr.size()) {
-        const int r = shortr[q], len = ptr[r + 1] - ptr[r];
+      const long long q0 = (long long)sl * kRows + 4 * l;
+      int r[4];
+      unsigned lens = 0;
+      for (int j = 0; j < 4; j++) {
+        r[j] = row_at(q0 + j);
+        const int len = len_of(r[j]);
         w = std::max(w, len);
-        rinfo[q] = (unsigned)r | ((unsigned)len << 26);
+        lens |= (unsigned)len << (8 * j);
       }
+      const bool consecutive = r[0] >= 0 && r[1] == r[0] + 1 && r[2] == r[0] + 2 && r[3] == r[0] + 3;
+      uint2 inf;
+      inf.x = consecutive ? (unsigned)r[0] : kQuadScattered;
+      inf.y = lens;
+      qinfo[(size_t)sl * 32 + l] = inf;
+      qrows[(size_t)sl * 32 + l] = make_int4(r[0], r[1], r[2], r[3]);
+      scattered = scattered || !consecutive;
     }
     sptr[sl + 1] = sptr[sl] + 32ll * w;
   }
-  const long long tot = sptr[ns];
-  std::vector<int> scol(std::max(tot, 1ll), 0);
-  std::vector<double> sval(std::max(tot, 1ll), 0.0);
+  const long long tot = sptr[ns] * 4;  // entries incl. padding
+  std::vector<int> scol(std::max(tot, 4ll), 0);
+  std::vector<double> sval(std::max(tot, 4ll), 0.0);
   std::vector<long long> pos(std::max<long long>(ptr[rows], 1), -1);
-  for (int sl = 0; sl < ns; sl++)
-    for (int l = 0; l < 32; l++) {
-      const size_t q = (size_t)sl * 32 + l;
-      if (q >= shortr.size()) continue;
-      const int r = shortr[q];
-      for (int j = 0; j < ptr[r + 1] - ptr[r]; j++) {
-        const long long e = sptr[sl] + (long long)j * 32 + l;
-        scol[e] = ind[ptr[r] + j];
-        sval[e] = val[ptr[r] + j];
-        pos[ptr[r] + j] = e;
+  for (int sl = 0; sl < ns; sl++) {
+    const int w = (int)((sptr[sl + 1] - sptr[sl]) / 32);
+    for (int l = 0; l < 32; l++)
+      for (int j = 0; j < 4; j++) {
+        const int r = row_at((long long)sl * kRows + 4 * l + j);
+        const int len = len_of(r);
+        int last = 0;
+        for (int k = 0; k < w; k++) {
+          const long long e = (sptr[sl] + (long long)k * 32 + l) * 4 + j;
+          if (k < len) {
+            last = ind[ptr[r] + k];
+            scol[e] = last;
+            sval[e] = val[ptr[r] + k];
+            pos[ptr[r] + k] = e;
+          } else {
+            scol[e] = last;  // padding: a column this row already reads, value 0, skipped
+          }
+        }
       }
-    }
+  }
   out->nslice = ns;
   out->padded = tot;
   out->nwarp = (int)wr.size();
   out->ncta = (int)cr.size();
   SB2_CUDA_TRY(cudaMalloc(&out->d_sptr, sizeof(long long) * (ns + 1)));
   SB2_CUDA_TRY(cudaMemcpy(out->d_sptr, sptr.data(), sizeof(long long) * (ns + 1), cudaMemcpyHostToDevice));
-  SB2_CUDA_TRY(cudaMalloc(&out->d_rinfo, sizeof(unsigned) * std::max<size_t>(rinfo.size(), 1)));
-  if (!rinfo.empty())
-    SB2_CUDA_TRY(cudaMemcpy(out->d_rinfo, rinfo.data(), sizeof(unsigned) * rinfo.size(), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMalloc(&out->d_qinfo, sizeof(uint2) * std::max<size_t>(qinfo.size(), 1)));
+  if (!qinfo.empty())
+    SB2_CUDA_TRY(cudaMemcpy(out->d_qinfo, qinfo.data(), sizeof(uint2) * qinfo.size(), cudaMemcpyHostToDevice));
+  if (scattered) {
+    SB2_CUDA_TRY(cudaMalloc(&out->d_qrows, sizeof(int4) * qrows.size()));
+    SB2_CUDA_TRY(cudaMemcpy(out->d_qrows, qrows.data(), sizeof(int4) * qrows.size(), cudaMemcpyHostToDevice));
+  }
   SB2_CUDA_TRY(cudaMalloc(&out->d_scol, sizeof(int) * scol.size()));
   SB2_CUDA_TRY(cudaMemcpy(out->d_scol, scol.data(), sizeof(int) * scol.size(), cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMalloc(&out->d_sval, sizeof(double) * sval.size()));
@@ -226,7 +251,8 @@ int build_sell_host(const int* ptr, const int* ind, const double* val, int rows,
 
 void free_sell(SellArrays* s) {
   cudaFree(s->d_sptr);
-  cudaFree(s->d_rinfo);
+  cudaFree(s->d_qinfo);
+  cudaFree(s->d_qrows);
   cudaFree(s->d_scol);
   cudaFree(s->d_sval);
   cudaFree(s->d_sval32);

@@ -74,7 +74,7 @@ static int ensure_fp32(const sb2_csr* cA, bool need_diag) {
 
 static SellOp<float> sell_op32(const sb2_csr* A) {
   const SellArrays& s = A->full.sell;
-  return SellOp<float>{s.nslice, s.d_sptr, s.d_rinfo, s.d_scol, s.d_sval32, s.nwarp, s.d_wrows,
+  return SellOp<float>{s.nslice, s.d_sptr, s.d_qinfo, s.d_qrows, s.d_scol, s.d_sval32, s.nwarp, s.d_wrows,
                        s.ncta, s.d_crows, A->full.d_ptr, A->full.d_ind, A->d_val32};
 }
 
@@ -93,7 +93,7 @@ struct EpiIrResidual {
 };
 
 template <int PART>
-__global__ void __launch_bounds__(IT, PART == 0 ? 8 : 1)
+__global__ void __launch_bounds__(IT, PART == 0 ? 4 : 1)
     k_ir_residual(SellOp<double> S, const double* __restrict__ x, const double* __restrict__ b,
                   double* __restrict__ r, float* __restrict__ r32, double* part, unsigned* cnt,
                   double* out, int slot0, int tot) {

@@ -109,6 +109,16 @@ template <typename T>
 struct XLoadCg {
   const T* x;
   __device__ __forceinline__ T operator()(int j) const { return __ldcg(x + j); }
+  template <typename O>
+  __device__ __forceinline__ void gather4(const int4& c, O (&o)[4]) const {
+    T v[4];
+    if (quad_contiguous(x, c)) {
+      vld4_cg(x + c.x, v);
+    } else {
+      v[0] = __ldcg(x + c.x); v[1] = __ldcg(x + c.y); v[2] = __ldcg(x + c.z); v[3] = __ldcg(x + c.w);
+    }
+    o[0] = O(v[0]); o[1] = O(v[1]); o[2] = O(v[2]); o[3] = O(v[3]);
+  }
 };
 
 #endif  // __CUDACC__

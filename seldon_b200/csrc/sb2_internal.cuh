@@ -61,9 +61,10 @@ inline long long padded_rows(long long rows) { return ((rows + 1 + 3) / 4) * 4 +
 // Binned sliced-ELLPACK copy of an operator (see sell.cuh).  nslice < 0:
 // not applicable (more than 2^26 rows).
 struct SellArrays {
-  int nslice = -1;
-  long long* d_sptr = nullptr;
-  unsigned* d_rinfo = nullptr;
+  int nslice = -1;             // slices of 128 rows (4 per lane)
+  long long* d_sptr = nullptr; // first group of each slice
+  uint2* d_qinfo = nullptr;    // per lane: row0 (or scattered flag), 4 lengths
+  int4* d_qrows = nullptr;     // per lane row ids, only when some lane is scattered
   int* d_scol = nullptr;
   double* d_sval = nullptr;
   float* d_sval32 = nullptr;  // FP32 copy (lazy, mixed precision)
@@ -84,7 +85,7 @@ struct CsrArrays {
   double* d_val = nullptr;  // [padded_nnz]
   Partition part;           // plain kernel: row blocks incl. long rows
   Partition tma;            // pipelined kernel (nblk == -1: not applicable)
-  SellArrays sell;          // binned SELL-32 (default product)
+  SellArrays sell;          // binned quad-row SELL (default product)
   int max_row = 0;          // longest row
 };
 
@@ -217,6 +218,65 @@ __device__ __forceinline__ void ld_stream_val4(const double* p, double v[4]) {
 __device__ __forceinline__ void ld_stream_val4(const float* p, float v[4]) {
   float4 a = __ldcs(reinterpret_cast<const float4*>(p));
   v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+
+// 16-byte vector accesses of 4 consecutive entries (p 16-byte aligned).
+template <typename T>
+__device__ __forceinline__ void vld4_cs(const T* p, T (&o)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  } else {
+    const float4 a = __ldcs(reinterpret_cast<const float4*>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void vld4_ldg(const T* p, T (&o)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  } else {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void vld4_cg(const T* p, T (&o)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  } else {
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void vst4(T* p, const T (&v)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+  } else {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ bool is_aligned16(const T* p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
+// The four columns c.x..c.w are c.x, c.x+1, c.x+2, c.x+3 and x + c.x is
+// 16-byte aligned: one vector load fetches the four x values.
+template <typename XT>
+__device__ __forceinline__ bool quad_contiguous(const XT* x, const int4& c) {
+  return c.y == c.x + 1 && c.z == c.x + 2 && c.w == c.x + 3 && is_aligned16(x + c.x);
 }
 
 #endif  // __CUDACC__

@@ -1,19 +1,30 @@
 // Row-length-binned SpMV over a sliced-ELLPACK copy of the short rows.
 //
 // Bins (chosen on the host from the row lengths):
-//   thread bin  rows of <= kSellMaxLen nonzeros, packed into slices of 32
-//               rows stored column-major (SELL-32): entry j of the 32 rows of
-//               a slice sits in 32 consecutive words, so a warp reads its
-//               values and column indices with fully coalesced loads and
-//               each lane sums ONE row in stored order -- the reference's
-//               sequential row sum (Functions_MatVect.cxx:423-428), bit for
-//               bit.  Padding entries are skipped, never multiplied.
+//   thread bin  rows of <= kSellMaxLen nonzeros, packed into slices of 128
+//               rows; lane l of the warp that takes a slice owns its rows
+//               4l..4l+3 ("quad rows").  Group g of a slice holds entry k of
+//               the four rows of one lane, so a lane reads the column
+//               indices of its four rows with one 16-byte load and their
+//               values with one (FP32) or two (FP64) 16-byte loads, and a
+//               warp's loads are 512 contiguous bytes.  When the four
+//               columns are consecutive and 16-byte aligned (banded and
+//               stencil matrices) the four x values come with one vector
+//               load too.  Each row is still summed alone, in stored order --
+//               the reference's sequential row sum (Functions_MatVect.cxx:
+//               423-428), bit for bit; padding entries are skipped, never
+//               multiplied.
 //   warp bin    rows of kSellMaxLen+1 .. kSellCtaLen nonzeros: one warp per
 //               row over the original CSR arrays, shuffle reduction.
 //   CTA bin     longer rows: one CTA per row, block reduction.
 // Rows of the thread bin may be sorted by length (irregular matrices) so the
-// slices carry little padding; the per-lane row id says where the result goes.
+// slices carry little padding; lanes whose four rows are not consecutive
+// read their row ids from a side table.
 #pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
 
 #include "sb2_internal.cuh"
 
@@ -21,16 +32,18 @@ namespace sb2 {
 
 constexpr int kSellMaxLen = 32;    // longest row of the thread bin
 constexpr int kSellCtaLen = 1024;  // longest row of the warp bin
-constexpr int kSellRowBits = 26;   // row id bits in a lane descriptor
-constexpr unsigned kSellRowMask = (1u << kSellRowBits) - 1u;
+constexpr int kQuadRows = 128;     // rows of a slice: 32 lanes x 4 rows
+constexpr unsigned kQuadScattered = 1u << 31;  // lane rows not row0..row0+3
 
 // Device view of the binned operator (value type VT).
 template <typename VT>
 struct SellOp {
-  int nslice;            // thread-bin slices of 32 rows
-  const long long* sptr; // [nslice+1] element offset of each slice (multiple of 32)
-  const unsigned* rinfo; // [nslice*32] row | len << 26; padding lanes: row field = mask
-  const int* scol;       // column indices, column-major per slice
+  int nslice;            // thread-bin slices of 128 rows
+  const long long* sptr; // [nslice+1] first group of each slice (a group = 4 entries)
+  const uint2* qinfo;    // [nslice*32] per lane: {row0 or kQuadScattered,
+                         //  lengths of its 4 rows, 8 bits each}
+  const int4* qrows;     // [nslice*32] row ids of scattered lanes (-1: none)
+  const int* scol;       // [groups*4] column indices, group-major
   const VT* sval;        // values, same layout
   int nwarp_rows;        // warp bin
   const int* wrows;
@@ -43,31 +56,77 @@ struct SellOp {
 
 #ifdef __CUDACC__
 
-// One slice: every lane sums its row (entries loaded U at a time, all
-// gathers of a group in flight before the first product).
-template <typename VT, typename AT, class XLoad, class Epi, int U = 4>
+// Epilogues may handle four consecutive rows at once: quad(row0, t[4]) is
+// called for lanes whose rows are row0..row0+3 with row0 % 4 == 0; without
+// it the scalar operator() runs for each row.
+template <class E, typename AT, class = void>
+struct HasQuad : std::false_type {};
+template <class E, typename AT>
+struct HasQuad<E, AT, std::void_t<decltype(std::declval<E&>().quad(0, std::declval<const AT*>()))>>
+    : std::true_type {};
+
+template <typename AT, class Epi>
+__device__ __forceinline__ void epi_quad(Epi& epi, int row0, const AT* t) {
+  if constexpr (HasQuad<Epi, AT>::value) {
+    epi.quad(row0, t);
+  } else {
+    epi(row0, t[0]);
+    epi(row0 + 1, t[1]);
+    epi(row0 + 2, t[2]);
+    epi(row0 + 3, t[3]);
+  }
+}
+
+// One slice: lane `lane` sums its four rows (U groups loaded before the
+// first product).
+template <typename VT, typename AT, class XLoad, class Epi, int U = 1>
 __device__ __forceinline__ void sell_slice(const SellOp<VT>& S, int slice, int lane,
                                            const XLoad& xl, Epi& epi) {
-  const unsigned info = __ldg(S.rinfo + (size_t)slice * 32 + lane);
-  const int len = (int)(info >> kSellRowBits);
-  const long long base = __ldg(S.sptr + slice) + lane;
-  AT t = AT(0);
-  for (int j0 = 0; j0 < len; j0 += U) {
-    AT vv[U], xv[U];
+  const size_t q = (size_t)slice * 32 + lane;
+  const uint2 inf = __ldg(S.qinfo + q);
+  const int ln[4] = {(int)(inf.y & 255u), (int)((inf.y >> 8) & 255u),
+                     (int)((inf.y >> 16) & 255u), (int)(inf.y >> 24)};
+  const int L = max(max(ln[0], ln[1]), max(ln[2], ln[3]));
+  const long long g0 = __ldg(S.sptr + slice) + lane;
+  const int4* __restrict__ col4 = reinterpret_cast<const int4*>(S.scol);
+  AT t[4] = {AT(0), AT(0), AT(0), AT(0)};
+  for (int k0 = 0; k0 < L; k0 += U) {
+    int4 c[U];
+    VT v[U][4];
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      if (j0 + u < len) {
-        const long long e = base + (long long)(j0 + u) * 32;
-        vv[u] = AT(__ldcs(S.sval + e));
-        xv[u] = AT(xl(__ldcs(S.scol + e)));
+      if (k0 + u < L) {
+        const long long g = g0 + (long long)(k0 + u) * 32;
+        c[u] = __ldcs(col4 + g);
+        vld4_cs(S.sval + g * 4, v[u]);
       }
     }
 #pragma unroll
-    for (int u = 0; u < U; u++)
-      if (j0 + u < len) t = add_rn(t, mul_rn(vv[u], xv[u]));
+    for (int u = 0; u < U; u++) {
+      if (k0 + u < L) {
+        AT xv[4];
+        xl.gather4(c[u], xv);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (k0 + u < ln[j]) t[j] = add_rn(t[j], mul_rn(AT(v[u][j]), xv[j]));
+      }
+    }
   }
-  const unsigned row = info & kSellRowMask;
-  if (row != kSellRowMask) epi((int)row, t);
+  if (!(inf.x & kQuadScattered)) {
+    const int row0 = (int)inf.x;
+    if ((row0 & 3) == 0) {
+      epi_quad<AT>(epi, row0, t);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) epi(row0 + j, t[j]);
+    }
+  } else {
+    const int4 rr = __ldg(S.qrows + q);
+    if (rr.x >= 0) epi(rr.x, t[0]);
+    if (rr.y >= 0) epi(rr.y, t[1]);
+    if (rr.z >= 0) epi(rr.z, t[2]);
+    if (rr.w >= 0) epi(rr.w, t[3]);
+  }
 }
 
 // Sum of the entries k0, k0+STEP, ... < e of a CSR row, four loads in
@@ -112,7 +171,7 @@ __device__ __forceinline__ void sell_cta_row(const SellOp<VT>& S, int row, const
 // warp-bin rows, CTAs take CTA-bin rows.  `cta`/`ncta` let a persistent
 // kernel pass its own CTA index and grid size.
 // The thread bin (slices), warps grid-strided from (cta, ncta).
-template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 4>
+template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 1>
 __device__ __forceinline__ void sell_spmv_slices(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
                                                  int cta, int ncta) {
   constexpr int W = NT / 32;
@@ -137,7 +196,7 @@ __device__ __forceinline__ void sell_spmv_long(const SellOp<VT>& S, const XLoad&
 // All bins of one product, work spread over the grid: warps take slices and
 // warp-bin rows, CTAs take CTA-bin rows.  `cta`/`ncta` let a persistent
 // kernel pass its own CTA index and grid size.
-template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 4>
+template <int NT, typename VT, typename AT, class XLoad, class Epi, int U = 1>
 __device__ __forceinline__ void sell_spmv(const SellOp<VT>& S, const XLoad& xl, Epi& epi,
                                           AT* s_red, int cta, int ncta) {
   sell_spmv_slices<NT, VT, AT, XLoad, Epi, U>(S, xl, epi, cta, ncta);

@@ -23,6 +23,17 @@ template <typename XT>
 struct XLoadLdg {
   const XT* __restrict__ x;
   __device__ __forceinline__ XT operator()(int j) const { return __ldg(x + j); }
+  // x[c.x], x[c.y], x[c.z], x[c.w]: one vector load when they are adjacent
+  template <typename O>
+  __device__ __forceinline__ void gather4(const int4& c, O (&o)[4]) const {
+    XT v[4];
+    if (quad_contiguous(x, c)) {
+      vld4_ldg(x + c.x, v);
+    } else {
+      v[0] = __ldg(x + c.x); v[1] = __ldg(x + c.y); v[2] = __ldg(x + c.z); v[3] = __ldg(x + c.w);
+    }
+    o[0] = O(v[0]); o[1] = O(v[1]); o[2] = O(v[2]); o[3] = O(v[3]);
+  }
 };
 
 // VT: matrix value type; AT: product/accumulation type (VT and XT are
