@@ -149,8 +149,15 @@ __device__ __forceinline__ void chain_after_delta(ChainArgs<T>& a, T delta) {
 // One SELL product fused with a reduction; MODE 0: q = A p and (p, q);
 // MODE 1: r = b - A x with ||r||^2, (r, z).  PART 0: slices, PART 1: long
 // rows (deposit slots after the slices').
+// Slice-kernel shape per value type: resident CTAs per SM (the launch
+// bound and the reducing grid) and groups in flight per lane.
+template <typename VT>
+constexpr int chain_spmv_occ() { return sizeof(VT) == 8 ? 4 : 4; }
+template <typename VT>
+constexpr int chain_spmv_unroll() { return sizeof(VT) == 8 ? 1 : 3; }
+
 template <typename T, typename VT, int MODE, int PART>
-__global__ void __launch_bounds__(CT, PART == 1 ? 1 : (sizeof(VT) == 8 ? 4 : 6))
+__global__ void __launch_bounds__(CT, PART == 1 ? 1 : chain_spmv_occ<VT>())
     k_spmv(ChainArgs<T> a, SellOp<VT> S, int slot0, int tot) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
@@ -159,7 +166,7 @@ __global__ void __launch_bounds__(CT, PART == 1 ? 1 : (sizeof(VT) == 8 ? 4 : 6))
     EpiChainDot<T> epi{a.q, a.p, T(0)};
     XLoadLdg<T> xl{a.p};
     if (PART == 0)
-      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainDot<T>, 1>(
+      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainDot<T>, chain_spmv_unroll<VT>()>(
           S, xl, epi, blockIdx.x, gridDim.x);
     else
       sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
@@ -171,7 +178,8 @@ __global__ void __launch_bounds__(CT, PART == 1 ? 1 : (sizeof(VT) == 8 ? 4 : 6))
     EpiChainResidual<T> epi{a, T(0), T(0)};
     XLoadLdg<T> xl{a.x};
     if (PART == 0)
-      sell_spmv_slices<CT, VT, T>(S, xl, epi, blockIdx.x, gridDim.x);
+      sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiChainResidual<T>, chain_spmv_unroll<VT>()>(
+          S, xl, epi, blockIdx.x, gridDim.x);
     else
       sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
     T v[2] = {block_sum<CT>(epi.rr, s_red), block_sum<CT>(epi.rz, s_red)};
@@ -448,12 +456,13 @@ static int chain_elem_grid(int n) {
   return std::max(1, std::min((n + CT * 32 - 1) / (CT * 32), cap));
 }
 
-// CTAs of a reducing product: one slice per warp up to four resident waves,
-// beyond that warps loop over slices (fewer deposits to sum at the end).
+// CTAs of a reducing product: one slice per warp up to one resident wave,
+// beyond that warps loop over slices: the fewer deposits, the shorter the
+// finishing sum.
 template <typename VT>
-static int reducing_slice_grid(const SellOp<VT>& S) {
+int reducing_slice_grid(const SellOp<VT>& S) {
   if (S.nslice <= 0) return 0;
-  const int cap = num_sms(current_device()) * 24;
+  const int cap = num_sms(current_device()) * chain_spmv_occ<VT>();
   return std::min((S.nslice + 7) / 8, cap);
 }
 
@@ -501,10 +510,13 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
   else
     SB2_TRY((launch_spmv_pair<T, VT>(1, a, S, s)));
   SB2_CUDA_TRY(cudaGetLastError());
-  // iterations in chunks; the stop flag is read back once per chunk
+  // iterations in chunks (8, 16, then 32), one chunk always queued behind
+  // the one whose state the host waits for
+  ChainPipe<T> pipe;
+  SB2_TRY(pipe.init());
+  ChunkPlanner plan;
   int launched = 0, chunk = 8;
-  ChainState<T> h{};
-  for (;;) {
+  auto enqueue = [&]() -> int {
     for (int c = 0; c < chunk; c++) {
       k_p<T><<<ge, CT, 0, s>>>(a);
       SB2_TRY((launch_spmv_pair<T, VT>(0, a, S, s)));
@@ -512,12 +524,21 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
     }
     SB2_CUDA_TRY(cudaGetLastError());
     launched += chunk;
-    SB2_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s));
-    SB2_CUDA_TRY(cudaStreamSynchronize(s));
-    if (h.done || launched > max_iter + 1) break;
-    chunk = std::min(chunk * 2, 32);
+    return pipe.mark(st, launched, s);
+  };
+  SB2_TRY(enqueue());
+  chunk = 16;
+  SB2_TRY(enqueue());
+  for (;;) {
+    ChainState<T> h;
+    int at = 0;
+    SB2_TRY(pipe.wait(&h, &at));
+    if (h.done || at > max_iter + 1) break;
+    chunk = plan.next(h.nb_iter, h.reste, tol, launched - at, std::min(chunk * 2, 32));
+    SB2_TRY(enqueue());
   }
-  *out = h;
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));
   return SB2_OK;
 }
 
@@ -527,7 +548,6 @@ int chain_ru_resume(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* wo
 
 // Reliable-update CG iterations: the caller's loop applies the corrections.
 // ru_start: state for an initial residual r already in place (x = 0);
-// ru_iterate: enqueue up to `chunk` iterations, return the state after them.
 template <typename T, typename VT>
 int chain_ru_start(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
                    ChainState<T>* st, T* part, double facteur, double tol, double delta,
@@ -553,9 +573,11 @@ int chain_ru_resume(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* wo
   return SB2_OK;
 }
 
+// ru_enqueue: `chunk` iterations queued on s (no wait; the caller's
+// ChainPipe reads the state behind them).
 template <typename T, typename VT>
-int chain_ru_iterate(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
-                     ChainState<T>* st, T* part, int chunk, cudaStream_t s, ChainState<T>* out) {
+int chain_ru_enqueue(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                     ChainState<T>* st, T* part, int chunk, cudaStream_t s) {
   ChainArgs<T> a{n, nullptr, x, r, work, work + n, diag, st, part, nullptr, nullptr};
   const int ge = chain_elem_grid(n);
   for (int c = 0; c < chunk; c++) {
@@ -564,8 +586,6 @@ int chain_ru_iterate(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* w
     k_x_ru<T><<<ge, CT, 0, s>>>(a);
   }
   SB2_CUDA_TRY(cudaGetLastError());
-  SB2_CUDA_TRY(cudaMemcpyAsync(out, st, sizeof(*out), cudaMemcpyDeviceToHost, s));
-  SB2_CUDA_TRY(cudaStreamSynchronize(s));
   return SB2_OK;
 }
 
@@ -575,10 +595,12 @@ template int chain_ru_start<float, float>(const SellOp<float>&, int, const float
 template int chain_ru_resume<float, float>(const SellOp<float>&, int, const float*, float*,
                                            float*, float*, ChainState<float>*, float*,
                                            cudaStream_t);
-template int chain_ru_iterate<float, float>(const SellOp<float>&, int, const float*, float*,
+template int chain_ru_enqueue<float, float>(const SellOp<float>&, int, const float*, float*,
                                             float*, float*, ChainState<float>*, float*, int,
-                                            cudaStream_t, ChainState<float>*);
+                                            cudaStream_t);
 
+template int reducing_slice_grid<double>(const SellOp<double>&);
+template int reducing_slice_grid<float>(const SellOp<float>&);
 template long long chain_part_slots<double>(const SellOp<double>&, int);
 template long long chain_part_slots<float>(const SellOp<float>&, int);
 template int chain_cg<double, double>(const SellOp<double>&, int, const double*, double*,

@@ -15,6 +15,9 @@
 // and the last depositor of the pair finishes it.
 #pragma once
 
+#include <algorithm>
+#include <cmath>
+
 #include "sell.cuh"
 
 namespace sb2 {
@@ -53,6 +56,94 @@ struct ChainArgs {
   T* part;        // deposits (2 per CTA at most)
   double* hist;   // relative residual of each Finished() test
   int* hist_it;
+};
+
+// Size of the next chunk of a chained loop: from the residual's decrease over
+// the last chunk, the iterations still needed to reach `target` (a relative
+// residual: the stop, or the next correction), less those already queued,
+// within [lo, hi]; `dflt` until two states have been seen.  Fewer iterations
+// queued past the stop means fewer kernels that only return.
+struct ChunkPlanner {
+  int prev_it = -1;
+  double prev_res = 0.0;
+  void reset() { prev_it = -1; }
+  int next(int it, double res, double target, int in_flight, int dflt, int lo = 8, int hi = 32) {
+    int c = dflt;
+    if (prev_it >= 0 && it > prev_it && res > 0.0 && res < prev_res && target > 0.0) {
+      const double q = std::pow(res / prev_res, 1.0 / (double)(it - prev_it));
+      const double need = target < res ? std::log(target / res) / std::log(q) : 0.0;
+      c = (int)std::ceil(need) - in_flight + 1;
+    }
+    prev_it = it;
+    prev_res = res;
+    return std::max(lo, std::min(hi, c));
+  }
+};
+
+// Host side of a chained loop.  After each chunk of iterations the state is
+// copied to pinned host memory and an event marks its arrival; the caller
+// keeps one chunk queued behind the one it waits on, so the device does not
+// idle while the host wakes up (kernels queued after the stop return at
+// once).  The two pinned snapshot slots are allocated once per host thread
+// and kept until exit.
+template <typename T>
+class ChainPipe {
+ public:
+  ChainPipe() = default;
+  ChainPipe(const ChainPipe&) = delete;
+  ChainPipe& operator=(const ChainPipe&) = delete;
+  ~ChainPipe() {
+    for (int i = 0; i < 2; i++)
+      if (ev_[i]) cudaEventDestroy(ev_[i]);
+  }
+  int init() {
+    static thread_local void* pinned = nullptr;
+    if (!pinned) {
+      cudaError_t e = cudaHostAlloc(&pinned, 2 * sizeof(ChainState<double>), cudaHostAllocPortable);
+      if (e != cudaSuccess) {
+        pinned = nullptr;
+        return map_cuda_error(e);
+      }
+    }
+    snap_ = static_cast<ChainState<T>*>(pinned);
+    for (int i = 0; i < 2; i++) {
+      cudaError_t e = cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming);
+      if (e != cudaSuccess) return map_cuda_error(e);
+    }
+    return SB2_OK;
+  }
+  // a chunk has been enqueued: snapshot the state behind it
+  int mark(const ChainState<T>* st, int launched, cudaStream_t s) {
+    const int k = w_;
+    w_ ^= 1;
+    at_[k] = launched;
+    out_++;
+    cudaError_t e = cudaMemcpyAsync(&snap_[k], st, sizeof(ChainState<T>), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_[k], s);
+    return map_cuda_error(e);
+  }
+  // the oldest snapshot not yet read (waits for its chunk)
+  int wait(ChainState<T>* h, int* launched) {
+    const int k = r_;
+    r_ ^= 1;
+    out_--;
+    cudaError_t e = cudaEventSynchronize(ev_[k]);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    *h = snap_[k];
+    if (launched) *launched = at_[k];
+    return SB2_OK;
+  }
+  int outstanding() const { return out_; }
+  // every marked chunk has completed (the stream was synchronized)
+  void reset() {
+    w_ = r_ = out_ = 0;
+  }
+
+ private:
+  ChainState<T>* snap_ = nullptr;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+  int at_[2] = {0, 0};
+  int w_ = 0, r_ = 0, out_ = 0;
 };
 
 #ifdef __CUDACC__

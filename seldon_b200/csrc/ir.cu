@@ -23,6 +23,8 @@ namespace sb2 {
 
 template <typename VT>
 long long chain_part_slots(const SellOp<VT>& S, int n);
+template <typename VT>
+int reducing_slice_grid(const SellOp<VT>& S);
 template <typename T, typename VT>
 int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* work,
              ChainState<T>* st, T* part, double* hist, int* hist_it, int hist_cap, double tol,
@@ -36,8 +38,8 @@ template <typename T, typename VT>
 int chain_ru_resume(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
                     ChainState<T>* st, T* part, cudaStream_t s);
 template <typename T, typename VT>
-int chain_ru_iterate(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
-                     ChainState<T>* st, T* part, int chunk, cudaStream_t s, ChainState<T>* out);
+int chain_ru_enqueue(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
+                     ChainState<T>* st, T* part, int chunk, cudaStream_t s);
 
 constexpr int IT = 256;
 
@@ -158,13 +160,15 @@ __global__ void __launch_bounds__(IT, 8) k_ir_normb(int n, const double* __restr
     *out = s_out[0];
 }
 
+// The deposit array holds `slots` values (chain_part_slots); this product
+// uses the same grid as the chained products, so its deposits fit.
 static int ir_residual(const SellOp<double>& S, int n, const double* x, const double* b,
                        double* r, float* r32, double* part, unsigned* cnt, double* out,
-                       cudaStream_t s) {
-  const int cap = num_sms(current_device()) * 32;
-  const int g1 = S.nslice > 0 ? std::min((S.nslice + 7) / 8, cap) : 0;
+                       long long slots, cudaStream_t s) {
+  const int g1 = reducing_slice_grid(S);
   const int g2 = (S.nwarp_rows + S.ncta_rows) > 0 ? std::max((S.nwarp_rows + 7) / 8, S.ncta_rows) : 0;
   const int tot = g1 + g2;
+  if (tot > slots) return SB2_ERR_INVALID_VALUE;
   if (g1) k_ir_residual<0><<<g1, IT, 0, s>>>(S, x, b, r, r32, part, cnt, out, 0, tot);
   if (g2) k_ir_residual<1><<<g2, IT, 0, s>>>(S, x, b, r, r32, part, cnt, out, g1, tot);
   SB2_CUDA_TRY(cudaGetLastError());
@@ -190,7 +194,10 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
   const SellOp<float> S32 = sell_op32(A);
 
   // workspace: r (FP64), r32, d, inner work (3 FP32 vectors), states, deposits
-  const long long slots = std::max(chain_part_slots(S32, n), chain_part_slots(S64, n));
+  // elementwise reductions of this solver: one deposit per CTA of `ge`
+  const int ge = std::max(1, std::min((n + IT * 4 - 1) / (IT * 4), num_sms(current_device()) * 8));
+  const long long slots =
+      std::max<long long>(std::max(chain_part_slots(S32, n), chain_part_slots(S64, n)), ge + 16);
   const int hcap = std::max(prm->max_inner, 0) + 2;
   const size_t nn = (size_t)n;
   size_t off = 0;
@@ -218,7 +225,6 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
   int* dhi = (int*)(base + o_hi);
   SB2_CUDA_TRY(cudaMemsetAsync(cnt, 0, 16, s));
 
-  const int ge = std::max(1, std::min((n + IT * 4 - 1) / (IT * 4), num_sms(current_device()) * 8));
   double h_out = 0.0;
   k_ir_normb<<<ge, IT, 0, s>>>(n, b, (double*)part, cnt, dout);
   SB2_CUDA_TRY(cudaMemcpyAsync(&h_out, dout, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -231,7 +237,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
   if (prm->init_guess_null)
     k_ir_init_null<<<ge, IT, 0, s>>>(n, b, x, r, r32, (double*)part, cnt, dout);
   else
-    SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, s));
+    SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, slots, s));
   SB2_CUDA_TRY(cudaGetLastError());
   int nh = 0, inner_total = 0, outer = 0;
   double rel = 0.0;
@@ -247,21 +253,47 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
     if (!(rel < prm->tol)) {
       SB2_TRY((chain_ru_start<float, float>(S32, n, dg, d, r32, w, st, (float*)part, 1.0 / nb,
                                             prm->tol, prm->inner_tol, prm->max_inner, s)));
-      int chunk = 8;
+      // chunks of 8, 16, then 32 iterations, one queued behind the one whose
+      // state the host waits for; a pending correction turns the queued
+      // chunk into no-ops
+      ChainPipe<float> pipe;
+      SB2_TRY(pipe.init());
+      ChunkPlanner plan;
+      int chunk = 8, launched = 0;
+      auto enqueue = [&]() -> int {
+        SB2_TRY((chain_ru_enqueue<float, float>(S32, n, dg, d, r32, w, st, (float*)part, chunk, s)));
+        launched += chunk;
+        return pipe.mark(st, launched, s);
+      };
+      auto prime = [&]() -> int {
+        plan.reset();
+        chunk = 8;
+        SB2_TRY(enqueue());
+        chunk = 16;
+        return enqueue();
+      };
+      SB2_TRY(prime());
       for (;;) {
         ChainState<float> o;
-        SB2_TRY((chain_ru_iterate<float, float>(S32, n, dg, d, r32, w, st, (float*)part, chunk, s,
-                                                &o)));
+        int at = 0;
+        SB2_TRY(pipe.wait(&o, &at));
         inner_total = o.nb_iter;
-        if (!o.pending) {
-          chunk = std::min(chunk * 2, 32);
+        // every stop of the FP32 iteration sets `pending`, except breakdown
+        // #2 inside the product, which sets `done` (and `fail`)
+        if (!o.pending && !o.done && launched <= prm->max_inner + 64) {
+          // the next correction comes when ||r|| has dropped by delta
+          const double target = std::max(prm->tol, o.delta * o.rmax * o.facteur);
+          chunk = plan.next(o.nb_iter, o.reste, target, launched - at, std::min(chunk * 2, 32));
+          SB2_TRY(enqueue());
           continue;
         }
+        if (o.done) o.fail = o.fail ? o.fail : 2;
         // FP64 correction: x += d, d = 0, r = b - A x, r32 = float(r)
         k_ir_update<<<ge, IT, 0, s>>>(n, x, d, true);
-        SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, s));
+        SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, slots, s));
         SB2_CUDA_TRY(cudaMemcpyAsync(&h_out, dout, sizeof(double), cudaMemcpyDeviceToHost, s));
         SB2_CUDA_TRY(cudaStreamSynchronize(s));
+        pipe.reset();  // the stream has drained: no chunk is outstanding
         rel = std::sqrt(h_out) / nb;
         if (hist && nh < hist_cap) hist[nh] = rel;
         nh++;
@@ -270,8 +302,9 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
             !(rel == rel))
           break;
         SB2_TRY((chain_ru_resume<float, float>(S32, n, dg, d, r32, w, st, (float*)part, s)));
-        chunk = 8;
+        SB2_TRY(prime());
       }
+      SB2_CUDA_TRY(cudaStreamSynchronize(s));
     }
     res->outer_iter = outer;
     res->inner_iter = inner_total;
@@ -296,7 +329,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
     outer++;
     if (o.init_failed) break;
     k_ir_update<<<ge, IT, 0, s>>>(n, x, d, false);
-    SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, s));
+    SB2_TRY(ir_residual(S64, n, x, b, r, r32, (double*)part, cnt, dout, slots, s));
   }
   res->outer_iter = outer;
   res->inner_iter = inner_total;

@@ -101,14 +101,17 @@ __device__ __forceinline__ void sell_slice(const SellOp<VT>& S, int slice, int l
         vld4_cs(S.sval + g * 4, v[u]);
       }
     }
+    // every group's gathers are issued before the first product waits on one
+    AT xv[U][4];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (k0 + u < L) xl.gather4(c[u], xv[u]);
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (k0 + u < L) {
-        AT xv[4];
-        xl.gather4(c[u], xv);
 #pragma unroll
         for (int j = 0; j < 4; j++)
-          if (k0 + u < ln[j]) t[j] = add_rn(t[j], mul_rn(AT(v[u][j]), xv[j]));
+          if (k0 + u < ln[j]) t[j] = add_rn(t[j], mul_rn(AT(v[u][j]), xv[u][j]));
       }
     }
   }

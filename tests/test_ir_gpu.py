@@ -68,3 +68,30 @@ def test_ir_warm_start_and_edges(api):
     from seldon_b200._lib import SeldonB200Error
     with pytest.raises(SeldonB200Error):
         api.IterativeRefinement(A, X, to_dev(b), api.SorPreconditioner())
+
+
+@pytest.mark.parametrize("restarted", [False, True])
+def test_ir_large_chained(api, restarted):
+    # 128^3: the chained FP32 kernels with many slices per reduction; the true
+    # residual is recomputed here, independent of the solver's own report
+    ptr, ind, val = matgen.poisson3d(128)
+    n = ptr.size - 1
+    xs = np.random.default_rng(5).uniform(-1, 1, n)
+    b = matgen.matvec(ptr, ind, val, xs)
+    A = api.RowSparse(n, n, ptr, ind, val)
+    X = to_dev(np.zeros(n))
+    code, info = api.IterativeRefinement(A, X, to_dev(b), tol=1e-10, restarted=restarted)
+    x = to_host(X)
+    assert code == 0, info
+    rel = np.linalg.norm(b - matgen.matvec(ptr, ind, val, x)) / np.linalg.norm(b)
+    assert rel < 1e-10 and rel == pytest.approx(info["rel_residual"], rel=1e-6)
+    X64 = to_dev(np.zeros(n))
+    it = api.Iteration(20000, 1e-10)
+    it.HideMessages()
+    assert api.Cg(A, X64, to_dev(b), api.Preconditioner_Base(), it) == 0
+    nb = it.GetNumberIteration()
+    if not restarted:
+        # FP32 CG with reliable updates needs about the FP64 iteration count:
+        # not fewer (CG's optimality) and not many more
+        assert 0.9 * nb <= info["inner_iter"] <= 1.2 * nb + 10, (info["inner_iter"], nb)
+    assert np.linalg.norm(x - to_host(X64)) / np.linalg.norm(xs) < 1e-7
