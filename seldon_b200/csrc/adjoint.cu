@@ -62,7 +62,7 @@ int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* strea
   const double* src = val;
   double* tmp = nullptr;
   if (!on_device) {
-    SB2_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * nnz, s));
+    SB2_CUDA_TRY(pool_malloc((void**)&tmp, sizeof(double) * nnz, s));
     SB2_CUDA_TRY(cudaMemcpyAsync(tmp, val, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
     src = tmp;
   }

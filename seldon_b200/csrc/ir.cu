@@ -211,7 +211,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
     ~Buf() { if (p) cudaFreeAsync(p, s); }
   } buf;
   buf.s = s;
-  SB2_CUDA_TRY(cudaMallocAsync(&buf.p, off, s));
+  SB2_CUDA_TRY(pool_malloc((void**)&buf.p, off, s));
   char* base = (char*)buf.p;
   double* r = (double*)(base + o_r);
   float* r32 = (float*)(base + o_r32);
@@ -283,7 +283,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
         if (!o.pending && !o.done && launched <= prm->max_inner + 64) {
           // the next correction comes when ||r|| has dropped by delta
           const double target = std::max(prm->tol, o.delta * o.rmax * o.facteur);
-          chunk = plan.next(o.nb_iter, o.reste, target, launched - at, std::min(chunk * 2, 32));
+          chunk = plan.next(o.nb_iter, o.reste, target, launched - at, std::min(chunk * 2, 32), 4);
           SB2_TRY(enqueue());
           continue;
         }

@@ -658,13 +658,13 @@ static int alloc_scratch(cudaStream_t s, int n, int nvec, int grid, int hist_cap
                          SolveScratch* S) {
   S->vecs.s = S->state.s = s;
   const size_t vbytes = sizeof(double) * (size_t)std::max(n, 1) * nvec;
-  SB2_CUDA_TRY(cudaMallocAsync(&S->vecs.p, vbytes, s));
+  SB2_CUDA_TRY(pool_malloc((void**)&S->vecs.p, vbytes, s));
   S->vec = (double*)S->vecs.p;
   S->hist_cap = std::max(hist_cap, 1);
   const size_t sync_b = 256, part_b = sizeof(double) * kMaxRed * grid, out_b = 256;
   const size_t hist_b = sizeof(double) * S->hist_cap, hit_b = sizeof(int) * S->hist_cap;
   const size_t total = sync_b + ((part_b + 255) / 256) * 256 + out_b + ((hist_b + 255) / 256) * 256 + hit_b;
-  SB2_CUDA_TRY(cudaMallocAsync(&S->state.p, total, s));
+  SB2_CUDA_TRY(pool_malloc((void**)&S->state.p, total, s));
   char* c = (char*)S->state.p;
   S->sync = (GridSync*)c;
   c += sync_b;
@@ -1006,7 +1006,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   const int nvec = which == kCg ? 4 : (which == kBicg ? 8 : 3 + m + 1);
   DeviceBuf buf;
   buf.s = s;
-  SB2_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (size_t)std::max(n, 1) * nvec, s));
+  SB2_CUDA_TRY(pool_malloc((void**)&buf.p, sizeof(double) * (size_t)std::max(n, 1) * nvec, s));
   Ops o{A, M, s, n};
   HostIter it;
   it.tol = prm->tol;
@@ -1054,7 +1054,7 @@ static int chain_cg_solve(const sb2_csr* A, const double* diag, double* x, const
   const size_t sb = 256, pb = sizeof(double) * slots, hb = sizeof(double) * hcap, ib = sizeof(int) * hcap;
   DeviceBuf buf;
   buf.s = s;
-  SB2_CUDA_TRY(cudaMallocAsync(&buf.p, vb + sb + pb + hb + ib + 64, s));
+  SB2_CUDA_TRY(pool_malloc((void**)&buf.p, vb + sb + pb + hb + ib + 64, s));
   char* c = (char*)buf.p;
   double* work = (double*)c;
   ChainState<double>* st = (ChainState<double>*)(c + vb);

@@ -139,6 +139,9 @@ int get_red_scratch(cudaStream_t s, RedScratch** out);
 
 int current_device();
 int num_sms(int device);
+// Stream-ordered workspace allocation from the library's own memory pool
+// (freed with cudaFreeAsync).
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s);
 
 // Launch y = beta*y + alpha*A*x (overwrite: y = alpha*A*x) on a CSR operator.
 int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,

@@ -35,6 +35,42 @@ int num_sms(int device) {
   return v;
 }
 
+// Solver workspaces are allocated per call in stream order.  They come from
+// a pool owned by the library that keeps up to kPoolKeepBytes of freed memory
+// mapped for the next call; the device's default pool would unmap freed
+// blocks at each synchronization, and the next solve would pay for mapping
+// them again (milliseconds for a few hundred MB).
+static constexpr unsigned long long kPoolKeepBytes = 8ull << 30;
+
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  const int dev = current_device();
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = pools.find(dev);
+    if (it == pools.end()) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaError_t e = cudaMemPoolCreate(&pool, &props);
+      if (e != cudaSuccess) return e;
+      unsigned long long keep = kPoolKeepBytes;
+      e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        return e;
+      }
+      pools[dev] = pool;
+    } else {
+      pool = it->second;
+    }
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
 int get_red_scratch(cudaStream_t s, RedScratch** out) {
   static std::mutex mu;
   static std::map<std::pair<int, cudaStream_t>, RedScratch*> table;
