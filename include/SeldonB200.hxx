@@ -33,7 +33,13 @@
 //   SOR                                       Relaxation_MatVect.cxx:41-95, 176-298
 //   Cg / BiCgStab / Gmres                     Cg.cxx:45-116, BiCgStab.cxx:43-145,
 //                                             Gmres.cxx:44-183
+//   Conjugate (no-op for real vectors)        Functions_Vector.hxx:351
 //   JacobiPreconditioner<T>                   (absent from Seldon) z_i = r_i / A(i,i)
+//
+// Seldon's other Krylov drivers (BiCg, BiCgStabl, BiCgcr, Cgne, Cgs, CoCg,
+// Gcr, Lsqr, MinRes, QCgs, Qmr, QmrSym, Symmlq, TfQmr) need no overload: their
+// generic templates, instantiated on the device types, call only the
+// operations above, so every vector operation runs on the GPU.
 //
 // The solver overloads run the library's fused kernels when the
 // preconditioner is Preconditioner_Base, JacobiPreconditioner or
@@ -709,6 +715,11 @@ namespace Seldon
     if (X.GetM() > 0)
       b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(double) * size_t(X.GetM()),
                              b200::GetStream()), "Copy(device, host)");
+  }
+
+  //! Real vectors are their own conjugate (Functions_Vector.hxx:351).
+  inline void Conjugate(Vector<double, VectFull, CudaAlloc<double> >&)
+  {
   }
 
   //! Sum of X_i Y_i (Functions_Vector.cxx:330-346), deterministic order.

@@ -222,6 +222,48 @@ int user_solve(const std::string& solver, MatrixT& A, VectorT& x, const VectorT&
   return Gmres(A, x, b, M, iter);
 }
 
+// Every driver with the identity preconditioner (more specialised than the
+// template above, so identity-preconditioned solves come here).  Seldon's
+// other drivers are its generic templates on either type.
+template <class MatrixT, class VectorT>
+int user_solve(const std::string& solver, MatrixT& A, VectorT& x, const VectorT& b,
+               Preconditioner_Base& M, Iteration<double>& iter)
+{
+  if (solver == "cg")
+    return Cg(A, x, b, M, iter);
+  if (solver == "bicgstab")
+    return BiCgStab(A, x, b, M, iter);
+  if (solver == "gmres")
+    return Gmres(A, x, b, M, iter);
+  if (solver == "bicg")
+    return BiCg(A, x, b, M, iter);
+  if (solver == "bicgstabl")
+    return BiCgStabl(A, x, b, M, iter);
+  if (solver == "bicgcr")
+    return BiCgcr(A, x, b, M, iter);
+  if (solver == "cgne")
+    return Cgne(A, x, b, M, iter);
+  if (solver == "cgs")
+    return Cgs(A, x, b, M, iter);
+  if (solver == "cocg")
+    return CoCg(A, x, b, M, iter);
+  if (solver == "gcr")
+    return Gcr(A, x, b, M, iter);
+  if (solver == "lsqr")
+    return Lsqr(A, x, b, M, iter);
+  if (solver == "minres")
+    return MinRes(A, x, b, M, iter);
+  if (solver == "qcgs")
+    return QCgs(A, x, b, M, iter);
+  if (solver == "qmr")
+    return Qmr(A, x, b, M, iter);
+  if (solver == "qmrsym")
+    return QmrSym(A, x, b, M, iter);
+  if (solver == "symmlq")
+    return Symmlq(A, x, b, M, iter);
+  return TfQmr(A, x, b, M, iter);
+}
+
 // A preconditioner the library does not know: Seldon's generic driver runs
 // with the device types (z = r / 4 through Copy and Mlt).
 class QuarterPreconditioner
@@ -450,6 +492,42 @@ int main()
     int cd2 = Cg(Sd, xd, bd, Md, id);
     report(ch == cd2 && identical(xh, download(xd)), "cg_zero_rhs",
            fmt("codes %g/%g, x untouched", ch, cd2));
+  }
+
+  // ------------------------------------------------ Seldon's other drivers
+  // Generic templates on device types (every vector operation on the GPU)
+  // against the same templates on host types.  Dots are summed in another
+  // order than Seldon's sequential loop, so iteration counts may differ by
+  // a few.
+  {
+    const char* nonsym[] = {"bicg", "bicgstabl", "bicgcr", "cgs", "gcr", "qcgs", "qmr", "tfqmr"};
+    for (const char* name : nonsym)
+      {
+        Preconditioner_Base Mh, Md;
+        compare_solve(std::string("generic_") + name, name, Gh, Gd, b_gen, Mh, Md, 4000, 1e-10,
+                      10, 1e-6, 3);
+      }
+    const char* sym[] = {"cocg", "minres", "qmrsym", "symmlq"};
+    for (const char* name : sym)
+      {
+        Preconditioner_Base Mh, Md;
+        compare_solve(std::string("generic_") + name, name, Sh, Sd, b_sym, Mh, Md, 4000, 1e-10,
+                      10, 1e-6, 3);
+      }
+    // normal-equation drivers converge slowly: a smaller system
+    Csr small = convdiff(12, 0.8, 0.3);
+    HostGen Th;
+    to_host(small, Th);
+    DevGen Td;
+    Td.Copy(Th);
+    HostVec b_small = random_vector(Th.GetM(), 11);
+    const char* normal[] = {"cgne", "lsqr"};
+    for (const char* name : normal)
+      {
+        Preconditioner_Base Mh, Md;
+        compare_solve(std::string("generic_") + name, name, Th, Td, b_small, Mh, Md, 4000,
+                      1e-10, 10, 1e-6, 3);
+      }
   }
 
   // ------------------------------------------------ errors

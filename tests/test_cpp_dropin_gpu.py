@@ -1,6 +1,7 @@
 """C++ drop-in: Seldon user code templated on the allocator runs on Seldon's
 host types and on the CudaAlloc device types of include/SeldonB200.hxx, and
-every result is compared (tests/cpp/dropin_test.cpp)."""
+every result is compared (tests/cpp/dropin_test.cpp): SpMV, BLAS-1, the fused
+Cg/BiCgStab/Gmres, and all of Seldon's other Krylov drivers."""
 import os
 import subprocess
 
@@ -25,3 +26,7 @@ def test_cpp_dropin(cuda):
                  "gmres20_jacobi", "bicgstab_identity", "cg_user_preconditioner",
                  "cg_zero_rhs", "invalid_csr_throws"):
         assert must in names, must
+    # Seldon's other Krylov drivers, its generic templates on device types
+    for drv in ("bicg", "bicgstabl", "bicgcr", "cgne", "cgs", "cocg", "gcr", "lsqr", "minres",
+                "qcgs", "qmr", "qmrsym", "symmlq", "tfqmr"):
+        assert "generic_" + drv in names, drv
