@@ -451,8 +451,10 @@ __global__ void __launch_bounds__(CT, 4) k_rho_ru(ChainArgs<T> a) {
 
 // ----------------------------------------------------------------- host driver
 
+// Elementwise passes: at most one resident wave (4 CTAs per SM), threads
+// looping over the vector; a partial second wave would leave SMs idle.
 static int chain_elem_grid(int n) {
-  const int cap = num_sms(current_device()) * 8;
+  const int cap = num_sms(current_device()) * 4;
   return std::max(1, std::min((n + CT * 32 - 1) / (CT * 32), cap));
 }
 
