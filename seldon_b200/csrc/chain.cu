@@ -161,6 +161,8 @@ __global__ void __launch_bounds__(CT, PART == 1 ? 1 : chain_spmv_occ<VT>())
     k_spmv(ChainArgs<T> a, SellOp<VT> S, int slot0, int tot) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
+  pdl_wait();
+  pdl_release();
   if (chain_done(a.st)) return;
   if (MODE == 0) {
     EpiChainDot<T> epi{a.q, a.p, T(0)};
@@ -226,6 +228,8 @@ __device__ __forceinline__ bool aligned16(const void* p) {
 // p = z (first iteration) | p = beta*p + z: Mlt(beta, p); Add(1, z, p).
 template <typename T>
 __global__ void __launch_bounds__(CT, 4) k_p(ChainArgs<T> a) {
+  pdl_wait();
+  pdl_release();
   if (chain_done(a.st)) return;
   const bool first = (a.st->nb_iter == 0);
   const T beta = a.st->beta;
@@ -265,6 +269,8 @@ template <typename T>
 __global__ void __launch_bounds__(CT, 4) k_x(ChainArgs<T> a) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
+  pdl_wait();
+  pdl_release();
   if (chain_done(a.st)) return;
   const T alpha = a.st->alpha;
   T* __restrict__ x = a.x;
@@ -340,6 +346,8 @@ template <typename T>
 __global__ void __launch_bounds__(CT, 4) k_x_ru(ChainArgs<T> a) {
   __shared__ T s_red[CT / 32];
   __shared__ T s_out[2];
+  pdl_wait();
+  pdl_release();
   if (chain_done(a.st)) return;
   const T alpha = a.st->alpha;
   T* __restrict__ x = a.x;
@@ -468,6 +476,24 @@ int reducing_slice_grid(const SellOp<VT>& S) {
   return std::min((S.nslice + 7) / 8, cap);
 }
 
+// Launch of an iteration kernel with programmatic stream serialization: it
+// is scheduled while the previous kernel drains and waits (pdl_wait) for its
+// results, which hides the launch latency between the passes.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*k)(KArgs...), int grid, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(CT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <typename T, typename VT>
 static int launch_spmv_pair(int mode, const ChainArgs<T>& a, const SellOp<VT>& S,
                             cudaStream_t s) {
@@ -476,8 +502,8 @@ static int launch_spmv_pair(int mode, const ChainArgs<T>& a, const SellOp<VT>& S
   const int tot = g1 + g2;
   if (tot == 0) return SB2_ERR_NOT_SUPPORTED;
   if (mode == 0) {
-    if (g1) k_spmv<T, VT, 0, 0><<<g1, CT, 0, s>>>(a, S, 0, tot);
-    if (g2) k_spmv<T, VT, 0, 1><<<g2, CT, 0, s>>>(a, S, g1, tot);
+    if (g1) SB2_CUDA_TRY(launch_pdl(k_spmv<T, VT, 0, 0>, g1, s, a, S, 0, tot));
+    if (g2) SB2_CUDA_TRY(launch_pdl(k_spmv<T, VT, 0, 1>, g2, s, a, S, g1, tot));
   } else {
     if (g1) k_spmv<T, VT, 1, 0><<<g1, CT, 0, s>>>(a, S, 0, tot);
     if (g2) k_spmv<T, VT, 1, 1><<<g2, CT, 0, s>>>(a, S, g1, tot);
@@ -520,9 +546,9 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
   int launched = 0, chunk = 8;
   auto enqueue = [&]() -> int {
     for (int c = 0; c < chunk; c++) {
-      k_p<T><<<ge, CT, 0, s>>>(a);
+      SB2_CUDA_TRY(launch_pdl(k_p<T>, ge, s, a));
       SB2_TRY((launch_spmv_pair<T, VT>(0, a, S, s)));
-      k_x<T><<<ge, CT, 0, s>>>(a);
+      SB2_CUDA_TRY(launch_pdl(k_x<T>, ge, s, a));
     }
     SB2_CUDA_TRY(cudaGetLastError());
     launched += chunk;
@@ -583,9 +609,9 @@ int chain_ru_enqueue(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* w
   ChainArgs<T> a{n, nullptr, x, r, work, work + n, diag, st, part, nullptr, nullptr};
   const int ge = chain_elem_grid(n);
   for (int c = 0; c < chunk; c++) {
-    k_p<T><<<ge, CT, 0, s>>>(a);
+    SB2_CUDA_TRY(launch_pdl(k_p<T>, ge, s, a));
     SB2_TRY((launch_spmv_pair<T, VT>(0, a, S, s)));
-    k_x_ru<T><<<ge, CT, 0, s>>>(a);
+    SB2_CUDA_TRY(launch_pdl(k_x_ru<T>, ge, s, a));
   }
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;

@@ -209,6 +209,17 @@ __device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned* p, unsigned v)
   return old;
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the previous kernel of its stream finishes:
+// pdl_wait() blocks until that kernel has completed and its writes are
+// visible (a no-op without the launch attribute); pdl_release() lets the
+// next kernel of the stream be scheduled once every CTA of this grid has
+// called it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Streaming loads of the matrix (read once per product: evict first).
 __device__ __forceinline__ int4 ld_stream_int4(const int* p) {
   return __ldcs(reinterpret_cast<const int4*>(p));
