@@ -282,7 +282,13 @@ def run_ours(args, rank, world, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         # the same workload before and after the timed region, so the sampler
-        # (100 ms period) sees the clocks the timed region ran at
+        # (100 ms period) sees the clocks the timed region ran at; nvidia-smi
+        # takes a while to start, so the load runs until it reports (3 s at
+        # most) and 0.4 s beyond
+        first_until = time.time() + 3.0
+        while time.time() < first_until and len(clk.lines) < 2:
+            graph.replay()
+            torch.cuda.synchronize()
         soak_until = time.time() + 0.4
         while time.time() < soak_until:
             graph.replay()
