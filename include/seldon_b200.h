@@ -364,9 +364,10 @@ int sb2_batch_set_threads(sb2_batch* B, int threads);
 int sb2_batch_get_threads(const sb2_batch* B);
 
 /* Size from which Cg runs as a chain of full-occupancy kernels (one per
- * pass, scalars in device memory) instead of one persistent kernel; chosen
- * by the autotuner, default 200000 rows.  Returns the previous value.  No
- * counterpart in the reference (a tuning knob of this engine). */
+ * pass, scalars in device memory) instead of one persistent kernel.  The
+ * default, 2800000 rows, is where the two cross on 7-point Poisson matrices
+ * on a B200.  Returns the previous value.  No counterpart in the reference
+ * (a tuning knob of this engine). */
 int sb2_krylov_set_config(int chain_min_n);
 
 /* Device-side wait limit for the fused solvers' grid barriers, in

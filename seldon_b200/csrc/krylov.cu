@@ -1039,9 +1039,12 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
              int max_iter, int init_guess_null, cudaStream_t s, ChainState<T>* out);
 
 // Systems at least this large run CG as a chain of full-occupancy kernels;
-// smaller ones as one persistent kernel (latency-bound, barriers are cheap).
-// Set by the autotuner (sb2_krylov_set_config).
-static int g_chain_min_n = 200000;
+// smaller ones as one persistent kernel, where an iteration is latency-bound
+// and grid barriers cost less than launches.  On a B200 the two cross near
+// 3e6 rows (7-point Poisson: persistent 70.6 us/iteration against 87.2 at
+// 2.1e6 rows, equal at 3.0e6, chained 213 against 249 at 7.1e6).
+// sb2_krylov_set_config changes it.
+static int g_chain_min_n = 2800000;
 
 static int chain_cg_solve(const sb2_csr* A, const double* diag, double* x, const double* b,
                           const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
