@@ -233,6 +233,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def job_throughput(ms_local, bytes_per_step, world, device=None):
+    """Whole-job throughput of `world` replicas, one per GPU: the per-step
+    time is the maximum over ranks (the slowest replica sets the job's pace)
+    and the bytes of all ranks add up.  Every rank calls this (it runs an
+    all-reduce when world > 1).  Returns (GB/s, max ms per step)."""
+    ms_max = float(ms_local)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms_max], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    return world * bytes_per_step / (ms_max * 1e-3) / 1e9, ms_max
+
+
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -303,12 +318,7 @@ def run_ours(args, rank, world, local):
             torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * B / (ms_max * 1e-3) / 1e9
+    value, ms_max = job_throughput(ms, B, world, dev)
     kernel_gbs = B / (ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
 
@@ -328,12 +338,7 @@ def run_ours(args, rank, world, local):
                        ctypes.c_void_p(yh.data_ptr()), sp)
     ev1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * B / (e2e_ms * 1e-3) / 1e9
+    e2e, e2e_ms = job_throughput(ev0.elapsed_time(ev1) / args.steps, B, world, dev)
     ok = np.allclose(yh.numpy(), y.cpu().numpy(), rtol=0, atol=0)
 
     extras = {}
