@@ -125,6 +125,17 @@ int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
 int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
                  const double* x_host, double* y_host, void* stream);
 
+/* Mlt over a batch of HOST vectors: y_i = alpha*op(A)*x_i for i < count, with
+ * x_host holding count vectors of op(A)'s column size back to back and
+ * y_host count vectors of its row size.  The copies in and out and the
+ * products are pipelined (copy of x_{i+1}, product i and copy of y_{i-1}
+ * overlap); pinned host memory lets the copies run asynchronously.  Returns
+ * after every y_i is on the host.  Each y_i is the same bits as sb2_mlt_host
+ * on x_i.  No reference counterpart: the reference calls Mlt once per
+ * vector (Functions_MatVect.cxx:72-83). */
+int sb2_mlt_host_batch(const sb2_csr* A, int trans, double alpha, int count,
+                       const double* x_host, double* y_host, void* stream);
+
 /* Product algorithm and launch configuration, chosen by the autotuner; no
  * counterpart in the reference (tuning knobs of this engine).
  *   algo     SB2_SPMV_SELL   binned SELL-32 (thread/warp/CTA per row), default

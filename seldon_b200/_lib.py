@@ -137,6 +137,8 @@ _PROTOS = [
      [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, ctypes.c_double, c_void_p, c_void_p]),
     ("sb2_mlt_host", ctypes.c_int,
      [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    ("sb2_mlt_host_batch", ctypes.c_int,
+     [c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
     ("sb2_spmv_set_config", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("sb2_krylov_set_config", ctypes.c_int, [ctypes.c_int]),
     ("sb2_dot", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_double_p, c_void_p]),

@@ -131,6 +131,32 @@ def Mlt(*args, trans=SeldonNoTrans, stream=None):
                      _dev_ptr(Y, ny, "Y"), _stream(stream)), "Mlt")
 
 
+def MltHostBatch(A, X, Y, alpha=1.0, trans=SeldonNoTrans, stream=None):
+    """Y[i] = alpha*op(A)*X[i] for host arrays X (count x cols of op(A)) and
+    Y (count x rows), C-contiguous float64 (numpy arrays or CPU tensors;
+    pinned memory lets the copies overlap the products).  Each Y[i] is the
+    same bits as Mlt on X[i]."""
+    import numpy as np
+    nx, ny = (A.m, A.n) if trans else (A.n, A.m)
+
+    def host_ptr(a, cols, name):
+        if hasattr(a, "data_ptr"):
+            if a.is_cuda or a.dtype.itemsize != 8 or not a.is_contiguous():
+                raise ValueError(f"{name}: a contiguous CPU float64 tensor is required")
+            count = a.numel() // max(cols, 1) if cols else a.shape[0]
+            return ctypes.c_void_p(a.data_ptr()), a.numel(), count
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+            raise ValueError(f"{name}: a C-contiguous float64 array is required")
+        count = a.size // max(cols, 1) if cols else a.shape[0]
+        return ctypes.c_void_p(a.ctypes.data), a.size, count
+    px, sx, count = host_ptr(X, nx, "X")
+    py, sy, _ = host_ptr(Y, ny, "Y")
+    if sx != count * nx or sy != count * ny:
+        raise ValueError("X and Y must hold the same number of vectors of op(A)'s sizes")
+    check(_L.sb2_mlt_host_batch(A.handle, int(trans), float(alpha), count, px, py,
+                                _stream(stream)), "MltHostBatch")
+
+
 def DotProd(X, Y, stream=None):
     out = ctypes.c_double()
     check(_L.sb2_dot(X.numel(), _dev_ptr(X), _dev_ptr(Y, X.numel(), "Y"), ctypes.byref(out),

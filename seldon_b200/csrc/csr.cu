@@ -417,6 +417,15 @@ int sb2_csr_destroy(sb2_csr* A) {
   cudaFree(A->d_diag32);
   cudaFree(A->d_hx);
   cudaFree(A->d_hy);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(A->d_bx[i]);
+    cudaFree(A->d_by[i]);
+    if (A->e_in[i]) cudaEventDestroy(A->e_in[i]);
+    if (A->e_kern[i]) cudaEventDestroy(A->e_kern[i]);
+    if (A->e_out[i]) cudaEventDestroy(A->e_out[i]);
+  }
+  if (A->s_in) cudaStreamDestroy(A->s_in);
+  if (A->s_out) cudaStreamDestroy(A->s_out);
   cudaSetDevice(prev);
   delete A;
   return SB2_OK;

@@ -108,6 +108,12 @@ struct sb2_csr {
   double* d_hx = nullptr;
   double* d_hy = nullptr;
   std::mutex host_mu;        // one host-buffer product at a time per matrix
+  // pipelined host-buffer batches (lazy): two buffers per side, copy streams
+  double* d_bx[2] = {nullptr, nullptr};
+  double* d_by[2] = {nullptr, nullptr};
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t e_in[2] = {nullptr, nullptr}, e_kern[2] = {nullptr, nullptr},
+              e_out[2] = {nullptr, nullptr};
 };
 
 namespace sb2 {

@@ -262,4 +262,57 @@ int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
                           (cudaStream_t)stream);
 }
 
+// y_i = alpha*op(A)*x_i for a batch of host vectors.  Two device buffers per
+// side and two copy streams: the copy of x_{i+1} in, the product i and the
+// copy of y_{i-1} out run at the same time (host-to-device and
+// device-to-host transfers use separate copy engines).  Events order the
+// reuse of each buffer: x into buffer b waits for the product that last read
+// it, the product into y buffer b waits for the copy out that last read it.
+int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
+                       const double* x_host, double* y_host, void* stream) {
+  if (!cA || count < 0) return SB2_ERR_INVALID_VALUE;
+  sb2_csr* A = const_cast<sb2_csr*>(cA);
+  const int nx = trans ? A->m : A->n, ny = trans ? A->n : A->m;
+  if (count == 0) return SB2_OK;
+  if ((nx > 0 && !x_host) || (ny > 0 && !y_host)) return SB2_ERR_INVALID_VALUE;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> g(A->host_mu);
+  const size_t len = (size_t)std::max(std::max(A->m, A->n), 1);
+  if (!A->s_in) {
+    for (int i = 0; i < 2; i++) {
+      SB2_CUDA_TRY(cudaMalloc(&A->d_bx[i], sizeof(double) * len));
+      SB2_CUDA_TRY(cudaMalloc(&A->d_by[i], sizeof(double) * len));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_in[i], cudaEventDisableTiming));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_kern[i], cudaEventDisableTiming));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_out[i], cudaEventDisableTiming));
+    }
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_out, cudaStreamNonBlocking));
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_in, cudaStreamNonBlocking));
+  }
+  // the copy streams start after the work already queued on the caller's stream
+  SB2_CUDA_TRY(cudaEventRecord(A->e_kern[0], s));
+  SB2_CUDA_TRY(cudaStreamWaitEvent(A->s_in, A->e_kern[0], 0));
+  SB2_CUDA_TRY(cudaStreamWaitEvent(A->s_out, A->e_kern[0], 0));
+  for (int i = 0; i < count; i++) {
+    const int b = i & 1;
+    if (i >= 2) SB2_CUDA_TRY(cudaStreamWaitEvent(A->s_in, A->e_kern[b], 0));
+    if (nx > 0)
+      SB2_CUDA_TRY(cudaMemcpyAsync(A->d_bx[b], x_host + (size_t)i * nx, sizeof(double) * nx,
+                                   cudaMemcpyHostToDevice, A->s_in));
+    SB2_CUDA_TRY(cudaEventRecord(A->e_in[b], A->s_in));
+    SB2_CUDA_TRY(cudaStreamWaitEvent(s, A->e_in[b], 0));
+    if (i >= 2) SB2_CUDA_TRY(cudaStreamWaitEvent(s, A->e_out[b], 0));
+    SB2_TRY(spmv_common(A, trans, alpha, A->d_bx[b], 0.0, A->d_by[b], true, s));
+    SB2_CUDA_TRY(cudaEventRecord(A->e_kern[b], s));
+    SB2_CUDA_TRY(cudaStreamWaitEvent(A->s_out, A->e_kern[b], 0));
+    if (ny > 0)
+      SB2_CUDA_TRY(cudaMemcpyAsync(y_host + (size_t)i * ny, A->d_by[b], sizeof(double) * ny,
+                                   cudaMemcpyDeviceToHost, A->s_out));
+    SB2_CUDA_TRY(cudaEventRecord(A->e_out[b], A->s_out));
+  }
+  // every product and every copy out has completed when s_out has
+  SB2_CUDA_TRY(cudaStreamSynchronize(A->s_out));
+  return SB2_OK;
+}
+
 }  // extern "C"

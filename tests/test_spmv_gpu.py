@@ -178,3 +178,28 @@ def test_blas1(api, oracle, n):
     assert np.array_equal(to_host(Z), to_host(Y))
     api.Add(0.0, to_dev(np.full(n, np.nan)), Z)  # alpha == 0 is a no-op
     assert not np.isnan(to_host(Z)).any()
+
+
+@pytest.mark.parametrize("case", ["conv_12", "rand_rect"])
+@pytest.mark.parametrize("trans", [0, 1])
+@pytest.mark.parametrize("count,pinned", [(1, False), (2, True), (3, False), (5, True)])
+def test_mlt_host_batch(api, case, trans, count, pinned):
+    # pipelined host-buffer batch: every Y[i] is the same bits as the
+    # single-vector product on the device
+    import torch
+    (ptr, ind, val), m, n = CASES[case]()
+    A = api.RowSparse(m, n, ptr, ind, val)
+    nx, ny = (m, n) if trans else (n, m)
+    rng = np.random.default_rng(31 + count)
+    X = rng.standard_normal((count, nx))
+    if pinned:
+        Xh = torch.from_numpy(X).pin_memory()
+        Yh = torch.full((count, ny), np.nan, dtype=torch.float64).pin_memory()
+    else:
+        Xh, Yh = X, np.full((count, ny), np.nan)
+    api.MltHostBatch(A, Xh, Yh, alpha=-0.75, trans=trans)
+    Y = Yh.numpy() if pinned else Yh
+    for i in range(count):
+        Z = to_dev(np.zeros(ny))
+        api.Mlt(-0.75, A, to_dev(X[i]), Z, trans=trans)
+        assert np.array_equal(Y[i], to_host(Z)), i
