@@ -381,6 +381,15 @@ int sb2_batch_get_threads(const sb2_batch* B);
  * (a tuning knob of this engine). */
 int sb2_krylov_set_config(int chain_min_n);
 
+/* Cluster-resident CG (on by default): a system whose matrix and vectors fit
+ * the shared memory of one thread-block cluster (up to 16 CTAs on 16 SMs)
+ * runs Cg inside that cluster, exchanging data through distributed shared
+ * memory and synchronizing with hardware cluster barriers; the arithmetic is
+ * the same as the persistent kernel's.  0 turns it off (the persistent
+ * kernel runs instead).  Returns the previous setting.  No counterpart in
+ * the reference (a tuning knob of this engine). */
+int sb2_krylov_set_cluster(int on);
+
 /* Device-side wait limit for the fused solvers' grid barriers, in
  * milliseconds (default 2000).  Returns the previous value. */
 int sb2_set_wait_limit_ms(int ms);

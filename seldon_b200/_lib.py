@@ -141,6 +141,7 @@ _PROTOS = [
      [c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
     ("sb2_spmv_set_config", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("sb2_krylov_set_config", ctypes.c_int, [ctypes.c_int]),
+    ("sb2_krylov_set_cluster", ctypes.c_int, [ctypes.c_int]),
     ("sb2_dot", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_double_p, c_void_p]),
     ("sb2_nrm2", ctypes.c_int, [ctypes.c_int, c_void_p, c_double_p, c_void_p]),
     ("sb2_dot_device", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -14,6 +14,8 @@
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Iterative.cxx:235-354.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -1045,6 +1047,274 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
 // 2.1e6 rows, equal at 3.0e6, chained 213 against 249 at 7.1e6).
 // sb2_krylov_set_config changes it.
 static int g_chain_min_n = 2800000;
+// Systems that fit one thread-block cluster's shared memory run CG there.
+static int g_cluster_cg = 1;
+
+// ----------------------------------------------------------------- cluster-resident CG
+//
+// Small systems: the whole solve in one thread-block cluster (up to 16 CTAs on
+// 16 SMs).  Each CTA keeps its block of rows of the matrix and its slice of
+// every vector in shared memory; the product reads the other CTAs' slices of
+// p through distributed shared memory, and the reductions exchange per-CTA
+// partials through it after a hardware cluster barrier.  Every CTA sums the
+// partials in rank order, so all of them take the same (deterministic)
+// decisions.  The arithmetic is cg_fused_kernel's, step for step (Cg.cxx:
+// 45-116): each row summed in stored order, the same fused reductions.
+
+constexpr int NTC = 512;           // threads per CTA of the cluster kernel
+constexpr int kClusterMaxRanks = 16;
+
+struct ClusterCgArgs {
+  const int* ptr;
+  const int* ind;
+  const double* val;
+  const double* diag;  // nullptr: identity, else Jacobi
+  const double* b;
+  double* x;
+  int n, rpc, nnz_max;  // rows per CTA, largest slice
+  IterArgs it;
+  History H;
+  SolveOut* out;
+};
+
+__global__ void __launch_bounds__(NTC, 1) cg_cluster_kernel(ClusterCgArgs a) {
+  namespace cgr = cooperative_groups;
+  cgr::cluster_group cl = cgr::this_cluster();
+  const int rank = (int)cl.block_rank(), C = (int)cl.num_blocks();
+  const int tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double s_red[NTC / 32];
+  __shared__ double s_bc[2];
+  // shared layout (the same offsets in every CTA)
+  double* sval = reinterpret_cast<double*>(smem);
+  double* xv = sval + a.nnz_max;
+  double* rv = xv + a.rpc;
+  double* pv = rv + a.rpc;
+  double* qv = pv + a.rpc;
+  double* dg = qv + a.rpc;
+  double* red = dg + a.rpc;  // [2 phases][2 values]
+  int* sidx = reinterpret_cast<int*>(red + 4);  // packed (owner << 24 | local row)
+  int* lptr = sidx + a.nnz_max;
+  const int r0 = rank * a.rpc;
+  const int nr = max(0, min(a.n, r0 + a.rpc) - r0);
+  const int e0 = nr > 0 ? __ldg(a.ptr + r0) : 0;
+  for (int i = tid; i <= nr; i += NTC) lptr[i] = nr > 0 ? __ldg(a.ptr + r0 + i) - e0 : 0;
+  __syncthreads();
+  const int nnz_l = lptr[nr];
+  for (int k = tid; k < nnz_l; k += NTC) {
+    const int j = __ldg(a.ind + e0 + k);
+    const int q = j / a.rpc;
+    sval[k] = __ldg(a.val + e0 + k);
+    sidx[k] = (q << 24) | (j - q * a.rpc);
+  }
+  for (int i = tid; i < nr; i += NTC) {
+    dg[i] = a.diag ? __ldg(a.diag + r0 + i) : 1.0;
+    xv[i] = a.it.init_guess_null ? 0.0 : a.x[r0 + i];
+  }
+  int phase = 0;
+  // sum of two per-thread values over the cluster, the same in every CTA
+  auto reduce = [&](double v0, double v1, double& o0, double& o1) {
+    v0 = block_sum<NTC>(v0, s_red);
+    v1 = block_sum<NTC>(v1, s_red);
+    double* slot = red + 2 * phase;
+    if (tid == 0) {
+      slot[0] = v0;
+      slot[1] = v1;
+    }
+    cl.sync();
+    if (tid == 0) {
+      double t0 = 0.0, t1 = 0.0;
+      for (int q = 0; q < C; q++) {
+        const double* rs = cl.map_shared_rank(slot, q);
+        t0 = add_rn(t0, rs[0]);
+        t1 = add_rn(t1, rs[1]);
+      }
+      s_bc[0] = t0;
+      s_bc[1] = t1;
+    }
+    __syncthreads();
+    o0 = s_bc[0];
+    o1 = s_bc[1];
+    phase ^= 1;
+  };
+  // row i of A times the vector whose local slices are `vec`
+  auto row_dot = [&](const double* vec, int i) {
+    double t = 0.0;
+    for (int k = lptr[i]; k < lptr[i + 1]; k++) {
+      const int w = sidx[k];
+      const int q = w >> 24, jj = w & 0xffffff;
+      const double xj = (q == rank) ? vec[jj] : *cl.map_shared_rank(vec + jj, q);
+      t = add_rn(t, mul_rn(sval[k], xj));
+    }
+    return t;
+  };
+  auto zval = [&](int i, double r) { return a.diag ? __ddiv_rn(r, dg[i]) : r; };
+  const bool lead = (rank == 0 && tid == 0);
+  int hlen = 0;
+
+  // iter.Init(b): facteur_reste = 1/||b|| (Iterative.cxx:235-249)
+  double acc = 0.0, unused;
+  for (int i = tid; i < nr; i += NTC) {
+    const double bi = __ldg(a.b + r0 + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  cl.sync();  // every slice is in place before any CTA reads another's
+  double nb2;
+  reduce(acc, 0.0, nb2, unused);
+  const double normb = sqrt(nb2);
+  if (normb == 0.0) {
+    if (lead) {
+      a.out->init_failed = 1;
+      a.out->hist_len = 0;
+    }
+    cl.sync();
+    return;
+  }
+  const double facteur = 1.0 / normb;
+  // r = b - A x (or r = b with x = 0), with ||r||^2 and (r, z)
+  double rr = 0.0, rz = 0.0;
+  for (int i = tid; i < nr; i += NTC) {
+    const double bi = __ldg(a.b + r0 + i);
+    const double ri = a.it.init_guess_null ? bi : add_rn(bi, -row_dot(xv, i));
+    rv[i] = ri;
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rz = add_rn(rz, mul_rn(ri, zval(i, ri)));
+  }
+  reduce(rr, rz, rr, rz);
+  double rho = rz, rho_1 = 1.0, reste;
+  int nb_iter = 0, fail = 0;
+  for (;;) {
+    // while (!iter.Finished(r))
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(a.H, &hlen, nb_iter, reste);
+    if (reste < a.it.tol || nb_iter >= a.it.max_iter) break;
+    if (rho == 0.0) {
+      fail = 1;
+      break;
+    }
+    // p = z (first) | p = beta*p + z
+    const double beta = rho / rho_1;
+    for (int i = tid; i < nr; i += NTC) {
+      const double z = zval(i, rv[i]);
+      pv[i] = nb_iter == 0 ? z : add_rn(mul_rn(pv[i], beta), z);
+    }
+    cl.sync();  // p complete in every CTA before the product reads it
+    // q = A p fused with delta = (p, q)
+    double d = 0.0;
+    for (int i = tid; i < nr; i += NTC) {
+      const double t = row_dot(pv, i);
+      qv[i] = t;
+      d = add_rn(d, mul_rn(pv[i], t));
+    }
+    double delta;
+    reduce(d, 0.0, delta, unused);
+    if (delta == 0.0) {
+      fail = 2;
+      break;
+    }
+    const double alpha = rho / delta;
+    rr = 0.0;
+    rz = 0.0;
+    for (int i = tid; i < nr; i += NTC) {
+      if (alpha != 0.0) xv[i] = add_rn(xv[i], mul_rn(alpha, pv[i]));
+      double ri = rv[i];
+      if (-alpha != 0.0) {
+        ri = add_rn(ri, mul_rn(-alpha, qv[i]));
+        rv[i] = ri;
+      }
+      rr = add_rn(rr, mul_rn(ri, ri));
+      rz = add_rn(rz, mul_rn(ri, zval(i, ri)));
+    }
+    reduce(rr, rz, rr, rz);
+    rho_1 = rho;
+    rho = rz;
+    nb_iter++;
+  }
+  for (int i = tid; i < nr; i += NTC) a.x[r0 + i] = xv[i];
+  if (lead) write_out(a.out, nb_iter, a.it.max_iter, fail, facteur, reste, hlen);
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Shared memory of one CTA for `rpc` rows and a largest slice of `nnz_max`.
+static size_t cluster_smem(int rpc, int nnz_max) {
+  return sizeof(double) * ((size_t)nnz_max + 5 * (size_t)rpc + 4) +
+         sizeof(int) * ((size_t)nnz_max + (size_t)rpc + 1);
+}
+
+// Plan (ranks, rows per CTA, largest slice) for A, from its row pointer;
+// ranks = 0 when A does not fit one cluster.
+static int cluster_plan(const sb2_csr* A, int* ranks, int* rpc, int* nnz_max) {
+  sb2_csr* M = const_cast<sb2_csr*>(A);
+  std::lock_guard<std::mutex> g(M->mu);
+  if (M->cl_ranks < 0) {
+    M->cl_ranks = 0;
+    const int n = A->m;
+    if (n >= 256 && n <= kClusterMaxRanks * 4096) {
+      std::vector<int> ptr(n + 1);
+      SB2_CUDA_TRY(cudaMemcpy(ptr.data(), A->full.d_ptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+      int dev_smem = 0;
+      cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, current_device());
+      const size_t limit = (size_t)std::max(dev_smem - 1024, 0);  // static shared memory
+      for (int c = kClusterMaxRanks; c >= 2; c /= 2) {
+        const int r = (n + c - 1) / c;
+        int mx = 0;
+        for (int q = 0; q < c; q++) {
+          const int a0 = std::min(n, q * r), a1 = std::min(n, (q + 1) * r);
+          mx = std::max(mx, ptr[a1] - ptr[a0]);
+        }
+        if (r < (1 << 24) && cluster_smem(r, mx) <= limit) {
+          // the most SMs whose shared memory holds the system
+          M->cl_ranks = c;
+          M->cl_rpc = r;
+          M->cl_nnz_max = mx;
+          break;
+        }
+      }
+    }
+  }
+  *ranks = M->cl_ranks;
+  *rpc = M->cl_rpc;
+  *nnz_max = M->cl_nnz_max;
+  return SB2_OK;
+}
+
+static int cluster_cg_solve(const sb2_csr* A, const double* diag, double* x, const double* b,
+                            const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
+                            int* hist_it, int hist_cap, cudaStream_t s) {
+  int C = 0, rpc = 0, nnz_max = 0;
+  SB2_TRY(cluster_plan(A, &C, &rpc, &nnz_max));
+  if (C < 2) return SB2_ERR_NOT_SUPPORTED;
+  const size_t smem = cluster_smem(rpc, nnz_max);
+  SB2_CUDA_TRY(cudaFuncSetAttribute(cg_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  SB2_CUDA_TRY(cudaFuncSetAttribute(cg_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(NTC);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, cg_cluster_kernel, &cfg) != cudaSuccess ||
+      clusters < 1) {
+    cudaGetLastError();
+    return SB2_ERR_NOT_SUPPORTED;
+  }
+  SolveScratch S;
+  const int hcap = std::max(hist_cap, 0) + 1;
+  SB2_TRY(alloc_scratch(s, A->m, 0, 1, hcap, &S));
+  ClusterCgArgs args{A->full.d_ptr, A->full.d_ind, A->full.d_val, diag, b, x, A->m, rpc, nnz_max,
+                     IterArgs{prm->tol, prm->max_iter, 1, prm->init_guess_null},
+                     History{S.hist, S.hist_it, hcap}, S.out};
+  SB2_CUDA_TRY(cudaLaunchKernelEx(&cfg, cg_cluster_kernel, args));
+  return finish_solve(S, s, res, hist, hist_it, hcap - 1 > 0 ? hcap - 1 : 0, prm->max_iter);
+}
 
 static int chain_cg_solve(const sb2_csr* A, const double* diag, double* x, const double* b,
                           const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
@@ -1099,6 +1369,10 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   }
   if (which == kCg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
     return chain_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
+  if (which == kCg && g_cluster_cg) {
+    const int st = cluster_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
+    if (st != SB2_ERR_NOT_SUPPORTED) return st;
+  }
   return fused_solve(which, A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
 }
 
@@ -1107,6 +1381,12 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
 using namespace sb2;
 
 extern "C" {
+
+int sb2_krylov_set_cluster(int on) {
+  const int old = g_cluster_cg;
+  g_cluster_cg = on ? 1 : 0;
+  return old;
+}
 
 int sb2_krylov_set_config(int chain_min_n) {
   if (chain_min_n < 0) return SB2_ERR_INVALID_VALUE;

@@ -317,3 +317,78 @@ def test_chain_cg_large_vs_oracle(api, oracle):
     assert api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it) == co == 0
     assert abs(it.GetNumberIteration() - no) <= max(2, no // 50)
     assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-5
+
+
+# ------------------------------------------------------------------ cluster-resident CG
+
+def _cluster_case(mat):
+    if mat == "lap60":
+        return matgen.lap2d(60)
+    if mat == "poisson20":
+        return matgen.poisson3d(20)
+    if mat == "lap_odd":
+        return matgen.lap2d(37, shift=0.3)
+    return matgen.lap2d(50)
+
+
+@pytest.mark.parametrize("mat,pc,warm", [("lap60", 0, False), ("lap60", 1, True),
+                                         ("poisson20", 1, False), ("lap_odd", 0, True),
+                                         ("sym_up", 0, False)])
+def test_cluster_cg_matches_persistent(api, oracle, mat, pc, warm):
+    # small systems run CG inside one thread-block cluster (shared and
+    # distributed shared memory); the persistent kernel is the other path:
+    # same stopping rule, iterations within the reduction-order slack,
+    # solutions within the parity bound, both against the oracle
+    from seldon_b200 import _lib
+    L = _lib.load()
+    ptr, ind, val = _cluster_case(mat)
+    n = ptr.size - 1
+    rng = np.random.default_rng(7)
+    b = matgen.matvec(ptr, ind, val, rng.uniform(-1, 1, n))
+    x0 = rng.uniform(-1, 1, n) if warm else np.zeros(n)
+    A = api.RowSymSparse(n, *matgen.upper(ptr, ind, val)) if mat == "sym_up" else \
+        api.RowSparse(n, n, ptr, ind, val)
+    out = {}
+    for on in (1, 0):
+        old = L.sb2_krylov_set_cluster(on)
+        try:
+            X = to_dev(x0)
+            it = api.Iteration(3000, 1e-10)
+            it.HideMessages()
+            it.SetInitGuess(not warm)
+            code = api.Cg(A, X, to_dev(b), _precond(api, pc), it)
+        finally:
+            L.sb2_krylov_set_cluster(old)
+        out[on] = (code, it.GetNumberIteration(), to_host(X), [r for _, r in it.history])
+    (c1, n1, x1, h1), (c0, n0, x0_, h0) = out[1], out[0]
+    assert c1 == c0 == 0
+    assert abs(n1 - n0) <= 2, (n1, n0)
+    assert h1[0] == pytest.approx(h0[0], rel=1e-13)
+    assert np.linalg.norm(x1 - x0_) / np.linalg.norm(x0_) < 1e-8
+    for xx in (x1, x0_):
+        r = b - matgen.matvec(ptr, ind, val, xx)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 50 * 1e-10
+    _, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b, x0=x0 if warm else None, precond=pc,
+                                   tol=1e-10, max_iter=3000)
+    assert co == 0 and abs(n1 - no) <= max(2, int(0.05 * no)), (n1, no)
+
+
+def test_cluster_cg_edges(api):
+    # zero right-hand side (x untouched, code 0) and a max_iter stop (-2),
+    # on a system small enough for the cluster path
+    ptr, ind, val = matgen.lap2d(40)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    x0 = np.arange(n, dtype=float)
+    X = to_dev(x0)
+    it = api.Iteration(100, 1e-10)
+    it.HideMessages()
+    it.SetInitGuess(False)
+    assert api.Cg(A, X, to_dev(np.zeros(n)), api.Preconditioner_Base(), it) == 0
+    assert np.array_equal(to_host(X), x0)
+    b = matgen.matvec(ptr, ind, val, np.ones(n))
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(7, 1e-14)
+    it.HideMessages()
+    assert api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it) == -2
+    assert it.GetNumberIteration() == 7
