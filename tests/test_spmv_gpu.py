@@ -203,3 +203,32 @@ def test_mlt_host_batch(api, case, trans, count, pinned):
         Z = to_dev(np.zeros(ny))
         api.Mlt(-0.75, A, to_dev(X[i]), Z, trans=trans)
         assert np.array_equal(Y[i], to_host(Z)), i
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("algo,threads,stages", [(1, 256, 4), (2, 256, 3), (2, 256, 4),
+                                                 (2, 512, 3), (2, 512, 4)])
+def test_spmv_engines(api, oracle, case, algo, threads, stages):
+    # the other product engines sb2_spmv_set_config selects (row-block stream
+    # kernel; TMA bulk-copy ring with 256/512 threads and 3/4 stages) against
+    # the oracle, MltAdd and the overwriting Mlt
+    from seldon_b200 import _lib
+    L = _lib.load()
+    (ptr, ind, val), m, n = CASES[case]()
+    rng = np.random.default_rng(41)
+    x, y = rng.standard_normal(n), rng.standard_normal(m)
+    A = api.RowSparse(m, n, ptr, ind, val)
+    _lib.check(L.sb2_spmv_set_config(algo, threads, stages), "sb2_spmv_set_config")
+    try:
+        Y = to_dev(y)
+        api.MltAdd(-1.3, A, to_dev(x), 0.7, Y)
+        Z = to_dev(np.full(m, np.nan))
+        api.Mlt(A, to_dev(x), Z)
+        import torch
+        torch.cuda.synchronize()
+    finally:
+        _lib.check(L.sb2_spmv_set_config(0, 256, 4), "sb2_spmv_set_config")
+    ref = oracle.mltadd(m, n, ptr, ind, val, -1.3, x, 0.7, y)
+    assert_spmv_close(to_host(Y), ref, 1.3 * abs_matvec(ptr, ind, val, x) + np.abs(0.7 * y))
+    ref0 = oracle.mltadd(m, n, ptr, ind, val, 1.0, x, 0.0, np.zeros(m))
+    assert_spmv_close(to_host(Z), ref0, abs_matvec(ptr, ind, val, x))
