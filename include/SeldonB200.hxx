@@ -62,6 +62,7 @@
 
 #include <atomic>
 #include <cstdlib>
+#include <fstream>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -365,6 +366,49 @@ namespace Seldon
       return *this;
     }
 
+    //! Saves the entries in Seldon's binary format (Vector.cxx:848-870):
+    //! the length first when with_size.
+    void Write(std::string FileName, bool with_size = true) const
+    {
+      std::ofstream f(FileName.c_str(), std::ofstream::binary);
+      if (!f.good())
+        throw IOError("Vector::Write(string FileName, bool with_size)",
+                      "Unable to open file \"" + FileName + "\".");
+      std::vector<T> h(this->m_);
+      if (this->m_ > 0)
+        b200::Check(sb2_memcpy(&h[0], this->data_, sizeof(T) * size_t(this->m_),
+                               b200::GetStream()), "Vector::Write");
+      if (with_size)
+        f.write(reinterpret_cast<const char*>(&this->m_), sizeof(int));
+      f.write(reinterpret_cast<const char*>(h.data()), sizeof(T) * h.size());
+      if (!f.good())
+        throw IOError("Vector::Write(string FileName, bool with_size)", "Output operation failed.");
+    }
+
+    //! Loads a file in Seldon's binary format: the length from the file when
+    //! with_size, else the vector's current length.
+    void Read(std::string FileName, bool with_size = true)
+    {
+      std::ifstream f(FileName.c_str(), std::ifstream::binary);
+      if (!f.good())
+        throw IOError("Vector::Read(string FileName, bool with_size)",
+                      "Unable to open file \"" + FileName + "\".");
+      int m = this->m_;
+      if (with_size)
+        f.read(reinterpret_cast<char*>(&m), sizeof(int));
+      if (!f.good() || m < 0)
+        throw IOError("Vector::Read(string FileName, bool with_size)", "Invalid length.");
+      std::vector<T> h(m);
+      f.read(reinterpret_cast<char*>(h.data()), sizeof(T) * h.size());
+      if (!f.good())
+        throw IOError("Vector::Read(string FileName, bool with_size)",
+                      "Input operation failed: the file holds fewer values.");
+      Reallocate(m);
+      if (m > 0)
+        b200::Check(sb2_memcpy(this->data_, h.data(), sizeof(T) * size_t(m), b200::GetStream()),
+                    "Vector::Read");
+    }
+
     //! Prints the entries (read back from the device) as Vector::Print does.
     void Print() const
     {
@@ -519,6 +563,51 @@ namespace Seldon
           return;
         Check(sb2_csr_download(h_, &ptr[0], nz_ ? &ind[0] : NULL,
                                nz_ ? &val[0] : NULL), "Matrix::Download");
+      }
+
+      //! Saves the stored arrays in Seldon's binary format (Matrix_Sparse.cxx:
+      //! 1531-1556; RowSymSparse writes the row count for n): a Seldon program
+      //! can Read the file back into a host matrix.
+      void Write(std::string FileName) const
+      {
+        std::ofstream f(FileName.c_str(), std::ofstream::binary);
+        if (!f.good())
+          throw IOError("Matrix::Write(string FileName)",
+                        "Unable to open file \"" + FileName + "\".");
+        std::vector<int> p, i;
+        std::vector<double> v;
+        Download(p, i, v);
+        int head[3] = {this->m_, Symmetric ? this->m_ : this->n_, nz_};
+        f.write(reinterpret_cast<const char*>(head), sizeof(head));
+        f.write(reinterpret_cast<const char*>(p.data()), sizeof(int) * p.size());
+        f.write(reinterpret_cast<const char*>(i.data()), sizeof(int) * i.size());
+        f.write(reinterpret_cast<const char*>(v.data()), sizeof(double) * v.size());
+        if (!f.good())
+          throw IOError("Matrix::Write(string FileName)", "Output operation failed.");
+      }
+
+      //! Loads a file in Seldon's binary format (Matrix_Sparse.cxx:1650-1680)
+      //! into the device matrix.
+      void Read(std::string FileName)
+      {
+        std::ifstream f(FileName.c_str(), std::ifstream::binary);
+        if (!f.good())
+          throw IOError("Matrix::Read(string FileName)",
+                        "Unable to open file \"" + FileName + "\".");
+        int head[3] = {0, 0, 0};
+        f.read(reinterpret_cast<char*>(head), sizeof(head));
+        if (!f.good() || head[0] < 0 || head[1] < 0 || head[2] < 0)
+          throw IOError("Matrix::Read(string FileName)", "Invalid header.");
+        std::vector<int> p(head[0] + 1), i(head[2]);
+        std::vector<double> v(head[2]);
+        f.read(reinterpret_cast<char*>(p.data()), sizeof(int) * p.size());
+        f.read(reinterpret_cast<char*>(i.data()), sizeof(int) * i.size());
+        f.read(reinterpret_cast<char*>(v.data()), sizeof(double) * v.size());
+        if (!f.good())
+          throw IOError("Matrix::Read(string FileName)",
+                        "Input operation failed: the file is shorter than its header says.");
+        Create(head[0], head[1], head[2], p.data(), i.empty() ? NULL : i.data(),
+               v.empty() ? NULL : v.data());
       }
 
     protected:

@@ -140,6 +140,33 @@ class Reference(_Base):
         L.ref_norm2.restype = _d
         L.ref_genrot.argtypes = [_vp, _vp, _vp, _vp]
         L.ref_genrot.restype = None
+        L.ref_write_csr.argtypes = [ctypes.c_char_p, _i, _i, _i, _vp, _vp, _vp, _i]
+        L.ref_write_csr.restype = _i
+        L.ref_read_csr_sizes.argtypes = [ctypes.c_char_p, _i, _vp, _vp, _vp]
+        L.ref_read_csr_sizes.restype = _i
+        L.ref_read_csr.argtypes = [ctypes.c_char_p, _i, _vp, _vp, _vp]
+        L.ref_read_csr.restype = _i
+        L.ref_write_vector.argtypes = [ctypes.c_char_p, _i, _vp, _i]
+        L.ref_write_vector.restype = _i
+
+    def write_csr(self, path, m, n, ptr, ind, val, sym=False):
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        self.lib.ref_write_csr(str(path).encode(), m, n, ind.size, _p(ptr), _p(ind), _p(val),
+                               int(sym))
+
+    def read_csr(self, path, sym=False):
+        m, n, nz = (ctypes.c_int() for _ in range(3))
+        self.lib.ref_read_csr_sizes(str(path).encode(), int(sym), ctypes.byref(m),
+                                    ctypes.byref(n), ctypes.byref(nz))
+        ptr = np.zeros(m.value + 1, dtype=np.int32)
+        ind = np.zeros(nz.value, dtype=np.int32)
+        val = np.zeros(nz.value)
+        self.lib.ref_read_csr(str(path).encode(), int(sym), _p(ptr), _p(ind), _p(val))
+        return m.value, n.value, ptr, ind, val
+
+    def write_vector(self, path, x, with_size=True):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self.lib.ref_write_vector(str(path).encode(), x.size, _p(x), int(with_size))
 
     def mltadd(self, m, n, ptr, ind, val, alpha, x, beta, y, sym=False, trans=False):
         ptr, ind, val = _csr_args(ptr, ind, val)

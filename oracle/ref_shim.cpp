@@ -160,6 +160,69 @@ namespace
 
 extern "C"
 {
+  // Seldon's binary matrix format through its own Write/Read
+  // (Matrix_Sparse.cxx:1531-1556, 1650-1680; Matrix_SymSparse.cxx:1440-1457).
+  int ref_write_csr(const char* path, int m, int n, int nnz, const int* ptr,
+                    const int* ind, const double* val, int sym)
+  {
+    Wrap A(m, n, nnz, ptr, ind, val, sym);
+    if (sym)
+      A.S.Write(std::string(path));
+    else
+      A.G.Write(std::string(path));
+    return 0;
+  }
+
+  // Sizes of a binary matrix file read by Seldon (m, n, stored nonzeros).
+  int ref_read_csr_sizes(const char* path, int sym, int* m, int* n, int* nnz)
+  {
+    if (sym)
+      {
+        SymMat S;
+        S.Read(std::string(path));
+        *m = S.GetM(); *n = S.GetN(); *nnz = S.GetNonZeros();
+      }
+    else
+      {
+        GenMat G;
+        G.Read(std::string(path));
+        *m = G.GetM(); *n = G.GetN(); *nnz = G.GetNonZeros();
+      }
+    return 0;
+  }
+
+  // Arrays of a binary matrix file read by Seldon (sizes from the above).
+  int ref_read_csr(const char* path, int sym, int* ptr, int* ind, double* val)
+  {
+    GenMat G;
+    SymMat S;
+    int m, nnz;
+    const int* p;
+    const int* i;
+    const double* v;
+    if (sym)
+      {
+        S.Read(std::string(path));
+        m = S.GetM(); nnz = S.GetNonZeros(); p = S.GetPtr(); i = S.GetInd(); v = S.GetData();
+      }
+    else
+      {
+        G.Read(std::string(path));
+        m = G.GetM(); nnz = G.GetNonZeros(); p = G.GetPtr(); i = G.GetInd(); v = G.GetData();
+      }
+    for (int k = 0; k <= m; k++) ptr[k] = p[k];
+    for (int k = 0; k < nnz; k++) { ind[k] = i[k]; val[k] = v[k]; }
+    return 0;
+  }
+
+  // Seldon's binary vector format (Vector.cxx:848-870): size, then values.
+  int ref_write_vector(const char* path, int n, const double* x, int with_size)
+  {
+    VWrap v(n, x);
+    v.v.Write(std::string(path), with_size != 0);
+    return 0;
+  }
+
   // Y = beta*Y + alpha*op(A)*X through Seldon's MltAdd.
   int ref_mltadd(int m, int n, int nnz, const int* ptr, const int* ind,
                  const double* val, int sym, int trans, double alpha,

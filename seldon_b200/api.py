@@ -82,6 +82,30 @@ class RowSparse:
     def GetNonZeros(self):
         return self.nnz_stored
 
+    def download(self):
+        """The stored arrays (ptr, ind, val) copied back to the host."""
+        import numpy as np
+        ptr = np.zeros(self.m + 1, dtype=np.int32)
+        ind = np.zeros(self.nnz_stored, dtype=np.int32)
+        val = np.zeros(self.nnz_stored)
+        check(_L.sb2_csr_download(self._h, _np_ptr(ptr), _np_ptr(ind), _np_ptr(val)),
+              "sb2_csr_download")
+        return ptr, ind, val
+
+    def Write(self, path):
+        """Save in Seldon's binary format (Matrix_Sparse::Write)."""
+        from seldon_b200 import io
+        io.write_csr(path, self.m, self.m if self.symmetric else self.n, *self.download())
+
+    @classmethod
+    def Read(cls, path, validate=True):
+        """Load a file in Seldon's binary format (Matrix_Sparse::Read)."""
+        from seldon_b200 import io
+        m, n, ptr, ind, val = io.read_csr(path)
+        if cls.symmetric:
+            return cls(m, ptr, ind, val, validate)
+        return cls(m, n, ptr, ind, val, validate)
+
     def close(self):
         if getattr(self, "_h", None):
             _L.sb2_csr_destroy(self._h)

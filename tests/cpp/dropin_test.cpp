@@ -530,6 +530,49 @@ int main()
       }
   }
 
+  // ------------------------------------------------ Seldon's binary files
+  {
+    const std::string fg = "dropin_gen.bin", fs = "dropin_sym.bin", fv = "dropin_vec.bin";
+    // device Write, Seldon Read
+    Gd.Write(fg);
+    Sd.Write(fs);
+    HostGen Gr;
+    HostSym Sr;
+    Gr.Read(fg);
+    Sr.Read(fs);
+    bool same = Gr.GetM() == Gh.GetM() && Gr.GetN() == Gh.GetN() &&
+                Gr.GetNonZeros() == Gh.GetNonZeros() && Sr.GetNonZeros() == Sh.GetNonZeros();
+    for (int k = 0; same && k <= Gh.GetM(); k++)
+      same = Gr.GetPtr()[k] == Gh.GetPtr()[k];
+    for (int k = 0; same && k < Gh.GetNonZeros(); k++)
+      same = Gr.GetInd()[k] == Gh.GetInd()[k] && Gr.GetData()[k] == Gh.GetData()[k];
+    for (int k = 0; same && k < Sh.GetNonZeros(); k++)
+      same = Sr.GetInd()[k] == Sh.GetInd()[k] && Sr.GetData()[k] == Sh.GetData()[k];
+    // Seldon Write, device Read, and the same products
+    Gh.Write(fg);
+    DevGen Gx;
+    Gx.Read(fg);
+    HostVec xh = random_vector(Gh.GetM(), 21), yh(Gh.GetM());
+    DevVec xd, yd(Gh.GetM());
+    Copy(xh, xd);
+    Mlt(Gh, xh, yh);
+    Mlt(Gx, xd, yd);
+    same = same && identical(yh, download(yd));
+    // vectors both ways
+    xd.Write(fv);
+    HostVec vr;
+    vr.Read(fv);
+    same = same && identical(vr, xh);
+    xh.Write(fv);
+    DevVec vd;
+    vd.Read(fv);
+    same = same && identical(download(vd), xh);
+    std::remove(fg.c_str());
+    std::remove(fs.c_str());
+    std::remove(fv.c_str());
+    report(same, "binary_files", "device Write -> Seldon Read, Seldon Write -> device Read");
+  }
+
   // ------------------------------------------------ errors
   {
     bool thrown = false;

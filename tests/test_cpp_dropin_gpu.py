@@ -13,10 +13,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "tests", "cpp", "_bin", "dropin_test")
 
 
-def test_cpp_dropin(cuda):
+def test_cpp_dropin(cuda, tmp_path):
     if not os.path.exists(BIN):
         pytest.skip("dropin_test not built (needs the reference headers: make -C tests/cpp)")
-    p = subprocess.run([BIN], capture_output=True, text=True, timeout=600)
+    p = subprocess.run([BIN], capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
     print(p.stdout)
     lines = [ln for ln in p.stdout.splitlines() if ln.startswith(("PASS", "FAIL"))]
     fails = [ln for ln in lines if ln.startswith("FAIL")]
@@ -24,7 +24,7 @@ def test_cpp_dropin(cuda):
     names = {ln.split()[1] for ln in lines}
     for must in ("spmv_general", "spmv_symmetric", "blas1", "cg_identity", "cg_ssor",
                  "gmres20_jacobi", "bicgstab_identity", "cg_user_preconditioner",
-                 "cg_zero_rhs", "invalid_csr_throws"):
+                 "cg_zero_rhs", "invalid_csr_throws", "binary_files"):
         assert must in names, must
     # Seldon's other Krylov drivers, its generic templates on device types
     for drv in ("bicg", "bicgstabl", "bicgcr", "cgne", "cgs", "cocg", "gcr", "lsqr", "minres",
