@@ -67,7 +67,8 @@ int sb2_stream_sync(void* stream);
  * row-block partition the SpMV kernels use). */
 typedef struct sb2_csr sb2_csr;
 
-/* Create a device matrix from HOST arrays in Seldon's layout.
+/* Create a device matrix from arrays in Seldon's layout (all three in host
+ * memory, or all three in device memory).
  *   m, n, nnz          sizes (nnz = ptr[m])
  *   ptr[m+1], ind[nnz], val[nnz]   Seldon's ptr_, ind_, data_
  *   symmetric_upper    0: Matrix<double, General, RowSparse>
@@ -77,7 +78,9 @@ typedef struct sb2_csr sb2_csr;
  *   validate           1: check ptr monotone, ptr[0]=0, ptr[m]=nnz,
  *                         0<=ind<n (and ind>=row for symmetric_upper), as
  *                         SELDON_CHECK_DIMENSIONS does (Matrix_Sparse.cxx:118-170)
- * The host arrays are copied; the caller keeps ownership.
+ * The arrays are copied; the caller keeps ownership.  They may also be
+ * device arrays (sb2_coo_to_csr's output): those are read back to the host,
+ * where the validator and the slice layout are built.
  * Replaces the constructor Matrix_Sparse(i, j, values, ptr, ind)
  * (Matrix_Sparse.cxx:105-180) and SetData (Matrix_Sparse.cxx:305-415). */
 int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
@@ -95,6 +98,29 @@ int sb2_csr_info(const sb2_csr* A, int* m, int* n, int* nnz_stored,
 /* Copy the stored arrays back to host buffers (ptr[m+1], ind[nnz_stored],
  * val[nnz_stored]); any pointer may be NULL. */
 int sb2_csr_download(const sb2_csr* A, int* ptr, int* ind, double* val);
+
+/* Assemble CSR arrays on the device from coordinate triplets, as
+ * ConvertMatrix_from_Coordinates does (Matrix_Conversions.cxx:1291-1334 for
+ * RowSparse, 1397-1467 for RowSymSparse; ReadText and FillRand reach it too).
+ *   row, col, val      DEVICE arrays of nnz triplets, indices from `index`
+ *   m_min, n_min       the target matrix's current size (GetM/GetN)
+ *   symmetric_upper    0: RowSparse.  m = max(largest row + 1, m_min),
+ *                         n = max(largest column + 1, n_min); an empty input
+ *                         gives max(1, m_min) x max(1, n_min)
+ *                      1: RowSymSparse.  Entries below the diagonal are
+ *                         dropped; m = n = largest row (of all entries) + 1;
+ *                         an empty input gives m_min x m_min with no entries
+ *   stream             orders the work; the call returns when it is done
+ * Entries come out in stable (row, column) order, duplicates kept, exactly
+ * Seldon's order (its merge sort is stable).  *ptr (m+1), *ind and *val_out
+ * (*nnz_out entries) are device arrays allocated here: release them with
+ * sb2_device_free.  An index below `index` or past INT_MAX-1 gives
+ * SB2_ERR_INVALID_VALUE (ReadCoordinateMatrix's IOError,
+ * Matrix_Sparse.cxx:1912-1921).  Nothing is returned on error. */
+int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val,
+                   int index, int m_min, int n_min, int symmetric_upper,
+                   void* stream, int* m, int* n, int* nnz_out, int** ptr,
+                   int** ind, double** val_out);
 
 /* ------------------------------------------------------------ SpMV */
 

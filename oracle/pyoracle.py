@@ -27,6 +27,11 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
+def _coo_args(row, col, val):
+    return (np.ascontiguousarray(row, dtype=np.int32), np.ascontiguousarray(col, dtype=np.int32),
+            np.ascontiguousarray(val, dtype=np.float64))
+
+
 def _csr_args(ptr, ind, val):
     ptr = np.ascontiguousarray(ptr, dtype=np.int32)
     ind = np.ascontiguousarray(ind, dtype=np.int32)
@@ -62,6 +67,24 @@ class Oracle(_Base):
         L.orc_solve.argtypes = [_i, _i, _i, _vp, _vp, _vp, _i, _i, _d, _i, _i, _vp, _vp,
                                 _d, _i, _i, _i, _vp, _vp, _vp, _i, _vp]
         L.orc_solve.restype = _i
+        L.orc_coo_sizes.argtypes = [_i, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp]
+        L.orc_coo_sizes.restype = _i
+        L.orc_coo_to_csr.argtypes = [_i, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]
+        L.orc_coo_to_csr.restype = None
+
+    def coo_to_csr(self, row, col, val, index=0, m_min=0, n_min=0, sym=False):
+        """ConvertMatrix_from_Coordinates restated: (m, n, ptr, ind, val)."""
+        row, col, val = _coo_args(row, col, val)
+        m, n, nz = (ctypes.c_int() for _ in range(3))
+        if self.lib.orc_coo_sizes(row.size, _p(row), _p(col), index, m_min, n_min, int(sym),
+                                  ctypes.byref(m), ctypes.byref(n), ctypes.byref(nz)) != 0:
+            raise ValueError("coordinate below the index base")
+        ptr = np.zeros(m.value + 1, dtype=np.int32)
+        ind = np.zeros(nz.value, dtype=np.int32)
+        out = np.zeros(nz.value)
+        self.lib.orc_coo_to_csr(row.size, _p(row), _p(col), _p(val), index, m.value, int(sym),
+                                _p(ptr), _p(ind), _p(out))
+        return m.value, n.value, ptr, ind, out
 
     def mltadd(self, m, n, ptr, ind, val, alpha, x, beta, y, sym=False, trans=False):
         """Returns a new y = beta*y + alpha*op(A)*x (MltAdd)."""
@@ -148,6 +171,24 @@ class Reference(_Base):
         L.ref_read_csr.restype = _i
         L.ref_write_vector.argtypes = [ctypes.c_char_p, _i, _vp, _i]
         L.ref_write_vector.restype = _i
+        L.ref_coo_to_csr.argtypes = [_i, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp,
+                                     _vp, _vp, _vp]
+        L.ref_coo_to_csr.restype = _i
+
+    def coo_to_csr(self, row, col, val, index=0, m_min=0, n_min=0, sym=False):
+        """Seldon's own ConvertMatrix_from_Coordinates: (m, n, ptr, ind, val)."""
+        row, col, val = _coo_args(row, col, val)
+        cap = max(m_min, n_min, 1, int(row.max(initial=0)) + 2, int(col.max(initial=0)) + 2)
+        ptr = np.zeros(cap + 1, dtype=np.int32)
+        ind = np.zeros(max(row.size, 1), dtype=np.int32)
+        out = np.zeros(max(row.size, 1))
+        m, n, nz = (ctypes.c_int() for _ in range(3))
+        if self.lib.ref_coo_to_csr(row.size, _p(row), _p(col), _p(val), index, m_min, n_min,
+                                   int(sym), cap, ctypes.byref(m), ctypes.byref(n),
+                                   ctypes.byref(nz), _p(ptr), _p(ind), _p(out)) != 0:
+            raise RuntimeError("ref_coo_to_csr: result larger than the buffers")
+        return (m.value, n.value, ptr[:m.value + 1].copy(), ind[:nz.value].copy(),
+                out[:nz.value].copy())
 
     def write_csr(self, path, m, n, ptr, ind, val, sym=False):
         ptr, ind, val = _csr_args(ptr, ind, val)

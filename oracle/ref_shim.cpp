@@ -281,6 +281,55 @@ extern "C"
                      nb_iter);
   }
 
+  // Seldon's coordinate -> CSR assembly (ConvertMatrix_from_Coordinates,
+  // Matrix_Conversions.cxx:1291-1334 RowSparse, 1397-1467 RowSymSparse) into
+  // a matrix that starts as an empty m_min x n_min one.  The caller's
+  // buffers hold at least cap_rows+1 row pointers and nnz entries; the
+  // result's sizes go to *m, *n, *nnz_out (-1 when they would not fit).
+  int ref_coo_to_csr(int nnz, const int* row, const int* col,
+                     const double* val, int index, int m_min, int n_min,
+                     int sym, int cap_rows, int* m, int* n, int* nnz_out,
+                     int* ptr, int* ind, double* vout)
+  {
+    Vector<int> R(nnz), C(nnz);
+    Vec V(nnz);
+    for (int i = 0; i < nnz; i++)
+      {
+        R(i) = row[i];
+        C(i) = col[i];
+        V(i) = val[i];
+      }
+    const int *p, *q;
+    const double* v;
+    if (sym)
+      {
+        SymMat A;
+        A.Reallocate(m_min, m_min);
+        ConvertMatrix_from_Coordinates(R, C, V, A, index);
+        *m = A.GetM();
+        *n = A.GetN();
+        *nnz_out = A.GetDataSize();
+        p = A.GetPtr(); q = A.GetInd(); v = A.GetData();
+        if (*m > cap_rows) return -1;
+        for (int i = 0; i <= *m; i++) ptr[i] = p[i];
+        for (int k = 0; k < *nnz_out; k++) { ind[k] = q[k]; vout[k] = v[k]; }
+      }
+    else
+      {
+        GenMat A;
+        A.Reallocate(m_min, n_min);
+        ConvertMatrix_from_Coordinates(R, C, V, A, index);
+        *m = A.GetM();
+        *n = A.GetN();
+        *nnz_out = A.GetDataSize();
+        p = A.GetPtr(); q = A.GetInd(); v = A.GetData();
+        if (*m > cap_rows) return -1;
+        for (int i = 0; i <= *m; i++) ptr[i] = p[i];
+        for (int k = 0; k < *nnz_out; k++) { ind[k] = q[k]; vout[k] = v[k]; }
+      }
+    return 0;
+  }
+
   // Seldon's generic BLAS-1 loops (Functions_Vector.cxx), for pinning.
   double ref_dot(int n, const double* x, const double* y)
   {

@@ -577,3 +577,89 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
   if (hist_len) *hist_len = it.hist_len;
   return code;
 }
+
+/* ------------------------------------------------- coordinate -> CSR */
+
+/* Sizes of the matrix ConvertMatrix_from_Coordinates builds
+ * (matrix_sparse/Matrix_Conversions.cxx:1300-1313 RowSparse: m = max(largest
+ * row - index + 1, A.GetM()), n likewise, GetNormInf of an empty vector
+ * being 0; 1410-1421 RowSymSparse: m = n = largest row - index + 1, entries
+ * below the diagonal dropped, an empty input returning early).  Returns -1
+ * for an index below `index` (ReadCoordinateMatrix's check,
+ * Matrix_Sparse.cxx:1912-1921). */
+int orc_coo_sizes(int nnz, const int* row, const int* col, int index,
+                  int m_min, int n_min, int sym, int* m, int* n,
+                  int* nnz_out) {
+  long long rmax = 0, cmax = 0;
+  int kept = 0;
+  for (int i = 0; i < nnz; i++) {
+    long long r = (long long)row[i] - index, c = (long long)col[i] - index;
+    if (r < 0 || c < 0) return -1;
+    if (r > rmax) rmax = r;
+    if (c > cmax) cmax = c;
+    if (r <= c) kept++;
+  }
+  if (sym) {
+    *m = nnz > 0 ? (int)(rmax + 1) : m_min;
+    *n = *m;
+    *nnz_out = kept;
+  } else {
+    *m = (int)(rmax + 1 > m_min ? rmax + 1 : m_min);
+    *n = (int)(cmax + 1 > n_min ? cmax + 1 : n_min);
+    *nnz_out = nnz;
+  }
+  return 0;
+}
+
+/* Stable merge sort of key[lo..hi) carrying val (equal keys keep their
+ * order, as Seldon's MergeSort does: vector/Functions_Arrays.cxx:412-500). */
+static void stable_sort_kv(int* key, double* val, int lo, int hi, int* tk,
+                           double* tv) {
+  if (hi - lo < 2) return;
+  int mid = lo + (hi - lo) / 2;
+  stable_sort_kv(key, val, lo, mid, tk, tv);
+  stable_sort_kv(key, val, mid, hi, tk, tv);
+  int a = lo, b = mid, o = lo;
+  while (a < mid && b < hi) {
+    if (key[b] < key[a]) { tk[o] = key[b]; tv[o++] = val[b++]; }
+    else { tk[o] = key[a]; tv[o++] = val[a++]; }
+  }
+  while (a < mid) { tk[o] = key[a]; tv[o++] = val[a++]; }
+  while (b < hi) { tk[o] = key[b]; tv[o++] = val[b++]; }
+  memcpy(key + lo, tk + lo, sizeof(int) * (hi - lo));
+  memcpy(val + lo, tv + lo, sizeof(double) * (hi - lo));
+}
+
+/* The CSR arrays (ptr[m+1], ind/vout[nnz_out] from orc_coo_sizes):
+ * Matrix_Conversions.cxx:1315-1333 (RowSparse) and 1423-1466 (RowSymSparse).
+ * Steps: drop the lower part (sym), order by row keeping input order among
+ * equal rows, count rows into ptr, order each row by column keeping the
+ * previous order among equal columns. */
+void orc_coo_to_csr(int nnz, const int* row, const int* col,
+                    const double* val, int index, int m, int sym, int* ptr,
+                    int* ind, double* vout) {
+  int* cnt = (int*)calloc((size_t)m + 1, sizeof(int));
+  int* fill = (int*)malloc(sizeof(int) * ((size_t)m + 1));
+  int* tk = (int*)malloc(sizeof(int) * ((size_t)nnz + 1));
+  double* tv = (double*)malloc(sizeof(double) * ((size_t)nnz + 1));
+  for (int i = 0; i < nnz; i++) {
+    int r = row[i] - index, c = col[i] - index;
+    if (sym && r > c) continue;
+    cnt[r + 1]++;
+  }
+  for (int i = 0; i < m; i++) cnt[i + 1] += cnt[i];
+  memcpy(ptr, cnt, sizeof(int) * ((size_t)m + 1));
+  memcpy(fill, cnt, sizeof(int) * ((size_t)m + 1));
+  for (int i = 0; i < nnz; i++) {
+    int r = row[i] - index, c = col[i] - index;
+    if (sym && r > c) continue;
+    ind[fill[r]] = c;
+    vout[fill[r]] = val[i];
+    fill[r]++;
+  }
+  for (int i = 0; i < m; i++) stable_sort_kv(ind, vout, ptr[i], ptr[i + 1], tk, tv);
+  free(cnt);
+  free(fill);
+  free(tk);
+  free(tv);
+}

@@ -129,6 +129,10 @@ _PROTOS = [
     ("sb2_csr_destroy", ctypes.c_int, [c_void_p]),
     ("sb2_csr_info", ctypes.c_int, [c_void_p, c_int_p, c_int_p, c_int_p, c_int_p]),
     ("sb2_csr_download", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_coo_to_csr", ctypes.c_int,
+     [ctypes.c_int, c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+      ctypes.c_int, c_void_p, c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p),
+      ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p)]),
     ("sb2_spmv", ctypes.c_int,
      [c_void_p, ctypes.c_int, ctypes.c_double, c_void_p, ctypes.c_double, c_void_p, c_void_p]),
     ("sb2_mlt", ctypes.c_int,

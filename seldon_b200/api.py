@@ -43,6 +43,69 @@ def _np_ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+class _DeviceArray:
+    """A device array allocated by the library (released with
+    sb2_device_free when the last tensor viewing it goes away)."""
+
+    def __init__(self, ptr, n, typestr):
+        self._p = ptr
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr or 0, False), "version": 2,
+                                         "strides": None}
+
+    def __del__(self):
+        if self._p:
+            _L.sb2_device_free(ctypes.c_void_p(self._p))
+            self._p = None
+
+
+def _as_tensor(ptr, n, typestr, dtype):
+    import torch
+    if n == 0:
+        if ptr:
+            _L.sb2_device_free(ctypes.c_void_p(ptr))
+        return torch.zeros(0, dtype=dtype, device="cuda")
+    return torch.as_tensor(_DeviceArray(ptr, n, typestr), device="cuda")
+
+
+def _int_dev_ptr(t, name):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.int32:
+        raise TypeError(f"{name}: expected a CUDA int32 tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def ConvertMatrix_from_Coordinates(IndRow, IndCol, Val, index=0, m=0, n=0, symmetric=False,
+                                   stream=None):
+    """Assemble CSR arrays on the device from coordinate triplets
+    (Matrix_Conversions.cxx:1291-1334 RowSparse, 1397-1467 RowSymSparse).
+
+    IndRow/IndCol: CUDA int32 tensors, Val: CUDA float64 tensor, indices from
+    `index`; (m, n) is the target matrix's current size.  Returns
+    (m, n, ptr, ind, val) with device tensors in Seldon's stable (row, column)
+    order, duplicates kept.  symmetric=True drops the entries below the
+    diagonal (RowSymSparse)."""
+    nnz = IndRow.numel()
+    if IndCol.numel() != nnz or Val.numel() != nnz:
+        raise ValueError("WrongDim: IndRow, IndCol and Val must have the same length")
+    rp = _int_dev_ptr(IndRow, "IndRow") if nnz else None
+    cp = _int_dev_ptr(IndCol, "IndCol") if nnz else None
+    vp = _dev_ptr(Val, nnz, "Val") if nnz else None
+    mo, no, zo = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    dp, di, dv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    check(_L.sb2_coo_to_csr(int(nnz), rp, cp, vp, int(index), int(m), int(n), int(symmetric),
+                            _stream(stream), ctypes.byref(mo), ctypes.byref(no),
+                            ctypes.byref(zo), ctypes.byref(dp), ctypes.byref(di),
+                            ctypes.byref(dv)), "sb2_coo_to_csr")
+    import torch
+    ptr = _as_tensor(dp.value, mo.value + 1, "<i4", torch.int32)
+    ind = _as_tensor(di.value, zo.value, "<i4", torch.int32)
+    val = _as_tensor(dv.value, zo.value, "<f8", torch.float64)
+    return mo.value, no.value, ptr, ind, val
+
+
 class RowSparse:
     """Matrix<double, General, RowSparse> held on the device.
 
@@ -53,18 +116,27 @@ class RowSparse:
 
     def __init__(self, m, n, ptr, ind, val, validate=True):
         import numpy as np
-        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
-        ind = np.ascontiguousarray(ind, dtype=np.int32)
-        val = np.ascontiguousarray(val, dtype=np.float64)
-        if ptr.size != m + 1 or ind.size != val.size:
-            raise ValueError("WrongDim: ptr must hold m+1 entries and ind/val nnz entries")
+        if hasattr(ptr, "is_cuda") and ptr.is_cuda:  # device arrays (e.g. assembled)
+            nz = int(ind.numel())
+            if ptr.numel() != m + 1 or val.numel() != nz:
+                raise ValueError("WrongDim: ptr must hold m+1 entries and ind/val nnz entries")
+            args = (_int_dev_ptr(ptr, "ptr"), _int_dev_ptr(ind, "ind") if nz else None,
+                    _dev_ptr(val, nz, "val") if nz else None)
+        else:
+            ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+            ind = np.ascontiguousarray(ind, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+            if ptr.size != m + 1 or ind.size != val.size:
+                raise ValueError("WrongDim: ptr must hold m+1 entries and ind/val nnz entries")
+            nz = int(ind.size)
+            args = (_np_ptr(ptr), _np_ptr(ind), _np_ptr(val))
         h = ctypes.c_void_p()
-        st = _L.sb2_csr_create(int(m), int(n), int(ind.size), _np_ptr(ptr), _np_ptr(ind),
-                               _np_ptr(val), int(self.symmetric), int(validate), ctypes.byref(h))
+        st = _L.sb2_csr_create(int(m), int(n), nz, *args, int(self.symmetric), int(validate),
+                               ctypes.byref(h))
         check(st, "sb2_csr_create")
         self._h = h
         self.m, self.n = int(m), int(n)
-        self.nnz_stored = int(ind.size)
+        self.nnz_stored = nz
         full = ctypes.c_int()
         _L.sb2_csr_info(h, None, None, None, ctypes.byref(full))
         self.nnz_full = full.value
@@ -102,6 +174,16 @@ class RowSparse:
         """Load a file in Seldon's binary format (Matrix_Sparse::Read)."""
         from seldon_b200 import io
         m, n, ptr, ind, val = io.read_csr(path)
+        if cls.symmetric:
+            return cls(m, ptr, ind, val, validate)
+        return cls(m, n, ptr, ind, val, validate)
+
+    @classmethod
+    def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):
+        """Matrix built from coordinate triplets on the device, as
+        ConvertMatrix_from_Coordinates fills an m x n matrix."""
+        m, n, ptr, ind, val = ConvertMatrix_from_Coordinates(
+            IndRow, IndCol, Val, index, m, n, cls.symmetric)
         if cls.symmetric:
             return cls(m, ptr, ind, val, validate)
         return cls(m, n, ptr, ind, val, validate)
@@ -491,6 +573,16 @@ class Batch:
         check(_L.sb2_batch_autotune(self._h, _dev_ptr(x, self.m, "x"), _dev_ptr(b, self.m, "b"),
                                     ctypes.byref(prm), _stream(stream)), "sb2_batch_autotune")
         return _L.sb2_batch_get_threads(self._h)
+
+    @classmethod
+    def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):
+        """Matrix built from coordinate triplets on the device, as
+        ConvertMatrix_from_Coordinates fills an m x n matrix."""
+        m, n, ptr, ind, val = ConvertMatrix_from_Coordinates(
+            IndRow, IndCol, Val, index, m, n, cls.symmetric)
+        if cls.symmetric:
+            return cls(m, ptr, ind, val, validate)
+        return cls(m, n, ptr, ind, val, validate)
 
     def close(self):
         if getattr(self, "_h", None):

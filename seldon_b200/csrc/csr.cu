@@ -377,6 +377,21 @@ int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
   if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
   if (symmetric_upper && m != n) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
+  // Device arrays (sb2_coo_to_csr's output, say) are read back first: the
+  // validator and the slice layout are built on the host.
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, ptr) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
+    std::vector<int> hp(m + 1), hi(nnz);
+    std::vector<double> hv(nnz);
+    SB2_CUDA_TRY(cudaMemcpy(hp.data(), ptr, sizeof(int) * (m + 1), cudaMemcpyDeviceToHost));
+    if (nnz > 0) {
+      SB2_CUDA_TRY(cudaMemcpy(hi.data(), ind, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
+      SB2_CUDA_TRY(cudaMemcpy(hv.data(), val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    }
+    return sb2_csr_create(m, n, nnz, hp.data(), hi.data(), hv.data(), symmetric_upper, validate,
+                          out);
+  }
+  cudaGetLastError();  // a host pointer unknown to CUDA is not an error
   if (validate) SB2_TRY(validate_csr(m, n, nnz, ptr, ind, symmetric_upper));
   else if (ptr[m] != nnz) return SB2_ERR_INVALID_CSR;
 

@@ -86,6 +86,22 @@ def main():
                  (-1e-300, 1e-300), (1.0, -1.0)]:
         rot.append([a, b, *R.genrot(a, b)])
     put("genrot", table=np.array(rot))
+
+    # coordinate -> CSR assembly (ConvertMatrix_from_Coordinates)
+    crng = np.random.default_rng(7)
+    coo_cases = {
+        "gen_dup_i1": (crng.integers(1, 31, 700), crng.integers(1, 23, 700), 1, 0, 0, 0),
+        "gen_min": (crng.integers(0, 12, 90), crng.integers(0, 9, 90), 0, 20, 15, 0),
+        "sym_both": (crng.integers(0, 40, 500), crng.integers(0, 40, 500), 0, 0, 0, 1),
+        "sym_i1_min": (crng.integers(1, 17, 200), crng.integers(1, 17, 200), 1, 30, 30, 1),
+        "empty_gen": (np.zeros(0, np.int32), np.zeros(0, np.int32), 0, 6, 4, 0),
+        "empty_sym": (np.zeros(0, np.int32), np.zeros(0, np.int32), 0, 6, 6, 1),
+    }
+    for name, (r, c, index, m_min, n_min, sym) in coo_cases.items():
+        v = crng.standard_normal(r.size)
+        m, n, op, oi, ov = R.coo_to_csr(r, c, v, index, m_min, n_min, bool(sym))
+        put(f"coo/{name}", row=r.astype(np.int32), col=c.astype(np.int32), val=v, index=index,
+            m_min=m_min, n_min=n_min, sym=sym, m=m, n=n, ptr=op, ind=oi, out=ov)
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {len(g)} arrays, {os.path.getsize(OUT)} bytes")
 

@@ -137,3 +137,45 @@ def test_breakdown_and_edge_codes(reference, oracle):
     xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b)
     xr, cr, nr = reference.solve("cg", ptr, ind, val, b)
     assert co == cr == 2
+
+
+COO_CASES = ["gen_dup_i1", "gen_min", "sym_both", "sym_i1_min", "empty_gen", "empty_sym"]
+
+
+def _coo(g, name):
+    k = f"coo/{name}"
+    return (g[k + "/row"], g[k + "/col"], g[k + "/val"], int(g[k + "/index"]),
+            int(g[k + "/m_min"]), int(g[k + "/n_min"]), bool(g[k + "/sym"]))
+
+
+@pytest.mark.parametrize("name", COO_CASES)
+def test_coo_to_csr_golden(golden, oracle, name):
+    row, col, val, index, m_min, n_min, sym = _coo(golden, name)
+    m, n, ptr, ind, out = oracle.coo_to_csr(row, col, val, index, m_min, n_min, sym)
+    k = f"coo/{name}"
+    assert (m, n) == (int(golden[k + "/m"]), int(golden[k + "/n"]))
+    assert np.array_equal(ptr, golden[k + "/ptr"])
+    assert np.array_equal(ind, golden[k + "/ind"])
+    assert np.array_equal(out, golden[k + "/out"])
+
+
+def test_coo_to_csr_live_fuzz(oracle, reference):
+    """Random triplets (many duplicates, both index bases, both storages,
+    current sizes larger and smaller than the entries) against Seldon's own
+    ConvertMatrix_from_Coordinates."""
+    rng = np.random.default_rng(11)
+    for _ in range(200):
+        nnz = int(rng.integers(0, 300))
+        m, n = int(rng.integers(1, 30)), int(rng.integers(1, 30))
+        index, sym = int(rng.integers(0, 2)), bool(rng.integers(0, 2))
+        if sym:
+            n = m
+        row = rng.integers(0, m, nnz) + index
+        col = rng.integers(0, n, nnz) + index
+        val = rng.standard_normal(nnz)
+        m_min, n_min = int(rng.integers(0, 40)), int(rng.integers(0, 40))
+        a = oracle.coo_to_csr(row, col, val, index, m_min, n_min, sym)
+        b = reference.coo_to_csr(row, col, val, index, m_min, n_min, sym)
+        assert a[:2] == b[:2]
+        for u, v in zip(a[2:], b[2:]):
+            assert np.array_equal(u, v)
