@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true", help="skip the solver/Zipf extras")
     p.add_argument("--extras", default="all",
-                   help="comma list of extras to run: c1, c3, gmres, zipf, batch, adjoint "
+                   help="comma list of extras to run: c1, c3, gmres, zipf, batch, adjoint, assemble "
                         "(default all)")
     p.add_argument("--cpu-seconds", type=float, default=8.0,
                    help="bounded CPU-baseline sample (seconds of work)")
@@ -393,7 +393,7 @@ def run_extras(api, matgen, torch, dev, which="all"):
     """Time-to-solution figures on the other configurations (device-timed).
     `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, or all."""
     out = {}
-    names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint"}
+    names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint", "assemble"}
     want = names if which == "all" else set(w.strip() for w in which.split(","))
     unknown = want - names
     if unknown:
@@ -421,6 +421,8 @@ def run_extras(api, matgen, torch, dev, which="all"):
         out.update(extra_gmres(api, matgen, torch, dev, timed, rng))
     if "zipf" in want:
         out.update(extra_zipf(api, matgen, torch, dev, timed))
+    if "assemble" in want:
+        out.update(extra_assemble(api, matgen, torch, dev, timed))
     if "batch" in want:
         out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed)
     if "adjoint" in want:
@@ -530,6 +532,45 @@ def extra_zipf(api, matgen, torch, dev, timed):
     Bz = spmv_bytes(n, n, ind.size)
     return {"spmv_zipf_1e6": {"gbs": round(Bz / (ms / 20 * 1e-3) / 1e9, 1), "nnz": int(ind.size),
                               "us": round(ms / 20 * 1e3, 1)}}
+
+
+def _shuffled_triplets(matgen, torch, dev, g, seed=3):
+    ptr, ind, val = matgen.convdiff3d(g)
+    m = ptr.size - 1
+    rows = np.repeat(np.arange(m, dtype=np.int32), np.diff(ptr))
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    perm = torch.randperm(ind.size, device=dev, generator=gen)
+    return m, [torch.as_tensor(a, device=dev)[perm].contiguous() for a in (rows, ind, val)]
+
+
+def extra_assemble(api, matgen, torch, dev, timed):
+    """COO -> CSR assembly (ConvertMatrix_from_Coordinates) of the 128^3
+    convection-diffusion operator's 14.6M triplets in random order, through
+    the public call (output allocation included); Seldon's own conversion
+    timed beside it on the 64^3 operator's triplets."""
+    m, (r, c, v) = _shuffled_triplets(matgen, torch, dev, 128)
+    nnz = r.numel()
+    for _ in range(3):
+        api.ConvertMatrix_from_Coordinates(r, c, v, 0, m, m)
+    ms, _ = timed(lambda: api.ConvertMatrix_from_Coordinates(r, c, v, 0, m, m), reps=5)
+    # least traffic any assembly needs: triplets in, ind/val/ptr out
+    min_bytes = nnz * 16 + nnz * 12 + 4 * (m + 1)
+    out = {"nnz": nnz, "ms": round(ms, 3), "entries_per_s": round(nnz / ms * 1e3, 1),
+           "min_bytes_gbs": round(min_bytes / (ms * 1e-3) / 1e9, 1)}
+    try:
+        from oracle.pyoracle import REF_FAST_SO, Reference
+        if Reference.available(REF_FAST_SO):
+            R = Reference(REF_FAST_SO)
+            ms_, (rs, cs, vs) = _shuffled_triplets(matgen, torch, dev, 64)
+            rs, cs, vs = (t.cpu().numpy() for t in (rs, cs, vs))
+            t0 = time.perf_counter()
+            R.coo_to_csr(rs, cs, vs, 0, ms_, ms_)
+            dt = time.perf_counter() - t0
+            out["cpu_reference"] = {"nnz": int(rs.size), "s": round(dt, 3),
+                                    "entries_per_s": round(rs.size / dt, 1), "cores": 1}
+    except Exception as e:  # the checker is optional here
+        out["cpu_reference"] = {"unavailable": str(e)[:120]}
+    return {"coo_to_csr_conv128": out}
 
 
 def run_batch(api, matgen, torch, dev, timed, nsys=4096, sample_every=8):

@@ -433,6 +433,33 @@ namespace Seldon
     //! Device CSR matrix behind the RowSparse and RowSymSparse
     //! specialisations: an opaque library handle that owns device copies
     //! of ptr_/ind_/data_ (and the SpMV layouts built from them).
+    //! Device scratch released on scope exit.
+    struct DeviceBuffer
+    {
+      void* p;
+      explicit DeviceBuffer(size_t bytes): p(NULL)
+      {
+        Check(sb2_device_alloc(bytes, &p), "sb2_device_alloc");
+      }
+      ~DeviceBuffer()
+      {
+        sb2_device_free(p);
+      }
+    private:
+      DeviceBuffer(const DeviceBuffer&);
+      DeviceBuffer& operator= (const DeviceBuffer&);
+    };
+
+    //! The Seldon host type a device matrix downloads into.
+    template <int Symmetric> struct HostMatrix
+    {
+      typedef Matrix<double, General, RowSparse> type;
+    };
+    template <> struct HostMatrix<1>
+    {
+      typedef Matrix<double, Symmetric, RowSymSparse> type;
+    };
+
     template <int Symmetric>
     class DeviceCsr: public Matrix_Base<double, CudaAlloc<double> >
     {
@@ -610,6 +637,94 @@ namespace Seldon
                v.empty() ? NULL : v.data());
       }
 
+      //! Builds the matrix on the device from DEVICE triplets, as
+      //! ConvertMatrix_from_Coordinates fills it (Matrix_Conversions.cxx:
+      //! 1291-1334 RowSparse, 1397-1467 RowSymSparse; sb2_coo_to_csr).
+      void AssembleDevice(int nnz, const int* row, const int* col,
+                          const double* val, int index)
+      {
+        int m = 0, n = 0, nz = 0;
+        int *p = NULL, *i = NULL;
+        double* v = NULL;
+        Check(sb2_coo_to_csr(nnz, row, col, val, index, this->m_, this->n_,
+                             Symmetric, GetStream(), &m, &n, &nz, &p, &i, &v),
+              "ConvertMatrix_from_Coordinates");
+        sb2_csr* h = 0;
+        int st = sb2_csr_create(m, n, nz, p, i, v, Symmetric, 1, &h);
+        sb2_device_free(p);
+        sb2_device_free(i);
+        sb2_device_free(v);
+        Check(st, "ConvertMatrix_from_Coordinates");
+        if (h_)
+          sb2_csr_destroy(h_);
+        h_ = h;
+        this->m_ = m;
+        this->n_ = n;
+        nz_ = nz;
+        serial_ = NextSerial();
+      }
+
+      //! The same from HOST triplets (copied to the device first).
+      void AssembleHost(int nnz, const int* row, const int* col,
+                        const double* val, int index)
+      {
+        DeviceBuffer r(sizeof(int) * size_t(nnz)), c(sizeof(int) * size_t(nnz)),
+          v(sizeof(double) * size_t(nnz));
+        if (nnz > 0)
+          {
+            Check(sb2_memcpy(r.p, row, sizeof(int) * size_t(nnz), GetStream()), "upload");
+            Check(sb2_memcpy(c.p, col, sizeof(int) * size_t(nnz), GetStream()), "upload");
+            Check(sb2_memcpy(v.p, val, sizeof(double) * size_t(nnz), GetStream()), "upload");
+          }
+        AssembleDevice(nnz, static_cast<const int*>(r.p), static_cast<const int*>(c.p),
+                       static_cast<const double*>(v.p), index);
+      }
+
+      //! Reads "row column value" lines (1-based) as Matrix_Sparse::ReadText
+      //! does (Matrix_Sparse.cxx:1692-1724, ReadCoordinateMatrix 1885-1980),
+      //! then assembles the matrix on the device.
+      void ReadText(std::string FileName)
+      {
+        std::ifstream f(FileName.c_str());
+        if (!f.is_open())
+          throw IOError("Matrix_Sparse::ReadText(string FileName)",
+                        std::string("Unable to open file \"") + FileName + "\".");
+        std::vector<int> r, c;
+        std::vector<double> v;
+        int row = 0, col = 0;
+        double entry = 0.0;
+        while (!f.eof())
+          {
+            f >> row >> col >> entry;
+            if (f.fail())
+              break;
+            if (row < 1)
+              throw IOError("ReadCoordinateMatrix",
+                            "Error : Row number should be greater than 0 but is equal to "
+                            + to_str(row));
+            if (col < 1)
+              throw IOError("ReadCoordinateMatrix",
+                            "Error : Column number should be greater than 0 but is equal to "
+                            + to_str(col));
+            r.push_back(row);
+            c.push_back(col);
+            v.push_back(entry);
+          }
+        Clear();
+        if (!r.empty())
+          AssembleHost(int(r.size()), &r[0], &c[0], &v[0], 1);
+      }
+
+      //! Writes "row column value" lines as Matrix_Sparse::WriteText does
+      //! (Matrix_Sparse.cxx:1568-1616): Seldon's own writer on a host copy,
+      //! so the text is the same byte for byte.
+      void WriteText(std::string FileName) const
+      {
+        typename HostMatrix<Symmetric>::type A;
+        DownloadTo(A);
+        A.WriteText(FileName);
+      }
+
     protected:
       void CopyDevice(const DeviceCsr& A)
       {
@@ -751,6 +866,86 @@ namespace Seldon
   };
 
 
+  ///////////////////////////////////
+  // ASSEMBLY FROM COORDINATE FORM //
+  ///////////////////////////////////
+
+
+  //! ConvertMatrix_from_Coordinates (Matrix_Conversions.cxx:1291-1334) with
+  //! the triplets in device memory: sorted and assembled on the device.  The
+  //! triplet vectors are emptied, as Seldon empties them.
+  template <class Prop>
+  void ConvertMatrix_from_Coordinates(Vector<int, VectFull, CudaAlloc<int> >& IndRow,
+                                      Vector<int, VectFull, CudaAlloc<int> >& IndCol,
+                                      Vector<double, VectFull, CudaAlloc<double> >& Val,
+                                      Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+                                      int index = 0)
+  {
+    if (IndCol.GetM() != IndRow.GetM() || Val.GetM() != IndRow.GetM())
+      throw WrongDim("ConvertMatrix_from_Coordinates", "triplet vectors differ in length");
+    A.AssembleDevice(IndRow.GetM(), IndRow.GetData(), IndCol.GetData(), Val.GetData(), index);
+    IndRow.Clear();
+    IndCol.Clear();
+    Val.Clear();
+  }
+
+
+  //! RowSymSparse form (Matrix_Conversions.cxx:1397-1467): entries below the
+  //! diagonal are dropped.
+  template <class Prop>
+  void ConvertMatrix_from_Coordinates(Vector<int, VectFull, CudaAlloc<int> >& IndRow,
+                                      Vector<int, VectFull, CudaAlloc<int> >& IndCol,
+                                      Vector<double, VectFull, CudaAlloc<double> >& Val,
+                                      Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+                                      int index = 0)
+  {
+    if (IndRow.GetM() <= 0)
+      return;
+    if (IndCol.GetM() != IndRow.GetM() || Val.GetM() != IndRow.GetM())
+      throw WrongDim("ConvertMatrix_from_Coordinates", "triplet vectors differ in length");
+    A.AssembleDevice(IndRow.GetM(), IndRow.GetData(), IndCol.GetData(), Val.GetData(), index);
+    IndRow.Clear();
+    IndCol.Clear();
+    Val.Clear();
+  }
+
+
+  //! Host triplets into a device matrix: copied to the device, then
+  //! assembled there.
+  template <class Prop, class Alloc1, class Alloc2, class Alloc3>
+  void ConvertMatrix_from_Coordinates(Vector<int, VectFull, Alloc1>& IndRow,
+                                      Vector<int, VectFull, Alloc2>& IndCol,
+                                      Vector<double, VectFull, Alloc3>& Val,
+                                      Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+                                      int index = 0)
+  {
+    if (IndCol.GetM() != IndRow.GetM() || Val.GetM() != IndRow.GetM())
+      throw WrongDim("ConvertMatrix_from_Coordinates", "triplet vectors differ in length");
+    A.AssembleHost(IndRow.GetM(), IndRow.GetData(), IndCol.GetData(), Val.GetData(), index);
+    IndRow.Clear();
+    IndCol.Clear();
+    Val.Clear();
+  }
+
+
+  template <class Prop, class Alloc1, class Alloc2, class Alloc3>
+  void ConvertMatrix_from_Coordinates(Vector<int, VectFull, Alloc1>& IndRow,
+                                      Vector<int, VectFull, Alloc2>& IndCol,
+                                      Vector<double, VectFull, Alloc3>& Val,
+                                      Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+                                      int index = 0)
+  {
+    if (IndRow.GetM() <= 0)
+      return;
+    if (IndCol.GetM() != IndRow.GetM() || Val.GetM() != IndRow.GetM())
+      throw WrongDim("ConvertMatrix_from_Coordinates", "triplet vectors differ in length");
+    A.AssembleHost(IndRow.GetM(), IndRow.GetData(), IndCol.GetData(), Val.GetData(), index);
+    IndRow.Clear();
+    IndCol.Clear();
+    Val.Clear();
+  }
+
+
   ////////////
   // BLAS-1 //
   ////////////
@@ -803,6 +998,28 @@ namespace Seldon
     Y.Reallocate(X.GetM());
     if (X.GetM() > 0)
       b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(double) * size_t(X.GetM()),
+                             b200::GetStream()), "Copy(device, host)");
+  }
+
+  //! Host index vector to device vector (device triplets for assembly).
+  template <class Allocator0>
+  void Copy(const Vector<int, VectFull, Allocator0>& X,
+            Vector<int, VectFull, CudaAlloc<int> >& Y)
+  {
+    Y.Reallocate(X.GetM());
+    if (X.GetM() > 0)
+      b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(int) * size_t(X.GetM()),
+                             b200::GetStream()), "Copy(host, device)");
+  }
+
+  //! Device index vector to host vector.
+  template <class Allocator0>
+  void Copy(const Vector<int, VectFull, CudaAlloc<int> >& X,
+            Vector<int, VectFull, Allocator0>& Y)
+  {
+    Y.Reallocate(X.GetM());
+    if (X.GetM() > 0)
+      b200::Check(sb2_memcpy(Y.GetData(), X.GetData(), sizeof(int) * size_t(X.GetM()),
                              b200::GetStream()), "Copy(device, host)");
   }
 

@@ -174,6 +174,27 @@ class Reference(_Base):
         L.ref_coo_to_csr.argtypes = [_i, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp,
                                      _vp, _vp, _vp]
         L.ref_coo_to_csr.restype = _i
+        L.ref_write_text.argtypes = [ctypes.c_char_p, _i, _i, _i, _vp, _vp, _vp, _i]
+        L.ref_write_text.restype = _i
+        L.ref_read_text_sizes.argtypes = [ctypes.c_char_p, _i, _vp, _vp, _vp]
+        L.ref_read_text_sizes.restype = _i
+        L.ref_read_text.argtypes = [ctypes.c_char_p, _i, _vp, _vp, _vp]
+        L.ref_read_text.restype = _i
+
+    def write_text(self, path, m, n, ptr, ind, val, sym=False):
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        self.lib.ref_write_text(str(path).encode(), m, n, ind.size, _p(ptr), _p(ind), _p(val),
+                                int(sym))
+
+    def read_text(self, path, sym=False):
+        m, n, nz = (ctypes.c_int() for _ in range(3))
+        self.lib.ref_read_text_sizes(str(path).encode(), int(sym), ctypes.byref(m),
+                                     ctypes.byref(n), ctypes.byref(nz))
+        ptr = np.zeros(m.value + 1, dtype=np.int32)
+        ind = np.zeros(max(nz.value, 1), dtype=np.int32)
+        val = np.zeros(max(nz.value, 1))
+        self.lib.ref_read_text(str(path).encode(), int(sym), _p(ptr), _p(ind), _p(val))
+        return m.value, n.value, ptr, ind[:nz.value], val[:nz.value]
 
     def coo_to_csr(self, row, col, val, index=0, m_min=0, n_min=0, sym=False):
         """Seldon's own ConvertMatrix_from_Coordinates: (m, n, ptr, ind, val)."""

@@ -215,6 +215,61 @@ extern "C"
     return 0;
   }
 
+  // Seldon's text format (Matrix_Sparse.cxx:1568-1616, 1692-1724): one
+  // "row column value" line per entry, 1-based.
+  int ref_write_text(const char* path, int m, int n, int nnz, const int* ptr,
+                     const int* ind, const double* val, int sym)
+  {
+    Wrap A(m, n, nnz, ptr, ind, val, sym);
+    if (sym)
+      A.S.WriteText(std::string(path));
+    else
+      A.G.WriteText(std::string(path));
+    return 0;
+  }
+
+  // ReadText into a matrix; sizes first, then the arrays (two calls, each
+  // reading the file).
+  int ref_read_text_sizes(const char* path, int sym, int* m, int* n, int* nnz)
+  {
+    if (sym)
+      {
+        SymMat S;
+        S.ReadText(std::string(path));
+        *m = S.GetM(); *n = S.GetN(); *nnz = S.GetNonZeros();
+      }
+    else
+      {
+        GenMat G;
+        G.ReadText(std::string(path));
+        *m = G.GetM(); *n = G.GetN(); *nnz = G.GetNonZeros();
+      }
+    return 0;
+  }
+
+  int ref_read_text(const char* path, int sym, int* ptr, int* ind, double* val)
+  {
+    GenMat G;
+    SymMat S;
+    int m, nnz;
+    const int* p;
+    const int* i;
+    const double* v;
+    if (sym)
+      {
+        S.ReadText(std::string(path));
+        m = S.GetM(); nnz = S.GetNonZeros(); p = S.GetPtr(); i = S.GetInd(); v = S.GetData();
+      }
+    else
+      {
+        G.ReadText(std::string(path));
+        m = G.GetM(); nnz = G.GetNonZeros(); p = G.GetPtr(); i = G.GetInd(); v = G.GetData();
+      }
+    for (int k = 0; k <= m && p; k++) ptr[k] = p[k];
+    for (int k = 0; k < nnz; k++) { ind[k] = i[k]; val[k] = v[k]; }
+    return 0;
+  }
+
   // Seldon's binary vector format (Vector.cxx:848-870): size, then values.
   int ref_write_vector(const char* path, int n, const double* x, int with_size)
   {

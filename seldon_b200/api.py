@@ -178,6 +178,25 @@ class RowSparse:
             return cls(m, ptr, ind, val, validate)
         return cls(m, n, ptr, ind, val, validate)
 
+    def WriteText(self, path):
+        """Save as "row column value" lines (Matrix_Sparse::WriteText)."""
+        from seldon_b200 import io
+        io.write_text(path, *self.download(), sym=self.symmetric)
+
+    @classmethod
+    def ReadText(cls, path, validate=True):
+        """Load "row column value" lines (Matrix_Sparse::ReadText): the
+        triplets are parsed on the host and assembled on the device."""
+        import torch
+        from seldon_b200 import io
+        r, c, v = io.read_text(path)
+        if r.size == 0:  # ReadCoordinateMatrix leaves the cleared 0 x 0 matrix
+            if cls.symmetric:
+                return cls(0, [0], [], [], validate)
+            return cls(0, 0, [0], [], [], validate)
+        dev = [torch.as_tensor(a, device="cuda") for a in (r, c, v)]
+        return cls.from_coordinates(*dev, index=1, validate=validate)
+
     @classmethod
     def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):
         """Matrix built from coordinate triplets on the device, as

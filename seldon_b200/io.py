@@ -10,7 +10,14 @@ resume, or shared inputs):
                  int32 m, int32 n, int32 nz, int32 ptr[m+1], int32 ind[nz],
                  float64 data[nz], native byte order;
   vector         Vector<VectFull>::Write / Read (Vector.cxx:848-870): an
-                 optional int32 length, then float64 values.
+                 optional int32 length, then float64 values;
+  text           Matrix_Sparse::WriteText / ReadText (Matrix_Sparse.cxx:
+                 1568-1616, 1692-1724): one "row column value" line per entry,
+                 1-based, values with 14 significant digits.  RowSymSparse
+                 writes both triangles ordered by (row, column)
+                 (ConvertMatrix_to_Coordinates, Matrix_Conversions.cxx:
+                 100-171).  Reading yields triplets; the matrix is assembled
+                 from them as ConvertMatrix_from_Coordinates does.
 """
 import os
 
@@ -73,3 +80,61 @@ def read_vector(path, n=None):
         elif size < 8 * n:
             raise ValueError(f"{path}: holds fewer than {n} values")
         return np.fromfile(f, dtype=_F8, count=n)
+
+
+def coordinates(ptr, ind, val, sym=False):
+    """0-based (row, col, val) in the order Seldon's
+    ConvertMatrix_to_Coordinates lists a matrix: stored order for RowSparse;
+    for RowSymSparse every stored entry and its mirror, ordered by
+    (row, column) with ties kept in listing order."""
+    ptr = np.asarray(ptr, dtype=np.int64)
+    ind = np.asarray(ind, dtype=np.int64)
+    val = np.asarray(val, dtype=_F8)
+    rows = np.repeat(np.arange(ptr.size - 1, dtype=np.int64), np.diff(ptr))
+    if not sym:
+        return rows, ind, val
+    off = ind != rows
+    # listing order: each stored entry, then its mirror when off the diagonal
+    k = np.arange(ind.size)
+    slot = 2 * k
+    r = np.concatenate([rows, ind[off]])
+    c = np.concatenate([ind, rows[off]])
+    v = np.concatenate([val, val[off]])
+    o = np.concatenate([slot, slot[off] + 1])
+    listing = np.argsort(o, kind="stable")
+    r, c, v = r[listing], c[listing], v[listing]
+    order = np.lexsort((c, r))
+    return r[order], c[order], v[order]
+
+
+def write_text(path, ptr, ind, val, sym=False):
+    """Matrix_Sparse::WriteText: "row column value" lines, 1-based, the value
+    as an ostream with precision 14 prints it (%.14g)."""
+    r, c, v = coordinates(ptr, ind, val, sym)
+    with open(path, "w") as f:
+        f.write("".join(f"{a + 1} {b + 1} {x:.14g}\n"
+                        for a, b, x in zip(r.tolist(), c.tolist(), v.tolist())))
+
+
+def read_text(path):
+    """ReadCoordinateMatrix (Matrix_Sparse.cxx:1885-1950): 1-based triplets
+    (row, col, val) up to the first line that does not parse.  A row or
+    column below 1 raises ValueError (Seldon's IOError)."""
+    with open(path) as f:
+        tok = f.read().split()
+    rows, cols, vals = [], [], []
+    for k in range(0, len(tok) - 2, 3):
+        try:
+            a, b, x = int(tok[k]), int(tok[k + 1]), float(tok[k + 2])
+        except ValueError:
+            break
+        if a < 1:
+            raise ValueError(f"{path}: Row number should be greater than 0 but is equal to {a}")
+        if b < 1:
+            raise ValueError(f"{path}: Column number should be greater than 0 but is equal "
+                             f"to {b}")
+        rows.append(a)
+        cols.append(b)
+        vals.append(x)
+    return (np.array(rows, dtype=np.int32), np.array(cols, dtype=np.int32),
+            np.array(vals, dtype=_F8))

@@ -573,6 +573,126 @@ int main()
     report(same, "binary_files", "device Write -> Seldon Read, Seldon Write -> device Read");
   }
 
+  // ------------------------------------------------ coordinate form
+  {
+    // 1-based triplets in scrambled order with many duplicates
+    const int nt = 5000, mr = 97, nc = 83;
+    Vector<int> R0(nt), C0(nt);
+    HostVec V0(nt);
+    unsigned long long st = 88172645463325252ULL;
+    for (int k = 0; k < nt; k++)
+      {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+        R0(k) = 1 + int(st % mr);
+        C0(k) = 1 + int((st >> 20) % nc);
+        V0(k) = double(int((st >> 40) % 2001) - 1000) / 7.0;
+      }
+    bool same = true;
+    for (int sym = 0; sym < 2; sym++)
+      for (int dev_triplets = 0; dev_triplets < 2; dev_triplets++)
+        {
+          Vector<int> R(R0), C(C0), R2(R0), C2(C0);
+          HostVec V(V0), V2(V0);
+          std::vector<int> hp, hi, dp, di;
+          std::vector<double> hv, dv;
+          if (sym)
+            {
+              // square the pattern so both triangles appear
+              for (int k = 0; k < nt; k++)
+                {
+                  C(k) = 1 + (C(k) - 1) % mr;
+                  C2(k) = C(k);
+                }
+              HostSym Ah;
+              ConvertMatrix_from_Coordinates(R, C, V, Ah, 1);
+              DevSym Ad;
+              if (dev_triplets)
+                {
+                  Vector<int, VectFull, CudaAlloc<int> > Rd, Cd;
+                  DevVec Vd;
+                  Copy(R2, Rd);
+                  Copy(C2, Cd);
+                  Copy(V2, Vd);
+                  ConvertMatrix_from_Coordinates(Rd, Cd, Vd, Ad, 1);
+                  same = same && Rd.GetM() == 0 && Vd.GetM() == 0;
+                }
+              else
+                ConvertMatrix_from_Coordinates(R2, C2, V2, Ad, 1);
+              same = same && Ad.GetM() == Ah.GetM() && Ad.GetN() == Ah.GetN();
+              Ad.Download(dp, di, dv);
+              for (int k = 0; same && k <= Ah.GetM(); k++)
+                same = dp[k] == Ah.GetPtr()[k];
+              for (int k = 0; same && k < Ah.GetNonZeros(); k++)
+                same = di[k] == Ah.GetInd()[k] && dv[k] == Ah.GetData()[k];
+              same = same && int(di.size()) == Ah.GetNonZeros();
+            }
+          else
+            {
+              HostGen Ah;
+              ConvertMatrix_from_Coordinates(R, C, V, Ah, 1);
+              DevGen Ad;
+              if (dev_triplets)
+                {
+                  Vector<int, VectFull, CudaAlloc<int> > Rd, Cd;
+                  DevVec Vd;
+                  Copy(R2, Rd);
+                  Copy(C2, Cd);
+                  Copy(V2, Vd);
+                  ConvertMatrix_from_Coordinates(Rd, Cd, Vd, Ad, 1);
+                }
+              else
+                ConvertMatrix_from_Coordinates(R2, C2, V2, Ad, 1);
+              same = same && Ad.GetM() == Ah.GetM() && Ad.GetN() == Ah.GetN();
+              Ad.Download(dp, di, dv);
+              for (int k = 0; same && k <= Ah.GetM(); k++)
+                same = dp[k] == Ah.GetPtr()[k];
+              for (int k = 0; same && k < Ah.GetNonZeros(); k++)
+                same = di[k] == Ah.GetInd()[k] && dv[k] == Ah.GetData()[k];
+              same = same && int(di.size()) == Ah.GetNonZeros();
+            }
+        }
+    report(same, "coordinate_assembly",
+           "ConvertMatrix_from_Coordinates on the device == Seldon's (host and device triplets)");
+
+    // text files both ways: Seldon's WriteText -> device ReadText, and the
+    // device WriteText gives the same bytes as Seldon's
+    const std::string t1 = "dropin_text_ref.txt", t2 = "dropin_text_dev.txt";
+    bool text_ok = true;
+    {
+      Gh.WriteText(t1);
+      DevGen Gx;
+      Gx.ReadText(t1);
+      HostGen Gr;
+      Gr.ReadText(t1);
+      std::vector<int> p, i;
+      std::vector<double> v;
+      Gx.Download(p, i, v);
+      text_ok = Gx.GetM() == Gr.GetM() && Gx.GetN() == Gr.GetN() && int(i.size()) == Gr.GetNonZeros();
+      for (int k = 0; text_ok && k < Gr.GetNonZeros(); k++)
+        text_ok = i[k] == Gr.GetInd()[k] && v[k] == Gr.GetData()[k];
+      Gd.WriteText(t2);
+      std::ifstream a(t1.c_str()), b(t2.c_str());
+      std::string sa((std::istreambuf_iterator<char>(a)), std::istreambuf_iterator<char>());
+      std::string sb((std::istreambuf_iterator<char>(b)), std::istreambuf_iterator<char>());
+      text_ok = text_ok && sa == sb && !sa.empty();
+    }
+    {
+      Sh.WriteText(t1);
+      Sd.WriteText(t2);
+      std::ifstream a(t1.c_str()), b(t2.c_str());
+      std::string sa((std::istreambuf_iterator<char>(a)), std::istreambuf_iterator<char>());
+      std::string sb((std::istreambuf_iterator<char>(b)), std::istreambuf_iterator<char>());
+      DevSym Sx;
+      Sx.ReadText(t1);
+      HostSym Sr;
+      Sr.ReadText(t1);
+      text_ok = text_ok && sa == sb && Sx.GetNonZeros() == Sr.GetNonZeros() && Sx.GetM() == Sr.GetM();
+    }
+    std::remove(t1.c_str());
+    std::remove(t2.c_str());
+    report(text_ok, "text_files", "ReadText/WriteText match Seldon's");
+  }
+
   // ------------------------------------------------ errors
   {
     bool thrown = false;

@@ -152,3 +152,26 @@ def test_symmetric_from_coordinates(cuda, oracle):
     api.Mlt(ref, x, y2)
     torch.cuda.synchronize()
     assert torch.equal(y1, y2)
+
+
+@pytest.mark.parametrize("sym", [False, True])
+def test_text_files_device(cuda, oracle, tmp_path, sym):
+    """ReadText assembles on the device what the oracle assembles from the
+    same lines; WriteText of the device matrix gives the same bytes as the
+    host arrays written directly."""
+    from seldon_b200 import api, io
+    ptr, ind, val = matgen.convdiff3d(9)
+    if sym:
+        ptr, ind, val = matgen.upper(*matgen.lap2d(30))
+    m = ptr.size - 1
+    f1, f2 = tmp_path / "a.txt", tmp_path / "b.txt"
+    io.write_text(f1, ptr, ind, val, sym=sym)
+    cls = api.RowSymSparse if sym else api.RowSparse
+    A = cls.ReadText(f1)
+    r, c, v = io.read_text(f1)
+    want = oracle.coo_to_csr(r, c, v, 1, 0, 0, sym)
+    assert (A.m, A.n) == want[:2] == (m, m)
+    for a, b in zip(A.download(), want[2:]):
+        assert np.array_equal(a, b)
+    A.WriteText(f2)
+    assert f1.read_bytes() == f2.read_bytes()

@@ -24,7 +24,8 @@ def test_cpp_dropin(cuda, tmp_path):
     names = {ln.split()[1] for ln in lines}
     for must in ("spmv_general", "spmv_symmetric", "blas1", "cg_identity", "cg_ssor",
                  "gmres20_jacobi", "bicgstab_identity", "cg_user_preconditioner",
-                 "cg_zero_rhs", "invalid_csr_throws", "binary_files"):
+                 "cg_zero_rhs", "invalid_csr_throws", "binary_files",
+                 "coordinate_assembly", "text_files"):
         assert must in names, must
     # Seldon's other Krylov drivers, its generic templates on device types
     for drv in ("bicg", "bicgstabl", "bicgcr", "cgne", "cgs", "cocg", "gcr", "lsqr", "minres",

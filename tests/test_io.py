@@ -58,3 +58,40 @@ def test_damaged_files_are_rejected(tmp_path):
     (tmp_path / "vs.bin").write_bytes(v.read_bytes()[:-1])
     with pytest.raises(ValueError):
         io.read_vector(tmp_path / "vs.bin")
+
+
+@pytest.mark.parametrize("name", list(_cases()))
+def test_text_same_bytes_and_read_back(reference, oracle, tmp_path, name):
+    """WriteText gives Seldon's bytes; ReadText's triplets assembled as
+    ConvertMatrix_from_Coordinates does give the matrix Seldon reads."""
+    m, n, ptr, ind, val, sym = _cases()[name]
+    ours, theirs = tmp_path / "ours.txt", tmp_path / "theirs.txt"
+    io.write_text(ours, ptr, ind, val, sym=sym)
+    reference.write_text(theirs, m, n, ptr, ind, val, sym=sym)
+    assert ours.read_bytes() == theirs.read_bytes()
+    r, c, v = io.read_text(theirs)
+    got = oracle.coo_to_csr(r, c, v, 1, 0, 0, sym)
+    want = reference.read_text(theirs, sym=sym)
+    assert got[:2] == want[:2]
+    for a, b in zip(got[2:], want[2:]):
+        assert np.array_equal(a, b)
+
+
+def test_text_values_printed_like_ostream(reference, tmp_path):
+    ptr = np.array([0, 4], dtype=np.int32)
+    ind = np.array([0, 1, 2, 3], dtype=np.int32)
+    val = np.array([1.0 / 3.0, -2.5e-300, 123456789012345.0, 0.1])
+    ours, theirs = tmp_path / "ours.txt", tmp_path / "theirs.txt"
+    io.write_text(ours, ptr, ind, val)
+    reference.write_text(theirs, 1, 4, ptr, ind, val)
+    assert ours.read_bytes() == theirs.read_bytes()
+
+
+def test_text_read_stops_and_rejects(tmp_path):
+    p = tmp_path / "t.txt"
+    p.write_text("1 1 2.0\n2 3 -1\nnot a number\n4 4 4\n")
+    r, c, v = io.read_text(p)
+    assert r.tolist() == [1, 2] and c.tolist() == [1, 3] and v.tolist() == [2.0, -1.0]
+    p.write_text("1 1 2.0\n0 3 -1\n")
+    with pytest.raises(ValueError):
+        io.read_text(p)
