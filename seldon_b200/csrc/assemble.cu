@@ -5,21 +5,25 @@
 // Seldon sorts the triplets by row, then each row by column, both times with
 // its bottom-up merge sort (vector/Functions_Arrays.cxx:412-500), which keeps
 // equal keys in input order.  The result is the triplets in stable
-// (row, column) order, duplicates kept as separate entries.  Here that order
-// comes from one stable LSD radix sort of the packed key (row << cb) | col,
-// with the input position carried as the payload:
+// (row, column) order, duplicates kept as separate entries.  Here:
 //
-//   k_coo_stats     sizes: largest row and column, bad indices, kept count
-//   k_coo_keys      packed keys and positions (RowSymSparse: entries below
-//                   the diagonal get row m, past every kept row)
-//   per 8-bit digit k_radix_hist  -> scan -> k_radix_scatter
-//   k_coo_ptr       ptr[r] = first sorted key of row >= r (binary search)
-//   k_coo_gather    ind from the keys, values through the positions
+//   k_coo_stats       sizes: largest row and column, bad indices, kept count
+//   k_row_count       entries per row (warp-aggregated atomics), scanned
+//                     into ptr
+//   k_row_scatter     each entry's key (column << ib | input position) to a
+//                     free slot of its row (atomics: any order inside a row)
+//   k_row_sort_short  rows of up to 32 entries, one thread each: an entry's
+//                     place is the number of smaller keys in its row; the
+//                     keys are distinct (they hold the input position), so
+//                     the order is (column, input position) exactly
+//   k_row_sort_cta    rows of 33..4096 entries, one CTA each: bitonic sort
+//                     in shared memory
+//   longer rows       the stable LSD radix sort below, on the row's keys
+//   (the sorted keys give ind directly and val through the position)
 //
-// All of it is integer and byte movement bound by HBM bandwidth.  A tile of
-// 4096 triplets is one CTA; the scatter ranks a tile's entries in 16 chunks
-// of 256 with a warp match plus per-warp digit counters in shared memory, so
-// the order inside a digit is the input order (stability).
+// All of it is integer and byte movement bound by HBM bandwidth and L2
+// atomics; the matrix comes out deterministic whatever order the atomics
+// take, because every row is sorted on distinct keys afterwards.
 #include <algorithm>
 #include <climits>
 #include <utility>
@@ -69,19 +73,6 @@ k_coo_stats(const int* __restrict__ row, const int* __restrict__ col, long long 
   }
 }
 
-template <typename K>
-__global__ void __launch_bounds__(kAsmThreads)
-k_coo_keys(const int* __restrict__ row, const int* __restrict__ col, long long nnz, int index,
-           int cb, int sym, int m, K* __restrict__ key, int* __restrict__ pos) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += stride) {
-    const int r = row[i] - index, c = col[i] - index;
-    const int rk = (sym && r > c) ? m : r;
-    key[i] = ((K)(unsigned)rk << cb) | (K)(unsigned)c;
-    pos[i] = (int)i;
-  }
-}
-
 // Digit counts of each tile, stored digit-major: hist[d * ntiles + tile].
 template <typename K>
 __global__ void __launch_bounds__(kAsmThreads)
@@ -121,7 +112,7 @@ k_radix_scatter(const K* __restrict__ kin, const int* __restrict__ pin, long lon
     const long long i = c0 + tid;
     const bool valid = i < nnz;
     const K k = valid ? kin[i] : K(0);
-    const int p = valid ? pin[i] : 0;
+    const int p = (valid && pin) ? pin[i] : 0;
     const unsigned d = valid ? ((unsigned)(k >> shift) & (kBins - 1)) : (unsigned)kBins;
     const unsigned peers = __match_any_sync(0xffffffffu, d);
     const unsigned before = peers & ((1u << lane) - 1u);
@@ -142,7 +133,7 @@ k_radix_scatter(const K* __restrict__ kin, const int* __restrict__ pin, long lon
     if (valid) {
       const int q = s_off[warp][d] + __popc(before);
       kout[q] = k;
-      pout[q] = p;
+      if (pout) pout[q] = p;
     }
   }
 }
@@ -220,33 +211,121 @@ k_scan_tiles(int* __restrict__ a, long long n, const int* __restrict__ sums) {
   }
 }
 
-template <typename K>
+// Entries per row.  Lanes of a warp that hit the same row add once.
 __global__ void __launch_bounds__(kAsmThreads)
-k_coo_ptr(const K* __restrict__ key, long long nnz, int m, int cb, int* __restrict__ ptr) {
+k_row_count(const int* __restrict__ row, const int* __restrict__ col, long long nnz, int index,
+            int sym, int* __restrict__ cnt) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r <= m; r += stride) {
-    // 64-bit target: rows up to m, past the largest stored row, may not fit K
-    const unsigned long long target = (unsigned long long)r << cb;
-    long long lo = 0, hi = nnz;  // first key >= target
-    while (lo < hi) {
-      const long long mid = (lo + hi) >> 1;
-      if ((unsigned long long)key[mid] < target) lo = mid + 1;
-      else hi = mid;
+  const int lane = threadIdx.x & 31;
+  for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < nnz; i0 += stride) {
+    const long long i = i0 + threadIdx.x;
+    int r = -1;
+    if (i < nnz) {
+      r = row[i] - index;
+      if (sym && r > col[i] - index) r = -1;  // below the diagonal: dropped
     }
-    ptr[r] = (int)lo;
+    const unsigned peers = __match_any_sync(0xffffffffu, r);
+    if (r >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[r], __popc(peers));
   }
 }
 
-template <typename K>
+// Each kept entry's key to a free slot of its row.
 __global__ void __launch_bounds__(kAsmThreads)
-k_coo_gather(const K* __restrict__ key, const int* __restrict__ pos,
-             const double* __restrict__ val, long long nout, K cmask, int* __restrict__ ind,
-             double* __restrict__ vout) {
+k_row_scatter(const int* __restrict__ row, const int* __restrict__ col, long long nnz, int index,
+              int sym, int ib, int* __restrict__ fill, unsigned long long* __restrict__ key) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nout; k += stride) {
-    ind[k] = (int)(key[k] & cmask);
-    vout[k] = val[pos[k]];
+  const int lane = threadIdx.x & 31;
+  for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < nnz; i0 += stride) {
+    const long long i = i0 + threadIdx.x;
+    int r = -1, c = 0;
+    if (i < nnz) {
+      r = row[i] - index;
+      c = col[i] - index;
+      if (sym && r > c) r = -1;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, r);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (r >= 0 && lane == leader) base = atomicAdd(&fill[r], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (r >= 0) {
+      const int slot = base + __popc(peers & ((1u << lane) - 1u));
+      key[slot] = ((unsigned long long)(unsigned)c << ib) | (unsigned long long)i;
+    }
   }
+}
+
+__device__ __forceinline__ void emit(unsigned long long k, long long at, int ib,
+                                     const double* __restrict__ val, int* __restrict__ ind,
+                                     double* __restrict__ vout) {
+  ind[at] = (int)(k >> ib);
+  vout[at] = val[k & ((1ull << ib) - 1ull)];
+}
+
+constexpr int kShortRow = 32;
+constexpr int kCtaRow = 4096;
+
+// Rows of up to kShortRow entries; longer ones are listed for the CTA and
+// segment sorts.
+__global__ void __launch_bounds__(kAsmThreads)
+k_row_sort_short(const int* __restrict__ ptr, int m, const unsigned long long* __restrict__ key,
+                 int ib, const double* __restrict__ val, int* __restrict__ ind,
+                 double* __restrict__ vout, int* __restrict__ long_rows, int* __restrict__ nlong) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += stride) {
+    const int b = ptr[r], e = ptr[r + 1];
+    if (e - b > kShortRow) {
+      long_rows[atomicAdd(nlong, 1)] = r;
+      continue;
+    }
+    for (int a = b; a < e; ++a) {
+      const unsigned long long ka = key[a];
+      int rank = 0;
+      for (int c = b; c < e; ++c) rank += key[c] < ka;
+      emit(ka, b + rank, ib, val, ind, vout);
+    }
+  }
+}
+
+// One CTA per listed row of kShortRow+1..kCtaRow entries: bitonic sort of the
+// row's keys (padded with the largest key) in shared memory.
+__global__ void __launch_bounds__(kAsmThreads)
+k_row_sort_cta(const int* __restrict__ ptr, const int* __restrict__ rows,
+               const unsigned long long* __restrict__ key, int ib,
+               const double* __restrict__ val, int* __restrict__ ind,
+               double* __restrict__ vout) {
+  __shared__ unsigned long long s[kCtaRow];
+  const int r = rows[blockIdx.x];
+  const int b = ptr[r], L = ptr[r + 1] - b;
+  if (L > kCtaRow) return;  // segment-sorted on its own
+  int P = 1;
+  while (P < L) P <<= 1;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) s[i] = i < L ? key[b + i] : ~0ull;
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int x = i ^ j;
+        if (x > i) {
+          const unsigned long long u = s[i], v = s[x];
+          if ((u > v) == ((i & k) == 0)) {
+            s[i] = v;
+            s[x] = u;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < L; i += blockDim.x) emit(s[i], b + i, ib, val, ind, vout);
+}
+
+// A sorted segment of keys written out.
+__global__ void __launch_bounds__(kAsmThreads)
+k_emit_segment(const unsigned long long* __restrict__ key, long long b, long long L, int ib,
+               const double* __restrict__ val, int* __restrict__ ind, double* __restrict__ vout) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride)
+    emit(key[b + i], b + i, ib, val, ind, vout);
 }
 
 int bits_for(long long v) {  // bits needed to store 0..v
@@ -271,7 +350,8 @@ int excl_scan(int* a, long long n, cudaStream_t s) {
   return map_cuda_error(cudaGetLastError());
 }
 
-// Sort keys/positions in place (the result ends in key/pos) over `bits` bits.
+// Stable sort of keys (and positions, when pos is not null) in place over
+// the low `bits` bits.
 template <typename K>
 int radix_sort(K* key, int* pos, long long nnz, int bits, cudaStream_t s) {
   if (nnz <= 1 || bits <= 0) return SB2_OK;
@@ -280,7 +360,7 @@ int radix_sort(K* key, int* pos, long long nnz, int bits, cudaStream_t s) {
   K* k2 = nullptr;
   int *p2 = nullptr, *hist = nullptr;
   cudaError_t e = pool_malloc((void**)&k2, sizeof(K) * nnz, s);
-  if (e == cudaSuccess) e = pool_malloc((void**)&p2, sizeof(int) * nnz, s);
+  if (e == cudaSuccess && pos) e = pool_malloc((void**)&p2, sizeof(int) * nnz, s);
   if (e == cudaSuccess) e = pool_malloc((void**)&hist, sizeof(int) * nh, s);
   int st = map_cuda_error(e);
   K *ka = key, *kb = k2;
@@ -297,7 +377,8 @@ int radix_sort(K* key, int* pos, long long nnz, int bits, cudaStream_t s) {
   }
   if (st == SB2_OK && ka != key) {
     e = cudaMemcpyAsync(key, ka, sizeof(K) * nnz, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(pos, pa, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && pos)
+      e = cudaMemcpyAsync(pos, pa, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s);
     st = map_cuda_error(e);
   }
   if (k2) cudaFreeAsync(k2, s);
@@ -306,32 +387,66 @@ int radix_sort(K* key, int* pos, long long nnz, int bits, cudaStream_t s) {
   return st;
 }
 
-template <typename K>
 int assemble(long long nnz, const int* row, const int* col, const double* val, int index, int m,
-             int n, int cb, int rbits, int sym, long long nout, int* ptr, int* ind, double* vout,
-             cudaStream_t s) {
+             int cb, int sym, long long nout, int* ptr, int* ind, double* vout, cudaStream_t s) {
   const int grid = num_sms(current_device()) * 8;
-  K* key = nullptr;
-  int* pos = nullptr;
-  cudaError_t e = cudaSuccess;
-  if (nnz > 0) {
-    e = pool_malloc((void**)&key, sizeof(K) * nnz, s);
-    if (e == cudaSuccess) e = pool_malloc((void**)&pos, sizeof(int) * nnz, s);
-  }
+  SB2_CUDA_TRY(cudaMemsetAsync(ptr, 0, sizeof(int) * ((size_t)m + 1), s));
+  if (nout == 0) return SB2_OK;
+  const int ib = bits_for(nnz - 1);  // input positions 0..nnz-1
+  if (ib + cb > 64) return SB2_ERR_INVALID_VALUE;
+  unsigned long long* key = nullptr;
+  int *fill = nullptr, *long_rows = nullptr, *nlong = nullptr;
+  cudaError_t e = pool_malloc((void**)&key, sizeof(unsigned long long) * nout, s);
+  if (e == cudaSuccess) e = pool_malloc((void**)&fill, sizeof(int) * ((size_t)m + 1), s);
+  if (e == cudaSuccess) e = pool_malloc((void**)&long_rows, sizeof(int) * ((size_t)m + 1), s);
+  if (e == cudaSuccess) e = pool_malloc((void**)&nlong, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(nlong, 0, sizeof(int), s);
   int st = map_cuda_error(e);
-  if (st == SB2_OK && nnz > 0) {
-    k_coo_keys<K><<<grid, kAsmThreads, 0, s>>>(row, col, nnz, index, cb, sym, m, key, pos);
-    st = radix_sort<K>(key, pos, nnz, rbits + cb, s);
+  int h_nlong = 0;
+  std::vector<int> hrows, hptr;
+  if (st == SB2_OK) {
+    k_row_count<<<grid, kAsmThreads, 0, s>>>(row, col, nnz, index, sym, ptr);
+    st = excl_scan(ptr, (long long)m + 1, s);
   }
   if (st == SB2_OK) {
-    k_coo_ptr<K><<<grid, kAsmThreads, 0, s>>>(key, nnz, m, cb, ptr);
-    if (nout > 0)
-      k_coo_gather<K><<<grid, kAsmThreads, 0, s>>>(key, pos, val, nout,
-                                                   (K)((1ull << cb) - 1ull), ind, vout);
-    st = map_cuda_error(cudaGetLastError());
+    e = cudaMemcpyAsync(fill, ptr, sizeof(int) * ((size_t)m + 1), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) {
+      k_row_scatter<<<grid, kAsmThreads, 0, s>>>(row, col, nnz, index, sym, ib, fill, key);
+      k_row_sort_short<<<grid, kAsmThreads, 0, s>>>(ptr, m, key, ib, val, ind, vout, long_rows,
+                                                    nlong);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_nlong, nlong, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    st = map_cuda_error(e);
   }
-  if (key) cudaFreeAsync(key, s);
-  if (pos) cudaFreeAsync(pos, s);
+  if (st == SB2_OK && h_nlong > 0) {
+    k_row_sort_cta<<<h_nlong, kAsmThreads, 0, s>>>(ptr, long_rows, key, ib, val, ind, vout);
+    // rows past the CTA sort: each sorted on its own
+    hrows.resize(h_nlong);
+    hptr.resize((size_t)m + 1);
+    e = cudaMemcpyAsync(hrows.data(), long_rows, sizeof(int) * h_nlong, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hptr.data(), ptr, sizeof(int) * ((size_t)m + 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    st = map_cuda_error(e);
+    for (int k = 0; st == SB2_OK && k < h_nlong; ++k) {
+      const int r = hrows[k];
+      const long long b = hptr[r], L = (long long)hptr[r + 1] - b;
+      if (L <= kCtaRow) continue;
+      st = radix_sort<unsigned long long>(key + b, nullptr, L, ib + cb, s);
+      if (st == SB2_OK) {
+        const int g = (int)std::min<long long>((L + kAsmThreads - 1) / kAsmThreads, grid);
+        k_emit_segment<<<g, kAsmThreads, 0, s>>>(key, b, L, ib, val, ind, vout);
+        st = map_cuda_error(cudaGetLastError());
+      }
+    }
+  }
+  if (st == SB2_OK) st = map_cuda_error(cudaGetLastError());
+  cudaFreeAsync(key, s);
+  cudaFreeAsync(fill, s);
+  cudaFreeAsync(long_rows, s);
+  cudaFreeAsync(nlong, s);
   return st;
 }
 
@@ -387,10 +502,7 @@ int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val, i
     nout = nnz;
   }
   if (m >= INT_MAX || n >= INT_MAX) return SB2_ERR_INVALID_VALUE;
-  // key bits: rows 0..m-1 (0..m with the RowSymSparse lower-part marker),
-  // columns 0..max(col)
-  const int rbits = bits_for(symmetric_upper ? m : m - 1);
-  const int cb = bits_for(nnz > 0 ? h.col_max : 0);
+  const int cb = bits_for(nnz > 0 ? h.col_max : 0);  // columns 0..max(col)
 
   int *dp = nullptr, *di = nullptr;
   double* dv = nullptr;
@@ -398,14 +510,8 @@ int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val, i
   if (e == cudaSuccess && nout > 0) e = cudaMalloc((void**)&di, sizeof(int) * nout);
   if (e == cudaSuccess && nout > 0) e = cudaMalloc((void**)&dv, sizeof(double) * nout);
   int st = map_cuda_error(e);
-  if (st == SB2_OK) {
-    if (rbits + cb <= 32)
-      st = assemble<unsigned>(nnz, row, col, val, index, (int)m, (int)n, cb, rbits,
-                              symmetric_upper, nout, dp, di, dv, s);
-    else
-      st = assemble<unsigned long long>(nnz, row, col, val, index, (int)m, (int)n, cb, rbits,
-                                        symmetric_upper, nout, dp, di, dv, s);
-  }
+  if (st == SB2_OK)
+    st = assemble(nnz, row, col, val, index, (int)m, cb, symmetric_upper, nout, dp, di, dv, s);
   if (st == SB2_OK) st = map_cuda_error(cudaStreamSynchronize(s));
   if (st != SB2_OK) {
     cudaFree(dp);
