@@ -71,6 +71,19 @@ class Oracle(_Base):
         L.orc_coo_sizes.restype = _i
         L.orc_coo_to_csr.argtypes = [_i, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]
         L.orc_coo_to_csr.restype = None
+        L.orc_ilut_solve.argtypes = [_i, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]
+        L.orc_ilut_solve.restype = None
+
+    def ilut_solve(self, factor, r, sym=False, trans=False):
+        """z = M^{-1} r (or M^{-T} r) with factor = (fptr, find, fval,
+        perm_row, perm_col) as the reference returns it."""
+        fp, fi, fv, pr, pc = (np.ascontiguousarray(a) for a in factor)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        self.lib.orc_ilut_solve(r.size, _p(fp.astype(np.int32)), _p(fi.astype(np.int32)),
+                                _p(fv.astype(np.float64)), int(sym), _p(pr.astype(np.int32)),
+                                _p(pc.astype(np.int32)), int(trans), _p(r), _p(z))
+        return z
 
     def coo_to_csr(self, row, col, val, index=0, m_min=0, n_min=0, sym=False):
         """ConvertMatrix_from_Coordinates restated: (m, n, ptr, ind, val)."""
@@ -180,6 +193,56 @@ class Reference(_Base):
         L.ref_read_text_sizes.restype = _i
         L.ref_read_text.argtypes = [ctypes.c_char_p, _i, _vp, _vp, _vp]
         L.ref_read_text.restype = _i
+        L.ref_ilut_factor.argtypes = [_i, _i, _vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _d, _d, _d,
+                                      _vp]
+        L.ref_ilut_factor.restype = _i
+        L.ref_ilut_get.argtypes = [_i, _vp, _vp, _vp, _vp, _vp]
+        L.ref_ilut_get.restype = _i
+        L.ref_ilut_solve.argtypes = [_i, _i, _vp, _vp]
+        L.ref_ilut_solve.restype = _i
+        L.ref_solve_ilut.argtypes = [_i, _i, _i, _vp, _vp, _vp, _i, _vp, _vp, _d, _i, _i, _i, _vp]
+        L.ref_solve_ilut.restype = _i
+
+    ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
+
+    def ilut_factor(self, ptr, ind, val, sym=False, perm=None, type_ilu=0, fill_level=1000000,
+                    additional_fill=1000000, mbloc=1000000, alpha=1.0, droptol=0.01,
+                    permtol=0.1):
+        """Seldon's IlutPreconditioning factorization (held for ilut_solve and
+        solve_ilut): returns (fptr, find, fval, perm_row, perm_col)."""
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        n = ptr.size - 1
+        pm = None if perm is None else np.ascontiguousarray(perm, dtype=np.int32)
+        nz = ctypes.c_int()
+        self.lib.ref_ilut_factor(n, ind.size, _p(ptr), _p(ind), _p(val), int(sym), _p(pm),
+                                 type_ilu, fill_level, additional_fill, mbloc, alpha, droptol,
+                                 permtol, ctypes.byref(nz))
+        fptr = np.zeros(n + 1, dtype=np.int32)
+        find = np.zeros(max(nz.value, 1), dtype=np.int32)
+        fval = np.zeros(max(nz.value, 1))
+        pr = np.zeros(max(n, 1), dtype=np.int32)
+        pc = np.zeros(max(n, 1), dtype=np.int32)
+        self.lib.ref_ilut_get(n, _p(fptr), _p(find), _p(fval), _p(pr), _p(pc))
+        return fptr, find[:nz.value], fval[:nz.value], pr[:n], pc[:n]
+
+    def ilut_solve(self, r, trans=False):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        self.lib.ref_ilut_solve(int(trans), r.size, _p(r), _p(z))
+        return z
+
+    def solve_ilut(self, which, ptr, ind, val, b, sym=False, x0=None, tol=1e-10,
+                   max_iter=400, restart=10):
+        """Cg/BiCgStab/Gmres preconditioned by the held ILUT factor."""
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+        nb = ctypes.c_int()
+        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        code = self.lib.ref_solve_ilut(w, ptr.size - 1, ind.size, _p(ptr), _p(ind), _p(val),
+                                       int(sym), _p(x), _p(b), tol, max_iter, restart,
+                                       int(x0 is None), ctypes.byref(nb))
+        return x, code, nb.value
 
     def write_text(self, path, m, n, ptr, ind, val, sym=False):
         ptr, ind, val = _csr_args(ptr, ind, val)

@@ -22,6 +22,15 @@
 // Matrices and vectors wrap the caller's buffers through SetData/Nullify
 // (Matrix_Sparse.cxx:397-412), so nothing is copied.
 
+// The ILUT preconditioner (computation/solver/preconditioner/) is compiled
+// in only with SELDON_WITH_PRECONDITIONING (SeldonSolver.hxx:49-51).  As
+// shipped it does not compile: GetIlut calls param.GetFactorizationType()
+// (IlutPreconditioning.cxx:509, SymmetricIlutPreconditioning.cxx:38) while
+// the class declares GetFactorisationType() (IlutPreconditioning.hxx:70).
+// The macro below maps the one misspelt name; nothing else is changed.
+#define SELDON_WITH_PRECONDITIONING
+#define GetFactorizationType GetFactorisationType
+
 #include "Seldon.hxx"
 
 namespace Seldon
@@ -383,6 +392,139 @@ extern "C"
         for (int k = 0; k < *nnz_out; k++) { ind[k] = q[k]; vout[k] = v[k]; }
       }
     return 0;
+  }
+
+  // ------------------------------------------------------------ ILUT
+  // IlutPreconditioning (IlutPreconditioning.cxx): Seldon factorizes with its
+  // own GetIlut; the factor (ArrayRowSparse / ArrayRowSymSparse rows in
+  // stored order) and the permutations are handed back as flat arrays.  One
+  // factorization is held at a time (test infrastructure, one thread).
+  typedef IlutPreconditioning<double, double> Ilut;
+
+  // Reads the factor out of the protected members through pointers to
+  // members named in a derived class.
+  struct IlutAccess : Ilut
+  {
+    static const Matrix<double, General, ArrayRowSparse>& unsym(const Ilut& p)
+    { return p.*(&IlutAccess::mat_unsym); }
+    static const Matrix<double, Symmetric, ArrayRowSymSparse>& sym(const Ilut& p)
+    { return p.*(&IlutAccess::mat_sym); }
+    static const IVect& prow(const Ilut& p) { return p.*(&IlutAccess::permutation_row); }
+    static const IVect& pcol(const Ilut& p) { return p.*(&IlutAccess::permutation_col); }
+  };
+
+  Ilut* g_ilut = 0;
+  bool g_ilut_sym = false;
+
+  // type_ilu: ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K (0..5).  sym selects
+  // RowSymSparse input and the symmetric algorithm (FactorizeSymMatrix);
+  // otherwise RowSparse and FactorizeMatrix.  perm may be NULL (identity).
+  int ref_ilut_factor(int n, int nnz, const int* ptr, const int* ind,
+                      const double* val, int sym, const int* perm, int type_ilu,
+                      int fill_level, int additional_fill, int mbloc,
+                      double alpha, double droptol, double permtol,
+                      int* nnz_factor)
+  {
+    delete g_ilut;
+    g_ilut = new Ilut();
+    g_ilut->SetFactorisationType(type_ilu);
+    g_ilut->SetFillLevel(fill_level);
+    g_ilut->SetAdditionalFillNumber(additional_fill);
+    g_ilut->SetPivotBlockInteger(mbloc);
+    g_ilut->SetDiagonalCoefficient(alpha);
+    g_ilut->SetDroppingThreshold(droptol);
+    g_ilut->SetPivotThreshold(permtol);
+    IVect P(n);
+    for (int i = 0; i < n; i++)
+      P(i) = perm ? perm[i] : i;
+    Vector<int> p(n + 1), q(nnz);
+    Vec v(nnz);
+    for (int i = 0; i <= n; i++) p(i) = ptr[i];
+    for (int k = 0; k < nnz; k++) { q(k) = ind[k]; v(k) = val[k]; }
+    g_ilut_sym = sym != 0;
+    int total = 0;
+    if (g_ilut_sym)
+      {
+        SymMat S(n, n, v, p, q);
+        g_ilut->SetSymmetricAlgorithm();
+        g_ilut->FactorizeSymMatrix(P, S);
+        const Matrix<double, Symmetric, ArrayRowSymSparse>& F = IlutAccess::sym(*g_ilut);
+        for (int i = 0; i < n; i++) total += F.GetRowSize(i);
+      }
+    else
+      {
+        GenMat G(n, n, v, p, q);
+        g_ilut->SetUnsymmetricAlgorithm();
+        g_ilut->FactorizeMatrix(P, G);
+        const Matrix<double, General, ArrayRowSparse>& F = IlutAccess::unsym(*g_ilut);
+        for (int i = 0; i < n; i++) total += F.GetRowSize(i);
+      }
+    *nnz_factor = total;
+    return 0;
+  }
+
+  // The held factor: fptr[n+1], find/fval[nnz_factor], permutation_row and
+  // permutation_col (the row permutation again for the symmetric algorithm).
+  int ref_ilut_get(int n, int* fptr, int* find, double* fval, int* perm_row,
+                   int* perm_col)
+  {
+    if (!g_ilut) return -1;
+    fptr[0] = 0;
+    int t = 0;
+    for (int i = 0; i < n; i++)
+      {
+        int len = g_ilut_sym ? IlutAccess::sym(*g_ilut).GetRowSize(i)
+          : IlutAccess::unsym(*g_ilut).GetRowSize(i);
+        for (int k = 0; k < len; k++, t++)
+          {
+            // the symmetric factor keeps 1/D in position 0, whose index
+            // GetIlut leaves unset and SolveLU never reads: i is written
+            find[t] = g_ilut_sym ? (k == 0 ? i : IlutAccess::sym(*g_ilut).Index(i, k))
+              : IlutAccess::unsym(*g_ilut).Index(i, k);
+            fval[t] = g_ilut_sym ? IlutAccess::sym(*g_ilut).Value(i, k)
+              : IlutAccess::unsym(*g_ilut).Value(i, k);
+          }
+        fptr[i + 1] = t;
+      }
+    const IVect& pr = IlutAccess::prow(*g_ilut);
+    const IVect& pc = g_ilut_sym ? pr : IlutAccess::pcol(*g_ilut);
+    for (int i = 0; i < n; i++) { perm_row[i] = pr(i); perm_col[i] = pc(i); }
+    return 0;
+  }
+
+  // z = M^{-1} r (Solve) or M^{-T} r (TransSolve) with the held factor.
+  int ref_ilut_solve(int trans, int n, const double* r, double* z)
+  {
+    if (!g_ilut) return -1;
+    Vec R(n), Z(n);
+    for (int i = 0; i < n; i++) R(i) = r[i];
+    Z.Zero();
+    GenMat dummy;
+    if (trans)
+      g_ilut->TransSolve(dummy, R, Z);
+    else
+      g_ilut->Solve(dummy, R, Z);
+    for (int i = 0; i < n; i++) z[i] = Z(i);
+    return 0;
+  }
+
+  // Cg / BiCgStab / Gmres (which 0/1/2) preconditioned by the held factor.
+  int ref_solve_ilut(int which, int m, int nnz, const int* ptr, const int* ind,
+                     const double* val, int sym, double* x, const double* b,
+                     double tol, int max_iter, int restart, int init_guess_null,
+                     int* nb_iter)
+  {
+    if (!g_ilut) return -100;
+    Wrap A(m, m, nnz, ptr, ind, val, sym);
+    VWrap X(m, x), B(m, b);
+    Iteration<double> it(max_iter, tol);
+    it.SetRestart(restart);
+    it.SetInitGuess(init_guess_null != 0);
+    it.HideMessages();
+    int code = sym ? run_solver(which, A.S, X.v, B.v, *g_ilut, it)
+      : run_solver(which, A.G, X.v, B.v, *g_ilut, it);
+    *nb_iter = it.GetNumberIteration();
+    return code;
   }
 
   // Seldon's generic BLAS-1 loops (Functions_Vector.cxx), for pinning.

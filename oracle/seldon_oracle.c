@@ -663,3 +663,69 @@ void orc_coo_to_csr(int nnz, const int* row, const int* col,
   free(tk);
   free(tv);
 }
+
+/* ------------------------------------------------- ILUT preconditioner */
+
+/* SolveLU on Seldon's incomplete factor, with the permutations of
+ * IlutPreconditioning::Solve / TransSolve
+ * (computation/solver/preconditioner/IlutPreconditioning.cxx:329-374).
+ * The factor rows are flat CSR arrays in stored order:
+ *   sym = 0: ArrayRowSparse, row i = L part (columns < i), then 1/U(i,i),
+ *            then the U part (SparseSolver.cxx:533-611);
+ *   sym = 1: ArrayRowSymSparse, row i = 1/D(i) at position 0, then row i of
+ *            L^T (SparseSolver.cxx:852-882); the transposed solve is the
+ *            same solve.
+ * The loops keep Seldon's order of operations, scatter form included. */
+static void orc_solve_lu(int n, const int* fp, const int* fi, const double* fv,
+                         int sym, int trans, double* x) {
+  if (sym) {
+    for (int ic = 0; ic < n; ic++)
+      for (int k = fp[ic] + 1; k < fp[ic + 1]; k++) x[fi[k]] -= fv[k] * x[ic];
+    for (int ic = 0; ic < n; ic++) x[ic] *= fv[fp[ic]];
+    for (int ic = n - 1; ic >= 0; ic--) {
+      double tmp = x[ic];
+      for (int k = fp[ic] + 1; k < fp[ic + 1]; k++) tmp -= fv[k] * x[fi[k]];
+      x[ic] = tmp;
+    }
+    return;
+  }
+  if (trans) {
+    for (int i = 0; i < n; i++) {
+      int k = fp[i];
+      while (fi[k] < i) k++;
+      x[i] *= fv[k];
+      for (int q = k + 1; q < fp[i + 1]; q++) x[fi[q]] -= fv[q] * x[i];
+    }
+    for (int i = n - 1; i >= 0; i--)
+      for (int k = fp[i]; fi[k] < i; k++) x[fi[k]] -= fv[k] * x[i];
+  } else {
+    for (int i = 0; i < n; i++)
+      for (int k = fp[i]; fi[k] < i; k++) x[i] -= fv[k] * x[fi[k]];
+    for (int i = n - 1; i >= 0; i--) {
+      int k = fp[i];
+      while (fi[k] < i) k++;
+      const double inv_diag = fv[k];
+      for (int q = k + 1; q < fp[i + 1]; q++) x[i] -= fv[q] * x[fi[q]];
+      x[i] *= inv_diag;
+    }
+  }
+}
+
+void orc_ilut_solve(int n, const int* fp, const int* fi, const double* fv,
+                    int sym, const int* perm_row, const int* perm_col,
+                    int trans, const double* r, double* z) {
+  double* t = (double*)malloc(sizeof(double) * ((size_t)n + 1));
+  if (sym || !trans) {
+    for (int i = 0; i < n; i++) t[perm_row[i]] = r[i];
+    orc_solve_lu(n, fp, fi, fv, sym, 0, t);
+    if (sym)
+      for (int i = 0; i < n; i++) z[i] = t[perm_row[i]];
+    else
+      for (int i = 0; i < n; i++) z[perm_col[i]] = t[i];
+  } else {
+    for (int i = 0; i < n; i++) t[i] = r[perm_col[i]];
+    orc_solve_lu(n, fp, fi, fv, 0, 1, t);
+    for (int i = 0; i < n; i++) z[i] = t[perm_row[i]];
+  }
+  free(t);
+}
