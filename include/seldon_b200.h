@@ -210,6 +210,7 @@ int sb2_fill(int n, double value, double* x, void* stream);
 #define SB2_PRECOND_IDENTITY 0 /* Preconditioner_Base (Iterative.cxx:50-77) */
 #define SB2_PRECOND_JACOBI 1   /* z_i = r_i / A(i,i); absent from the reference */
 #define SB2_PRECOND_SOR 2      /* SorPreconditioner (Precond_Ssor.cxx:24-90) */
+#define SB2_PRECOND_ILUT 3     /* IlutPreconditioning's apply (IlutPreconditioning.cxx) */
 
 typedef struct sb2_precond sb2_precond;
 
@@ -219,6 +220,31 @@ typedef struct sb2_precond sb2_precond;
 int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
                        int symmetric, sb2_precond** out);
 int sb2_precond_destroy(sb2_precond* M);
+
+/* ILUT preconditioner from a factor computed on the host by Seldon's
+ * IlutPreconditioning (FactorizeMatrix / FactorizeSymMatrix, GetIlut):
+ *   fptr[n+1], find, fval   the factor's rows in stored order
+ *       symmetric = 0: ArrayRowSparse rows: L part (columns < i), then
+ *                      1/U(i,i), then the U part (columns > i)
+ *                      (SparseSolver.cxx:533-611)
+ *       symmetric = 1: ArrayRowSymSparse rows: 1/D(i) first (its index is
+ *                      not read), then row i of L^T (columns > i)
+ *                      (SparseSolver.cxx:852-882)
+ *   perm_row, perm_col      permutation_row / permutation_col (perm_col is
+ *                           not read when symmetric)
+ *   A                       the system matrix the solvers are given (may be
+ *                           NULL for sb2_precond_solve alone)
+ * Solve / TransSolve (IlutPreconditioning.cxx:329-374) then run on the
+ * device as level-scheduled sweeps with the reference's own operation order:
+ * z is the reference's z bit for bit.  The arrays are copied.  A factor
+ * whose rows break the layout above gives SB2_ERR_INVALID_CSR, a
+ * permutation that is not one SB2_ERR_INVALID_VALUE.  The Krylov drivers
+ * accept it (host-driven iterations); sb2_ir_cg does not
+ * (SB2_ERR_NOT_SUPPORTED). */
+int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr,
+                            const int* find, const double* fval,
+                            const int* perm_row, const int* perm_col,
+                            int symmetric, sb2_precond** out);
 
 /* z = M^{-1} r (Solve) / M^{-T} r (TransSolve).  z and r must not overlap.
  * Precond_Ssor.cxx:62-90: z is zeroed, then SOR type 0 (symmetric), 2

@@ -25,6 +25,7 @@ SPMV_TMA = 2
 PRECOND_IDENTITY = 0
 PRECOND_JACOBI = 1
 PRECOND_SOR = 2
+PRECOND_ILUT = 3
 
 c_int_p = ctypes.POINTER(ctypes.c_int)
 c_double_p = ctypes.POINTER(ctypes.c_double)
@@ -129,6 +130,9 @@ _PROTOS = [
     ("sb2_csr_destroy", ctypes.c_int, [c_void_p]),
     ("sb2_csr_info", ctypes.c_int, [c_void_p, c_int_p, c_int_p, c_int_p, c_int_p]),
     ("sb2_csr_download", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_precond_create_ilut", ctypes.c_int,
+     [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int,
+      ctypes.POINTER(c_void_p)]),
     ("sb2_coo_to_csr", ctypes.c_int,
      [ctypes.c_int, c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
       ctypes.c_int, c_void_p, c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p),

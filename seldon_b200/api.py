@@ -396,6 +396,55 @@ class SorPreconditioner(_DevicePrecond):
         return self.omega, self.nb_iter, int(self.symmetric)
 
 
+class IlutPreconditioning(_DevicePrecond):
+    """IlutPreconditioning's Solve / TransSolve (IlutPreconditioning.cxx:
+    329-374) on the device, from a factor computed on the host by Seldon's
+    GetIlut (FactorizeMatrix / FactorizeSymMatrix).  SetFactor takes the
+    factor's rows in stored order as flat CSR arrays and the permutations;
+    the sweeps reproduce SolveLU bit for bit."""
+
+    kind = _lib.PRECOND_ILUT
+
+    def __init__(self):
+        super().__init__()
+        self._factor = None
+        self._serial = 0
+
+    def SetFactor(self, fptr, find, fval, perm_row, perm_col=None, symmetric=False):
+        import numpy as np
+        fptr = np.ascontiguousarray(fptr, dtype=np.int32)
+        n = fptr.size - 1
+        find = np.ascontiguousarray(find, dtype=np.int32)
+        fval = np.ascontiguousarray(fval, dtype=np.float64)
+        prow = np.ascontiguousarray(perm_row, dtype=np.int32)
+        pcol = prow if perm_col is None else np.ascontiguousarray(perm_col, dtype=np.int32)
+        if find.size != fval.size or find.size < fptr[-1] or prow.size != n or pcol.size != n:
+            raise ValueError("WrongDim: factor arrays and permutations do not match")
+        self._factor = (n, fptr, find, fval, prow, pcol, bool(symmetric))
+        self._serial += 1
+
+    def _params(self):
+        return self._serial
+
+    def handle_for(self, A):
+        if self._factor is None:
+            raise RuntimeError("IlutPreconditioning: no factor (call SetFactor first)")
+        key = id(A)
+        ent = self._cache.get(key)
+        if ent is None or ent[0] is not A or ent[2] != self._serial:
+            n, fptr, find, fval, prow, pcol, sym = self._factor
+            h = ctypes.c_void_p()
+            check(_L.sb2_precond_create_ilut(A.handle, n, _np_ptr(fptr), _np_ptr(find),
+                                             _np_ptr(fval), _np_ptr(prow), _np_ptr(pcol),
+                                             int(sym), ctypes.byref(h)),
+                  "sb2_precond_create_ilut")
+            if ent is not None:
+                _L.sb2_precond_destroy(ent[1])
+            ent = (A, h, self._serial)
+            self._cache[key] = ent
+        return ent[1]
+
+
 def SOR(A, X, B, omega, iter, type_ssor=2, stream=None):
     """In-place relaxation (Relaxation_MatVect.cxx:41-95, :176-298)."""
     check(_L.sb2_sor(A.handle, _dev_ptr(X, A.m, "X"), _dev_ptr(B, A.m, "B"), float(omega),

@@ -1360,7 +1360,7 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   if (A->m <= 0) return SB2_OK;
   const int kind = M ? precond_kind(M) : SB2_PRECOND_IDENTITY;
   if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
-  if (kind == SB2_PRECOND_SOR)
+  if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;
   if (kind == SB2_PRECOND_JACOBI) {

@@ -1,4 +1,4 @@
-// Preconditioners: identity, Jacobi and level-scheduled SOR.
+// Preconditioners: identity, Jacobi, level-scheduled SOR and the ILUT apply.
 //
 // SOR reproduces the reference's strictly sequential sweeps
 // (Relaxation_MatVect.cxx:41-95 RowSparse, :176-298 RowSymSparse) bit for
@@ -7,6 +7,17 @@
 // already-updated rows AND anti-dependencies on rows that must still hold
 // their old value), and each row repeats the reference's own operation order
 // with separately rounded products.
+//
+// The ILUT apply runs Seldon's SolveLU (computation/solver/SparseSolver.cxx:
+// 533-611 and 852-882) on a factor computed on the host.  Its loops are
+// either row gathers (x_i -= v * x_c over row i) or column scatters
+// (x_c -= v * x_i for each entry of row i).  Every sweep is put in gather
+// form: target j collects its updates in the order the sequential loop
+// would have applied them (the scatter sources in increasing or decreasing
+// row order, each row's entries in stored order), and the rows are grouped
+// into levels on their dependencies.  Each row then repeats the reference's
+// own operations with separately rounded products, so the result is the
+// reference's bit for bit.
 #include <algorithm>
 #include <vector>
 
@@ -208,6 +219,36 @@ __global__ void __launch_bounds__(1024) level_single_cta(int nlev, const int* __
   }
 }
 
+// x_j = (x_j * pre_j - v_1 x_{c1} - v_2 x_{c2} - ...) * post_j, the
+// subtractions in the listed order (pre/post may be null).
+struct GatherSub {
+  const int* ptr; const int* ind; const double* val;
+  const double* pre; const double* post; double* x;
+  __device__ void operator()(int j) const {
+    double v = ldx(x + j);
+    if (pre) v = mul_rn(v, pre[j]);
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) v = __dsub_rn(v, mul_rn(val[k], ldx(x + ind[k])));
+    if (post) v = mul_rn(v, post[j]);
+    x[j] = v;
+  }
+};
+
+// out[idx[i]] = in[i]
+__global__ void perm_scatter_kernel(int n, const int* __restrict__ idx,
+                                    const double* __restrict__ in, double* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[idx[i]] = in[i];
+}
+
+// out[i] = in[idx[i]]
+__global__ void perm_gather_kernel(int n, const int* __restrict__ idx,
+                                   const double* __restrict__ in, double* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[idx[i]];
+}
+
 __global__ void jacobi_kernel(int n, const double* __restrict__ r,
                               const double* __restrict__ d, double* __restrict__ z) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -243,6 +284,24 @@ static int run_rows(int n, const Op& op, cudaStream_t s) {
 
 }  // namespace sb2
 
+namespace sb2 {
+// One triangular sweep in gather form: rows' update lists and their levels.
+struct GatherSweep {
+  int* d_ptr = nullptr;
+  int* d_ind = nullptr;
+  double* d_val = nullptr;
+  LevelPlan lv;
+  void release() {
+    cudaFree(d_ptr);
+    cudaFree(d_ind);
+    cudaFree(d_val);
+    d_ptr = d_ind = nullptr;
+    d_val = nullptr;
+    lv.release();
+  }
+};
+}  // namespace sb2
+
 struct sb2_precond {
   const sb2_csr* A = nullptr;
   int kind = 0;
@@ -252,9 +311,18 @@ struct sb2_precond {
   // SOR schedules: general forward/backward sweeps, or for symmetric storage
   // the lower (forward) and upper (backward) triangular solves.
   sb2::LevelPlan fwd, bwd;
-  double* d_t = nullptr;  // scratch of the symmetric sweeps
+  double* d_t = nullptr;  // scratch of the symmetric sweeps and of ILUT
   std::mutex mu;
   bool planned = false;
+  // ILUT: order, storage, permutations, 1/U(i,i) or 1/D(i), and the sweeps
+  // (unsymmetric: L forward, U backward, U^T forward, L^T backward;
+  // symmetric: L forward through the transposed rows, L^T backward)
+  int n_ilu = 0;
+  int ilu_sym = 0;
+  int* d_prow = nullptr;
+  int* d_pcol = nullptr;
+  double* d_dinv = nullptr;
+  sb2::GatherSweep s_lf, s_ub, s_utf, s_ltb;
 };
 
 namespace sb2 {
@@ -322,12 +390,183 @@ static int sor_apply(sb2_precond* M, double* x, const double* b, double omega,
   return SB2_OK;
 }
 
+// Levels of a gather sweep: row j waits for every row it reads; rows are
+// visited in dependency order (increasing j when reads are of smaller
+// rows, decreasing otherwise).
+static void gather_levels(int n, const std::vector<int>& ptr, const std::vector<int>& ind,
+                          bool ascending, std::vector<int>& level) {
+  level.assign(n, 0);
+  for (int s = 0; s < n; s++) {
+    const int j = ascending ? s : n - 1 - s;
+    int lev = 0;
+    for (int k = ptr[j]; k < ptr[j + 1]; k++) lev = std::max(lev, level[ind[k]] + 1);
+    level[j] = lev;
+  }
+}
+
+static int upload_sweep(int n, const std::vector<int>& ptr, const std::vector<int>& ind,
+                        const std::vector<double>& val, bool ascending, GatherSweep* S) {
+  const size_t nz = ind.size();
+  SB2_CUDA_TRY(cudaMalloc(&S->d_ptr, sizeof(int) * (n + 1)));
+  SB2_CUDA_TRY(cudaMalloc(&S->d_ind, sizeof(int) * std::max<size_t>(nz, 1)));
+  SB2_CUDA_TRY(cudaMalloc(&S->d_val, sizeof(double) * std::max<size_t>(nz, 1)));
+  SB2_CUDA_TRY(cudaMemcpy(S->d_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  if (nz) {
+    SB2_CUDA_TRY(cudaMemcpy(S->d_ind, ind.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
+    SB2_CUDA_TRY(cudaMemcpy(S->d_val, val.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+  }
+  std::vector<int> level;
+  gather_levels(n, ptr, ind, ascending, level);
+  return upload_plan(level, n, &S->lv);
+}
+
+// Update lists of a column scatter: entry (i -> c, v) for the rows i in the
+// order the sequential loop visits them, each row's entries in stored order.
+struct ListBuilder {
+  std::vector<std::vector<int>> src;
+  std::vector<std::vector<double>> v;
+  explicit ListBuilder(int n) : src(n), v(n) {}
+  void add(int target, int source, double value) {
+    src[target].push_back(source);
+    v[target].push_back(value);
+  }
+  void flatten(std::vector<int>& ptr, std::vector<int>& ind, std::vector<double>& val) const {
+    const int n = (int)src.size();
+    ptr.assign(n + 1, 0);
+    for (int j = 0; j < n; j++) ptr[j + 1] = ptr[j] + (int)src[j].size();
+    ind.clear();
+    val.clear();
+    ind.reserve(ptr[n]);
+    val.reserve(ptr[n]);
+    for (int j = 0; j < n; j++) {
+      ind.insert(ind.end(), src[j].begin(), src[j].end());
+      val.insert(val.end(), v[j].begin(), v[j].end());
+    }
+  }
+};
+
+static bool is_permutation(int n, const int* p) {
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; i++) {
+    if (p[i] < 0 || p[i] >= n || seen[p[i]]) return false;
+    seen[p[i]] = 1;
+  }
+  return true;
+}
+
+// Builds every sweep of the factor (host arrays in Seldon's stored order).
+static int plan_ilut(sb2_precond* M, int n, const int* fp, const int* fi, const double* fv,
+                     const int* prow, const int* pcol) {
+  if (fp[0] != 0) return SB2_ERR_INVALID_CSR;
+  for (int i = 0; i < n; i++)
+    if (fp[i + 1] < fp[i]) return SB2_ERR_INVALID_CSR;
+  if (!is_permutation(n, prow) || (!M->ilu_sym && !is_permutation(n, pcol)))
+    return SB2_ERR_INVALID_VALUE;
+  std::vector<double> dinv(n);
+  std::vector<int> ptr, ind;
+  std::vector<double> val;
+  if (M->ilu_sym) {
+    // row i: 1/D(i) at the first position, then row i of L^T (columns > i)
+    ListBuilder fwd(n);
+    std::vector<int> bptr(n + 1, 0), bind;
+    std::vector<double> bval;
+    for (int i = 0; i < n; i++) {
+      if (fp[i + 1] <= fp[i]) return SB2_ERR_INVALID_CSR;
+      dinv[i] = fv[fp[i]];
+      for (int k = fp[i] + 1; k < fp[i + 1]; k++) {
+        if (fi[k] <= i || fi[k] >= n) return SB2_ERR_INVALID_CSR;
+        fwd.add(fi[k], i, fv[k]);  // L y = b: x(j) -= A(i,k) x(i), i increasing
+        bind.push_back(fi[k]);
+        bval.push_back(fv[k]);
+      }
+      bptr[i + 1] = (int)bind.size();
+    }
+    fwd.flatten(ptr, ind, val);
+    SB2_TRY(upload_sweep(n, ptr, ind, val, true, &M->s_lf));
+    SB2_TRY(upload_sweep(n, bptr, bind, bval, false, &M->s_ub));
+  } else {
+    // row i: L part (columns < i), then 1/U(i,i), then the U part
+    std::vector<int> lptr(n + 1, 0), lind, uptr(n + 1, 0), uind;
+    std::vector<double> lval, uval;
+    ListBuilder utf(n), ltb(n);
+    std::vector<int> dpos(n);
+    for (int i = 0; i < n; i++) {
+      int k = fp[i];
+      while (k < fp[i + 1] && fi[k] < i) {
+        if (fi[k] < 0) return SB2_ERR_INVALID_CSR;
+        lind.push_back(fi[k]);
+        lval.push_back(fv[k]);
+        k++;
+      }
+      if (k == fp[i + 1]) return SB2_ERR_INVALID_CSR;  // no diagonal position
+      dpos[i] = k;
+      dinv[i] = fv[k];
+      for (int q = k + 1; q < fp[i + 1]; q++) {
+        if (fi[q] <= i || fi[q] >= n) return SB2_ERR_INVALID_CSR;
+        uind.push_back(fi[q]);
+        uval.push_back(fv[q]);
+        utf.add(fi[q], i, fv[q]);  // U^T: x(c) -= U(i,c) x(i), i increasing
+      }
+      lptr[i + 1] = (int)lind.size();
+      uptr[i + 1] = (int)uind.size();
+    }
+    for (int i = n - 1; i >= 0; i--)  // L^T: x(k) -= L(i,k) x(i), i decreasing
+      for (int k = fp[i]; k < dpos[i]; k++) ltb.add(fi[k], i, fv[k]);
+    SB2_TRY(upload_sweep(n, lptr, lind, lval, true, &M->s_lf));
+    SB2_TRY(upload_sweep(n, uptr, uind, uval, false, &M->s_ub));
+    utf.flatten(ptr, ind, val);
+    SB2_TRY(upload_sweep(n, ptr, ind, val, true, &M->s_utf));
+    ltb.flatten(ptr, ind, val);
+    SB2_TRY(upload_sweep(n, ptr, ind, val, false, &M->s_ltb));
+  }
+  SB2_CUDA_TRY(cudaMalloc(&M->d_dinv, sizeof(double) * std::max(n, 1)));
+  SB2_CUDA_TRY(cudaMalloc(&M->d_prow, sizeof(int) * std::max(n, 1)));
+  SB2_CUDA_TRY(cudaMalloc(&M->d_pcol, sizeof(int) * std::max(n, 1)));
+  SB2_CUDA_TRY(cudaMalloc(&M->d_t, sizeof(double) * std::max(n, 1)));
+  SB2_CUDA_TRY(cudaMemcpy(M->d_dinv, dinv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMemcpy(M->d_prow, prow, sizeof(int) * n, cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMemcpy(M->d_pcol, M->ilu_sym ? prow : pcol, sizeof(int) * n,
+                          cudaMemcpyHostToDevice));
+  return SB2_OK;
+}
+
+static GatherSub sweep_op(const GatherSweep& S, const double* pre, const double* post, double* x) {
+  return GatherSub{S.d_ptr, S.d_ind, S.d_val, pre, post, x};
+}
+
+// IlutPreconditioning::Solve / TransSolve (IlutPreconditioning.cxx:329-374).
+static int ilut_apply(const sb2_precond* M, bool trans, const double* r, double* z,
+                      cudaStream_t s) {
+  const int n = M->n_ilu;
+  double* t = M->d_t;
+  const int g = std::min((n + 255) / 256, num_sms(current_device()) * 8);
+  if (M->ilu_sym) {
+    perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_prow, r, t);
+    SB2_TRY(run_levels(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
+    SB2_TRY(run_levels(M->s_ub.lv, n, sweep_op(M->s_ub, M->d_dinv, nullptr, t), s));
+    perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_prow, t, z);
+  } else if (!trans) {
+    perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_prow, r, t);
+    SB2_TRY(run_levels(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
+    SB2_TRY(run_levels(M->s_ub.lv, n, sweep_op(M->s_ub, nullptr, M->d_dinv, t), s));
+    perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_pcol, t, z);
+  } else {
+    perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_pcol, r, t);
+    SB2_TRY(run_levels(M->s_utf.lv, n, sweep_op(M->s_utf, nullptr, M->d_dinv, t), s));
+    SB2_TRY(run_levels(M->s_ltb.lv, n, sweep_op(M->s_ltb, nullptr, nullptr, t), s));
+    perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_prow, t, z);
+  }
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
 int precond_kind(const sb2_precond* M) { return M->kind; }
 const sb2_csr* precond_matrix(const sb2_precond* M) { return M->A; }
 
 int precond_apply(const sb2_precond* cM, bool trans, const double* r, double* z,
                   cudaStream_t s) {
   sb2_precond* M = const_cast<sb2_precond*>(cM);
+  if (M->kind == SB2_PRECOND_ILUT) return M->n_ilu ? ilut_apply(M, trans, r, z, s) : SB2_OK;
   const int n = M->A->m;
   if (n == 0) return SB2_OK;
   if (M->kind == SB2_PRECOND_IDENTITY) {
@@ -373,22 +612,58 @@ int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
   return SB2_OK;
 }
 
+int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int* find,
+                            const double* fval, const int* perm_row, const int* perm_col,
+                            int symmetric, sb2_precond** out) {
+  if (!out || n < 0 || (n > 0 && (!fptr || !perm_row || (!symmetric && !perm_col))))
+    return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  if (A && (A->m != n || A->n != n)) return SB2_ERR_INVALID_VALUE;
+  if (n > 0 && fptr[n] > 0 && (!find || !fval)) return SB2_ERR_INVALID_VALUE;
+  // every index the sweeps read is checked while they are built
+  sb2_precond* M = new sb2_precond();
+  M->A = A;
+  M->kind = SB2_PRECOND_ILUT;
+  M->n_ilu = n;
+  M->ilu_sym = symmetric ? 1 : 0;
+  int st = n > 0 ? plan_ilut(M, n, fptr, find, fval, perm_row, perm_col) : SB2_OK;
+  if (st != SB2_OK) {
+    sb2_precond_destroy(M);
+    return st;
+  }
+  *out = M;
+  return SB2_OK;
+}
+
 int sb2_precond_destroy(sb2_precond* M) {
   if (!M) return SB2_OK;
   M->fwd.release();
   M->bwd.release();
   cudaFree(M->d_t);
+  M->s_lf.release();
+  M->s_ub.release();
+  M->s_utf.release();
+  M->s_ltb.release();
+  cudaFree(M->d_prow);
+  cudaFree(M->d_pcol);
+  cudaFree(M->d_dinv);
   delete M;
   return SB2_OK;
 }
 
+static int precond_size(const sb2_precond* M) {
+  return M->kind == SB2_PRECOND_ILUT ? M->n_ilu : M->A->m;
+}
+
 int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
-  if (!M || (M->A->m > 0 && (!r || !z)) || (r == z && M->A->m > 0)) return SB2_ERR_INVALID_VALUE;
+  if (!M || (precond_size(M) > 0 && (!r || !z)) || (r == z && precond_size(M) > 0))
+    return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, false, r, z, (cudaStream_t)stream);
 }
 
 int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
-  if (!M || (M->A->m > 0 && (!r || !z)) || (r == z && M->A->m > 0)) return SB2_ERR_INVALID_VALUE;
+  if (!M || (precond_size(M) > 0 && (!r || !z)) || (r == z && precond_size(M) > 0))
+    return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, true, r, z, (cudaStream_t)stream);
 }
 

@@ -102,6 +102,22 @@ def main():
         m, n, op, oi, ov = R.coo_to_csr(r, c, v, index, m_min, n_min, bool(sym))
         put(f"coo/{name}", row=r.astype(np.int32), col=c.astype(np.int32), val=v, index=index,
             m_min=m_min, n_min=n_min, sym=sym, m=m, n=n, ptr=op, ind=oi, out=ov)
+    # ILUT: Seldon's own factor (GetIlut) and its Solve / TransSolve
+    irng = np.random.default_rng(13)
+    ilut_cases = {
+        "conv5_ilut": (matgen.convdiff3d(5), False, None, dict(droptol=1e-3)),
+        "conv5_perm_piv": (matgen.convdiff3d(5), False, irng.permutation(125),
+                           dict(droptol=1e-4, permtol=0.5)),
+        "conv5_ilu0": (matgen.convdiff3d(5), False, None, dict(type_ilu=R.ILU_0)),
+        "conv5_iluk2": (matgen.convdiff3d(5), False, None, dict(type_ilu=R.ILU_K, fill_level=2)),
+        "lap9_sym": (matgen.upper(*matgen.lap2d(9)), True, None, dict(droptol=1e-3)),
+    }
+    for name, ((p, i_, v), sym, perm, kw) in ilut_cases.items():
+        fptr, find, fval, prow, pcol = R.ilut_factor(p, i_, v, sym=sym, perm=perm, **kw)
+        n = p.size - 1
+        r = irng.standard_normal(n)
+        put(f"ilut/{name}", fptr=fptr, find=find, fval=fval, prow=prow, pcol=pcol, sym=int(sym),
+            r=r, z=R.ilut_solve(r), zt=R.ilut_solve(r, trans=True))
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {len(g)} arrays, {os.path.getsize(OUT)} bytes")
 

@@ -1,0 +1,140 @@
+"""ILUT preconditioner apply on the device (sb2_precond_create_ilut):
+Solve and TransSolve against the reference's golden vectors and the oracle
+bit for bit, from factors Seldon's GetIlut computed, on level schedules of
+one CTA (n <= 65536) and of one launch per level; and Cg / BiCgStab / Gmres
+preconditioned by it against the reference's own preconditioned solves."""
+import os
+
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+from tests.helpers import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "seldon_golden.npz")
+ILUT_CASES = ["conv5_ilut", "conv5_perm_piv", "conv5_ilu0", "conv5_iluk2", "lap9_sym"]
+
+
+@pytest.fixture(scope="module")
+def api(cuda):
+    from seldon_b200 import api as a
+    return a
+
+
+def _precond(api, factor, sym):
+    M = api.IlutPreconditioning()
+    fptr, find, fval, prow, pcol = factor
+    M.SetFactor(fptr, find, fval, prow, pcol, symmetric=sym)
+    return M
+
+
+def _apply(api, M, A, r, trans):
+    R = to_dev(r)
+    Z = to_dev(np.zeros_like(r))
+    (M.TransSolve if trans else M.Solve)(A, R, Z)
+    return to_host(Z)
+
+
+def _dummy(api, n):
+    ptr = np.arange(n + 1, dtype=np.int32)
+    return api.RowSparse(n, n, ptr, np.arange(n, dtype=np.int32), np.ones(n))
+
+
+@pytest.mark.parametrize("name", ILUT_CASES)
+def test_ilut_golden(api, name):
+    g = np.load(GOLDEN)
+    k = f"ilut/{name}"
+    factor = tuple(g[f"{k}/{a}"] for a in ("fptr", "find", "fval", "prow", "pcol"))
+    sym = bool(g[k + "/sym"])
+    n = factor[0].size - 1
+    M = _precond(api, factor, sym)
+    A = _dummy(api, n)
+    assert np.array_equal(_apply(api, M, A, g[k + "/r"], False), g[k + "/z"])
+    assert np.array_equal(_apply(api, M, A, g[k + "/r"], True), g[k + "/zt"])
+
+
+# (matrix, symmetric storage, factor options): the 3D ones are large enough
+# for one launch per level (n > 65536)
+LARGE = [
+    ("conv20", lambda: matgen.convdiff3d(20), False, dict(droptol=1e-3)),
+    ("conv20_perm", lambda: matgen.convdiff3d(20), False, dict(droptol=1e-3, permtol=0.3)),
+    ("conv42", lambda: matgen.convdiff3d(42), False, dict(droptol=1e-2)),
+    ("conv42_ilu0", lambda: matgen.convdiff3d(42), False, dict(type_ilu=3)),
+    ("lap300_sym", lambda: matgen.upper(*matgen.lap2d(300)), True, dict(droptol=1e-2)),
+]
+
+
+@pytest.mark.parametrize("name,make,sym,kw", LARGE, ids=[c[0] for c in LARGE])
+def test_ilut_vs_oracle(api, oracle, reference, name, make, sym, kw):
+    p, i, v = make()
+    n = p.size - 1
+    rng = np.random.default_rng(n)
+    perm = rng.permutation(n) if name.endswith("_perm") else None
+    factor = reference.ilut_factor(p, i, v, sym=sym, perm=perm, **kw)
+    M = _precond(api, factor, sym)
+    A = _dummy(api, n)
+    for trans in (False, True):
+        r = rng.standard_normal(n)
+        z = _apply(api, M, A, r, trans)
+        assert np.array_equal(z, oracle.ilut_solve(factor, r, sym=sym, trans=trans))
+
+
+def test_ilut_rejects_bad_factor(api):
+    from seldon_b200._lib import SeldonB200Error
+    # a row without a diagonal position (all columns below the row)
+    fptr = np.array([0, 1, 2], dtype=np.int32)
+    find = np.array([0, 0], dtype=np.int32)
+    M = api.IlutPreconditioning()
+    M.SetFactor(fptr, find, np.ones(2), np.arange(2), np.arange(2))
+    with pytest.raises(SeldonB200Error):
+        M.Solve(_dummy(api, 2), to_dev(np.ones(2)), to_dev(np.zeros(2)))
+    # a permutation that is not one
+    fptr = np.array([0, 1, 2], dtype=np.int32)
+    find = np.array([0, 1], dtype=np.int32)
+    M.SetFactor(fptr, find, np.ones(2), np.array([0, 0]), np.arange(2))
+    with pytest.raises(SeldonB200Error):
+        M.Solve(_dummy(api, 2), to_dev(np.ones(2)), to_dev(np.zeros(2)))
+
+
+@pytest.mark.parametrize("which,sym", [("bicgstab", False), ("gmres", False), ("cg", True),
+                                       ("gmres", True)])
+def test_krylov_with_ilut(api, reference, which, sym):
+    """Preconditioned drivers reach the reference's iterate: same exit code,
+    iteration count within the drift of the dot products' summation order,
+    and the same solution to 1e-7."""
+    if sym:
+        full = matgen.lap2d(40)
+        A = matgen.upper(*full)
+    else:
+        A = full = matgen.convdiff3d(14)
+    n = A[0].size - 1
+    factor = reference.ilut_factor(*A, sym=sym, droptol=1e-2)
+    b = matgen.matvec(*full, np.random.default_rng(5).uniform(-1, 1, n))
+    tol, restart = 1e-10, 10
+    xr, cr, nr = reference.solve_ilut(which, *A, b, sym=sym, tol=tol, max_iter=500,
+                                      restart=restart)
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(500, tol)
+    it.SetRestart(restart)
+    it.HideMessages()
+    fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
+    code = fn(M, X, to_dev(b), _precond(api, factor, sym), it)
+    x = to_host(X)
+    assert code == cr == 0
+    nb = it.GetNumberIteration()
+    assert abs(nb - nr) <= max(1, int(0.05 * nr)), (nb, nr)
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-7
+    assert nb < 0.5 * _plain_iterations(api, M, b, which, tol, restart)
+
+
+def _plain_iterations(api, M, b, which, tol, restart):
+    X = to_dev(np.zeros(b.size))
+    it = api.Iteration(5000, tol)
+    it.SetRestart(restart)
+    it.HideMessages()
+    fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
+    fn(M, X, to_dev(b), api.Preconditioner_Base(), it)
+    return it.GetNumberIteration()

@@ -179,3 +179,37 @@ def test_coo_to_csr_live_fuzz(oracle, reference):
         assert a[:2] == b[:2]
         for u, v in zip(a[2:], b[2:]):
             assert np.array_equal(u, v)
+
+
+ILUT_CASES = ["conv5_ilut", "conv5_perm_piv", "conv5_ilu0", "conv5_iluk2", "lap9_sym"]
+
+
+def ilut_factor(g, name):
+    k = f"ilut/{name}"
+    return tuple(g[f"{k}/{a}"] for a in ("fptr", "find", "fval", "prow", "pcol"))
+
+
+@pytest.mark.parametrize("name", ILUT_CASES)
+def test_ilut_solve_golden(golden, oracle, name):
+    k = f"ilut/{name}"
+    sym = bool(golden[k + "/sym"])
+    f = ilut_factor(golden, name)
+    assert np.array_equal(oracle.ilut_solve(f, golden[k + "/r"], sym=sym), golden[k + "/z"])
+    assert np.array_equal(oracle.ilut_solve(f, golden[k + "/r"], sym=sym, trans=True),
+                          golden[k + "/zt"])
+
+
+def test_ilut_solve_live(oracle, reference):
+    """Seldon's factorization of larger and harder systems; the oracle's
+    solve equals Seldon's bit for bit."""
+    rng = np.random.default_rng(17)
+    cases = [(matgen.convdiff3d(9), False, dict(droptol=1e-4)),
+             (matgen.convdiff3d(8), False, dict(droptol=1e-5, permtol=0.3)),
+             (matgen.upper(*matgen.lap2d(25)), True, dict(droptol=1e-4)),
+             (matgen.convdiff3d(8), False, dict(type_ilu=reference.MILU_0))]
+    for (p, i, v), sym, kw in cases:
+        f = reference.ilut_factor(p, i, v, sym=sym, perm=rng.permutation(p.size - 1), **kw)
+        for trans in (False, True):
+            r = rng.standard_normal(p.size - 1)
+            assert np.array_equal(oracle.ilut_solve(f, r, sym=sym, trans=trans),
+                                  reference.ilut_solve(r, trans=trans))
