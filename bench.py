@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true", help="skip the solver/Zipf extras")
     p.add_argument("--extras", default="all",
-                   help="comma list of extras to run: c1, c3, gmres, zipf, batch, adjoint, assemble "
+                   help="comma list of extras to run: c1, c3, gmres, zipf, batch, adjoint, assemble, ilu0 "
                         "(default all)")
     p.add_argument("--cpu-seconds", type=float, default=8.0,
                    help="bounded CPU-baseline sample (seconds of work)")
@@ -393,7 +393,7 @@ def run_extras(api, matgen, torch, dev, which="all"):
     """Time-to-solution figures on the other configurations (device-timed).
     `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, or all."""
     out = {}
-    names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint", "assemble"}
+    names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint", "assemble", "ilu0"}
     want = names if which == "all" else set(w.strip() for w in which.split(","))
     unknown = want - names
     if unknown:
@@ -423,6 +423,8 @@ def run_extras(api, matgen, torch, dev, which="all"):
         out.update(extra_zipf(api, matgen, torch, dev, timed))
     if "assemble" in want:
         out.update(extra_assemble(api, matgen, torch, dev, timed))
+    if "ilu0" in want:
+        out.update(extra_ilu0(api, matgen, torch, dev, timed))
     if "batch" in want:
         out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed)
     if "adjoint" in want:
@@ -571,6 +573,56 @@ def extra_assemble(api, matgen, torch, dev, timed):
     except Exception as e:  # the checker is optional here
         out["cpu_reference"] = {"unavailable": str(e)[:120]}
     return {"coo_to_csr_conv128": out}
+
+
+def extra_ilu0(api, matgen, torch, dev, timed):
+    """ILU(0) of the 128^3 convection-diffusion operator: factored on the
+    device (GetIlu0's order), applied (SolveLU sweeps, level-scheduled), and
+    BiCGSTAB with it against BiCGSTAB without.  Seldon's own apply of the
+    same factor is timed on one host core beside it."""
+    ptr, ind, val = matgen.convdiff3d(128)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    M = api.IlutPreconditioning()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    M.FactorizeMatrix(A)
+    torch.cuda.synchronize()
+    out = {"n": n, "nnz": int(ind.size), "factor_s": round(time.perf_counter() - t0, 3)}
+    r = torch.rand(n, dtype=torch.float64, device=dev)
+    z = torch.empty_like(r)
+    for _ in range(3):
+        M.Solve(A, r, z)
+    ms, _ = timed(lambda: [M.Solve(A, r, z) for _ in range(10)])
+    out["apply_ms"] = round(ms / 10, 3)
+    # factor entries and the vector traffic one apply needs at least
+    out["apply_min_gbs"] = round((ind.size * 12 + n * 8 * 6) / (ms / 10 * 1e-3) / 1e9, 1)
+    b = torch.as_tensor(matgen.matvec(ptr, ind, val, np.random.default_rng(1).uniform(-1, 1, n)),
+                        device=dev)
+    for key, P in (("bicgstab_plain", api.Preconditioner_Base()), ("bicgstab_ilu0", M)):
+        X = torch.zeros(n, dtype=torch.float64, device=dev)
+
+        def solve():
+            X.zero_()
+            it = api.Iteration(2000, 1e-8)
+            it.HideMessages()
+            api.BiCgStab(A, X, b, P, it)
+            return it
+        solve()
+        ms, it = timed(solve)
+        out[key] = {"ms": round(ms, 2), "iterations": it.GetNumberIteration()}
+    try:
+        from oracle.pyoracle import REF_FAST_SO, Reference
+        if Reference.available(REF_FAST_SO):
+            R = Reference(REF_FAST_SO)
+            R.ilut_factor(ptr, ind, val, type_ilu=R.ILU_0)
+            rh = r.cpu().numpy()
+            t0 = time.perf_counter()
+            R.ilut_solve(rh)
+            out["cpu_reference_apply_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    except Exception as e:  # the checker is optional here
+        out["cpu_reference_apply_ms"] = f"unavailable: {str(e)[:100]}"
+    return {"ilu0_conv128": out}
 
 
 def run_batch(api, matgen, torch, dev, timed, nsys=4096, sample_every=8):

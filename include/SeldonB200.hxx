@@ -1602,6 +1602,290 @@ namespace Seldon
     return b200::Solve(b200::kGmres, A, x, b, M, outer);
   }
 
+
+  ///////////////////////////////////////////
+  // ILUT: SELDON'S FACTOR, APPLIED ON GPU //
+  ///////////////////////////////////////////
+
+
+#ifdef SELDON_FILE_ILUT_PRECONDITIONING_HXX
+
+  namespace b200
+  {
+    //! Reads Seldon's factor and permutations out of IlutPreconditioning's
+    //! protected members (pointers to members named in a derived class).
+    template <class Alloc>
+    struct IlutState: public IlutPreconditioning<double, double, Alloc>
+    {
+      typedef IlutPreconditioning<double, double, Alloc> base;
+      static const Matrix<double, General, ArrayRowSparse, Alloc>& Unsym(const base& p)
+      {
+        return p.*(&IlutState::mat_unsym);
+      }
+      static const Matrix<double, Symmetric, ArrayRowSymSparse, Alloc>& Sym(const base& p)
+      {
+        return p.*(&IlutState::mat_sym);
+      }
+      static const IVect& RowPerm(const base& p)
+      {
+        return p.*(&IlutState::permutation_row);
+      }
+      static const IVect& ColPerm(const base& p)
+      {
+        return p.*(&IlutState::permutation_col);
+      }
+    };
+  }
+
+
+  //! IlutPreconditioning whose Solve / TransSolve run on the device
+  //! (IlutPreconditioning.cxx:329-374).  The factorization is Seldon's own:
+  //! parameters and FactorizeMatrix go to a host IlutPreconditioning (GetIlut
+  //! on the CPU, as in the reference), and the factor is then copied to the
+  //! GPU, where the triangular sweeps reproduce SolveLU bit for bit.  Device
+  //! matrices given to FactorizeMatrix are read back first.
+  template <>
+  class IlutPreconditioning<double, double, CudaAlloc<double> >
+  {
+  public:
+    typedef IlutPreconditioning<double, double> host_type;
+    typedef Vector<double, VectFull, CudaAlloc<double> > vector_type;
+
+    enum {ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K};
+
+  protected:
+    host_type host_;
+    bool symmetric_;
+    sb2_precond* M_;
+
+  public:
+    IlutPreconditioning(): symmetric_(false), M_(0) {}
+    ~IlutPreconditioning()
+    {
+      if (M_)
+        sb2_precond_destroy(M_);
+    }
+
+    void Clear()
+    {
+      host_.Clear();
+      if (M_)
+        sb2_precond_destroy(M_);
+      M_ = 0;
+    }
+
+    int GetFactorisationType() const { return host_.GetFactorisationType(); }
+    int GetFillLevel() const { return host_.GetFillLevel(); }
+    int GetAdditionalFillNumber() const { return host_.GetAdditionalFillNumber(); }
+    int GetPrintLevel() const { return host_.GetPrintLevel(); }
+    int GetPivotBlockInteger() const { return host_.GetPivotBlockInteger(); }
+    double GetDroppingThreshold() const { return host_.GetDroppingThreshold(); }
+    double GetDiagonalCoefficient() const { return host_.GetDiagonalCoefficient(); }
+    double GetPivotThreshold() const { return host_.GetPivotThreshold(); }
+
+    void SetFactorisationType(int t) { host_.SetFactorisationType(t); }
+    void SetFillLevel(int k) { host_.SetFillLevel(k); }
+    void SetAdditionalFillNumber(int k) { host_.SetAdditionalFillNumber(k); }
+    void SetPrintLevel(int k) { host_.SetPrintLevel(k); }
+    void SetPivotBlockInteger(int k) { host_.SetPivotBlockInteger(k); }
+    void SetDroppingThreshold(double t) { host_.SetDroppingThreshold(t); }
+    void SetDiagonalCoefficient(double a) { host_.SetDiagonalCoefficient(a); }
+    void SetPivotThreshold(double t) { host_.SetPivotThreshold(t); }
+    void SetSymmetricAlgorithm()
+    {
+      host_.SetSymmetricAlgorithm();
+      symmetric_ = true;
+    }
+    void SetUnsymmetricAlgorithm()
+    {
+      host_.SetUnsymmetricAlgorithm();
+      symmetric_ = false;
+    }
+
+    //! Seldon's factorization of a host matrix, then the upload.
+    template <class Prop0, class Storage0, class Allocator0>
+    void FactorizeMatrix(const IVect& perm, Matrix<double, Prop0, Storage0, Allocator0>& mat,
+                         bool keep_matrix = false)
+    {
+      FactorizeHost(perm, mat, keep_matrix);
+      Upload();
+    }
+
+    //! Device matrices are read back and factorized on the host.
+    template <class Prop0>
+    void FactorizeMatrix(const IVect& perm,
+                         Matrix<double, Prop0, RowSparse, CudaAlloc<double> >& mat,
+                         bool keep_matrix = false)
+    {
+      Matrix<double, General, RowSparse> h;
+      mat.CopyToHost(h);
+      FactorizeMatrix(perm, h, false);
+      if (!keep_matrix)
+        mat.Clear();
+    }
+
+    template <class Prop0>
+    void FactorizeMatrix(const IVect& perm,
+                         Matrix<double, Prop0, RowSymSparse, CudaAlloc<double> >& mat,
+                         bool keep_matrix = false)
+    {
+      Matrix<double, Symmetric, RowSymSparse> h;
+      mat.CopyToHost(h);
+      FactorizeMatrix(perm, h, false);
+      if (!keep_matrix)
+        mat.Clear();
+    }
+
+    //! Library handle of the device factor.
+    sb2_precond* GetHandle() const
+    {
+      if (!M_)
+        throw WrongArgument("IlutPreconditioning", "no factor: call FactorizeMatrix first");
+      return M_;
+    }
+
+    template <class Matrix1>
+    void Solve(const Matrix1&, const vector_type& r, vector_type& z)
+    {
+      Apply(false, r, z);
+    }
+
+    template <class Matrix1>
+    void TransSolve(const Matrix1&, const vector_type& r, vector_type& z)
+    {
+      Apply(true, r, z);
+    }
+
+    void Solve(vector_type& z)
+    {
+      vector_type r(z);
+      Apply(false, r, z);
+    }
+
+    void TransSolve(vector_type& z)
+    {
+      vector_type r(z);
+      Apply(true, r, z);
+    }
+
+    template <class TransStatus>
+    void Solve(const TransStatus& transA, vector_type& z)
+    {
+      if (transA.Trans())
+        TransSolve(z);
+      else
+        Solve(z);
+    }
+
+  protected:
+    template <class Storage0, class Allocator0>
+    void FactorizeHost(const IVect& perm, Matrix<double, General, Storage0, Allocator0>& mat,
+                       bool keep_matrix)
+    {
+      if (symmetric_)
+        throw Undefined("IlutPreconditioning::FactorizeMatrix",
+                        "the symmetric algorithm needs symmetric storage");
+      host_.FactorizeMatrix(perm, mat, keep_matrix);
+    }
+
+    // The unsymmetric algorithm on symmetric storage does not compile in the
+    // reference (no Copy from RowSymSparse to ArrayRowSparse): only the
+    // symmetric algorithm is offered for it.
+    template <class Storage0, class Allocator0>
+    void FactorizeHost(const IVect& perm, Matrix<double, Symmetric, Storage0, Allocator0>& mat,
+                       bool keep_matrix)
+    {
+      if (!symmetric_)
+        throw Undefined("IlutPreconditioning::FactorizeMatrix",
+                        "symmetric storage needs SetSymmetricAlgorithm()");
+      host_.FactorizeSymMatrix(perm, mat, keep_matrix);
+    }
+
+    void Upload()
+    {
+      typedef b200::IlutState<SELDON_DEFAULT_ALLOCATOR<double> > state;
+      std::vector<int> fptr(1, 0), find;
+      std::vector<double> fval;
+      int n;
+      if (symmetric_)
+        {
+          const Matrix<double, Symmetric, ArrayRowSymSparse>& F = state::Sym(host_);
+          n = F.GetM();
+          for (int i = 0; i < n; i++)
+            {
+              for (int k = 0; k < F.GetRowSize(i); k++)
+                {
+                  // position 0 holds 1/D(i); its index is never read
+                  find.push_back(k == 0 ? i : F.Index(i, k));
+                  fval.push_back(F.Value(i, k));
+                }
+              fptr.push_back(int(find.size()));
+            }
+        }
+      else
+        {
+          const Matrix<double, General, ArrayRowSparse>& F = state::Unsym(host_);
+          n = F.GetM();
+          for (int i = 0; i < n; i++)
+            {
+              for (int k = 0; k < F.GetRowSize(i); k++)
+                {
+                  find.push_back(F.Index(i, k));
+                  fval.push_back(F.Value(i, k));
+                }
+              fptr.push_back(int(find.size()));
+            }
+        }
+      const IVect& pr = state::RowPerm(host_);
+      const IVect& pc = symmetric_ ? pr : state::ColPerm(host_);
+      std::vector<int> prow(n), pcol(n);
+      for (int i = 0; i < n; i++)
+        {
+          prow[i] = pr(i);
+          pcol[i] = pc(i);
+        }
+      sb2_precond* M = 0;
+      b200::Check(sb2_precond_create_ilut(NULL, n, &fptr[0], find.empty() ? NULL : &find[0],
+                                          fval.empty() ? NULL : &fval[0],
+                                          n ? &prow[0] : NULL, n ? &pcol[0] : NULL,
+                                          symmetric_ ? 1 : 0, &M),
+                  "IlutPreconditioning::FactorizeMatrix");
+      if (M_)
+        sb2_precond_destroy(M_);
+      M_ = M;
+    }
+
+    void Apply(bool trans, const vector_type& r, vector_type& z)
+    {
+      if (z.GetM() != r.GetM())
+        z.Reallocate(r.GetM());
+      b200::Check(trans ? sb2_precond_trans_solve(GetHandle(), r.GetData(), z.GetData(),
+                                                  b200::GetStream())
+                        : sb2_precond_solve(GetHandle(), r.GetData(), z.GetData(),
+                                            b200::GetStream()),
+                  trans ? "IlutPreconditioning::TransSolve" : "IlutPreconditioning::Solve");
+    }
+  };
+
+
+  namespace b200
+  {
+    //! The library's Krylov drivers take the device factor directly.
+    template <>
+    struct PrecondTraits<IlutPreconditioning<double, double, CudaAlloc<double> > >
+    {
+      static const bool native = true;
+      template <class MatrixD>
+      static void Acquire(IlutPreconditioning<double, double, CudaAlloc<double> >& M,
+                          const MatrixD&, PrecondHandle& h)
+      {
+        h.use = M.GetHandle();
+      }
+    };
+  }
+
+#endif
+
 } // namespace Seldon.
 
 #endif

@@ -232,8 +232,9 @@ int sb2_precond_destroy(sb2_precond* M);
  *                      (SparseSolver.cxx:852-882)
  *   perm_row, perm_col      permutation_row / permutation_col (perm_col is
  *                           not read when symmetric)
- *   A                       the system matrix the solvers are given (may be
- *                           NULL for sb2_precond_solve alone)
+ *   A                       the system matrix, or NULL: the factor is all
+ *                           the apply reads, and the solvers then accept it
+ *                           for any matrix of order n
  * Solve / TransSolve (IlutPreconditioning.cxx:329-374) then run on the
  * device as level-scheduled sweeps with the reference's own operation order:
  * z is the reference's z bit for bit.  The arrays are copied.  A factor
@@ -245,6 +246,16 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr,
                             const int* find, const double* fval,
                             const int* perm_row, const int* perm_col,
                             int symmetric, sb2_precond** out);
+
+/* ILU(0) computed on the device: IlutPreconditioning with
+ * SetFactorisationType(ILU_0) and the identity ordering on a RowSparse
+ * matrix (GetIlu0, IlutPreconditioning.cxx:1115-1176), row by row in levels
+ * of the L pattern, each row in the reference's operation order: the factor
+ * is GetIlu0's bit for bit.  A's rows must be sorted by column, without
+ * repeats, and hold their diagonal (SB2_ERR_INVALID_CSR otherwise); a zero
+ * pivot gives SB2_ERR_INVALID_VALUE (the reference aborts).  The result is an
+ * SB2_PRECOND_ILUT preconditioner bound to A. */
+int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out);
 
 /* z = M^{-1} r (Solve) / M^{-T} r (TransSolve).  z and r must not overlap.
  * Precond_Ssor.cxx:62-90: z is zeroed, then SOR type 0 (symmetric), 2

@@ -423,12 +423,34 @@ class IlutPreconditioning(_DevicePrecond):
         self._factor = (n, fptr, find, fval, prow, pcol, bool(symmetric))
         self._serial += 1
 
+    ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
+
+    def FactorizeMatrix(self, A, stream=None):
+        """ILU(0) of a RowSparse matrix computed on the device, as
+        SetFactorisationType(ILU_0) with the identity ordering gives it
+        (GetIlu0).  Other factorizations come from Seldon through SetFactor."""
+        if A.symmetric:
+            raise NotImplementedError("device ILU(0) takes RowSparse matrices")
+        h = ctypes.c_void_p()
+        check(_L.sb2_precond_create_ilu0(A.handle, _stream(stream), ctypes.byref(h)),
+              "sb2_precond_create_ilu0")
+        for _, old, _s in self._cache.values():
+            _L.sb2_precond_destroy(old)
+        self._factor = ("device", A.m)
+        self._serial += 1
+        self._cache = {id(A): (A, h, self._serial)}
+
     def _params(self):
         return self._serial
 
     def handle_for(self, A):
         if self._factor is None:
             raise RuntimeError("IlutPreconditioning: no factor (call SetFactor first)")
+        if self._factor[0] == "device":
+            ent = self._cache.get(id(A))
+            if ent is None or ent[0] is not A:
+                raise ValueError("IlutPreconditioning: factorized for another matrix")
+            return ent[1]
         key = id(A)
         ent = self._cache.get(key)
         if ent is None or ent[0] is not A or ent[2] != self._serial:

@@ -1359,7 +1359,14 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   // Solvers return 0 for an empty system before touching anything (Cg.cxx:50-51)
   if (A->m <= 0) return SB2_OK;
   const int kind = M ? precond_kind(M) : SB2_PRECOND_IDENTITY;
-  if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
+  // ILUT holds its own factor: it may be bound to no matrix, but its order
+  // must be the system's
+  if (kind == SB2_PRECOND_ILUT) {
+    if ((precond_matrix(M) && precond_matrix(M) != A) || precond_n(M) != A->m)
+      return SB2_ERR_INVALID_VALUE;
+  } else if (M && precond_matrix(M) != A) {
+    return SB2_ERR_INVALID_VALUE;
+  }
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;

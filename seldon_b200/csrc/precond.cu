@@ -233,6 +233,37 @@ struct GatherSub {
   }
 };
 
+// One row of GetIlu0 (IlutPreconditioning.cxx:1115-1176), in place on the
+// CSR values: rows sorted by column with the diagonal at dpos.  For each L
+// entry (stored order) tl = a_ij / u_jj (1/u_jj is already stored), then
+// a_ic -= tl * u_jc for the columns c of row j's U part that row i holds;
+// finally the diagonal is inverted.  A zero pivot is recorded in *status
+// (row + 1) and left as it is.
+struct Ilu0Row {
+  const int* ptr; const int* ind; double* val; const int* dpos; int* status;
+  __device__ void operator()(int i) const {
+    const int d = dpos[i], e = ptr[i + 1];
+    for (int j = ptr[i]; j < d; j++) {
+      const int jr = ind[j];
+      const double tl = mul_rn(ldx(val + j), ldx(val + dpos[jr]));
+      val[j] = tl;
+      int q = j + 1;
+      for (int k = dpos[jr] + 1; k < ptr[jr + 1]; k++) {
+        const int c = ind[k];
+        while (q < e && ind[q] < c) q++;
+        if (q == e) break;
+        if (ind[q] == c) val[q] = __dsub_rn(ldx(val + q), mul_rn(tl, ldx(val + k)));
+      }
+    }
+    const double piv = ldx(val + d);
+    if (piv == 0.0) {
+      atomicCAS(status, 0, i + 1);
+      return;
+    }
+    val[d] = __ddiv_rn(1.0, piv);
+  }
+};
+
 // out[idx[i]] = in[i]
 __global__ void perm_scatter_kernel(int n, const int* __restrict__ idx,
                                     const double* __restrict__ in, double* __restrict__ out) {
@@ -530,6 +561,66 @@ static int plan_ilut(sb2_precond* M, int n, const int* fp, const int* fi, const 
   return SB2_OK;
 }
 
+// GetIlu0 on the device: rows in levels of their L dependencies, each row
+// factored by one thread in the reference's operation order.  The factor
+// (A's pattern, Seldon's ArrayRowSparse layout) is returned on the host.
+static int ilu0_factor(const sb2_csr* A, std::vector<int>& ptr, std::vector<int>& ind,
+                       std::vector<double>& val, cudaStream_t s) {
+  const int n = A->m;
+  const CsrArrays& f = A->full;
+  ptr.resize(n + 1);
+  ind.resize(f.nnz);
+  val.resize(f.nnz);
+  SB2_CUDA_TRY(cudaMemcpy(ptr.data(), f.d_ptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+  if (f.nnz) {
+    SB2_CUDA_TRY(cudaMemcpy(ind.data(), f.d_ind, sizeof(int) * f.nnz, cudaMemcpyDeviceToHost));
+  }
+  // GetIlu0 reads the row prefix before the diagonal as L and needs every
+  // row sorted, with its diagonal, and no repeated column
+  std::vector<int> dpos(n, -1), lptr(n + 1, 0), lind;
+  for (int i = 0; i < n; i++) {
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      if (ind[k] < 0 || ind[k] >= n) return SB2_ERR_INVALID_CSR;
+      if (k > ptr[i] && ind[k] <= ind[k - 1]) return SB2_ERR_INVALID_CSR;
+      if (ind[k] == i) dpos[i] = k;
+      if (ind[k] < i) lind.push_back(ind[k]);
+    }
+    if (dpos[i] < 0) return SB2_ERR_INVALID_CSR;
+    lptr[i + 1] = (int)lind.size();
+  }
+  std::vector<int> level;
+  gather_levels(n, lptr, lind, true, level);
+  LevelPlan plan;
+  int st = upload_plan(level, n, &plan);
+  double* d_val = nullptr;
+  int *d_dpos = nullptr, *d_status = nullptr;
+  cudaError_t e = cudaMalloc(&d_val, sizeof(double) * std::max<long long>(f.nnz, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_dpos, sizeof(int) * std::max(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_status, sizeof(int));
+  if (e == cudaSuccess && f.nnz)
+    e = cudaMemcpyAsync(d_val, f.d_val, sizeof(double) * f.nnz, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_dpos, dpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_status, 0, sizeof(int), s);
+  if (st == SB2_OK) st = map_cuda_error(e);
+  int status = 0;
+  if (st == SB2_OK)
+    st = run_levels(plan, n, Ilu0Row{f.d_ptr, f.d_ind, d_val, d_dpos, d_status}, s);
+  if (st == SB2_OK) {
+    e = cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && f.nnz)
+      e = cudaMemcpyAsync(val.data(), d_val, sizeof(double) * f.nnz, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    st = map_cuda_error(e);
+  }
+  if (st == SB2_OK && status != 0) st = SB2_ERR_INVALID_VALUE;  // zero pivot
+  cudaFree(d_val);
+  cudaFree(d_dpos);
+  cudaFree(d_status);
+  plan.release();
+  return st;
+}
+
 static GatherSub sweep_op(const GatherSweep& S, const double* pre, const double* post, double* x) {
   return GatherSub{S.d_ptr, S.d_ind, S.d_val, pre, post, x};
 }
@@ -561,6 +652,7 @@ static int ilut_apply(const sb2_precond* M, bool trans, const double* r, double*
 }
 
 int precond_kind(const sb2_precond* M) { return M->kind; }
+int precond_n(const sb2_precond* M) { return M->kind == SB2_PRECOND_ILUT ? M->n_ilu : M->A->m; }
 const sb2_csr* precond_matrix(const sb2_precond* M) { return M->A; }
 
 int precond_apply(const sb2_precond* cM, bool trans, const double* r, double* z,
@@ -635,6 +727,21 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int*
   return SB2_OK;
 }
 
+int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out) {
+  if (!out || !A || A->m != A->n || A->sym) return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  const int n = A->m;
+  std::vector<int> ptr, ind;
+  std::vector<double> val;
+  if (n > 0) SB2_TRY(ilu0_factor(A, ptr, ind, val, (cudaStream_t)stream));
+  std::vector<int> ident(std::max(n, 1));
+  for (int i = 0; i < n; i++) ident[i] = i;
+  if (ptr.empty()) ptr.assign(1, 0);
+  return sb2_precond_create_ilut(A, n, ptr.data(), ind.empty() ? nullptr : ind.data(),
+                                 val.empty() ? nullptr : val.data(), ident.data(), ident.data(), 0,
+                                 out);
+}
+
 int sb2_precond_destroy(sb2_precond* M) {
   if (!M) return SB2_OK;
   M->fwd.release();
@@ -651,18 +758,14 @@ int sb2_precond_destroy(sb2_precond* M) {
   return SB2_OK;
 }
 
-static int precond_size(const sb2_precond* M) {
-  return M->kind == SB2_PRECOND_ILUT ? M->n_ilu : M->A->m;
-}
-
 int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
-  if (!M || (precond_size(M) > 0 && (!r || !z)) || (r == z && precond_size(M) > 0))
+  if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, false, r, z, (cudaStream_t)stream);
 }
 
 int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
-  if (!M || (precond_size(M) > 0 && (!r || !z)) || (r == z && precond_size(M) > 0))
+  if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, true, r, z, (cudaStream_t)stream);
 }

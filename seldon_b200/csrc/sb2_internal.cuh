@@ -133,6 +133,7 @@ int ensure_transpose(const sb2_csr* A);
 int ensure_diag(const sb2_csr* A);
 int precond_kind(const sb2_precond* M);
 const sb2_csr* precond_matrix(const sb2_precond* M);
+int precond_n(const sb2_precond* M);  // order of the system M applies to
 
 // Per-(device, stream) scratch for reductions: kRedSlots partial sums and a
 // completion counter that the last CTA resets to zero.

@@ -25,7 +25,8 @@ def test_cpp_dropin(cuda, tmp_path):
     for must in ("spmv_general", "spmv_symmetric", "blas1", "cg_identity", "cg_ssor",
                  "gmres20_jacobi", "bicgstab_identity", "cg_user_preconditioner",
                  "cg_zero_rhs", "invalid_csr_throws", "binary_files",
-                 "coordinate_assembly", "text_files"):
+                 "coordinate_assembly", "text_files", "ilut_apply", "ilut_gmres",
+                 "ilut_bicgstab", "ilut_sym_apply", "ilut_cg"):
         assert must in names, must
     # Seldon's other Krylov drivers, its generic templates on device types
     for drv in ("bicg", "bicgstabl", "bicgcr", "cgne", "cgs", "cocg", "gcr", "lsqr", "minres",

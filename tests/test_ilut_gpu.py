@@ -138,3 +138,44 @@ def _plain_iterations(api, M, b, which, tol, restart):
     fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
     fn(M, X, to_dev(b), api.Preconditioner_Base(), it)
     return it.GetNumberIteration()
+
+
+@pytest.mark.parametrize("name,make", [
+    ("conv9", lambda: matgen.convdiff3d(9)),
+    ("conv45", lambda: matgen.convdiff3d(45)),          # one launch per level
+    ("rand", lambda: _diag_dominant(3000, 0.004, 2)),
+])
+def test_ilu0_device_factor(api, oracle, reference, name, make):
+    """ILU(0) factored on the device applies exactly like the factor Seldon's
+    GetIlu0 computes (so the two factors agree bit for bit)."""
+    p, i, v = make()
+    n = p.size - 1
+    A = api.RowSparse(n, n, p, i, v)
+    M = api.IlutPreconditioning()
+    M.FactorizeMatrix(A)
+    factor = reference.ilut_factor(p, i, v, type_ilu=reference.ILU_0)
+    rng = np.random.default_rng(7)
+    for trans in (False, True):
+        r = rng.standard_normal(n)
+        assert np.array_equal(_apply(api, M, A, r, trans),
+                              oracle.ilut_solve(factor, r, trans=trans))
+
+
+def test_ilu0_rejects_unsorted_and_missing_diagonal(api):
+    from seldon_b200._lib import SeldonB200Error
+    ptr = np.array([0, 2, 3], dtype=np.int32)
+    M = api.IlutPreconditioning()
+    A = api.RowSparse(2, 2, ptr, np.array([1, 0, 1], dtype=np.int32), np.ones(3))
+    with pytest.raises(SeldonB200Error):
+        M.FactorizeMatrix(A)
+    A = api.RowSparse(2, 2, ptr, np.array([0, 1, 0], dtype=np.int32), np.ones(3))
+    with pytest.raises(SeldonB200Error):
+        M.FactorizeMatrix(A)
+
+
+def _diag_dominant(n, density, seed):
+    import scipy.sparse as sp
+    p, i, v = matgen.random_csr(n, n, density, seed=seed)
+    S = sp.csr_matrix((v, i, p), shape=(n, n)) + sp.identity(n) * 4.0
+    S.sort_indices()
+    return S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data
