@@ -354,6 +354,16 @@ struct sb2_precond {
   int* d_pcol = nullptr;
   double* d_dinv = nullptr;
   sb2::GatherSweep s_lf, s_ub, s_utf, s_ltb;
+  // Applies with one launch per level, recorded once per (r, z, direction)
+  // as CUDA graphs and replayed (the Krylov drivers reuse their buffers).
+  struct Recorded {
+    const double* r;
+    double* z;
+    bool trans;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Recorded> graphs;
+  cudaStream_t cap_stream = nullptr;
 };
 
 namespace sb2 {
@@ -625,9 +635,10 @@ static GatherSub sweep_op(const GatherSweep& S, const double* pre, const double*
   return GatherSub{S.d_ptr, S.d_ind, S.d_val, pre, post, x};
 }
 
-// IlutPreconditioning::Solve / TransSolve (IlutPreconditioning.cxx:329-374).
-static int ilut_apply(const sb2_precond* M, bool trans, const double* r, double* z,
-                      cudaStream_t s) {
+// IlutPreconditioning::Solve / TransSolve (IlutPreconditioning.cxx:329-374):
+// the launches.
+static int ilut_launch(const sb2_precond* M, bool trans, const double* r, double* z,
+                       cudaStream_t s) {
   const int n = M->n_ilu;
   double* t = M->d_t;
   const int g = std::min((n + 255) / 256, num_sms(current_device()) * 8);
@@ -648,6 +659,45 @@ static int ilut_apply(const sb2_precond* M, bool trans, const double* r, double*
     perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_prow, t, z);
   }
   SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+constexpr int kIluGraphs = 8;  // recorded applies kept per preconditioner
+
+// Small systems run every level in one CTA (one launch).  Larger ones
+// replay a recorded graph of the per-level launches: the launches then cost
+// the device's dependency resolution only, not a host call each.
+static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cudaStream_t s) {
+  if (M->n_ilu <= kSorSingleCtaMaxN) return ilut_launch(M, trans, r, z, s);
+  std::lock_guard<std::mutex> g(M->mu);
+  for (const auto& e : M->graphs)
+    if (e.r == r && e.z == z && e.trans == trans) {
+      SB2_CUDA_TRY(cudaGraphLaunch(e.exec, s));
+      return SB2_OK;
+    }
+  if (!M->cap_stream)
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&M->cap_stream, cudaStreamNonBlocking));
+  SB2_CUDA_TRY(cudaStreamBeginCapture(M->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int st = ilut_launch(M, trans, r, z, M->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(M->cap_stream, &graph);
+  if (st != SB2_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  SB2_CUDA_TRY(e);
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  SB2_CUDA_TRY(e);
+  if ((int)M->graphs.size() >= kIluGraphs) {
+    // the oldest recording goes once the stream has no launch of it pending
+    cudaStreamSynchronize(s);
+    cudaGraphExecDestroy(M->graphs.front().exec);
+    M->graphs.erase(M->graphs.begin());
+  }
+  M->graphs.push_back({r, z, trans, exec});
+  SB2_CUDA_TRY(cudaGraphLaunch(exec, s));
   return SB2_OK;
 }
 
@@ -744,6 +794,9 @@ int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out) {
 
 int sb2_precond_destroy(sb2_precond* M) {
   if (!M) return SB2_OK;
+  if (!M->graphs.empty()) cudaDeviceSynchronize();  // no replay may be in flight
+  for (auto& e : M->graphs) cudaGraphExecDestroy(e.exec);
+  if (M->cap_stream) cudaStreamDestroy(M->cap_stream);
   M->fwd.release();
   M->bwd.release();
   cudaFree(M->d_t);
