@@ -392,3 +392,55 @@ def test_cluster_cg_edges(api):
     it.HideMessages()
     assert api.Cg(A, X, to_dev(b), api.Preconditioner_Base(), it) == -2
     assert it.GetNumberIteration() == 7
+
+
+# ------------------------------------------------------------------ non-finite input
+
+def _nonfinite(name):
+    p, i, v = matgen.lap2d(12)
+    n = p.size - 1
+    b, x0 = np.ones(n), None
+    v = v.copy()
+    if name == "nan_b":
+        b[5] = np.nan
+    elif name == "inf_b":
+        b[3] = np.inf
+    elif name == "nan_A":
+        v[7] = np.nan
+    elif name == "inf_A":
+        v[10] = np.inf
+    elif name == "nan_x0":
+        x0 = np.zeros(n)
+        x0[2] = np.nan
+    return p, i, v, b, x0
+
+
+@pytest.mark.parametrize("name", ["nan_b", "inf_b", "nan_A", "inf_A", "nan_x0"])
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres"])
+@pytest.mark.parametrize("pc", [0, 1, 2])
+@pytest.mark.parametrize("cluster", [True, False])
+def test_nonfinite_inputs(api, oracle, name, which, pc, cluster):
+    """NaN / Inf in b, A or x0: the same exit code (-2, max_iter reached) and
+    iteration count as the oracle (pinned to Seldon), and NaN where the
+    oracle has NaN."""
+    from seldon_b200 import _lib
+    p, i, v, b, x0 = _nonfinite(name)
+    n = p.size - 1
+    xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, omega=1.2,
+                                    tol=1e-10, max_iter=25, restart=5)
+    A = api.RowSparse(n, n, p, i, v, validate=True)
+    X = to_dev(np.zeros(n) if x0 is None else x0)
+    it = api.Iteration(25, 1e-10)
+    it.SetRestart(5)
+    it.HideMessages()
+    if x0 is not None:
+        it.SetInitGuess(False)
+    old = _lib.load().sb2_krylov_set_cluster(int(cluster))
+    try:
+        fn = {"cg": api.Cg, "bicgstab": api.BiCgStab, "gmres": api.Gmres}[which]
+        code = fn(A, X, to_dev(b), _precond(api, pc), it)
+    finally:
+        _lib.load().sb2_krylov_set_cluster(old)
+    x = to_host(X)
+    assert (code, it.GetNumberIteration()) == (co, no) == (-2, 25)
+    assert np.array_equal(np.isnan(x), np.isnan(xo))

@@ -213,3 +213,41 @@ def test_ilut_solve_live(oracle, reference):
             r = rng.standard_normal(p.size - 1)
             assert np.array_equal(oracle.ilut_solve(f, r, sym=sym, trans=trans),
                                   reference.ilut_solve(r, trans=trans))
+
+
+def _nonfinite_cases():
+    p, i, v = matgen.lap2d(12)
+    n = p.size - 1
+    out = {}
+    b = np.ones(n)
+    b[5] = np.nan
+    out["nan_b"] = (p, i, v, b, None)
+    b = np.ones(n)
+    b[3] = np.inf
+    out["inf_b"] = (p, i, v, b, None)
+    v2 = v.copy()
+    v2[7] = np.nan
+    out["nan_A"] = (p, i, v2, np.ones(n), None)
+    v3 = v.copy()
+    v3[10] = np.inf
+    out["inf_A"] = (p, i, v3, np.ones(n), None)
+    x0 = np.zeros(n)
+    x0[2] = np.nan
+    out["nan_x0"] = (p, i, v, np.ones(n), x0)
+    return out
+
+
+@pytest.mark.parametrize("name", list(_nonfinite_cases()))
+def test_nonfinite_inputs_live(oracle, reference, name):
+    """NaN and Inf in b, A or x0: Seldon's drivers never see the residual
+    fall below tol and stop at max_iter with -2; the oracle does the same,
+    with the same iterate (NaNs included)."""
+    p, i, v, b, x0 = _nonfinite_cases()[name]
+    for which in ("cg", "bicgstab", "gmres"):
+        for pc in (0, 1, 2):
+            xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
+                                            max_iter=25, restart=5)
+            xr, cr, nr = reference.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
+                                         max_iter=25, restart=5)
+            assert (co, no) == (cr, nr) == (-2, 25)
+            assert np.array_equal(xo, xr, equal_nan=True)
