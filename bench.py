@@ -326,8 +326,10 @@ def run_ours(args, rank, world, local):
 
     # e2e: host (pinned) x in, y out, every step, through the C ABI's
     # pipelined host-buffer batch (the copy of x_{i+1} in, product i and the
-    # copy of y_{i-1} out overlap); G host vectors per call
-    G = max(1, min(args.steps, 8))
+    # copy of y_{i-1} out overlap); G host vectors per call.  Each call fills
+    # and drains the pipeline once (one copy direction alone at each end),
+    # so the K steps go in as few calls as 64-vector buffers allow.
+    G = max(1, min(args.steps, 64))
     xh = torch.empty((G, n), dtype=torch.float64).pin_memory()
     yh = torch.empty((G, n), dtype=torch.float64).pin_memory()
     xh.copy_(x.cpu().expand(G, n))
