@@ -231,64 +231,7 @@ struct GatherSub {
     if (post) v = mul_rn(v, post[j]);
     x[j] = v;
   }
-  // The same row inside one launch over all levels: each value read waits
-  // for its row's ready flag (bounded), and the row then publishes its own.
-  __device__ void sync_row(int j, unsigned* ready, unsigned* err,
-                           unsigned long long limit_ns) const {
-    double v = __ldcg(x + j);
-    if (pre) v = mul_rn(v, pre[j]);
-    for (int k = ptr[j]; k < ptr[j + 1]; k++) {
-      const int c = ind[k];
-      if (!wait_ready(ready + c, err, limit_ns)) break;
-      v = __dsub_rn(v, mul_rn(val[k], __ldcg(x + c)));
-    }
-    if (post) v = mul_rn(v, post[j]);
-    x[j] = v;
-    st_release_u32(ready + j, 1u);
-  }
-  // True once the flag is set; false when the wait ran out (recorded in
-  // *err) or another row's wait had already run out.
-  __device__ static bool wait_ready(const unsigned* f, unsigned* err,
-                                    unsigned long long limit_ns) {
-    if (ld_acquire_u32(f)) return true;
-    const unsigned long long t0 = global_timer_ns();
-    unsigned ns = 32;
-    for (;;) {
-      if (ld_acquire_u32(f)) return true;
-      if (ld_acquire_u32(err)) return false;
-      if (global_timer_ns() - t0 > limit_ns) {
-        atomicExch(err, 1u);
-        return false;
-      }
-      __nanosleep(ns);
-      if (ns < 512) ns <<= 1;
-    }
-  }
 };
-
-// One sweep in one launch.  Warps take chunks of at most 32 rows from a
-// counter in level order; a chunk never spans two levels, so the rows of a
-// warp never wait for one another, and every row a warp waits for belongs to
-// a chunk some running warp took before (the counter only moves forward), so
-// the waits end.
-template <class Op>
-__global__ void __launch_bounds__(256) syncfree_sweep(const int2* __restrict__ chunks,
-                                                      int nchunk, const int* __restrict__ rows,
-                                                      unsigned* counter, unsigned* ready,
-                                                      unsigned* err, unsigned long long limit_ns,
-                                                      Op op) {
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    unsigned c = 0;
-    if (lane == 0) c = atomicAdd(counter, 1u);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= (unsigned)nchunk) return;
-    const int2 ch = chunks[c];
-    const int i = ch.x + lane;
-    if (i < ch.y) op.sync_row(rows[i], ready, err, limit_ns);
-    __syncwarp();
-  }
-}
 
 // One row of GetIlu0 (IlutPreconditioning.cxx:1115-1176), in place on the
 // CSR values: rows sorted by column with the diagonal at dpos.  For each L
@@ -379,17 +322,12 @@ struct GatherSweep {
   int* d_ind = nullptr;
   double* d_val = nullptr;
   LevelPlan lv;
-  int nchunk = 0;
-  int2* d_chunk = nullptr;  // [nchunk] row ranges of lv.d_rows, within one level
   void release() {
     cudaFree(d_ptr);
     cudaFree(d_ind);
     cudaFree(d_val);
-    cudaFree(d_chunk);
     d_ptr = d_ind = nullptr;
     d_val = nullptr;
-    d_chunk = nullptr;
-    nchunk = 0;
     lv.release();
   }
 };
@@ -416,10 +354,16 @@ struct sb2_precond {
   int* d_pcol = nullptr;
   double* d_dinv = nullptr;
   sb2::GatherSweep s_lf, s_ub, s_utf, s_ltb;
-  // sync-free sweeps: per-row ready flags, the two chunk counters and the
-  // wait status
-  unsigned* d_ready = nullptr;
-  unsigned* d_ctl = nullptr;  // [0], [1] counters; [2] status
+  // Applies with one launch per level, recorded once per (r, z, direction)
+  // as CUDA graphs and replayed (the Krylov drivers reuse their buffers).
+  struct Recorded {
+    const double* r;
+    double* z;
+    bool trans;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Recorded> graphs;
+  cudaStream_t cap_stream = nullptr;
 };
 
 namespace sb2 {
@@ -514,18 +458,7 @@ static int upload_sweep(int n, const std::vector<int>& ptr, const std::vector<in
   }
   std::vector<int> level;
   gather_levels(n, ptr, ind, ascending, level);
-  SB2_TRY(upload_plan(level, n, &S->lv));
-  std::vector<int2> chunks;
-  for (int l = 0; l < S->lv.nlev; l++)
-    for (int b = S->lv.h_lvl[l]; b < S->lv.h_lvl[l + 1]; b += 32)
-      chunks.push_back(make_int2(b, std::min(b + 32, S->lv.h_lvl[l + 1])));
-  S->nchunk = (int)chunks.size();
-  if (S->nchunk) {
-    SB2_CUDA_TRY(cudaMalloc(&S->d_chunk, sizeof(int2) * chunks.size()));
-    SB2_CUDA_TRY(cudaMemcpy(S->d_chunk, chunks.data(), sizeof(int2) * chunks.size(),
-                            cudaMemcpyHostToDevice));
-  }
-  return SB2_OK;
+  return upload_plan(level, n, &S->lv);
 }
 
 // Update lists of a column scatter: entry (i -> c, v) for the rows i in the
@@ -631,8 +564,6 @@ static int plan_ilut(sb2_precond* M, int n, const int* fp, const int* fi, const 
   SB2_CUDA_TRY(cudaMalloc(&M->d_prow, sizeof(int) * std::max(n, 1)));
   SB2_CUDA_TRY(cudaMalloc(&M->d_pcol, sizeof(int) * std::max(n, 1)));
   SB2_CUDA_TRY(cudaMalloc(&M->d_t, sizeof(double) * std::max(n, 1)));
-  SB2_CUDA_TRY(cudaMalloc(&M->d_ready, sizeof(unsigned) * std::max(n, 1)));
-  SB2_CUDA_TRY(cudaMalloc(&M->d_ctl, sizeof(unsigned) * 4));
   SB2_CUDA_TRY(cudaMemcpy(M->d_dinv, dinv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMemcpy(M->d_prow, prow, sizeof(int) * n, cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMemcpy(M->d_pcol, M->ilu_sym ? prow : pcol, sizeof(int) * n,
@@ -731,61 +662,43 @@ static int ilut_launch(const sb2_precond* M, bool trans, const double* r, double
   return SB2_OK;
 }
 
-// One sweep as a single sync-free launch (rows wait for their inputs' ready
-// flags).  The flags and the chunk counter are cleared first, in stream order.
-static int syncfree_run(sb2_precond* M, const GatherSweep& S, const GatherSub& op, int which,
-                        cudaStream_t s) {
-  const int n = M->n_ilu;
-  SB2_CUDA_TRY(cudaMemsetAsync(M->d_ready, 0, sizeof(unsigned) * n, s));
-  SB2_CUDA_TRY(cudaMemsetAsync(M->d_ctl + which, 0, sizeof(unsigned), s));
-  const int grid = std::min(num_sms(current_device()) * 8, std::max(1, (S.nchunk + 7) / 8));
-  syncfree_sweep<GatherSub><<<grid, 256, 0, s>>>(
-      S.d_chunk, S.nchunk, S.lv.d_rows, M->d_ctl + which, M->d_ready, M->d_ctl + 2,
-      (unsigned long long)g_wait_limit_ms * 1000000ull, op);
-  SB2_CUDA_TRY(cudaGetLastError());
-  return SB2_OK;
-}
+constexpr int kIluGraphs = 8;  // recorded applies kept per preconditioner
 
-// Small systems run every level in one CTA (one launch).  Larger ones run
-// each sweep as one sync-free launch; a wait that ran out makes the call
-// return SB2_ERR_TIMEOUT.
+// Small systems run every level in one CTA (one launch).  Larger ones
+// replay a recorded graph of the per-level launches: the launches then cost
+// the device's dependency resolution only, not a host call each.
 static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cudaStream_t s) {
-  const int n = M->n_ilu;
-  if (n <= kSorSingleCtaMaxN) return ilut_launch(M, trans, r, z, s);
+  if (M->n_ilu <= kSorSingleCtaMaxN) return ilut_launch(M, trans, r, z, s);
   std::lock_guard<std::mutex> g(M->mu);
-  double* t = M->d_t;
-  const int g2 = std::min((n + 255) / 256, num_sms(current_device()) * 8);
-  SB2_CUDA_TRY(cudaMemsetAsync(M->d_ctl + 2, 0, sizeof(unsigned), s));
-  const GatherSweep *first, *second;
-  const double *pre1 = nullptr, *post1 = nullptr, *pre2 = nullptr, *post2 = nullptr;
-  if (M->ilu_sym) {
-    perm_scatter_kernel<<<g2, 256, 0, s>>>(n, M->d_prow, r, t);
-    first = &M->s_lf;
-    second = &M->s_ub;
-    pre2 = M->d_dinv;
-  } else if (!trans) {
-    perm_scatter_kernel<<<g2, 256, 0, s>>>(n, M->d_prow, r, t);
-    first = &M->s_lf;
-    second = &M->s_ub;
-    post2 = M->d_dinv;
-  } else {
-    perm_gather_kernel<<<g2, 256, 0, s>>>(n, M->d_pcol, r, t);
-    first = &M->s_utf;
-    second = &M->s_ltb;
-    post1 = M->d_dinv;
+  for (const auto& e : M->graphs)
+    if (e.r == r && e.z == z && e.trans == trans) {
+      SB2_CUDA_TRY(cudaGraphLaunch(e.exec, s));
+      return SB2_OK;
+    }
+  if (!M->cap_stream)
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&M->cap_stream, cudaStreamNonBlocking));
+  SB2_CUDA_TRY(cudaStreamBeginCapture(M->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int st = ilut_launch(M, trans, r, z, M->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(M->cap_stream, &graph);
+  if (st != SB2_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
   }
-  SB2_CUDA_TRY(cudaGetLastError());
-  SB2_TRY(syncfree_run(M, *first, sweep_op(*first, pre1, post1, t), 0, s));
-  SB2_TRY(syncfree_run(M, *second, sweep_op(*second, pre2, post2, t), 1, s));
-  if (M->ilu_sym || trans)
-    perm_gather_kernel<<<g2, 256, 0, s>>>(n, M->d_prow, t, z);
-  else
-    perm_scatter_kernel<<<g2, 256, 0, s>>>(n, M->d_pcol, t, z);
-  SB2_CUDA_TRY(cudaGetLastError());
-  unsigned status = 0;
-  SB2_CUDA_TRY(cudaMemcpyAsync(&status, M->d_ctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-  SB2_CUDA_TRY(cudaStreamSynchronize(s));
-  return status ? SB2_ERR_TIMEOUT : SB2_OK;
+  SB2_CUDA_TRY(e);
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  SB2_CUDA_TRY(e);
+  if ((int)M->graphs.size() >= kIluGraphs) {
+    // the oldest recording goes once the stream has no launch of it pending
+    cudaStreamSynchronize(s);
+    cudaGraphExecDestroy(M->graphs.front().exec);
+    M->graphs.erase(M->graphs.begin());
+  }
+  M->graphs.push_back({r, z, trans, exec});
+  SB2_CUDA_TRY(cudaGraphLaunch(exec, s));
+  return SB2_OK;
 }
 
 int precond_kind(const sb2_precond* M) { return M->kind; }
@@ -881,6 +794,9 @@ int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out) {
 
 int sb2_precond_destroy(sb2_precond* M) {
   if (!M) return SB2_OK;
+  if (!M->graphs.empty()) cudaDeviceSynchronize();  // no replay may be in flight
+  for (auto& e : M->graphs) cudaGraphExecDestroy(e.exec);
+  if (M->cap_stream) cudaStreamDestroy(M->cap_stream);
   M->fwd.release();
   M->bwd.release();
   cudaFree(M->d_t);
@@ -891,8 +807,6 @@ int sb2_precond_destroy(sb2_precond* M) {
   cudaFree(M->d_prow);
   cudaFree(M->d_pcol);
   cudaFree(M->d_dinv);
-  cudaFree(M->d_ready);
-  cudaFree(M->d_ctl);
   delete M;
   return SB2_OK;
 }
