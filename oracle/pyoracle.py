@@ -205,6 +205,29 @@ class Reference(_Base):
 
     ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
 
+    def write_hb(self, path, m, n, ptr, ind, val):
+        """Seldon's WriteHarwellBoeing of a RowSparse matrix."""
+        ptr, ind, val = _csr_args(ptr, ind, val)
+        self.lib.ref_write_hb.argtypes = [ctypes.c_char_p, _i, _i, _i, _vp, _vp, _vp]
+        self.lib.ref_write_hb(str(path).encode(), m, n, ind.size, _p(ptr), _p(ind), _p(val))
+
+    def read_hb(self, path, cap_cols=1 << 20, cap_nnz=1 << 24):
+        """Seldon's ReadHarwellBoeing into ColSparse: (m, n, colptr, rowind,
+        val), or raises RuntimeError with Seldon's message."""
+        L = self.lib
+        L.ref_read_hb.argtypes = [ctypes.c_char_p, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
+                                  ctypes.c_char_p, _i]
+        m, n, nz = (ctypes.c_int() for _ in range(3))
+        cp = np.zeros(cap_cols + 1, dtype=np.int32)
+        ri = np.zeros(cap_nnz, dtype=np.int32)
+        v = np.zeros(cap_nnz)
+        msg = ctypes.create_string_buffer(512)
+        st = L.ref_read_hb(str(path).encode(), ctypes.byref(m), ctypes.byref(n), ctypes.byref(nz),
+                           cap_cols, cap_nnz, _p(cp), _p(ri), _p(v), msg, 512)
+        if st != 0:
+            raise RuntimeError(msg.value.decode() or f"ref_read_hb status {st}")
+        return m.value, n.value, cp[:n.value + 1].copy(), ri[:nz.value].copy(), v[:nz.value].copy()
+
     def ilut_factor(self, ptr, ind, val, sym=False, perm=None, type_ilu=0, fill_level=1000000,
                     additional_fill=1000000, mbloc=1000000, alpha=1.0, droptol=0.01,
                     permtol=0.1):

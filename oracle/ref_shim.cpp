@@ -53,6 +53,8 @@ namespace Seldon
 }
 
 #include "SeldonSolver.hxx"
+// Harwell-Boeing files: Seldon.hxx does not include these (users do)
+#include "matrix_sparse/IOMatrixMarket.cxx"
 
 using namespace Seldon;
 
@@ -277,6 +279,38 @@ extern "C"
     for (int k = 0; k <= m && p; k++) ptr[k] = p[k];
     for (int k = 0; k < nnz; k++) { ind[k] = i[k]; val[k] = v[k]; }
     return 0;
+  }
+
+  // WriteHarwellBoeing (IOMatrixMarket.cxx:394-511) of a RowSparse matrix.
+  int ref_write_hb(const char* path, int m, int n, int nnz, const int* ptr,
+                   const int* ind, const double* val)
+  {
+    Wrap A(m, n, nnz, ptr, ind, val, 0);
+    WriteHarwellBoeing(A.G, std::string(path));
+    return 0;
+  }
+
+  // ReadHarwellBoeing (IOMatrixMarket.cxx:45-329) into ColSparse: sizes,
+  // then the arrays.  Returns -1 with *msg filled when Seldon throws.
+  int ref_read_hb(const char* path, int* m, int* n, int* nnz, int cap_cols,
+                  int cap_nnz, int* colptr, int* rowind, double* val,
+                  char* msg, int msg_cap)
+  {
+    try
+      {
+        Matrix<double, General, ColSparse> C;
+        ReadHarwellBoeing(std::string(path), C);
+        *m = C.GetM(); *n = C.GetN(); *nnz = C.GetDataSize();
+        if (*n > cap_cols || *nnz > cap_nnz) return -2;
+        for (int k = 0; k <= *n; k++) colptr[k] = C.GetPtr()[k];
+        for (int k = 0; k < *nnz; k++) { rowind[k] = C.GetInd()[k]; val[k] = C.GetData()[k]; }
+        return 0;
+      }
+    catch (Error& e)
+      {
+        std::snprintf(msg, msg_cap, "%s", e.What().c_str());
+        return -1;
+      }
   }
 
   // Seldon's binary vector format (Vector.cxx:848-870): size, then values.

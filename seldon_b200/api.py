@@ -197,6 +197,30 @@ class RowSparse:
         dev = [torch.as_tensor(a, device="cuda") for a in (r, c, v)]
         return cls.from_coordinates(*dev, index=1, validate=validate)
 
+    def WriteHarwellBoeing(self, path):
+        """WriteHarwellBoeing (IOMatrixMarket.cxx:394-511): the file
+        Seldon's writer produces for this matrix."""
+        if self.symmetric:
+            raise NotImplementedError("Harwell-Boeing files of RowSparse matrices only")
+        from seldon_b200 import io
+        io.write_harwell_boeing(path, self.m, self.n, *self.download())
+
+    @classmethod
+    def ReadHarwellBoeing(cls, path, validate=True):
+        """ReadHarwellBoeing (IOMatrixMarket.cxx:45-329): the file's
+        compressed columns, assembled into rows on the device."""
+        if cls.symmetric:
+            raise NotImplementedError("the reference reads unsymmetric Harwell-Boeing files only")
+        import numpy as np
+        import torch
+        from seldon_b200 import io
+        m, n, colptr, rowind, val = io.read_harwell_boeing(path)
+        cols = np.repeat(np.arange(n, dtype=np.int32), np.diff(colptr))
+        if rowind.size == 0:
+            return cls(m, n, np.zeros(m + 1, dtype=np.int32), [], [], validate)
+        dev = [torch.as_tensor(a, device="cuda") for a in (rowind, cols, val)]
+        return cls.from_coordinates(*dev, index=0, m=m, n=n, validate=validate)
+
     @classmethod
     def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):
         """Matrix built from coordinate triplets on the device, as

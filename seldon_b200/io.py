@@ -17,9 +17,13 @@ resume, or shared inputs):
                  writes both triangles ordered by (row, column)
                  (ConvertMatrix_to_Coordinates, Matrix_Conversions.cxx:
                  100-171).  Reading yields triplets; the matrix is assembled
-                 from them as ConvertMatrix_from_Coordinates does.
+                 from them as ConvertMatrix_from_Coordinates does;
+  Harwell-Boeing WriteHarwellBoeing / ReadHarwellBoeing (IOMatrixMarket.cxx):
+                 fixed-width text in compressed columns.
 """
+import math
 import os
+import re
 
 import numpy as np
 
@@ -138,3 +142,132 @@ def read_text(path):
         vals.append(x)
     return (np.array(rows, dtype=np.int32), np.array(cols, dtype=np.int32),
             np.array(vals, dtype=_F8))
+
+
+# ------------------------------------------------------------------ Harwell-Boeing
+
+def _hb_ptr_layout(n, nnz):
+    # WriteHarwellBoeing's field widths and counts (IOMatrixMarket.cxx:415-440)
+    ptr_len = int(math.ceil(math.log10(0.1 + nnz + 1))) + 1
+    ptr_nperline = min(80 // ptr_len, n + 1)
+    ind_len = int(math.ceil(math.log10(0.1 + n + 1))) + 1
+    ind_nperline = min(80 // ind_len, nnz)
+    return ptr_len, ptr_nperline, ind_len, ind_nperline
+
+
+def write_harwell_boeing(path, m, n, ptr, ind, val):
+    """WriteHarwellBoeing (IOMatrixMarket.cxx:394-511) of a RowSparse matrix:
+    the matrix in compressed columns (ConvertToCSC keeps the rows of a column
+    in increasing order), fixed-width fields, left-aligned, values as
+    %-23.15e three to a line, type RUA (square) or RRA.  nnz must be > 0
+    (the reference divides by the count per line, which is 0 otherwise)."""
+    ptr = np.asarray(ptr, dtype=np.int64)
+    ind = np.asarray(ind, dtype=np.int64)
+    val = np.asarray(val, dtype=_F8)
+    nnz = ind.size
+    if nnz == 0:
+        raise ValueError("WriteHarwellBoeing needs at least one entry")
+    rows = np.repeat(np.arange(m, dtype=np.int64), np.diff(ptr))
+    order = np.argsort(ind, kind="stable")
+    rowind, colv = rows[order], val[order]
+    colptr = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(colptr, ind + 1, 1)
+    colptr = np.cumsum(colptr)
+    ptr_len, ptr_nper, ind_len, ind_nper = _hb_ptr_layout(n, nnz)
+    ptrcrd = n // ptr_nper + 1
+    indcrd = (nnz - 1) // ind_nper + 1
+    valcrd = (nnz - 1) // 3 + 1
+    out = ["%-72s%-8s\n" % ("Seldon", "S0000008"),
+           "%-14d%-14d%-14d%-14d%-14d\n" % (ptrcrd + indcrd + valcrd, ptrcrd, indcrd, valcrd, 0),
+           "%s           %-14d%-14d%-14d%-14d\n" % ("RUA" if m == n else "RRA", m, n, nnz, 0),
+           "%-16s%-16s%-20s%-20s\n" % (f"({ptr_nper}I{ptr_len})", f"({ind_nper}I{ind_len})",
+                                      "(3D23.15)", "(3D23.15)")]
+    fp, fi = "%%-%dd" % ptr_len, "%%-%dd" % ind_len
+    p1 = (colptr + 1).tolist()
+    for i in range(0, n + 1, ptr_nper):
+        out.append("".join(fp % v for v in p1[i:i + ptr_nper]) + "\n")
+    r1 = (rowind + 1).tolist()
+    for i in range(0, nnz, ind_nper):
+        out.append("".join(fi % v for v in r1[i:i + ind_nper]) + "\n")
+    vl = colv.tolist()
+    for i in range(0, nnz, 3):
+        out.append("".join("%-23.15e" % v for v in vl[i:i + 3]) + "\n")
+    with open(path, "w") as f:
+        f.write("".join(out))
+
+
+_LEADING_INT = re.compile(r"\s*[+-]?\d+")
+_LEADING_FLOAT = re.compile(r"\s*[+-]?(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?")
+
+
+def _lead_int(s):
+    mt = _LEADING_INT.match(s)
+    if not mt:
+        raise ValueError(f"no integer in {s!r}")
+    return int(mt.group(0))
+
+
+def _lead_float(s):
+    mt = _LEADING_FLOAT.match(s.replace("D", "E").replace("d", "e"))
+    if not mt:
+        raise ValueError(f"no number in {s!r}")
+    return float(mt.group(0))
+
+
+def read_harwell_boeing(path):
+    """ReadHarwellBoeing (IOMatrixMarket.cxx:45-329): a real ('R') or
+    pattern ('P') assembled unsymmetric or rectangular matrix, returned as
+    Seldon's ColSparse arrays (m, n, colptr, rowind, val), 0-based.  Types
+    the reference rejects (complex, Hermitian, skew, symmetric, elemental)
+    raise ValueError.  Beyond the reference, Fortran 'D' is read in the value
+    format and in the values: the reference rejects its own writer's
+    "(3D23.15)" format."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    head2 = lines[1].split()
+    head3 = lines[2].split()
+    if len(head2) < 5 or len(head3) < 5:
+        raise ValueError(f"{path}: incomplete Harwell-Boeing header")
+    nl_ptr, nl_ind, nl_val, nl_rhs = (int(t) for t in head2[1:5])
+    typ = head3[0]
+    nrow, ncol, nnz, nelt = (int(t) for t in head3[1:5])
+    if len(typ) != 3 or typ[0] not in "RCP":
+        raise ValueError(f"{path}: type {typ!r} is not a valid type")
+    if typ[0] == "C":
+        raise ValueError(f"{path}: complex-valued matrices are not supported")
+    if typ[1] in "HZS":
+        raise ValueError(f"{path}: Hermitian, skew or symmetric matrices are not supported")
+    if nelt != 0 or typ[2] == "E":
+        raise ValueError(f"{path}: elemental matrices are not supported")
+    fmt = lines[3]
+    lw_ptr, ew_ptr = (int(t) for t in re.match(r"\s*\((\d+)I(\d+)\)", fmt[0:16]).groups())
+    lw_ind, ew_ind = (int(t) for t in re.match(r"\s*\((\d+)I(\d+)\)", fmt[16:32]).groups())
+    lw_val = ew_val = 0
+    if typ[0] != "P":
+        nums = [int(t) for t in re.split(r"[ (ABDEFGILOPZ*.)]+", fmt[32:48]) if t.isdigit()]
+        if len(nums) < 3:
+            raise ValueError(f"{path}: value format {fmt[32:48]!r} could not be parsed")
+        lw_val, ew_val = nums[-3], nums[-2]
+    pos = 4 + (1 if nl_rhs != 0 else 0)
+
+    def fixed(count, nlines, per_line, width, conv):
+        nonlocal pos
+        out = []
+        for _ in range(nlines):
+            line = lines[pos]
+            pos += 1
+            for j in range(per_line):
+                out.append(conv(line[j * width:(j + 1) * width]))
+                if len(out) == count:
+                    return out
+        if len(out) < count:
+            raise ValueError(f"{path}: fewer entries than the header announces")
+        return out
+
+    colptr = np.array(fixed(ncol + 1, nl_ptr, lw_ptr, ew_ptr, _lead_int), dtype=np.int32) - 1
+    rowind = np.array(fixed(nnz, nl_ind, lw_ind, ew_ind, _lead_int), dtype=np.int32) - 1
+    if typ[0] == "P":
+        val = np.ones(nnz)
+    else:
+        val = np.array(fixed(nnz, nl_val, lw_val, ew_val, _lead_float), dtype=_F8)
+    return nrow, ncol, colptr, rowind, val

@@ -95,3 +95,79 @@ def test_text_read_stops_and_rejects(tmp_path):
     p.write_text("1 1 2.0\n0 3 -1\n")
     with pytest.raises(ValueError):
         io.read_text(p)
+
+
+# ------------------------------------------------------------------ Harwell-Boeing
+
+@pytest.mark.parametrize("name", ["general", "rect_empty_rows"])
+def test_harwell_boeing_write_same_bytes(reference, tmp_path, name):
+    m, n, ptr, ind, val, _ = _cases()[name]
+    ours, theirs = tmp_path / "ours.rua", tmp_path / "theirs.rua"
+    io.write_harwell_boeing(ours, m, n, ptr, ind, val)
+    reference.write_hb(theirs, m, n, ptr, ind, val)
+    assert ours.read_bytes() == theirs.read_bytes()
+
+
+def _hb_case(seed, m, n):
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    A = sp.random(m, n, density=0.08, random_state=seed, format="csc")
+    A.data = rng.standard_normal(A.nnz) * 10.0 ** rng.integers(-30, 30, A.nnz)
+    A.sort_indices()
+    return A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data
+
+
+@pytest.mark.parametrize("typ,m,n", [("RUA", 60, 60), ("RRA", 45, 70), ("PUA", 50, 50)])
+def test_harwell_boeing_read_like_seldon(reference, tmp_path, typ, m, n):
+    """Files in the collection's layout (fields of width 6 with a blank, E
+    format for values): the arrays Seldon reads, bit for bit."""
+    colptr, rowind, val = _hb_case(m + n, m, n)
+    path = tmp_path / "a.hb"
+    _write_collection_hb(path, typ, m, n, colptr, rowind, val)
+    ours = io.read_harwell_boeing(path)
+    theirs = reference.read_hb(path)
+    assert ours[:2] == theirs[:2] == (m, n)
+    for a, b in zip(ours[2:], theirs[2:]):
+        assert np.array_equal(a, b)
+
+
+def _write_collection_hb(path, typ, m, n, colptr, rowind, val):
+    nnz = rowind.size
+    ptr_lines = ["".join("%6d" % (v + 1) for v in colptr[i:i + 10]) for i in range(0, n + 1, 10)]
+    ind_lines = ["".join("%6d" % (v + 1) for v in rowind[i:i + 10]) for i in range(0, nnz, 10)]
+    val_lines = [] if typ[0] == "P" else [
+        "".join("%20.12E" % v for v in val[i:i + 4]) for i in range(0, nnz, 4)]
+    with open(path, "w") as f:
+        f.write("%-72s%-8s\n" % ("test matrix", "TEST"))
+        tot = len(ptr_lines) + len(ind_lines) + len(val_lines)
+        f.write("%14d%14d%14d%14d%14d\n" % (tot, len(ptr_lines), len(ind_lines),
+                                             len(val_lines), 0))
+        f.write("%-14s%14d%14d%14d%14d\n" % (typ, m, n, nnz, 0))
+        f.write("%-16s%-16s%-20s\n" % ("(10I6)", "(10I6)",
+                                       "(4E20.12)" if typ[0] != "P" else ""))
+        f.write("".join(ln + "\n" for ln in ptr_lines + ind_lines + val_lines))
+
+
+@pytest.mark.parametrize("typ", ["RSA", "CUA", "RUE"])
+def test_harwell_boeing_rejects_like_seldon(reference, tmp_path, typ):
+    colptr, rowind, val = _hb_case(3, 20, 20)
+    path = tmp_path / "a.hb"
+    _write_collection_hb(path, typ, 20, 20, colptr, rowind, val)
+    with pytest.raises(ValueError):
+        io.read_harwell_boeing(path)
+    with pytest.raises(RuntimeError):
+        reference.read_hb(path)
+
+
+def test_harwell_boeing_reads_own_files(tmp_path):
+    """The reference cannot read what its writer produces ("(3D23.15)" is
+    not parsed); this reader can, to the 16 digits written."""
+    g = matgen.lap2d(9)
+    path = tmp_path / "a.rua"
+    io.write_harwell_boeing(path, 81, 81, *g)
+    m, n, cp, ri, v = io.read_harwell_boeing(path)
+    import scipy.sparse as sp
+    C = sp.csr_matrix((g[2], g[1], g[0]), shape=(81, 81)).tocsc()
+    assert (m, n) == (81, 81)
+    assert np.array_equal(cp, C.indptr) and np.array_equal(ri, C.indices)
+    assert np.allclose(v, C.data, rtol=1e-15, atol=0)
