@@ -1603,6 +1603,48 @@ namespace Seldon
   }
 
 
+  //////////////////////////////
+  // HARWELL-BOEING FILES     //
+  //////////////////////////////
+
+
+#ifdef SELDON_FILE_MATRIX_SPARSE_IOMATRIXMARKET_CXX
+
+  //! WriteHarwellBoeing (IOMatrixMarket.cxx:394-511) of a device matrix:
+  //! Seldon's writer on a host copy, so the file is the same byte for byte.
+  template <class Prop>
+  void WriteHarwellBoeing(const Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+                          const string& file_name)
+  {
+    Matrix<double, General, RowSparse> h;
+    A.CopyToHost(h);
+    WriteHarwellBoeing(h, file_name);
+  }
+
+  //! ReadHarwellBoeing (IOMatrixMarket.cxx:45-329) into a device matrix:
+  //! Seldon reads the compressed columns on the host, and the matrix is
+  //! assembled by rows on the device.
+  template <class Prop>
+  void ReadHarwellBoeing(string filename, Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A)
+  {
+    Matrix<double, General, ColSparse> C;
+    ReadHarwellBoeing(filename, C);
+    const int n = C.GetN(), nnz = C.GetDataSize();
+    std::vector<int> rows(nnz), cols(nnz);
+    for (int j = 0; j < n; j++)
+      for (int k = C.GetPtr()[j]; k < C.GetPtr()[j + 1]; k++)
+        {
+          rows[k] = C.GetInd()[k];
+          cols[k] = j;
+        }
+    A.Reallocate(C.GetM(), n);
+    if (nnz > 0)
+      A.AssembleHost(nnz, &rows[0], &cols[0], C.GetData(), 0);
+  }
+
+#endif
+
+
   ///////////////////////////////////////////
   // ILUT: SELDON'S FACTOR, APPLIED ON GPU //
   ///////////////////////////////////////////

@@ -45,6 +45,7 @@ namespace Seldon
 }
 
 #include "SeldonSolver.hxx"
+#include "matrix_sparse/IOMatrixMarket.cxx"
 #include "SeldonB200.hxx"
 
 using namespace Seldon;
@@ -747,6 +748,52 @@ int main()
     std::remove(t1.c_str());
     std::remove(t2.c_str());
     report(text_ok, "text_files", "ReadText/WriteText match Seldon's");
+  }
+
+  // ------------------------------------------------ Harwell-Boeing files
+  {
+    const std::string f1 = "dropin_ref.rua", f2 = "dropin_dev.rua", f3 = "dropin_in.rua";
+    WriteHarwellBoeing(Gh, f1);
+    WriteHarwellBoeing(Gd, f2);
+    std::ifstream a(f1.c_str()), b(f2.c_str());
+    std::string sa((std::istreambuf_iterator<char>(a)), std::istreambuf_iterator<char>());
+    std::string sb((std::istreambuf_iterator<char>(b)), std::istreambuf_iterator<char>());
+    bool ok = sa == sb && !sa.empty();
+    // a 3 x 4 file in the collection's layout (E format, which Seldon reads)
+    {
+      std::ofstream f(f3.c_str());
+      f << "small test matrix                                                       TEST0001\n"
+        << "             4             1             1             2             0\n"
+        << "RRA                        3             4             5             0\n"
+        << "(10I6)          (10I6)          (4E20.12)           \n"
+        << "     1     3     4     5     6\n"
+        << "     1     3     2     1     3\n"
+        << "  1.000000000000E+00 -2.500000000000E+00  3.000000000000E-01  4.000000000000E+02\n"
+        << " -5.000000000000E+00\n";
+    }
+    Matrix<double, General, ColSparse> Ch;
+    ReadHarwellBoeing(f3, Ch);
+    DevGen Hd;
+    ReadHarwellBoeing(f3, Hd);
+    std::vector<int> p, i;
+    std::vector<double> v;
+    Hd.Download(p, i, v);
+    // the same matrix by rows: (0,0)=1 (0,2)=0.3 (1,3)=-5 ... from the columns
+    ok = ok && Hd.GetM() == 3 && Hd.GetN() == 4 && Hd.GetNonZeros() == Ch.GetDataSize();
+    for (int c = 0; ok && c < Ch.GetN(); c++)
+      for (int k = Ch.GetPtr()[c]; ok && k < Ch.GetPtr()[c + 1]; k++)
+        {
+          const int r = Ch.GetInd()[k];
+          bool found = false;
+          for (int q = p[r]; q < p[r + 1]; q++)
+            if (i[q] == c)
+              found = v[q] == Ch.GetData()[k];
+          ok = found;
+        }
+    std::remove(f1.c_str());
+    std::remove(f2.c_str());
+    std::remove(f3.c_str());
+    report(ok, "harwell_boeing", "device WriteHarwellBoeing == Seldon's; ReadHarwellBoeing by rows");
   }
 
   // ------------------------------------------------ errors
