@@ -51,7 +51,9 @@ int sb2_version(void);
  * allocator concept's allocate/deallocate/memorycpy (share/Allocator.hxx:
  * 31-48, share/Allocator.cxx:33-65) on device memory.
  *   sb2_device_alloc  cudaMalloc of `bytes` (bytes == 0 gives NULL)
- *   sb2_device_free   cudaFree (NULL is a no-op)
+ *   sb2_device_free   cudaFree (NULL is a no-op); arrays that sb2_coo_to_csr
+ *                     returned go back to the library's memory pool, after
+ *                     the device has finished its work, as cudaFree waits
  *   sb2_memcpy        copy `bytes` between host and/or device memory
  *                     (unified addressing decides the direction), on
  *                     `stream`; returns after the copy has completed

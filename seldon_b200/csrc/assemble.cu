@@ -506,17 +506,17 @@ int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val, i
 
   int *dp = nullptr, *di = nullptr;
   double* dv = nullptr;
-  cudaError_t e = cudaMalloc((void**)&dp, sizeof(int) * (m + 1));
-  if (e == cudaSuccess && nout > 0) e = cudaMalloc((void**)&di, sizeof(int) * nout);
-  if (e == cudaSuccess && nout > 0) e = cudaMalloc((void**)&dv, sizeof(double) * nout);
+  cudaError_t e = pool_malloc_owned((void**)&dp, sizeof(int) * (m + 1), s);
+  if (e == cudaSuccess && nout > 0) e = pool_malloc_owned((void**)&di, sizeof(int) * nout, s);
+  if (e == cudaSuccess && nout > 0) e = pool_malloc_owned((void**)&dv, sizeof(double) * nout, s);
   int st = map_cuda_error(e);
   if (st == SB2_OK)
     st = assemble(nnz, row, col, val, index, (int)m, cb, symmetric_upper, nout, dp, di, dv, s);
   if (st == SB2_OK) st = map_cuda_error(cudaStreamSynchronize(s));
   if (st != SB2_OK) {
-    cudaFree(dp);
-    cudaFree(di);
-    cudaFree(dv);
+    sb2_device_free(dp);
+    sb2_device_free(di);
+    sb2_device_free(dv);
     return st;
   }
   *m_out = (int)m;

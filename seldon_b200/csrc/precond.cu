@@ -39,7 +39,8 @@ struct LevelPlan {
   }
 };
 
-static int upload_plan(const std::vector<int>& level, int n, LevelPlan* P) {
+static int upload_plan(const std::vector<int>& level, int n, LevelPlan* P,
+                       std::vector<int>* order = nullptr) {
   int nlev = 0;
   for (int i = 0; i < n; i++) nlev = std::max(nlev, level[i] + 1);
   P->nlev = nlev;
@@ -52,6 +53,7 @@ static int upload_plan(const std::vector<int>& level, int n, LevelPlan* P) {
   SB2_CUDA_TRY(cudaMalloc(&P->d_lvl, sizeof(int) * (nlev + 1)));
   SB2_CUDA_TRY(cudaMemcpy(P->d_rows, rows.data(), sizeof(int) * std::max(n, 1), cudaMemcpyHostToDevice));
   SB2_CUDA_TRY(cudaMemcpy(P->d_lvl, P->h_lvl.data(), sizeof(int) * (nlev + 1), cudaMemcpyHostToDevice));
+  if (order) order->assign(rows.begin(), rows.begin() + n);
   return SB2_OK;
 }
 
@@ -219,19 +221,41 @@ __global__ void __launch_bounds__(1024) level_single_cta(int nlev, const int* __
   }
 }
 
+// The same kernels for ops that take the position in level order.
+template <class Op>
+__global__ void level_kernel_pos(int begin, int end, Op op) {
+  int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < end) op(i);
+}
+
+template <class Op>
+__global__ void __launch_bounds__(1024) level_single_cta_pos(int nlev, const int* __restrict__ lvl,
+                                                             Op op) {
+  for (int l = 0; l < nlev; l++) {
+    for (int i = lvl[l] + threadIdx.x; i < lvl[l + 1]; i += blockDim.x) op(i);
+    __syncthreads();
+  }
+}
+
 // x_j = (x_j * pre_j - v_1 x_{c1} - v_2 x_{c2} - ...) * post_j, the
-// subtractions in the listed order (pre/post may be null).
-struct GatherSub {
-  const int* ptr; const int* ind; const double* val;
+// subtractions in the listed order (pre/post may be null), for a gather
+// sweep whose update lists are stored in level order: position i
+// holds row rows[i] and its list ptr[i]..ptr[i+1], so the row id, the list
+// bounds and (through them) the entries load without waiting on each other.
+struct GatherSubPacked {
+  const int* rows; const int* ptr; const int* ind; const double* val;
   const double* pre; const double* post; double* x;
-  __device__ void operator()(int j) const {
+  __device__ void operator()(int i) const {
+    const int j = rows[i];
+    const int e = ptr[i + 1];
     double v = ldx(x + j);
     if (pre) v = mul_rn(v, pre[j]);
-    for (int k = ptr[j]; k < ptr[j + 1]; k++) v = __dsub_rn(v, mul_rn(val[k], ldx(x + ind[k])));
+    for (int k = ptr[i]; k < e; k++) v = __dsub_rn(v, mul_rn(val[k], ldx(x + ind[k])));
     if (post) v = mul_rn(v, post[j]);
     x[j] = v;
   }
 };
+
 
 // One row of GetIlu0 (IlutPreconditioning.cxx:1115-1176), in place on the
 // CSR values: rows sorted by column with the diagonal at dpos.  For each L
@@ -306,6 +330,21 @@ static int run_levels(const LevelPlan& P, int n, const Op& op, cudaStream_t s) {
 }
 
 template <class Op>
+static int run_levels_pos(const LevelPlan& P, int n, const Op& op, cudaStream_t s) {
+  if (n == 0 || P.nlev == 0) return SB2_OK;
+  if (n <= kSorSingleCtaMaxN) {
+    level_single_cta_pos<Op><<<1, 1024, 0, s>>>(P.nlev, P.d_lvl, op);
+  } else {
+    for (int l = 0; l < P.nlev; l++) {
+      const int cnt = P.h_lvl[l + 1] - P.h_lvl[l];
+      level_kernel_pos<Op><<<(cnt + 255) / 256, 256, 0, s>>>(P.h_lvl[l], P.h_lvl[l + 1], op);
+    }
+  }
+  SB2_CUDA_TRY(cudaGetLastError());
+  return SB2_OK;
+}
+
+template <class Op>
 static int run_rows(int n, const Op& op, cudaStream_t s) {
   if (n == 0) return SB2_OK;
   rows_kernel<Op><<<(n + 255) / 256, 256, 0, s>>>(n, op);
@@ -316,7 +355,8 @@ static int run_rows(int n, const Op& op, cudaStream_t s) {
 }  // namespace sb2
 
 namespace sb2 {
-// One triangular sweep in gather form: rows' update lists and their levels.
+// One triangular sweep in gather form: the rows' update lists, stored in
+// level order (list i belongs to row lv.d_rows[i]), and the levels.
 struct GatherSweep {
   int* d_ptr = nullptr;
   int* d_ind = nullptr;
@@ -447,18 +487,30 @@ static void gather_levels(int n, const std::vector<int>& ptr, const std::vector<
 
 static int upload_sweep(int n, const std::vector<int>& ptr, const std::vector<int>& ind,
                         const std::vector<double>& val, bool ascending, GatherSweep* S) {
-  const size_t nz = ind.size();
+  std::vector<int> level, order;
+  gather_levels(n, ptr, ind, ascending, level);
+  SB2_TRY(upload_plan(level, n, &S->lv, &order));
+  // the lists in level order
+  std::vector<int> pptr(n + 1, 0), pind;
+  std::vector<double> pval;
+  pind.reserve(ind.size());
+  pval.reserve(val.size());
+  for (int i = 0; i < n; i++) {
+    const int j = order[i];
+    pind.insert(pind.end(), ind.begin() + ptr[j], ind.begin() + ptr[j + 1]);
+    pval.insert(pval.end(), val.begin() + ptr[j], val.begin() + ptr[j + 1]);
+    pptr[i + 1] = (int)pind.size();
+  }
+  const size_t nz = pind.size();
   SB2_CUDA_TRY(cudaMalloc(&S->d_ptr, sizeof(int) * (n + 1)));
   SB2_CUDA_TRY(cudaMalloc(&S->d_ind, sizeof(int) * std::max<size_t>(nz, 1)));
   SB2_CUDA_TRY(cudaMalloc(&S->d_val, sizeof(double) * std::max<size_t>(nz, 1)));
-  SB2_CUDA_TRY(cudaMemcpy(S->d_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  SB2_CUDA_TRY(cudaMemcpy(S->d_ptr, pptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
   if (nz) {
-    SB2_CUDA_TRY(cudaMemcpy(S->d_ind, ind.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
-    SB2_CUDA_TRY(cudaMemcpy(S->d_val, val.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    SB2_CUDA_TRY(cudaMemcpy(S->d_ind, pind.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
+    SB2_CUDA_TRY(cudaMemcpy(S->d_val, pval.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
   }
-  std::vector<int> level;
-  gather_levels(n, ptr, ind, ascending, level);
-  return upload_plan(level, n, &S->lv);
+  return SB2_OK;
 }
 
 // Update lists of a column scatter: entry (i -> c, v) for the rows i in the
@@ -631,8 +683,9 @@ static int ilu0_factor(const sb2_csr* A, std::vector<int>& ptr, std::vector<int>
   return st;
 }
 
-static GatherSub sweep_op(const GatherSweep& S, const double* pre, const double* post, double* x) {
-  return GatherSub{S.d_ptr, S.d_ind, S.d_val, pre, post, x};
+static GatherSubPacked sweep_op(const GatherSweep& S, const double* pre, const double* post,
+                                double* x) {
+  return GatherSubPacked{S.lv.d_rows, S.d_ptr, S.d_ind, S.d_val, pre, post, x};
 }
 
 // IlutPreconditioning::Solve / TransSolve (IlutPreconditioning.cxx:329-374):
@@ -644,18 +697,18 @@ static int ilut_launch(const sb2_precond* M, bool trans, const double* r, double
   const int g = std::min((n + 255) / 256, num_sms(current_device()) * 8);
   if (M->ilu_sym) {
     perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_prow, r, t);
-    SB2_TRY(run_levels(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
-    SB2_TRY(run_levels(M->s_ub.lv, n, sweep_op(M->s_ub, M->d_dinv, nullptr, t), s));
+    SB2_TRY(run_levels_pos(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
+    SB2_TRY(run_levels_pos(M->s_ub.lv, n, sweep_op(M->s_ub, M->d_dinv, nullptr, t), s));
     perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_prow, t, z);
   } else if (!trans) {
     perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_prow, r, t);
-    SB2_TRY(run_levels(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
-    SB2_TRY(run_levels(M->s_ub.lv, n, sweep_op(M->s_ub, nullptr, M->d_dinv, t), s));
+    SB2_TRY(run_levels_pos(M->s_lf.lv, n, sweep_op(M->s_lf, nullptr, nullptr, t), s));
+    SB2_TRY(run_levels_pos(M->s_ub.lv, n, sweep_op(M->s_ub, nullptr, M->d_dinv, t), s));
     perm_scatter_kernel<<<g, 256, 0, s>>>(n, M->d_pcol, t, z);
   } else {
     perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_pcol, r, t);
-    SB2_TRY(run_levels(M->s_utf.lv, n, sweep_op(M->s_utf, nullptr, M->d_dinv, t), s));
-    SB2_TRY(run_levels(M->s_ltb.lv, n, sweep_op(M->s_ltb, nullptr, nullptr, t), s));
+    SB2_TRY(run_levels_pos(M->s_utf.lv, n, sweep_op(M->s_utf, nullptr, M->d_dinv, t), s));
+    SB2_TRY(run_levels_pos(M->s_ltb.lv, n, sweep_op(M->s_ltb, nullptr, nullptr, t), s));
     perm_gather_kernel<<<g, 256, 0, s>>>(n, M->d_prow, t, z);
   }
   SB2_CUDA_TRY(cudaGetLastError());

@@ -151,6 +151,10 @@ int num_sms(int device);
 // Stream-ordered workspace allocation from the library's own memory pool
 // (freed with cudaFreeAsync).
 cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s);
+// The same for arrays handed to the caller: sb2_device_free returns them to
+// the pool (release_owned is false for any other pointer).
+cudaError_t pool_malloc_owned(void** p, size_t bytes, cudaStream_t s);
+bool release_owned(void* p, cudaError_t* err);
 
 // Launch y = beta*y + alpha*A*x (overwrite: y = alpha*A*x) on a CSR operator.
 int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,

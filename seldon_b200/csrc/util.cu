@@ -71,6 +71,40 @@ cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s) {
   return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
+// Arrays handed to the caller from the pool (sb2_coo_to_csr's outputs):
+// sb2_device_free gives them back to the pool instead of the driver, which
+// saves the unmapping (and the next call's mapping) of large buffers.
+static std::mutex g_owned_mu;
+static std::map<void*, int> g_owned;  // pointer -> device
+
+cudaError_t pool_malloc_owned(void** p, size_t bytes, cudaStream_t s) {
+  cudaError_t e = pool_malloc(p, bytes, s);
+  if (e == cudaSuccess) {
+    std::lock_guard<std::mutex> g(g_owned_mu);
+    g_owned[*p] = current_device();
+  }
+  return e;
+}
+
+bool release_owned(void* p, cudaError_t* err) {
+  int dev;
+  {
+    std::lock_guard<std::mutex> g(g_owned_mu);
+    auto it = g_owned.find(p);
+    if (it == g_owned.end()) return false;
+    dev = it->second;
+    g_owned.erase(it);
+  }
+  // cudaFree's guarantee: no work on the device still uses p
+  int prev = current_device();
+  cudaSetDevice(dev);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaFreeAsync(p, 0);
+  cudaSetDevice(prev);
+  *err = e;
+  return true;
+}
+
 int get_red_scratch(cudaStream_t s, RedScratch** out) {
   static std::mutex mu;
   static std::map<std::pair<int, cudaStream_t>, RedScratch*> table;
@@ -130,6 +164,8 @@ int sb2_device_alloc(size_t bytes, void** out) {
 
 int sb2_device_free(void* p) {
   if (!p) return SB2_OK;
+  cudaError_t e;
+  if (sb2::release_owned(p, &e)) return sb2::map_cuda_error(e);
   return sb2::map_cuda_error(cudaFree(p));
 }
 
