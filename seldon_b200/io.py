@@ -120,12 +120,34 @@ def write_text(path, ptr, ind, val, sym=False):
                         for a, b, x in zip(r.tolist(), c.tolist(), v.tolist())))
 
 
+_INT_FIELDS = re.compile(r"[ +\-0-9]*")
+
+
 def read_text(path):
     """ReadCoordinateMatrix (Matrix_Sparse.cxx:1885-1950): 1-based triplets
     (row, col, val) up to the first line that does not parse.  A row or
     column below 1 raises ValueError (Seldon's IOError)."""
     with open(path) as f:
-        tok = f.read().split()
+        text = f.read()
+    tok = text.split()
+    n3 = len(tok) // 3
+    # the common case, whole lines of numbers with integer row and column
+    # fields: parsed at once
+    r = None
+    if tok and len(tok) % 3 == 0 and _INT_FIELDS.fullmatch(
+            " ".join(tok[0::3]) + " " + " ".join(tok[1::3])):
+        try:
+            a = np.fromstring(text, dtype=_F8, sep=" ").reshape(-1, 3)
+        except ValueError:
+            a = None
+        if a is not None and a.shape[0] == n3 and np.all(np.abs(a[:, :2]) < 2**31):
+            r, c, v = a[:, 0].astype(np.int64), a[:, 1].astype(np.int64), a[:, 2].copy()
+    if r is not None:
+        for name, a in (("Row", r), ("Column", c)):
+            if a.size and a.min() < 1:
+                raise ValueError(f"{path}: {name} number should be greater than 0 but is equal "
+                                 f"to {int(a[np.argmax(a < 1)])}")
+        return r.astype(np.int32), c.astype(np.int32), v
     rows, cols, vals = [], [], []
     for k in range(0, len(tok) - 2, 3):
         try:
