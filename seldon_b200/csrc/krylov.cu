@@ -50,7 +50,6 @@ struct IterArgs {
   int max_iter;
   int restart;
   int init_guess_null;
-  int wcache;  // GMRES: elements of w each thread keeps in shared memory (0: none)
 };
 
 #define SB2_SHARED_DECL                     \
@@ -472,11 +471,6 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
   double* sv = Hm + ld * ld;     // s(0..m)
   double* cs = sv + ld;          // rotations_cos
   double* sn = cs + ld;          // rotations_sin
-  // During the Gram-Schmidt passes w stays in shared memory when it fits:
-  // element j of a thread's grid-stride sequence at wc[j * NT + tid].  The
-  // passes then read only the basis vectors from HBM.
-  double* wc = sn + ld;
-  const int kw = it.wcache;
   const int tid = threadIdx.x;
   const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
   const int n = A.n;
@@ -543,10 +537,6 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
       double d = block_sum<NT>(epi.acc, s_red);
       if (tid == 0) s_vals[0] = d;
       if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
-      if (kw) {
-        int j = 0;
-        for (long long e = gt; e < n; e += gs, ++j) wc[j * NT + tid] = __ldcg(v.w + e);
-      }
       // modified Gram-Schmidt: H(k,i) = (V_k, w); Add(-H(k,i), V_k, w)
       for (int k = 0; k <= i; k++) {
         const double h = s_vals[0];
@@ -557,19 +547,7 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
         double* __restrict__ wp = v.w;
         const double* __restrict__ vk = Vk;
         const double* __restrict__ vn = Vn;
-        if (kw) {
-          // the same operations on the shared-memory copy of w
-          int j = 0;
-#pragma unroll 4
-          for (long long e = gt; e < n; e += gs, ++j) {
-            double we = wc[j * NT + tid];
-            if (-h != 0.0) {
-              we = add_rn(we, mul_rn(-h, __ldcg(vk + e)));
-              wc[j * NT + tid] = we;
-            }
-            acc = add_rn(acc, vn ? mul_rn(__ldcg(vn + e), we) : mul_rn(we, we));
-          }
-        } else if (vn) {
+        if (vn) {
 #pragma unroll 4
           for (long long e = gt; e < n; e += gs) {
             double we = __ldcg(wp + e);
@@ -598,12 +576,9 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
       double hi_ip1 = sqrt(s_vals[0]);
       double* Vn = v.V + (size_t)(i + 1) * nn;
       const double inv_h = (hi_ip1 != 0.0) ? 1.0 / hi_ip1 : 1.0;
-      {
-        int j = 0;
-        for (long long e = gt; e < n; e += gs, ++j) {
-          const double we = kw ? wc[j * NT + tid] : __ldcg(v.w + e);
-          Vn[e] = (hi_ip1 != 0.0) ? mul_rn(we, inv_h) : we;
-        }
+      for (long long e = gt; e < n; e += gs) {
+        const double we = __ldcg(v.w + e);
+        Vn[e] = (hi_ip1 != 0.0) ? mul_rn(we, inv_h) : we;
       }
       // rotations (every CTA computes the same scalars)
       if (tid == 0) {
@@ -770,25 +745,6 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   }
   const int grid = coop_grid(kern, smem, A);
   if (grid < 1) return SB2_ERR_CUDA;
-  int wcache = 0;
-  if (which == kGmres && n > 0) {
-    // keep w in shared memory when its per-thread share fits without
-    // lowering the number of resident CTAs the grid was sized for
-    const int kw = (int)(((long long)n + (long long)grid * NT - 1) / ((long long)grid * NT));
-    const size_t smem_c = smem + sizeof(double) * (size_t)NT * kw;
-    int per_sm_base = 0, per_sm_c = 0;
-    if (smem_c <= 160 * 1024 &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_base, kern, NT, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(gmres_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_c) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, kern, NT, smem_c) == cudaSuccess &&
-        per_sm_c >= std::min(per_sm_base, (grid + num_sms(current_device()) - 1) /
-                                              num_sms(current_device()))) {
-      wcache = kw;
-      smem = smem_c;
-    }
-    cudaGetLastError();
-  }
   SolveScratch S;
   // history: every Finished() test; GMRES tests once per inner step and once
   // per restart
@@ -796,7 +752,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   SB2_TRY(alloc_scratch(s, n, nvec, grid, hcap, &S));
   Persist P{S.sync, S.partials, (unsigned long long)g_wait_limit_ms * 1000000ull};
   History H{S.hist, S.hist_it, hcap};
-  IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null, wcache};
+  IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null};
   OpArgs op = op_args(A, diag);
   const size_t nn = (size_t)std::max(n, 1);
   double* V = S.vec;
