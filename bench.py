@@ -590,6 +590,7 @@ def extra_ilu0(api, matgen, torch, dev, timed):
     n = ptr.size - 1
     A = api.RowSparse(n, n, ptr, ind, val)
     M = api.IlutPreconditioning()
+    M.SetFactorisationType(M.ILU_0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     M.FactorizeMatrix(A)

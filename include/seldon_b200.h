@@ -251,13 +251,15 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr,
 
 /* ILU(0) computed on the device: IlutPreconditioning with
  * SetFactorisationType(ILU_0) and the identity ordering on a RowSparse
- * matrix (GetIlu0, IlutPreconditioning.cxx:1115-1176), row by row in levels
- * of the L pattern, each row in the reference's operation order: the factor
- * is GetIlu0's bit for bit.  A's rows must be sorted by column, without
+ * matrix (GetIlu0, IlutPreconditioning.cxx:1115-1176), or with `modified`
+ * MILU_0 (GetMilu0, :1178-1243), row by row in levels of the L pattern,
+ * each row in the reference's operation order: the factor is the
+ * reference's bit for bit.  A's rows must be sorted by column, without
  * repeats, and hold their diagonal (SB2_ERR_INVALID_CSR otherwise); a zero
  * pivot gives SB2_ERR_INVALID_VALUE (the reference aborts).  The result is an
  * SB2_PRECOND_ILUT preconditioner bound to A. */
-int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out);
+int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream,
+                            sb2_precond** out);
 
 /* z = M^{-1} r (Solve) / M^{-T} r (TransSolve).  z and r must not overlap.
  * Precond_Ssor.cxx:62-90: z is zeroed, then SOR type 0 (symmetric), 2

@@ -133,7 +133,8 @@ _PROTOS = [
     ("sb2_precond_create_ilut", ctypes.c_int,
      [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int,
       ctypes.POINTER(c_void_p)]),
-    ("sb2_precond_create_ilu0", ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(c_void_p)]),
+    ("sb2_precond_create_ilu0", ctypes.c_int,
+     [c_void_p, ctypes.c_int, c_void_p, ctypes.POINTER(c_void_p)]),
     ("sb2_coo_to_csr", ctypes.c_int,
      [ctypes.c_int, c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
       ctypes.c_int, c_void_p, c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p),

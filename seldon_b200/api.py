@@ -433,6 +433,13 @@ class IlutPreconditioning(_DevicePrecond):
         super().__init__()
         self._factor = None
         self._serial = 0
+        self.type_ilu = self.ILUT  # IlutPreconditioning's default
+
+    def SetFactorisationType(self, t):
+        self.type_ilu = int(t)
+
+    def GetFactorisationType(self):
+        return self.type_ilu
 
     def SetFactor(self, fptr, find, fval, perm_row, perm_col=None, symmetric=False):
         import numpy as np
@@ -450,13 +457,19 @@ class IlutPreconditioning(_DevicePrecond):
     ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
 
     def FactorizeMatrix(self, A, stream=None):
-        """ILU(0) of a RowSparse matrix computed on the device, as
-        SetFactorisationType(ILU_0) with the identity ordering gives it
-        (GetIlu0).  Other factorizations come from Seldon through SetFactor."""
+        """ILU(0) or MILU(0) (SetFactorisationType(ILU_0 / MILU_0)) of a
+        RowSparse matrix computed on the device, as GetIlu0 / GetMilu0 do with
+        the identity ordering.  The other factorizations (ILUT, ILU_D, ILUT_K,
+        ILU_K) come from Seldon through SetFactor."""
+        if self.type_ilu not in (self.ILU_0, self.MILU_0):
+            raise NotImplementedError(
+                "the device factors ILU_0 and MILU_0; factor the others with Seldon "
+                "(IlutPreconditioning::FactorizeMatrix) and pass them to SetFactor")
         if A.symmetric:
             raise NotImplementedError("device ILU(0) takes RowSparse matrices")
         h = ctypes.c_void_p()
-        check(_L.sb2_precond_create_ilu0(A.handle, _stream(stream), ctypes.byref(h)),
+        check(_L.sb2_precond_create_ilu0(A.handle, int(self.type_ilu == self.MILU_0),
+                                         _stream(stream), ctypes.byref(h)),
               "sb2_precond_create_ilu0")
         for _, old, _s in self._cache.values():
             _L.sb2_precond_destroy(old)

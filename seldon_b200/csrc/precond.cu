@@ -257,16 +257,18 @@ struct GatherSubPacked {
 };
 
 
-// One row of GetIlu0 (IlutPreconditioning.cxx:1115-1176), in place on the
-// CSR values: rows sorted by column with the diagonal at dpos.  For each L
-// entry (stored order) tl = a_ij / u_jj (1/u_jj is already stored), then
-// a_ic -= tl * u_jc for the columns c of row j's U part that row i holds;
-// finally the diagonal is inverted.  A zero pivot is recorded in *status
-// (row + 1) and left as it is.
+// One row of GetIlu0 (IlutPreconditioning.cxx:1115-1176) or, with
+// `modified`, of GetMilu0 (:1178-1243), in place on the CSR values: rows
+// sorted by column with the diagonal at dpos.  For each L entry (stored
+// order) tl = a_ij / u_jj (1/u_jj is already stored), then a_ic -= tl * u_jc
+// for the columns c of row j's U part that row i holds; MILU(0) sums the
+// others into s and takes s off the diagonal.  Finally the diagonal is
+// inverted.  A zero pivot is recorded in *status (row + 1) and left as it is.
 struct Ilu0Row {
-  const int* ptr; const int* ind; double* val; const int* dpos; int* status;
+  const int* ptr; const int* ind; double* val; const int* dpos; int* status; int modified;
   __device__ void operator()(int i) const {
     const int d = dpos[i], e = ptr[i + 1];
+    double s = 0.0;
     for (int j = ptr[i]; j < d; j++) {
       const int jr = ind[j];
       const double tl = mul_rn(ldx(val + j), ldx(val + dpos[jr]));
@@ -275,11 +277,19 @@ struct Ilu0Row {
       for (int k = dpos[jr] + 1; k < ptr[jr + 1]; k++) {
         const int c = ind[k];
         while (q < e && ind[q] < c) q++;
-        if (q == e) break;
-        if (ind[q] == c) val[q] = __dsub_rn(ldx(val + q), mul_rn(tl, ldx(val + k)));
+        if (q < e && ind[q] == c)
+          val[q] = __dsub_rn(ldx(val + q), mul_rn(tl, ldx(val + k)));
+        else if (modified)
+          s = add_rn(s, mul_rn(tl, ldx(val + k)));
+        else if (q == e)
+          break;  // ILU(0): no column of row i is left to update
       }
     }
-    const double piv = ldx(val + d);
+    double piv = ldx(val + d);
+    if (modified) {
+      piv = __dsub_rn(piv, s);
+      val[d] = piv;
+    }
     if (piv == 0.0) {
       atomicCAS(status, 0, i + 1);
       return;
@@ -626,8 +636,8 @@ static int plan_ilut(sb2_precond* M, int n, const int* fp, const int* fi, const 
 // GetIlu0 on the device: rows in levels of their L dependencies, each row
 // factored by one thread in the reference's operation order.  The factor
 // (A's pattern, Seldon's ArrayRowSparse layout) is returned on the host.
-static int ilu0_factor(const sb2_csr* A, std::vector<int>& ptr, std::vector<int>& ind,
-                       std::vector<double>& val, cudaStream_t s) {
+static int ilu0_factor(const sb2_csr* A, int modified, std::vector<int>& ptr,
+                       std::vector<int>& ind, std::vector<double>& val, cudaStream_t s) {
   const int n = A->m;
   const CsrArrays& f = A->full;
   ptr.resize(n + 1);
@@ -667,7 +677,7 @@ static int ilu0_factor(const sb2_csr* A, std::vector<int>& ptr, std::vector<int>
   if (st == SB2_OK) st = map_cuda_error(e);
   int status = 0;
   if (st == SB2_OK)
-    st = run_levels(plan, n, Ilu0Row{f.d_ptr, f.d_ind, d_val, d_dpos, d_status}, s);
+    st = run_levels(plan, n, Ilu0Row{f.d_ptr, f.d_ind, d_val, d_dpos, d_status, modified}, s);
   if (st == SB2_OK) {
     e = cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && f.nnz)
@@ -830,13 +840,13 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int*
   return SB2_OK;
 }
 
-int sb2_precond_create_ilu0(const sb2_csr* A, void* stream, sb2_precond** out) {
+int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_precond** out) {
   if (!out || !A || A->m != A->n || A->sym) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
   const int n = A->m;
   std::vector<int> ptr, ind;
   std::vector<double> val;
-  if (n > 0) SB2_TRY(ilu0_factor(A, ptr, ind, val, (cudaStream_t)stream));
+  if (n > 0) SB2_TRY(ilu0_factor(A, modified ? 1 : 0, ptr, ind, val, (cudaStream_t)stream));
   std::vector<int> ident(std::max(n, 1));
   for (int i = 0; i < n; i++) ident[i] = i;
   if (ptr.empty()) ptr.assign(1, 0);

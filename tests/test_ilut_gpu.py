@@ -145,15 +145,19 @@ def _plain_iterations(api, M, b, which, tol, restart):
     ("conv45", lambda: matgen.convdiff3d(45)),          # one launch per level
     ("rand", lambda: _diag_dominant(3000, 0.004, 2)),
 ])
-def test_ilu0_device_factor(api, oracle, reference, name, make):
-    """ILU(0) factored on the device applies exactly like the factor Seldon's
-    GetIlu0 computes (so the two factors agree bit for bit)."""
+@pytest.mark.parametrize("milu", [False, True])
+def test_ilu0_device_factor(api, oracle, reference, name, make, milu):
+    """ILU(0) and MILU(0) factored on the device apply exactly like the
+    factor Seldon's GetIlu0 / GetMilu0 computes (so the factors agree bit for
+    bit)."""
     p, i, v = make()
     n = p.size - 1
     A = api.RowSparse(n, n, p, i, v)
     M = api.IlutPreconditioning()
+    M.SetFactorisationType(M.MILU_0 if milu else M.ILU_0)
     M.FactorizeMatrix(A)
-    factor = reference.ilut_factor(p, i, v, type_ilu=reference.ILU_0)
+    factor = reference.ilut_factor(p, i, v,
+                                   type_ilu=reference.MILU_0 if milu else reference.ILU_0)
     rng = np.random.default_rng(7)
     for trans in (False, True):
         r = rng.standard_normal(n)
@@ -165,6 +169,7 @@ def test_ilu0_rejects_unsorted_and_missing_diagonal(api):
     from seldon_b200._lib import SeldonB200Error
     ptr = np.array([0, 2, 3], dtype=np.int32)
     M = api.IlutPreconditioning()
+    M.SetFactorisationType(M.ILU_0)
     A = api.RowSparse(2, 2, ptr, np.array([1, 0, 1], dtype=np.int32), np.ones(3))
     with pytest.raises(SeldonB200Error):
         M.FactorizeMatrix(A)
@@ -179,3 +184,14 @@ def _diag_dominant(n, density, seed):
     S = sp.csr_matrix((v, i, p), shape=(n, n)) + sp.identity(n) * 4.0
     S.sort_indices()
     return S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data
+
+
+def test_device_factor_types(api):
+    """The device factors ILU_0 and MILU_0 only; the default ILUT asks for
+    Seldon's factor."""
+    p, i, v = matgen.convdiff3d(4)
+    A = api.RowSparse(64, 64, p, i, v)
+    M = api.IlutPreconditioning()
+    assert M.GetFactorisationType() == M.ILUT
+    with pytest.raises(NotImplementedError):
+        M.FactorizeMatrix(A)
