@@ -910,6 +910,31 @@ namespace Seldon
   }
 
 
+  //! Copy(ArrayRowSparse -> RowSparse) (Matrix_Conversions.cxx:3843-3857)
+  //! into a device matrix: Seldon's own flattening of the rows, which are
+  //! already sorted and merged, then one upload.
+  template <class T0, class Prop0, class Allocator0, class Prop1>
+  void Copy(const Matrix<T0, Prop0, ArrayRowSparse, Allocator0>& A,
+            Matrix<double, Prop1, RowSparse, CudaAlloc<double> >& B)
+  {
+    Matrix<double, General, RowSparse> h;
+    Copy(A, h);
+    B.Copy(h);
+  }
+
+
+  //! Copy(ArrayRowSymSparse -> RowSymSparse) (Matrix_Conversions.cxx:
+  //! 3859-3875) into a device matrix.
+  template <class T0, class Prop0, class Allocator0, class Prop1>
+  void Copy(const Matrix<T0, Prop0, ArrayRowSymSparse, Allocator0>& A,
+            Matrix<double, Prop1, RowSymSparse, CudaAlloc<double> >& B)
+  {
+    Matrix<double, Symmetric, RowSymSparse> h;
+    Copy(A, h);
+    B.Copy(h);
+  }
+
+
   //! Host triplets into a device matrix: copied to the device, then
   //! assembled there.
   template <class Prop, class Alloc1, class Alloc2, class Alloc3>

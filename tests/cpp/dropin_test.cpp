@@ -750,6 +750,48 @@ int main()
     report(text_ok, "text_files", "ReadText/WriteText match Seldon's");
   }
 
+  // ------------------------------------------------ ArrayRowSparse
+  // a matrix assembled entry by entry (AddInteraction merges repeats), then
+  // Copy to RowSparse on the host (Seldon) and into a device matrix
+  {
+    Matrix<double, General, ArrayRowSparse> Ga(60, 50);
+    Matrix<double, Symmetric, ArrayRowSymSparse> Sa(40, 40);
+    unsigned long long st = 0x243F6A8885A308D3ULL;
+    for (int k = 0; k < 900; k++)
+      {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+        const int i = int(st % 60), j = int((st >> 16) % 50);
+        const double v = double(int((st >> 32) % 1000) - 500) / 16.0;
+        Ga.AddInteraction(i, j, v);
+        const int a = int((st >> 8) % 40), b = int((st >> 24) % 40);
+        if (a <= b)
+          Sa.AddInteraction(a, b, v);
+      }
+    HostGen Gh2;
+    Copy(Ga, Gh2);
+    DevGen Gd2;
+    Copy(Ga, Gd2);
+    HostSym Sh2;
+    Copy(Sa, Sh2);
+    DevSym Sd2;
+    Copy(Sa, Sd2);
+    std::vector<int> p, i, p2, i2;
+    std::vector<double> v, v2;
+    Gd2.Download(p, i, v);
+    Sd2.Download(p2, i2, v2);
+    bool ok = Gd2.GetM() == Gh2.GetM() && Gd2.GetN() == Gh2.GetN()
+      && int(i.size()) == Gh2.GetNonZeros() && int(i2.size()) == Sh2.GetNonZeros();
+    for (int k = 0; ok && k <= Gh2.GetM(); k++)
+      ok = p[k] == Gh2.GetPtr()[k];
+    for (int k = 0; ok && k < Gh2.GetNonZeros(); k++)
+      ok = i[k] == Gh2.GetInd()[k] && v[k] == Gh2.GetData()[k];
+    for (int k = 0; ok && k <= Sh2.GetM(); k++)
+      ok = p2[k] == Sh2.GetPtr()[k];
+    for (int k = 0; ok && k < Sh2.GetNonZeros(); k++)
+      ok = i2[k] == Sh2.GetInd()[k] && v2[k] == Sh2.GetData()[k];
+    report(ok, "array_row_sparse", "Copy(ArrayRow(Sym)Sparse -> device) == Seldon's Copy");
+  }
+
   // ------------------------------------------------ Harwell-Boeing files
   {
     const std::string f1 = "dropin_ref.rua", f2 = "dropin_dev.rua", f3 = "dropin_in.rua";

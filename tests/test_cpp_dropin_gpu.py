@@ -26,7 +26,7 @@ def test_cpp_dropin(cuda, tmp_path):
                  "gmres20_jacobi", "bicgstab_identity", "cg_user_preconditioner",
                  "cg_zero_rhs", "invalid_csr_throws", "binary_files",
                  "coordinate_assembly", "text_files", "ilut_apply", "ilut_gmres",
-                 "ilut_bicgstab", "ilut_sym_apply", "ilut_cg", "harwell_boeing"):
+                 "ilut_bicgstab", "ilut_sym_apply", "ilut_cg", "harwell_boeing", "array_row_sparse"):
         assert must in names, must
     # Seldon's other Krylov drivers, its generic templates on device types
     for drv in ("bicg", "bicgstabl", "bicgcr", "cgne", "cgs", "cocg", "gcr", "lsqr", "minres",
