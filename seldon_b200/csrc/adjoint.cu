@@ -89,6 +89,7 @@ int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* strea
 
 int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const double* x,
                      double* grad_val, void* stream) {
+  SB2_TRACE("sb2_grad_pattern");
   if (!A || (A->nnz > 0 && (!lambda || !x || !grad_val))) return SB2_ERR_INVALID_VALUE;
   if (A->sym) return SB2_ERR_NOT_SUPPORTED;
   if (A->m == 0) return SB2_OK;
@@ -101,6 +102,7 @@ int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const
 
 int sb2_grad_edges(int nedges, const int* ei, const int* ej, const double* lambda,
                    const double* x, double* grad, void* stream) {
+  SB2_TRACE("sb2_grad_edges");
   if (nedges < 0 || (nedges > 0 && (!ei || !ej || !lambda || !x || !grad)))
     return SB2_ERR_INVALID_VALUE;
   if (nedges == 0) return SB2_OK;

@@ -412,6 +412,7 @@ int sb2_batch_destroy(sb2_batch* B) {
 
 int sb2_batch_solve(const sb2_batch* B, double* x, const double* b, const sb2_batch_params* prm,
                     int* d_iters, double* d_relres, sb2_batch_result* result, void* stream) {
+  SB2_TRACE("sb2_batch_solve");
   if (!B || !prm || (B->m > 0 && (!x || !b)) || x == b) return SB2_ERR_INVALID_VALUE;
   if (prm->mode < 0 || prm->mode > 1) return SB2_ERR_INVALID_VALUE;
   cudaStream_t s = (cudaStream_t)stream;

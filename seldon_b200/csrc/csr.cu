@@ -373,6 +373,7 @@ extern "C" {
 int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
                    const double* val, int symmetric_upper, int validate,
                    sb2_csr** out) {
+  SB2_TRACE("sb2_csr_create");
   if (!out || m < 0 || n < 0 || nnz < 0 || !ptr) return SB2_ERR_INVALID_VALUE;
   if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
   if (symmetric_upper && m != n) return SB2_ERR_INVALID_VALUE;

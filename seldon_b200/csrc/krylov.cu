@@ -1405,6 +1405,7 @@ int sb2_krylov_set_config(int chain_min_n) {
 int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
            const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,
            int hist_cap, void* stream) {
+  SB2_TRACE("sb2_cg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 }
@@ -1412,6 +1413,7 @@ int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
 int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                  const sb2_iter_params* params, sb2_iter_result* result, double* hist,
                  int* hist_it, int hist_cap, void* stream) {
+  SB2_TRACE("sb2_bicgstab");
   return solve_entry(kBicg, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 }
@@ -1419,6 +1421,7 @@ int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x, const double
 int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
               int* hist_it, int hist_cap, void* stream) {
+  SB2_TRACE("sb2_gmres");
   return solve_entry(kGmres, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 }

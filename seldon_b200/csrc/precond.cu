@@ -820,6 +820,7 @@ int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
 int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int* find,
                             const double* fval, const int* perm_row, const int* perm_col,
                             int symmetric, sb2_precond** out) {
+  SB2_TRACE("sb2_precond_create_ilut");
   if (!out || n < 0 || (n > 0 && (!fptr || !perm_row || (!symmetric && !perm_col))))
     return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
@@ -841,6 +842,7 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int*
 }
 
 int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_precond** out) {
+  SB2_TRACE("sb2_precond_create_ilu0");
   if (!out || !A || A->m != A->n || A->sym) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
   const int n = A->m;
@@ -875,12 +877,14 @@ int sb2_precond_destroy(sb2_precond* M) {
 }
 
 int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+  SB2_TRACE("sb2_precond_solve");
   if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, false, r, z, (cudaStream_t)stream);
 }
 
 int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+  SB2_TRACE("sb2_precond_trans_solve");
   if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, true, r, z, (cudaStream_t)stream);
@@ -888,6 +892,7 @@ int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, vo
 
 int sb2_sor(const sb2_csr* A, double* x, const double* b, double omega, int iter,
             int type_ssor, void* stream) {
+  SB2_TRACE("sb2_sor");
   if (!A || A->m != A->n || (A->m > 0 && (!x || !b)) || x == b) return SB2_ERR_INVALID_VALUE;
   sb2_precond tmp;
   tmp.A = A;

@@ -8,9 +8,24 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "seldon_b200.h"
 
 namespace sb2 {
+
+// ----------------------------------------------------------------- tracing
+
+// An NVTX range around a C entry point: a profiler's timeline shows each
+// library call by name.  NVTX v3 is header-only and costs a few nanoseconds
+// when no tool is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+#define SB2_TRACE(name) ::sb2::TraceRange sb2_trace_range_(name)
 
 // ----------------------------------------------------------------- status
 

@@ -204,11 +204,13 @@ extern "C" {
 
 int sb2_spmv(const sb2_csr* A, int trans, double alpha, const double* x,
              double beta, double* y, void* stream) {
+  SB2_TRACE("sb2_spmv");
   return spmv_common(A, trans, alpha, x, beta, y, false, (cudaStream_t)stream);
 }
 
 int sb2_mlt(const sb2_csr* A, int trans, double alpha, const double* x,
             double* y, void* stream) {
+  SB2_TRACE("sb2_mlt");
   return spmv_common(A, trans, alpha, x, 0.0, y, true, (cudaStream_t)stream);
 }
 
@@ -241,6 +243,7 @@ static int spmv_host_common(const sb2_csr* cA, int trans, double alpha,
 int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
                   const double* x_host, double beta, double* y_host,
                   void* stream) {
+  SB2_TRACE("sb2_spmv_host");
   // y is copied in too: MltAdd scales it by beta even when beta == 0.
   return spmv_host_common(A, trans, alpha, x_host, beta, y_host, false,
                           (cudaStream_t)stream);
@@ -258,6 +261,7 @@ int sb2_spmv_set_config(int algo, int threads, int stages) {
 
 int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
                  const double* x_host, double* y_host, void* stream) {
+  SB2_TRACE("sb2_mlt_host");
   return spmv_host_common(A, trans, alpha, x_host, 0.0, y_host, true,
                           (cudaStream_t)stream);
 }
@@ -270,6 +274,7 @@ int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
 // it, the product into y buffer b waits for the copy out that last read it.
 int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
                        const double* x_host, double* y_host, void* stream) {
+  SB2_TRACE("sb2_mlt_host_batch");
   if (!cA || count < 0) return SB2_ERR_INVALID_VALUE;
   sb2_csr* A = const_cast<sb2_csr*>(cA);
   const int nx = trans ? A->m : A->n, ny = trans ? A->n : A->m;
