@@ -453,8 +453,9 @@ int sb2_krylov_set_config(int chain_min_n);
  * runs Cg inside that cluster, exchanging data through distributed shared
  * memory and synchronizing with hardware cluster barriers; the arithmetic is
  * the same as the persistent kernel's.  0 turns it off (the persistent
- * kernel runs instead).  Returns the previous setting.  No counterpart in
- * the reference (a tuning knob of this engine). */
+ * kernel runs instead); 1 turns it on with up to 16 CTAs; 2, 4, 8 or 16 turn
+ * it on with at most that many.  Returns the previous setting (0 or the
+ * cap).  No counterpart in the reference (a tuning knob of this engine). */
 int sb2_krylov_set_cluster(int on);
 
 /* Device-side wait limit for the fused solvers' grid barriers, in

@@ -1049,6 +1049,7 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
 static int g_chain_min_n = 2800000;
 // Systems that fit one thread-block cluster's shared memory run CG there.
 static int g_cluster_cg = 1;
+static int g_cluster_cap = 16;  // most CTAs a cluster may take
 
 // ----------------------------------------------------------------- cluster-resident CG
 //
@@ -1246,8 +1247,9 @@ static size_t cluster_smem(int rpc, int nnz_max) {
 static int cluster_plan(const sb2_csr* A, int* ranks, int* rpc, int* nnz_max) {
   sb2_csr* M = const_cast<sb2_csr*>(A);
   std::lock_guard<std::mutex> g(M->mu);
-  if (M->cl_ranks < 0) {
+  if (M->cl_ranks < 0 || M->cl_cap != g_cluster_cap) {
     M->cl_ranks = 0;
+    M->cl_cap = g_cluster_cap;
     const int n = A->m;
     if (n >= 256 && n <= kClusterMaxRanks * 4096) {
       std::vector<int> ptr(n + 1);
@@ -1255,7 +1257,7 @@ static int cluster_plan(const sb2_csr* A, int* ranks, int* rpc, int* nnz_max) {
       int dev_smem = 0;
       cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, current_device());
       const size_t limit = (size_t)std::max(dev_smem - 1024, 0);  // static shared memory
-      for (int c = kClusterMaxRanks; c >= 2; c /= 2) {
+      for (int c = std::min(kClusterMaxRanks, g_cluster_cap); c >= 2; c /= 2) {
         const int r = (n + c - 1) / c;
         int mx = 0;
         for (int q = 0; q < c; q++) {
@@ -1390,8 +1392,15 @@ using namespace sb2;
 extern "C" {
 
 int sb2_krylov_set_cluster(int on) {
-  const int old = g_cluster_cg;
+  const int old = g_cluster_cg ? g_cluster_cap : 0;
   g_cluster_cg = on ? 1 : 0;
+  if (on >= 2) {
+    int c = 2;
+    while (c * 2 <= std::min(on, kClusterMaxRanks)) c *= 2;
+    g_cluster_cap = c;
+  } else if (on == 1) {
+    g_cluster_cap = kClusterMaxRanks;
+  }
   return old;
 }
 

@@ -120,7 +120,7 @@ struct sb2_csr {
   float* d_diag32 = nullptr; // FP32 copy of d_diag (lazy)
   std::mutex mu;             // guards the lazy members
   // cluster-resident CG plan (lazy; cl_ranks < 0: not planned yet, 0: no fit)
-  int cl_ranks = -1, cl_rpc = 0, cl_nnz_max = 0;
+  int cl_ranks = -1, cl_rpc = 0, cl_nnz_max = 0, cl_cap = 0;
   // staging vectors of the host-buffer entry points (lazy, reused)
   double* d_hx = nullptr;
   double* d_hy = nullptr;
