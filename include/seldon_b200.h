@@ -249,6 +249,48 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr,
                             const int* perm_row, const int* perm_col,
                             int symmetric, sb2_precond** out);
 
+/* ILUT factorization on the host, as IlutPreconditioning::FactorizeMatrix
+ * computes it for a RowSparse matrix with the unsymmetric algorithm
+ * (IlutPreconditioning.cxx:266-323, GetIlut :503-878): the same factor and
+ * permutations, bit for bit, for sb2_precond_create_ilut.  Fields follow the
+ * reference's setters and defaults (IlutPreconditioning.cxx:27-40):
+ *   type             SB2_ILUT (default), SB2_ILU_D or SB2_ILUT_K
+ *   fill_level       lfil, the entries kept per part (default 1000000)
+ *   additional_fill  ILUT_K: lfil = row length + this (default 1000000)
+ *   mbloc            pivots are sought within blocks of mbloc columns
+ *                    (default 1000000)
+ *   alpha            ILU_D: weight of the dropped sum added to the pivot
+ *                    (default 1)
+ *   droptol          dropping threshold (default 0.01)
+ *   permtol          pivoting threshold (default 0.1) */
+#define SB2_ILUT 0
+#define SB2_ILU_D 1
+#define SB2_ILUT_K 2
+typedef struct {
+  int type;
+  int fill_level;
+  int additional_fill;
+  int mbloc;
+  double alpha;
+  double droptol;
+  double permtol;
+} sb2_ilut_params;
+
+/* The factor of a RowSparse matrix given by HOST arrays (ptr[n+1], ind, val;
+ * no repeated column in a row: SB2_ERR_NOT_SUPPORTED) and an ordering perm
+ * (FactorizeMatrix's perm; the identity for none).  A row whose entries are
+ * all zero gives SB2_ERR_INVALID_VALUE (the reference aborts).  The result
+ * is read with sb2_ilut_size / sb2_ilut_arrays (fptr[n+1], find[nnz],
+ * fval[nnz], perm_row[n], perm_col[n]) and released with sb2_ilut_destroy. */
+typedef struct sb2_ilut sb2_ilut;
+int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val,
+                    const int* perm, const sb2_ilut_params* params,
+                    sb2_ilut** out);
+int sb2_ilut_size(const sb2_ilut* f, int* n, int* nnz);
+int sb2_ilut_arrays(const sb2_ilut* f, int* fptr, int* find, double* fval,
+                    int* perm_row, int* perm_col);
+int sb2_ilut_destroy(sb2_ilut* f);
+
 /* ILU(0) computed on the device: IlutPreconditioning with
  * SetFactorisationType(ILU_0) and the identity ordering on a RowSparse
  * matrix (GetIlu0, IlutPreconditioning.cxx:1115-1176), or with `modified`

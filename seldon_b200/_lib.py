@@ -32,6 +32,20 @@ c_double_p = ctypes.POINTER(ctypes.c_double)
 c_void_p = ctypes.c_void_p
 
 
+class IlutParams(ctypes.Structure):
+    """sb2_ilut_params: IlutPreconditioning's settings."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("fill_level", ctypes.c_int),
+        ("additional_fill", ctypes.c_int),
+        ("mbloc", ctypes.c_int),
+        ("alpha", ctypes.c_double),
+        ("droptol", ctypes.c_double),
+        ("permtol", ctypes.c_double),
+    ]
+
+
 class IterParams(ctypes.Structure):
     """sb2_iter_params: Seldon's Iteration<double> settings."""
 
@@ -133,6 +147,12 @@ _PROTOS = [
     ("sb2_precond_create_ilut", ctypes.c_int,
      [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int,
       ctypes.POINTER(c_void_p)]),
+    ("sb2_ilut_factor", ctypes.c_int,
+     [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IlutParams),
+      ctypes.POINTER(c_void_p)]),
+    ("sb2_ilut_size", ctypes.c_int, [c_void_p, c_int_p, c_int_p]),
+    ("sb2_ilut_arrays", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("sb2_ilut_destroy", ctypes.c_int, [c_void_p]),
     ("sb2_precond_create_ilu0", ctypes.c_int,
      [c_void_p, ctypes.c_int, c_void_p, ctypes.POINTER(c_void_p)]),
     ("sb2_coo_to_csr", ctypes.c_int,

@@ -433,13 +433,71 @@ class IlutPreconditioning(_DevicePrecond):
         super().__init__()
         self._factor = None
         self._serial = 0
-        self.type_ilu = self.ILUT  # IlutPreconditioning's default
+        # IlutPreconditioning's defaults (IlutPreconditioning.cxx:27-40)
+        self.type_ilu = self.ILUT
+        self.fill_level = 1000000
+        self.additional_fill = 1000000
+        self.mbloc = 1000000
+        self.alpha = 1.0
+        self.droptol = 0.01
+        self.permtol = 0.1
 
     def SetFactorisationType(self, t):
         self.type_ilu = int(t)
 
     def GetFactorisationType(self):
         return self.type_ilu
+
+    def SetFillLevel(self, k):
+        self.fill_level = int(k)
+
+    def SetAdditionalFillNumber(self, k):
+        self.additional_fill = int(k)
+
+    def SetPivotBlockInteger(self, k):
+        self.mbloc = int(k)
+
+    def SetDiagonalCoefficient(self, a):
+        self.alpha = float(a)
+
+    def SetDroppingThreshold(self, t):
+        self.droptol = float(t)
+
+    def SetPivotThreshold(self, t):
+        self.permtol = float(t)
+
+    def factor_host(self, n, ptr, ind, val, perm=None):
+        """The ILUT / ILU_D / ILUT_K factor of host CSR arrays, computed on
+        the host in the reference's order (sb2_ilut_factor): (fptr, find,
+        fval, perm_row, perm_col)."""
+        import numpy as np
+        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+        ind = np.ascontiguousarray(ind, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        perm = (np.arange(n, dtype=np.int32) if perm is None
+                else np.ascontiguousarray(perm, dtype=np.int32))
+        types = {self.ILUT: 0, self.ILU_D: 1, self.ILUT_K: 2}
+        if self.type_ilu not in types:
+            raise NotImplementedError("host factorization of ILUT, ILU_D and ILUT_K")
+        prm = _lib.IlutParams(types[self.type_ilu], self.fill_level, self.additional_fill,
+                              self.mbloc, self.alpha, self.droptol, self.permtol)
+        h = ctypes.c_void_p()
+        check(_L.sb2_ilut_factor(int(n), _np_ptr(ptr), _np_ptr(ind), _np_ptr(val),
+                                 _np_ptr(perm), ctypes.byref(prm), ctypes.byref(h)),
+              "sb2_ilut_factor")
+        try:
+            nn, nz = ctypes.c_int(), ctypes.c_int()
+            _L.sb2_ilut_size(h, ctypes.byref(nn), ctypes.byref(nz))
+            fptr = np.zeros(n + 1, dtype=np.int32)
+            find = np.zeros(max(nz.value, 1), dtype=np.int32)
+            fval = np.zeros(max(nz.value, 1))
+            prow = np.zeros(max(n, 1), dtype=np.int32)
+            pcol = np.zeros(max(n, 1), dtype=np.int32)
+            _L.sb2_ilut_arrays(h, _np_ptr(fptr), _np_ptr(find), _np_ptr(fval), _np_ptr(prow),
+                               _np_ptr(pcol))
+        finally:
+            _L.sb2_ilut_destroy(h)
+        return fptr, find[:nz.value], fval[:nz.value], prow[:n], pcol[:n]
 
     def SetFactor(self, fptr, find, fval, perm_row, perm_col=None, symmetric=False):
         import numpy as np
@@ -456,17 +514,23 @@ class IlutPreconditioning(_DevicePrecond):
 
     ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
 
-    def FactorizeMatrix(self, A, stream=None):
-        """ILU(0) or MILU(0) (SetFactorisationType(ILU_0 / MILU_0)) of a
-        RowSparse matrix computed on the device, as GetIlu0 / GetMilu0 do with
-        the identity ordering.  The other factorizations (ILUT, ILU_D, ILUT_K,
-        ILU_K) come from Seldon through SetFactor."""
+    def FactorizeMatrix(self, A, perm=None, stream=None):
+        """FactorizeMatrix of a RowSparse matrix with the unsymmetric
+        algorithm.  ILU_0 / MILU_0 (identity ordering) are factored on the
+        device, as GetIlu0 / GetMilu0 do; ILUT, ILU_D and ILUT_K on the host
+        in GetIlut's order (`perm`: the ordering, identity by default).  ILU_K
+        and the symmetric algorithm come from Seldon through SetFactor."""
+        if A.symmetric:
+            raise NotImplementedError("FactorizeMatrix here takes RowSparse matrices")
+        if self.type_ilu in (self.ILUT, self.ILU_D, self.ILUT_K):
+            self.SetFactor(*self.factor_host(A.m, *A.download(), perm=perm))
+            return
         if self.type_ilu not in (self.ILU_0, self.MILU_0):
             raise NotImplementedError(
-                "the device factors ILU_0 and MILU_0; factor the others with Seldon "
-                "(IlutPreconditioning::FactorizeMatrix) and pass them to SetFactor")
-        if A.symmetric:
-            raise NotImplementedError("device ILU(0) takes RowSparse matrices")
+                "ILU_K is not factored here: factor it with Seldon "
+                "(IlutPreconditioning::FactorizeMatrix) and pass it to SetFactor")
+        if perm is not None:
+            raise NotImplementedError("the device ILU(0) uses the identity ordering")
         h = ctypes.c_void_p()
         check(_L.sb2_precond_create_ilu0(A.handle, int(self.type_ilu == self.MILU_0),
                                          _stream(stream), ctypes.byref(h)),

@@ -1,0 +1,78 @@
+"""The host ILUT factorization (sb2_ilut_factor) against Seldon's own
+IlutPreconditioning::FactorizeMatrix: the factor's rows, in stored order,
+and both permutations, bit for bit.  Host code only: no GPU needed."""
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+
+
+@pytest.fixture(scope="module")
+def api():
+    from seldon_b200 import api as a
+    return a
+
+
+def _diag_dominant(n, density, seed, shift=4.0):
+    import scipy.sparse as sp
+    p, i, v = matgen.random_csr(n, n, density, seed=seed)
+    S = sp.csr_matrix((v, i, p), shape=(n, n)) + sp.identity(n) * shift
+    S.sort_indices()
+    return S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data
+
+
+def _ours(api, p, i, v, perm, type_ilu, **kw):
+    M = api.IlutPreconditioning()
+    M.SetFactorisationType(type_ilu)
+    for key, set_ in (("fill_level", M.SetFillLevel), ("additional_fill", M.SetAdditionalFillNumber),
+                      ("mbloc", M.SetPivotBlockInteger), ("alpha", M.SetDiagonalCoefficient),
+                      ("droptol", M.SetDroppingThreshold), ("permtol", M.SetPivotThreshold)):
+        if key in kw:
+            set_(kw[key])
+    return M.factor_host(p.size - 1, p, i, v, perm=perm)
+
+
+CASES = [
+    # (name, matrix, factorization type, options)
+    ("conv6_ilut", lambda: matgen.convdiff3d(6), 0, dict(droptol=1e-3)),
+    ("conv6_ilut_lfil", lambda: matgen.convdiff3d(6), 0, dict(droptol=1e-4, fill_level=3)),
+    ("conv6_pivot", lambda: matgen.convdiff3d(6), 0, dict(droptol=1e-4, permtol=0.5)),
+    ("conv6_pivot_blocks", lambda: matgen.convdiff3d(6), 0,
+     dict(droptol=1e-4, permtol=0.9, mbloc=17)),
+    ("conv6_ilu_d", lambda: matgen.convdiff3d(6), 1, dict(droptol=1e-2, alpha=0.7)),
+    ("conv6_ilut_k", lambda: matgen.convdiff3d(6), 2, dict(droptol=1e-3, additional_fill=2)),
+    ("rand_ilut", lambda: _diag_dominant(400, 0.02, 3), 0, dict(droptol=1e-3)),
+    ("rand_pivot", lambda: _diag_dominant(400, 0.02, 5, shift=0.5), 0,
+     dict(droptol=1e-4, permtol=0.3, fill_level=8)),
+    ("rand_pivot_blocks", lambda: _diag_dominant(400, 0.02, 5, shift=0.5), 0,
+     dict(droptol=1e-4, permtol=0.3, fill_level=8, mbloc=13)),
+    ("rand_ilu_d", lambda: _diag_dominant(300, 0.03, 7), 1, dict(droptol=0.05)),
+    ("lap_ilut_k", lambda: matgen.lap2d(20), 2, dict(droptol=1e-2, additional_fill=1)),
+]
+
+
+@pytest.mark.parametrize("name,make,type_ilu,kw", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("ordered", [False, True])
+def test_factor_matches_reference(api, reference, name, make, type_ilu, kw, ordered):
+    p, i, v = make()
+    n = p.size - 1
+    perm = np.random.default_rng(n).permutation(n) if ordered else None
+    ours = _ours(api, p, i, v, perm, type_ilu, **kw)
+    theirs = reference.ilut_factor(p, i, v, perm=perm, type_ilu=type_ilu, **kw)
+    for name_, a, b in zip(("fptr", "find", "fval", "perm_row", "perm_col"), ours, theirs):
+        assert a.shape == b.shape, name_
+        assert np.array_equal(a, b), name_
+
+
+def test_rejections(api):
+    from seldon_b200._lib import SeldonB200Error
+    p = np.array([0, 1, 2], dtype=np.int32)
+    i = np.array([0, 1], dtype=np.int32)
+    M = api.IlutPreconditioning()
+    with pytest.raises(SeldonB200Error):  # a row of zeros
+        M.factor_host(2, p, i, np.array([1.0, 0.0]))
+    with pytest.raises(SeldonB200Error):  # not a permutation
+        M.factor_host(2, p, i, np.ones(2), perm=np.array([0, 0]))
+    with pytest.raises(SeldonB200Error):  # a repeated column
+        M.factor_host(1, np.array([0, 2], dtype=np.int32), np.array([0, 0], dtype=np.int32),
+                      np.ones(2))

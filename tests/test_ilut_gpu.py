@@ -186,12 +186,22 @@ def _diag_dominant(n, density, seed):
     return S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data
 
 
-def test_device_factor_types(api):
-    """The device factors ILU_0 and MILU_0 only; the default ILUT asks for
-    Seldon's factor."""
-    p, i, v = matgen.convdiff3d(4)
-    A = api.RowSparse(64, 64, p, i, v)
+def test_factor_types(api, oracle, reference):
+    """ILUT (the default) is factored on the host in GetIlut's order and
+    applied on the device like Seldon's; ILU_K asks for Seldon's factor."""
+    p, i, v = matgen.convdiff3d(12)
+    n = p.size - 1
+    A = api.RowSparse(n, n, p, i, v)
     M = api.IlutPreconditioning()
     assert M.GetFactorisationType() == M.ILUT
+    M.SetDroppingThreshold(1e-3)
+    perm = np.random.default_rng(2).permutation(n)
+    M.FactorizeMatrix(A, perm=perm)
+    factor = reference.ilut_factor(p, i, v, perm=perm, droptol=1e-3)
+    r = np.random.default_rng(4).standard_normal(n)
+    for trans in (False, True):
+        assert np.array_equal(_apply(api, M, A, r, trans),
+                              oracle.ilut_solve(factor, r, trans=trans))
+    M.SetFactorisationType(M.ILU_K)
     with pytest.raises(NotImplementedError):
         M.FactorizeMatrix(A)
