@@ -286,6 +286,14 @@ typedef struct sb2_ilut sb2_ilut;
 int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val,
                     const int* perm, const sb2_ilut_params* params,
                     sb2_ilut** out);
+/* The symmetric algorithm (SetSymmetricAlgorithm; FactorizeSymMatrix,
+ * IlutPreconditioning.cxx:216-263, GetIlut of SymmetricIlutPreconditioning.cxx:
+ * 27-346) for a RowSymSparse matrix given by its upper triangle: row i of
+ * the factor holds 1/D(i) first, then row i of L^T.  perm_col repeats
+ * perm_row. */
+int sb2_ilut_factor_sym(int n, const int* ptr, const int* ind,
+                        const double* val, const int* perm,
+                        const sb2_ilut_params* params, sb2_ilut** out);
 int sb2_ilut_size(const sb2_ilut* f, int* n, int* nnz);
 int sb2_ilut_arrays(const sb2_ilut* f, int* fptr, int* find, double* fval,
                     int* perm_row, int* perm_col);

@@ -150,6 +150,9 @@ _PROTOS = [
     ("sb2_ilut_factor", ctypes.c_int,
      [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IlutParams),
       ctypes.POINTER(c_void_p)]),
+    ("sb2_ilut_factor_sym", ctypes.c_int,
+     [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IlutParams),
+      ctypes.POINTER(c_void_p)]),
     ("sb2_ilut_size", ctypes.c_int, [c_void_p, c_int_p, c_int_p]),
     ("sb2_ilut_arrays", ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sb2_ilut_destroy", ctypes.c_int, [c_void_p]),

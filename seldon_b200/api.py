@@ -441,6 +441,13 @@ class IlutPreconditioning(_DevicePrecond):
         self.alpha = 1.0
         self.droptol = 0.01
         self.permtol = 0.1
+        self.symmetric_algorithm = False
+
+    def SetSymmetricAlgorithm(self):
+        self.symmetric_algorithm = True
+
+    def SetUnsymmetricAlgorithm(self):
+        self.symmetric_algorithm = False
 
     def SetFactorisationType(self, t):
         self.type_ilu = int(t)
@@ -466,9 +473,10 @@ class IlutPreconditioning(_DevicePrecond):
     def SetPivotThreshold(self, t):
         self.permtol = float(t)
 
-    def factor_host(self, n, ptr, ind, val, perm=None):
+    def factor_host(self, n, ptr, ind, val, perm=None, symmetric=False):
         """The ILUT / ILU_D / ILUT_K factor of host CSR arrays, computed on
-        the host in the reference's order (sb2_ilut_factor): (fptr, find,
+        the host in the reference's order (sb2_ilut_factor, or with
+        `symmetric` sb2_ilut_factor_sym on the upper triangle): (fptr, find,
         fval, perm_row, perm_col)."""
         import numpy as np
         ptr = np.ascontiguousarray(ptr, dtype=np.int32)
@@ -482,9 +490,9 @@ class IlutPreconditioning(_DevicePrecond):
         prm = _lib.IlutParams(types[self.type_ilu], self.fill_level, self.additional_fill,
                               self.mbloc, self.alpha, self.droptol, self.permtol)
         h = ctypes.c_void_p()
-        check(_L.sb2_ilut_factor(int(n), _np_ptr(ptr), _np_ptr(ind), _np_ptr(val),
-                                 _np_ptr(perm), ctypes.byref(prm), ctypes.byref(h)),
-              "sb2_ilut_factor")
+        fn = _L.sb2_ilut_factor_sym if symmetric else _L.sb2_ilut_factor
+        check(fn(int(n), _np_ptr(ptr), _np_ptr(ind), _np_ptr(val), _np_ptr(perm),
+                 ctypes.byref(prm), ctypes.byref(h)), "sb2_ilut_factor")
         try:
             nn, nz = ctypes.c_int(), ctypes.c_int()
             _L.sb2_ilut_size(h, ctypes.byref(nn), ctypes.byref(nz))
@@ -520,11 +528,18 @@ class IlutPreconditioning(_DevicePrecond):
         device, as GetIlu0 / GetMilu0 do; ILUT, ILU_D and ILUT_K on the host
         in GetIlut's order (`perm`: the ordering, identity by default).  ILU_K
         and the symmetric algorithm come from Seldon through SetFactor."""
-        if A.symmetric:
-            raise NotImplementedError("FactorizeMatrix here takes RowSparse matrices")
+        if A.symmetric != self.symmetric_algorithm:
+            # the reference factors symmetric storage with the symmetric
+            # algorithm only (its other path does not compile) and aborts on
+            # the symmetric algorithm with general storage
+            raise NotImplementedError(
+                "RowSymSparse takes SetSymmetricAlgorithm(), RowSparse the unsymmetric one")
         if self.type_ilu in (self.ILUT, self.ILU_D, self.ILUT_K):
-            self.SetFactor(*self.factor_host(A.m, *A.download(), perm=perm))
+            f = self.factor_host(A.m, *A.download(), perm=perm, symmetric=A.symmetric)
+            self.SetFactor(*f, symmetric=A.symmetric)
             return
+        if A.symmetric:
+            raise NotImplementedError("the reference has no symmetric ILU(0) or ILU(k) here")
         if self.type_ilu not in (self.ILU_0, self.MILU_0):
             raise NotImplementedError(
                 "ILU_K is not factored here: factor it with Seldon "

@@ -231,6 +231,200 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
   return SB2_OK;
 }
 
+// The symmetric algorithm (SymmetricIlutPreconditioning.cxx:27-346): B holds
+// the full rows of the symmetric matrix, sorted by column; row i of the
+// factor keeps 1/D(i) first and then its U part (no pivoting, no L part
+// kept); at the end every U entry is scaled by its row's 1/D.
+int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
+               std::vector<Row>& F) {
+  const bool variable_fill = (p.type == SB2_ILUT_K);
+  const bool standard_dropping = (p.type == SB2_ILU_D);
+  int lfil = p.fill_level;
+  if (lfil < 0) return SB2_ERR_INVALID_VALUE;
+  F.assign(n, Row());
+  std::vector<double> w(n, 0.0);
+  std::vector<int> wi(n, -1), where(n, -1);
+  for (int i = 0; i < n; i++) {
+    const Row& a = B[i];
+    const int size_row = (int)a.idx.size();
+    double tnorm = 0.0;
+    for (int k = 0; k < size_row; k++) tnorm += std::fabs(a.val[k]);
+    if (tnorm == 0.0) return SB2_ERR_INVALID_VALUE;  // structurally singular row
+    tnorm /= (double)size_row;
+    if (variable_fill) lfil = size_row + p.additional_fill;
+    double dropsum = 0.0;
+    int nl = 0, nu = 1;
+    wi[i] = i;
+    w[i] = 0.0;
+    where[i] = i;
+    for (int k = 0; k < size_row; k++) {
+      const int c = a.idx[k];
+      const double t = a.val[k];
+      if (c < i) {
+        wi[nl] = c;
+        w[nl] = t;
+        where[c] = nl;
+        ++nl;
+      } else if (c == i) {
+        w[i] = t;
+      } else {
+        const int at = i + nu;
+        wi[at] = c;
+        w[at] = t;
+        where[c] = at;
+        nu++;
+      }
+    }
+    int kept = 0;
+    for (int jc = 0; jc < nl; jc++) {
+      int jrow = wi[jc], kmin = jc;
+      for (int j = jc + 1; j < nl; j++)
+        if (wi[j] < jrow) {
+          jrow = wi[j];
+          kmin = j;
+        }
+      if (kmin != jc) {
+        const int other = wi[jc];
+        wi[jc] = wi[kmin];
+        wi[kmin] = other;
+        where[jrow] = jc;
+        where[other] = kmin;
+        std::swap(w[jc], w[kmin]);
+      }
+      where[jrow] = -1;
+      bool dropped = false;
+      if (standard_dropping && std::fabs(w[jc]) <= p.droptol * tnorm) {
+        dropsum += w[jc];
+        dropped = true;
+      }
+      double fact = 0.0;
+      if (!dropped) {
+        fact = w[jc] * F[jrow].val[0];
+        if (!standard_dropping && std::fabs(fact) <= p.droptol) dropped = true;
+      }
+      if (!dropped) {
+        const Row& u = F[jrow];
+        for (int k = 1; k < (int)u.idx.size(); k++) {
+          const double s = fact * u.val[k];
+          const int c = u.idx[k];
+          const int at = where[c];
+          if (c >= i) {
+            if (at == -1) {
+              const int slot = i + nu;
+              wi[slot] = c;
+              where[c] = slot;
+              w[slot] = -s;
+              ++nu;
+            } else {
+              w[at] -= s;
+            }
+          } else {
+            if (at == -1) {
+              wi[nl] = c;
+              where[c] = nl;
+              w[nl] = -s;
+              ++nl;
+            } else {
+              w[at] -= s;
+            }
+          }
+        }
+        w[kept] = fact;
+        wi[kept] = jrow;
+        ++kept;
+      }
+    }
+    for (int k = 0; k < nu; k++) where[wi[i + k]] = -1;
+    int lu = 0;
+    for (int k = 1; k <= nu - 1; k++) {
+      if (std::fabs(w[i + k]) > p.droptol * tnorm) {
+        ++lu;
+        w[i + lu] = w[i + k];
+        wi[i + lu] = wi[i + k];
+      } else {
+        dropsum += w[i + k];
+      }
+    }
+    if (!standard_dropping) {
+      const int nup = lu + 1;
+      lu = std::min(nup, lfil);
+      quick_split(w, wi, i + 1, i + nup, i + lu + 1);
+    } else {
+      lu++;
+    }
+    Row& f = F[i];
+    f.idx.assign(1, i);  // 1/D(i); the reference leaves this index unset
+    f.val.assign(1, 0.0);
+    for (int k = i + 1; k <= i + lu - 1; k++) {
+      f.idx.push_back(wi[k]);
+      f.val.push_back(w[k]);
+    }
+    if (standard_dropping) w[i] += p.alpha * dropsum;
+    if (w[i] == 0.0) w[i] = (p.droptol + 1e-4) * tnorm;
+    f.val[0] = 1.0 / w[i];
+  }
+  for (int i = 0; i < n; i++)
+    for (size_t j = 1; j < F[i].val.size(); j++) F[i].val[j] *= F[i].val[0];
+  return SB2_OK;
+}
+
+int check_params(const sb2_ilut_params* params) {
+  if (!params) return SB2_ERR_INVALID_VALUE;
+  if (params->type != SB2_ILUT && params->type != SB2_ILU_D && params->type != SB2_ILUT_K)
+    return SB2_ERR_NOT_SUPPORTED;
+  if (params->mbloc < 1) return SB2_ERR_INVALID_VALUE;
+  return SB2_OK;
+}
+
+int check_csr_perm(int n, const int* ptr, const int* ind, const double* val, const int* perm,
+                   std::vector<int>& inv) {
+  if (n < 0 || (n > 0 && (!ptr || !perm))) return SB2_ERR_INVALID_VALUE;
+  if (ptr && ptr[0] != 0) return SB2_ERR_INVALID_CSR;
+  for (int i = 0; i < n; i++)
+    if (ptr[i + 1] < ptr[i]) return SB2_ERR_INVALID_CSR;
+  if (n > 0 && ptr[n] > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
+  for (int i = 0; n > 0 && i < ptr[n]; i++)
+    if (ind[i] < 0 || ind[i] >= n) return SB2_ERR_INVALID_CSR;
+  // perm must be a permutation; inv(perm(i)) = i
+  inv.assign(n, -1);
+  for (int i = 0; i < n; i++) {
+    if (perm[i] < 0 || perm[i] >= n || inv[perm[i]] != -1) return SB2_ERR_INVALID_VALUE;
+    inv[perm[i]] = i;
+  }
+  return SB2_OK;
+}
+
+sb2_ilut* flatten(int n, const std::vector<Row>& F) {
+  sb2_ilut* f = new sb2_ilut();
+  f->n = n;
+  f->fptr.assign(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    f->find.insert(f->find.end(), F[i].idx.begin(), F[i].idx.end());
+    f->fval.insert(f->fval.end(), F[i].val.begin(), F[i].val.end());
+    f->fptr[i + 1] = (int)f->find.size();
+  }
+  return f;
+}
+
+// Rows sorted by column, a repeated column refused.
+int sort_rows(std::vector<std::vector<std::pair<int, double>>>& rows, std::vector<Row>& out) {
+  out.assign(rows.size(), Row());
+  for (size_t i = 0; i < rows.size(); i++) {
+    auto& e = rows[i];
+    std::sort(e.begin(), e.end(),
+              [](const std::pair<int, double>& x, const std::pair<int, double>& y) {
+                return x.first < y.first;
+              });
+    for (size_t k = 1; k < e.size(); k++)
+      if (e[k].first == e[k - 1].first) return SB2_ERR_NOT_SUPPORTED;
+    for (const auto& q : e) {
+      out[i].idx.push_back(q.first);
+      out[i].val.push_back(q.second);
+    }
+  }
+  return SB2_OK;
+}
+
 }  // namespace
 }  // namespace sb2
 
@@ -241,60 +435,60 @@ extern "C" {
 int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val, const int* perm,
                     const sb2_ilut_params* params, sb2_ilut** out) {
   SB2_TRACE("sb2_ilut_factor");
-  if (!out || !params || n < 0 || (n > 0 && (!ptr || !perm))) return SB2_ERR_INVALID_VALUE;
+  if (!out) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
-  const sb2_ilut_params& p = *params;
-  if (p.type != SB2_ILUT && p.type != SB2_ILU_D && p.type != SB2_ILUT_K)
-    return SB2_ERR_NOT_SUPPORTED;
-  if (p.mbloc < 1) return SB2_ERR_INVALID_VALUE;
-  if (ptr && ptr[0] != 0) return SB2_ERR_INVALID_CSR;
-  for (int i = 0; i < n; i++)
-    if (ptr[i + 1] < ptr[i]) return SB2_ERR_INVALID_CSR;
-  if (n > 0 && ptr[n] > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
-  // perm must be a permutation; inv(perm(i)) = i
-  std::vector<int> inv(n, -1);
-  for (int i = 0; i < n; i++) {
-    if (perm[i] < 0 || perm[i] >= n || inv[perm[i]] != -1) return SB2_ERR_INVALID_VALUE;
-    inv[perm[i]] = i;
-  }
+  SB2_TRY(check_params(params));
+  std::vector<int> inv;
+  SB2_TRY(check_csr_perm(n, ptr, ind, val, perm, inv));
   // rows and columns permuted, each row sorted by its new columns
   // (ApplyInversePermutation, Permutation_ScalingMatrix.cxx:215-256, on the
-  // ArrayRowSparse copy); a repeated column is not supported
-  std::vector<Row> A0(n);
-  for (int i = 0; i < n; i++) {
-    Row& r = A0[perm[i]];
-    std::vector<std::pair<int, double>> e;
-    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
-      if (ind[k] < 0 || ind[k] >= n) return SB2_ERR_INVALID_CSR;
-      e.emplace_back(perm[ind[k]], val[k]);
-    }
-    std::sort(e.begin(), e.end(),
-              [](const std::pair<int, double>& x, const std::pair<int, double>& y) {
-                return x.first < y.first;
-              });
-    for (size_t k = 1; k < e.size(); k++)
-      if (e[k].first == e[k - 1].first) return SB2_ERR_NOT_SUPPORTED;
-    for (const auto& q : e) {
-      r.idx.push_back(q.first);
-      r.val.push_back(q.second);
-    }
-  }
+  // ArrayRowSparse copy)
+  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  for (int i = 0; i < n; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) rows[perm[i]].emplace_back(perm[ind[k]], val[k]);
+  std::vector<Row> A0;
+  SB2_TRY(sort_rows(rows, A0));
   std::vector<Row> F;
   std::vector<int> iperm, rperm;
-  SB2_TRY(factor(n, A0, p, F, iperm, rperm));
-  sb2_ilut* f = new sb2_ilut();
-  f->n = n;
-  f->fptr.assign(n + 1, 0);
-  for (int i = 0; i < n; i++) {
-    f->find.insert(f->find.end(), F[i].idx.begin(), F[i].idx.end());
-    f->fval.insert(f->fval.end(), F[i].val.begin(), F[i].val.end());
-    f->fptr[i + 1] = (int)f->find.size();
-  }
+  SB2_TRY(factor(n, A0, *params, F, iperm, rperm));
+  sb2_ilut* f = flatten(n, F);
   // permutation_col(i) = inv(iperm(i)), permutation_row = perm
   // (IlutPreconditioning.cxx:315-322)
   f->perm_row.assign(perm, perm + n);
   f->perm_col.resize(n);
   for (int i = 0; i < n; i++) f->perm_col[i] = inv[iperm[i]];
+  *out = f;
+  return SB2_OK;
+}
+
+int sb2_ilut_factor_sym(int n, const int* ptr, const int* ind, const double* val,
+                        const int* perm, const sb2_ilut_params* params, sb2_ilut** out) {
+  SB2_TRACE("sb2_ilut_factor_sym");
+  if (!out) return SB2_ERR_INVALID_VALUE;
+  *out = nullptr;
+  SB2_TRY(check_params(params));
+  std::vector<int> inv;
+  SB2_TRY(check_csr_perm(n, ptr, ind, val, perm, inv));
+  // the upper triangle permuted, each entry kept as (min, max)
+  // (Permutation_ScalingMatrix.cxx:465-525), then both triangles of every
+  // row sorted by column (Copy to ArrayRowSparse, Matrix_Conversions.cxx:
+  // 4155-4200)
+  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  for (int i = 0; i < n; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+      if (ind[k] < i) return SB2_ERR_INVALID_CSR;  // upper triangle only
+      int r = perm[i], c = perm[ind[k]];
+      if (c < r) std::swap(r, c);
+      rows[r].emplace_back(c, val[k]);
+      if (c != r) rows[c].emplace_back(r, val[k]);
+    }
+  std::vector<Row> B;
+  SB2_TRY(sort_rows(rows, B));
+  std::vector<Row> F;
+  SB2_TRY(factor_sym(n, B, *params, F));
+  sb2_ilut* f = flatten(n, F);
+  f->perm_row.assign(perm, perm + n);
+  f->perm_col = f->perm_row;
   *out = f;
   return SB2_OK;
 }

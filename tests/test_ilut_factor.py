@@ -21,7 +21,7 @@ def _diag_dominant(n, density, seed, shift=4.0):
     return S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data
 
 
-def _ours(api, p, i, v, perm, type_ilu, **kw):
+def _ours(api, p, i, v, perm, type_ilu, sym=False, **kw):
     M = api.IlutPreconditioning()
     M.SetFactorisationType(type_ilu)
     for key, set_ in (("fill_level", M.SetFillLevel), ("additional_fill", M.SetAdditionalFillNumber),
@@ -29,7 +29,7 @@ def _ours(api, p, i, v, perm, type_ilu, **kw):
                       ("droptol", M.SetDroppingThreshold), ("permtol", M.SetPivotThreshold)):
         if key in kw:
             set_(kw[key])
-    return M.factor_host(p.size - 1, p, i, v, perm=perm)
+    return M.factor_host(p.size - 1, p, i, v, perm=perm, symmetric=sym)
 
 
 CASES = [
@@ -76,3 +76,36 @@ def test_rejections(api):
     with pytest.raises(SeldonB200Error):  # a repeated column
         M.factor_host(1, np.array([0, 2], dtype=np.int32), np.array([0, 0], dtype=np.int32),
                       np.ones(2))
+
+
+SYM_CASES = [
+    ("lap_ilut", lambda: matgen.upper(*matgen.lap2d(20)), 0, dict(droptol=1e-3)),
+    ("lap_ilut_lfil", lambda: matgen.upper(*matgen.lap2d(20)), 0, dict(droptol=1e-4, fill_level=4)),
+    ("lap_ilu_d", lambda: matgen.upper(*matgen.lap2d(20)), 1, dict(droptol=1e-2, alpha=0.5)),
+    ("lap_ilut_k", lambda: matgen.upper(*matgen.lap2d(20)), 2, dict(droptol=1e-3, additional_fill=2)),
+    ("poisson_ilut", lambda: matgen.upper(*matgen.poisson3d(7)), 0, dict(droptol=1e-3)),
+    ("spd_rand", lambda: _spd_upper(300, 0.02, 9), 0, dict(droptol=1e-3, fill_level=10)),
+]
+
+
+def _spd_upper(n, density, seed):
+    import scipy.sparse as sp
+    p, i, v = matgen.random_csr(n, n, density, seed=seed)
+    S = sp.csr_matrix((v, i, p), shape=(n, n))
+    S = (S + S.T) * 0.5 + sp.identity(n) * 8.0
+    U = sp.triu(S).tocsr()
+    U.sort_indices()
+    return U.indptr.astype(np.int32), U.indices.astype(np.int32), U.data
+
+
+@pytest.mark.parametrize("name,make,type_ilu,kw", SYM_CASES, ids=[c[0] for c in SYM_CASES])
+@pytest.mark.parametrize("ordered", [False, True])
+def test_symmetric_factor_matches_reference(api, reference, name, make, type_ilu, kw, ordered):
+    p, i, v = make()
+    n = p.size - 1
+    perm = np.random.default_rng(n + 1).permutation(n) if ordered else None
+    ours = _ours(api, p, i, v, perm, type_ilu, sym=True, **kw)
+    theirs = reference.ilut_factor(p, i, v, sym=True, perm=perm, type_ilu=type_ilu, **kw)
+    for name_, a, b in zip(("fptr", "find", "fval", "perm_row", "perm_col"), ours, theirs):
+        assert a.shape == b.shape, name_
+        assert np.array_equal(a, b), name_

@@ -205,3 +205,28 @@ def test_factor_types(api, oracle, reference):
     M.SetFactorisationType(M.ILU_K)
     with pytest.raises(NotImplementedError):
         M.FactorizeMatrix(A)
+
+
+def test_symmetric_factor_on_host_and_cg(api, oracle, reference):
+    """The symmetric algorithm factored on the host (GetIlut of the symmetric
+    preconditioner, bit for bit) applies on the device like Seldon's factor,
+    and preconditions CG."""
+    full = matgen.lap2d(60)
+    up = matgen.upper(*full)
+    n = up[0].size - 1
+    S = api.RowSymSparse(n, *up)
+    M = api.IlutPreconditioning()
+    M.SetSymmetricAlgorithm()
+    M.SetDroppingThreshold(1e-3)
+    M.FactorizeMatrix(S)
+    factor = reference.ilut_factor(*up, sym=True, droptol=1e-3)
+    r = np.random.default_rng(8).standard_normal(n)
+    assert np.array_equal(_apply(api, M, S, r, False), oracle.ilut_solve(factor, r, sym=True))
+    b = matgen.matvec(*full, np.random.default_rng(9).uniform(-1, 1, n))
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(1000, 1e-10)
+    it.HideMessages()
+    assert api.Cg(S, X, to_dev(b), M, it) == 0
+    assert it.GetNumberIteration() < 0.5 * _plain_iterations(api, S, b, "cg", 1e-10, 10)
+    with pytest.raises(NotImplementedError):  # symmetric storage needs the symmetric algorithm
+        api.IlutPreconditioning().FactorizeMatrix(S)
