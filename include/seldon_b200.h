@@ -14,7 +14,9 @@
  *   - Vector arguments are DEVICE pointers unless the name says _host.
  *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
  *   - Every function returns an int status: SB2_OK (0) or a negative SB2_ERR_*
- *     code.  Nothing throws, nothing aborts.  Solver convergence/breakdown is
+ *     code.  Nothing throws, nothing aborts: a host allocation that fails
+ *     inside a call gives SB2_ERR_NO_MEMORY, any other C++ exception raised
+ *     inside it SB2_ERR_HOST.  Solver convergence/breakdown is
  *     NOT a status: it is reported in sb2_iter_result.error_code exactly as
  *     Seldon's Iteration::ErrorCode() (Iterative.cxx:344-354).
  *   - Device-side waits (grid barriers of the fused solvers) are bounded; a
@@ -32,11 +34,12 @@ extern "C" {
 /* ------------------------------------------------------------ status codes */
 #define SB2_OK 0
 #define SB2_ERR_INVALID_VALUE -1 /* bad sizes / null pointers / aliasing */
-#define SB2_ERR_NO_MEMORY -2     /* a device allocation failed */
+#define SB2_ERR_NO_MEMORY -2     /* a device or host allocation failed */
 #define SB2_ERR_CUDA -3          /* any other CUDA runtime error */
 #define SB2_ERR_TIMEOUT -4       /* a bounded device-side wait ran out */
 #define SB2_ERR_INVALID_CSR -5   /* CSR invariants violated (validator) */
 #define SB2_ERR_NOT_SUPPORTED -6 /* option combination not implemented */
+#define SB2_ERR_HOST -7          /* any other host-side failure */
 
 /* Human-readable text for a status code (static storage). */
 const char* sb2_status_string(int status);

@@ -17,6 +17,7 @@ SB2_ERR_CUDA = -3
 SB2_ERR_TIMEOUT = -4
 SB2_ERR_INVALID_CSR = -5
 SB2_ERR_NOT_SUPPORTED = -6
+SB2_ERR_HOST = -7
 
 SPMV_SELL = 0
 SPMV_STREAM = 1

@@ -52,7 +52,7 @@ using namespace sb2;
 
 extern "C" {
 
-int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* stream) {
+int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* stream) try {
   if (!A || (A->nnz_stored > 0 && !val)) return SB2_ERR_INVALID_VALUE;
   if (A->sym) return SB2_ERR_NOT_SUPPORTED;  // the expanded copy keeps no map to the stored half
   cudaStream_t s = (cudaStream_t)stream;
@@ -85,10 +85,10 @@ int sb2_csr_set_values(sb2_csr* A, const double* val, int on_device, void* strea
   A->full.sell.d_sval32 = nullptr;
   free_csr(&A->trans);
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const double* x,
-                     double* grad_val, void* stream) {
+                     double* grad_val, void* stream) try {
   SB2_TRACE("sb2_grad_pattern");
   if (!A || (A->nnz > 0 && (!lambda || !x || !grad_val))) return SB2_ERR_INVALID_VALUE;
   if (A->sym) return SB2_ERR_NOT_SUPPORTED;
@@ -98,10 +98,10 @@ int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const
                                                               alpha, lambda, x, grad_val);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_grad_edges(int nedges, const int* ei, const int* ej, const double* lambda,
-                   const double* x, double* grad, void* stream) {
+                   const double* x, double* grad, void* stream) try {
   SB2_TRACE("sb2_grad_edges");
   if (nedges < 0 || (nedges > 0 && (!ei || !ej || !lambda || !x || !grad)))
     return SB2_ERR_INVALID_VALUE;
@@ -110,6 +110,6 @@ int sb2_grad_edges(int nedges, const int* ei, const int* ej, const double* lambd
   grad_edges_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(nedges, ei, ej, lambda, x, grad);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

@@ -459,7 +459,7 @@ extern "C" {
 
 int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val, int index,
                    int m_min, int n_min, int symmetric_upper, void* stream, int* m_out,
-                   int* n_out, int* nnz_out, int** ptr, int** ind, double** val_out) {
+                   int* n_out, int* nnz_out, int** ptr, int** ind, double** val_out) try {
   SB2_TRACE("sb2_coo_to_csr");
   if (nnz < 0 || m_min < 0 || n_min < 0 || !m_out || !n_out || !nnz_out || !ptr || !ind ||
       !val_out)
@@ -527,6 +527,6 @@ int sb2_coo_to_csr(int nnz, const int* row, const int* col, const double* val, i
   *ind = di;
   *val_out = dv;
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

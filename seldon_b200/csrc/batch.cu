@@ -335,7 +335,7 @@ using namespace sb2;
 extern "C" {
 
 int sb2_batch_create(int nsys, const int* sys_row, const int* ptr, const int* ind,
-                     const double* val, sb2_batch** out) {
+                     const double* val, sb2_batch** out) try {
   if (!out || nsys < 0 || !sys_row || !ptr) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
   const int m = sys_row[nsys];
@@ -393,9 +393,9 @@ int sb2_batch_create(int nsys, const int* sys_row, const int* ptr, const int* in
   }
   *out = B;
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_batch_destroy(sb2_batch* B) {
+int sb2_batch_destroy(sb2_batch* B) try {
   if (!B) return SB2_OK;
   cudaFree(B->d_sys_row);
   cudaFree(B->d_order);
@@ -408,10 +408,10 @@ int sb2_batch_destroy(sb2_batch* B) {
   cudaFree(B->d_queue);
   delete B;
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_batch_solve(const sb2_batch* B, double* x, const double* b, const sb2_batch_params* prm,
-                    int* d_iters, double* d_relres, sb2_batch_result* result, void* stream) {
+                    int* d_iters, double* d_relres, sb2_batch_result* result, void* stream) try {
   SB2_TRACE("sb2_batch_solve");
   if (!B || !prm || (B->m > 0 && (!x || !b)) || x == b) return SB2_ERR_INVALID_VALUE;
   if (prm->mode < 0 || prm->mode > 1) return SB2_ERR_INVALID_VALUE;
@@ -440,20 +440,20 @@ int sb2_batch_solve(const sb2_batch* B, double* x, const double* b, const sb2_ba
   }
   *result = R;
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_batch_set_threads(sb2_batch* B, int threads) {
+int sb2_batch_set_threads(sb2_batch* B, int threads) try {
   if (!B || (threads != 128 && threads != 256 && threads != 512)) return SB2_ERR_INVALID_VALUE;
   B->threads = threads;
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_batch_get_threads(const sb2_batch* B) { return B ? B->threads : 0; }
 
 }  // extern "C"
 
 extern "C" int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
-                                  const sb2_batch_params* prm, void* stream) {
+                                  const sb2_batch_params* prm, void* stream) try {
   if (!B || !prm) return SB2_ERR_INVALID_VALUE;
   if (B->nsys == 0) return SB2_OK;
   cudaStream_t s = (cudaStream_t)stream;
@@ -483,4 +483,4 @@ extern "C" int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
   cudaEventDestroy(e1);
   if (st == SB2_OK) B->threads = best_t;
   return st;
-}
+} SB2_CATCH

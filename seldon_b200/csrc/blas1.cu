@@ -115,65 +115,65 @@ using namespace sb2;
 
 extern "C" {
 
-int sb2_dot(int n, const double* x, const double* y, double* result, void* stream) {
+int sb2_dot(int n, const double* x, const double* y, double* result, void* stream) try {
   if (n < 0 || !result || (n > 0 && (!x || !y))) return SB2_ERR_INVALID_VALUE;
   if (n == 0) { *result = 0.0; return SB2_OK; }
   return reduce_to_host(kRedDot, n, x, y, result, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_nrm2(int n, const double* x, double* result, void* stream) {
+int sb2_nrm2(int n, const double* x, double* result, void* stream) try {
   if (n < 0 || !result || (n > 0 && !x)) return SB2_ERR_INVALID_VALUE;
   if (n == 0) { *result = 0.0; return SB2_OK; }
   return reduce_to_host(kRedNrm2, n, x, nullptr, result, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_dot_device(int n, const double* x, const double* y, double* d_result, void* stream) {
+int sb2_dot_device(int n, const double* x, const double* y, double* d_result, void* stream) try {
   if (n < 0 || !d_result || (n > 0 && (!x || !y))) return SB2_ERR_INVALID_VALUE;
   if (n == 0) {
     SB2_CUDA_TRY(cudaMemsetAsync(d_result, 0, sizeof(double), (cudaStream_t)stream));
     return SB2_OK;
   }
   return launch_reduce(kRedDot, n, x, y, d_result, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_nrm2_device(int n, const double* x, double* d_result, void* stream) {
+int sb2_nrm2_device(int n, const double* x, double* d_result, void* stream) try {
   if (n < 0 || !d_result || (n > 0 && !x)) return SB2_ERR_INVALID_VALUE;
   if (n == 0) {
     SB2_CUDA_TRY(cudaMemsetAsync(d_result, 0, sizeof(double), (cudaStream_t)stream));
     return SB2_OK;
   }
   return launch_reduce(kRedNrm2, n, x, nullptr, d_result, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_axpy(int n, double alpha, const double* x, double* y, void* stream) {
+int sb2_axpy(int n, double alpha, const double* x, double* y, void* stream) try {
   if (n < 0 || (n > 0 && (!x || !y))) return SB2_ERR_INVALID_VALUE;
   if (n == 0 || alpha == 0.0) return SB2_OK;  // Functions_Vector.cxx:94
   axpy_kernel<<<elem_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, alpha, x, y);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_scal(int n, double alpha, double* x, void* stream) {
+int sb2_scal(int n, double alpha, double* x, void* stream) try {
   if (n < 0 || (n > 0 && !x)) return SB2_ERR_INVALID_VALUE;
   if (n == 0) return SB2_OK;
   scal_kernel<<<elem_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, alpha, x);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_copy(int n, const double* x, double* y, void* stream) {
+int sb2_copy(int n, const double* x, double* y, void* stream) try {
   if (n < 0 || (n > 0 && (!x || !y))) return SB2_ERR_INVALID_VALUE;
   if (n == 0 || x == y) return SB2_OK;
   SB2_CUDA_TRY(cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_fill(int n, double value, double* x, void* stream) {
+int sb2_fill(int n, double value, double* x, void* stream) try {
   if (n < 0 || (n > 0 && !x)) return SB2_ERR_INVALID_VALUE;
   if (n == 0) return SB2_OK;
   fill_kernel<<<elem_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, value, x);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

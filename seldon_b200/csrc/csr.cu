@@ -372,7 +372,7 @@ extern "C" {
 
 int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
                    const double* val, int symmetric_upper, int validate,
-                   sb2_csr** out) {
+                   sb2_csr** out) try {
   SB2_TRACE("sb2_csr_create");
   if (!out || m < 0 || n < 0 || nnz < 0 || !ptr) return SB2_ERR_INVALID_VALUE;
   if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
@@ -396,7 +396,7 @@ int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
   if (validate) SB2_TRY(validate_csr(m, n, nnz, ptr, ind, symmetric_upper));
   else if (ptr[m] != nnz) return SB2_ERR_INVALID_CSR;
 
-  sb2_csr* A = new sb2_csr();
+  std::unique_ptr<sb2_csr, int (*)(sb2_csr*)> A(new sb2_csr(), sb2_csr_destroy);
   A->device = current_device();
   A->m = m;
   A->n = n;
@@ -412,16 +412,13 @@ int sb2_csr_create(int m, int n, int nnz, const int* ptr, const int* ind,
   } else {
     st = upload_csr(m, n, ptr, ind, val, &A->full);
   }
-  if (st != SB2_OK) {
-    sb2_csr_destroy(A);
-    return st;
-  }
+  if (st != SB2_OK) return st;
   A->nnz = A->full.nnz;
-  *out = A;
+  *out = A.release();
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_csr_destroy(sb2_csr* A) {
+int sb2_csr_destroy(sb2_csr* A) try {
   if (!A) return SB2_OK;
   int prev = current_device();
   cudaSetDevice(A->device);
@@ -445,24 +442,24 @@ int sb2_csr_destroy(sb2_csr* A) {
   cudaSetDevice(prev);
   delete A;
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_csr_info(const sb2_csr* A, int* m, int* n, int* nnz_stored, int* nnz_full) {
+int sb2_csr_info(const sb2_csr* A, int* m, int* n, int* nnz_stored, int* nnz_full) try {
   if (!A) return SB2_ERR_INVALID_VALUE;
   if (m) *m = A->m;
   if (n) *n = A->n;
   if (nnz_stored) *nnz_stored = A->nnz_stored;
   if (nnz_full) *nnz_full = (int)A->nnz;
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_csr_download(const sb2_csr* A, int* ptr, int* ind, double* val) {
+int sb2_csr_download(const sb2_csr* A, int* ptr, int* ind, double* val) try {
   if (!A) return SB2_ERR_INVALID_VALUE;
   const CsrArrays& s = A->sym ? A->upper : A->full;
   if (ptr) SB2_CUDA_TRY(cudaMemcpy(ptr, s.d_ptr, sizeof(int) * (A->m + 1), cudaMemcpyDeviceToHost));
   if (ind && s.nnz) SB2_CUDA_TRY(cudaMemcpy(ind, s.d_ind, sizeof(int) * s.nnz, cudaMemcpyDeviceToHost));
   if (val && s.nnz) SB2_CUDA_TRY(cudaMemcpy(val, s.d_val, sizeof(double) * s.nnz, cudaMemcpyDeviceToHost));
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

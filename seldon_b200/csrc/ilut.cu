@@ -15,6 +15,7 @@
 // mbloc columns, and the replacement of a zero pivot.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <utility>
 #include <vector>
 
@@ -433,7 +434,7 @@ using namespace sb2;
 extern "C" {
 
 int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val, const int* perm,
-                    const sb2_ilut_params* params, sb2_ilut** out) {
+                    const sb2_ilut_params* params, sb2_ilut** out) try {
   SB2_TRACE("sb2_ilut_factor");
   if (!out) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
@@ -451,18 +452,18 @@ int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val, co
   std::vector<Row> F;
   std::vector<int> iperm, rperm;
   SB2_TRY(factor(n, A0, *params, F, iperm, rperm));
-  sb2_ilut* f = flatten(n, F);
+  std::unique_ptr<sb2_ilut> f(flatten(n, F));
   // permutation_col(i) = inv(iperm(i)), permutation_row = perm
   // (IlutPreconditioning.cxx:315-322)
   f->perm_row.assign(perm, perm + n);
   f->perm_col.resize(n);
   for (int i = 0; i < n; i++) f->perm_col[i] = inv[iperm[i]];
-  *out = f;
+  *out = f.release();
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_ilut_factor_sym(int n, const int* ptr, const int* ind, const double* val,
-                        const int* perm, const sb2_ilut_params* params, sb2_ilut** out) {
+                        const int* perm, const sb2_ilut_params* params, sb2_ilut** out) try {
   SB2_TRACE("sb2_ilut_factor_sym");
   if (!out) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
@@ -486,22 +487,22 @@ int sb2_ilut_factor_sym(int n, const int* ptr, const int* ind, const double* val
   SB2_TRY(sort_rows(rows, B));
   std::vector<Row> F;
   SB2_TRY(factor_sym(n, B, *params, F));
-  sb2_ilut* f = flatten(n, F);
+  std::unique_ptr<sb2_ilut> f(flatten(n, F));
   f->perm_row.assign(perm, perm + n);
   f->perm_col = f->perm_row;
-  *out = f;
+  *out = f.release();
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_ilut_size(const sb2_ilut* f, int* n, int* nnz) {
+int sb2_ilut_size(const sb2_ilut* f, int* n, int* nnz) try {
   if (!f) return SB2_ERR_INVALID_VALUE;
   if (n) *n = f->n;
   if (nnz) *nnz = (int)f->find.size();
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_ilut_arrays(const sb2_ilut* f, int* fptr, int* find, double* fval, int* perm_row,
-                    int* perm_col) {
+                    int* perm_col) try {
   if (!f) return SB2_ERR_INVALID_VALUE;
   if (fptr) std::copy(f->fptr.begin(), f->fptr.end(), fptr);
   if (find) std::copy(f->find.begin(), f->find.end(), find);
@@ -509,11 +510,11 @@ int sb2_ilut_arrays(const sb2_ilut* f, int* fptr, int* find, double* fval, int* 
   if (perm_row) std::copy(f->perm_row.begin(), f->perm_row.end(), perm_row);
   if (perm_col) std::copy(f->perm_col.begin(), f->perm_col.end(), perm_col);
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_ilut_destroy(sb2_ilut* f) {
+int sb2_ilut_destroy(sb2_ilut* f) try {
   delete f;
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

@@ -343,7 +343,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
 
 extern "C" int sb2_ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                             const sb2_ir_params* params, sb2_ir_result* result, double* hist,
-                            int hist_cap, void* stream) {
+                            int hist_cap, void* stream) try {
   SB2_TRACE("sb2_ir_solve");
   return sb2::ir_solve(A, M, x, b, params, result, hist, hist_cap, (cudaStream_t)stream);
-}
+} SB2_CATCH

@@ -1391,7 +1391,7 @@ using namespace sb2;
 
 extern "C" {
 
-int sb2_krylov_set_cluster(int on) {
+int sb2_krylov_set_cluster(int on) try {
   const int old = g_cluster_cg ? g_cluster_cap : 0;
   g_cluster_cg = on ? 1 : 0;
   if (on >= 2) {
@@ -1402,38 +1402,38 @@ int sb2_krylov_set_cluster(int on) {
     g_cluster_cap = kClusterMaxRanks;
   }
   return old;
-}
+} SB2_CATCH
 
-int sb2_krylov_set_config(int chain_min_n) {
+int sb2_krylov_set_config(int chain_min_n) try {
   if (chain_min_n < 0) return SB2_ERR_INVALID_VALUE;
   const int old = g_chain_min_n;
   g_chain_min_n = chain_min_n;
   return old;
-}
+} SB2_CATCH
 
 int sb2_cg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
            const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,
-           int hist_cap, void* stream) {
+           int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                  const sb2_iter_params* params, sb2_iter_result* result, double* hist,
-                 int* hist_it, int hist_cap, void* stream) {
+                 int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_bicgstab");
   return solve_entry(kBicg, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
-              int* hist_it, int hist_cap, void* stream) {
+              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_gmres");
   return solve_entry(kGmres, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 }  // extern "C"
 
@@ -1520,6 +1520,6 @@ static int cg_noalloc(const sb2_csr* A, double* x, const double* b, const sb2_it
 
 extern "C" int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
                               const sb2_iter_params* params, sb2_iter_result* result,
-                              void* stream) {
+                              void* stream) try {
   return sb2::cg_noalloc(A, x, b, params, result, (cudaStream_t)stream);
-}
+} SB2_CATCH

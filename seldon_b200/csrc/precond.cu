@@ -798,28 +798,26 @@ using namespace sb2;
 extern "C" {
 
 int sb2_precond_create(const sb2_csr* A, int kind, double omega, int nb_iter,
-                       int symmetric, sb2_precond** out) {
+                       int symmetric, sb2_precond** out) try {
   if (!out || !A) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
   if (kind < SB2_PRECOND_IDENTITY || kind > SB2_PRECOND_SOR) return SB2_ERR_INVALID_VALUE;
   if (A->m != A->n) return SB2_ERR_INVALID_VALUE;
-  sb2_precond* M = new sb2_precond();
+  std::unique_ptr<sb2_precond, int (*)(sb2_precond*)> M(new sb2_precond(),
+                                                         sb2_precond_destroy);
   M->A = A;
   M->kind = kind;
   M->omega = omega;
   M->nb_iter = nb_iter;
   M->symmetric = symmetric ? 1 : 0;
-  if (kind == SB2_PRECOND_JACOBI) {
-    int st = ensure_diag(A);
-    if (st != SB2_OK) { delete M; return st; }
-  }
-  *out = M;
+  if (kind == SB2_PRECOND_JACOBI) SB2_TRY(ensure_diag(A));
+  *out = M.release();
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int* find,
                             const double* fval, const int* perm_row, const int* perm_col,
-                            int symmetric, sb2_precond** out) {
+                            int symmetric, sb2_precond** out) try {
   SB2_TRACE("sb2_precond_create_ilut");
   if (!out || n < 0 || (n > 0 && (!fptr || !perm_row || (!symmetric && !perm_col))))
     return SB2_ERR_INVALID_VALUE;
@@ -827,21 +825,18 @@ int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr, const int*
   if (A && (A->m != n || A->n != n)) return SB2_ERR_INVALID_VALUE;
   if (n > 0 && fptr[n] > 0 && (!find || !fval)) return SB2_ERR_INVALID_VALUE;
   // every index the sweeps read is checked while they are built
-  sb2_precond* M = new sb2_precond();
+  std::unique_ptr<sb2_precond, int (*)(sb2_precond*)> M(new sb2_precond(),
+                                                         sb2_precond_destroy);
   M->A = A;
   M->kind = SB2_PRECOND_ILUT;
   M->n_ilu = n;
   M->ilu_sym = symmetric ? 1 : 0;
-  int st = n > 0 ? plan_ilut(M, n, fptr, find, fval, perm_row, perm_col) : SB2_OK;
-  if (st != SB2_OK) {
-    sb2_precond_destroy(M);
-    return st;
-  }
-  *out = M;
+  if (n > 0) SB2_TRY(plan_ilut(M.get(), n, fptr, find, fval, perm_row, perm_col));
+  *out = M.release();
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_precond** out) {
+int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_precond** out) try {
   SB2_TRACE("sb2_precond_create_ilu0");
   if (!out || !A || A->m != A->n || A->sym) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
@@ -855,9 +850,9 @@ int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_pr
   return sb2_precond_create_ilut(A, n, ptr.data(), ind.empty() ? nullptr : ind.data(),
                                  val.empty() ? nullptr : val.data(), ident.data(), ident.data(), 0,
                                  out);
-}
+} SB2_CATCH
 
-int sb2_precond_destroy(sb2_precond* M) {
+int sb2_precond_destroy(sb2_precond* M) try {
   if (!M) return SB2_OK;
   if (!M->graphs.empty()) cudaDeviceSynchronize();  // no replay may be in flight
   for (auto& e : M->graphs) cudaGraphExecDestroy(e.exec);
@@ -874,24 +869,24 @@ int sb2_precond_destroy(sb2_precond* M) {
   cudaFree(M->d_dinv);
   delete M;
   return SB2_OK;
-}
+} SB2_CATCH
 
-int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+int sb2_precond_solve(const sb2_precond* M, const double* r, double* z, void* stream) try {
   SB2_TRACE("sb2_precond_solve");
   if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, false, r, z, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) {
+int sb2_precond_trans_solve(const sb2_precond* M, const double* r, double* z, void* stream) try {
   SB2_TRACE("sb2_precond_trans_solve");
   if (!M || (precond_n(M) > 0 && (!r || !z)) || (r == z && precond_n(M) > 0))
     return SB2_ERR_INVALID_VALUE;
   return precond_apply(M, true, r, z, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 int sb2_sor(const sb2_csr* A, double* x, const double* b, double omega, int iter,
-            int type_ssor, void* stream) {
+            int type_ssor, void* stream) try {
   SB2_TRACE("sb2_sor");
   if (!A || A->m != A->n || (A->m > 0 && (!x || !b)) || x == b) return SB2_ERR_INVALID_VALUE;
   sb2_precond tmp;
@@ -905,6 +900,6 @@ int sb2_sor(const sb2_csr* A, double* x, const double* b, double omega, int iter
   cudaFree(tmp.d_t);
   if (st == SB2_OK && e != cudaSuccess) st = map_cuda_error(e);
   return st;
-}
+} SB2_CATCH
 
 }  // extern "C"

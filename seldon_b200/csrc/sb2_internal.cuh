@@ -5,7 +5,9 @@
 #include <stdint.h>
 
 #include <map>
+#include <memory>
 #include <mutex>
+#include <new>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -42,6 +44,16 @@ struct TraceRange {
   } while (0)
 
 int map_cuda_error(cudaError_t e);
+
+// Closes every C entry point's function-try-block: no C++ exception leaves
+// the C ABI (a ctypes, cgo or JNI caller cannot catch one).
+#define SB2_CATCH                          \
+  catch (const std::bad_alloc&) {          \
+    return SB2_ERR_NO_MEMORY;              \
+  }                                        \
+  catch (...) {                            \
+    return SB2_ERR_HOST;                   \
+  }
 
 // ----------------------------------------------------------------- tuning
 

@@ -203,16 +203,16 @@ using namespace sb2;
 extern "C" {
 
 int sb2_spmv(const sb2_csr* A, int trans, double alpha, const double* x,
-             double beta, double* y, void* stream) {
+             double beta, double* y, void* stream) try {
   SB2_TRACE("sb2_spmv");
   return spmv_common(A, trans, alpha, x, beta, y, false, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 int sb2_mlt(const sb2_csr* A, int trans, double alpha, const double* x,
-            double* y, void* stream) {
+            double* y, void* stream) try {
   SB2_TRACE("sb2_mlt");
   return spmv_common(A, trans, alpha, x, 0.0, y, true, (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 static int spmv_host_common(const sb2_csr* cA, int trans, double alpha,
                             const double* x_host, double beta, double* y_host,
@@ -242,14 +242,14 @@ static int spmv_host_common(const sb2_csr* cA, int trans, double alpha,
 
 int sb2_spmv_host(const sb2_csr* A, int trans, double alpha,
                   const double* x_host, double beta, double* y_host,
-                  void* stream) {
+                  void* stream) try {
   SB2_TRACE("sb2_spmv_host");
   // y is copied in too: MltAdd scales it by beta even when beta == 0.
   return spmv_host_common(A, trans, alpha, x_host, beta, y_host, false,
                           (cudaStream_t)stream);
-}
+} SB2_CATCH
 
-int sb2_spmv_set_config(int algo, int threads, int stages) {
+int sb2_spmv_set_config(int algo, int threads, int stages) try {
   if (algo < SB2_SPMV_SELL || algo > SB2_SPMV_TMA) return SB2_ERR_INVALID_VALUE;
   if ((threads != 256 && threads != 512) || (stages != 3 && stages != 4))
     return SB2_ERR_INVALID_VALUE;
@@ -257,14 +257,14 @@ int sb2_spmv_set_config(int algo, int threads, int stages) {
   g_spmv_threads = threads;
   g_spmv_stages = stages;
   return SB2_OK;
-}
+} SB2_CATCH
 
 int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
-                 const double* x_host, double* y_host, void* stream) {
+                 const double* x_host, double* y_host, void* stream) try {
   SB2_TRACE("sb2_mlt_host");
   return spmv_host_common(A, trans, alpha, x_host, 0.0, y_host, true,
                           (cudaStream_t)stream);
-}
+} SB2_CATCH
 
 // y_i = alpha*op(A)*x_i for a batch of host vectors.  Two device buffers per
 // side and two copy streams: the copy of x_{i+1} in, the product i and the
@@ -273,7 +273,7 @@ int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
 // reuse of each buffer: x into buffer b waits for the product that last read
 // it, the product into y buffer b waits for the copy out that last read it.
 int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
-                       const double* x_host, double* y_host, void* stream) {
+                       const double* x_host, double* y_host, void* stream) try {
   SB2_TRACE("sb2_mlt_host_batch");
   if (!cA || count < 0) return SB2_ERR_INVALID_VALUE;
   sb2_csr* A = const_cast<sb2_csr*>(cA);
@@ -318,6 +318,6 @@ int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
   // every product and every copy out has completed when s_out has
   SB2_CUDA_TRY(cudaStreamSynchronize(A->s_out));
   return SB2_OK;
-}
+} SB2_CATCH
 
 }  // extern "C"

@@ -144,48 +144,49 @@ const char* sb2_status_string(int status) {
   switch (status) {
     case SB2_OK: return "ok";
     case SB2_ERR_INVALID_VALUE: return "invalid value (sizes, null or overlapping pointers)";
-    case SB2_ERR_NO_MEMORY: return "device allocation failed";
+    case SB2_ERR_NO_MEMORY: return "device or host allocation failed";
     case SB2_ERR_CUDA: return "CUDA runtime error";
     case SB2_ERR_TIMEOUT: return "a bounded device-side wait ran out";
     case SB2_ERR_INVALID_CSR: return "CSR invariants violated";
     case SB2_ERR_NOT_SUPPORTED: return "option combination not supported";
+    case SB2_ERR_HOST: return "host-side failure";
     default: return "unknown status";
   }
 }
 
 int sb2_version(void) { return 10000; }
 
-int sb2_device_alloc(size_t bytes, void** out) {
+int sb2_device_alloc(size_t bytes, void** out) try {
   if (!out) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
   if (bytes == 0) return SB2_OK;
   return sb2::map_cuda_error(cudaMalloc(out, bytes));
-}
+} SB2_CATCH
 
-int sb2_device_free(void* p) {
+int sb2_device_free(void* p) try {
   if (!p) return SB2_OK;
   cudaError_t e;
   if (sb2::release_owned(p, &e)) return sb2::map_cuda_error(e);
   return sb2::map_cuda_error(cudaFree(p));
-}
+} SB2_CATCH
 
-int sb2_memcpy(void* dst, const void* src, size_t bytes, void* stream) {
+int sb2_memcpy(void* dst, const void* src, size_t bytes, void* stream) try {
   if (bytes == 0) return SB2_OK;
   if (!dst || !src) return SB2_ERR_INVALID_VALUE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return sb2::map_cuda_error(e);
-}
+} SB2_CATCH
 
-int sb2_stream_sync(void* stream) {
+int sb2_stream_sync(void* stream) try {
   return sb2::map_cuda_error(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-}
+} SB2_CATCH
 
-int sb2_set_wait_limit_ms(int ms) {
+int sb2_set_wait_limit_ms(int ms) try {
   int old = sb2::g_wait_limit_ms;
   if (ms > 0) sb2::g_wait_limit_ms = ms;
   return old;
-}
+} SB2_CATCH
 
 }  // extern "C"

@@ -40,3 +40,38 @@ def test_status_strings_without_gpu():
     assert lib.sb2_status_string(0) == b"ok"
     assert b"CSR" in lib.sb2_status_string(_lib.SB2_ERR_INVALID_CSR)
     assert lib.sb2_version() >= 10000
+    assert lib.sb2_status_string(_lib.SB2_ERR_HOST) == b"host-side failure"
+
+
+_OOM_CHILD = r"""
+import ctypes, re, resource, sys
+import numpy as np
+from seldon_b200 import _lib
+lib = _lib.load()
+n = 4_000_000
+ptr = np.arange(n + 1, dtype=np.int32)
+ind = np.arange(n, dtype=np.int32)
+val = np.ones(n)
+perm = np.arange(n, dtype=np.int32)
+prm = _lib.IlutParams(0, 10, 0, 100, 1.0, 1e-3, 0.0)
+h = ctypes.c_void_p()
+vm = int(re.search(r"VmSize:\s+(\d+)", open("/proc/self/status").read()).group(1)) * 1024
+resource.setrlimit(resource.RLIMIT_AS, (vm + (96 << 20), resource.RLIM_INFINITY))
+p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+st = lib.sb2_ilut_factor(n, p(ptr), p(ind), p(val), p(perm), ctypes.byref(prm), ctypes.byref(h))
+print("status", st, h.value)
+"""
+
+
+def test_host_allocation_failure_is_a_status():
+    """No C++ exception crosses the C ABI: a host allocation that fails
+    inside an entry point (here the ILUT factorization of a 4M-row matrix
+    under a 96 MB address-space allowance) returns SB2_ERR_NO_MEMORY and the
+    caller's process goes on."""
+    import subprocess
+    import sys
+    from seldon_b200 import _lib
+    out = subprocess.run([sys.executable, "-c", _OOM_CHILD], cwd=ROOT, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.split() == ["status", str(_lib.SB2_ERR_NO_MEMORY), "None"], out.stdout
