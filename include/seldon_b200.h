@@ -21,6 +21,16 @@
  *     Seldon's Iteration::ErrorCode() (Iterative.cxx:344-354).
  *   - Device-side waits (grid barriers of the fused solvers) are bounded; a
  *     wait that runs out ends the kernel and the call returns SB2_ERR_TIMEOUT.
+ *   - Threads: calls from several host threads, each on its own stream, may
+ *     share a matrix handle.  Its lazily built members (transpose, diagonal,
+ *     FP32 copy, cluster plan) are built under the handle's lock and
+ *     published only when complete.  Solver work vectors come from a
+ *     stream-ordered pool, and reduction scratch is kept per (device,
+ *     stream).  A preconditioner or batch handle holds work arrays of its
+ *     own (the SOR and ILUT sweeps' temporary, the batch residuals): one
+ *     stream at a time, as Seldon's objects are used by one thread at a time.
+ *     sb2_cg_noalloc shares one scratch per device (see its declaration).
+ *     Destroying a handle that a call still uses is the caller's error.
  */
 #ifndef SELDON_B200_H
 #define SELDON_B200_H

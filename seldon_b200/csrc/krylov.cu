@@ -1046,10 +1046,10 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
 // 3e6 rows (7-point Poisson: persistent 70.6 us/iteration against 87.2 at
 // 2.1e6 rows, equal at 3.0e6, chained 213 against 249 at 7.1e6).
 // sb2_krylov_set_config changes it.
-static int g_chain_min_n = 2800000;
+static std::atomic<int> g_chain_min_n{2800000};
 // Systems that fit one thread-block cluster's shared memory run CG there.
-static int g_cluster_cg = 1;
-static int g_cluster_cap = 16;  // most CTAs a cluster may take
+static std::atomic<int> g_cluster_cg{1};
+static std::atomic<int> g_cluster_cap{16};  // most CTAs a cluster may take
 
 // ----------------------------------------------------------------- cluster-resident CG
 //
@@ -1247,9 +1247,10 @@ static size_t cluster_smem(int rpc, int nnz_max) {
 static int cluster_plan(const sb2_csr* A, int* ranks, int* rpc, int* nnz_max) {
   sb2_csr* M = const_cast<sb2_csr*>(A);
   std::lock_guard<std::mutex> g(M->mu);
-  if (M->cl_ranks < 0 || M->cl_cap != g_cluster_cap) {
+  const int cap = g_cluster_cap.load();
+  if (M->cl_ranks < 0 || M->cl_cap != cap) {
     M->cl_ranks = 0;
-    M->cl_cap = g_cluster_cap;
+    M->cl_cap = cap;
     const int n = A->m;
     if (n >= 256 && n <= kClusterMaxRanks * 4096) {
       std::vector<int> ptr(n + 1);
@@ -1257,7 +1258,7 @@ static int cluster_plan(const sb2_csr* A, int* ranks, int* rpc, int* nnz_max) {
       int dev_smem = 0;
       cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, current_device());
       const size_t limit = (size_t)std::max(dev_smem - 1024, 0);  // static shared memory
-      for (int c = std::min(kClusterMaxRanks, g_cluster_cap); c >= 2; c /= 2) {
+      for (int c = std::min(kClusterMaxRanks, cap); c >= 2; c /= 2) {
         const int r = (n + c - 1) / c;
         int mx = 0;
         for (int q = 0; q < c; q++) {
@@ -1392,7 +1393,7 @@ using namespace sb2;
 extern "C" {
 
 int sb2_krylov_set_cluster(int on) try {
-  const int old = g_cluster_cg ? g_cluster_cap : 0;
+  const int old = g_cluster_cg ? g_cluster_cap.load() : 0;
   g_cluster_cg = on ? 1 : 0;
   if (on >= 2) {
     int c = 2;

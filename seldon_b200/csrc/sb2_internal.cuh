@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -187,7 +188,7 @@ bool release_owned(void* p, cudaError_t* err);
 int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
                 double* y, bool overwrite, cudaStream_t s);
 
-extern int g_wait_limit_ms;
+extern std::atomic<int> g_wait_limit_ms;
 
 // ----------------------------------------------------------------- device code
 

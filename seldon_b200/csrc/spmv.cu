@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(NT, 2) spmv_tma_kernel(
 // Product algorithm (set by the autotuner): binned SELL-32 by default, the
 // row-block stream kernel or the TMA-pipelined kernel; and the TMA launch
 // configuration (threads per CTA, ring stages).
-static int g_spmv_algo = SB2_SPMV_SELL, g_spmv_threads = 256, g_spmv_stages = 4;
+static std::atomic<int> g_spmv_algo{SB2_SPMV_SELL}, g_spmv_threads{256}, g_spmv_stages{4};
 
 // y = beta*y + alpha*t, or y = alpha*t when OVERWRITE (Mlt)
 template <bool OVERWRITE>
@@ -117,18 +117,28 @@ SellOp<double> sell_op(const CsrArrays& a) {
 template <int NT, int S>
 static int launch_tma(const CsrArrays& a, double alpha, const double* x, double beta, double* y,
                       bool overwrite, cudaStream_t s, int* status) {
-  static int per_sm = -1;
+  // the shared-memory opt-in is a per-device setting: taken, with the
+  // occupancy it gives, on each device's first launch
+  static std::mutex mu;
+  static std::map<int, int> per_sm_of;
   const size_t smem = TmaRing<S, double, double>::smem_bytes();
-  if (per_sm < 0) {
-    cudaFuncSetAttribute(spmv_tma_kernel<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    int v = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, spmv_tma_kernel<NT, S>, NT, smem) !=
-        cudaSuccess)
-      v = 1;
-    per_sm = v < 1 ? 1 : v;
+  const int dev = current_device();
+  int per_sm;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = per_sm_of.find(dev);
+    if (it == per_sm_of.end()) {
+      SB2_CUDA_TRY(cudaFuncSetAttribute(spmv_tma_kernel<NT, S>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int v = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, spmv_tma_kernel<NT, S>, NT, smem) !=
+          cudaSuccess)
+        v = 1;
+      it = per_sm_of.emplace(dev, v < 1 ? 1 : v).first;
+    }
+    per_sm = it->second;
   }
-  const int g = std::min(a.tma.nblk, per_sm * num_sms(current_device()));
+  const int g = std::min(a.tma.nblk, per_sm * num_sms(dev));
   TmaOp<double> op{a.d_ptr, a.d_ind, a.d_val, a.tma.d_desc, a.tma.nblk, a.rows};
   spmv_tma_kernel<NT, S><<<g, NT, smem, s>>>(op, alpha, x, beta, y, overwrite, status,
                                              (unsigned long long)g_wait_limit_ms * 1000000ull);

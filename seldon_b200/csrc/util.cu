@@ -5,7 +5,7 @@
 
 namespace sb2 {
 
-int g_wait_limit_ms = 2000;
+std::atomic<int> g_wait_limit_ms{2000};
 
 int map_cuda_error(cudaError_t e) {
   if (e == cudaSuccess) return SB2_OK;
