@@ -292,7 +292,10 @@ typedef struct {
 /* The factor of a RowSparse matrix given by HOST arrays (ptr[n+1], ind, val;
  * no repeated column in a row: SB2_ERR_NOT_SUPPORTED) and an ordering perm
  * (FactorizeMatrix's perm; the identity for none).  A row whose entries are
- * all zero gives SB2_ERR_INVALID_VALUE (the reference aborts).  The result
+ * all zero gives SB2_ERR_INVALID_VALUE (the reference aborts), and so does
+ * an ILUT or ILUT_K fill below 1 for some row (fill_level 0, or
+ * additional_fill <= -row length), which keeps no pivot and where the
+ * reference writes past the row it resized.  The result
  * is read with sb2_ilut_size / sb2_ilut_arrays (fptr[n+1], find[nnz],
  * fval[nnz], perm_row[n], perm_col[n]) and released with sb2_ilut_destroy. */
 typedef struct sb2_ilut sb2_ilut;

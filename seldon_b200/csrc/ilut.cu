@@ -80,6 +80,9 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
     if (tnorm == 0.0) return SB2_ERR_INVALID_VALUE;  // structurally singular row
     tnorm /= (double)size_row;
     if (variable_fill) lfil = size_row + p.additional_fill;
+    // A fill below 1 keeps no U entry, not even the pivot: the reference then
+    // stores 1/U(i,i) one position past the row it resized, so it is refused.
+    if (!standard_dropping && lfil < 1) return SB2_ERR_INVALID_VALUE;
     double dropsum = 0.0;
     // the row's L part at w[0..nl), its diagonal at w[i], its U part after
     int nl = 0, nu = 1;
@@ -253,6 +256,9 @@ int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
     if (tnorm == 0.0) return SB2_ERR_INVALID_VALUE;  // structurally singular row
     tnorm /= (double)size_row;
     if (variable_fill) lfil = size_row + p.additional_fill;
+    // A fill below 1 leaves the row empty: the reference then stores 1/D(i)
+    // in a row it reallocated to length 0, so it is refused.
+    if (!standard_dropping && lfil < 1) return SB2_ERR_INVALID_VALUE;
     double dropsum = 0.0;
     int nl = 0, nu = 1;
     wi[i] = i;

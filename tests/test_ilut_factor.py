@@ -78,6 +78,22 @@ def test_rejections(api):
                       np.ones(2))
 
 
+@pytest.mark.parametrize("sym", [False, True])
+def test_fill_below_one_is_refused(api, sym):
+    """ILUT with fill level 0, or ILUT_K with additional fill at or below
+    minus a row's length, keeps no pivot; the reference then writes past the
+    row it resized, so the factorization is refused.  ILU_D ignores the fill
+    level and keeps the pivot."""
+    from seldon_b200._lib import SeldonB200Error, SB2_ERR_INVALID_VALUE
+    A = matgen.upper(*matgen.lap2d(6)) if sym else matgen.convdiff3d(4)
+    for type_ilu, kw in ((0, dict(fill_level=0)), (2, dict(additional_fill=-7))):
+        with pytest.raises(SeldonB200Error) as e:
+            _ours(api, *A, None, type_ilu, sym=sym, droptol=1e-3, **kw)
+        assert e.value.status == SB2_ERR_INVALID_VALUE
+    fptr, find, fval, prow, pcol = _ours(api, *A, None, 1, sym=sym, droptol=1e-3, fill_level=0)
+    assert np.all(np.diff(fptr) >= 1)
+
+
 SYM_CASES = [
     ("lap_ilut", lambda: matgen.upper(*matgen.lap2d(20)), 0, dict(droptol=1e-3)),
     ("lap_ilut_lfil", lambda: matgen.upper(*matgen.lap2d(20)), 0, dict(droptol=1e-4, fill_level=4)),
