@@ -323,7 +323,9 @@ int sb2_ilut_destroy(sb2_ilut* f);
  * reference's bit for bit.  A's rows must be sorted by column, without
  * repeats, and hold their diagonal (SB2_ERR_INVALID_CSR otherwise); a zero
  * pivot gives SB2_ERR_INVALID_VALUE (the reference aborts).  The result is an
- * SB2_PRECOND_ILUT preconditioner bound to A. */
+ * SB2_PRECOND_ILUT preconditioner that keeps no reference to A (as one made
+ * by sb2_precond_create_ilut with A == NULL): A may be destroyed after the
+ * call, and the solvers take it with any matrix of order n. */
 int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream,
                             sb2_precond** out);
 

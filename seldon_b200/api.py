@@ -236,6 +236,17 @@ class RowSparse:
             _L.sb2_csr_destroy(self._h)
             self._h = None
 
+    def Clear(self):
+        """Matrix_Sparse::Clear (Matrix_Sparse.cxx:278-281): the device
+        arrays are released and the matrix becomes 0 x 0."""
+        import numpy as np
+        h = ctypes.c_void_p()
+        check(_L.sb2_csr_create(0, 0, 0, _np_ptr(np.zeros(1, dtype=np.int32)), None, None,
+                                int(self.symmetric), 1, ctypes.byref(h)), "sb2_csr_create")
+        self.close()
+        self._h = h
+        self.m = self.n = self.nnz_stored = self.nnz_full = 0
+
     def __del__(self):
         try:
             self.close()
@@ -432,6 +443,7 @@ class IlutPreconditioning(_DevicePrecond):
     def __init__(self):
         super().__init__()
         self._factor = None
+        self._device_handle = None
         self._serial = 0
         # IlutPreconditioning's defaults (IlutPreconditioning.cxx:27-40)
         self.type_ilu = self.ILUT
@@ -442,6 +454,19 @@ class IlutPreconditioning(_DevicePrecond):
         self.droptol = 0.01
         self.permtol = 0.1
         self.symmetric_algorithm = False
+        self.print_level = 0
+
+    def Clear(self):
+        """Releases the factor and its device sweeps (IlutPreconditioning.cxx:
+        43-50); the settings stay."""
+        for _, h, _s in self._cache.values():
+            _L.sb2_precond_destroy(h)
+        if self._device_handle is not None:
+            _L.sb2_precond_destroy(self._device_handle)
+        self._cache = {}
+        self._device_handle = None
+        self._factor = None
+        self._serial += 1
 
     def SetSymmetricAlgorithm(self):
         self.symmetric_algorithm = True
@@ -472,6 +497,31 @@ class IlutPreconditioning(_DevicePrecond):
 
     def SetPivotThreshold(self, t):
         self.permtol = float(t)
+
+    def SetPrintLevel(self, k):
+        """Kept for the interface; the factorization prints nothing."""
+        self.print_level = int(k)
+
+    def GetFillLevel(self):
+        return self.fill_level
+
+    def GetAdditionalFillNumber(self):
+        return self.additional_fill
+
+    def GetPrintLevel(self):
+        return self.print_level
+
+    def GetPivotBlockInteger(self):
+        return self.mbloc
+
+    def GetDroppingThreshold(self):
+        return self.droptol
+
+    def GetDiagonalCoefficient(self):
+        return self.alpha
+
+    def GetPivotThreshold(self):
+        return self.permtol
 
     def factor_host(self, n, ptr, ind, val, perm=None, symmetric=False):
         """The ILUT / ILU_D / ILUT_K factor of host CSR arrays, computed on
@@ -522,18 +572,62 @@ class IlutPreconditioning(_DevicePrecond):
 
     ILUT, ILU_D, ILUT_K, ILU_0, MILU_0, ILU_K = range(6)
 
-    def FactorizeMatrix(self, A, perm=None, stream=None):
-        """FactorizeMatrix of a RowSparse matrix with the unsymmetric
-        algorithm.  ILU_0 / MILU_0 (identity ordering) are factored on the
-        device, as GetIlu0 / GetMilu0 do; ILUT, ILU_D and ILUT_K on the host
-        in GetIlut's order (`perm`: the ordering, identity by default).  ILU_K
-        and the symmetric algorithm come from Seldon through SetFactor."""
+    @staticmethod
+    def _factorize_args(args, perm):
+        """(A, perm, keep_matrix) from FactorizeMatrix(A, perm=None), which
+        keeps A, or from the reference's FactorizeMatrix(perm, A,
+        keep_matrix=False), which clears A afterwards unless keep_matrix."""
+        if len(args) == 1:
+            return args[0], perm, True
+        if len(args) in (2, 3) and perm is None:
+            return args[1], args[0], bool(args[2]) if len(args) == 3 else False
+        raise TypeError("FactorizeMatrix(A, perm=None) or FactorizeMatrix(perm, A[, keep_matrix])")
+
+    def FactorizeSymMatrix(self, *args, perm=None, stream=None):
+        """The symmetric algorithm on a RowSymSparse matrix, whatever
+        SetSymmetricAlgorithm says (IlutPreconditioning.cxx:216-263)."""
+        A, perm, keep = self._factorize_args(args, perm)
+        if not A.symmetric:
+            raise NotImplementedError("FactorizeSymMatrix takes a RowSymSparse matrix here")
+        self._factorize(A, perm, keep, stream)
+
+    def FactorizeUnsymMatrix(self, *args, perm=None, stream=None):
+        """The unsymmetric algorithm on a RowSparse matrix, whatever
+        SetSymmetricAlgorithm says (IlutPreconditioning.cxx:266-323)."""
+        A, perm, keep = self._factorize_args(args, perm)
+        if A.symmetric:
+            # the reference's unsymmetric algorithm on symmetric storage
+            # does not compile
+            raise NotImplementedError("FactorizeUnsymMatrix takes a RowSparse matrix")
+        self._factorize(A, perm, keep, stream)
+
+    def FactorizeMatrix(self, *args, perm=None, stream=None):
+        """FactorizeMatrix (IlutPreconditioning.cxx:186-213), called as
+        FactorizeMatrix(A, perm=None) or as the reference's
+        FactorizeMatrix(perm, A, keep_matrix=False).  ILU_0 / MILU_0
+        (identity ordering) are factored on the device, as GetIlu0 / GetMilu0
+        do; ILUT, ILU_D and ILUT_K on the host in GetIlut's order, with the
+        unsymmetric algorithm on RowSparse and the symmetric one on
+        RowSymSparse.  ILU_K comes from Seldon through SetFactor."""
+        A, perm, keep = self._factorize_args(args, perm)
         if A.symmetric != self.symmetric_algorithm:
             # the reference factors symmetric storage with the symmetric
             # algorithm only (its other path does not compile) and aborts on
             # the symmetric algorithm with general storage
             raise NotImplementedError(
                 "RowSymSparse takes SetSymmetricAlgorithm(), RowSparse the unsymmetric one")
+        self._factorize(A, perm, keep, stream)
+
+    def _factorize(self, A, perm, keep, stream):
+        if perm is not None and len(perm) != A.m:
+            # the reference aborts: "Numbering array should have the same
+            # size as matrix."
+            raise ValueError("WrongDim: the ordering must have one entry per row")
+        self._factorize_kept(A, perm, stream)
+        if not keep:
+            A.Clear()
+
+    def _factorize_kept(self, A, perm, stream):
         if self.type_ilu in (self.ILUT, self.ILU_D, self.ILUT_K):
             f = self.factor_host(A.m, *A.download(), perm=perm, symmetric=A.symmetric)
             self.SetFactor(*f, symmetric=A.symmetric)
@@ -544,35 +638,67 @@ class IlutPreconditioning(_DevicePrecond):
             raise NotImplementedError(
                 "ILU_K is not factored here: factor it with Seldon "
                 "(IlutPreconditioning::FactorizeMatrix) and pass it to SetFactor")
-        if perm is not None:
+        import numpy as np
+        if perm is not None and not np.array_equal(np.asarray(perm), np.arange(A.m)):
             raise NotImplementedError("the device ILU(0) uses the identity ordering")
         h = ctypes.c_void_p()
         check(_L.sb2_precond_create_ilu0(A.handle, int(self.type_ilu == self.MILU_0),
                                          _stream(stream), ctypes.byref(h)),
               "sb2_precond_create_ilu0")
-        for _, old, _s in self._cache.values():
-            _L.sb2_precond_destroy(old)
+        self.Clear()
         self._factor = ("device", A.m)
-        self._serial += 1
-        self._cache = {id(A): (A, h, self._serial)}
+        self._device_handle = h
 
     def _params(self):
         return self._serial
+
+    def Solve(self, *args, stream=None):
+        """Solve(A, r, z), or in place Solve(z) and Solve(trans, z)
+        (IlutPreconditioning.cxx:329-374)."""
+        if len(args) == 3:
+            return super().Solve(*args, stream=stream)
+        if len(args) == 1:
+            return self._in_place(args[0], False, stream)
+        if len(args) == 2:
+            return self._in_place(args[1], args[0] == SeldonTrans, stream)
+        raise TypeError("Solve(A, r, z), Solve(z) or Solve(trans, z)")
+
+    def TransSolve(self, *args, stream=None):
+        """TransSolve(A, r, z), or in place TransSolve(z)."""
+        if len(args) == 3:
+            return super().TransSolve(*args, stream=stream)
+        if len(args) == 1:
+            return self._in_place(args[0], True, stream)
+        raise TypeError("TransSolve(A, r, z) or TransSolve(z)")
+
+    def _in_place(self, z, trans, stream):
+        h = self.handle_for(None)
+        n = self._factor[1] if self._factor[0] == "device" else self._factor[0]
+        r = z.clone()
+        fn = _L.sb2_precond_trans_solve if trans else _L.sb2_precond_solve
+        check(fn(h, _dev_ptr(r, n, "z"), _dev_ptr(z, n, "z"), _stream(stream)),
+              "TransSolve" if trans else "Solve")
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
 
     def handle_for(self, A):
         if self._factor is None:
             raise RuntimeError("IlutPreconditioning: no factor (call SetFactor first)")
         if self._factor[0] == "device":
-            ent = self._cache.get(id(A))
-            if ent is None or ent[0] is not A:
-                raise ValueError("IlutPreconditioning: factorized for another matrix")
-            return ent[1]
+            # the device factor keeps no reference to the matrix it came from
+            if A is not None and A.m != self._factor[1]:
+                raise ValueError("WrongDim: the factor's order differs from the matrix's")
+            return self._device_handle
         key = id(A)
         ent = self._cache.get(key)
         if ent is None or ent[0] is not A or ent[2] != self._serial:
             n, fptr, find, fval, prow, pcol, sym = self._factor
             h = ctypes.c_void_p()
-            check(_L.sb2_precond_create_ilut(A.handle, n, _np_ptr(fptr), _np_ptr(find),
+            check(_L.sb2_precond_create_ilut(None if A is None else A.handle, n, _np_ptr(fptr), _np_ptr(find),
                                              _np_ptr(fval), _np_ptr(prow), _np_ptr(pcol),
                                              int(sym), ctypes.byref(h)),
                   "sb2_precond_create_ilut")

@@ -847,7 +847,9 @@ int sb2_precond_create_ilu0(const sb2_csr* A, int modified, void* stream, sb2_pr
   std::vector<int> ident(std::max(n, 1));
   for (int i = 0; i < n; i++) ident[i] = i;
   if (ptr.empty()) ptr.assign(1, 0);
-  return sb2_precond_create_ilut(A, n, ptr.data(), ind.empty() ? nullptr : ind.data(),
+  // the factor no longer needs A: like the reference's preconditioner, it
+  // applies to whichever matrix of order n the solver is given
+  return sb2_precond_create_ilut(nullptr, n, ptr.data(), ind.empty() ? nullptr : ind.data(),
                                  val.empty() ? nullptr : val.data(), ident.data(), ident.data(), 0,
                                  out);
 } SB2_CATCH

@@ -125,3 +125,67 @@ def test_symmetric_factor_matches_reference(api, reference, name, make, type_ilu
     for name_, a, b in zip(("fptr", "find", "fval", "perm_row", "perm_col"), ours, theirs):
         assert a.shape == b.shape, name_
         assert np.array_equal(a, b), name_
+
+
+class _HostMatrix:
+    """Stands in for RowSparse / RowSymSparse on the host: the factorization
+    only downloads the arrays (and clears the matrix unless asked to keep it)."""
+
+    def __init__(self, p, i, v, symmetric=False):
+        self.m = p.size - 1
+        self.symmetric = symmetric
+        self._arrays = (p, i, v)
+        self.cleared = False
+
+    def download(self):
+        return self._arrays
+
+    def Clear(self):
+        self.cleared = True
+        self.m = 0
+
+
+def test_interface_matches_reference(api):
+    """Defaults and accessors of IlutPreconditioning (IlutPreconditioning.cxx:
+    27-168), and FactorizeMatrix in both call forms: (A, perm=None) keeps A,
+    the reference's (perm, A, keep_matrix=False) clears it unless asked."""
+    M = api.IlutPreconditioning()
+    assert (M.GetFactorisationType(), M.GetFillLevel(), M.GetAdditionalFillNumber(),
+            M.GetPivotBlockInteger(), M.GetPrintLevel()) == (M.ILUT, 1000000, 1000000, 1000000, 0)
+    assert (M.GetDiagonalCoefficient(), M.GetDroppingThreshold(), M.GetPivotThreshold()) == \
+        (1.0, 0.01, 0.1)
+    M.SetFillLevel(7)
+    M.SetAdditionalFillNumber(3)
+    M.SetPivotBlockInteger(11)
+    M.SetPrintLevel(2)
+    M.SetDiagonalCoefficient(0.5)
+    M.SetDroppingThreshold(1e-3)
+    M.SetPivotThreshold(0.4)
+    assert (M.GetFillLevel(), M.GetAdditionalFillNumber(), M.GetPivotBlockInteger(),
+            M.GetPrintLevel(), M.GetDiagonalCoefficient(), M.GetDroppingThreshold(),
+            M.GetPivotThreshold()) == (7, 3, 11, 2, 0.5, 1e-3, 0.4)
+    p, i, v = matgen.convdiff3d(5)
+    n = p.size - 1
+    perm = np.random.default_rng(1).permutation(n).astype(np.int32)
+    want = M.factor_host(n, p, i, v, perm=perm)
+    for args, kw, cleared in (((None,), dict(perm=perm), False), ((perm, None), {}, True),
+                              ((perm, None, True), {}, False), ((perm, None, False), {}, True)):
+        A = _HostMatrix(p, i, v)
+        args = tuple(A if a is None else a for a in args)
+        M.FactorizeMatrix(*args, **kw)
+        assert A.cleared == cleared
+        got = M._factor
+        for a, b in zip(got[1:6], want):
+            assert np.array_equal(a, b)
+    M.Clear()
+    assert M._factor is None
+    with pytest.raises(ValueError):  # the reference aborts on a wrong-size ordering
+        M.FactorizeMatrix(perm[:-1], _HostMatrix(p, i, v))
+    with pytest.raises(NotImplementedError):
+        M.FactorizeSymMatrix(perm, _HostMatrix(p, i, v))
+    up = matgen.upper(*matgen.lap2d(5))
+    S = _HostMatrix(*up, symmetric=True)
+    with pytest.raises(NotImplementedError):
+        M.FactorizeUnsymMatrix(np.arange(25), S)
+    M.FactorizeSymMatrix(np.arange(25), S, True)
+    assert not S.cleared and M._factor[6]

@@ -230,3 +230,45 @@ def test_symmetric_factor_on_host_and_cg(api, oracle, reference):
     assert it.GetNumberIteration() < 0.5 * _plain_iterations(api, S, b, "cg", 1e-10, 10)
     with pytest.raises(NotImplementedError):  # symmetric storage needs the symmetric algorithm
         api.IlutPreconditioning().FactorizeMatrix(S)
+
+
+def test_reference_call_forms(api, oracle, reference):
+    """The reference's FactorizeMatrix(perm, A) clears A (keep_matrix false);
+    the device ILU(0) factor keeps no reference to A and applies to another
+    matrix of the same order, in Solve / TransSolve and in BiCgStab; the
+    in-place forms Solve(z), TransSolve(z) and Solve(SeldonTrans, z) equal
+    the three-argument ones, for a device and a host factor."""
+    p, i, v = matgen.convdiff3d(9)
+    n = p.size - 1
+    rng = np.random.default_rng(12)
+    r = rng.standard_normal(n)
+    A = api.RowSparse(n, n, p, i, v)
+    M = api.IlutPreconditioning()
+    M.SetFactorisationType(M.ILU_0)
+    M.FactorizeMatrix(np.arange(n), A)
+    assert A.GetM() == 0
+    A2 = api.RowSparse(n, n, p, i, v)
+    factor = reference.ilut_factor(p, i, v, type_ilu=reference.ILU_0)
+    for trans in (False, True):
+        assert np.array_equal(_apply(api, M, A2, r, trans),
+                              oracle.ilut_solve(factor, r, trans=trans))
+    b = matgen.matvec(p, i, v, rng.uniform(-1, 1, n))
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(500, 1e-10)
+    it.HideMessages()
+    assert api.BiCgStab(A2, X, to_dev(b), M, it) == 0
+    H = api.IlutPreconditioning()
+    H.SetDroppingThreshold(1e-3)
+    H.FactorizeMatrix(rng.permutation(n), A2, True)
+    assert A2.GetM() == n
+    for P in (M, H):
+        want, want_t = _apply(api, P, A2, r, False), _apply(api, P, A2, r, True)
+        Z = to_dev(r)
+        P.Solve(Z)
+        assert np.array_equal(to_host(Z), want)
+        Z = to_dev(r)
+        P.TransSolve(Z)
+        assert np.array_equal(to_host(Z), want_t)
+        Z = to_dev(r)
+        P.Solve(api.SeldonTrans, Z)
+        assert np.array_equal(to_host(Z), want_t)
