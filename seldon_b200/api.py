@@ -358,6 +358,13 @@ class Preconditioner_Base:
     def handle_for(self, A):
         return None
 
+    def Solve(self, A, r, z, stream=None):
+        """z = r (Copy)."""
+        Copy(r, z, stream=stream)
+
+    def TransSolve(self, A, r, z, stream=None):
+        Copy(r, z, stream=stream)
+
 
 class _DevicePrecond:
     kind = None
@@ -732,6 +739,65 @@ class Iteration:
         self.facteur_reste = 0.0
         self.history = []      # (iteration, relative residual) of each Finished() test
         self.init_failed = False
+        self.fail_convergence = False
+        self.type_solver = 0
+        self.type_preconditioning = 0
+
+    def copy(self):
+        """The copy constructor (Iterative.cxx:110-122): settings, factor and
+        error code carried over, iteration count reset, null initial guess."""
+        it = Iteration(self.max_iter, self.tolerance)
+        it.facteur_reste = self.facteur_reste
+        it.print_level = self.print_level
+        it.error_code = self.error_code
+        it.type_solver = self.type_solver
+        it.parameter_restart = self.parameter_restart
+        it.type_preconditioning = self.type_preconditioning
+        return it
+
+    def GetTypeSolver(self):
+        return self.type_solver
+
+    def SetSolver(self, type_resolution, param_restart, type_prec):
+        self.type_solver = int(type_resolution)
+        self.parameter_restart = int(param_restart)
+        self.type_preconditioning = int(type_prec)
+
+    def Init(self, r):
+        """Iteration::Init (Iterative.cxx:236-251) on a device vector: -1 for
+        a zero right-hand side, otherwise 1/Norm2(r) becomes the factor of
+        the relative residual and the count restarts."""
+        norm = Norm2(r)
+        if norm == 0.0:
+            return -1
+        self.facteur_reste = 1.0 / norm
+        self.nb_iter = 0
+        return 0
+
+    def First(self):
+        return self.nb_iter == 0
+
+    def Finished(self, r):
+        """Iteration::Finished (Iterative.cxx:272-321) on a residual vector
+        (its Norm2 on the device) or on a residual norm: true once the
+        relative residual is below the tolerance or the count reaches
+        max_iter, printing the reference's lines at its print levels."""
+        reste = self.facteur_reste * (float(r) if isinstance(r, (int, float)) else Norm2(r))
+        if (self.print_level >= 1 and self.nb_iter % 100 == 0) or self.print_level >= 6:
+            print(f"Residu at iteration number {self.nb_iter}  {reste:g}")
+        return reste < self.tolerance or self.nb_iter >= self.max_iter
+
+    def Fail(self, i, s):
+        """Iteration::Fail (Iterative.cxx:324-333)."""
+        self.fail_convergence = True
+        self.error_code = int(i)
+        if self.print_level >= 1 and self.nb_iter % 100 == 0:
+            print(f"Error during resolution : {s}")
+
+    def __iadd__(self, k):
+        """`it += 1` for the reference's ++iter."""
+        self.nb_iter += int(k)
+        return self
 
     def SetRestart(self, m):
         self.parameter_restart = int(m)
@@ -773,7 +839,12 @@ class Iteration:
         return self.init_guess_null
 
     def ErrorCode(self):
-        return self.error_code
+        """Iteration::ErrorCode (Iterative.cxx:345-354)."""
+        if self.nb_iter >= self.max_iter:
+            return -2
+        if self.fail_convergence:
+            return self.error_code
+        return 0
 
     def _replay(self):
         # the lines Iteration::Finished prints (Iterative.cxx:282-287)
@@ -796,6 +867,7 @@ def _solve(fn, A, x, b, M, iteration, hist_cap, stream):
     check(st, fn.__name__)
     iteration.nb_iter = res.nb_iter
     iteration.error_code = res.error_code
+    iteration.fail_convergence = res.error_code not in (0, -2)
     iteration.facteur_reste = res.facteur_reste
     iteration.init_failed = bool(res.init_failed)
     iteration.history = list(zip(hist_it[:res.hist_len].tolist(), hist[:res.hist_len].tolist()))

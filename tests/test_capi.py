@@ -75,3 +75,30 @@ def test_host_allocation_failure_is_a_status():
                          text=True, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
     assert out.stdout.split() == ["status", str(_lib.SB2_ERR_NO_MEMORY), "None"], out.stdout
+
+
+def test_iteration_loop_interface(capsys):
+    """Iteration's loop interface for hand-written drivers (Iterative.cxx:
+    236-354): First, Finished on a residual norm (with the reference's
+    printed lines), Fail, ++ (as +=) and ErrorCode's rule."""
+    from seldon_b200 import api
+    it = api.Iteration(250, 1e-8)
+    assert it.First() and it.ErrorCode() == 0 and it.GetTypeSolver() == 0
+    it.SetSolver(3, 30, 1)
+    assert (it.GetTypeSolver(), it.GetRestart()) == (3, 30)
+    it.facteur_reste = 0.5
+    assert not it.Finished(1.0)
+    assert capsys.readouterr().out == "Residu at iteration number 0  0.5\n"
+    it += 1
+    assert not it.First()
+    assert it.Finished(1e-8) and not it.Finished(2e-8)
+    assert capsys.readouterr().out == ""          # print level 1: every 100th only
+    it.ShowFullHistory()
+    it.Finished(3e-8)
+    assert capsys.readouterr().out == "Residu at iteration number 1  1.5e-08\n"
+    it.Fail(3, "breakdown")
+    assert it.ErrorCode() == 3
+    c = it.copy()
+    assert (c.GetNumberIteration(), c.GetFactor(), c.GetRestart()) == (0, 0.5, 30)
+    it.SetNumberIteration(250)
+    assert it.Finished(1.0) and it.ErrorCode() == -2   # max_iter outranks a failure

@@ -444,3 +444,65 @@ def test_nonfinite_inputs(api, oracle, name, which, pc, cluster):
     x = to_host(X)
     assert (code, it.GetNumberIteration()) == (co, no) == (-2, 25)
     assert np.array_equal(np.isnan(x), np.isnan(xo))
+
+
+def _cg_by_hand(api, A, x, b, M, it):
+    """Cg.cxx:45-116 written over the Python mirror's operations and
+    Iteration's loop interface, as a user's own driver would be."""
+    if A.GetM() <= 0:
+        return 0
+    p, q, r, z = (b.clone() for _ in range(4))
+    if it.Init(b) != 0:
+        return it.ErrorCode()
+    api.Copy(b, r)
+    if not it.IsInitGuess_Null():
+        api.MltAdd(-1.0, A, x, 1.0, r)
+    else:
+        api.Fill(x, 0.0)
+    it.SetNumberIteration(0)
+    rho_1 = 1.0
+    while not it.Finished(r):
+        M.Solve(A, r, z)
+        rho = api.DotProd(r, z)
+        if rho == 0.0:
+            it.Fail(1, "Cg breakdown #1")
+            break
+        if it.First():
+            api.Copy(z, p)
+        else:
+            api.Mlt(rho / rho_1, p)
+            api.Add(1.0, z, p)
+        api.Mlt(A, p, q)
+        delta = api.DotProd(p, q)
+        if delta == 0.0:
+            it.Fail(2, "Cg breakdown #2")
+            break
+        alpha = rho / delta
+        api.Add(alpha, p, x)
+        api.Add(-alpha, q, r)
+        rho_1 = rho
+        it += 1
+    return it.ErrorCode()
+
+
+@pytest.mark.parametrize("pc", [0, 1])
+def test_hand_written_driver(api, pc):
+    """A driver written against the Python mirror (its BLAS-1, MltAdd, the
+    preconditioners' Solve and Iteration's Init/Finished/First/Fail/++)
+    reaches the fused Cg's iterate: same exit code, iteration count within
+    the reduction-order slack, same solution to 1e-8."""
+    ptr, ind, val = matgen.lap2d(40)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    b = to_dev(matgen.matvec(ptr, ind, val, np.random.default_rng(21).uniform(-1, 1, n)))
+    out = []
+    for solve in (_cg_by_hand, lambda api_, *a: api_.Cg(*a)):
+        X = to_dev(np.zeros(n))
+        it = api.Iteration(2000, 1e-10)
+        it.HideMessages()
+        code = solve(api, A, X, b, _precond(api, pc), it)
+        out.append((code, it.GetNumberIteration(), to_host(X), it.ErrorCode()))
+    (c0, n0, x0, e0), (c1, n1, x1, e1) = out
+    assert c0 == c1 == e0 == e1 == 0
+    assert abs(n0 - n1) <= max(2, n1 // 50), (n0, n1)
+    assert np.linalg.norm(x0 - x1) / np.linalg.norm(x1) < 1e-8
