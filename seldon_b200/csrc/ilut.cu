@@ -14,6 +14,7 @@
 // fill-in append order, the quick-split, the pivot search within blocks of
 // mbloc columns, and the replacement of a zero pivot.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <memory>
 #include <utility>
@@ -54,29 +55,42 @@ void quick_split(std::vector<double>& a, std::vector<int>& ind, int first, int n
   }
 }
 
-struct Row {
-  std::vector<int> idx;
+// Rows in one flat CSR: the input rows, and the factor, whose rows are
+// appended in order (the elimination of row i reads only rows before i).
+struct Csr {
+  std::vector<int> ptr{0}, idx;
   std::vector<double> val;
+  int begin(int i) const { return ptr[i]; }
+  int end(int i) const { return ptr[i + 1]; }
+  // closes the row just appended; the factor's indices are int32
+  bool close_row() {
+    if (idx.size() > (size_t)INT_MAX) return false;
+    ptr.push_back((int)idx.size());
+    return true;
+  }
 };
 
-int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vector<Row>& F,
-           std::vector<int>& iperm, std::vector<int>& rperm) {
+int factor(int n, const Csr& A0, const sb2_ilut_params& p, Csr& F, std::vector<int>& iperm,
+           std::vector<int>& rperm) {
   const bool variable_fill = (p.type == SB2_ILUT_K);
   const bool standard_dropping = (p.type == SB2_ILU_D);
   int lfil = p.fill_level;
   if (lfil < 0) return SB2_ERR_INVALID_VALUE;
-  F.assign(n, Row());
+  F = Csr();
+  F.ptr.reserve((size_t)n + 1);
   std::vector<double> w(n, 0.0);
   std::vector<int> wi(n, -1), where(n, -1), diag_at(n, -1);
   iperm.resize(n);
   rperm.resize(n);
   for (int i = 0; i < n; i++) iperm[i] = rperm[i] = i;
   for (int i = 0; i < n; i++) {
-    const Row& a = A0[i];
-    const int size_row = (int)a.idx.size();
+    const int a0 = A0.begin(i);
+    const int size_row = A0.end(i) - a0;
+    const int* a_idx = A0.idx.data() + a0;
+    const double* a_val = A0.val.data() + a0;
     double tnorm = 0.0;
     for (int k = 0; k < size_row; k++)
-      if (a.val[k] != 0.0) tnorm += std::fabs(a.val[k]);
+      if (a_val[k] != 0.0) tnorm += std::fabs(a_val[k]);
     if (tnorm == 0.0) return SB2_ERR_INVALID_VALUE;  // structurally singular row
     tnorm /= (double)size_row;
     if (variable_fill) lfil = size_row + p.additional_fill;
@@ -90,8 +104,8 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
     w[i] = 0.0;
     where[i] = i;
     for (int k = 0; k < size_row; k++) {
-      const int c = rperm[a.idx[k]];
-      const double t = a.val[k];
+      const int c = rperm[a_idx[k]];
+      const double t = a_val[k];
       if (c < i) {
         wi[nl] = c;
         w[nl] = t;
@@ -132,14 +146,13 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
       }
       double fact = 0.0;
       if (!dropped) {
-        fact = w[jc] * F[jrow].val[diag_at[jrow]];
+        fact = w[jc] * F.val[F.begin(jrow) + diag_at[jrow]];
         if (!standard_dropping && std::fabs(fact) <= p.droptol) dropped = true;
       }
       if (!dropped) {
-        const Row& u = F[jrow];
-        for (int k = diag_at[jrow] + 1; k < (int)u.idx.size(); k++) {
-          const double s = fact * u.val[k];
-          const int c = rperm[u.idx[k]];
+        for (int k = F.begin(jrow) + diag_at[jrow] + 1; k < F.end(jrow); k++) {
+          const double s = fact * F.val[k];
+          const int c = rperm[F.idx[k]];
           const int at = where[c];
           if (c >= i) {
             if (at == -1) {
@@ -175,12 +188,10 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
       len = std::min(kept, lfil);
       quick_split(w, wi, 0, kept, len);
     }
-    Row& f = F[i];
-    f.idx.clear();
-    f.val.clear();
+    const size_t row0 = F.idx.size();
     for (int k = 0; k < len; k++) {
-      f.val.push_back(w[k]);
-      f.idx.push_back(iperm[wi[k]]);
+      F.val.push_back(w[k]);
+      F.idx.push_back(iperm[wi[k]]);
     }
     const int index_diag = len;
     diag_at[i] = index_diag;
@@ -223,15 +234,15 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
     rperm[iperm[i]] = i;
     rperm[iperm[jcol]] = jcol;
     for (int k = i; k <= i + lu - 1; k++) {
-      f.idx.push_back(iperm[wi[k]]);
-      f.val.push_back(w[k]);
+      F.idx.push_back(iperm[wi[k]]);
+      F.val.push_back(w[k]);
     }
     if (standard_dropping) w[i] += p.alpha * dropsum;
     if (w[i] == 0.0) w[i] = (p.droptol + 1e-4) * tnorm;
-    f.val[index_diag] = 1.0 / w[i];
+    F.val[row0 + index_diag] = 1.0 / w[i];
+    if (!F.close_row()) return SB2_ERR_NOT_SUPPORTED;
   }
-  for (int i = 0; i < n; i++)
-    for (int& c : F[i].idx) c = rperm[c];
+  for (int& c : F.idx) c = rperm[c];
   return SB2_OK;
 }
 
@@ -239,20 +250,22 @@ int factor(int n, const std::vector<Row>& A0, const sb2_ilut_params& p, std::vec
 // the full rows of the symmetric matrix, sorted by column; row i of the
 // factor keeps 1/D(i) first and then its U part (no pivoting, no L part
 // kept); at the end every U entry is scaled by its row's 1/D.
-int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
-               std::vector<Row>& F) {
+int factor_sym(int n, const Csr& B, const sb2_ilut_params& p, Csr& F) {
   const bool variable_fill = (p.type == SB2_ILUT_K);
   const bool standard_dropping = (p.type == SB2_ILU_D);
   int lfil = p.fill_level;
   if (lfil < 0) return SB2_ERR_INVALID_VALUE;
-  F.assign(n, Row());
+  F = Csr();
+  F.ptr.reserve((size_t)n + 1);
   std::vector<double> w(n, 0.0);
   std::vector<int> wi(n, -1), where(n, -1);
   for (int i = 0; i < n; i++) {
-    const Row& a = B[i];
-    const int size_row = (int)a.idx.size();
+    const int b0 = B.begin(i);
+    const int size_row = B.end(i) - b0;
+    const int* a_idx = B.idx.data() + b0;
+    const double* a_val = B.val.data() + b0;
     double tnorm = 0.0;
-    for (int k = 0; k < size_row; k++) tnorm += std::fabs(a.val[k]);
+    for (int k = 0; k < size_row; k++) tnorm += std::fabs(a_val[k]);
     if (tnorm == 0.0) return SB2_ERR_INVALID_VALUE;  // structurally singular row
     tnorm /= (double)size_row;
     if (variable_fill) lfil = size_row + p.additional_fill;
@@ -265,8 +278,8 @@ int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
     w[i] = 0.0;
     where[i] = i;
     for (int k = 0; k < size_row; k++) {
-      const int c = a.idx[k];
-      const double t = a.val[k];
+      const int c = a_idx[k];
+      const double t = a_val[k];
       if (c < i) {
         wi[nl] = c;
         w[nl] = t;
@@ -306,14 +319,13 @@ int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
       }
       double fact = 0.0;
       if (!dropped) {
-        fact = w[jc] * F[jrow].val[0];
+        fact = w[jc] * F.val[F.begin(jrow)];
         if (!standard_dropping && std::fabs(fact) <= p.droptol) dropped = true;
       }
       if (!dropped) {
-        const Row& u = F[jrow];
-        for (int k = 1; k < (int)u.idx.size(); k++) {
-          const double s = fact * u.val[k];
-          const int c = u.idx[k];
+        for (int k = F.begin(jrow) + 1; k < F.end(jrow); k++) {
+          const double s = fact * F.val[k];
+          const int c = F.idx[k];
           const int at = where[c];
           if (c >= i) {
             if (at == -1) {
@@ -359,19 +371,20 @@ int factor_sym(int n, const std::vector<Row>& B, const sb2_ilut_params& p,
     } else {
       lu++;
     }
-    Row& f = F[i];
-    f.idx.assign(1, i);  // 1/D(i); the reference leaves this index unset
-    f.val.assign(1, 0.0);
+    const size_t row0 = F.idx.size();
+    F.idx.push_back(i);  // 1/D(i); the reference leaves this index unset
+    F.val.push_back(0.0);
     for (int k = i + 1; k <= i + lu - 1; k++) {
-      f.idx.push_back(wi[k]);
-      f.val.push_back(w[k]);
+      F.idx.push_back(wi[k]);
+      F.val.push_back(w[k]);
     }
     if (standard_dropping) w[i] += p.alpha * dropsum;
     if (w[i] == 0.0) w[i] = (p.droptol + 1e-4) * tnorm;
-    f.val[0] = 1.0 / w[i];
+    F.val[row0] = 1.0 / w[i];
+    if (!F.close_row()) return SB2_ERR_NOT_SUPPORTED;
   }
   for (int i = 0; i < n; i++)
-    for (size_t j = 1; j < F[i].val.size(); j++) F[i].val[j] *= F[i].val[0];
+    for (int k = F.begin(i) + 1; k < F.end(i); k++) F.val[k] *= F.val[F.begin(i)];
   return SB2_OK;
 }
 
@@ -401,36 +414,59 @@ int check_csr_perm(int n, const int* ptr, const int* ind, const double* val, con
   return SB2_OK;
 }
 
-sb2_ilut* flatten(int n, const std::vector<Row>& F) {
-  sb2_ilut* f = new sb2_ilut();
+// The result handle, taking the factor's arrays.
+std::unique_ptr<sb2_ilut> to_handle(int n, Csr& F) {
+  std::unique_ptr<sb2_ilut> f(new sb2_ilut());
   f->n = n;
-  f->fptr.assign(n + 1, 0);
-  for (int i = 0; i < n; i++) {
-    f->find.insert(f->find.end(), F[i].idx.begin(), F[i].idx.end());
-    f->fval.insert(f->fval.end(), F[i].val.begin(), F[i].val.end());
-    f->fptr[i + 1] = (int)f->find.size();
-  }
+  f->fptr = std::move(F.ptr);
+  f->find = std::move(F.idx);
+  f->fval = std::move(F.val);
   return f;
 }
 
-// Rows sorted by column, a repeated column refused.
-int sort_rows(std::vector<std::vector<std::pair<int, double>>>& rows, std::vector<Row>& out) {
-  out.assign(rows.size(), Row());
-  for (size_t i = 0; i < rows.size(); i++) {
-    auto& e = rows[i];
-    std::sort(e.begin(), e.end(),
-              [](const std::pair<int, double>& x, const std::pair<int, double>& y) {
-                return x.first < y.first;
-              });
-    for (size_t k = 1; k < e.size(); k++)
-      if (e[k].first == e[k - 1].first) return SB2_ERR_NOT_SUPPORTED;
-    for (const auto& q : e) {
-      out[i].idx.push_back(q.first);
-      out[i].val.push_back(q.second);
-    }
+// Input rows from (row, column, value) entries: a counting pass sizes the
+// rows, a second pass places the entries, then each row is sorted by column
+// and a repeated column is refused.
+struct RowBuilder {
+  int n;
+  std::vector<long long> count;
+  std::vector<int> fill;
+  Csr out;
+  explicit RowBuilder(int n_) : n(n_), count((size_t)n_ + 1, 0) {}
+  void tally(int r) { count[r + 1]++; }
+  int start() {
+    for (int i = 0; i < n; i++) count[i + 1] += count[i];
+    if (count[n] > INT_MAX) return SB2_ERR_NOT_SUPPORTED;  // int32 row offsets
+    out.ptr.assign(count.begin(), count.end());
+    fill.assign(out.ptr.begin(), out.ptr.end() - 1);
+    out.idx.resize(count[n]);
+    out.val.resize(count[n]);
+    return SB2_OK;
   }
-  return SB2_OK;
-}
+  void put(int r, int c, double v) {
+    const int at = fill[r]++;
+    out.idx[at] = c;
+    out.val[at] = v;
+  }
+  int finish() {
+    std::vector<std::pair<int, double>> e;
+    for (int i = 0; i < n; i++) {
+      const int b = out.begin(i), len = out.end(i) - b;
+      e.resize(len);
+      for (int k = 0; k < len; k++) e[k] = {out.idx[b + k], out.val[b + k]};
+      std::sort(e.begin(), e.end(),
+                [](const std::pair<int, double>& x, const std::pair<int, double>& y) {
+                  return x.first < y.first;
+                });
+      for (int k = 0; k < len; k++) {
+        if (k && e[k].first == e[k - 1].first) return SB2_ERR_NOT_SUPPORTED;
+        out.idx[b + k] = e[k].first;
+        out.val[b + k] = e[k].second;
+      }
+    }
+    return SB2_OK;
+  }
+};
 
 }  // namespace
 }  // namespace sb2
@@ -450,15 +486,16 @@ int sb2_ilut_factor(int n, const int* ptr, const int* ind, const double* val, co
   // rows and columns permuted, each row sorted by its new columns
   // (ApplyInversePermutation, Permutation_ScalingMatrix.cxx:215-256, on the
   // ArrayRowSparse copy)
-  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  RowBuilder rows(n);
+  for (int i = 0; i < n; i++) rows.count[perm[i] + 1] += ptr[i + 1] - ptr[i];
+  SB2_TRY(rows.start());
   for (int i = 0; i < n; i++)
-    for (int k = ptr[i]; k < ptr[i + 1]; k++) rows[perm[i]].emplace_back(perm[ind[k]], val[k]);
-  std::vector<Row> A0;
-  SB2_TRY(sort_rows(rows, A0));
-  std::vector<Row> F;
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) rows.put(perm[i], perm[ind[k]], val[k]);
+  SB2_TRY(rows.finish());
+  Csr F;
   std::vector<int> iperm, rperm;
-  SB2_TRY(factor(n, A0, *params, F, iperm, rperm));
-  std::unique_ptr<sb2_ilut> f(flatten(n, F));
+  SB2_TRY(factor(n, rows.out, *params, F, iperm, rperm));
+  std::unique_ptr<sb2_ilut> f = to_handle(n, F);
   // permutation_col(i) = inv(iperm(i)), permutation_row = perm
   // (IlutPreconditioning.cxx:315-322)
   f->perm_row.assign(perm, perm + n);
@@ -480,20 +517,26 @@ int sb2_ilut_factor_sym(int n, const int* ptr, const int* ind, const double* val
   // (Permutation_ScalingMatrix.cxx:465-525), then both triangles of every
   // row sorted by column (Copy to ArrayRowSparse, Matrix_Conversions.cxx:
   // 4155-4200)
-  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  RowBuilder rows(n);
   for (int i = 0; i < n; i++)
     for (int k = ptr[i]; k < ptr[i + 1]; k++) {
       if (ind[k] < i) return SB2_ERR_INVALID_CSR;  // upper triangle only
+      const int r = perm[i], c = perm[ind[k]];
+      rows.tally(r);
+      if (c != r) rows.tally(c);
+    }
+  SB2_TRY(rows.start());
+  for (int i = 0; i < n; i++)
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) {
       int r = perm[i], c = perm[ind[k]];
       if (c < r) std::swap(r, c);
-      rows[r].emplace_back(c, val[k]);
-      if (c != r) rows[c].emplace_back(r, val[k]);
+      rows.put(r, c, val[k]);
+      if (c != r) rows.put(c, r, val[k]);
     }
-  std::vector<Row> B;
-  SB2_TRY(sort_rows(rows, B));
-  std::vector<Row> F;
-  SB2_TRY(factor_sym(n, B, *params, F));
-  std::unique_ptr<sb2_ilut> f(flatten(n, F));
+  SB2_TRY(rows.finish());
+  Csr F;
+  SB2_TRY(factor_sym(n, rows.out, *params, F));
+  std::unique_ptr<sb2_ilut> f = to_handle(n, F);
   f->perm_row.assign(perm, perm + n);
   f->perm_col = f->perm_row;
   *out = f.release();
