@@ -376,7 +376,9 @@ class _DevicePrecond:
         return 1.0, 1, 1
 
     def handle_for(self, A):
-        key = id(A)
+        # keyed on the matrix object and its current library handle (Clear
+        # replaces the handle)
+        key = (id(A), getattr(A.handle, "value", None))
         ent = self._cache.get(key)
         if ent is None or ent[0] is not A or ent[2] != self._params():
             omega, nb, sym = self._params()
@@ -700,7 +702,7 @@ class IlutPreconditioning(_DevicePrecond):
             if A is not None and A.m != self._factor[1]:
                 raise ValueError("WrongDim: the factor's order differs from the matrix's")
             return self._device_handle
-        key = id(A)
+        key = (id(A), None if A is None else getattr(A.handle, "value", None))
         ent = self._cache.get(key)
         if ent is None or ent[0] is not A or ent[2] != self._serial:
             n, fptr, find, fval, prow, pcol, sym = self._factor
