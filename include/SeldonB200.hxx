@@ -567,6 +567,37 @@ namespace Seldon
       //! Stored entries (the upper triangle for RowSymSparse).
       int GetNonZeros() const { return nz_; }
       int GetDataSize() const { return nz_; }
+      //! Lengths of ptr and ind (Matrix_Sparse.cxx:1018-1037).
+      int GetPtrSize() const { return this->m_ + 1; }
+      int GetIndSize() const { return nz_; }
+
+      //! Element (i, j) by the reference's lookup (Matrix_Sparse.cxx:
+      //! 1054-1083; RowSymSparse reads (min, max) in the upper triangle,
+      //! Matrix_SymSparse.cxx:1013-1053).  Each call downloads the stored
+      //! arrays: it is for inspection, not for loops.
+      double operator() (int i, int j) const
+      {
+        CheckIndex(i, j, "Matrix::operator()");
+        std::vector<int> ptr, ind;
+        std::vector<double> val;
+        Download(ptr, ind, val);
+        return Lookup(ptr, ind, val, i, j);
+      }
+
+      //! The dense matrix, row by row (Matrix_Sparse::Print,
+      //! Matrix_Sparse.cxx:1491-1499), from one download.
+      void Print() const
+      {
+        std::vector<int> ptr, ind;
+        std::vector<double> val;
+        Download(ptr, ind, val);
+        for (int i = 0; i < this->m_; i++)
+          {
+            for (int j = 0; j < this->n_; j++)
+              std::cout << Lookup(ptr, ind, val, i, j) << "\t";
+            std::cout << std::endl;
+          }
+      }
 
       //! Library handle (for the C ABI of seldon_b200.h).
       sb2_csr* GetHandle() const
@@ -726,6 +757,32 @@ namespace Seldon
       }
 
     protected:
+      void CheckIndex(int i, int j, const char* function) const
+      {
+#ifdef SELDON_CHECK_BOUNDS
+        if (i < 0 || i >= this->m_)
+          throw WrongRow(function, "row index out of range");
+        if (j < 0 || j >= this->n_)
+          throw WrongCol(function, "column index out of range");
+#endif
+      }
+
+      //! The reference's element lookup on downloaded arrays: scan row i
+      //! while k < b-1 and ind[k] < j, then test ind[k] == j.
+      static double Lookup(const std::vector<int>& ptr, const std::vector<int>& ind,
+                           const std::vector<double>& val, int i, int j)
+      {
+        if (Symmetric && i > j)
+          std::swap(i, j);
+        const int a = ptr[i], b = ptr[i + 1];
+        if (a == b)
+          return 0.0;
+        int k = a;
+        while (k < b - 1 && ind[k] < j)
+          k++;
+        return ind[k] == j ? val[k] : 0.0;
+      }
+
       void CopyDevice(const DeviceCsr& A)
       {
         if (&A == this)

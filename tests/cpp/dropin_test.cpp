@@ -50,6 +50,10 @@ namespace Seldon
 
 using namespace Seldon;
 
+// every member of the device matrix types compiles, whether a case uses it
+template class Seldon::b200::DeviceCsr<0>;
+template class Seldon::b200::DeviceCsr<1>;
+
 typedef Matrix<double, General, RowSparse> HostGen;
 typedef Matrix<double, Symmetric, RowSymSparse> HostSym;
 typedef Vector<double> HostVec;
