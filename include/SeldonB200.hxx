@@ -409,6 +409,99 @@ namespace Seldon
                     "Vector::Read");
     }
 
+    //! Seldon's host vector holding these entries (read back from the device).
+    Vector<T, VectFull> HostCopy() const
+    {
+      Vector<T, VectFull> h(this->m_);
+      if (this->m_ > 0)
+        b200::Check(sb2_memcpy(h.GetData(), this->data_, sizeof(T) * size_t(this->m_),
+                               b200::GetStream()), "Vector::HostCopy");
+      return h;
+    }
+
+    //! Takes the length and entries of a host vector.
+    template <class Allocator0>
+    void Upload(const Vector<T, VectFull, Allocator0>& h)
+    {
+      Reallocate(h.GetM());
+      if (this->m_ > 0)
+        b200::Check(sb2_memcpy(this->data_, h.GetData(), sizeof(T) * size_t(this->m_),
+                               b200::GetStream()), "Vector::Upload");
+    }
+
+    //! Largest absolute value and its index, as Vector::GetNormInf and
+    //! GetNormInfIndex compute them (Vector.cxx:765-800), on the entries
+    //! read back from the device: for inspection, not for loops.
+    value_type GetNormInf() const
+    {
+      return HostCopy().GetNormInf();
+    }
+
+    int GetNormInfIndex() const
+    {
+      return HostCopy().GetNormInfIndex();
+    }
+
+    //! Seldon's FillRand values (drawn on the host), then uploaded.
+    void FillRand()
+    {
+      Vector<T, VectFull> h(this->m_);
+      h.FillRand();
+      Upload(h);
+    }
+
+    //! Seldon's text format (Vector::WriteText / ReadText), through a host copy.
+    void WriteText(std::string FileName) const
+    {
+      HostCopy().WriteText(FileName);
+    }
+
+    void WriteText(std::ostream& FileStream) const
+    {
+      HostCopy().WriteText(FileStream);
+    }
+
+    void ReadText(std::string FileName)
+    {
+      Vector<T, VectFull> h;
+      h.ReadText(FileName);
+      Upload(h);
+    }
+
+    void ReadText(std::istream& FileStream)
+    {
+      Vector<T, VectFull> h;
+      h.ReadText(FileStream);
+      Upload(h);
+    }
+
+    //! One entry added at the end (Vector::Append, PushBack): the buffer is
+    //! reallocated, so build long vectors on the host and copy them instead.
+    void Append(const T& x)
+    {
+      const int m = this->m_;
+      Resize(m + 1);
+      b200::Check(sb2_memcpy(this->data_ + m, &x, sizeof(T), b200::GetStream()),
+                  "Vector::Append");
+    }
+
+    template <class T0>
+    void PushBack(const T0& x)
+    {
+      Append(T(x));
+    }
+
+    //! The entries of X (host or device) added at the end.
+    template <class Allocator0>
+    void PushBack(const Vector<T, VectFull, Allocator0>& X)
+    {
+      const int m = this->m_;
+      Resize(m + X.GetM());
+      if (X.GetM() > 0)
+        b200::Check(sb2_memcpy(this->data_ + m, X.GetData(), sizeof(T) * size_t(X.GetM()),
+                               b200::GetStream()), "Vector::PushBack");
+    }
+
     //! Prints the entries (read back from the device) as Vector::Print does.
     void Print() const
     {

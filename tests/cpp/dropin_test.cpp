@@ -53,6 +53,7 @@ using namespace Seldon;
 // every member of the device matrix types compiles, whether a case uses it
 template class Seldon::b200::DeviceCsr<0>;
 template class Seldon::b200::DeviceCsr<1>;
+template class Seldon::Vector<double, Seldon::VectFull, Seldon::CudaAlloc<double> >;
 
 typedef Matrix<double, General, RowSparse> HostGen;
 typedef Matrix<double, Symmetric, RowSymSparse> HostSym;
