@@ -106,6 +106,21 @@ def ConvertMatrix_from_Coordinates(IndRow, IndCol, Val, index=0, m=0, n=0, symme
     return mo.value, no.value, ptr, ind, val
 
 
+def lookup(ptr, ind, val, i, j, symmetric=False):
+    """The reference's element lookup on CSR arrays: scan row i while k < b-1
+    and ind[k] < j, then test ind[k] == j (Matrix_Sparse.cxx:1054-1083); the
+    symmetric storage looks up (min(i, j), max(i, j))."""
+    if symmetric and i > j:
+        i, j = j, i
+    a, b = int(ptr[i]), int(ptr[i + 1])
+    if a == b:
+        return 0.0
+    k = a
+    while k < b - 1 and ind[k] < j:
+        k += 1
+    return float(val[k]) if ind[k] == j else 0.0
+
+
 class RowSparse:
     """Matrix<double, General, RowSparse> held on the device.
 
@@ -153,6 +168,31 @@ class RowSparse:
 
     def GetNonZeros(self):
         return self.nnz_stored
+
+    def GetDataSize(self):
+        return self.nnz_stored
+
+    def GetPtrSize(self):
+        return self.m + 1
+
+    def GetIndSize(self):
+        return self.nnz_stored
+
+    def __call__(self, i, j):
+        """Element (i, j) by the reference's lookup (Matrix_Sparse.cxx:
+        1054-1083; RowSymSparse reads (min, max), Matrix_SymSparse.cxx:
+        1013-1053).  Each call downloads the matrix: for inspection."""
+        if not (0 <= i < self.m and 0 <= j < self.n):
+            raise IndexError("WrongRow/WrongCol: index out of range")
+        return lookup(*self.download(), i, j, self.symmetric)
+
+    def Print(self):
+        """The dense matrix, row by row, tab-separated (Matrix_Sparse::Print,
+        Matrix_Sparse.cxx:1491-1499), from one download."""
+        ptr, ind, val = self.download()
+        for i in range(self.m):
+            print("".join(f"{lookup(ptr, ind, val, i, j, self.symmetric):g}\t"
+                          for j in range(self.n)))
 
     def download(self):
         """The stored arrays (ptr, ind, val) copied back to the host."""

@@ -102,3 +102,38 @@ def test_iteration_loop_interface(capsys):
     assert (c.GetNumberIteration(), c.GetFactor(), c.GetRestart()) == (0, 0.5, 30)
     it.SetNumberIteration(250)
     assert it.Finished(1.0) and it.ErrorCode() == -2   # max_iter outranks a failure
+
+
+def test_element_lookup_rule():
+    """RowSparse(i, j) and Print use the reference's lookup: the scan stops
+    at the first column >= j, so with unsorted rows an entry after a larger
+    column is not found, and a repeated column gives its first copy."""
+    import numpy as np
+    from seldon_b200.api import lookup
+    ptr = np.array([0, 3, 3, 5])
+    ind = np.array([2, 0, 1, 1, 1])
+    val = np.array([5.0, 6.0, 7.0, 8.0, 9.0])
+    assert lookup(ptr, ind, val, 0, 2) == 5.0
+    assert lookup(ptr, ind, val, 0, 0) == 0.0   # stored after column 2: not reached
+    assert lookup(ptr, ind, val, 0, 1) == 0.0
+    assert lookup(ptr, ind, val, 1, 0) == 0.0   # empty row
+    assert lookup(ptr, ind, val, 2, 1) == 8.0   # first of the repeated column
+    rng = np.random.default_rng(3)
+    for _ in range(200):                          # sorted, unique rows: the dense value
+        n = int(rng.integers(1, 9))
+        dense = np.where(rng.random((n, n)) < 0.4, rng.standard_normal((n, n)), 0.0)
+        rows = [np.nonzero(dense[i])[0] for i in range(n)]
+        p = np.concatenate([[0], np.cumsum([r.size for r in rows])])
+        c = np.concatenate(rows) if p[-1] else np.zeros(0, dtype=int)
+        v = dense[dense != 0]
+        for i in range(n):
+            for j in range(n):
+                assert lookup(p, c, v, i, j) == dense[i, j]
+        up = np.triu(dense)
+        rows = [np.nonzero(up[i])[0] for i in range(n)]
+        p = np.concatenate([[0], np.cumsum([r.size for r in rows])])
+        c = np.concatenate(rows) if p[-1] else np.zeros(0, dtype=int)
+        v = up[up != 0]
+        for i in range(n):
+            for j in range(n):
+                assert lookup(p, c, v, i, j, True) == up[min(i, j), max(i, j)]
