@@ -186,8 +186,8 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
   if (n == 0) return SB2_OK;
   if (A->full.sell.nslice < 0) return SB2_ERR_NOT_SUPPORTED;
   int kind = M ? precond_kind(M) : SB2_PRECOND_IDENTITY;
-  if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) return SB2_ERR_NOT_SUPPORTED;
+  if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
   const bool jac = (kind == SB2_PRECOND_JACOBI);
   SB2_TRY(ensure_fp32(A, jac));
   const SellOp<double> S64 = sell_op(A->full);
