@@ -120,13 +120,44 @@ def write_text(path, ptr, ind, val, sym=False):
                         for a, b, x in zip(r.tolist(), c.tolist(), v.tolist())))
 
 
-_INT_FIELDS = re.compile(r"[ +\-0-9]*")
+# `stream >> int` and `stream >> double` as libstdc++ extracts them: skip
+# white space, then an int is a sign and digits (within int32), and a double
+# takes the longest prefix of sign, digits, point, digits, exponent, which
+# must then be a whole finite number (so "nan", "inf", "1e400" and "1e"
+# fail).  The first failed extraction ends the reading.
+_WS = re.compile(r"\s*")
+_INT_PREFIX = re.compile(r"[+-]?[0-9]+")
+_FLOAT_PREFIX = re.compile(r"[+-]?[0-9]*(?:\.[0-9]*)?(?:[eE][+-]?[0-9]*)?")
+_FLOAT_WHOLE = r"[+-]?(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:[eE][+-]?[0-9]+)?"
+_FLOAT_TOKEN = re.compile(_FLOAT_WHOLE)
+# whole files of such tokens take the vectorised path
+_INT_FIELDS = re.compile(r"(?:[+-]?[0-9]+ )*[+-]?[0-9]+")
+_FLOAT_FIELDS = re.compile(f"(?:{_FLOAT_WHOLE} )*{_FLOAT_WHOLE}")
+
+
+def _extract_int(text, pos):
+    pos = _WS.match(text, pos).end()
+    m = _INT_PREFIX.match(text, pos)
+    if m is None:
+        return None, pos
+    v = int(m.group())
+    return (v if -2**31 <= v < 2**31 else None), m.end()
+
+
+def _extract_double(text, pos):
+    pos = _WS.match(text, pos).end()
+    m = _FLOAT_PREFIX.match(text, pos)
+    if not _FLOAT_TOKEN.fullmatch(m.group()):
+        return None, pos
+    x = float(m.group())
+    return (x if math.isfinite(x) else None), m.end()
 
 
 def read_text(path):
     """ReadCoordinateMatrix (Matrix_Sparse.cxx:1885-1950): 1-based triplets
-    (row, col, val) up to the first line that does not parse.  A row or
-    column below 1 raises ValueError (Seldon's IOError)."""
+    (row, col, val) read as `stream >> row >> col >> entry` reads them, up to
+    the first extraction that fails.  A row or column below 1 raises
+    ValueError (Seldon's IOError), for the first such entry in file order."""
     with open(path) as f:
         text = f.read()
     tok = text.split()
@@ -135,24 +166,35 @@ def read_text(path):
     # fields: parsed at once
     r = None
     if tok and len(tok) % 3 == 0 and _INT_FIELDS.fullmatch(
-            " ".join(tok[0::3]) + " " + " ".join(tok[1::3])):
+            " ".join(tok[0::3]) + " " + " ".join(tok[1::3])) and _FLOAT_FIELDS.fullmatch(
+            " ".join(tok[2::3])):
         try:
             a = np.fromstring(text, dtype=_F8, sep=" ").reshape(-1, 3)
         except ValueError:
             a = None
-        if a is not None and a.shape[0] == n3 and np.all(np.abs(a[:, :2]) < 2**31):
+        if (a is not None and a.shape[0] == n3 and np.all(np.abs(a[:, :2]) < 2**31)
+                and np.all(np.isfinite(a[:, 2]))):
             r, c, v = a[:, 0].astype(np.int64), a[:, 1].astype(np.int64), a[:, 2].copy()
     if r is not None:
-        for name, a in (("Row", r), ("Column", c)):
-            if a.size and a.min() < 1:
-                raise ValueError(f"{path}: {name} number should be greater than 0 but is equal "
-                                 f"to {int(a[np.argmax(a < 1)])}")
+        bad = (r < 1) | (c < 1)
+        if bad.any():
+            k = int(np.argmax(bad))
+            name, x = ("Row", r[k]) if r[k] < 1 else ("Column", c[k])
+            raise ValueError(f"{path}: {name} number should be greater than 0 but is equal "
+                             f"to {int(x)}")
         return r.astype(np.int32), c.astype(np.int32), v
     rows, cols, vals = [], [], []
-    for k in range(0, len(tok) - 2, 3):
-        try:
-            a, b, x = int(tok[k]), int(tok[k + 1]), float(tok[k + 2])
-        except ValueError:
+    pos = 0
+    while True:
+        # `stream >> row >> col >> entry` until an extraction fails
+        a, pos = _extract_int(text, pos)
+        if a is None:
+            break
+        b, pos = _extract_int(text, pos)
+        if b is None:
+            break
+        x, pos = _extract_double(text, pos)
+        if x is None:
             break
         if a < 1:
             raise ValueError(f"{path}: Row number should be greater than 0 but is equal to {a}")
@@ -246,6 +288,8 @@ def read_harwell_boeing(path):
     "(3D23.15)" format."""
     with open(path) as f:
         lines = f.read().split("\n")
+    if len(lines) < 4:
+        raise ValueError(f"{path}: incomplete Harwell-Boeing header")
     head2 = lines[1].split()
     head3 = lines[2].split()
     if len(head2) < 5 or len(head3) < 5:
@@ -262,8 +306,10 @@ def read_harwell_boeing(path):
     if nelt != 0 or typ[2] == "E":
         raise ValueError(f"{path}: elemental matrices are not supported")
     fmt = lines[3]
-    lw_ptr, ew_ptr = (int(t) for t in re.match(r"\s*\((\d+)I(\d+)\)", fmt[0:16]).groups())
-    lw_ind, ew_ind = (int(t) for t in re.match(r"\s*\((\d+)I(\d+)\)", fmt[16:32]).groups())
+    int_fmts = [re.match(r"\s*\((\d+)I(\d+)\)", fmt[a:a + 16]) for a in (0, 16)]
+    if None in int_fmts:
+        raise ValueError(f"{path}: pointer or index format {fmt[0:32]!r} could not be parsed")
+    (lw_ptr, ew_ptr), (lw_ind, ew_ind) = ((int(t) for t in f.groups()) for f in int_fmts)
     lw_val = ew_val = 0
     if typ[0] != "P":
         nums = [int(t) for t in re.split(r"[ (ABDEFGILOPZ*.)]+", fmt[32:48]) if t.isdigit()]
@@ -276,6 +322,8 @@ def read_harwell_boeing(path):
         nonlocal pos
         out = []
         for _ in range(nlines):
+            if pos >= len(lines):
+                raise ValueError(f"{path}: fewer lines than the header announces")
             line = lines[pos]
             pos += 1
             for j in range(per_line):

@@ -171,3 +171,64 @@ def test_harwell_boeing_reads_own_files(tmp_path):
     assert (m, n) == (81, 81)
     assert np.array_equal(cp, C.indptr) and np.array_equal(ri, C.indices)
     assert np.allclose(v, C.data, rtol=1e-15, atol=0)
+
+
+@pytest.mark.parametrize("text", [
+    "1 1 2.0\n2 99999999999 3.0\n3 3 1.0\n",      # an index past int32 ends the data
+    "1 1 nan\n2 2 1\n",                              # libstdc++ reads no nan ...
+    "1 1 2.5\n2 2 inf\n3 3 1\n",                     # ... nor inf
+    "1 1 2.5\n2 2 1e400\n3 3 1\n",                   # an overflowing value fails
+    "1 1 2.5\n2 2 1e-400\n3 3 1\n",                  # an underflowing one reads as 0
+    "1 1 1_0\n2 2 3\n",                              # the numeric prefix is taken
+    "1 2 0x10\n3 3 1\n",
+    "1 1 1e\n2 2 2\n",                               # an exponent without digits fails
+    "1.5 2 3\n",
+    "+1 +2 +.5\n2 1 -2.\n",
+    "1 1 5\n2 2\n",                                  # a trailing partial entry
+    "",
+])
+def test_text_read_like_seldon_stream(reference, oracle, tmp_path, text):
+    """ReadText on malformed files takes exactly the entries Seldon's
+    `stream >> row >> col >> entry` loop takes (the reference itself reads
+    the same file), before and after assembly."""
+    p = tmp_path / "t.txt"
+    p.write_text(text)
+    r, c, v = io.read_text(p)
+    want = reference.read_text(p)
+    if r.size == 0:  # nothing read: ReadText leaves a 0 x 0 matrix
+        assert want[:2] == (0, 0) and want[3].size == 0
+        return
+    got = oracle.coo_to_csr(r, c, v, 1, 0, 0, False)
+    assert got[:2] == want[:2]
+    for a, b in zip(got[2:], want[2:]):
+        assert np.array_equal(a, b)
+
+
+def test_damaged_text_and_hb_files_raise_value_error_only(tmp_path):
+    """Randomly damaged text and Harwell-Boeing files are either read or
+    refused with ValueError (Seldon's IOError), never another exception."""
+    import random
+    p, i, v = matgen.random_csr(30, 25, 0.1, seed=1)
+    txt, hb = tmp_path / "a.txt", tmp_path / "a.rua"
+    io.write_text(txt, p, i, v)
+    io.write_harwell_boeing(hb, 30, 25, p, i, v)
+    rnd = random.Random(0)
+    for path, reader in ((txt, io.read_text), (hb, io.read_harwell_boeing)):
+        base = path.read_bytes()
+        bad = tmp_path / ("bad" + path.suffix)
+        for _ in range(400):
+            b = bytearray(base)
+            for _ in range(rnd.randint(1, 6)):
+                k = rnd.randrange(len(b))
+                op = rnd.random()
+                if op < 0.4:
+                    b[k] = rnd.choice(b"0123456789 -+.eE\n\tx")
+                elif op < 0.7:
+                    del b[k:k + rnd.randint(1, 40)]
+                else:
+                    b[k:k] = rnd.choice([b"999999999", b"-1", b"nan", b"\n\n", b"1e308"])
+            bad.write_bytes(bytes(b))
+            try:
+                reader(bad)
+            except ValueError:
+                pass
