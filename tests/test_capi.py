@@ -137,3 +137,60 @@ def test_element_lookup_rule():
         for i in range(n):
             for j in range(n):
                 assert lookup(p, c, v, i, j, True) == up[min(i, j), max(i, j)]
+
+
+def test_preconditioner_handle_cache(monkeypatch):
+    """The Python preconditioners create one library handle per (matrix,
+    matrix handle, settings): repeated solves reuse it, a matrix whose handle
+    was replaced (Clear) gets a new one, changed settings rebuild it and free
+    the old one, and Clear / destruction free them all.  The library calls
+    are replaced by a recorder, so no device is needed."""
+    import numpy as np
+    from seldon_b200 import api
+    calls = {"create": 0, "destroy": 0}
+
+    class Recorder:
+        def _new(self, out, base):
+            calls["create"] += 1
+            ctypes.cast(out, ctypes.POINTER(ctypes.c_void_p))[0] = base + calls["create"]
+            return 0
+
+        def sb2_precond_create(self, A, kind, omega, nb, sym, out):
+            return self._new(out, 1000)
+
+        def sb2_precond_create_ilut(self, A, n, *rest):
+            return self._new(rest[-1], 2000)
+
+        def sb2_precond_destroy(self, h):
+            calls["destroy"] += 1
+            return 0
+
+    class Matrix:
+        symmetric = False
+        m = 4
+
+        def __init__(self, h):
+            self.handle = ctypes.c_void_p(h)
+
+    monkeypatch.setattr(api, "_L", Recorder())
+    A = Matrix(77)
+    J = api.JacobiPreconditioner()
+    assert J.handle_for(A).value == J.handle_for(A).value and calls["create"] == 1
+    A.handle = ctypes.c_void_p(78)
+    J.handle_for(A)
+    assert calls["create"] == 2
+    S = api.SorPreconditioner()
+    S.handle_for(A)
+    S.SetParameterRelaxation(1.3)
+    S.handle_for(A)
+    assert (calls["create"], calls["destroy"]) == (4, 1)
+    M = api.IlutPreconditioning()
+    M.SetFactor(np.array([0, 1, 2, 3, 4]), np.arange(4), np.ones(4), np.arange(4))
+    a, b, c = M.handle_for(A), M.handle_for(A), M.handle_for(None)
+    assert a.value == b.value != c.value and calls["create"] == 6
+    M.Clear()
+    assert calls["destroy"] == 3
+    del J, S
+    import gc
+    gc.collect()
+    assert calls["destroy"] == 6
