@@ -338,26 +338,30 @@ int sb2_batch_create(int nsys, const int* sys_row, const int* ptr, const int* in
                      const double* val, sb2_batch** out) try {
   if (!out || nsys < 0 || !sys_row || !ptr) return SB2_ERR_INVALID_VALUE;
   *out = nullptr;
-  const int m = sys_row[nsys];
-  if (sys_row[0] != 0 || m < 0) return SB2_ERR_INVALID_CSR;
-  const long long nnz = ptr[m];
-  if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
-  // validation: monotone row ranges, every entry inside its own system
-  std::vector<int> local(std::max<long long>(nnz, 1));
+  // validation, each pass reading only what the previous one proved in
+  // range: monotone system ranges from 0, then monotone row pointers from 0,
+  // then every entry inside its own system
+  if (sys_row[0] != 0) return SB2_ERR_INVALID_CSR;
   int maxrows = 0;
   for (int s = 0; s < nsys; s++) {
+    if (sys_row[s + 1] < sys_row[s]) return SB2_ERR_INVALID_CSR;
+    maxrows = std::max(maxrows, sys_row[s + 1] - sys_row[s]);
+  }
+  const int m = sys_row[nsys];
+  if (ptr[0] != 0) return SB2_ERR_INVALID_CSR;
+  for (int i = 0; i < m; i++)
+    if (ptr[i + 1] < ptr[i]) return SB2_ERR_INVALID_CSR;
+  const long long nnz = ptr[m];
+  if (nnz > 0 && (!ind || !val)) return SB2_ERR_INVALID_VALUE;
+  std::vector<int> local(std::max<long long>(nnz, 1));
+  for (int s = 0; s < nsys; s++) {
     const int a = sys_row[s], e = sys_row[s + 1];
-    if (e < a) return SB2_ERR_INVALID_CSR;
-    maxrows = std::max(maxrows, e - a);
-    for (int i = a; i < e; i++) {
-      if (ptr[i + 1] < ptr[i]) return SB2_ERR_INVALID_CSR;
+    for (int i = a; i < e; i++)
       for (int k = ptr[i]; k < ptr[i + 1]; k++) {
         if (ind[k] < a || ind[k] >= e) return SB2_ERR_INVALID_CSR;
         local[k] = ind[k] - a;
       }
-    }
   }
-  if (ptr[0] != 0) return SB2_ERR_INVALID_CSR;
   std::vector<int> order(nsys);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int p, int q) {

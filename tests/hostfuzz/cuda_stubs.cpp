@@ -55,3 +55,14 @@ cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) { *s = nullptr;
 cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
 }
 
+extern "C" {
+cudaError_t cudaEventCreate(cudaEvent_t* e) { *e = nullptr; return cudaSuccess; }
+cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t) { return cudaSuccess; }
+cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
+cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) { *ms = 1.0f; return cudaSuccess; }
+cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(int* n, const void*, int, size_t,
+                                                                   unsigned) {
+  *n = 1;
+  return cudaSuccess;
+}
+}

@@ -1,11 +1,12 @@
 """The library's host code under AddressSanitizer and UBSan, on a machine
-without a GPU.  Three drivers in tests/hostfuzz feed it random well-formed
+without a GPU.  Four drivers in tests/hostfuzz feed it random well-formed
 and malformed inputs:
 
 - sb2_csr_create's validator, symmetric expansion and layouts;
 - the ILUT apply's planning (sb2_precond_create_ilut), with an independent
   check that every accepted factor's indices are in range;
-- the host ILUT factorization (sb2_ilut_factor, sb2_ilut_factor_sym).
+- the host ILUT factorization (sb2_ilut_factor, sb2_ilut_factor_sym);
+- sb2_batch_create's validation of the systems' CSR arrays.
 
 Host memory operations stand in for the CUDA runtime calls of that code
 (tests/hostfuzz/cuda_stubs.cpp), and no kernel runs."""
@@ -66,6 +67,13 @@ def test_ilut_plan_host_code(tmp_path):
     _clean(out)
     planned, refused = int(out.split()[1]), int(out.split()[3])
     assert planned > 500 and refused > 500
+
+
+def test_batch_create_host_code(tmp_path):
+    out = _run([_driver(str(tmp_path), "fuzz_batch"), "3000"], str(tmp_path))
+    _clean(out)
+    created, refused = int(out.split()[1]), int(out.split()[3])
+    assert created > 500 and refused > 300
 
 
 def test_ilut_factor_host_code(tmp_path):
