@@ -458,7 +458,10 @@ int sb2_grad_pattern(const sb2_csr* A, double alpha, const double* lambda, const
 
 /* grad[e] = -(lambda[i] - lambda[j]) * (x[i] - x[j]) for edges e = (ei[e], ej[e]):
  * dL/dtheta_e of a weighted graph Laplacian (A_ii, A_jj += theta_e,
- * A_ij = A_ji -= theta_e). */
+ * A_ij = A_ji -= theta_e).  ei, ej, lambda, x and grad are device arrays;
+ * the call takes no vertex count, so every ei[e] and ej[e] must already lie
+ * in [0, length of lambda and x): the indices are not checked (the Python
+ * autograd wrapper builds them from the graph it was given). */
 int sb2_grad_edges(int nedges, const int* ei, const int* ej, const double* lambda,
                    const double* x, double* grad, void* stream);
 
