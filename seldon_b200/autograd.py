@@ -113,6 +113,13 @@ class GraphLaplacian:
 
     def __init__(self, n, edges, shift):
         edges = np.asarray(edges, dtype=np.int64)
+        if edges.size == 0:
+            edges = edges.reshape(0, 2)
+        if edges.ndim != 2 or edges.shape[1] != 2:
+            raise ValueError("WrongDim: edges must be an (E, 2) array of vertex pairs")
+        if edges.size and (edges.min() < 0 or edges.max() >= n):
+            # sb2_grad_edges reads lambda and x through these indices unchecked
+            raise ValueError(f"WrongRow: an edge index lies outside [0, {n})")
         self.n, self.shift = int(n), float(shift)
         self.E = edges.shape[0]
         rows = np.concatenate([edges[:, 0], edges[:, 1], np.arange(n)])

@@ -194,3 +194,12 @@ def test_preconditioner_handle_cache(monkeypatch):
     import gc
     gc.collect()
     assert calls["destroy"] == 6
+
+
+def test_graph_edges_checked_before_the_device():
+    """GraphLaplacian refuses malformed or out-of-range edges on the host
+    (the gradient kernel reads through them unchecked)."""
+    from seldon_b200.autograd import GraphLaplacian
+    for edges in ([[0, 3]], [[-1, 1]], [[0, 1, 2]]):
+        with pytest.raises(ValueError):
+            GraphLaplacian(3, edges, 0.1)
