@@ -393,11 +393,20 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
  * n <= 131072 rows (about 3.2 MB, held on every GPU that loads the library
  * until the process exits); larger systems are rejected with
  * SB2_ERR_INVALID_VALUE.  The first call on a device looks up that array's
- * device address, so make it before any stream capture.  All calls on a
- * device share the one array: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialized by the caller.  Iteration
- * count, error code and last residual are reported; no residual history.
- * Same arithmetic and results as sb2_cg with M == NULL. */
+ * device address, so make it before any stream capture.  The address is
+ * kept for the life of the process: cudaDeviceReset destroys the array with
+ * the context, and this entry point must not be called on that device
+ * afterwards (matrix handles made before the reset are gone too).  All
+ * calls on a device share the one array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialized by the
+ * caller.  The call returns after the solve has finished: it reads the
+ * result record back to the host.  Iteration count, error code and last
+ * residual are reported; no residual history.
+ * It runs the persistent CG kernel of sb2_cg (M == NULL).  sb2_cg runs that
+ * same kernel, and gives the same bits, when the system is below the chained
+ * size (sb2_krylov_set_config) and its cluster-resident form is off
+ * (sb2_krylov_set_cluster(0)); with the cluster form on, sb2_cg groups its
+ * sums by cluster rank and agrees to rounding only. */
 int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
                    const sb2_iter_params* params, sb2_iter_result* result, void* stream);
 
@@ -530,8 +539,19 @@ int sb2_krylov_set_config(int chain_min_n);
 int sb2_krylov_set_cluster(int on);
 
 /* Device-side wait limit for the fused solvers' grid barriers, in
- * milliseconds (default 2000).  Returns the previous value. */
+ * milliseconds (default 2000).  Values <= 0 leave it unchanged.  Returns the
+ * previous value (rounded up to whole milliseconds).  No counterpart in the
+ * reference (the reference runs on the host and never waits on a device). */
 int sb2_set_wait_limit_ms(int ms);
+
+/* The same limit in microseconds (>= 1; values <= 0 leave it unchanged);
+ * returns the previous value in microseconds.  A limit below the time one
+ * CTA may wait for the slowest at a grid barrier makes the fused solvers end
+ * with SB2_ERR_TIMEOUT: every CTA leaves the kernel, the context stays
+ * usable, and the next call with a longer limit solves normally.  The TMA
+ * product's ring waits keep a floor of 1 s whatever this limit is.  No
+ * counterpart in the reference. */
+int sb2_set_wait_limit_us(int us);
 
 #ifdef __cplusplus
 }

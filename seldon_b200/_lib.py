@@ -139,6 +139,7 @@ _PROTOS = [
     ("sb2_memcpy", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_size_t, c_void_p]),
     ("sb2_stream_sync", ctypes.c_int, [c_void_p]),
     ("sb2_set_wait_limit_ms", ctypes.c_int, [ctypes.c_int]),
+    ("sb2_set_wait_limit_us", ctypes.c_int, [ctypes.c_int]),
     ("sb2_csr_create", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p,
       ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_void_p)]),

@@ -750,7 +750,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   // per restart
   const int hcap = std::max(hist_cap, 0) + 1;
   SB2_TRY(alloc_scratch(s, n, nvec, grid, hcap, &S));
-  Persist P{S.sync, S.partials, (unsigned long long)g_wait_limit_ms * 1000000ull};
+  Persist P{S.sync, S.partials, barrier_wait_ns()};
   History H{S.hist, S.hist_it, hcap};
   IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null};
   OpArgs op = op_args(A, diag);
@@ -1494,7 +1494,7 @@ static int cg_noalloc(const sb2_csr* A, double* x, const double* b, const sb2_it
   int* hist_it = reinterpret_cast<int*>(hist + 8);
   // the barrier word and the result record must start at zero on every call
   SB2_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(double) * 128, s));
-  Persist P{sync, partials, (unsigned long long)g_wait_limit_ms * 1000000ull};
+  Persist P{sync, partials, barrier_wait_ns()};
   History H{hist, hist_it, 1};
   IterArgs it{prm->tol, prm->max_iter, std::max(prm->restart, 1), prm->init_guess_null};
   OpArgs op = op_args(A, nullptr);

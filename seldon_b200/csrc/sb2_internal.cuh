@@ -188,7 +188,14 @@ bool release_owned(void* p, cudaError_t* err);
 int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
                 double* y, bool overwrite, cudaStream_t s);
 
-extern std::atomic<int> g_wait_limit_ms;
+// Limit of the persistent solvers' bounded grid-barrier waits, microseconds.
+extern std::atomic<long long> g_wait_limit_us;
+inline unsigned long long barrier_wait_ns() { return (unsigned long long)g_wait_limit_us.load() * 1000ull; }
+// The TMA product's ring waits (bulk copies in flight) never use less than 1 s.
+inline unsigned long long ring_wait_ns() {
+  const unsigned long long ns = barrier_wait_ns();
+  return ns < 1000000000ull ? 1000000000ull : ns;
+}
 
 // ----------------------------------------------------------------- device code
 

@@ -141,7 +141,7 @@ static int launch_tma(const CsrArrays& a, double alpha, const double* x, double 
   const int g = std::min(a.tma.nblk, per_sm * num_sms(dev));
   TmaOp<double> op{a.d_ptr, a.d_ind, a.d_val, a.tma.d_desc, a.tma.nblk, a.rows};
   spmv_tma_kernel<NT, S><<<g, NT, smem, s>>>(op, alpha, x, beta, y, overwrite, status,
-                                             (unsigned long long)g_wait_limit_ms * 1000000ull);
+                                             ring_wait_ns());
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
 }
@@ -294,15 +294,47 @@ int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
   std::lock_guard<std::mutex> g(A->host_mu);
   const size_t len = (size_t)std::max(std::max(A->m, A->n), 1);
   if (!A->s_in) {
+    // Everything is created into locals and published only when all of it
+    // exists; a failure part-way releases what was made, so a later call
+    // starts the set-up afresh without leaking.
+    struct Pipe {
+      double *bx[2] = {nullptr, nullptr}, *by[2] = {nullptr, nullptr};
+      cudaEvent_t ein[2] = {nullptr, nullptr}, ekern[2] = {nullptr, nullptr},
+                  eout[2] = {nullptr, nullptr};
+      cudaStream_t sin = nullptr, sout = nullptr;
+      bool keep = false;
+      ~Pipe() {
+        if (keep) return;
+        for (int i = 0; i < 2; i++) {
+          if (bx[i]) cudaFree(bx[i]);
+          if (by[i]) cudaFree(by[i]);
+          if (ein[i]) cudaEventDestroy(ein[i]);
+          if (ekern[i]) cudaEventDestroy(ekern[i]);
+          if (eout[i]) cudaEventDestroy(eout[i]);
+        }
+        if (sin) cudaStreamDestroy(sin);
+        if (sout) cudaStreamDestroy(sout);
+      }
+    } p;
     for (int i = 0; i < 2; i++) {
-      SB2_CUDA_TRY(cudaMalloc(&A->d_bx[i], sizeof(double) * len));
-      SB2_CUDA_TRY(cudaMalloc(&A->d_by[i], sizeof(double) * len));
-      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_in[i], cudaEventDisableTiming));
-      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_kern[i], cudaEventDisableTiming));
-      SB2_CUDA_TRY(cudaEventCreateWithFlags(&A->e_out[i], cudaEventDisableTiming));
+      SB2_CUDA_TRY(cudaMalloc(&p.bx[i], sizeof(double) * len));
+      SB2_CUDA_TRY(cudaMalloc(&p.by[i], sizeof(double) * len));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&p.ein[i], cudaEventDisableTiming));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&p.ekern[i], cudaEventDisableTiming));
+      SB2_CUDA_TRY(cudaEventCreateWithFlags(&p.eout[i], cudaEventDisableTiming));
     }
-    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_out, cudaStreamNonBlocking));
-    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_in, cudaStreamNonBlocking));
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&p.sout, cudaStreamNonBlocking));
+    SB2_CUDA_TRY(cudaStreamCreateWithFlags(&p.sin, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+      A->d_bx[i] = p.bx[i];
+      A->d_by[i] = p.by[i];
+      A->e_in[i] = p.ein[i];
+      A->e_kern[i] = p.ekern[i];
+      A->e_out[i] = p.eout[i];
+    }
+    A->s_out = p.sout;
+    A->s_in = p.sin;
+    p.keep = true;
   }
   // the copy streams start after the work already queued on the caller's stream
   SB2_CUDA_TRY(cudaEventRecord(A->e_kern[0], s));

@@ -1,11 +1,13 @@
 // Status codes, device queries and per-stream reduction scratch.
+#include <algorithm>
+#include <climits>
 #include <cstdio>
 
 #include "sb2_internal.cuh"
 
 namespace sb2 {
 
-std::atomic<int> g_wait_limit_ms{2000};
+std::atomic<long long> g_wait_limit_us{2000000};
 
 int map_cuda_error(cudaError_t e) {
   if (e == cudaSuccess) return SB2_OK;
@@ -184,9 +186,15 @@ int sb2_stream_sync(void* stream) try {
 } SB2_CATCH
 
 int sb2_set_wait_limit_ms(int ms) try {
-  int old = sb2::g_wait_limit_ms;
-  if (ms > 0) sb2::g_wait_limit_ms = ms;
-  return old;
+  const long long old_us = sb2::g_wait_limit_us;
+  if (ms > 0) sb2::g_wait_limit_us = (long long)ms * 1000;
+  return (int)std::min<long long>((old_us + 999) / 1000, INT_MAX);
+} SB2_CATCH
+
+int sb2_set_wait_limit_us(int us) try {
+  const long long old_us = sb2::g_wait_limit_us;
+  if (us > 0) sb2::g_wait_limit_us = us;
+  return (int)std::min<long long>(old_us, INT_MAX);
 } SB2_CATCH
 
 }  // extern "C"

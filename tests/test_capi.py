@@ -43,6 +43,20 @@ def test_status_strings_without_gpu():
     assert lib.sb2_status_string(_lib.SB2_ERR_HOST) == b"host-side failure"
 
 
+def test_wait_limit_setters_round_trip():
+    """ms and us setters share one limit; values <= 0 leave it unchanged."""
+    from seldon_b200 import _lib
+    L = _lib.load()
+    old = L.sb2_set_wait_limit_us(2500)
+    try:
+        assert L.sb2_set_wait_limit_us(0) == 2500
+        assert L.sb2_set_wait_limit_ms(-1) == 3  # 2500 us, rounded up
+        assert L.sb2_set_wait_limit_ms(7) == 3
+        assert L.sb2_set_wait_limit_us(-5) == 7000
+    finally:
+        L.sb2_set_wait_limit_us(old)
+
+
 _OOM_CHILD = r"""
 import ctypes, re, resource, sys
 import numpy as np

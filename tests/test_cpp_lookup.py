@@ -8,12 +8,14 @@ import subprocess
 
 import pytest
 
+from oracle.refpath import have_reference, reference_tree
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPP = os.path.join(ROOT, "tests", "cpp")
-REF = os.environ.get("SELDON_REF", "/root/reference")
+REF = reference_tree()
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "Seldon.hxx")),
+@pytest.mark.skipif(not have_reference(),
                     reason="the reference's headers are not present")
 def test_lookup_matches_seldon():
     subprocess.run(["make", "-s", "_bin/lookup_test", f"REF={REF}"], cwd=CPP, check=True,
