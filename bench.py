@@ -56,6 +56,8 @@ def parse():
                         "(default all)")
     p.add_argument("--cpu-seconds", type=float, default=8.0,
                    help="bounded CPU-baseline sample (seconds of work)")
+    p.add_argument("--no-cpu-solves", action="store_true",
+                   help="skip the reference's host solves beside the solver extras")
     return p.parse_args()
 
 
@@ -354,7 +356,8 @@ def run_ours(args, rank, world, local):
 
     extras = {}
     if rank == 0 and not args.no_extras:
-        extras = run_extras(api, matgen, torch, dev, args.extras)
+        extras = run_extras(api, matgen, torch, dev, args.extras,
+                            cpu=(world == 1 and not args.no_cpu_solves))
 
     cpu = None
     if rank == 0 and world == 1:
@@ -393,9 +396,12 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
-def run_extras(api, matgen, torch, dev, which="all"):
+def run_extras(api, matgen, torch, dev, which="all", cpu=True):
     """Time-to-solution figures on the other configurations (device-timed).
-    `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, or all."""
+    `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, assemble,
+    ilu0, or all.  With `cpu`, the reference's own solvers then run on the
+    host cores on the same systems (after every device measurement, so they
+    do not disturb it) and each record gains a `cpu_reference` entry."""
     out = {}
     names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint", "assemble", "ilu0"}
     want = names if which == "all" else set(w.strip() for w in which.split(","))
@@ -416,53 +422,130 @@ def run_extras(api, matgen, torch, dev, which="all"):
             best = ms if best is None else min(best, ms)
         return best, r
 
-    rng = np.random.default_rng(2024)
-    if "c1" in want:
-        out.update(extra_c1(api, matgen, torch, dev, timed, rng))
-    if "c3" in want:
-        out.update(extra_c3(api, matgen, torch, dev, timed, rng))
-    if "gmres" in want:
-        out.update(extra_gmres(api, matgen, torch, dev, timed, rng))
+    jobs = []  # (record key, function run on the host afterwards)
+    # records whose CPU comparison matters most go last: the line's tail is
+    # what a truncated log keeps
     if "zipf" in want:
         out.update(extra_zipf(api, matgen, torch, dev, timed))
     if "assemble" in want:
         out.update(extra_assemble(api, matgen, torch, dev, timed))
     if "ilu0" in want:
         out.update(extra_ilu0(api, matgen, torch, dev, timed))
-    if "batch" in want:
-        out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed)
     if "adjoint" in want:
         out["adjoint_aniso512"] = run_adjoint(matgen, torch, dev, timed)
+    if "batch" in want:
+        out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed, jobs)
+    if "c1" in want:
+        out.update(extra_c1(api, matgen, torch, dev, timed, jobs))
+    if "gmres" in want:
+        out.update(extra_gmres(api, matgen, torch, dev, timed, jobs))
+    if "c3" in want:
+        out.update(extra_c3(api, matgen, torch, dev, timed, jobs))
+    if cpu and jobs:
+        run_cpu_jobs(out, jobs)
     return out
 
 
-def extra_c1(api, matgen, torch, dev, timed, rng):
+def _reference_fast():
+    """The reference compiled at -O3 from its headers (oracle/_ref); the
+    parity build (for residual checks) beside it."""
+    from oracle.pyoracle import REF_FAST_SO, REF_SO, Reference
+    if not (Reference.available(REF_FAST_SO) and Reference.available(REF_SO)):
+        return None, None
+    return Reference(REF_FAST_SO), Reference(REF_SO)
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_cpu_jobs(out, jobs):
+    """Run the reference's host solves, one thread each (Seldon is
+    single-threaded; ctypes releases the interpreter lock during the call),
+    all at once, and attach each result to its record.  Jobs that use several
+    threads themselves (the batch) run afterwards, alone."""
+    single = [(k, f) for k, f, multi in jobs if not multi]
+    multi = [(k, f) for k, f, multi in jobs if multi]
+    results = {}
+
+    def run(key, fn):
+        try:
+            results[key] = fn()
+        except Exception as e:  # the checker is optional here
+            results[key] = {"unavailable": str(e)[:160]}
+    ths = [threading.Thread(target=run, args=kf) for kf in single]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    for k, f in multi:
+        run(k, f)
+    for k, r in results.items():
+        out[k]["cpu_reference"] = r
+
+
+def _cpu_solve(which, ptr, ind, val, b, x_gpu, sym=False, precond=0, restart=10, tol=1e-10,
+               max_iter=20000):
+    """The reference's solver on the host (one core), timed; its x compared
+    with the device's, both residuals recomputed by the reference's MltAdd."""
+    fast, parity = _reference_fast()
+    if fast is None:
+        return {"unavailable": "oracle/_ref is not built"}
+    n = ptr.size - 1
+    t0 = time.perf_counter()
+    xr, code, it = fast.solve(which, ptr, ind, val, b, sym=sym, precond=precond, tol=tol,
+                              max_iter=max_iter, restart=restart)
+    dt = time.perf_counter() - t0
+
+    def relres(x):
+        r = parity.mltadd(n, n, ptr, ind, val, -1.0, x, 1.0, b, sym=sym)
+        return float(np.linalg.norm(r) / np.linalg.norm(b))
+    return {"ms": round(dt * 1e3, 1), "iterations": it, "error_code": code,
+            "true_rel_residual": relres(xr), "gpu_true_rel_residual": relres(x_gpu),
+            "forward_diff_gpu_vs_reference": float(np.linalg.norm(x_gpu - xr) /
+                                                  np.linalg.norm(xr)),
+            "cores": 1, "host_threads": host_threads(), "cpu": cpu_model(),
+            "build": "Seldon's templates from the reference's headers, g++ -O3"}
+
+
+def extra_c1(api, matgen, torch, dev, timed, jobs):
     """CG, identity, 100^2 Laplacian stored RowSymSparse."""
     ptr, ind, val = matgen.lap2d(100)
     n = ptr.size - 1
-    xs = rng.uniform(-1, 1, n)
-    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
-    S = api.RowSymSparse(n, *matgen.upper(ptr, ind, val))
+    xs = np.random.default_rng(100).uniform(-1, 1, n)
+    bh = matgen.matvec(ptr, ind, val, xs)
+    b = torch.as_tensor(bh, device=dev)
+    up, ui, uv = matgen.upper(ptr, ind, val)
+    S = api.RowSymSparse(n, up, ui, uv)
 
     def cg_c1():
         X = torch.zeros(n, dtype=torch.float64, device=dev)
         it = api.Iteration(10000, 1e-10)
         it.HideMessages()
         api.Cg(S, X, b, api.Preconditioner_Base(), it)
-        return it
+        return it, X
     cg_c1()
-    ms, it = timed(cg_c1, reps=5)
+    ms, (it, X) = timed(cg_c1, reps=5)
+    x = X.cpu().numpy()
+    jobs.append(("cg_lap2d_100", lambda: _cpu_solve("cg", up, ui, uv, bh, x, sym=True), False))
     return {"cg_lap2d_100": {"ms": round(ms, 3), "iterations": it.GetNumberIteration(),
-                             "rel_residual": it.history[-1][1]}}
+                             "rel_residual": it.history[-1][1], "timing": "best of 5"}}
 
 
-def extra_c3(api, matgen, torch, dev, timed, rng):
+def extra_c3(api, matgen, torch, dev, timed, jobs):
     """FP64 CG and FP32/FP64 iterative refinement on the 192^3 Poisson problem."""
     out = {}
     ptr, ind, val = matgen.poisson3d(192)
     n = ptr.size - 1
-    xs = rng.uniform(-1, 1, n)
-    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
+    xs = np.random.default_rng(192).uniform(-1, 1, n)
+    bh = matgen.matvec(ptr, ind, val, xs)
+    b = torch.as_tensor(bh, device=dev)
     A = api.RowSparse(n, n, ptr, ind, val)
 
     def cg_c3():
@@ -481,6 +564,8 @@ def extra_c3(api, matgen, torch, dev, timed, rng):
                                  "gbs_per_iteration_model": round(
                                      per_it * it.GetNumberIteration() / (ms * 1e-3) / 1e9, 1),
                                  "timing": "best of 3"}
+    jobs.append(("cg_fp64_poisson192",
+                 lambda: _cpu_solve("cg", ptr, ind, val, bh, X64), False))
     # mixed precision: FP32 inner CG, FP64 outer residual/update to 1e-10
     for key, restarted, inner in (("ir_reliable_poisson192", False, 1e-2),
                                   ("ir_restarted_poisson192", True, 1e-5)):
@@ -502,15 +587,19 @@ def extra_c3(api, matgen, torch, dev, timed, rng):
                     "forward_error_vs_fp64_cg": float(np.linalg.norm(Xi - X64) / np.linalg.norm(X64)),
                     "forward_error_vs_xstar": float(np.linalg.norm(Xi - xs) / np.linalg.norm(xs)),
                     "speedup_vs_fp64_cg": round(ms / ms_ir, 3), "timing": "best of 3"}
+    out["ir_reliable_poisson192"]["config_deviation"] = (
+        "reliable updates, correction each time the FP32 residual drops by 1e-2 "
+        "(the configuration's inner tolerance 1e-5 is ir_restarted_poisson192)")
     return out
 
 
-def extra_gmres(api, matgen, torch, dev, timed, rng):
+def extra_gmres(api, matgen, torch, dev, timed, jobs):
     """GMRES(30) + Jacobi on the 128^3 convection-diffusion problem."""
     ptr, ind, val = matgen.convdiff3d(GRID)
     n = ptr.size - 1
-    xs = rng.uniform(-1, 1, n)
-    b = torch.as_tensor(matgen.matvec(ptr, ind, val, xs), device=dev)
+    xs = np.random.default_rng(GRID).uniform(-1, 1, n)
+    bh = matgen.matvec(ptr, ind, val, xs)
+    b = torch.as_tensor(bh, device=dev)
     A = api.RowSparse(n, n, ptr, ind, val)
 
     def gm():
@@ -519,10 +608,13 @@ def extra_gmres(api, matgen, torch, dev, timed, rng):
         it.HideMessages()
         it.SetRestart(30)
         api.Gmres(A, X, b, J, it)
-        return it
+        return it, X
     J = api.JacobiPreconditioner()
     gm()  # warm-up: the Krylov basis (0.5 GB) is mapped into the pool once
-    ms, it = timed(gm)
+    ms, (it, X) = timed(gm)
+    x = X.cpu().numpy()
+    jobs.append(("gmres30_jacobi_convdiff128",
+                 lambda: _cpu_solve("gmres", ptr, ind, val, bh, x, precond=1, restart=30), False))
     return {"gmres30_jacobi_convdiff128": {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
                                            "rel_residual": it.history[-1][1]}}
 
@@ -632,9 +724,11 @@ def extra_ilu0(api, matgen, torch, dev, timed):
     return {"ilu0_conv128": out}
 
 
-def run_batch(api, matgen, torch, dev, timed, nsys=4096, sample_every=8):
+def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every=8):
     """4096 shifted 2D Laplacians (side uniform in [8,140]) in one persistent
-    launch, against a loop of plain FP64 CG calls over every 8th system."""
+    launch, against a loop of plain FP64 CG calls over every 8th system; on
+    the host, the reference's Cg on the same sample, K systems at a time on K
+    threads."""
     from seldon_b200 import _lib
     rng = np.random.default_rng(7)
     gs = rng.integers(8, 141, nsys)
@@ -689,7 +783,58 @@ def run_batch(api, matgen, torch, dev, timed, nsys=4096, sample_every=8):
                            "est_ms_all": round(per * nsys, 1)}
     out["speedup_mixed_vs_loop"] = round(out["loop_fp64_cg"]["est_ms_all"] / out["mixed"]["ms"], 1)
     Bt.close()
+    if jobs is not None:
+        sample = list(range(0, nsys, sample_every))
+        jobs.append(("batch_lap2d_4096",
+                     lambda: _cpu_batch(systems, rhs, sample, nsys, X.cpu().numpy(),
+                                        np.concatenate([[0], np.cumsum([s[0].size - 1 for s in systems])])),
+                     True))
     return out
+
+
+def _cpu_batch(systems, rhs, sample, nsys, x_gpu, offs, tol=1e-9):
+    """The reference's FP64 Cg on the sampled systems, K independent solves at
+    a time on K host threads (one system per thread), timed as a whole."""
+    fast, parity = _reference_fast()
+    if fast is None:
+        return {"unavailable": "oracle/_ref is not built"}
+    K = max(1, min(host_threads(), 64))
+    todo = list(sample)
+    lock = threading.Lock()
+    res = {}
+
+    def worker():
+        while True:
+            with lock:
+                if not todo:
+                    return
+                s = todo.pop()
+            p, i, v = systems[s]
+            xr, code, it = fast.solve("cg", p, i, v, rhs[s], tol=tol, max_iter=10000)
+            res[s] = (xr, code, it)
+    ths = [threading.Thread(target=worker) for _ in range(K)]
+    t0 = time.perf_counter()
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    wall = time.perf_counter() - t0
+    worst_rel, worst_fd, conv = 0.0, 0.0, 0
+    for s, (xr, code, it) in res.items():
+        p, i, v = systems[s]
+        n = p.size - 1
+        r = parity.mltadd(n, n, p, i, v, -1.0, xr, 1.0, rhs[s])
+        worst_rel = max(worst_rel, float(np.linalg.norm(r) / np.linalg.norm(rhs[s])))
+        xg = x_gpu[offs[s]:offs[s + 1]]
+        worst_fd = max(worst_fd, float(np.linalg.norm(xg - xr) / np.linalg.norm(xr)))
+        conv += int(code == 0)
+    per_s = len(sample) / wall
+    return {"systems": len(sample), "threads": K, "wall_ms": round(wall * 1e3, 1),
+            "systems_per_s": round(per_s, 1), "est_ms_all": round(nsys / per_s * 1e3, 1),
+            "converged": conv, "max_true_rel_residual": worst_rel,
+            "max_forward_diff_gpu_mixed_vs_reference": worst_fd, "cpu": cpu_model(),
+            "sample": f"every {nsys // len(sample)}th system, FP64 Cg to {tol}, "
+                      f"{K} concurrent single-threaded solves"}
 
 
 def run_adjoint(matgen, torch, dev, timed, g=512, n_fd=64, h=1e-6):

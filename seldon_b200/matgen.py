@@ -98,17 +98,24 @@ def zipf_csr(n, seed=0, a=1.5, lo=1, hi=2000):
     cols = rng.integers(0, n, rows.size, dtype=np.int64)
     keys = rows * n + cols
     keys = keys[rows != cols]
-    keys = np.unique(keys)
+    # sorted distinct keys: an in-place sort and a neighbour test (the same
+    # array np.unique gives, without its cost on tens of millions of keys)
+    keys.sort()
+    if keys.size:
+        first = np.empty(keys.size, dtype=bool)
+        first[0] = True
+        np.not_equal(keys[1:], keys[:-1], out=first[1:])
+        keys = keys[first]
     r = keys // n
     c = keys % n
     v = rng.standard_normal(keys.size)
     absum = np.bincount(r, weights=np.abs(v), minlength=n)
+    # the diagonal entries merged in column order (no off-diagonal key equals
+    # a diagonal one)
     dkeys = np.arange(n, dtype=np.int64) * (n + 1)
-    allk = np.concatenate([keys, dkeys])
-    allv = np.concatenate([v, 1.0 + absum])
-    order = np.argsort(allk, kind="stable")
-    allk = allk[order]
-    allv = allv[order]
+    at = np.searchsorted(keys, dkeys)
+    allk = np.insert(keys, at, dkeys)
+    allv = np.insert(v, at, 1.0 + absum)
     r = allk // n
     ptr = np.zeros(n + 1, dtype=np.int64)
     np.cumsum(np.bincount(r, minlength=n), out=ptr[1:])
