@@ -593,30 +593,101 @@ def extra_c3(api, matgen, torch, dev, timed, jobs):
     return out
 
 
+def gmres_bytes(n, nnz, iterations, m, vw, mw, variant):
+    """Least HBM traffic of a GMRES(m) solve that took `iterations` Arnoldi
+    steps, restarts every m steps: per step i of a cycle the product
+    (nnz*(mw+4) + 4(n+1) + 2*n*vw) plus the orthogonalization's vector
+    passes, and per restart the FP64 residual product and the update
+    x += V y.  vw: basis element bytes; mw: matrix value bytes.
+      mgs   Seldon's modified Gram-Schmidt (Gmres.cxx:127-132): pass k reads
+            w, V_k and V_{k+1} and writes w (4 vectors), i+1 passes, then
+            V_{i+1} = w / h (2 vectors)
+      cgs2  three passes over V_0..V_i (dots; projection and dots; projection
+            and norm), the write of V_i, and w read and written, w read and u
+            written (5 vectors); the second read of V in the projection-and-
+            dots pass comes from cache"""
+    spmv = nnz * (mw + 4) + 4 * (n + 1) + 2 * n * vw
+    spmv64 = nnz * 12 + 4 * (n + 1) + 3 * n * 8  # residual: x in, b in, r out
+    total, done = 0, 0
+    while done < iterations:
+        steps = min(m, iterations - done)
+        for i in range(steps):
+            vec = 4 * (i + 1) + 2 if variant == "mgs" else 3 * (i + 1) + 5
+            total += spmv + vec * n * vw
+        total += spmv64 + steps * n * vw + 2 * n * 8
+        done += steps
+    return total
+
+
 def extra_gmres(api, matgen, torch, dev, timed, jobs):
-    """GMRES(30) + Jacobi on the 128^3 convection-diffusion problem."""
+    """GMRES(30) + Jacobi on the 128^3 convection-diffusion problem: Seldon's
+    modified Gram-Schmidt order, the CGS2 variant, and the iterative
+    refinement whose inner solve is GMRES(30) with an FP32 basis."""
     ptr, ind, val = matgen.convdiff3d(GRID)
     n = ptr.size - 1
     xs = np.random.default_rng(GRID).uniform(-1, 1, n)
     bh = matgen.matvec(ptr, ind, val, xs)
     b = torch.as_tensor(bh, device=dev)
     A = api.RowSparse(n, n, ptr, ind, val)
-
-    def gm():
-        X = torch.zeros(n, dtype=torch.float64, device=dev)
-        it = api.Iteration(20000, 1e-10)
-        it.HideMessages()
-        it.SetRestart(30)
-        api.Gmres(A, X, b, J, it)
-        return it, X
     J = api.JacobiPreconditioner()
-    gm()  # warm-up: the Krylov basis (0.5 GB) is mapped into the pool once
-    ms, (it, X) = timed(gm)
+    peak, _ = measured_peak()
+
+    def gm(orth):
+        def run():
+            X = torch.zeros(n, dtype=torch.float64, device=dev)
+            it = api.Iteration(20000, 1e-10)
+            it.HideMessages()
+            it.SetRestart(30)
+            api.Gmres(A, X, b, J, it, orthogonalization=orth)
+            return it, X
+        return run
+
+    def host_relres(x):
+        return float(np.linalg.norm(matgen.matvec(ptr, ind, val, x) - bh) / np.linalg.norm(bh))
+    out = {}
+    xs_gpu = {}
+    for key, orth in (("gmres30_jacobi_convdiff128", "mgs"), ("gmres30_cgs2_jacobi_convdiff128", "cgs2")):
+        gm(orth)()  # warm-up: the Krylov basis (0.5 GB) is mapped into the pool once
+        ms, (it, X) = timed(gm(orth), reps=2)
+        x = X.cpu().numpy()
+        xs_gpu[orth] = x
+        nbytes = gmres_bytes(n, ind.size, it.GetNumberIteration(), 30, 8, 8, orth)
+        out[key] = {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
+                    "rel_residual": it.history[-1][1], "ms_per_iteration":
+                    round(ms / it.GetNumberIteration(), 4),
+                    "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                    "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
+                    "timing": "best of 2"}
+    out["gmres30_cgs2_jacobi_convdiff128"]["forward_diff_vs_mgs"] = float(
+        np.linalg.norm(xs_gpu["cgs2"] - xs_gpu["mgs"]) / np.linalg.norm(xs_gpu["mgs"]))
+    out["gmres30_cgs2_jacobi_convdiff128"]["speedup_vs_mgs"] = round(
+        out["gmres30_jacobi_convdiff128"]["ms"] / out["gmres30_cgs2_jacobi_convdiff128"]["ms"], 3)
+
+    def ir():
+        X = torch.zeros(n, dtype=torch.float64, device=dev)
+        code, info = api.IterativeRefinement(A, X, b, M=J, tol=1e-10, solver="gmres", restart=30)
+        return code, info, X
+    ir()
+    ms, (code, info, X) = timed(ir, reps=2)
     x = X.cpu().numpy()
+    best64 = min(out["gmres30_jacobi_convdiff128"]["ms"], out["gmres30_cgs2_jacobi_convdiff128"]["ms"])
+    nbytes = gmres_bytes(n, ind.size, info["inner_iter"], 30, 4, 4, "cgs2")
+    out["ir_gmres30_jacobi_convdiff128"] = {
+        "ms": round(ms, 2), "error_code": code, "outer_iter": info["outer_iter"],
+        "inner_iter": info["inner_iter"], "rel_residual_fp64": info["rel_residual"],
+        "rel_residual_host_check": host_relres(x),
+        "forward_error_vs_fp64_gmres": float(np.linalg.norm(x - xs_gpu["mgs"]) /
+                                             np.linalg.norm(xs_gpu["mgs"])),
+        "forward_error_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs)),
+        "speedup_vs_fp64_gmres_mgs": round(out["gmres30_jacobi_convdiff128"]["ms"] / ms, 3),
+        "speedup_vs_best_fp64_gmres": round(best64 / ms, 3),
+        "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
+        "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
+        "timing": "best of 2"}
+    x = xs_gpu["mgs"]
     jobs.append(("gmres30_jacobi_convdiff128",
                  lambda: _cpu_solve("gmres", ptr, ind, val, bh, x, precond=1, restart=30), False))
-    return {"gmres30_jacobi_convdiff128": {"ms": round(ms, 2), "iterations": it.GetNumberIteration(),
-                                           "rel_residual": it.history[-1][1]}}
+    return out
 
 
 def extra_zipf(api, matgen, torch, dev, timed):

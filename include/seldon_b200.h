@@ -382,6 +382,21 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
               sb2_iter_result* result, double* hist, int* hist_it,
               int hist_cap, void* stream);
 
+/* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
+ * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
+ * step projects the new vector on the whole basis at once, twice, so it
+ * takes three grid-wide reductions where the modified order takes i + 2.
+ * Restarts, Givens rotations, back-solve, stopping rule, error codes and
+ * history are those of sb2_gmres (Gmres.cxx:44-183); the iterates agree with
+ * the reference's to rounding, not bit for bit.  M: NULL (identity) or
+ * Jacobi; restart (m) <= 32.  Other preconditioners or a larger restart give
+ * SB2_ERR_NOT_SUPPORTED.  No counterpart in the reference (a labelled
+ * variant of its Gmres). */
+int sb2_gmres_cgs2(const sb2_csr* A, const sb2_precond* M, double* x,
+                   const double* b, const sb2_iter_params* params,
+                   sb2_iter_result* result, double* hist, int* hist_it,
+                   int hist_cap, void* stream);
+
 /* Cg with the identity preconditioner that allocates no memory at all.
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc -- code whose device memory is entirely owned by another
@@ -415,15 +430,26 @@ int sb2_cg_noalloc(const sb2_csr* A, double* x, const double* b,
 /* Iterative refinement with FP32 inner Krylov solves (FP32 values, vectors
  * and accumulation) inside an FP64 outer loop: the residual r = b - A x, the
  * solution update and the stopping test stay in FP64.  New form beside the
- * reference's drivers (no counterpart in Seldon); the inner solver follows
- * Cg.cxx:45-116 and the stopping rule Iterative.cxx:272-319. */
+ * reference's drivers (no counterpart in Seldon); the inner solvers follow
+ * Cg.cxx:45-116 and Gmres.cxx:44-183, the stopping rule Iterative.cxx:272-319.
+ *
+ * solver 1 (GMRES) is restarted GMRES(restart) whose restarts are the
+ * refinement steps: each cycle builds its Krylov basis in FP32 (FP32 products,
+ * basis vectors and per-thread sums, orthogonalized by CGS2), while the
+ * Hessenberg matrix, its Givens rotations and back-solve, the update
+ * x += V y and the residual that starts the next cycle are FP64.  A cycle
+ * ends after `restart` steps, when its residual estimate has dropped by
+ * inner_tol, or when the estimate of ||M^-1 r|| / ||M^-1 r0|| is below tol;
+ * the solve stops when the FP64 ||b - A x|| / ||b|| < tol at a restart.
+ * max_inner bounds the Arnoldi steps, max_outer the cycles; mode is not
+ * read. */
 typedef struct {
   double tol;          /* outer target: ||b - A x|| / ||b|| < tol (FP64) */
   double inner_tol;    /* relative residual reduction of each inner solve */
   int max_outer;       /* refinement steps at most */
   int max_inner;       /* iterations of one inner solve at most */
-  int solver;          /* inner solver: 0 = CG (the only one implemented) */
-  int restart;         /* reserved (GMRES restart) */
+  int solver;          /* inner solver: 0 = CG, 1 = GMRES */
+  int restart;         /* GMRES: steps per cycle (<= 32; <= 0 means 30) */
   int init_guess_null; /* 1: x = 0; 0: start from x */
   int mode;            /* 0: reliable updates -- one FP32 CG run whose residual
                           is replaced by the FP64 true residual each time it has
@@ -443,8 +469,9 @@ typedef struct {
 } sb2_ir_result;
 
 /* M: NULL (identity) or a Jacobi preconditioner of A (applied in FP32 inside
- * the inner solves).  hist (host, may be NULL) receives the FP64 relative
- * residual before each refinement step and at the end. */
+ * the inner solves, in FP64 to the outer residual).  hist (host, may be NULL)
+ * receives the FP64 relative residual before each refinement step and at
+ * the end. */
 int sb2_ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                  const sb2_ir_params* params, sb2_ir_result* result, double* hist,
                  int hist_cap, void* stream);

@@ -927,16 +927,32 @@ def BiCgStab(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_bicgstab, A, x, b, M, iteration, hist_cap, stream)
 
 
-def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None):
-    """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183)."""
-    return _solve(_L.sb2_gmres, A, x, b, M, iteration, hist_cap, stream)
+def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None, orthogonalization="mgs"):
+    """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183).
+
+    orthogonalization="mgs" runs the reference's modified Gram-Schmidt loop
+    (Gmres.cxx:127-132); "cgs2" the labelled variant that projects on the
+    whole basis at once, twice (three grid reductions per step instead of
+    i + 2; identity or Jacobi preconditioner, restart <= 32)."""
+    if orthogonalization not in ("mgs", "cgs2"):
+        raise ValueError(f"orthogonalization must be 'mgs' or 'cgs2', not {orthogonalization!r}")
+    fn = _L.sb2_gmres if orthogonalization == "mgs" else _L.sb2_gmres_cgs2
+    return _solve(fn, A, x, b, M, iteration, hist_cap, stream)
 
 
 # ------------------------------------------------------------------ mixed precision
 
-def IterativeRefinement(A, x, b, M=None, tol=1e-10, inner_tol=None, max_outer=50,
-                        max_inner=20000, init_guess_null=True, restarted=False, stream=None):
-    """FP32-inner / FP64-outer iterative refinement with CG.
+def IterativeRefinement(A, x, b, M=None, tol=1e-10, inner_tol=None, max_outer=None,
+                        max_inner=20000, init_guess_null=True, restarted=False, stream=None,
+                        solver="cg", restart=30):
+    """FP32-inner / FP64-outer iterative refinement with CG or GMRES.
+
+    solver="gmres": restarted GMRES(restart) whose restarts are the FP64
+    refinement steps (FP32 Arnoldi basis, FP64 Hessenberg, update and
+    residual); a cycle also ends once its residual estimate has dropped by
+    inner_tol (default 1e-6); max_outer bounds the cycles (default 1000;
+    50 refinement steps for CG), max_inner the Arnoldi steps; `restarted` is
+    not read.
 
     restarted=False: reliable updates -- one FP32 CG run whose residual is
     replaced by the FP64 true residual each time it has dropped by inner_tol
@@ -945,10 +961,15 @@ def IterativeRefinement(A, x, b, M=None, tol=1e-10, inner_tol=None, max_outer=50
     corrections, FP32 iterations, final FP64 relative residual and the
     residual history."""
     import numpy as np
+    if solver not in ("cg", "gmres"):
+        raise ValueError(f"solver must be 'cg' or 'gmres', not {solver!r}")
+    gm = solver == "gmres"
     if inner_tol is None:
-        inner_tol = 1e-5 if restarted else 1e-2
-    prm = IrParams(tol, inner_tol, max_outer, max_inner, 0, 0, int(init_guess_null),
-                   1 if restarted else 0)
+        inner_tol = 1e-6 if gm else (1e-5 if restarted else 1e-2)
+    if max_outer is None:
+        max_outer = 1000 if gm else 50
+    prm = IrParams(tol, inner_tol, max_outer, max_inner, 1 if gm else 0, int(restart) if gm else 0,
+                   int(init_guess_null), 1 if restarted else 0)
     res = IrResult()
     hist = np.zeros(max_outer + 2)
     Mh = None if (M is None or M.kind == _lib.PRECOND_IDENTITY) else M.handle_for(A)

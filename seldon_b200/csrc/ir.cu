@@ -1,5 +1,7 @@
 // Mixed-precision iterative refinement: FP32 inner Krylov solves inside an
-// FP64 outer loop.
+// FP64 outer loop.  This file holds the CG inner solve; the GMRES one
+// (restarted GMRES whose restarts are the FP64 refinement steps) is in
+// gmres_cgs2.cu.
 //
 //   x = x0 (or 0);  r = b - A x                       FP64 (SELL SpMV)
 //   while ||r|| / ||b|| >= tol:
@@ -41,6 +43,10 @@ template <typename T, typename VT>
 int chain_ru_enqueue(const SellOp<VT>& S, int n, const T* diag, T* x, T* r, T* work,
                      ChainState<T>* st, T* part, int chunk, cudaStream_t s);
 
+int ir_gmres_solve(const sb2_csr* A, bool jacobi, double* x, const double* b,
+                   const sb2_ir_params* prm, sb2_ir_result* res, double* hist, int hist_cap,
+                   cudaStream_t s);
+
 constexpr int IT = 256;
 
 __global__ void to_float_kernel(long long n, const double* __restrict__ a, float* __restrict__ b) {
@@ -51,7 +57,7 @@ __global__ void to_float_kernel(long long n, const double* __restrict__ a, float
 
 // FP32 copies of the operator's values (SELL values and CSR values of the
 // long-row bins) and of the diagonal, built once per matrix.
-static int ensure_fp32(const sb2_csr* cA, bool need_diag) {
+int ensure_fp32(const sb2_csr* cA, bool need_diag) {
   sb2_csr* A = const_cast<sb2_csr*>(cA);
   if (need_diag) SB2_TRY(ensure_diag(A));
   std::lock_guard<std::mutex> g(A->mu);
@@ -74,7 +80,7 @@ static int ensure_fp32(const sb2_csr* cA, bool need_diag) {
   return SB2_OK;
 }
 
-static SellOp<float> sell_op32(const sb2_csr* A) {
+SellOp<float> sell_op32(const sb2_csr* A) {
   const SellArrays& s = A->full.sell;
   return SellOp<float>{s.nslice, s.d_sptr, s.d_qinfo, s.d_qrows, s.d_scol, s.d_sval32, s.nwarp, s.d_wrows,
                        s.ncta, s.d_crows, A->full.d_ptr, A->full.d_ind, A->d_val32};
@@ -180,7 +186,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
                     cudaStream_t s) {
   if (!A || !prm || !res || A->m != A->n) return SB2_ERR_INVALID_VALUE;
   if (A->m > 0 && (!x || !b || x == b)) return SB2_ERR_INVALID_VALUE;
-  if (prm->solver != 0) return SB2_ERR_NOT_SUPPORTED;
+  if (prm->solver != 0 && prm->solver != 1) return SB2_ERR_NOT_SUPPORTED;
   *res = sb2_ir_result{};
   const int n = A->m;
   if (n == 0) return SB2_OK;
@@ -189,6 +195,7 @@ static int ir_solve(const sb2_csr* A, const sb2_precond* M, double* x, const dou
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) return SB2_ERR_NOT_SUPPORTED;
   if (M && precond_matrix(M) != A) return SB2_ERR_INVALID_VALUE;
   const bool jac = (kind == SB2_PRECOND_JACOBI);
+  if (prm->solver == 1) return ir_gmres_solve(A, jac, x, b, prm, res, hist, hist_cap, s);
   SB2_TRY(ensure_fp32(A, jac));
   const SellOp<double> S64 = sell_op(A->full);
   const SellOp<float> S32 = sell_op32(A);
