@@ -691,7 +691,11 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs):
 
 
 def extra_zipf(api, matgen, torch, dev, timed):
-    """SpMV on the Zipf(1.5) random matrix, n = 10^6."""
+    """SpMV on the Zipf(1.5) random matrix, n = 10^6; beside it the gather
+    bound: the same index and value streams and x gathers with no rows
+    (sb2_probe_gather), the least time any row binning can take."""
+    from seldon_b200 import _lib
+    L = _lib.load()
     ptr, ind, val = matgen.zipf_csr(1_000_000, seed=1)
     n = ptr.size - 1
     A = api.RowSparse(n, n, ptr, ind, val)
@@ -699,10 +703,36 @@ def extra_zipf(api, matgen, torch, dev, timed):
     y = torch.zeros(n, dtype=torch.float64, device=dev)
     for _ in range(3):
         api.Mlt(A, x, y)
-    ms, _ = timed(lambda: [api.Mlt(A, x, y) for _ in range(20)])
+    ms, _ = timed(lambda: [api.Mlt(A, x, y) for _ in range(20)], reps=3)
     Bz = spmv_bytes(n, n, ind.size)
-    return {"spmv_zipf_1e6": {"gbs": round(Bz / (ms / 20 * 1e-3) / 1e9, 1), "nnz": int(ind.size),
-                              "us": round(ms / 20 * 1e3, 1)}}
+    us = ms / 20 * 1e3
+    out = {"gbs": round(Bz / (us * 1e-6) / 1e9, 1), "nnz": int(ind.size), "us": round(us, 1)}
+    di = torch.as_tensor(ind, device=dev)
+    dv = torch.as_tensor(val, device=dev)
+    part = torch.empty(4096, dtype=torch.float64, device=dev)
+    nb = ctypes.c_int(0)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def probe(with_val):
+        def run():
+            for _ in range(20):
+                _lib.check(L.sb2_probe_gather(int(ind.size), ctypes.c_void_p(di.data_ptr()),
+                                              ctypes.c_void_p(dv.data_ptr()) if with_val else None,
+                                              ctypes.c_void_p(x.data_ptr()),
+                                              ctypes.c_void_p(part.data_ptr()), 4096,
+                                              ctypes.byref(nb), sp), "sb2_probe_gather")
+        run()
+        t, _ = timed(run, reps=3)
+        return t / 20 * 1e3
+    pv, pi = probe(True), probe(False)
+    out["gather_bound"] = {
+        "us": round(pv, 1), "index_and_gather_only_us": round(pi, 1),
+        "gbs_algorithmic": round(Bz / (pv * 1e-6) / 1e9, 1),
+        "gather_sectors_per_s": round(ind.size / (pi * 1e-6), 1),
+        "spmv_frac_of_bound": round(pv / us, 3),
+        "what": "sum of val[k]*x[ind[k]] over all 68.8M entries in one stream, no rows "
+                "(sb2_probe_gather): the same index, value and x traffic as the product"}
+    return {"spmv_zipf_1e6": out}
 
 
 def _shuffled_triplets(matgen, torch, dev, g, seed=3):

@@ -188,6 +188,18 @@ int sb2_mlt_host_batch(const sb2_csr* A, int trans, double alpha, int count,
 #define SB2_SPMV_TMA 2
 int sb2_spmv_set_config(int algo, int threads, int stages);
 
+/* Measurement of the gather bound of a product: partials[c] (device, one per
+ * CTA; *blocks CTAs, at most max_blocks) receive the CTA sums of
+ * val[k] * x[ind[k]] (val == NULL: of x[ind[k]]) over k < nnz, all entries
+ * in one stream with no rows.  It reads the index and value arrays and
+ * gathers x as a CSR product over the same arrays does, so its time bounds
+ * from below what any row binning of that product can reach.  ind and val
+ * must be 16-byte aligned; ind entries must index x (not checked).  No
+ * counterpart in the reference: a measurement kernel the solvers never
+ * call. */
+int sb2_probe_gather(long long nnz, const int* ind, const double* val, const double* x,
+                     double* partials, int max_blocks, int* blocks, void* stream);
+
 /* ------------------------------------------------------------ BLAS-1 (FP64) */
 /* All reductions are deterministic: the same n gives the same summation tree
  * on every call and every run. */
@@ -541,12 +553,24 @@ int sb2_batch_solve(const sb2_batch* B, double* x, const double* b,
                     const sb2_batch_params* params, int* d_iters, double* d_relres,
                     sb2_batch_result* result, void* stream);
 
-/* Autotuner: times the solve of this batch (x is overwritten) with CTAs of
- * 128, 256 and 512 threads and keeps the fastest for later solves. */
+/* The solve's plan, chosen per size class of the systems:
+ *   threads   CTA size (128, 256 or 512) of the systems a whole CTA solves
+ *   warp_max  systems of at most this many rows are solved by one warp each
+ *             (a CTA holds several of them), with shuffle reductions and no
+ *             CTA barrier; 0: every system gets a CTA
+ * The queue hands systems out largest first, so a CTA that takes a system of
+ * at most warp_max rows turns to warps for the rest of the launch.
+ * Autotuner: times the solve of this batch (x is overwritten) under each
+ * candidate plan (threads 128, 256, 512 by warp_max 0, 256, 1024) and keeps
+ * the fastest for later solves.  The choice is cached per (histogram of the
+ * systems' sizes in power-of-two classes, mode): a later batch with the same
+ * histogram takes it without timing. */
 int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
                        const sb2_batch_params* params, void* stream);
 int sb2_batch_set_threads(sb2_batch* B, int threads);
 int sb2_batch_get_threads(const sb2_batch* B);
+int sb2_batch_set_plan(sb2_batch* B, int threads, int warp_max);
+int sb2_batch_get_plan(const sb2_batch* B, int* threads, int* warp_max);
 
 /* Size from which Cg runs as a chain of full-occupancy kernels (one per
  * pass, scalars in device memory) instead of one persistent kernel.  The
@@ -564,6 +588,17 @@ int sb2_krylov_set_config(int chain_min_n);
  * it on with at most that many.  Returns the previous setting (0 or the
  * cap).  No counterpart in the reference (a tuning knob of this engine). */
 int sb2_krylov_set_cluster(int on);
+
+/* Cg with an SOR or ILUT preconditioner: 1 (default) runs it as a chain of
+ * device kernels whose scalars (rho, alpha, beta, the residual and the stop
+ * flag) stay in device memory, the preconditioner's sweeps enqueued between
+ * them, with no host synchronization per iteration; 0 runs the host-driven
+ * loop of library calls (a dot product returned to the host each time, as
+ * the reference's generic driver does).  The two group their reductions
+ * differently, so their iterates agree to rounding.  BiCgStab and Gmres
+ * with these preconditioners are host-driven.  Returns the previous setting.
+ * No counterpart in the reference (a tuning knob of this engine). */
+int sb2_krylov_set_pcg(int device_resident);
 
 /* Device-side wait limit for the fused solvers' grid barriers, in
  * milliseconds (default 2000).  Values <= 0 leave it unchanged.  Returns the

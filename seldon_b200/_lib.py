@@ -140,6 +140,9 @@ _PROTOS = [
     ("sb2_stream_sync", ctypes.c_int, [c_void_p]),
     ("sb2_set_wait_limit_ms", ctypes.c_int, [ctypes.c_int]),
     ("sb2_set_wait_limit_us", ctypes.c_int, [ctypes.c_int]),
+    ("sb2_krylov_set_pcg", ctypes.c_int, [ctypes.c_int]),
+    ("sb2_probe_gather", ctypes.c_int,
+     [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p]),
     ("sb2_csr_create", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p,
       ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_void_p)]),
@@ -213,6 +216,8 @@ _PROTOS += [
      [c_void_p, c_void_p, c_void_p, ctypes.POINTER(BatchParams), c_void_p]),
     ("sb2_batch_set_threads", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("sb2_batch_get_threads", ctypes.c_int, [c_void_p]),
+    ("sb2_batch_set_plan", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("sb2_batch_get_plan", ctypes.c_int, [c_void_p, c_int_p, c_int_p]),
 ]
 _PROTOS += [
     ("sb2_csr_set_values", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p]),

@@ -1036,10 +1036,22 @@ class Batch:
         return res if summary else None
 
     def autotune(self, x, b, stream=None, **kw):
+        """Times the candidate plans on this batch (x is overwritten) and keeps
+        the fastest; a batch with the same size histogram reuses the cached
+        choice.  Returns the CTA size (see plan())."""
         prm = self.params(**kw)
         check(_L.sb2_batch_autotune(self._h, _dev_ptr(x, self.m, "x"), _dev_ptr(b, self.m, "b"),
                                     ctypes.byref(prm), _stream(stream)), "sb2_batch_autotune")
         return _L.sb2_batch_get_threads(self._h)
+
+    def plan(self):
+        """(threads per CTA, largest system one warp solves; 0: none)."""
+        t, w = ctypes.c_int(0), ctypes.c_int(0)
+        check(_L.sb2_batch_get_plan(self._h, ctypes.byref(t), ctypes.byref(w)), "sb2_batch_get_plan")
+        return t.value, w.value
+
+    def set_plan(self, threads, warp_max=0):
+        check(_L.sb2_batch_set_plan(self._h, int(threads), int(warp_max)), "sb2_batch_set_plan")
 
     @classmethod
     def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):

@@ -20,6 +20,8 @@
 // so the whole batch solve can be captured in a CUDA graph and replayed.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -32,15 +34,21 @@ struct sb2_batch {
   int* d_sys_row = nullptr;  // [nsys+1]
   int* d_order = nullptr;    // systems by decreasing size
   int* d_ptr = nullptr;      // [m+1] global CSR
-  int* d_ind = nullptr;      // local column (row offset of the system subtracted)
+  void* d_ind = nullptr;     // local column (row offset of the system subtracted):
+                             // uint16 when every system has <= 65536 rows, else int32
+  bool ind16 = false;
   double* d_val = nullptr;
   float* d_val32 = nullptr;
-  // scratch: FP64 residual, FP32 r, p, q, d
+  // scratch: FP64 residual; mode 0: FP32 r, p (two), q, d; mode 1: FP64 p
+  // (two), q in the same space
   double* d_r64 = nullptr;
   float* d_w32 = nullptr;
   unsigned* d_queue = nullptr;
-  int threads = 256;         // CTA size (autotuned)
+  // plan (autotuned): CTA size, and the largest system a single warp solves
+  int threads = 256;
+  int warp_max = 0;
   int max_rows = 0;
+  unsigned long long histo_key = 0;  // size histogram, for the tuned-plan cache
 };
 
 namespace sb2 {
@@ -50,13 +58,13 @@ struct BatchArgs {
   const int* sys_row;
   const int* order;
   const int* ptr;
-  const int* ind;
+  const void* ind;
   const double* val;
   const float* val32;
   const double* b;
   double* x;
   double* r64;
-  float* w32;  // 4 * m floats: r, p, q, d
+  float* w32;  // 6 * m floats
   int m;
   unsigned* queue;
   double tol;
@@ -64,163 +72,221 @@ struct BatchArgs {
   int max_iter;
   int mode;
   int init_guess_null;
+  int warp_max;     // systems of at most this many rows: one warp each
   int* iters;       // per system (may be null)
   double* relres;   // per system (may be null)
 };
 
-template <int NT, typename T>
-__device__ __forceinline__ T cta_sum(T v, T* red) {
-  v = block_sum<NT>(v, red);
-  __shared__ T s_bcast;
-  if (threadIdx.x == 0) s_bcast = v;
-  __syncthreads();
-  const T out = s_bcast;
-  __syncthreads();
-  return out;
-}
-
-// y_i = sum_j A_ij x_j over the rows [r0, r1) of one system, thread per row,
-// entries in stored order.
-template <typename VT, typename XT, typename AT>
-__device__ __forceinline__ AT row_dot(const int* __restrict__ ptr, const int* __restrict__ ind,
-                                      const VT* __restrict__ val, const XT* __restrict__ x,
-                                      int i) {
-  const int a = __ldg(ptr + i), e = __ldg(ptr + i + 1);
-  AT t = AT(0);
-  for (int k = a; k < e; k++) t = add_rn(t, mul_rn(AT(__ldg(val + k)), AT(x[__ldg(ind + k)])));
-  return t;
-}
-
-// r64 = b - A x (FP64, x in local indexing at xs), returns ||r64||^2.
+// The threads that solve one system: a whole CTA, or one warp.  sums()
+// reduces K per-thread values into every thread in a fixed order (a shuffle
+// tree per warp, then the warps in order); the CTA form takes one
+// __syncthreads, alternating between two buffers so that the next reduction
+// may start while slow threads still read this one.
 template <int NT>
-__device__ double fp64_residual(const BatchArgs& a, int r0, int n, const double* xs,
-                                double* red) {
+struct CtaGroup {
+  double* red;  // shared: 2 buffers x 2 values x NT/32 warps
+  int ph;
+  static constexpr int kSize = NT;
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  template <int K, typename T>
+  __device__ __forceinline__ void sums(T (&v)[K]) {
+    constexpr int W = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* buf = red + ph * 2 * W;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const T t = warp_sum(v[k]);
+      if (lane == 0) buf[k * W + w] = (double)t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      T acc = T(0);
+      for (int q = 0; q < W; q++) acc = add_rn(acc, (T)buf[k * W + q]);
+      v[k] = acc;
+    }
+    ph ^= 1;
+  }
+  template <typename T>
+  __device__ __forceinline__ T sum(T v) {
+    T o[1] = {v};
+    sums<1>(o);
+    return o[0];
+  }
+};
+
+struct WarpGroup {
+  static constexpr int kSize = 32;
+  __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  // __syncwarp orders the lanes' memory accesses around the reduction
+  // (shuffles alone do not), as __syncthreads does for the CTA form
+  template <int K, typename T>
+  __device__ __forceinline__ void sums(T (&v)[K]) {
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = __shfl_sync(0xffffffffu, warp_sum(v[k]), 0);
+  }
+  template <typename T>
+  __device__ __forceinline__ T sum(T v) {
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, warp_sum(v), 0);
+  }
+};
+
+// r64 = b - A x over one system (FP64, entries in stored order); returns
+// ||r64||^2 in every thread of the group.  x must be complete (synced).
+template <class G, typename IT>
+__device__ double fp64_residual(G& g, const BatchArgs& a, int r0, int n, const double* xs) {
+  const IT* __restrict__ ind = static_cast<const IT*>(a.ind);
   double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += NT) {
-    const double t = row_dot<double, double, double>(a.ptr + r0, a.ind, a.val, xs, i);
+  for (int i = g.rank(); i < n; i += G::kSize) {
+    const int k0 = __ldg(a.ptr + r0 + i), k1 = __ldg(a.ptr + r0 + i + 1);
+    double t = 0.0;
+    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(__ldg(a.val + k), xs[__ldg(ind + k)]));
     const double v = add_rn(__ldg(a.b + r0 + i), -t);
     a.r64[r0 + i] = v;
     acc = add_rn(acc, mul_rn(v, v));
   }
-  __syncthreads();
-  return cta_sum<NT>(acc, red);
+  return g.sum(acc);
 }
 
-template <int NT>
-__device__ void solve_fp64(const BatchArgs& a, int s, int r0, int n, double nb) {
-  __shared__ double red[NT / 32];
+// One CG iteration's product with the direction update folded in: the
+// direction p_new = first ? r : beta*p_old + zc*r is computed where the
+// product reads it (p_old and r are complete), written for the group's own
+// rows into the other buffer, and q = A p_new with (p_new, q).  This saves
+// the separate direction pass and its synchronization; every thread that
+// needs p_new(c) computes it from the same values, so all agree bit for bit.
+template <class G, typename IT, typename VT, typename T>
+__device__ __forceinline__ T fused_direction_product(G& g, const BatchArgs& a, const VT* __restrict__ val,
+                                                     int r0, int n, const T* __restrict__ r,
+                                                     const T* __restrict__ po, T* __restrict__ pw,
+                                                     T* __restrict__ q, bool first, T beta, T zc) {
+  const IT* __restrict__ ind = static_cast<const IT*>(a.ind);
+  T pq = T(0);
+  for (int i = g.rank(); i < n; i += G::kSize) {
+    const int k0 = __ldg(a.ptr + r0 + i), k1 = __ldg(a.ptr + r0 + i + 1);
+    T t = T(0);
+    for (int k = k0; k < k1; k++) {
+      const int c = __ldg(ind + k);
+      const T pc = first ? r[c] : add_rn(mul_rn(po[c], beta), mul_rn(zc, r[c]));
+      t = add_rn(t, mul_rn(T(__ldg(val + k)), pc));
+    }
+    const T pi = first ? r[i] : add_rn(mul_rn(po[i], beta), mul_rn(zc, r[i]));
+    pw[i] = pi;
+    q[i] = t;
+    pq = add_rn(pq, mul_rn(pi, t));
+  }
+  return g.sum(pq);
+}
+
+// Plain FP64 CG (Cg.cxx:45-116, identity preconditioner).
+template <class G, typename IT>
+__device__ void solve_fp64(G& g, const BatchArgs& a, int s, int r0, int n, double nb) {
   double* x = a.x + r0;
   double* r = a.r64 + r0;
-  // FP64 work vectors in the FP32 scratch: p and q take two floats each
-  double* p = reinterpret_cast<double*>(a.w32) + r0;
-  double* q = reinterpret_cast<double*>(a.w32 + a.m * 2) + r0;
+  double* po = reinterpret_cast<double*>(a.w32) + r0;  // the two direction buffers
+  double* pw = reinterpret_cast<double*>(a.w32) + (size_t)a.m + r0;
+  double* q = reinterpret_cast<double*>(a.w32) + 2 * (size_t)a.m + r0;
   double rr;
   if (a.init_guess_null) {
-    for (int i = threadIdx.x; i < n; i += NT) {
-      x[i] = 0.0;
-      r[i] = __ldg(a.b + r0 + i);
-    }
-    rr = nb * nb;
-    __syncthreads();
     double acc = 0.0;
-    for (int i = threadIdx.x; i < n; i += NT) acc = add_rn(acc, mul_rn(r[i], r[i]));
-    rr = cta_sum<NT>(acc, red);
+    for (int i = g.rank(); i < n; i += G::kSize) {
+      x[i] = 0.0;
+      const double bi = __ldg(a.b + r0 + i);
+      r[i] = bi;
+      acc = add_rn(acc, mul_rn(bi, bi));
+    }
+    rr = g.sum(acc);
   } else {
-    rr = fp64_residual<NT>(a, r0, n, x, red);
+    rr = fp64_residual<G, IT>(g, a, r0, n, x);
   }
   const double facteur = 1.0 / nb;
-  double rho = rr, rho_1 = 1.0, res = facteur * sqrt(rr);
+  double rho = rr, rho_1 = 1.0, res = facteur * sqrt(rr), beta = 0.0;
   int it = 0;
   while (!(res < a.tol) && it < a.max_iter) {
     if (rho == 0.0) break;
-    const double beta = rho / rho_1;
-    for (int i = threadIdx.x; i < n; i += NT) p[i] = (it == 0) ? r[i] : add_rn(mul_rn(p[i], beta), r[i]);
-    __syncthreads();
-    double pq = 0.0;
-    for (int i = threadIdx.x; i < n; i += NT) {
-      const double t = row_dot<double, double, double>(a.ptr + r0, a.ind, a.val, p, i);
-      q[i] = t;
-      pq = add_rn(pq, mul_rn(p[i], t));
-    }
-    const double delta = cta_sum<NT>(pq, red);
+    const double delta = fused_direction_product<G, IT, double, double>(
+        g, a, a.val, r0, n, r, po, pw, q, it == 0, beta, 1.0);
+    double* t = po;  // the new direction is now the current one
+    po = pw;
+    pw = t;
     if (delta == 0.0) break;
     const double alpha = rho / delta;
+    const double* p = po;
     double acc = 0.0;
-    for (int i = threadIdx.x; i < n; i += NT) {
+    for (int i = g.rank(); i < n; i += G::kSize) {
       x[i] = add_rn(x[i], mul_rn(alpha, p[i]));
       const double ri = add_rn(r[i], mul_rn(-alpha, q[i]));
       r[i] = ri;
       acc = add_rn(acc, mul_rn(ri, ri));
     }
-    rr = cta_sum<NT>(acc, red);
+    rr = g.sum(acc);
     rho_1 = rho;
     rho = rr;
+    beta = rho / rho_1;
     res = facteur * sqrt(rr);
     it++;
   }
-  if (threadIdx.x == 0) {
+  if (g.rank() == 0) {
     if (a.iters) a.iters[s] = it;
     if (a.relres) a.relres[s] = res;
   }
 }
 
-template <int NT>
-__device__ void solve_mixed(const BatchArgs& a, int s, int r0, int n, double nb) {
-  __shared__ double red64[NT / 32];
-  __shared__ float red32[NT / 32];
+// FP32 CG with FP64 reliable updates.
+template <class G, typename IT>
+__device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, double nb) {
   double* x = a.x + r0;
   float* r = a.w32 + r0;
-  float* p = a.w32 + a.m + r0;
-  float* q = a.w32 + 2 * (size_t)a.m + r0;
-  float* d = a.w32 + 3 * (size_t)a.m + r0;
+  float* po = a.w32 + (size_t)a.m + r0;  // the two direction buffers
+  float* pw = a.w32 + 2 * (size_t)a.m + r0;
+  float* q = a.w32 + 3 * (size_t)a.m + r0;
+  float* d = a.w32 + 4 * (size_t)a.m + r0;
   if (a.init_guess_null)
-    for (int i = threadIdx.x; i < n; i += NT) x[i] = 0.0;
-  __syncthreads();
-  double rr64 = fp64_residual<NT>(a, r0, n, x, red64);
+    for (int i = g.rank(); i < n; i += G::kSize) x[i] = 0.0;
+  g.sync();
+  double rr64 = fp64_residual<G, IT>(g, a, r0, n, x);
   double res = sqrt(rr64) / nb;
   int it = 0;
   if (res < a.tol) {
-    if (threadIdx.x == 0) {
+    if (g.rank() == 0) {
       if (a.iters) a.iters[s] = 0;
       if (a.relres) a.relres[s] = res;
     }
     return;
   }
   const float fnb = (float)nb;
-  for (int i = threadIdx.x; i < n; i += NT) {
-    r[i] = (float)a.r64[r0 + i];
-    d[i] = 0.0f;
-  }
-  __syncthreads();
   float acc = 0.0f;
-  for (int i = threadIdx.x; i < n; i += NT) acc = add_rn(acc, mul_rn(r[i], r[i]));
-  float rho = cta_sum<NT>(acc, red32), rho_1 = 1.0f, zc = 1.0f;
+  for (int i = g.rank(); i < n; i += G::kSize) {
+    const float ri = (float)a.r64[r0 + i];
+    r[i] = ri;
+    d[i] = 0.0f;
+    acc = add_rn(acc, mul_rn(ri, ri));
+  }
+  float rho = g.sum(acc), rho_1 = 1.0f, zc = 1.0f, beta = 0.0f;
   float rmax = sqrtf(rho);
   bool first = true;
   for (;;) {
-    const float beta = first ? 0.0f : rho / rho_1;
-    for (int i = threadIdx.x; i < n; i += NT)
-      p[i] = first ? r[i] : add_rn(mul_rn(p[i], beta), mul_rn(zc, r[i]));
-    __syncthreads();
+    const float delta = fused_direction_product<G, IT, float, float>(
+        g, a, a.val32, r0, n, r, po, pw, q, first, beta, zc);
+    float* t = po;  // the new direction is now the current one
+    po = pw;
+    pw = t;
     first = false;
     zc = 1.0f;
-    float pq = 0.0f;
-    for (int i = threadIdx.x; i < n; i += NT) {
-      const float t = row_dot<float, float, float>(a.ptr + r0, a.ind, a.val32, p, i);
-      q[i] = t;
-      pq = add_rn(pq, mul_rn(p[i], t));
-    }
-    const float delta = cta_sum<NT>(pq, red32);
     if (delta == 0.0f) break;
     const float alpha = rho / delta;
+    const float* p = po;
     acc = 0.0f;
-    for (int i = threadIdx.x; i < n; i += NT) {
+    for (int i = g.rank(); i < n; i += G::kSize) {
       d[i] = add_rn(d[i], mul_rn(alpha, p[i]));
       const float ri = add_rn(r[i], mul_rn(-alpha, q[i]));
       r[i] = ri;
       acc = add_rn(acc, mul_rn(ri, ri));
     }
-    const float rr = cta_sum<NT>(acc, red32);
+    const float rr = g.sum(acc);
     it++;
     const float rn = sqrtf(rr);
     const bool correct = (rn / fnb < (float)a.tol) || (rn < (float)a.ratio * rmax) ||
@@ -228,44 +294,74 @@ __device__ void solve_mixed(const BatchArgs& a, int s, int r0, int n, double nb)
     if (!correct) {
       rho_1 = rho;
       rho = rr;
+      beta = rho / rho_1;
       continue;
     }
     // FP64 correction: x += d, d = 0, r64 = b - A x
-    for (int i = threadIdx.x; i < n; i += NT) {
+    for (int i = g.rank(); i < n; i += G::kSize) {
       x[i] = add_rn(x[i], (double)d[i]);
       d[i] = 0.0f;
     }
-    __syncthreads();
-    rr64 = fp64_residual<NT>(a, r0, n, x, red64);
+    g.sync();
+    rr64 = fp64_residual<G, IT>(g, a, r0, n, x);
     res = sqrt(rr64) / nb;
     if (res < a.tol || it >= a.max_iter) break;
     // replace the FP32 residual; keep the direction, minus its component
     // along the new residual
-    float r2 = 0.0f, rp = 0.0f;
-    for (int i = threadIdx.x; i < n; i += NT) {
+    float v2[2] = {0.0f, 0.0f};
+    for (int i = g.rank(); i < n; i += G::kSize) {
       const float ri = (float)a.r64[r0 + i];
       r[i] = ri;
-      r2 = add_rn(r2, mul_rn(ri, ri));
-      rp = add_rn(rp, mul_rn(ri, p[i]));
+      v2[0] = add_rn(v2[0], mul_rn(ri, ri));
+      v2[1] = add_rn(v2[1], mul_rn(ri, p[i]));
     }
-    r2 = cta_sum<NT>(r2, red32);
-    rp = cta_sum<NT>(rp, red32);
-    rmax = sqrtf(r2);
+    g.sums(v2);
+    rmax = sqrtf(v2[0]);
     rho_1 = rho;
-    rho = r2;
+    rho = v2[0];
     if (rho == 0.0f) break;
-    zc = 1.0f - (rho / rho_1) * (rp / rho);
+    beta = rho / rho_1;
+    zc = 1.0f - beta * (v2[1] / rho);
   }
-  if (threadIdx.x == 0) {
+  if (g.rank() == 0) {
     if (a.iters) a.iters[s] = it;
     if (a.relres) a.relres[s] = res;
   }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) batch_kernel(BatchArgs a) {
+template <class G, typename IT>
+__device__ void solve_system(G& g, const BatchArgs& a, int s) {
+  const int r0 = __ldg(a.sys_row + s), n = __ldg(a.sys_row + s + 1) - r0;
+  double acc = 0.0;
+  for (int i = g.rank(); i < n; i += G::kSize) {
+    const double bi = __ldg(a.b + r0 + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  const double nb = sqrt(g.sum(acc));
+  if (nb == 0.0) {  // zero right-hand side: x untouched (Iterative.cxx:240-241)
+    if (g.rank() == 0) {
+      if (a.iters) a.iters[s] = 0;
+      if (a.relres) a.relres[s] = 0.0;
+    }
+    return;
+  }
+  if (a.mode == 1)
+    solve_fp64<G, IT>(g, a, s, r0, n, nb);
+  else
+    solve_mixed<G, IT>(g, a, s, r0, n, nb);
+}
+
+// One persistent launch.  CTAs take systems from the queue (largest first)
+// and solve each with all their threads; the first system of at most
+// warp_max rows that a CTA takes switches it to warps: from then on (every
+// later system is as small or smaller) each warp takes and solves systems on
+// its own, with shuffle reductions and no CTA barrier.
+template <int NT, typename IT>
+__global__ void __launch_bounds__(NT, 1280 / NT) batch_kernel(BatchArgs a) {
   __shared__ int s_sys;
-  __shared__ double red[NT / 32];
+  __shared__ double s_red[2 * 2 * (NT / 32)];
+  CtaGroup<NT> cg{s_red, 0};
+  int small = -1;
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned k = atomicAdd(a.queue, 1u);
@@ -275,51 +371,67 @@ __global__ void __launch_bounds__(NT) batch_kernel(BatchArgs a) {
     const int s = s_sys;
     __syncthreads();
     if (s < 0) return;
-    const int r0 = __ldg(a.sys_row + s), n = __ldg(a.sys_row + s + 1) - r0;
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < n; i += NT) {
-      const double bi = __ldg(a.b + r0 + i);
-      acc = add_rn(acc, mul_rn(bi, bi));
+    if (__ldg(a.sys_row + s + 1) - __ldg(a.sys_row + s) <= a.warp_max) {
+      small = s;
+      break;
     }
-    const double nb = sqrt(cta_sum<NT>(acc, red));
-    if (nb == 0.0) {  // zero right-hand side: x untouched (Iterative.cxx:240-241)
-      if (threadIdx.x == 0) {
-        if (a.iters) a.iters[s] = 0;
-        if (a.relres) a.relres[s] = 0.0;
-      }
-      continue;
-    }
-    if (a.mode == 1)
-      solve_fp64<NT>(a, s, r0, n, nb);
-    else
-      solve_mixed<NT>(a, s, r0, n, nb);
+    solve_system<CtaGroup<NT>, IT>(cg, a, s);
     __syncthreads();
+  }
+  WarpGroup wg;
+  const int lane = threadIdx.x & 31;
+  int s = (threadIdx.x >> 5) == 0 ? small : -2;
+  for (;;) {
+    if (s == -2) {
+      int t = -1;
+      if (lane == 0) {
+        const unsigned k = atomicAdd(a.queue, 1u);
+        t = (k < (unsigned)a.nsys) ? __ldg(a.order + k) : -1;
+      }
+      s = __shfl_sync(0xffffffffu, t, 0);
+    }
+    if (s < 0) return;
+    solve_system<WarpGroup, IT>(wg, a, s);
+    __syncwarp();
+    s = -2;
   }
 }
 
-template <int NT>
+template <int NT, typename IT>
 static int launch_batch(const BatchArgs& a, cudaStream_t s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT>, NT, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT, IT>, NT, 0) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const int grid = std::min(a.nsys, per_sm * num_sms(current_device()));
-  batch_kernel<NT><<<std::max(grid, 1), NT, 0, s>>>(a);
+  batch_kernel<NT, IT><<<std::max(grid, 1), NT, 0, s>>>(a);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
 }
 
+template <typename IT>
+static int launch_batch_t(const BatchArgs& a, int threads, cudaStream_t s) {
+  switch (threads) {
+    case 128: return launch_batch<128, IT>(a, s);
+    case 512: return launch_batch<512, IT>(a, s);
+    default: return launch_batch<256, IT>(a, s);
+  }
+}
+
 static int batch_run(const sb2_batch* B, double* x, const double* b, const sb2_batch_params* prm,
-                     int* iters, double* relres, int threads, cudaStream_t s) {
+                     int* iters, double* relres, int threads, int warp_max, cudaStream_t s) {
   BatchArgs a{B->nsys, B->d_sys_row, B->d_order, B->d_ptr, B->d_ind, B->d_val, B->d_val32,
               b, x, B->d_r64, B->d_w32, B->m, B->d_queue, prm->tol, prm->update_ratio,
-              prm->max_iter, prm->mode, prm->init_guess_null, iters, relres};
+              prm->max_iter, prm->mode, prm->init_guess_null, warp_max, iters, relres};
   SB2_CUDA_TRY(cudaMemsetAsync(B->d_queue, 0, sizeof(unsigned), s));
-  switch (threads) {
-    case 128: return launch_batch<128>(a, s);
-    case 512: return launch_batch<512>(a, s);
-    default: return launch_batch<256>(a, s);
-  }
+  return B->ind16 ? launch_batch_t<unsigned short>(a, threads, s)
+                  : launch_batch_t<int>(a, threads, s);
+}
+
+__global__ void batch_ind16(long long n, const int* __restrict__ a, unsigned short* __restrict__ b) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = (unsigned short)a[i];
 }
 
 __global__ void batch_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
@@ -327,6 +439,35 @@ __global__ void batch_to_float(long long n, const double* __restrict__ a, float*
        i += (long long)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
 }
+
+// Key of the tuned-plan cache: the count of systems in each power-of-two
+// row-count class (and the number of systems), hashed.
+static unsigned long long size_histogram_key(int nsys, const int* sys_row) {
+  int cnt[33] = {0};
+  for (int s = 0; s < nsys; s++) {
+    unsigned v = (unsigned)(sys_row[s + 1] - sys_row[s]);
+    int c = 0;
+    while (v) {
+      v >>= 1;
+      c++;
+    }
+    cnt[c]++;
+  }
+  unsigned long long h = 1469598103934665603ull ^ (unsigned long long)nsys;
+  for (int c = 0; c < 33; c++) {
+    h ^= (unsigned long long)cnt[c] + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+struct BatchPlan {
+  int threads, warp_max;
+};
+// Plans chosen by sb2_batch_autotune, per (size histogram, mode): a later
+// batch with the same histogram takes its plan without timing.
+static std::mutex g_plan_mu;
+static std::map<std::pair<unsigned long long, int>, BatchPlan> g_plans;
 
 }  // namespace sb2
 
@@ -373,19 +514,34 @@ int sb2_batch_create(int nsys, const int* sys_row, const int* ptr, const int* in
   B->m = m;
   B->nnz = nnz;
   B->max_rows = maxrows;
+  B->histo_key = size_histogram_key(nsys, sys_row);
   cudaError_t e = cudaMalloc(&B->d_sys_row, sizeof(int) * (nsys + 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int) * std::max(nsys, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_ptr, sizeof(int) * (m + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_ind, sizeof(int) * std::max<long long>(nnz, 1));
+  B->ind16 = (maxrows <= 65536);
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_ind, (B->ind16 ? sizeof(unsigned short) : sizeof(int)) *
+                                                      std::max<long long>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_val, sizeof(double) * std::max<long long>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_val32, sizeof(float) * std::max<long long>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_r64, sizeof(double) * std::max(m, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_w32, sizeof(float) * 4 * (size_t)std::max(m, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_w32, sizeof(float) * 6 * (size_t)std::max(m, 1));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_queue, sizeof(unsigned) * 4);
   if (e == cudaSuccess) e = cudaMemcpy(B->d_sys_row, sys_row, sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && nsys) e = cudaMemcpy(B->d_order, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(B->d_ptr, ptr, sizeof(int) * (m + 1), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && nnz) e = cudaMemcpy(B->d_ind, local.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nnz && !B->ind16)
+    e = cudaMemcpy(B->d_ind, local.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nnz && B->ind16) {
+    // 2-byte local columns: stage the 4-byte ones and narrow them on the device
+    int* tmp = nullptr;
+    e = cudaMalloc(&tmp, sizeof(int) * nnz);
+    if (e == cudaSuccess) e = cudaMemcpy(tmp, local.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      batch_ind16<<<num_sms(B->device) * 8, 256>>>(nnz, tmp, static_cast<unsigned short*>(B->d_ind));
+      e = cudaDeviceSynchronize();
+    }
+    cudaFree(tmp);
+  }
   if (e == cudaSuccess && nnz) e = cudaMemcpy(B->d_val, val, sizeof(double) * nnz, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && nnz) {
     batch_to_float<<<num_sms(B->device) * 8, 256>>>(nnz, B->d_val, B->d_val32);
@@ -424,7 +580,7 @@ int sb2_batch_solve(const sb2_batch* B, double* x, const double* b, const sb2_ba
     if (result) *result = sb2_batch_result{};
     return SB2_OK;
   }
-  SB2_TRY(batch_run(B, x, b, prm, d_iters, d_relres, B->threads, s));
+  SB2_TRY(batch_run(B, x, b, prm, d_iters, d_relres, B->threads, B->warp_max, s));
   if (!result) return SB2_OK;
   // host summary (synchronizes): per-system counts and residuals
   std::vector<int> it(B->nsys);
@@ -454,37 +610,71 @@ int sb2_batch_set_threads(sb2_batch* B, int threads) try {
 
 int sb2_batch_get_threads(const sb2_batch* B) { return B ? B->threads : 0; }
 
+int sb2_batch_set_plan(sb2_batch* B, int threads, int warp_max) try {
+  if (!B || (threads != 128 && threads != 256 && threads != 512) || warp_max < 0)
+    return SB2_ERR_INVALID_VALUE;
+  B->threads = threads;
+  B->warp_max = warp_max;
+  return SB2_OK;
+} SB2_CATCH
+
+int sb2_batch_get_plan(const sb2_batch* B, int* threads, int* warp_max) try {
+  if (!B || !threads || !warp_max) return SB2_ERR_INVALID_VALUE;
+  *threads = B->threads;
+  *warp_max = B->warp_max;
+  return SB2_OK;
+} SB2_CATCH
+
 }  // extern "C"
 
 extern "C" int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
                                   const sb2_batch_params* prm, void* stream) try {
   if (!B || !prm) return SB2_ERR_INVALID_VALUE;
   if (B->nsys == 0) return SB2_OK;
+  const std::pair<unsigned long long, int> key{B->histo_key, prm->mode};
+  {
+    std::lock_guard<std::mutex> g(sb2::g_plan_mu);
+    auto it = sb2::g_plans.find(key);
+    if (it != sb2::g_plans.end()) {
+      B->threads = it->second.threads;
+      B->warp_max = it->second.warp_max;
+      return SB2_OK;
+    }
+  }
   cudaStream_t s = (cudaStream_t)stream;
   cudaEvent_t e0, e1;
   SB2_CUDA_TRY(cudaEventCreate(&e0));
   SB2_CUDA_TRY(cudaEventCreate(&e1));
-  const int cand[3] = {128, 256, 512};
+  // CTA sizes x the largest system one warp solves (0: none)
+  const int cand_t[3] = {128, 256, 512};
+  const int cand_w[3] = {0, 256, 1024};
   float best = 1e30f;
-  int best_t = B->threads;
+  sb2::BatchPlan bp{B->threads, B->warp_max};
   int st = SB2_OK;
-  for (int c = 0; c < 3 && st == SB2_OK; c++) {
+  for (int ci = 0; ci < 9 && st == SB2_OK; ci++) {
+    const int t = cand_t[ci / 3], w = cand_w[ci % 3];
+    if (w > 0 && ci % 3 > 0 && cand_w[ci % 3 - 1] >= B->max_rows) continue;  // same plan as a smaller w
     // one untimed run, one timed run of the same solve
-    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, cand[c], s);
+    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, t, w, s);
     if (st != SB2_OK) break;
     cudaEventRecord(e0, s);
-    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, cand[c], s);
+    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, t, w, s);
     cudaEventRecord(e1, s);
     if (cudaEventSynchronize(e1) != cudaSuccess) st = SB2_ERR_CUDA;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (st == SB2_OK && ms < best) {
       best = ms;
-      best_t = cand[c];
+      bp = sb2::BatchPlan{t, w};
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (st == SB2_OK) B->threads = best_t;
+  if (st == SB2_OK) {
+    B->threads = bp.threads;
+    B->warp_max = bp.warp_max;
+    std::lock_guard<std::mutex> g(sb2::g_plan_mu);
+    sb2::g_plans[key] = bp;
+  }
   return st;
 } SB2_CATCH

@@ -457,6 +457,85 @@ __global__ void __launch_bounds__(CT, 4) k_rho_ru(ChainArgs<T> a) {
   }
 }
 
+// ----------------------------------------------------------------- any preconditioner
+//
+// Cg with a preconditioner applied by its own launches (SOR sweeps, ILUT
+// sweeps): z = M^{-1} r is materialized between the passes, and the loop is
+//   [M apply] -> K_rz (rho = (r, z), beta) -> K_pz (p) -> K_q (q = A p, delta,
+//   alpha) -> K_xr (x, r, ||r||^2, the test)
+// with every scalar in device memory, as in the chain above.  The apply's
+// launches do not read the stop flag: after the stop they recompute z from
+// the final r, and the passes after them return at once.
+
+// rho = (r, z) (Cg.cxx: DotProdConj(r, z)); breakdown #1; beta = rho / rho_1.
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_pc_rz(ChainArgs<T> a, const T* __restrict__ z) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (chain_done(a.st)) return;
+  T rz = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT)
+    rz = add_rn(rz, mul_rn(__ldg(a.r + i), __ldg(z + i)));
+  T v[1] = {block_sum<CT>(rz, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->rho = s_out[0];
+    if (st->rho == T(0)) {
+      st->fail = 1;
+      st->done = 1;
+      return;
+    }
+    if (st->nb_iter > 0) st->beta = st->rho / st->rho_1;
+  }
+}
+
+// p = z (first) | p = beta*p + z: Mlt(beta, p); Add(1, z, p).
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_pc_p(ChainArgs<T> a, const T* __restrict__ z) {
+  pdl_wait();
+  pdl_release();
+  if (chain_done(a.st)) return;
+  const bool first = (a.st->nb_iter == 0);
+  const T beta = a.st->beta;
+  T* __restrict__ p = a.p;
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const T zi = __ldg(z + i);
+    p[i] = first ? zi : add_rn(mul_rn(p[i], beta), zi);
+  }
+}
+
+// Add(alpha, p, x); Add(-alpha, q, r); rho_1 = rho; ++iter; Finished(r).
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_pc_x(ChainArgs<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (chain_done(a.st)) return;
+  const T alpha = a.st->alpha;
+  T rr = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    if (alpha != T(0)) a.x[i] = add_rn(a.x[i], mul_rn(alpha, __ldg(a.p + i)));
+    T ri = a.r[i];
+    if (-alpha != T(0)) {
+      ri = add_rn(ri, mul_rn(-alpha, __ldg(a.q + i)));
+      a.r[i] = ri;
+    }
+    rr = add_rn(rr, mul_rn(ri, ri));
+  }
+  T v[1] = {block_sum<CT>(rr, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->rho_1 = st->rho;
+    st->nb_iter++;
+    if (chain_finished(a, s_out[0])) st->done = 1;
+  }
+}
+
 // ----------------------------------------------------------------- host driver
 
 // Elementwise passes: at most one resident wave (4 CTAs per SM), threads
@@ -563,6 +642,65 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
     SB2_TRY(pipe.wait(&h, &at));
     if (h.done || at > max_iter + 1) break;
     chunk = plan.next(h.nb_iter, h.reste, tol, launched - at, std::min(chunk * 2, 32));
+    SB2_TRY(enqueue());
+  }
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));
+  return SB2_OK;
+}
+
+// Cg with a preconditioner applied by `apply(r, z, stream)` (any launches on
+// the stream); the same chunked pipeline as chain_cg.  work holds p, q, r and
+// z (4 n).
+int chain_pcg(const SellOp<double>& S, int n, const PrecondLaunch& apply, double* x,
+              const double* b, double* work, ChainState<double>* st, double* part, double* hist,
+              int* hist_it, int hist_cap, double tol, int max_iter, int init_guess_null,
+              cudaStream_t s, ChainState<double>* out) {
+  ChainState<double> init{};
+  init.max_iter = max_iter;
+  init.tol = tol;
+  init.hist_cap = hist_cap;
+  init.zc = 1.0;
+  SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  double* z = work + 3 * (size_t)n;
+  // ChainArgs: r = work, p = work + n, q = work + 2n; no diagonal (the
+  // initial (r, z) of k_init_null / the residual product is discarded)
+  ChainArgs<double> a{n, b, x, work, work + n, work + 2 * (size_t)n, nullptr, st, part, hist,
+                      hist_it};
+  const int ge = chain_elem_grid(n);
+  k_norm_b<double><<<ge, CT, 0, s>>>(a);
+  if (init_guess_null)
+    k_init_null<double><<<ge, CT, 0, s>>>(a);
+  else
+    SB2_TRY((launch_spmv_pair<double, double>(1, a, S, s)));
+  SB2_CUDA_TRY(cudaGetLastError());
+  ChainPipe<double> pipe;
+  SB2_TRY(pipe.init());
+  ChunkPlanner plan;
+  int launched = 0, chunk = 4;
+  auto enqueue = [&]() -> int {
+    for (int c = 0; c < chunk; c++) {
+      SB2_TRY(apply(a.r, z, s));
+      SB2_CUDA_TRY(launch_pdl(k_pc_rz<double>, ge, s, a, (const double*)z));
+      SB2_CUDA_TRY(launch_pdl(k_pc_p<double>, ge, s, a, (const double*)z));
+      SB2_TRY((launch_spmv_pair<double, double>(0, a, S, s)));
+      SB2_CUDA_TRY(launch_pdl(k_pc_x<double>, ge, s, a));
+    }
+    SB2_CUDA_TRY(cudaGetLastError());
+    launched += chunk;
+    return pipe.mark(st, launched, s);
+  };
+  SB2_TRY(enqueue());
+  chunk = 8;
+  SB2_TRY(enqueue());
+  for (;;) {
+    ChainState<double> h;
+    int at = 0;
+    SB2_TRY(pipe.wait(&h, &at));
+    if (h.done || at > max_iter + 1) break;
+    // iterations here cost a preconditioner apply each: few are queued past
+    // the stop
+    chunk = plan.next(h.nb_iter, h.reste, tol, launched - at, std::min(chunk * 2, 16), 2, 16);
     SB2_TRY(enqueue());
   }
   SB2_CUDA_TRY(cudaStreamSynchronize(s));

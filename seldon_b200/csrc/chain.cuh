@@ -58,6 +58,13 @@ struct ChainArgs {
   int* hist_it;
 };
 
+// A preconditioner apply z = M^{-1} r enqueued on a stream (chain_pcg).
+struct PrecondLaunch {
+  const sb2_precond* M;
+  bool trans;
+  int operator()(const double* r, double* z, cudaStream_t s) const;
+};
+
 // Size of the next chunk of a chained loop: from the residual's decrease over
 // the last chunk, the iterations still needed to reach `target` (a relative
 // residual: the stop, or the next correction), less those already queued,

@@ -1019,6 +1019,9 @@ static std::atomic<int> g_chain_min_n{2800000};
 // Systems that fit one thread-block cluster's shared memory run CG there.
 static std::atomic<int> g_cluster_cg{1};
 static std::atomic<int> g_cluster_cap{16};  // most CTAs a cluster may take
+// Cg with SOR or ILUT preconditioning runs as a device-resident chain (1) or
+// host-driven, one library call per operation (0): sb2_krylov_set_pcg.
+static std::atomic<int> g_pcg_device{1};
 
 // ----------------------------------------------------------------- cluster-resident CG
 //
@@ -1322,6 +1325,51 @@ static int chain_cg_solve(const sb2_csr* A, const double* diag, double* x, const
   return SB2_OK;
 }
 
+int chain_pcg(const SellOp<double>& S, int n, const PrecondLaunch& apply, double* x,
+              const double* b, double* work, ChainState<double>* st, double* part, double* hist,
+              int* hist_it, int hist_cap, double tol, int max_iter, int init_guess_null,
+              cudaStream_t s, ChainState<double>* out);
+
+int PrecondLaunch::operator()(const double* r, double* z, cudaStream_t s) const {
+  return precond_apply(M, trans, r, z, s);
+}
+
+// Cg with an SOR or ILUT preconditioner: the chained passes with the
+// preconditioner's own launches between them, scalars on the device.
+static int pcg_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+                     const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
+                     int* hist_it, int hist_cap, cudaStream_t s) {
+  const SellOp<double> S = sell_op(A->full);
+  const int n = A->m;
+  const long long slots = chain_part_slots(S, n);
+  const int hcap = std::max(hist_cap, 1);
+  const size_t vb = sizeof(double) * 4 * (size_t)n;
+  const size_t sb = 256, pb = sizeof(double) * slots, hb = sizeof(double) * hcap, ib = sizeof(int) * hcap;
+  DeviceBuf buf;
+  buf.s = s;
+  SB2_CUDA_TRY(pool_malloc((void**)&buf.p, vb + sb + pb + hb + ib + 64, s));
+  char* c = (char*)buf.p;
+  double* work = (double*)c;
+  ChainState<double>* st = (ChainState<double>*)(c + vb);
+  double* part = (double*)(c + vb + sb);
+  double* dh = (double*)(c + vb + sb + pb);
+  int* dhi = (int*)(c + vb + sb + pb + hb);
+  ChainState<double> o;
+  SB2_TRY(chain_pcg(S, n, PrecondLaunch{M, false}, x, b, work, st, part, dh, dhi, hcap, prm->tol,
+                    prm->max_iter, prm->init_guess_null, s, &o));
+  const int nh = std::min(o.hist_len, std::max(hist_cap, 0));
+  if (hist && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist, dh, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+  if (hist_it && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist_it, dhi, sizeof(int) * nh, cudaMemcpyDeviceToHost));
+  res->init_failed = o.init_failed;
+  res->nb_iter = o.init_failed ? 0 : o.nb_iter;
+  res->error_code = o.init_failed ? (prm->max_iter <= 0 ? -2 : 0)
+                                  : (o.nb_iter >= prm->max_iter ? -2 : o.fail);
+  res->hist_len = o.init_failed ? 0 : nh;
+  res->facteur_reste = o.facteur;
+  res->last_residual = o.reste;
+  return SB2_OK;
+}
+
 static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
                        double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
@@ -1339,6 +1387,9 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   } else if (M && precond_matrix(M) != A) {
     return SB2_ERR_INVALID_VALUE;
   }
+  if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && which == kCg &&
+      A->full.sell.nslice >= 0 && g_pcg_device)
+    return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;
@@ -1371,6 +1422,12 @@ int sb2_krylov_set_cluster(int on) try {
   } else if (on == 1) {
     g_cluster_cap = kClusterMaxRanks;
   }
+  return old;
+} SB2_CATCH
+
+int sb2_krylov_set_pcg(int device_resident) try {
+  const int old = g_pcg_device;
+  g_pcg_device = device_resident ? 1 : 0;
   return old;
 } SB2_CATCH
 

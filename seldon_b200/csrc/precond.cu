@@ -450,10 +450,10 @@ static int plan_sor(sb2_precond* M) {
   return SB2_OK;
 }
 
-// SOR(A, X, B, omega, iter, type_ssor) on device, in place on x.
-static int sor_apply(sb2_precond* M, double* x, const double* b, double omega,
-                     int iter, int type_ssor, cudaStream_t s) {
-  SB2_TRY(plan_sor(M));
+// SOR(A, X, B, omega, iter, type_ssor) on device, in place on x, once the
+// level plans and the diagonal exist (sor_apply makes them).
+static int sor_run(sb2_precond* M, double* x, const double* b, double omega,
+                   int iter, int type_ssor, cudaStream_t s) {
   const sb2_csr* A = M->A;
   const int n = A->m;
   if (!A->sym) {
@@ -479,6 +479,13 @@ static int sor_apply(sb2_precond* M, double* x, const double* b, double omega,
       SB2_TRY(run_levels(M->bwd, n, SymBwd2{u.d_ptr, u.d_ind, u.d_val, M->d_t, x, omega}, s));
     }
   return SB2_OK;
+}
+
+static int sor_apply(sb2_precond* M, double* x, const double* b, double omega,
+                     int iter, int type_ssor, cudaStream_t s) {
+  SB2_TRY(plan_sor(M));
+  if (!M->A->sym) SB2_TRY(ensure_diag(M->A));
+  return sor_run(M, x, b, omega, iter, type_ssor, s);
 }
 
 // Levels of a gather sweep: row j waits for every row it reads; rows are
@@ -727,11 +734,13 @@ static int ilut_launch(const sb2_precond* M, bool trans, const double* r, double
 
 constexpr int kIluGraphs = 8;  // recorded applies kept per preconditioner
 
-// Small systems run every level in one CTA (one launch).  Larger ones
-// replay a recorded graph of the per-level launches: the launches then cost
-// the device's dependency resolution only, not a host call each.
-static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cudaStream_t s) {
-  if (M->n_ilu <= kSorSingleCtaMaxN) return ilut_launch(M, trans, r, z, s);
+// Applies of large systems launch once per level: they are recorded once per
+// (r, z, direction) as a CUDA graph and replayed, so the launches cost the
+// device's dependency resolution only, not a host call each.  `launch`
+// enqueues the apply on the stream it is given.
+template <class Launch>
+static int replay_recorded(sb2_precond* M, bool trans, const double* r, double* z,
+                           cudaStream_t s, const Launch& launch) {
   std::lock_guard<std::mutex> g(M->mu);
   for (const auto& e : M->graphs)
     if (e.r == r && e.z == z && e.trans == trans) {
@@ -741,7 +750,7 @@ static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cu
   if (!M->cap_stream)
     SB2_CUDA_TRY(cudaStreamCreateWithFlags(&M->cap_stream, cudaStreamNonBlocking));
   SB2_CUDA_TRY(cudaStreamBeginCapture(M->cap_stream, cudaStreamCaptureModeThreadLocal));
-  int st = ilut_launch(M, trans, r, z, M->cap_stream);
+  int st = launch(M->cap_stream);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(M->cap_stream, &graph);
   if (st != SB2_OK) {
@@ -762,6 +771,15 @@ static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cu
   M->graphs.push_back({r, z, trans, exec});
   SB2_CUDA_TRY(cudaGraphLaunch(exec, s));
   return SB2_OK;
+}
+
+// Small systems run every level in one CTA (one launch); larger ones replay
+// a recorded graph of the per-level launches.
+static int ilut_apply(sb2_precond* M, bool trans, const double* r, double* z, cudaStream_t s) {
+  if (M->n_ilu <= kSorSingleCtaMaxN) return ilut_launch(M, trans, r, z, s);
+  return replay_recorded(M, trans, r, z, s, [&](cudaStream_t cs) {
+    return ilut_launch(M, trans, r, z, cs);
+  });
 }
 
 int precond_kind(const sb2_precond* M) { return M->kind; }
@@ -786,9 +804,16 @@ int precond_apply(const sb2_precond* cM, bool trans, const double* r, double* z,
     return SB2_OK;
   }
   // SorPreconditioner::Solve / TransSolve (Precond_Ssor.cxx:62-90)
-  SB2_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(double) * n, s));
   const int type = M->symmetric ? 0 : (trans ? 3 : 2);
-  return sor_apply(M, z, r, M->omega, M->nb_iter, type, s);
+  SB2_TRY(plan_sor(M));
+  if (!M->A->sym) SB2_TRY(ensure_diag(M->A));
+  auto launch = [&](cudaStream_t cs) -> int {
+    SB2_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(double) * n, cs));
+    return sor_run(M, z, r, M->omega, M->nb_iter, type, cs);
+  };
+  if (n <= kSorSingleCtaMaxN) return launch(s);
+  // the symmetric sweeps' trans flag does not change the launches
+  return replay_recorded(M, M->symmetric ? false : trans, r, z, s, launch);
 }
 
 }  // namespace sb2

@@ -108,6 +108,38 @@ __global__ void __launch_bounds__(NT) sell_long_kernel(SellOp<double> S, double 
   sell_spmv_long<NT, double, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
 }
 
+// Measurement kernel: sum_k val[k] * x[ind[k]] over one array of entries,
+// with no rows (val == nullptr: sum_k x[ind[k]]).  It streams the index and
+// value arrays and gathers x exactly as a CSR product over the same arrays
+// does, without the per-row sums: its time bounds from below what any row
+// binning of that product can reach.  Each CTA writes one partial sum.
+__global__ void __launch_bounds__(256) probe_gather_kernel(long long nnz, const int* __restrict__ ind,
+                                                          const double* __restrict__ val,
+                                                          const double* __restrict__ x,
+                                                          double* __restrict__ partials) {
+  __shared__ double s_red[8];
+  double acc0 = 0.0, acc1 = 0.0;
+  const long long q4 = nnz / 4;  // groups of 4 entries (16-byte index loads)
+  for (long long g = (long long)blockIdx.x * 256 + threadIdx.x; g < q4; g += (long long)gridDim.x * 256) {
+    const int4 c = __ldcs(reinterpret_cast<const int4*>(ind) + g);
+    const double x0 = __ldg(x + c.x), x1 = __ldg(x + c.y), x2 = __ldg(x + c.z), x3 = __ldg(x + c.w);
+    if (val) {
+      double v[4];
+      ld_stream_val4(val + 4 * g, v);
+      acc0 = add_rn(acc0, add_rn(mul_rn(v[0], x0), mul_rn(v[1], x1)));
+      acc1 = add_rn(acc1, add_rn(mul_rn(v[2], x2), mul_rn(v[3], x3)));
+    } else {
+      acc0 = add_rn(acc0, add_rn(x0, x1));
+      acc1 = add_rn(acc1, add_rn(x2, x3));
+    }
+  }
+  for (long long k = 4 * q4 + (long long)blockIdx.x * 256 + threadIdx.x; k < nnz;
+       k += (long long)gridDim.x * 256)
+    acc0 = add_rn(acc0, val ? mul_rn(__ldg(val + k), __ldg(x + __ldg(ind + k))) : __ldg(x + __ldg(ind + k)));
+  const double t = block_sum<256>(add_rn(acc0, acc1), s_red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
 SellOp<double> sell_op(const CsrArrays& a) {
   const SellArrays& s = a.sell;
   return SellOp<double>{s.nslice, s.d_sptr, s.d_qinfo, s.d_qrows, s.d_scol, s.d_sval, s.nwarp,
@@ -360,6 +392,18 @@ int sb2_mlt_host_batch(const sb2_csr* cA, int trans, double alpha, int count,
   // every product and every copy out has completed when s_out has
   SB2_CUDA_TRY(cudaStreamSynchronize(A->s_out));
   return SB2_OK;
+} SB2_CATCH
+
+int sb2_probe_gather(long long nnz, const int* ind, const double* val, const double* x,
+                     double* partials, int max_blocks, int* blocks, void* stream) try {
+  if (nnz < 0 || max_blocks < 1 || !blocks || (nnz > 0 && (!ind || !x || !partials)))
+    return SB2_ERR_INVALID_VALUE;
+  if ((reinterpret_cast<uintptr_t>(ind) & 15u) || (val && (reinterpret_cast<uintptr_t>(val) & 15u)))
+    return SB2_ERR_INVALID_VALUE;  // 16-byte loads of the streams
+  const int g = std::max(1, std::min(max_blocks, num_sms(current_device()) * 8));
+  *blocks = g;
+  probe_gather_kernel<<<g, 256, 0, (cudaStream_t)stream>>>(nnz, ind, val, x, partials);
+  return map_cuda_error(cudaGetLastError());
 } SB2_CATCH
 
 }  // extern "C"

@@ -28,10 +28,17 @@ def _systems(seed, k, lo, hi, zero=()):
     return systems, rhs, xs
 
 
+PLANS = [(128, 0), (256, 0), (512, 0), (256, 64), (512, 1024), (128, 100000)]
+
+
 @pytest.mark.parametrize("mixed", [True, False])
-def test_batch_matches_oracle(api, oracle, mixed):
+@pytest.mark.parametrize("plan", PLANS)
+def test_batch_matches_oracle(api, oracle, mixed, plan):
+    """Every plan: CTAs only, warps for the smaller systems, warps for all."""
     systems, rhs, xs = _systems(1, 40, 4, 30)
     B = api.Batch(systems)
+    B.set_plan(*plan)
+    assert B.plan() == plan
     import torch
     X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
     it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
@@ -79,6 +86,14 @@ def test_batch_autotune_and_graph(api):
     b = to_dev(np.concatenate(rhs))
     X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
     assert B.autotune(X, b, tol=1e-9) in (128, 256, 512)
+    chosen = B.plan()
+    assert chosen[1] in (0, 256, 1024)
+    # a batch with the same size histogram takes the cached plan
+    B2 = api.Batch(systems)
+    B2.set_plan(128, 0)
+    B2.autotune(X, b, tol=1e-9)
+    assert B2.plan() == chosen
+    B2.close()
     # the solve enqueues only device work: capture it once, replay it
     X.zero_()
     it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
