@@ -56,6 +56,13 @@ def parse():
                         "(default all)")
     p.add_argument("--cpu-seconds", type=float, default=8.0,
                    help="bounded CPU-baseline sample (seconds of work)")
+    p.add_argument("--gmres-grid", type=int, default=GRID,
+                   help="grid side of the GMRES extras' convection-diffusion problem (profiling "
+                        "captures take a smaller one)")
+    p.add_argument("--batch-systems", type=int, default=4096,
+                   help="systems of the batch extra (profiling captures take fewer)")
+    p.add_argument("--batch-plan", default=None,
+                   help="threads,warp_max: a fixed batch plan instead of the autotuner's")
     p.add_argument("--no-cpu-solves", action="store_true",
                    help="skip the reference's host solves beside the solver extras")
     return p.parse_args()
@@ -357,7 +364,8 @@ def run_ours(args, rank, world, local):
     extras = {}
     if rank == 0 and not args.no_extras:
         extras = run_extras(api, matgen, torch, dev, args.extras,
-                            cpu=(world == 1 and not args.no_cpu_solves))
+                            cpu=(world == 1 and not args.no_cpu_solves), gmres_grid=args.gmres_grid,
+                            batch_systems=args.batch_systems, batch_plan=args.batch_plan)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -396,7 +404,8 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
-def run_extras(api, matgen, torch, dev, which="all", cpu=True):
+def run_extras(api, matgen, torch, dev, which="all", cpu=True, gmres_grid=128, batch_systems=4096,
+               batch_plan=None):
     """Time-to-solution figures on the other configurations (device-timed).
     `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, assemble,
     ilu0, or all.  With `cpu`, the reference's own solvers then run on the
@@ -434,11 +443,13 @@ def run_extras(api, matgen, torch, dev, which="all", cpu=True):
     if "adjoint" in want:
         out["adjoint_aniso512"] = run_adjoint(matgen, torch, dev, timed)
     if "batch" in want:
-        out["batch_lap2d_4096"] = run_batch(api, matgen, torch, dev, timed, jobs)
+        key = "batch_lap2d_4096" if batch_systems == 4096 else f"batch_lap2d_{batch_systems}"
+        out[key] = run_batch(api, matgen, torch, dev, timed, jobs, nsys=batch_systems,
+                             plan=batch_plan)
     if "c1" in want:
         out.update(extra_c1(api, matgen, torch, dev, timed, jobs))
     if "gmres" in want:
-        out.update(extra_gmres(api, matgen, torch, dev, timed, jobs))
+        out.update(extra_gmres(api, matgen, torch, dev, timed, jobs, gmres_grid))
     if "c3" in want:
         out.update(extra_c3(api, matgen, torch, dev, timed, jobs))
     if cpu and jobs:
@@ -619,13 +630,13 @@ def gmres_bytes(n, nnz, iterations, m, vw, mw, variant):
     return total
 
 
-def extra_gmres(api, matgen, torch, dev, timed, jobs):
+def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
     """GMRES(30) + Jacobi on the 128^3 convection-diffusion problem: Seldon's
     modified Gram-Schmidt order, the CGS2 variant, and the iterative
     refinement whose inner solve is GMRES(30) with an FP32 basis."""
-    ptr, ind, val = matgen.convdiff3d(GRID)
+    ptr, ind, val = matgen.convdiff3d(g)
     n = ptr.size - 1
-    xs = np.random.default_rng(GRID).uniform(-1, 1, n)
+    xs = np.random.default_rng(g).uniform(-1, 1, n)
     bh = matgen.matvec(ptr, ind, val, xs)
     b = torch.as_tensor(bh, device=dev)
     A = api.RowSparse(n, n, ptr, ind, val)
@@ -646,7 +657,10 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs):
         return float(np.linalg.norm(matgen.matvec(ptr, ind, val, x) - bh) / np.linalg.norm(bh))
     out = {}
     xs_gpu = {}
-    for key, orth in (("gmres30_jacobi_convdiff128", "mgs"), ("gmres30_cgs2_jacobi_convdiff128", "cgs2")):
+    sfx = f"convdiff{g}"
+    k_mgs, k_cgs2, k_ir = (f"gmres30_jacobi_{sfx}", f"gmres30_cgs2_jacobi_{sfx}",
+                           f"ir_gmres30_jacobi_{sfx}")
+    for key, orth in ((k_mgs, "mgs"), (k_cgs2, "cgs2")):
         gm(orth)()  # warm-up: the Krylov basis (0.5 GB) is mapped into the pool once
         ms, (it, X) = timed(gm(orth), reps=2)
         x = X.cpu().numpy()
@@ -658,10 +672,10 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs):
                     "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
                     "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
                     "timing": "best of 2"}
-    out["gmres30_cgs2_jacobi_convdiff128"]["forward_diff_vs_mgs"] = float(
+    out[k_cgs2]["forward_diff_vs_mgs"] = float(
         np.linalg.norm(xs_gpu["cgs2"] - xs_gpu["mgs"]) / np.linalg.norm(xs_gpu["mgs"]))
-    out["gmres30_cgs2_jacobi_convdiff128"]["speedup_vs_mgs"] = round(
-        out["gmres30_jacobi_convdiff128"]["ms"] / out["gmres30_cgs2_jacobi_convdiff128"]["ms"], 3)
+    out[k_cgs2]["speedup_vs_mgs"] = round(
+        out[k_mgs]["ms"] / out[k_cgs2]["ms"], 3)
 
     def ir():
         X = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -670,22 +684,22 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs):
     ir()
     ms, (code, info, X) = timed(ir, reps=2)
     x = X.cpu().numpy()
-    best64 = min(out["gmres30_jacobi_convdiff128"]["ms"], out["gmres30_cgs2_jacobi_convdiff128"]["ms"])
+    best64 = min(out[k_mgs]["ms"], out[k_cgs2]["ms"])
     nbytes = gmres_bytes(n, ind.size, info["inner_iter"], 30, 4, 4, "cgs2")
-    out["ir_gmres30_jacobi_convdiff128"] = {
+    out[k_ir] = {
         "ms": round(ms, 2), "error_code": code, "outer_iter": info["outer_iter"],
         "inner_iter": info["inner_iter"], "rel_residual_fp64": info["rel_residual"],
         "rel_residual_host_check": host_relres(x),
         "forward_error_vs_fp64_gmres": float(np.linalg.norm(x - xs_gpu["mgs"]) /
                                              np.linalg.norm(xs_gpu["mgs"])),
         "forward_error_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs)),
-        "speedup_vs_fp64_gmres_mgs": round(out["gmres30_jacobi_convdiff128"]["ms"] / ms, 3),
+        "speedup_vs_fp64_gmres_mgs": round(out[k_mgs]["ms"] / ms, 3),
         "speedup_vs_best_fp64_gmres": round(best64 / ms, 3),
         "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
         "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
         "timing": "best of 2"}
     x = xs_gpu["mgs"]
-    jobs.append(("gmres30_jacobi_convdiff128",
+    jobs.append((k_mgs,
                  lambda: _cpu_solve("gmres", ptr, ind, val, bh, x, precond=1, restart=30), False))
     return out
 
@@ -825,7 +839,7 @@ def extra_ilu0(api, matgen, torch, dev, timed):
     return {"ilu0_conv128": out}
 
 
-def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every=8):
+def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every=8, plan=None):
     """4096 shifted 2D Laplacians (side uniform in [8,140]) in one persistent
     launch, against a loop of plain FP64 CG calls over every 8th system; on
     the host, the reference's Cg on the same sample, K systems at a time on K
@@ -846,14 +860,34 @@ def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every
     X = torch.zeros(Bt.m, dtype=torch.float64, device=dev)
     its = torch.zeros(Bt.nsys, dtype=torch.int32, device=dev)
     rr = torch.zeros(Bt.nsys, dtype=torch.float64, device=dev)
+    t0 = time.perf_counter()
+    if plan:
+        Bt.set_plan(*(int(v) for v in plan.split(",")))
+    else:
+        Bt.autotune(X, b, tol=1e-9)
+    tune_s = time.perf_counter() - t0
+    threads, warp_max = Bt.plan()
     out = {"systems": nsys, "rows": Bt.m, "nnz": int(sum(s[1].size for s in systems)),
-           "tol": 1e-9, "autotuned_threads": Bt.autotune(X, b, tol=1e-9)}
+           "tol": 1e-9, "plan": {"threads": threads, "warp_max_rows": warp_max,
+                                 "autotune_s": round(tune_s, 2)}}
+    rows = np.array([s[0].size - 1 for s in systems], dtype=np.float64)
+    nnzs = np.array([s[1].size for s in systems], dtype=np.float64)
+    peak, _ = measured_peak()
     for key, mixed in (("mixed", True), ("fp64", False)):
         Bt.solve(X, b, its, rr, tol=1e-9, mixed=mixed)
-        ms, res = timed(lambda: Bt.solve(X, b, its, rr, tol=1e-9, mixed=mixed))
+        ms, res = timed(lambda: Bt.solve(X, b, its, rr, tol=1e-9, mixed=mixed), reps=2)
+        it_s = its.cpu().numpy().astype(np.float64)
+        # least traffic per iteration of one system: its matrix (values and
+        # 2-byte columns), row pointers, and the vector passes (the product
+        # gathers r and p and writes p and q; the update reads d or x, p, r, q
+        # and writes d or x, r)
+        vb, mb = (4, 6) if mixed else (8, 10)
+        nbytes = float(np.sum(it_s * (nnzs * mb + rows * (4 + 10 * vb))))
         out[key] = {"ms": round(ms, 2), "systems_per_s": round(nsys / ms * 1e3, 1),
                     "converged": res.converged, "max_iter": res.max_iter,
-                    "total_iter": res.total_iter, "max_rel_residual": res.max_rel_residual}
+                    "total_iter": res.total_iter, "max_rel_residual": res.max_rel_residual,
+                    "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                    "frac_of_measured_hbm_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3)}
     # graph-captured launch (no host synchronisation inside)
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g):

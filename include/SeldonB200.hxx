@@ -1599,7 +1599,7 @@ namespace Seldon
       }
     };
 
-    enum SolverKind { kCg, kBiCgStab, kGmres };
+    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2 };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
@@ -1649,10 +1649,14 @@ namespace Seldon
         st = sb2_bicgstab(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                           cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                           GetStream());
-      else
+      else if (kind == kGmres)
         st = sb2_gmres(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                        cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                        GetStream());
+      else
+        st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                            cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
+                            GetStream());
       Check(st, kind == kCg ? "Cg" : (kind == kBiCgStab ? "BiCgStab" : "Gmres"));
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1775,6 +1779,31 @@ namespace Seldon
             Preconditioner& M, Iteration<Titer>& outer)
   {
     return b200::Solve(b200::kGmres, A, x, b, M, outer);
+  }
+
+  //! Gmres(m) with classical Gram-Schmidt applied twice in place of the
+  //! reference's modified Gram-Schmidt loop (sb2_gmres_cgs2): a labelled
+  //! variant with no counterpart in the reference, same restarts, rotations,
+  //! stopping rule and Iteration state; identity or Jacobi preconditioner
+  //! and restart <= 32 (SorPreconditioner, the ILUT preconditioner or a
+  //! larger restart raise Error).  For a preconditioner class this header
+  //! does not know, Seldon's own Gmres runs on the device types.
+  template <class Titer, class Prop, class Preconditioner>
+  int GmresCgs2(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+                Vector<double, VectFull, CudaAlloc<double> >& x,
+                const Vector<double, VectFull, CudaAlloc<double> >& b,
+                Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGmresCgs2, A, x, b, M, outer);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int GmresCgs2(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+                Vector<double, VectFull, CudaAlloc<double> >& x,
+                const Vector<double, VectFull, CudaAlloc<double> >& b,
+                Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGmresCgs2, A, x, b, M, outer);
   }
 
 

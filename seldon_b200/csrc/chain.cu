@@ -674,11 +674,15 @@ int chain_pcg(const SellOp<double>& S, int n, const PrecondLaunch& apply, double
   else
     SB2_TRY((launch_spmv_pair<double, double>(1, a, S, s)));
   SB2_CUDA_TRY(cudaGetLastError());
+  // An iteration here costs a preconditioner apply, whose launches cannot
+  // see the stop flag: no chunk is queued ahead of the one the host waits
+  // for (an apply after the stop would be wasted), and the chunk is sized
+  // from the residual's decay so that it ends near the stop.
   ChainPipe<double> pipe;
   SB2_TRY(pipe.init());
   ChunkPlanner plan;
   int launched = 0, chunk = 4;
-  auto enqueue = [&]() -> int {
+  for (;;) {
     for (int c = 0; c < chunk; c++) {
       SB2_TRY(apply(a.r, z, s));
       SB2_CUDA_TRY(launch_pdl(k_pc_rz<double>, ge, s, a, (const double*)z));
@@ -688,20 +692,12 @@ int chain_pcg(const SellOp<double>& S, int n, const PrecondLaunch& apply, double
     }
     SB2_CUDA_TRY(cudaGetLastError());
     launched += chunk;
-    return pipe.mark(st, launched, s);
-  };
-  SB2_TRY(enqueue());
-  chunk = 8;
-  SB2_TRY(enqueue());
-  for (;;) {
+    SB2_TRY(pipe.mark(st, launched, s));
     ChainState<double> h;
     int at = 0;
     SB2_TRY(pipe.wait(&h, &at));
     if (h.done || at > max_iter + 1) break;
-    // iterations here cost a preconditioner apply each: few are queued past
-    // the stop
-    chunk = plan.next(h.nb_iter, h.reste, tol, launched - at, std::min(chunk * 2, 16), 2, 16);
-    SB2_TRY(enqueue());
+    chunk = plan.next(h.nb_iter, h.reste, tol, 0, std::min(chunk * 2, 16), 1, 16);
   }
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));
