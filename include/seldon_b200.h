@@ -177,6 +177,19 @@ int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
 int sb2_mlt_host_batch(const sb2_csr* A, int trans, double alpha, int count,
                        const double* x_host, double* y_host, void* stream);
 
+/* The x-tiled product of long rows (standalone products only; the solvers'
+ * fused kernels keep the binned product).  On an operator's first product,
+ * if its rows longer than min_row_len (33..1024; default 128) hold at least
+ * min_entries entries (default 2^20) and x spans more than a quarter of a
+ * tile, those rows get a second, tile-major copy of their entries (2-byte
+ * columns relative to a tile of 12288 entries of x), and the product copies
+ * x through shared memory tile by tile (bulk copies, double buffered)
+ * instead of gathering it from L2.  A row is still summed in stored order,
+ * so rows whose columns are sorted give the reference's bits.  The setting
+ * applies to operators not yet multiplied.  No counterpart in the reference
+ * (a layout choice of this engine). */
+int sb2_spmv_set_tiling(int min_row_len, long long min_entries);
+
 /* Product algorithm and launch configuration, chosen by the autotuner; no
  * counterpart in the reference (tuning knobs of this engine).
  *   algo     SB2_SPMV_SELL   binned SELL-32 (thread/warp/CTA per row), default

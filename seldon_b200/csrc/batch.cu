@@ -152,31 +152,28 @@ __device__ double fp64_residual(G& g, const BatchArgs& a, int r0, int n, const d
   return g.sum(acc);
 }
 
-// One CG iteration's product with the direction update folded in: the
-// direction p_new = first ? r : beta*p_old + zc*r is computed where the
-// product reads it (p_old and r are complete), written for the group's own
-// rows into the other buffer, and q = A p_new with (p_new, q).  This saves
-// the separate direction pass and its synchronization; every thread that
-// needs p_new(c) computes it from the same values, so all agree bit for bit.
+// p = first ? r : beta*p + zc*r on the group's rows (Mlt(beta, p); Add(zc, r, p)).
+template <class G, typename T>
+__device__ __forceinline__ void direction(G& g, int n, const T* __restrict__ r, T* __restrict__ p,
+                                          bool first, T beta, T zc) {
+  for (int i = g.rank(); i < n; i += G::kSize)
+    p[i] = first ? r[i] : add_rn(mul_rn(p[i], beta), mul_rn(zc, r[i]));
+}
+
+// q = A p over one system (entries in stored order) with (p, q), summed over
+// the group (its reduction orders the writes of q before any later read).
 template <class G, typename IT, typename VT, typename T>
-__device__ __forceinline__ T fused_direction_product(G& g, const BatchArgs& a, const VT* __restrict__ val,
-                                                     int r0, int n, const T* __restrict__ r,
-                                                     const T* __restrict__ po, T* __restrict__ pw,
-                                                     T* __restrict__ q, bool first, T beta, T zc) {
+__device__ __forceinline__ T product_dot(G& g, const BatchArgs& a, const VT* __restrict__ val,
+                                         int r0, int n, const T* __restrict__ p,
+                                         T* __restrict__ q) {
   const IT* __restrict__ ind = static_cast<const IT*>(a.ind);
   T pq = T(0);
   for (int i = g.rank(); i < n; i += G::kSize) {
     const int k0 = __ldg(a.ptr + r0 + i), k1 = __ldg(a.ptr + r0 + i + 1);
     T t = T(0);
-    for (int k = k0; k < k1; k++) {
-      const int c = __ldg(ind + k);
-      const T pc = first ? r[c] : add_rn(mul_rn(po[c], beta), mul_rn(zc, r[c]));
-      t = add_rn(t, mul_rn(T(__ldg(val + k)), pc));
-    }
-    const T pi = first ? r[i] : add_rn(mul_rn(po[i], beta), mul_rn(zc, r[i]));
-    pw[i] = pi;
+    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(T(__ldg(val + k)), p[__ldg(ind + k)]));
     q[i] = t;
-    pq = add_rn(pq, mul_rn(pi, t));
+    pq = add_rn(pq, mul_rn(p[i], t));
   }
   return g.sum(pq);
 }
@@ -186,8 +183,7 @@ template <class G, typename IT>
 __device__ void solve_fp64(G& g, const BatchArgs& a, int s, int r0, int n, double nb) {
   double* x = a.x + r0;
   double* r = a.r64 + r0;
-  double* po = reinterpret_cast<double*>(a.w32) + r0;  // the two direction buffers
-  double* pw = reinterpret_cast<double*>(a.w32) + (size_t)a.m + r0;
+  double* p = reinterpret_cast<double*>(a.w32) + r0;
   double* q = reinterpret_cast<double*>(a.w32) + 2 * (size_t)a.m + r0;
   double rr;
   if (a.init_guess_null) {
@@ -207,14 +203,11 @@ __device__ void solve_fp64(G& g, const BatchArgs& a, int s, int r0, int n, doubl
   int it = 0;
   while (!(res < a.tol) && it < a.max_iter) {
     if (rho == 0.0) break;
-    const double delta = fused_direction_product<G, IT, double, double>(
-        g, a, a.val, r0, n, r, po, pw, q, it == 0, beta, 1.0);
-    double* t = po;  // the new direction is now the current one
-    po = pw;
-    pw = t;
+    direction(g, n, r, p, it == 0, beta, 1.0);
+    g.sync();
+    const double delta = product_dot<G, IT, double, double>(g, a, a.val, r0, n, p, q);
     if (delta == 0.0) break;
     const double alpha = rho / delta;
-    const double* p = po;
     double acc = 0.0;
     for (int i = g.rank(); i < n; i += G::kSize) {
       x[i] = add_rn(x[i], mul_rn(alpha, p[i]));
@@ -240,8 +233,7 @@ template <class G, typename IT>
 __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, double nb) {
   double* x = a.x + r0;
   float* r = a.w32 + r0;
-  float* po = a.w32 + (size_t)a.m + r0;  // the two direction buffers
-  float* pw = a.w32 + 2 * (size_t)a.m + r0;
+  float* p = a.w32 + (size_t)a.m + r0;
   float* q = a.w32 + 3 * (size_t)a.m + r0;
   float* d = a.w32 + 4 * (size_t)a.m + r0;
   if (a.init_guess_null)
@@ -269,16 +261,13 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
   float rmax = sqrtf(rho);
   bool first = true;
   for (;;) {
-    const float delta = fused_direction_product<G, IT, float, float>(
-        g, a, a.val32, r0, n, r, po, pw, q, first, beta, zc);
-    float* t = po;  // the new direction is now the current one
-    po = pw;
-    pw = t;
+    direction(g, n, r, p, first, beta, zc);
+    g.sync();
+    const float delta = product_dot<G, IT, float, float>(g, a, a.val32, r0, n, p, q);
     first = false;
     zc = 1.0f;
     if (delta == 0.0f) break;
     const float alpha = rho / delta;
-    const float* p = po;
     acc = 0.0f;
     for (int i = g.rank(); i < n; i += G::kSize) {
       d[i] = add_rn(d[i], mul_rn(alpha, p[i]));
@@ -356,8 +345,8 @@ __device__ void solve_system(G& g, const BatchArgs& a, int s) {
 // warp_max rows that a CTA takes switches it to warps: from then on (every
 // later system is as small or smaller) each warp takes and solves systems on
 // its own, with shuffle reductions and no CTA barrier.
-template <int NT, typename IT>
-__global__ void __launch_bounds__(NT, 1280 / NT) batch_kernel(BatchArgs a) {
+template <int NT, typename IT, bool WARPS>
+__global__ void __launch_bounds__(NT, 1536 / NT) batch_kernel(BatchArgs a) {
   __shared__ int s_sys;
   __shared__ double s_red[2 * 2 * (NT / 32)];
   CtaGroup<NT> cg{s_red, 0};
@@ -371,13 +360,14 @@ __global__ void __launch_bounds__(NT, 1280 / NT) batch_kernel(BatchArgs a) {
     const int s = s_sys;
     __syncthreads();
     if (s < 0) return;
-    if (__ldg(a.sys_row + s + 1) - __ldg(a.sys_row + s) <= a.warp_max) {
+    if (WARPS && __ldg(a.sys_row + s + 1) - __ldg(a.sys_row + s) <= a.warp_max) {
       small = s;
       break;
     }
     solve_system<CtaGroup<NT>, IT>(cg, a, s);
     __syncthreads();
   }
+  if constexpr (WARPS) {
   WarpGroup wg;
   const int lane = threadIdx.x & 31;
   int s = (threadIdx.x >> 5) == 0 ? small : -2;
@@ -395,27 +385,36 @@ __global__ void __launch_bounds__(NT, 1280 / NT) batch_kernel(BatchArgs a) {
     __syncwarp();
     s = -2;
   }
+  }
 }
 
-template <int NT, typename IT>
+template <int NT, typename IT, bool WARPS>
 static int launch_batch(const BatchArgs& a, cudaStream_t s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT, IT>, NT, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT, IT, WARPS>, NT, 0) !=
+          cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const int grid = std::min(a.nsys, per_sm * num_sms(current_device()));
-  batch_kernel<NT, IT><<<std::max(grid, 1), NT, 0, s>>>(a);
+  batch_kernel<NT, IT, WARPS><<<std::max(grid, 1), NT, 0, s>>>(a);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
 }
 
+// the kernel without the warp path (warp_max == 0) keeps fewer registers
+template <typename IT, bool WARPS>
+static int launch_batch_w(const BatchArgs& a, int threads, cudaStream_t s) {
+  switch (threads) {
+    case 128: return launch_batch<128, IT, WARPS>(a, s);
+    case 512: return launch_batch<512, IT, WARPS>(a, s);
+    default: return launch_batch<256, IT, WARPS>(a, s);
+  }
+}
+
 template <typename IT>
 static int launch_batch_t(const BatchArgs& a, int threads, cudaStream_t s) {
-  switch (threads) {
-    case 128: return launch_batch<128, IT>(a, s);
-    case 512: return launch_batch<512, IT>(a, s);
-    default: return launch_batch<256, IT>(a, s);
-  }
+  return a.warp_max > 0 ? launch_batch_w<IT, true>(a, threads, s)
+                        : launch_batch_w<IT, false>(a, threads, s);
 }
 
 static int batch_run(const sb2_batch* B, double* x, const double* b, const sb2_batch_params* prm,

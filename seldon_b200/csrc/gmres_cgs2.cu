@@ -43,6 +43,7 @@ constexpr int kWarpsG = NTG / 32;
 constexpr int kDotChunk = 16;   // dot products one pass accumulates (registers)
 
 SellOp<double> sell_op(const CsrArrays& a);
+size_t vector_stride(int n, size_t elem_bytes);
 int ensure_fp32(const sb2_csr* A, bool need_diag);
 SellOp<float> sell_op32(const sb2_csr* A);
 
@@ -638,7 +639,7 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = cgs2_grid<VT>(smem, Ain, n);
   if (grid < 1) return SB2_ERR_CUDA;
-  const long long ldv = ((long long)n + 3) / 4 * 4;
+  const long long ldv = (long long)vector_stride(n, sizeof(VT));
   const int hcap = std::max(hist_cap, 0) + 1;
   size_t off = 0;
   auto take = [&](size_t bytes) {

@@ -414,7 +414,8 @@ __global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVec
 
 struct GmresVecs {
   const double* b;
-  double *x, *r, *w, *V;  // V: (m+1) vectors of length n, contiguous
+  double *x, *r, *w, *V;  // V: (m+1) vectors of length n, `ld` apart
+  long long ld;
 };
 
 // epilogue of u = A V_i: w_r = M^{-1} u_r, acc += V0_r * w_r (first MGS dot)
@@ -443,7 +444,7 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
   const int tid = threadIdx.x;
   const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
   const int n = A.n;
-  const size_t nn = (size_t)n;
+  const size_t nn = (size_t)v.ld;
   const bool lead = (blockIdx.x == 0 && tid == 0);
   unsigned epoch = 0;
   int hlen = 0;
@@ -625,10 +626,20 @@ struct SolveScratch {
   int hist_cap = 0;
 };
 
+// Distance between the work vectors of one solve: n rounded up so that the
+// vectors do not start a power of two apart (a solve streaming many of them
+// at once, as GMRES's Gram-Schmidt passes do, would otherwise have its
+// streams fall on the same L2 sets and DRAM channels when n is a power of
+// two): 256 bytes past a multiple of 512.
+size_t vector_stride(int n, size_t elem_bytes) {
+  const size_t bytes = ((size_t)std::max(n, 1) * elem_bytes + 511) / 512 * 512 + 256;
+  return bytes / elem_bytes;
+}
+
 static int alloc_scratch(cudaStream_t s, int n, int nvec, int grid, int hist_cap,
                          SolveScratch* S) {
   S->vecs.s = S->state.s = s;
-  const size_t vbytes = sizeof(double) * (size_t)std::max(n, 1) * nvec;
+  const size_t vbytes = sizeof(double) * vector_stride(n, sizeof(double)) * nvec;
   SB2_CUDA_TRY(pool_malloc((void**)&S->vecs.p, vbytes, s));
   S->vec = (double*)S->vecs.p;
   S->hist_cap = std::max(hist_cap, 1);
@@ -723,7 +734,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   History H{S.hist, S.hist_it, hcap};
   IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null};
   OpArgs op = op_args(A, diag);
-  const size_t nn = (size_t)std::max(n, 1);
+  const size_t nn = vector_stride(n, sizeof(double));
   double* V = S.vec;
   void* args[6];
   CgVecs cv;
@@ -742,7 +753,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
                   V + 7 * nn};
     args[1] = &bv;
   } else {
-    gv = GmresVecs{b, x, V, V + nn, V + 2 * nn};
+    gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
   }
   SB2_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(NT), args, smem, s));

@@ -35,6 +35,8 @@ __attribute__((weak)) int current_device() { return 0; }
 __attribute__((weak)) int map_cuda_error(cudaError_t) { return -3; }
 __attribute__((weak)) int num_sms(int) { return 148; }
 __attribute__((weak)) int ensure_diag(const sb2_csr*) { return 0; }
+struct TiledArrays;
+__attribute__((weak)) void free_tiled(TiledArrays*) {}
 }
 extern "C" {
 cudaError_t cudaGraphDestroy(cudaGraph_t) { return cudaSuccess; }
@@ -57,6 +59,7 @@ cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
 
 extern "C" {
 cudaError_t cudaEventCreate(cudaEvent_t* e) { *e = nullptr; return cudaSuccess; }
+cudaError_t cudaFuncSetAttribute(const void*, cudaFuncAttribute, int) { return cudaSuccess; }
 cudaError_t cudaEventRecord(cudaEvent_t, cudaStream_t) { return cudaSuccess; }
 cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
 cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) { *ms = 1.0f; return cudaSuccess; }
