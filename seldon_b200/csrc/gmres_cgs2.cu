@@ -107,8 +107,18 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
     const int lane = tid & 31, warp = tid >> 5;
     for (int k = warp; k < K; k += kWarpsG) {
       const double* pv = P.partials + (size_t)k * G;
+      // every load of a lane issued before the first add waits on one
       double v = 0.0;
-      for (unsigned g = lane; g < G; g += 32) v = add_rn(v, __ldcg(pv + g));
+      for (unsigned g0 = lane; g0 < G; g0 += 32 * 8) {
+        double part[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const unsigned g = g0 + 32u * q;
+          part[q] = g < G ? __ldcg(pv + g) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) v = add_rn(v, part[q]);
+      }
       v = warp_sum(v);
       if (lane == 0) {
         wide[k] = v;
@@ -412,7 +422,7 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(NTG, 2)
+__global__ void __launch_bounds__(NTG, 3)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];

@@ -113,6 +113,8 @@ struct TiledArrays {
   int* d_rows = nullptr;       // rows, CTA-major, each CTA's by decreasing length
   int* d_rptr = nullptr;       // [ncta+1]
   long long* d_cbase = nullptr;  // [ncta*ntile+1] first entry of each (CTA, tile) chunk
+  long long* d_sbase = nullptr;  // [ncta] first row offset of each CTA's blocks
+  int emax = 0, spmax = 0;     // largest chunk and row-offset block (entries)
   unsigned short* d_seg = nullptr;  // per (CTA, tile): rows+1 offsets into the chunk
   unsigned short* d_col = nullptr;  // column - tile * T
   double* d_val = nullptr;

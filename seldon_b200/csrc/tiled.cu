@@ -28,7 +28,7 @@
 namespace sb2 {
 
 constexpr int kTiledThreads = 512;   // threads (and rows at most) per CTA
-constexpr int kTiledCols = 12288;    // columns per x tile (96 KB, two buffers)
+constexpr int kTiledCols = 6144;     // widest x tile (48 KB a stage)
 
 // Rows longer than this go to the tiled product once the operator has at
 // least kTiledMinEntries entries in such rows (sb2_spmv_set_tiling).
@@ -37,39 +37,57 @@ static std::atomic<long long> g_tiled_min_entries{1 << 20};
 
 struct TiledView {
   int ncta, ntile, T, cols;
+  int emax, spmax;                // largest chunk (entries) and offset block, both padded to 8
   const int* rows;                // [total rows] CTA-major
   const int* rptr;                // [ncta+1]
-  const long long* cbase;         // [ncta*ntile+1] first entry of chunk (c, t)
-  const unsigned short* seg;      // per (c, t): R_c+1 offsets into the chunk
+  const long long* cbase;         // [ncta*ntile+1] first entry of chunk (c, t), a multiple of 8
+  const long long* sbase;         // [ncta] first row offset of CTA c's blocks
+  const unsigned short* seg;      // per (c, t): R_c+1 offsets into the chunk, padded to 8
   const unsigned short* col;      // column - t*T
   const double* val;
 };
 
 #ifdef __CUDACC__
 
+// Stage layout in shared memory (two stages): x tile (T doubles), the chunk's
+// values (emax doubles), its 2-byte columns (emax), its row offsets (spmax).
 template <int NT>
 __global__ void __launch_bounds__(NT, 1)
     tiled_long_kernel(TiledView v, double alpha, const double* __restrict__ x, double beta,
                       double* __restrict__ y, bool overwrite, int* status,
                       unsigned long long limit_ns) {
   extern __shared__ __align__(128) unsigned char smem[];
-  double* xs0 = reinterpret_cast<double*>(smem);
-  double* xs1 = xs0 + v.T;
+  const size_t stage_bytes = (size_t)v.T * 8 + (size_t)v.emax * 10 + (size_t)v.spmax * 2;
   __shared__ __align__(8) unsigned long long bar[2];
   __shared__ int s_abort;
   const int c = blockIdx.x, tid = threadIdx.x;
   const int r0 = v.rptr[c], R = v.rptr[c + 1] - r0;
-  const unsigned short* seg = v.seg + (size_t)v.ntile * (r0 + c);
-  // thread 0 copies tile t of x into buffer t & 1; the bytes up to the last
-  // 16-byte boundary go by bulk copy, a trailing odd entry by a plain load
+  const int SP = (R + 1 + 7) / 8 * 8;  // row offsets per tile, padded to 16 bytes
+  auto xs_of = [&](int st) { return reinterpret_cast<double*>(smem + st * stage_bytes); };
+  auto val_of = [&](int st) { return xs_of(st) + v.T; };
+  auto col_of = [&](int st) {
+    return reinterpret_cast<unsigned short*>(val_of(st) + v.emax);
+  };
+  auto seg_of = [&](int st) { return col_of(st) + v.emax; };
+  // thread 0 copies what tile t needs into stage t & 1: the x tile (a
+  // trailing odd entry by a plain load after the wait), the chunk's values
+  // and columns and the row offsets, all with bulk copies
   auto issue = [&](int t) {
+    const int st = t & 1;
     const long long c0 = (long long)t * v.T;
     const long long cn = min((long long)v.T, (long long)v.cols - c0);
-    const unsigned bytes = (unsigned)((cn * 8) & ~15ll);
-    double* dst = (t & 1) ? xs1 : xs0;
-    fence_proxy_async_smem();  // earlier reads of the buffer come first
-    mbar_expect_tx(&bar[t & 1], bytes);
-    if (bytes) bulk_g2s(dst, x + c0, bytes, &bar[t & 1]);
+    const unsigned xb = (unsigned)((cn * 8) & ~15ll);
+    const long long e0 = v.cbase[(size_t)c * v.ntile + t];
+    const unsigned ne = (unsigned)(v.cbase[(size_t)c * v.ntile + t + 1] - e0);  // multiple of 8
+    const unsigned short* sg = v.seg + v.sbase[c] + (long long)t * SP;
+    fence_proxy_async_smem();  // earlier reads of the stage come first
+    mbar_expect_tx(&bar[st], xb + ne * 10u + (unsigned)SP * 2u);
+    if (xb) bulk_g2s(xs_of(st), x + c0, xb, &bar[st]);
+    if (ne) {
+      bulk_g2s(val_of(st), v.val + e0, ne * 8u, &bar[st]);
+      bulk_g2s(col_of(st), v.col + e0, ne * 2u, &bar[st]);
+    }
+    bulk_g2s(seg_of(st), sg, (unsigned)SP * 2u, &bar[st]);
   };
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -82,30 +100,31 @@ __global__ void __launch_bounds__(NT, 1)
   double acc = 0.0;
   int t = 0;
   for (; t < v.ntile; t++) {
+    const int st = t & 1;
     if (tid == 0) {
       if (t + 1 < v.ntile) issue(t + 1);
-      // bounded wait for tile t (phase t >> 1 of its buffer's barrier)
-      if (!mbar_wait_bounded(&bar[t & 1], (unsigned)((t >> 1) & 1), limit_ns)) {
+      // bounded wait for tile t (phase t >> 1 of its stage's barrier)
+      if (!mbar_wait_bounded(&bar[st], (unsigned)((t >> 1) & 1), limit_ns)) {
         atomicExch(status, 1);
         s_abort = 1;
       } else {
         const long long c0 = (long long)t * v.T;
         const long long cn = min((long long)v.T, (long long)v.cols - c0);
-        if (cn & 1) ((t & 1) ? xs1 : xs0)[cn - 1] = __ldg(x + c0 + cn - 1);
+        if (cn & 1) xs_of(st)[cn - 1] = __ldg(x + c0 + cn - 1);
       }
     }
     __syncthreads();
     if (s_abort) break;
     if (tid < R) {
-      const double* xt = (t & 1) ? xs1 : xs0;
-      const unsigned short* sg = seg + (size_t)t * (R + 1);
-      const long long base = v.cbase[(size_t)c * v.ntile + t];
+      const double* xt = xs_of(st);
+      const double* vt = val_of(st);
+      const unsigned short* ct = col_of(st);
+      const unsigned short* sg = seg_of(st);
       const int k0 = sg[tid], k1 = sg[tid + 1];
 #pragma unroll 4
-      for (int k = k0; k < k1; k++)
-        acc = add_rn(acc, mul_rn(__ldg(v.val + base + k), xt[__ldg(v.col + base + k)]));
+      for (int k = k0; k < k1; k++) acc = add_rn(acc, mul_rn(vt[k], xt[ct[k]]));
     }
-    __syncthreads();  // the buffer is read before tile t + 2 lands in it
+    __syncthreads();  // the stage is read before tile t + 2 lands in it
   }
   if (s_abort) {
     // let the copies issued for tiles t and t + 1 land before the CTA exits
@@ -127,8 +146,8 @@ __global__ void __launch_bounds__(NT, 1)
 #endif  // __CUDACC__
 
 // Host plan.  Returns SB2_OK with a->tiled.ncta == 0 when the operator does
-// not qualify (too few entries in long rows, x within one tile, or a chunk
-// beyond 65535 entries).
+// not qualify (too few entries in long rows, x within a quarter of a tile,
+// or no tile width whose two stages fit a CTA's shared memory).
 int build_tiled(CsrArrays* a) {
   TiledArrays& tl = a->tiled;
   tl.built = true;
@@ -152,8 +171,6 @@ int build_tiled(CsrArrays* a) {
   // rows longer than kSellCtaLen but at most min_len (possible only when the
   // threshold is raised) would fall in neither list
   if (min_len > kSellCtaLen) return SB2_OK;
-  const int T = kTiledCols;
-  const int ntile = (int)((n + (long long)T - 1) / T);
   const int nsm = num_sms(current_device());
   const int G = std::max(nsm, (int)((longr.size() + kTiledThreads - 1) / kTiledThreads));
   // longest-processing-time deal of rows to CTAs (no CTA above kTiledThreads rows)
@@ -185,43 +202,65 @@ int build_tiled(CsrArrays* a) {
   for (int r : longr)
     for (int k = ptr[r]; k < ptr[r + 1]; k++)
       if (ind[k] < 0 || ind[k] >= n) return SB2_OK;
+  // the x tile: the widest whose two stages (x tile, largest chunk and its
+  // row offsets) fit the shared memory of a CTA
+  int T = 0, ntile = 0, emax = 0, spmax = 0;
+  const size_t smem_cap = 220 * 1024;
+  for (int Tc : {kTiledCols, kTiledCols * 2 / 3, kTiledCols / 3, kTiledCols / 6}) {
+    const int nt = (int)((n + (long long)Tc - 1) / Tc);
+    int em = 0, sp = 0;
+    for (int c = 0; c < G; c++) {
+      std::vector<int> chunk(nt, 0);
+      for (int r : deal[c])
+        for (int k = ptr[r]; k < ptr[r + 1]; k++) chunk[ind[k] / Tc]++;
+      for (int t = 0; t < nt; t++) em = std::max(em, (chunk[t] + 7) / 8 * 8);
+      sp = std::max(sp, ((int)deal[c].size() + 1 + 7) / 8 * 8);
+    }
+    const size_t need = 2 * ((size_t)Tc * 8 + (size_t)em * 10 + (size_t)sp * 2);
+    if (em <= 65535 && need <= smem_cap) {
+      T = Tc;
+      ntile = nt;
+      emax = em;
+      spmax = sp;
+      break;
+    }
+  }
+  if (T == 0) return SB2_OK;  // some chunk too large for shared memory
   std::vector<int> rows, rptr(G + 1, 0);
-  std::vector<long long> cbase((size_t)G * ntile + 1, 0);
+  std::vector<long long> cbase((size_t)G * ntile + 1, 0), sbase(G, 0);
   std::vector<unsigned short> seg, col;
   std::vector<double> tval;
-  seg.reserve((size_t)ntile * (longr.size() + G));
-  col.reserve(lnnz);
-  tval.reserve(lnnz);
+  col.reserve(lnnz + 8ll * G * ntile);
+  tval.reserve(lnnz + 8ll * G * ntile);
   for (int c = 0; c < G; c++) {
     std::vector<int>& rs = deal[c];  // already by decreasing length
     rptr[c + 1] = rptr[c] + (int)rs.size();
     rows.insert(rows.end(), rs.begin(), rs.end());
     const int R = (int)rs.size();
+    const int SP = (R + 1 + 7) / 8 * 8;
+    sbase[c] = (long long)seg.size();
     // entries of (row j, tile t)
     std::vector<int> cnt((size_t)R * ntile, 0);
     for (int j = 0; j < R; j++)
       for (int k = ptr[rs[j]]; k < ptr[rs[j] + 1]; k++) cnt[(size_t)j * ntile + ind[k] / T]++;
-    // start of (row j, tile t) inside chunk t, and chunk sizes
+    // start of (row j, tile t) inside chunk t; chunks padded to 8 entries
+    // (16-byte bulk copies of the 2-byte columns), the padding never read
     std::vector<int> off((size_t)R * ntile);
     for (int t = 0; t < ntile; t++) {
-      long long s = 0;
+      int sz = 0;
       for (int j = 0; j < R; j++) {
-        off[(size_t)j * ntile + t] = (int)s;
-        s += cnt[(size_t)j * ntile + t];
+        off[(size_t)j * ntile + t] = sz;
+        sz += cnt[(size_t)j * ntile + t];
       }
-      if (s > 65535) {  // offsets are 2-byte
-        tl = TiledArrays();
-        tl.built = true;
-        return SB2_OK;
-      }
-      cbase[(size_t)c * ntile + t + 1] = cbase[(size_t)c * ntile + t] + s;
+      cbase[(size_t)c * ntile + t + 1] = cbase[(size_t)c * ntile + t] + (sz + 7) / 8 * 8;
       for (int j = 0; j < R; j++) seg.push_back((unsigned short)off[(size_t)j * ntile + t]);
-      seg.push_back((unsigned short)s);
+      seg.push_back((unsigned short)sz);
+      for (int q = R + 1; q < SP; q++) seg.push_back((unsigned short)sz);
     }
     // chunk (c+1, 0) starts where (c, ntile-1) ends: the same cbase slot
     const long long cend = cbase[(size_t)c * ntile + ntile];
-    col.resize(cend);
-    tval.resize(cend);
+    col.resize(cend, 0);
+    tval.resize(cend, 0.0);
     std::vector<int> fill(off);
     for (int j = 0; j < R; j++)
       for (int k = ptr[rs[j]]; k < ptr[rs[j] + 1]; k++) {
@@ -242,6 +281,7 @@ int build_tiled(CsrArrays* a) {
   cudaError_t e = up((void**)&out.d_rows, rows.data(), sizeof(int) * rows.size());
   if (e == cudaSuccess) e = up((void**)&out.d_rptr, rptr.data(), sizeof(int) * rptr.size());
   if (e == cudaSuccess) e = up((void**)&out.d_cbase, cbase.data(), sizeof(long long) * cbase.size());
+  if (e == cudaSuccess) e = up((void**)&out.d_sbase, sbase.data(), sizeof(long long) * sbase.size());
   if (e == cudaSuccess) e = up((void**)&out.d_seg, seg.data(), sizeof(unsigned short) * seg.size());
   if (e == cudaSuccess) e = up((void**)&out.d_col, col.data(), sizeof(unsigned short) * col.size());
   if (e == cudaSuccess) e = up((void**)&out.d_val, tval.data(), sizeof(double) * tval.size());
@@ -253,6 +293,8 @@ int build_tiled(CsrArrays* a) {
   out.ncta = G;
   out.ntile = ntile;
   out.T = T;
+  out.emax = emax;
+  out.spmax = spmax;
   out.nwshort = (int)shortw.size();
   out.entries = (long long)col.size();
   tl = out;
@@ -263,6 +305,7 @@ void free_tiled(TiledArrays* t) {
   cudaFree(t->d_rows);
   cudaFree(t->d_rptr);
   cudaFree(t->d_cbase);
+  cudaFree(t->d_sbase);
   cudaFree(t->d_seg);
   cudaFree(t->d_col);
   cudaFree(t->d_val);
@@ -292,20 +335,21 @@ int launch_tiled_product(const CsrArrays& a, double alpha, const double* x, doub
     SB2_TRY((launch_sell_warp_rows<256, true>(op, alpha, x, beta, y, s)));
   else
     SB2_TRY((launch_sell_warp_rows<256, false>(op, alpha, x, beta, y, s)));
-  const size_t smem = sizeof(double) * 2 * (size_t)tl.T;
+  const size_t smem = 2 * ((size_t)tl.T * 8 + (size_t)tl.emax * 10 + (size_t)tl.spmax * 2);
   static std::mutex mu;
   static std::vector<int> opted(64, 0);
   {
+    // the opt-in covers the largest stage any plan may take
     std::lock_guard<std::mutex> g(mu);
     const int dev = current_device();
     if (dev >= 0 && dev < 64 && !opted[dev]) {
       SB2_CUDA_TRY(cudaFuncSetAttribute(tiled_long_kernel<kTiledThreads>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
       opted[dev] = 1;
     }
   }
-  TiledView v{tl.ncta, tl.ntile, tl.T, a.cols, tl.d_rows, tl.d_rptr, tl.d_cbase, tl.d_seg,
-              tl.d_col, tl.d_val};
+  TiledView v{tl.ncta, tl.ntile, tl.T, a.cols, tl.emax, tl.spmax, tl.d_rows, tl.d_rptr,
+              tl.d_cbase, tl.d_sbase, tl.d_seg, tl.d_col, tl.d_val};
   tiled_long_kernel<kTiledThreads><<<tl.ncta, kTiledThreads, smem, s>>>(
       v, alpha, x, beta, y, overwrite, status, ring_wait_ns());
   SB2_CUDA_TRY(cudaGetLastError());

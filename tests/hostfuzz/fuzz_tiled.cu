@@ -3,9 +3,11 @@
 // operators with long rows, sorted or not, through sb2_csr_create and
 // build_tiled, and an independent check of every layout accepted: each long
 // row is dealt to exactly one CTA, no CTA holds more rows than it has
-// threads, every chunk's offsets rise to its size, and reading a row back
-// tile by tile gives its columns and values in stored order within each
-// tile.  Argument: the number of operators.  Test infrastructure only.
+// threads, chunks start on 8-entry boundaries and hold at most emax entries,
+// every chunk's offsets rise to its size, the two stages fit the shared
+// memory the kernel is given, and reading a row back tile by tile gives its
+// columns and values in stored order within each tile.  Argument: the
+// number of operators.  Test infrastructure only.
 #include "../../seldon_b200/csrc/csr.cu"
 #include "../../seldon_b200/csrc/tiled.cu"
 #include <cstdio>
@@ -65,10 +67,14 @@ int main(int argc, char** argv) {
     built++;
     // the device arrays are host memory under the stubs
     std::vector<int> seen(m, 0);
+    if (2 * ((size_t)t.T * 8 + (size_t)t.emax * 10 + (size_t)t.spmax * 2) > 220 * 1024)
+      return fail("stages beyond shared memory", trial);
     for (int c = 0; c < t.ncta; c++) {
       const int r0 = t.d_rptr[c], R = t.d_rptr[c + 1] - r0;
       if (R < 0 || R > 512) return fail("rows per CTA", trial);
-      const unsigned short* seg = t.d_seg + (size_t)t.ntile * (r0 + c);
+      const int SP = (R + 1 + 7) / 8 * 8;
+      if (SP > t.spmax || t.d_sbase[c] % 8) return fail("offset blocks", trial);
+      const unsigned short* seg = t.d_seg + t.d_sbase[c];
       for (int j = 0; j < R; j++) {
         const int row = t.d_rows[r0 + j];
         if (row < 0 || row >= m || seen[row]++) return fail("row dealt twice", trial);
@@ -76,9 +82,11 @@ int main(int argc, char** argv) {
         // read the row back tile by tile
         std::vector<std::pair<int, double>> got;
         for (int tt = 0; tt < t.ntile; tt++) {
-          const unsigned short* sg = seg + (size_t)tt * (R + 1);
+          const unsigned short* sg = seg + (size_t)tt * SP;
           const long long base = t.d_cbase[(size_t)c * t.ntile + tt];
-          if (sg[j] > sg[j + 1] || sg[R] != t.d_cbase[(size_t)c * t.ntile + tt + 1] - base)
+          const long long cap = t.d_cbase[(size_t)c * t.ntile + tt + 1] - base;
+          if (base % 8 || cap % 8 || cap > t.emax || sg[j] > sg[j + 1] || sg[R] > cap ||
+              cap - sg[R] >= 8)
             return fail("offsets", trial);
           for (int k = sg[j]; k < sg[j + 1]; k++)
             got.emplace_back(tt * t.T + t.d_col[base + k], t.d_val[base + k]);
