@@ -190,6 +190,15 @@ int sb2_mlt_host_batch(const sb2_csr* A, int trans, double alpha, int count,
  * (a layout choice of this engine). */
 int sb2_spmv_set_tiling(int min_row_len, long long min_entries);
 
+/* Device-side condition of the standalone products queued on `stream` so
+ * far (the TMA ring's and the tiled product's bounded waits and self-checks
+ * record it there; the products themselves return before their kernels
+ * run): *status receives 0 (none), 1 (a bounded wait ran out: the CTA left
+ * its share of rows unwritten), 3 or 4 (a copy or an index that a
+ * self-check refused: the row's rest skipped), and the word is cleared.
+ * Waits for the stream.  No counterpart in the reference. */
+int sb2_spmv_status(void* stream, int* status);
+
 /* Product algorithm and launch configuration, chosen by the autotuner; no
  * counterpart in the reference (tuning knobs of this engine).
  *   algo     SB2_SPMV_SELL   binned SELL-32 (thread/warp/CTA per row), default

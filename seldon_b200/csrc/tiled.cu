@@ -71,21 +71,29 @@ __global__ void __launch_bounds__(NT, 1)
   auto seg_of = [&](int st) { return col_of(st) + v.emax; };
   // thread 0 copies what tile t needs into stage t & 1: the x tile (a
   // trailing odd entry by a plain load after the wait), the chunk's values
-  // and columns and the row offsets, all with bulk copies
+  // and columns and the row offsets, all with bulk copies.  A copy that would
+  // not fit its stage is not issued: the status records it (3) and the CTA
+  // stops.
   auto issue = [&](int t) {
     const int st = t & 1;
     const long long c0 = (long long)t * v.T;
     const long long cn = min((long long)v.T, (long long)v.cols - c0);
     const unsigned xb = (unsigned)((cn * 8) & ~15ll);
     const long long e0 = v.cbase[(size_t)c * v.ntile + t];
-    const unsigned ne = (unsigned)(v.cbase[(size_t)c * v.ntile + t + 1] - e0);  // multiple of 8
+    const long long ne = v.cbase[(size_t)c * v.ntile + t + 1] - e0;  // a multiple of 8
     const unsigned short* sg = v.seg + v.sbase[c] + (long long)t * SP;
     fence_proxy_async_smem();  // earlier reads of the stage come first
-    mbar_expect_tx(&bar[st], xb + ne * 10u + (unsigned)SP * 2u);
+    if (ne < 0 || ne > v.emax || SP > v.spmax || (e0 & 7) || (ne & 7) || cn <= 0) {
+      atomicCAS(status, 0, 3);
+      s_abort = 1;
+      mbar_expect_tx(&bar[st], 0u);  // completes the phase: the wait below returns
+      return;
+    }
+    mbar_expect_tx(&bar[st], xb + (unsigned)ne * 10u + (unsigned)SP * 2u);
     if (xb) bulk_g2s(xs_of(st), x + c0, xb, &bar[st]);
     if (ne) {
-      bulk_g2s(val_of(st), v.val + e0, ne * 8u, &bar[st]);
-      bulk_g2s(col_of(st), v.col + e0, ne * 2u, &bar[st]);
+      bulk_g2s(val_of(st), v.val + e0, (unsigned)ne * 8u, &bar[st]);
+      bulk_g2s(col_of(st), v.col + e0, (unsigned)ne * 2u, &bar[st]);
     }
     bulk_g2s(seg_of(st), sg, (unsigned)SP * 2u, &bar[st]);
   };
@@ -116,13 +124,29 @@ __global__ void __launch_bounds__(NT, 1)
     __syncthreads();
     if (s_abort) break;
     if (tid < R) {
+      // every index read from the stage is checked against the stage's own
+      // extent (status 4 and the row's rest skipped): what the copies
+      // delivered can never send a read outside the CTA's shared memory
+      const long long c0 = (long long)t * v.T;
+      const int cn = (int)min((long long)v.T, (long long)v.cols - c0);
+      const int ne = (int)(v.cbase[(size_t)c * v.ntile + t + 1] - v.cbase[(size_t)c * v.ntile + t]);
       const double* xt = xs_of(st);
       const double* vt = val_of(st);
       const unsigned short* ct = col_of(st);
       const unsigned short* sg = seg_of(st);
       const int k0 = sg[tid], k1 = sg[tid + 1];
-#pragma unroll 4
-      for (int k = k0; k < k1; k++) acc = add_rn(acc, mul_rn(vt[k], xt[ct[k]]));
+      if (k0 > k1 || k1 > ne) {
+        atomicCAS(status, 0, 4);
+      } else {
+        for (int k = k0; k < k1; k++) {
+          const int col = ct[k];
+          if (col >= cn) {
+            atomicCAS(status, 0, 4);
+            break;
+          }
+          acc = add_rn(acc, mul_rn(vt[k], xt[col]));
+        }
+      }
     }
     __syncthreads();  // the stage is read before tile t + 2 lands in it
   }

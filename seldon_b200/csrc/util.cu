@@ -191,6 +191,18 @@ int sb2_set_wait_limit_ms(int ms) try {
   return (int)std::min<long long>((old_us + 999) / 1000, INT_MAX);
 } SB2_CATCH
 
+int sb2_spmv_status(void* stream, int* status) try {
+  if (!status) return SB2_ERR_INVALID_VALUE;
+  sb2::RedScratch* rs = nullptr;
+  const int st = sb2::get_red_scratch(static_cast<cudaStream_t>(stream), &rs);
+  if (st != SB2_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  SB2_CUDA_TRY(cudaMemcpyAsync(status, rs->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SB2_CUDA_TRY(cudaMemsetAsync(rs->status, 0, sizeof(int), s));
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  return SB2_OK;
+} SB2_CATCH
+
 int sb2_set_wait_limit_us(int us) try {
   const long long old_us = sb2::g_wait_limit_us;
   if (us > 0) sb2::g_wait_limit_us = us;
