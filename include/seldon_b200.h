@@ -177,26 +177,12 @@ int sb2_mlt_host(const sb2_csr* A, int trans, double alpha,
 int sb2_mlt_host_batch(const sb2_csr* A, int trans, double alpha, int count,
                        const double* x_host, double* y_host, void* stream);
 
-/* The x-tiled product of long rows (standalone products only; the solvers'
- * fused kernels keep the binned product).  On an operator's first product,
- * if its rows longer than min_row_len (33..1024; default 128) hold at least
- * min_entries entries (default 2^20) and x spans more than a quarter of a
- * tile, those rows get a second, tile-major copy of their entries (2-byte
- * columns relative to a tile of 12288 entries of x), and the product copies
- * x through shared memory tile by tile (bulk copies, double buffered)
- * instead of gathering it from L2.  A row is still summed in stored order,
- * so rows whose columns are sorted give the reference's bits.  The setting
- * applies to operators not yet multiplied.  No counterpart in the reference
- * (a layout choice of this engine). */
-int sb2_spmv_set_tiling(int min_row_len, long long min_entries);
-
 /* Device-side condition of the standalone products queued on `stream` so
- * far (the TMA ring's and the tiled product's bounded waits and self-checks
- * record it there; the products themselves return before their kernels
- * run): *status receives 0 (none), 1 (a bounded wait ran out: the CTA left
- * its share of rows unwritten), 3 or 4 (a copy or an index that a
- * self-check refused: the row's rest skipped), and the word is cleared.
- * Waits for the stream.  No counterpart in the reference. */
+ * far (the TMA ring engine's bounded waits record it there; the product
+ * calls themselves return before their kernels run): *status receives 0
+ * (none) or 1 (a bounded wait ran out: the CTA left its share of rows
+ * unwritten), and the word is cleared.  Waits for the stream.  No
+ * counterpart in the reference. */
 int sb2_spmv_status(void* stream, int* status);
 
 /* Product algorithm and launch configuration, chosen by the autotuner; no

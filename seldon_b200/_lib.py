@@ -141,7 +141,6 @@ _PROTOS = [
     ("sb2_set_wait_limit_ms", ctypes.c_int, [ctypes.c_int]),
     ("sb2_set_wait_limit_us", ctypes.c_int, [ctypes.c_int]),
     ("sb2_krylov_set_pcg", ctypes.c_int, [ctypes.c_int]),
-    ("sb2_spmv_set_tiling", ctypes.c_int, [ctypes.c_int, ctypes.c_longlong]),
     ("sb2_spmv_status", ctypes.c_int, [c_void_p, c_int_p]),
     ("sb2_probe_gather", ctypes.c_int,
      [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p]),

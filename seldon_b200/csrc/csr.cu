@@ -297,7 +297,6 @@ void free_csr(CsrArrays* a) {
   cudaFree(a->tma.d_kind);
   cudaFree(a->tma.d_desc);
   free_sell(&a->sell);
-  free_tiled(&a->tiled);
   *a = CsrArrays();
 }
 

@@ -422,7 +422,7 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(NTG, 3)
+__global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];

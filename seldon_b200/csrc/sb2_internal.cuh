@@ -105,24 +105,6 @@ struct SellArrays {
                               // bin, -1 for entries of the warp/CTA bins
 };
 
-// x-tiled layout of the long rows (tiled.cu), built on the first standalone
-// product of an operator that qualifies.
-struct TiledArrays {
-  bool built = false;          // planned (ncta == 0: the operator does not qualify)
-  int ncta = 0, ntile = 0, T = 0;
-  int* d_rows = nullptr;       // rows, CTA-major, each CTA's by decreasing length
-  int* d_rptr = nullptr;       // [ncta+1]
-  long long* d_cbase = nullptr;  // [ncta*ntile+1] first entry of each (CTA, tile) chunk
-  long long* d_sbase = nullptr;  // [ncta] first row offset of each CTA's blocks
-  int emax = 0, spmax = 0;     // largest chunk and row-offset block (entries)
-  unsigned short* d_seg = nullptr;  // per (CTA, tile): rows+1 offsets into the chunk
-  unsigned short* d_col = nullptr;  // column - tile * T
-  double* d_val = nullptr;
-  int nwshort = 0;             // rows of 33..(tiled threshold) entries: warp each
-  int* d_wshort = nullptr;
-  long long entries = 0;
-};
-
 struct CsrArrays {
   int rows = 0, cols = 0;
   long long nnz = 0;
@@ -132,7 +114,6 @@ struct CsrArrays {
   Partition part;           // plain kernel: row blocks incl. long rows
   Partition tma;            // pipelined kernel (nblk == -1: not applicable)
   SellArrays sell;          // binned quad-row SELL (default product)
-  TiledArrays tiled;        // x-tiled long rows (standalone products)
   int max_row = 0;          // longest row
 };
 
@@ -175,8 +156,6 @@ void free_csr(CsrArrays* a);
 int build_partition_host(const int* ptr, int rows, Partition* out);
 int build_tma_partition_host(const int* ptr, int rows, Partition* out);
 int build_sell_host(const int* ptr, const int* ind, const double* val, int rows, SellArrays* out);
-int build_tiled(CsrArrays* a);
-void free_tiled(TiledArrays* t);
 void free_sell(SellArrays* s);
 int ensure_transpose(const sb2_csr* A);
 int ensure_diag(const sb2_csr* A);

@@ -140,25 +140,6 @@ __global__ void __launch_bounds__(256) probe_gather_kernel(long long nnz, const 
   if (threadIdx.x == 0) partials[blockIdx.x] = t;
 }
 
-// The warp and CTA bins of op alone (the tiled product gives this the rows
-// it does not take).
-template <int NT, bool OVERWRITE>
-int launch_sell_warp_rows(const SellOp<double>& S, double alpha, const double* x, double beta,
-                          double* y, cudaStream_t s) {
-  if (S.nwarp_rows + S.ncta_rows == 0) return SB2_OK;
-  const unsigned g = (unsigned)std::max<long long>(((long long)S.nwarp_rows + 7) / 8, S.ncta_rows);
-  sell_long_kernel<NT, OVERWRITE><<<g, NT, 0, s>>>(S, alpha, x, beta, y);
-  SB2_CUDA_TRY(cudaGetLastError());
-  return SB2_OK;
-}
-template int launch_sell_warp_rows<256, true>(const SellOp<double>&, double, const double*, double,
-                                              double*, cudaStream_t);
-template int launch_sell_warp_rows<256, false>(const SellOp<double>&, double, const double*, double,
-                                               double*, cudaStream_t);
-
-int launch_tiled_product(const CsrArrays& a, double alpha, const double* x, double beta,
-                         double* y, bool overwrite, int* status, cudaStream_t s);
-
 SellOp<double> sell_op(const CsrArrays& a) {
   const SellArrays& s = a.sell;
   return SellOp<double>{s.nslice, s.d_sptr, s.d_qinfo, s.d_qrows, s.d_scol, s.d_sval, s.nwarp,
@@ -209,12 +190,6 @@ int launch_spmv(const CsrArrays& a, double alpha, const double* x, double beta,
       else
         sell_slices_kernel<256, false><<<g, 256, 0, s>>>(op, alpha, x, beta, y);
     }
-    if (a.tiled.ncta > 0) {
-      RedScratch* rs = nullptr;
-      SB2_TRY(get_red_scratch(s, &rs));
-      const int st = launch_tiled_product(a, alpha, x, beta, y, overwrite, rs->status, s);
-      if (st != SB2_ERR_NOT_SUPPORTED) return st;
-    }
     if (a.sell.nwarp + a.sell.ncta > 0) {
       const unsigned g = (unsigned)std::max<long long>(((long long)a.sell.nwarp + 7) / 8, a.sell.ncta);
       if (overwrite)
@@ -247,17 +222,6 @@ static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
   return pa < pb + nb && pb < pa + na;
 }
 
-// The x-tiled layout of an operator's long rows, planned on its first
-// standalone product (under the matrix's lock; read-only afterwards).
-static int ensure_tiled(const sb2_csr* cA, bool trans) {
-  if (g_spmv_algo != SB2_SPMV_SELL) return SB2_OK;
-  sb2_csr* A = const_cast<sb2_csr*>(cA);
-  std::lock_guard<std::mutex> g(A->mu);
-  CsrArrays& a = trans ? A->trans : A->full;
-  if (a.tiled.built || a.sell.nslice < 0) return SB2_OK;
-  return build_tiled(&a);
-}
-
 static int spmv_common(const sb2_csr* A, int trans, double alpha,
                        const double* x, double beta, double* y, bool overwrite,
                        cudaStream_t s) {
@@ -269,10 +233,8 @@ static int spmv_common(const sb2_csr* A, int trans, double alpha,
   // A symmetric operator is its own transpose (Functions_MatVect.cxx:915-927).
   if (trans && !A->sym) {
     SB2_TRY(ensure_transpose(A));
-    SB2_TRY(ensure_tiled(A, true));
     return launch_spmv(A->trans, alpha, x, beta, y, overwrite, s);
   }
-  SB2_TRY(ensure_tiled(A, false));
   return launch_spmv(A->full, alpha, x, beta, y, overwrite, s);
 }
 

@@ -35,8 +35,6 @@ __attribute__((weak)) int current_device() { return 0; }
 __attribute__((weak)) int map_cuda_error(cudaError_t) { return -3; }
 __attribute__((weak)) int num_sms(int) { return 148; }
 __attribute__((weak)) int ensure_diag(const sb2_csr*) { return 0; }
-struct TiledArrays;
-__attribute__((weak)) void free_tiled(TiledArrays*) {}
 }
 extern "C" {
 cudaError_t cudaGraphDestroy(cudaGraph_t) { return cudaSuccess; }

@@ -6,8 +6,8 @@ the measurement:
 
   - FP64 SpMV on the full 128^3 convection-diffusion operator (2.1M rows)
     and on the full Zipf(1.5) matrix (10^6 rows, 68.8M entries): rows of up
-    to 32 entries and rows of more than 128 (the x-tiled product) bit for
-    bit with Seldon's MltAdd, every row within the 1e-12 FP64 bound;
+    to 32 entries bit for bit with Seldon's MltAdd, every row within the
+    1e-12 FP64 bound;
   - Cg with the identity on the 100^2 Laplacian stored RowSymSparse (the
     configuration's matrix and tolerance), on the same b as the reference;
   - Gmres(30) with Jacobi on upwind convection-diffusion operators (the
@@ -77,10 +77,8 @@ def test_spmv_zipf_1e6_full(api, oracle):
     api.Mlt(A, to_dev(x), Y)
     y = to_host(Y)
     ref = oracle.mltadd(n, n, ptr, ind, val, 1.0, x, 0.0, np.zeros(n))
-    # the slice kernel (rows of up to 32 entries) and the x-tiled kernel (rows
-    # of more than 128) sum each row alone in stored order: Seldon's bits
-    exact = (lens <= 32) | (lens > 128)
-    assert np.array_equal(y[exact], ref[exact])
+    short = lens <= 32  # the thread bin sums each row alone, in stored order
+    assert np.array_equal(y[short], ref[short])
     assert_spmv_close(y, ref, abs_matvec(ptr, ind, val, x))
 
 

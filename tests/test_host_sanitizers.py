@@ -6,9 +6,7 @@ and malformed inputs:
 - the ILUT apply's planning (sb2_precond_create_ilut), with an independent
   check that every accepted factor's indices are in range;
 - the host ILUT factorization (sb2_ilut_factor, sb2_ilut_factor_sym);
-- sb2_batch_create's validation of the systems' CSR arrays;
-- the x-tiled product's layout planning (build_tiled), with an independent
-  reading-back of every layout it accepts.
+- sb2_batch_create's validation of the systems' CSR arrays.
 
 Host memory operations stand in for the CUDA runtime calls of that code
 (tests/hostfuzz/cuda_stubs.cpp), and no kernel runs."""
@@ -55,14 +53,6 @@ def _driver(tmp, name):
 
 def _clean(out):
     assert "runtime error" not in out and "AddressSanitizer" not in out
-
-
-def test_tiled_layout_host_code(tmp_path):
-    out = _run([_driver(str(tmp_path), "fuzz_tiled"), "60"], str(tmp_path))
-    _clean(out)
-    assert "tiled" in out and "layout error" not in out
-    built = int(out.split("tiled ")[1].split()[0])
-    assert built > 10, out
 
 
 def test_csr_create_host_code(tmp_path):
