@@ -40,7 +40,6 @@ namespace sb2 {
 constexpr int NTG = 256;        // threads per CTA
 constexpr int kCgs2MaxK = 32;   // basis vectors one projection covers (restart <= 32)
 constexpr int kWarpsG = NTG / 32;
-constexpr int kDotChunk = 16;   // dot products one pass accumulates (registers)
 
 SellOp<double> sell_op(const CsrArrays& a);
 size_t vector_stride(int n, size_t elem_bytes);
@@ -150,25 +149,28 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
   return s_ok != 0;
 }
 
-// Sums of `cnt` per-thread values over the CTA into out[0..cnt) (shared):
-// a fixed shuffle tree per warp, then the warps in order.  s_part holds
-// kWarpsG * KM doubles.
-template <int KM, typename T>
-__device__ __forceinline__ void block_sum_many(const T (&acc)[KM], int cnt, double* s_part,
-                                               double* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < KM; k++) {
-    if (k < cnt) {
-      const T v = warp_sum(acc[k]);
-      if (lane == 0) s_part[warp * KM + k] = (double)v;
-    }
+// Sums over the CTA of the per-thread accumulators acc[k * NTG + tid]
+// (shared memory, k < cnt) into out[0..cnt): thread (k, q) of the first
+// cnt * kWarpsG threads adds the 32 entries of warp q in thread order, then
+// thread k adds the warps' sums in warp order -- a fixed order, the same on
+// every run.  `tmp` holds kCgs2MaxK * kWarpsG doubles.
+template <typename VT>
+__device__ __forceinline__ void block_sum_columns(const VT* acc, int cnt, double* tmp,
+                                                  double* out) {
+  __syncthreads();
+  const int tid = threadIdx.x;
+  for (int w = tid; w < cnt * kWarpsG; w += NTG) {
+    const int k = w / kWarpsG, q = w % kWarpsG;
+    const VT* a = acc + (size_t)k * NTG + q * 32;
+    VT t = VT(0);
+    for (int l = 0; l < 32; l++) t = add_rn(t, a[l]);
+    tmp[w] = (double)t;
   }
   __syncthreads();
-  if ((int)threadIdx.x < cnt) {
+  if (tid < cnt) {
     double t = 0.0;
-    for (int q = 0; q < kWarpsG; q++) t = add_rn(t, s_part[q * KM + threadIdx.x]);
-    out[threadIdx.x] = t;
+    for (int q = 0; q < kWarpsG; q++) t = add_rn(t, tmp[tid * kWarpsG + q]);
+    out[tid] = t;
   }
   __syncthreads();
 }
@@ -240,40 +242,37 @@ struct EpiArnoldi {
   }
 };
 
-// acc[j] += (V_{k0+j}, w) over the owned rows, for k0 + j <= k1 (j < KC)
+// acc[k * NTG + tid] += (V_k, w) over the owned rows, k <= i; acc is this
+// thread's column of shared accumulators
 template <typename VT>
 struct PassDots {
   const VT* V;
   const VT* w;
   long long ldv;
-  int k0, k1;
-  VT acc[kDotChunk];
+  int i;
+  VT* acc;
   __device__ __forceinline__ void quad(int r) {
     VT wq[4];
     vld4_cg(w + r, wq);
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) {
+      VT v[4];
+      vld4_cg(V + k * ldv + r, v);
+      VT a = acc[k * NTG];
 #pragma unroll
-    for (int j = 0; j < kDotChunk; j++) {
-      if (k0 + j <= k1) {
-        VT v[4];
-        vld4_cg(V + (k0 + j) * ldv + r, v);
-        VT a = acc[j];
-#pragma unroll
-        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-        acc[j] = a;
-      }
+      for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
+      acc[k * NTG] = a;
     }
   }
   __device__ __forceinline__ void row(int r) {
     const VT wr = __ldcg(w + r);
-#pragma unroll
-    for (int j = 0; j < kDotChunk; j++)
-      if (k0 + j <= k1) acc[j] = add_rn(acc[j], mul_rn(__ldcg(V + (k0 + j) * ldv + r), wr));
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) acc[k * NTG] = add_rn(acc[k * NTG], mul_rn(__ldcg(V + k * ldv + r), wr));
   }
 };
 
-// w -= sum_k h_k V_k (k <= i) on the owned rows, then acc[k] += (V_k, w) for
-// the first chunk of k (k < kDotChunk, k <= i); the vectors just read are
-// read again for the dots, from cache
+// w -= sum_k h_k V_k (k <= i) on the owned rows, then acc[k] += (V_k, w);
+// the vectors just read are read again for the dots, from cache
 template <typename VT>
 struct PassProjectDots {
   const VT* V;
@@ -281,7 +280,7 @@ struct PassProjectDots {
   const double* h;  // shared memory
   long long ldv;
   int i;
-  VT acc[kDotChunk];
+  VT* acc;
   __device__ __forceinline__ void quad(int r) {
     VT wq[4];
     vld4_cg(w + r, wq);
@@ -294,16 +293,14 @@ struct PassProjectDots {
       for (int q = 0; q < 4; q++) wq[q] = add_rn(wq[q], -mul_rn(hk, v[q]));
     }
     vst4(w + r, wq);
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) {
+      VT v[4];
+      vld4_cg(V + k * ldv + r, v);
+      VT a = acc[k * NTG];
 #pragma unroll
-    for (int k = 0; k < kDotChunk; k++) {
-      if (k <= i) {
-        VT v[4];
-        vld4_cg(V + k * ldv + r, v);
-        VT a = acc[k];
-#pragma unroll
-        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-        acc[k] = a;
-      }
+      for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
+      acc[k * NTG] = a;
     }
   }
   __device__ __forceinline__ void row(int r) {
@@ -311,9 +308,8 @@ struct PassProjectDots {
 #pragma unroll 4
     for (int k = 0; k <= i; k++) wr = add_rn(wr, -mul_rn((VT)h[k], __ldcg(V + k * ldv + r)));
     w[r] = wr;
-#pragma unroll
-    for (int k = 0; k < kDotChunk; k++)
-      if (k <= i) acc[k] = add_rn(acc[k], mul_rn(__ldcg(V + k * ldv + r), wr));
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) acc[k * NTG] = add_rn(acc[k * NTG], mul_rn(__ldcg(V + k * ldv + r), wr));
   }
 };
 
@@ -422,11 +418,11 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(NTG, 3)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];
-  __shared__ double s_part[kWarpsG * kDotChunk];
+  __shared__ double s_part[kWarpsG * kCgs2MaxK];
   __shared__ double s_vals[kCgs2MaxK];
   __shared__ double s_h1[kCgs2MaxK];
   __shared__ double s_h2[kCgs2MaxK];
@@ -436,6 +432,9 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
   double* sv = Hm + ld * ld;  // s(0..m)
   double* cs = sv + ld;       // rotations_cos
   double* sn = cs + ld;       // rotations_sin
+  // per-thread dot accumulators: column tid of m rows (k <= i <= m - 1)
+  VT* s_acc = reinterpret_cast<VT*>(sn + ld);
+  VT* my_acc = s_acc + threadIdx.x;
   const int tid = threadIdx.x;
   const bool lead = (blockIdx.x == 0 && tid == 0);
   unsigned epoch = 0;
@@ -518,31 +517,20 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
         EpiArnoldi<VT> e{a.u, Vi, a.w, a.diag_in, inv_h};
         XLoadCg<VT> xl{a.u};
         sell_spmv<NTG, VT, VT>(a.Ain, xl, e, s_redv, blockIdx.x, gridDim.x);
-        for (int k0 = 0; k0 <= i; k0 += kDotChunk) {
-          PassDots<VT> f{a.V, a.w, a.ldv, k0, i, {}};
-#pragma unroll
-          for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
-          own_rows(a.Ain, f);
-          block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
-        }
+        for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
+        PassDots<VT> f{a.V, a.w, a.ldv, i, my_acc};
+        own_rows(a.Ain, f);
+        block_sum_columns(s_acc, i + 1, s_part, s_vals);
         if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
         if (tid <= i) s_h1[tid] = s_vals[tid];
         __syncthreads();
       }
       // 2. w -= V h1; h2_k = (V_k, w)
       {
-        PassProjectDots<VT> f{a.V, a.w, s_h1, a.ldv, i, {}};
-#pragma unroll
-        for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
+        for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
+        PassProjectDots<VT> f{a.V, a.w, s_h1, a.ldv, i, my_acc};
         own_rows(a.Ain, f);
-        block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1), s_part, s_vals);
-        for (int k0 = kDotChunk; k0 <= i; k0 += kDotChunk) {
-          PassDots<VT> g{a.V, a.w, a.ldv, k0, i, {}};
-#pragma unroll
-          for (int j = 0; j < kDotChunk; j++) g.acc[j] = VT(0);
-          own_rows(a.Ain, g);
-          block_sum_many<kDotChunk>(g.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
-        }
+        block_sum_columns(s_acc, i + 1, s_part, s_vals);
         if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
         if (tid <= i) s_h2[tid] = s_vals[tid];
         __syncthreads();
@@ -644,7 +632,11 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
                       double inner_tol, int max_iter, int max_cycles, int init_guess_null, int ir,
                       Cgs2Out* o, double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
   const int n = A->m;
-  const size_t smem = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1));
+  // Hessenberg matrix, rotations, s, and the threads' dot accumulators (m
+  // rows: a step projects on at most m basis vectors); with m = 30 three
+  // CTAs of the FP64 form fit an SM's shared memory
+  const size_t smem = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
+                      sizeof(VT) * (size_t)m * NTG;
   SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = cgs2_grid<VT>(smem, Ain, n);
