@@ -40,6 +40,7 @@ namespace sb2 {
 constexpr int NTG = 256;        // threads per CTA
 constexpr int kCgs2MaxK = 32;   // basis vectors one projection covers (restart <= 32)
 constexpr int kWarpsG = NTG / 32;
+constexpr int kDotChunk = 16;   // dot products one register pass accumulates (FP64 basis)
 
 SellOp<double> sell_op(const CsrArrays& a);
 size_t vector_stride(int n, size_t elem_bytes);
@@ -175,6 +176,29 @@ __device__ __forceinline__ void block_sum_columns(const VT* acc, int cnt, double
   __syncthreads();
 }
 
+// Sums of `cnt` per-thread values over the CTA into out[0..cnt) (shared):
+// a fixed shuffle tree per warp, then the warps in order.  s_part holds
+// kWarpsG * KM doubles.
+template <int KM, typename T>
+__device__ __forceinline__ void block_sum_many(const T (&acc)[KM], int cnt, double* s_part,
+                                               double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < KM; k++) {
+    if (k < cnt) {
+      const T v = warp_sum(acc[k]);
+      if (lane == 0) s_part[warp * KM + k] = (double)v;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < cnt) {
+    double t = 0.0;
+    for (int q = 0; q < kWarpsG; q++) t = add_rn(t, s_part[q * KM + threadIdx.x]);
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
 // The rows this thread writes in a product over S with (blockIdx.x,
 // gridDim.x): f.quad(r0) for a lane's 4 consecutive rows r0..r0+3 with
 // r0 % 4 == 0, f.row(r) for any other row.  Mirrors sell_spmv's assignment.
@@ -242,8 +266,8 @@ struct EpiArnoldi {
   }
 };
 
-// acc[k * NTG + tid] += (V_k, w) over the owned rows, k <= i; acc is this
-// thread's column of shared accumulators
+// Shared-memory forms (the FP32 basis): acc[k * NTG + tid] += (V_k, w) over
+// the owned rows, k <= i; acc is this thread's column of shared accumulators
 template <typename VT>
 struct PassDots {
   const VT* V;
@@ -310,6 +334,84 @@ struct PassProjectDots {
     w[r] = wr;
 #pragma unroll 4
     for (int k = 0; k <= i; k++) acc[k * NTG] = add_rn(acc[k * NTG], mul_rn(__ldcg(V + k * ldv + r), wr));
+  }
+};
+
+// Register forms (the FP64 basis): acc[j] += (V_{k0+j}, w) over the owned
+// rows, for k0 + j <= k1 (j < kDotChunk)
+template <typename VT>
+struct PassDotsReg {
+  const VT* V;
+  const VT* w;
+  long long ldv;
+  int k0, k1;
+  VT acc[kDotChunk];
+  __device__ __forceinline__ void quad(int r) {
+    VT wq[4];
+    vld4_cg(w + r, wq);
+#pragma unroll
+    for (int j = 0; j < kDotChunk; j++) {
+      if (k0 + j <= k1) {
+        VT v[4];
+        vld4_cg(V + (k0 + j) * ldv + r, v);
+        VT a = acc[j];
+#pragma unroll
+        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
+        acc[j] = a;
+      }
+    }
+  }
+  __device__ __forceinline__ void row(int r) {
+    const VT wr = __ldcg(w + r);
+#pragma unroll
+    for (int j = 0; j < kDotChunk; j++)
+      if (k0 + j <= k1) acc[j] = add_rn(acc[j], mul_rn(__ldcg(V + (k0 + j) * ldv + r), wr));
+  }
+};
+
+// w -= sum_k h_k V_k (k <= i) on the owned rows, then acc[k] += (V_k, w) for
+// the first chunk of k (k < kDotChunk, k <= i); the vectors just read are
+// read again for the dots, from cache
+template <typename VT>
+struct PassProjectDotsReg {
+  const VT* V;
+  VT* w;
+  const double* h;  // shared memory
+  long long ldv;
+  int i;
+  VT acc[kDotChunk];
+  __device__ __forceinline__ void quad(int r) {
+    VT wq[4];
+    vld4_cg(w + r, wq);
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) {
+      const VT hk = (VT)h[k];
+      VT v[4];
+      vld4_cg(V + k * ldv + r, v);
+#pragma unroll
+      for (int q = 0; q < 4; q++) wq[q] = add_rn(wq[q], -mul_rn(hk, v[q]));
+    }
+    vst4(w + r, wq);
+#pragma unroll
+    for (int k = 0; k < kDotChunk; k++) {
+      if (k <= i) {
+        VT v[4];
+        vld4_cg(V + k * ldv + r, v);
+        VT a = acc[k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
+        acc[k] = a;
+      }
+    }
+  }
+  __device__ __forceinline__ void row(int r) {
+    VT wr = __ldcg(w + r);
+#pragma unroll 4
+    for (int k = 0; k <= i; k++) wr = add_rn(wr, -mul_rn((VT)h[k], __ldcg(V + k * ldv + r)));
+    w[r] = wr;
+#pragma unroll
+    for (int k = 0; k < kDotChunk; k++)
+      if (k <= i) acc[k] = add_rn(acc[k], mul_rn(__ldcg(V + k * ldv + r), wr));
   }
 };
 
@@ -418,11 +520,11 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(NTG, 3)
+__global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];
-  __shared__ double s_part[kWarpsG * kCgs2MaxK];
+  __shared__ double s_part[kWarpsG * kCgs2MaxK];  // both reductions use it
   __shared__ double s_vals[kCgs2MaxK];
   __shared__ double s_h1[kCgs2MaxK];
   __shared__ double s_h2[kCgs2MaxK];
@@ -517,20 +619,45 @@ __global__ void __launch_bounds__(NTG, 3)
         EpiArnoldi<VT> e{a.u, Vi, a.w, a.diag_in, inv_h};
         XLoadCg<VT> xl{a.u};
         sell_spmv<NTG, VT, VT>(a.Ain, xl, e, s_redv, blockIdx.x, gridDim.x);
-        for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
-        PassDots<VT> f{a.V, a.w, a.ldv, i, my_acc};
-        own_rows(a.Ain, f);
-        block_sum_columns(s_acc, i + 1, s_part, s_vals);
+        if constexpr (sizeof(VT) == 4) {
+          for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
+          PassDots<VT> f{a.V, a.w, a.ldv, i, my_acc};
+          own_rows(a.Ain, f);
+          block_sum_columns(s_acc, i + 1, s_part, s_vals);
+        } else {
+          for (int k0 = 0; k0 <= i; k0 += kDotChunk) {
+            PassDotsReg<VT> f{a.V, a.w, a.ldv, k0, i, {}};
+#pragma unroll
+            for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
+            own_rows(a.Ain, f);
+            block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
+          }
+        }
         if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
         if (tid <= i) s_h1[tid] = s_vals[tid];
         __syncthreads();
       }
       // 2. w -= V h1; h2_k = (V_k, w)
       {
-        for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
-        PassProjectDots<VT> f{a.V, a.w, s_h1, a.ldv, i, my_acc};
-        own_rows(a.Ain, f);
-        block_sum_columns(s_acc, i + 1, s_part, s_vals);
+        if constexpr (sizeof(VT) == 4) {
+          for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
+          PassProjectDots<VT> f{a.V, a.w, s_h1, a.ldv, i, my_acc};
+          own_rows(a.Ain, f);
+          block_sum_columns(s_acc, i + 1, s_part, s_vals);
+        } else {
+          PassProjectDotsReg<VT> f{a.V, a.w, s_h1, a.ldv, i, {}};
+#pragma unroll
+          for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
+          own_rows(a.Ain, f);
+          block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1), s_part, s_vals);
+          for (int k0 = kDotChunk; k0 <= i; k0 += kDotChunk) {
+            PassDotsReg<VT> g{a.V, a.w, a.ldv, k0, i, {}};
+#pragma unroll
+            for (int j = 0; j < kDotChunk; j++) g.acc[j] = VT(0);
+            own_rows(a.Ain, g);
+            block_sum_many<kDotChunk>(g.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
+          }
+        }
         if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
         if (tid <= i) s_h2[tid] = s_vals[tid];
         __syncthreads();
@@ -632,11 +759,12 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
                       double inner_tol, int max_iter, int max_cycles, int init_guess_null, int ir,
                       Cgs2Out* o, double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
   const int n = A->m;
-  // Hessenberg matrix, rotations, s, and the threads' dot accumulators (m
-  // rows: a step projects on at most m basis vectors); with m = 30 three
-  // CTAs of the FP64 form fit an SM's shared memory
+  // Hessenberg matrix, rotations, s, and (FP32 basis) the threads' dot
+  // accumulators: m rows, a step projects on at most m basis vectors.  The
+  // FP64 form accumulates in registers: shared accumulators measured slower
+  // there (the L1 they take served the projection pass's second read)
   const size_t smem = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
-                      sizeof(VT) * (size_t)m * NTG;
+                      (sizeof(VT) == 4 ? sizeof(VT) * (size_t)m * NTG : 0);
   SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = cgs2_grid<VT>(smem, Ain, n);
