@@ -385,12 +385,15 @@ def run_ours(args, rank, world, local):
             "config": {"workload": WORKLOAD, "nnz": int(nnz), "n": int(n),
                        "bytes_per_step": int(B), "l2": "inputs 217 MB > 126 MB L2",
                        "parallelism": f"replicas x{world}"},
+            # 2 flops (one multiply, one add) per stored entry and product
+            "gflops": round(world * 2 * nnz / (ms_max * 1e-3) / 1e9, 2),
             "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(kernel_gbs / peak, 4),
                          "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "sb2::sell_slices_kernel<256, true>"},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n, "ms_per_step": round(e2e_ms, 4),
+                    "gflops": round(world * 2 * nnz / (e2e_ms * 1e-3) / 1e9, 2),
                     "api": f"sb2_mlt_host_batch, {G} pinned host vectors per call",
                     "matches_device_result": ok},
             "gpu_launches": args.steps * launches_per_spmv,
@@ -605,8 +608,10 @@ def extra_c3(api, matgen, torch, dev, timed, jobs):
 
 
 def gmres_bytes(n, nnz, iterations, m, vw, mw, variant):
-    """Least HBM traffic of a GMRES(m) solve that took `iterations` Arnoldi
-    steps, restarts every m steps: per step i of a cycle the product
+    """Bytes that the passes of a GMRES(m) solve read and write, for a solve
+    that took `iterations` Arnoldi steps and restarts every m steps (L2 can
+    serve part of them: w between the MGS passes, and part of the basis when
+    it is not much larger than L2): per step i of a cycle the product
     (nnz*(mw+4) + 4(n+1) + 2*n*vw) plus the orthogonalization's vector
     passes, and per restart the FP64 residual product and the update
     x += V y.  vw: basis element bytes; mw: matrix value bytes.
@@ -720,7 +725,8 @@ def extra_zipf(api, matgen, torch, dev, timed):
     ms, _ = timed(lambda: [api.Mlt(A, x, y) for _ in range(20)], reps=3)
     Bz = spmv_bytes(n, n, ind.size)
     us = ms / 20 * 1e3
-    out = {"gbs": round(Bz / (us * 1e-6) / 1e9, 1), "nnz": int(ind.size), "us": round(us, 1)}
+    out = {"gbs": round(Bz / (us * 1e-6) / 1e9, 1), "gflops": round(2 * ind.size / (us * 1e-6) / 1e9, 1),
+           "nnz": int(ind.size), "us": round(us, 1)}
     di = torch.as_tensor(ind, device=dev)
     dv = torch.as_tensor(val, device=dev)
     part = torch.empty(4096, dtype=torch.float64, device=dev)
