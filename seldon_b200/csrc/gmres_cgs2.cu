@@ -41,6 +41,8 @@ constexpr int NTG = 256;        // threads per CTA
 constexpr int kCgs2MaxK = 32;   // basis vectors one projection covers (restart <= 32)
 constexpr int kWarpsG = NTG / 32;
 constexpr int kDotChunk = 16;   // dot products one register pass accumulates (FP64 basis)
+constexpr int kDelChunk = 8;    // basis vectors one pass of the delayed form's dots covers
+constexpr int kWide = 2 * kCgs2MaxK + 2;  // values one wide barrier reduces
 
 SellOp<double> sell_op(const CsrArrays& a);
 size_t vector_stride(int n, size_t elem_bytes);
@@ -70,7 +72,7 @@ struct Cgs2Args {
   VT* V;                 // (m+1) basis vectors, `ldv` apart
   VT* w;
   VT* u;
-  double* wide;          // [kCgs2MaxK] results of the last wide barrier
+  double* wide;          // [kWide] results of the last wide barrier
   long long ldv;
   int n, m;
   double tol, inner_tol;
@@ -80,7 +82,7 @@ struct Cgs2Args {
 
 #ifdef __CUDACC__
 
-// Grid barrier that reduces K <= kCgs2MaxK values: each CTA deposits s_vals[0..K)
+// Grid barrier that reduces K <= kWide values: each CTA deposits s_vals[0..K)
 // (threads 0..K-1, one value each), the last CTA to arrive sums every value
 // over the CTAs in CTA order (warp k % 8 takes value k, lanes stride over the
 // CTAs, a fixed shuffle tree combines them), publishes the K sums and
@@ -141,10 +143,11 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
       __nanosleep(32);
     }
   }
-  if (tid == 0) {
-    for (int k = 0; k < K; k++) s_vals[k] = __ldcg(wide + k);
-    s_ok = (*((volatile int*)&P.sync->status) == 0) ? 1 : 0;
-  }
+  // thread 0's acquire, then the CTA barrier, orders every thread's reads
+  // of the published sums after the release
+  __syncthreads();
+  if (tid < K) s_vals[tid] = __ldcg(wide + tid);
+  if (tid == 0) s_ok = (*((volatile int*)&P.sync->status) == 0) ? 1 : 0;
   __syncthreads();
   epoch++;
   return s_ok != 0;
@@ -449,6 +452,136 @@ struct PassProjectNorm {
   }
 };
 
+// Delayed form, product epilogue: w = M^{-1} A u (u unnormalized).
+template <typename VT>
+struct EpiPrecond {
+  VT* w;
+  const VT* diag;
+  __device__ __forceinline__ void operator()(int r, VT t) { w[r] = precond_v(diag, r, t); }
+  __device__ __forceinline__ void quad(int r, const VT* t) {
+    VT wq[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) wq[j] = precond_v(diag, r + j, t[j]);
+    vst4(w + r, wq);
+  }
+};
+
+// Delayed form, dots of one step over the owned rows: acc[2j] += (V_k, u)
+// and acc[2j+1] += (V_k, w) for k = k0 + j < kend (j < kDelChunk); with
+// `norms`, nrm[0] += (u, u) and nrm[1] += (u, w).  Without W the w terms
+// are skipped (the cycle's last step has no product).
+template <typename VT, bool W>
+struct PassDotsUW {
+  const VT* V;
+  const VT* u;
+  const VT* w;
+  long long ldv;
+  int k0, kend;
+  bool norms;
+  VT acc[2 * kDelChunk];
+  VT nrm[2];
+  __device__ __forceinline__ void quad(int r) {
+    VT uq[4], wq[4];
+    vld4_cg(u + r, uq);
+    if constexpr (W) vld4_cg(w + r, wq);
+    if (norms) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        nrm[0] = add_rn(nrm[0], mul_rn(uq[q], uq[q]));
+        if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(uq[q], wq[q]));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kDelChunk; j++) {
+      if (k0 + j < kend) {
+        VT v[4];
+        vld4_cg(V + (k0 + j) * ldv + r, v);
+        VT a = acc[2 * j], c = acc[2 * j + 1];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          a = add_rn(a, mul_rn(v[q], uq[q]));
+          if constexpr (W) c = add_rn(c, mul_rn(v[q], wq[q]));
+        }
+        acc[2 * j] = a;
+        acc[2 * j + 1] = c;
+      }
+    }
+  }
+  __device__ __forceinline__ void row(int r) {
+    const VT ur = __ldcg(u + r);
+    const VT wr = W ? __ldcg(w + r) : VT(0);
+    if (norms) {
+      nrm[0] = add_rn(nrm[0], mul_rn(ur, ur));
+      if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(ur, wr));
+    }
+#pragma unroll
+    for (int j = 0; j < kDelChunk; j++) {
+      if (k0 + j < kend) {
+        const VT v = __ldcg(V + (k0 + j) * ldv + r);
+        acc[2 * j] = add_rn(acc[2 * j], mul_rn(v, ur));
+        if constexpr (W) acc[2 * j + 1] = add_rn(acc[2 * j + 1], mul_rn(v, wr));
+      }
+    }
+  }
+};
+
+// Delayed form, the step's one update pass on the owned rows:
+//   V_i = (u - sum_{k<i} s_k V_k) / rho        (u's delayed second projection)
+//   u   = w / rho - sum_{k<=i} d_k V_k         (w's first projection, scaled)
+// where V_i in the last term is the value just formed.
+template <typename VT>
+struct PassDelayed {
+  const VT* V;
+  VT* vi;
+  VT* u;
+  const VT* w;
+  const double* sc;  // s_k (shared)
+  const double* dc;  // d_k (shared)
+  long long ldv;
+  int i;
+  VT inv_rho;
+  __device__ __forceinline__ void quad(int r) {
+    VT a[4], b[4], wq[4];
+    vld4_cg(u + r, a);
+    vld4_cg(w + r, wq);
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = mul_rn(wq[q], inv_rho);
+#pragma unroll 4
+    for (int k = 0; k < i; k++) {
+      const VT sk = (VT)sc[k], dk = (VT)dc[k];
+      VT v[4];
+      vld4_cg(V + k * ldv + r, v);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        a[q] = add_rn(a[q], -mul_rn(sk, v[q]));
+        b[q] = add_rn(b[q], -mul_rn(dk, v[q]));
+      }
+    }
+    const VT di = (VT)dc[i];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      a[q] = mul_rn(a[q], inv_rho);
+      b[q] = add_rn(b[q], -mul_rn(di, a[q]));
+    }
+    vst4(vi + r, a);
+    vst4(u + r, b);
+  }
+  __device__ __forceinline__ void row(int r) {
+    VT a = __ldcg(u + r);
+    VT b = mul_rn(__ldcg(w + r), inv_rho);
+#pragma unroll 4
+    for (int k = 0; k < i; k++) {
+      const VT v = __ldcg(V + k * ldv + r);
+      a = add_rn(a, -mul_rn((VT)sc[k], v));
+      b = add_rn(b, -mul_rn((VT)dc[k], v));
+    }
+    a = mul_rn(a, inv_rho);
+    b = add_rn(b, -mul_rn((VT)dc[i], a));
+    vi[r] = a;
+    u[r] = b;
+  }
+};
+
 // x += sum_{k < cnt} y_k V_k in FP64 on the owned rows (Add skipped for y_k == 0)
 template <typename VT>
 struct PassUpdate {
@@ -511,6 +644,20 @@ struct PassNullGuess {
   }
 };
 
+// Delayed form, the step's reductions into s_vals (CTA sums): [2k] = (V_k, u),
+// [2k+1] = (V_k, w) for k < i, [2i] = (u, u), [2i+1] = (u, w).
+template <typename VT, bool W>
+__device__ __forceinline__ void delayed_dots(const Cgs2Args<VT>& a, int i, double* s_part,
+                                             double* s_vals) {
+  for (int k0 = 0; k0 < max(i, 1); k0 += kDelChunk) {
+    PassDotsUW<VT, W> f{a.V, a.u, a.w, a.ldv, k0, i, k0 == 0, {}, {}};
+    own_rows(a.Ain, f);
+    const int cnt = min(kDelChunk, i - k0);
+    if (cnt > 0) block_sum_many<2 * kDelChunk>(f.acc, 2 * cnt, s_part, s_vals + 2 * k0);
+    if (k0 == 0) block_sum_many<2>(f.nrm, 2, s_part, s_vals + 2 * i);
+  }
+}
+
 __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, double res) {
   if (*len < h.cap) {
     h.res[*len] = res;
@@ -519,29 +666,34 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
   (*len)++;
 }
 
-template <typename VT>
+static_assert(kWide <= NTG, "a wide barrier deposits one value per thread");
+
+template <typename VT, bool DEL>
 __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];
-  __shared__ double s_part[kWarpsG * kCgs2MaxK];  // both reductions use it
-  __shared__ double s_vals[kCgs2MaxK];
+  __shared__ double s_part[kWarpsG * kCgs2MaxK];  // every CTA reduction uses it
+  __shared__ double s_vals[kWide];
   __shared__ double s_h1[kCgs2MaxK];
-  __shared__ double s_h2[kCgs2MaxK];
+  __shared__ double s_h2[kCgs2MaxK + 1];
+  __shared__ double s_rho[2];
   extern __shared__ double s_dyn[];
   const int m = a.m, ld = m + 1;
-  double* Hm = s_dyn;         // (m+1) x (m+1), column-major
+  double* Hm = s_dyn;         // (m+1) x (m+1), column-major, rotated in place
   double* sv = Hm + ld * ld;  // s(0..m)
   double* cs = sv + ld;       // rotations_cos
   double* sn = cs + ld;       // rotations_sin
-  // per-thread dot accumulators: column tid of m rows (k <= i <= m - 1)
+  // three-pass form, FP32 basis: per-thread dot accumulators, column tid of
+  // m rows (k <= i <= m - 1); delayed form: the Hessenberg matrix unrotated
   VT* s_acc = reinterpret_cast<VT*>(sn + ld);
   VT* my_acc = s_acc + threadIdx.x;
+  double* Hr = sn + ld;
   const int tid = threadIdx.x;
   const bool lead = (blockIdx.x == 0 && tid == 0);
   unsigned epoch = 0;
   int hlen = 0;
-  for (int k = tid; k < ld * ld + 3 * ld; k += NTG) s_dyn[k] = 0.0;
+  for (int k = tid; k < (DEL ? 2 : 1) * ld * ld + 3 * ld; k += NTG) s_dyn[k] = 0.0;
 
   // ||b||^2: the refinement form stops on ||b - A x|| / ||b||
   double nb = 1.0;
@@ -608,9 +760,90 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
       sv[0] = beta;
     }
     const double beta_cycle = beta;
-    double h = beta;
     const int inner_max = nb_iter + m;
     int i = 0;
+    if constexpr (DEL) {
+      // Delayed reorthogonalization.  Entering step i, V_0..V_{i-1} are
+      // final and u is the next vector projected once, not normalized
+      // (u = r at i = 0).  Step i:
+      //   A. w = M^{-1} A u and the 2i+2 dots (V_k, u), (V_k, w), (u, u), (u, w)
+      //      in one pass                                          -> barrier
+      //      s_k = (V_k, u) is u's second projection, rho^2 = (u,u) - |s|^2;
+      //      column i-1 of H becomes h + s with H(i,i-1) = rho, and its
+      //      rotation gives the residual estimate of step i-1 (the stopping
+      //      test, one step late: a converged cycle wastes one product);
+      //   B. V_i = (u - V s) / rho and u = (w - V z - e V_i) / rho in one
+      //      pass, z_k = (V_k, w), e = (V_i, w)                       -> barrier
+      //      Column i's first coefficients are h_k = (z_k - t_k) / rho and
+      //      h_i = (e - t_i) / rho, with t = H(:, 0..i-1) s: A V_i equals
+      //      (w - A V s) / rho and A V_{0..i-1} = V H, so the projection
+      //      of w stands for that of A V_i.
+      // Step m has no product: it only finalizes column m-1.
+      for (;;) {
+        const bool prod = i < m;
+        if (prod) {
+          EpiPrecond<VT> e{a.w, a.diag_in};
+          XLoadCg<VT> xl{a.u};
+          sell_spmv<NTG, VT, VT>(a.Ain, xl, e, s_redv, blockIdx.x, gridDim.x);
+          delayed_dots<VT, true>(a, i, s_part, s_vals);
+        } else {
+          delayed_dots<VT, false>(a, i, s_part, s_vals);
+        }
+        if (!grid_sync_wide(P, a.wide, epoch, 2 * i + 2, s_vals)) return;
+        if (tid == 0) {
+          double ss = 0.0, sz = 0.0;
+          for (int k = 0; k < i; k++) {
+            ss = add_rn(ss, mul_rn(s_vals[2 * k], s_vals[2 * k]));
+            sz = add_rn(sz, mul_rn(s_vals[2 * k], s_vals[2 * k + 1]));
+          }
+          const double rho = i == 0 ? beta_cycle : sqrt(fmax(add_rn(s_vals[2 * i], -ss), 0.0));
+          s_rho[0] = rho;
+          s_rho[1] = (prod && rho != 0.0) ? add_rn(s_vals[2 * i + 1], -sz) / rho : 0.0;
+          if (i >= 1) {  // column i-1 final: H(k,c) = h_k + s_k, H(i,c) = rho
+            const int c = i - 1;
+            for (int k = 0; k <= c; k++) Hr[k + c * ld] = add_rn(Hr[k + c * ld], s_vals[2 * k]);
+            Hr[i + c * ld] = rho;
+            for (int k = 0; k <= i; k++) Hm[k + c * ld] = Hr[k + c * ld];
+            for (int k = 0; k < c; k++) apply_rot(Hm[k + c * ld], Hm[k + 1 + c * ld], cs[k], sn[k]);
+            if (rho != 0.0) {
+              double hc = rho;
+              gen_rot(Hm[c + c * ld], hc, cs[c], sn[c]);
+              apply_rot(sv[c], sv[c + 1], cs[c], sn[c]);
+            }
+          }
+        }
+        if (tid < i) s_h1[tid] = s_vals[2 * tid];
+        __syncthreads();
+        const double rho = s_rho[0];
+        if (i >= 1) {  // inner.Finished(|s(i)|) of step i-1
+          nb_iter++;
+          const double rin = fabs(sv[i]);
+          reste = facteur * rin;
+          if (lead && !a.ir) cgs2_hist(H, &hlen, nb_iter, reste);
+          bool stop = (reste < a.tol) || (nb_iter >= inner_max) || (rho == 0.0);
+          if (a.ir) stop = stop || (rin <= a.inner_tol * beta_cycle) || (nb_iter >= a.max_iter);
+          if (stop) break;
+        }
+        // column i's first coefficients (into Hr) and the update's d_k (s_h2)
+        if (tid <= i) {
+          double t = 0.0;
+          for (int k = max(tid - 1, 0); k < i; k++) t = add_rn(t, mul_rn(Hr[tid + k * ld], s_h1[k]));
+          const double zk = tid < i ? s_vals[2 * tid + 1] : s_rho[1];
+          Hr[tid + i * ld] = add_rn(zk, -t) / rho;
+          s_h2[tid] = zk / rho;
+        }
+        __syncthreads();
+        {
+          PassDelayed<VT> f{a.V, a.V + (long long)i * a.ldv, a.u, a.w, s_h1, s_h2, a.ldv, i,
+                            (VT)(1.0 / rho)};
+          own_rows(a.Ain, f);
+          __syncthreads();
+          if (!grid_sync_wide(P, a.wide, epoch, 0, s_vals)) return;
+        }
+        i++;
+      }
+    } else {
+    double h = beta;
     for (;;) {
       VT* Vi = a.V + (long long)i * a.ldv;
       const VT inv_h = (VT)(1.0 / h);
@@ -694,6 +927,7 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
       if (a.ir) stop = stop || (rin <= a.inner_tol * beta_cycle) || (nb_iter >= a.max_iter);
       if (stop) break;
     }
+    }
     // Solve(H, s): netlib DTRSV column sweep on the leading i x i block
     if (tid == 0) {
       for (int j = i - 1; j >= 0; j--)
@@ -733,10 +967,18 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
 
 // ----------------------------------------------------------------- host side
 
+#ifndef SB2_CGS2_DELAYED
+#define SB2_CGS2_DELAYED 1
+#endif
+// The Arnoldi form both precisions run: delayed reorthogonalization (two
+// basis reads and two grid barriers a step) or three passes (three and three).
+constexpr bool kDelayed = SB2_CGS2_DELAYED != 0;
+
 template <typename VT>
 static int cgs2_grid(size_t smem, const SellOp<VT>& S, int n) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_cgs2_kernel<VT>, NTG, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_cgs2_kernel<VT, kDelayed>, NTG,
+                                                    smem) !=
           cudaSuccess ||
       per_sm < 1)
     return 0;
@@ -763,9 +1005,10 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
   // accumulators: m rows, a step projects on at most m basis vectors.  The
   // FP64 form accumulates in registers: shared accumulators measured slower
   // there (the L1 they take served the projection pass's second read)
-  const size_t smem = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
-                      (sizeof(VT) == 4 ? sizeof(VT) * (size_t)m * NTG : 0);
-  SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT>,
+  const size_t smem =
+      sizeof(double) * ((kDelayed ? 2 : 1) * (size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
+      (!kDelayed && sizeof(VT) == 4 ? sizeof(VT) * (size_t)m * NTG : 0);
+  SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT, kDelayed>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = cgs2_grid<VT>(smem, Ain, n);
   if (grid < 1) return SB2_ERR_CUDA;
@@ -779,8 +1022,8 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
   };
   const size_t o_vec = take(sizeof(VT) * (size_t)ldv * (size_t)(m + 3));
   const size_t o_sync = take(sizeof(GridSync));
-  const size_t o_part = take(sizeof(double) * (size_t)kCgs2MaxK * grid);
-  const size_t o_wide = take(sizeof(double) * kCgs2MaxK);
+  const size_t o_part = take(sizeof(double) * (size_t)kWide * grid);
+  const size_t o_wide = take(sizeof(double) * kWide);
   const size_t o_out = take(sizeof(Cgs2Out));
   const size_t o_h = take(sizeof(double) * hcap), o_hi = take(sizeof(int) * hcap);
   struct Buf {
@@ -804,7 +1047,7 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
   History H{reinterpret_cast<double*>(base + o_h), reinterpret_cast<int*>(base + o_hi), hcap};
   Cgs2Out* d_out = reinterpret_cast<Cgs2Out*>(base + o_out);
   void* kargs[4] = {&args, &P, &H, &d_out};
-  SB2_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)gmres_cgs2_kernel<VT>, dim3(grid),
+  SB2_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)gmres_cgs2_kernel<VT, kDelayed>, dim3(grid),
                                            dim3(NTG), kargs, smem, s));
   GridSync gs;
   SB2_CUDA_TRY(cudaMemcpyAsync(o, d_out, sizeof(Cgs2Out), cudaMemcpyDeviceToHost, s));
