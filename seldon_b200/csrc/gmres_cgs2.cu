@@ -1,5 +1,6 @@
-// Restarted GMRES(m) with classical Gram-Schmidt applied twice (CGS2), as one
-// cooperative persistent kernel, in two precisions:
+// Restarted GMRES(m) with classical Gram-Schmidt applied twice (CGS2), the
+// second projection delayed by one step, as one cooperative persistent
+// kernel, in two precisions:
 //
 //   VT = double  the FP64 solver (sb2_gmres_cgs2): Seldon's Gmres (Gmres.cxx:
 //                44-183) with its modified Gram-Schmidt loop (:127-132)
@@ -13,15 +14,14 @@
 //                is a refinement step: the cycle's FP32 Krylov space corrects
 //                the FP64 x, and the next cycle starts from the FP64 residual.
 //
-// One Arnoldi step (V_0..V_i orthonormal, u = the unnormalized V_i, h = its
-// norm) takes three grid barriers, where the modified Gram-Schmidt order takes
-// i + 2:
-//   1. w = M^{-1} A u / h, V_i = u / h (the product's epilogue), then the
-//      i+1 dots (V_k, w) in one pass                      -> barrier
-//   2. w -= sum_k h1_k V_k, then the i+1 dots (V_k, w)     -> barrier
-//   3. u = w - sum_k h2_k V_k and ||u||^2                  -> barrier
-// H(k,i) = h1_k + h2_k and H(i+1,i) = ||u||.  The product of the next step
-// reads u and scales by 1/||u||, so normalizing V_{i+1} costs no pass.
+// One Arnoldi step reads the basis twice and takes two grid barriers, where
+// the modified Gram-Schmidt order reads it about once (the second touch of
+// each vector comes from L2) but takes i + 2 barriers, and CGS2 done in
+// order reads it three times behind three barriers.  A step projects the new
+// product once and finishes the previous vector's second projection, whose
+// coefficients come out of the same reduction (the low-synchronization
+// DCGS2 scheme of Bielich, Langou, Thomas, Swirydowicz, Yamazaki and Boman,
+// Parallel Computing 2022); the kernel's loop states the algebra.
 //
 // Every vector pass walks the rows each thread owns in the product (the rows
 // of its SELL quad, or the warp- or CTA-bin row its product epilogue wrote),
@@ -40,8 +40,6 @@ namespace sb2 {
 constexpr int NTG = 256;        // threads per CTA
 constexpr int kCgs2MaxK = 32;   // basis vectors one projection covers (restart <= 32)
 constexpr int kWarpsG = NTG / 32;
-constexpr int kDotChunk = 16;   // dot products one register pass accumulates (FP64 basis)
-constexpr int kDelChunk = 8;    // basis vectors one pass of the delayed form's dots covers
 constexpr int kWide = 2 * kCgs2MaxK + 2;  // values one wide barrier reduces
 
 SellOp<double> sell_op(const CsrArrays& a);
@@ -109,24 +107,23 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
     const int lane = tid & 31, warp = tid >> 5;
     for (int k = warp; k < K; k += kWarpsG) {
       const double* pv = P.partials + (size_t)k * G;
-      // every load of a lane issued before the first add waits on one
+      // every load of a lane issued before the first add waits on one: one
+      // round trip per value up to 512 CTAs
       double v = 0.0;
-      for (unsigned g0 = lane; g0 < G; g0 += 32 * 8) {
-        double part[8];
+      for (unsigned g0 = lane; g0 < G; g0 += 32 * 16) {
+        double part[16];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
+        for (int q = 0; q < 16; q++) {
           const unsigned g = g0 + 32u * q;
           part[q] = g < G ? __ldcg(pv + g) : 0.0;
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) v = add_rn(v, part[q]);
+        for (int q = 0; q < 16; q++) v = add_rn(v, part[q]);
       }
       v = warp_sum(v);
-      if (lane == 0) {
-        wide[k] = v;
-        __threadfence();
-      }
+      if (lane == 0) wide[k] = v;
     }
+    if (lane == 0) __threadfence();
     __syncthreads();
     if (tid == 0) {
       P.sync->count = 0u;
@@ -151,55 +148,6 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
   __syncthreads();
   epoch++;
   return s_ok != 0;
-}
-
-// Sums over the CTA of the per-thread accumulators acc[k * NTG + tid]
-// (shared memory, k < cnt) into out[0..cnt): thread (k, q) of the first
-// cnt * kWarpsG threads adds the 32 entries of warp q in thread order, then
-// thread k adds the warps' sums in warp order -- a fixed order, the same on
-// every run.  `tmp` holds kCgs2MaxK * kWarpsG doubles.
-template <typename VT>
-__device__ __forceinline__ void block_sum_columns(const VT* acc, int cnt, double* tmp,
-                                                  double* out) {
-  __syncthreads();
-  const int tid = threadIdx.x;
-  for (int w = tid; w < cnt * kWarpsG; w += NTG) {
-    const int k = w / kWarpsG, q = w % kWarpsG;
-    const VT* a = acc + (size_t)k * NTG + q * 32;
-    VT t = VT(0);
-    for (int l = 0; l < 32; l++) t = add_rn(t, a[l]);
-    tmp[w] = (double)t;
-  }
-  __syncthreads();
-  if (tid < cnt) {
-    double t = 0.0;
-    for (int q = 0; q < kWarpsG; q++) t = add_rn(t, tmp[tid * kWarpsG + q]);
-    out[tid] = t;
-  }
-  __syncthreads();
-}
-
-// Sums of `cnt` per-thread values over the CTA into out[0..cnt) (shared):
-// a fixed shuffle tree per warp, then the warps in order.  s_part holds
-// kWarpsG * KM doubles.
-template <int KM, typename T>
-__device__ __forceinline__ void block_sum_many(const T (&acc)[KM], int cnt, double* s_part,
-                                               double* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < KM; k++) {
-    if (k < cnt) {
-      const T v = warp_sum(acc[k]);
-      if (lane == 0) s_part[warp * KM + k] = (double)v;
-    }
-  }
-  __syncthreads();
-  if ((int)threadIdx.x < cnt) {
-    double t = 0.0;
-    for (int q = 0; q < kWarpsG; q++) t = add_rn(t, s_part[q * KM + threadIdx.x]);
-    out[threadIdx.x] = t;
-  }
-  __syncthreads();
 }
 
 // The rows this thread writes in a product over S with (blockIdx.x,
@@ -244,214 +192,6 @@ __device__ __forceinline__ VT precond_v(const VT* diag, int i, VT r) {
   else return __fdiv_rn(r, diag[i]);
 }
 
-// Product epilogue of step i: V_i = u / h, w = M^{-1} (A u) / h.
-template <typename VT>
-struct EpiArnoldi {
-  const VT* u;
-  VT* vi;
-  VT* w;
-  const VT* diag;
-  VT inv_h;
-  __device__ __forceinline__ void operator()(int r, VT t) {
-    vi[r] = mul_rn(__ldcg(u + r), inv_h);
-    w[r] = precond_v(diag, r, mul_rn(t, inv_h));
-  }
-  __device__ __forceinline__ void quad(int r, const VT* t) {
-    VT uq[4], vq[4], wq[4];
-    vld4_cg(u + r, uq);
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      vq[j] = mul_rn(uq[j], inv_h);
-      wq[j] = precond_v(diag, r + j, mul_rn(t[j], inv_h));
-    }
-    vst4(vi + r, vq);
-    vst4(w + r, wq);
-  }
-};
-
-// Shared-memory forms (the FP32 basis): acc[k * NTG + tid] += (V_k, w) over
-// the owned rows, k <= i; acc is this thread's column of shared accumulators
-template <typename VT>
-struct PassDots {
-  const VT* V;
-  const VT* w;
-  long long ldv;
-  int i;
-  VT* acc;
-  __device__ __forceinline__ void quad(int r) {
-    VT wq[4];
-    vld4_cg(w + r, wq);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) {
-      VT v[4];
-      vld4_cg(V + k * ldv + r, v);
-      VT a = acc[k * NTG];
-#pragma unroll
-      for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-      acc[k * NTG] = a;
-    }
-  }
-  __device__ __forceinline__ void row(int r) {
-    const VT wr = __ldcg(w + r);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) acc[k * NTG] = add_rn(acc[k * NTG], mul_rn(__ldcg(V + k * ldv + r), wr));
-  }
-};
-
-// w -= sum_k h_k V_k (k <= i) on the owned rows, then acc[k] += (V_k, w);
-// the vectors just read are read again for the dots, from cache
-template <typename VT>
-struct PassProjectDots {
-  const VT* V;
-  VT* w;
-  const double* h;  // shared memory
-  long long ldv;
-  int i;
-  VT* acc;
-  __device__ __forceinline__ void quad(int r) {
-    VT wq[4];
-    vld4_cg(w + r, wq);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) {
-      const VT hk = (VT)h[k];
-      VT v[4];
-      vld4_cg(V + k * ldv + r, v);
-#pragma unroll
-      for (int q = 0; q < 4; q++) wq[q] = add_rn(wq[q], -mul_rn(hk, v[q]));
-    }
-    vst4(w + r, wq);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) {
-      VT v[4];
-      vld4_cg(V + k * ldv + r, v);
-      VT a = acc[k * NTG];
-#pragma unroll
-      for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-      acc[k * NTG] = a;
-    }
-  }
-  __device__ __forceinline__ void row(int r) {
-    VT wr = __ldcg(w + r);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) wr = add_rn(wr, -mul_rn((VT)h[k], __ldcg(V + k * ldv + r)));
-    w[r] = wr;
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) acc[k * NTG] = add_rn(acc[k * NTG], mul_rn(__ldcg(V + k * ldv + r), wr));
-  }
-};
-
-// Register forms (the FP64 basis): acc[j] += (V_{k0+j}, w) over the owned
-// rows, for k0 + j <= k1 (j < kDotChunk)
-template <typename VT>
-struct PassDotsReg {
-  const VT* V;
-  const VT* w;
-  long long ldv;
-  int k0, k1;
-  VT acc[kDotChunk];
-  __device__ __forceinline__ void quad(int r) {
-    VT wq[4];
-    vld4_cg(w + r, wq);
-#pragma unroll
-    for (int j = 0; j < kDotChunk; j++) {
-      if (k0 + j <= k1) {
-        VT v[4];
-        vld4_cg(V + (k0 + j) * ldv + r, v);
-        VT a = acc[j];
-#pragma unroll
-        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-        acc[j] = a;
-      }
-    }
-  }
-  __device__ __forceinline__ void row(int r) {
-    const VT wr = __ldcg(w + r);
-#pragma unroll
-    for (int j = 0; j < kDotChunk; j++)
-      if (k0 + j <= k1) acc[j] = add_rn(acc[j], mul_rn(__ldcg(V + (k0 + j) * ldv + r), wr));
-  }
-};
-
-// w -= sum_k h_k V_k (k <= i) on the owned rows, then acc[k] += (V_k, w) for
-// the first chunk of k (k < kDotChunk, k <= i); the vectors just read are
-// read again for the dots, from cache
-template <typename VT>
-struct PassProjectDotsReg {
-  const VT* V;
-  VT* w;
-  const double* h;  // shared memory
-  long long ldv;
-  int i;
-  VT acc[kDotChunk];
-  __device__ __forceinline__ void quad(int r) {
-    VT wq[4];
-    vld4_cg(w + r, wq);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) {
-      const VT hk = (VT)h[k];
-      VT v[4];
-      vld4_cg(V + k * ldv + r, v);
-#pragma unroll
-      for (int q = 0; q < 4; q++) wq[q] = add_rn(wq[q], -mul_rn(hk, v[q]));
-    }
-    vst4(w + r, wq);
-#pragma unroll
-    for (int k = 0; k < kDotChunk; k++) {
-      if (k <= i) {
-        VT v[4];
-        vld4_cg(V + k * ldv + r, v);
-        VT a = acc[k];
-#pragma unroll
-        for (int q = 0; q < 4; q++) a = add_rn(a, mul_rn(v[q], wq[q]));
-        acc[k] = a;
-      }
-    }
-  }
-  __device__ __forceinline__ void row(int r) {
-    VT wr = __ldcg(w + r);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) wr = add_rn(wr, -mul_rn((VT)h[k], __ldcg(V + k * ldv + r)));
-    w[r] = wr;
-#pragma unroll
-    for (int k = 0; k < kDotChunk; k++)
-      if (k <= i) acc[k] = add_rn(acc[k], mul_rn(__ldcg(V + k * ldv + r), wr));
-  }
-};
-
-// u = w - sum_k h_k V_k (k <= i) on the owned rows; acc += ||u||^2
-template <typename VT>
-struct PassProjectNorm {
-  const VT* V;
-  const VT* w;
-  VT* u;
-  const double* h;
-  long long ldv;
-  int i;
-  VT acc;
-  __device__ __forceinline__ void quad(int r) {
-    VT wq[4];
-    vld4_cg(w + r, wq);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) {
-      const VT hk = (VT)h[k];
-      VT v[4];
-      vld4_cg(V + k * ldv + r, v);
-#pragma unroll
-      for (int j = 0; j < 4; j++) wq[j] = add_rn(wq[j], -mul_rn(hk, v[j]));
-    }
-    vst4(u + r, wq);
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc = add_rn(acc, mul_rn(wq[j], wq[j]));
-  }
-  __device__ __forceinline__ void row(int r) {
-    VT wr = __ldcg(w + r);
-#pragma unroll 4
-    for (int k = 0; k <= i; k++) wr = add_rn(wr, -mul_rn((VT)h[k], __ldcg(V + k * ldv + r)));
-    u[r] = wr;
-    acc = add_rn(acc, mul_rn(wr, wr));
-  }
-};
-
 // Delayed form, product epilogue: w = M^{-1} A u (u unnormalized).
 template <typename VT>
 struct EpiPrecond {
@@ -463,65 +203,6 @@ struct EpiPrecond {
 #pragma unroll
     for (int j = 0; j < 4; j++) wq[j] = precond_v(diag, r + j, t[j]);
     vst4(w + r, wq);
-  }
-};
-
-// Delayed form, dots of one step over the owned rows: acc[2j] += (V_k, u)
-// and acc[2j+1] += (V_k, w) for k = k0 + j < kend (j < kDelChunk); with
-// `norms`, nrm[0] += (u, u) and nrm[1] += (u, w).  Without W the w terms
-// are skipped (the cycle's last step has no product).
-template <typename VT, bool W>
-struct PassDotsUW {
-  const VT* V;
-  const VT* u;
-  const VT* w;
-  long long ldv;
-  int k0, kend;
-  bool norms;
-  VT acc[2 * kDelChunk];
-  VT nrm[2];
-  __device__ __forceinline__ void quad(int r) {
-    VT uq[4], wq[4];
-    vld4_cg(u + r, uq);
-    if constexpr (W) vld4_cg(w + r, wq);
-    if (norms) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        nrm[0] = add_rn(nrm[0], mul_rn(uq[q], uq[q]));
-        if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(uq[q], wq[q]));
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < kDelChunk; j++) {
-      if (k0 + j < kend) {
-        VT v[4];
-        vld4_cg(V + (k0 + j) * ldv + r, v);
-        VT a = acc[2 * j], c = acc[2 * j + 1];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          a = add_rn(a, mul_rn(v[q], uq[q]));
-          if constexpr (W) c = add_rn(c, mul_rn(v[q], wq[q]));
-        }
-        acc[2 * j] = a;
-        acc[2 * j + 1] = c;
-      }
-    }
-  }
-  __device__ __forceinline__ void row(int r) {
-    const VT ur = __ldcg(u + r);
-    const VT wr = W ? __ldcg(w + r) : VT(0);
-    if (norms) {
-      nrm[0] = add_rn(nrm[0], mul_rn(ur, ur));
-      if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(ur, wr));
-    }
-#pragma unroll
-    for (int j = 0; j < kDelChunk; j++) {
-      if (k0 + j < kend) {
-        const VT v = __ldcg(V + (k0 + j) * ldv + r);
-        acc[2 * j] = add_rn(acc[2 * j], mul_rn(v, ur));
-        if constexpr (W) acc[2 * j + 1] = add_rn(acc[2 * j + 1], mul_rn(v, wr));
-      }
-    }
   }
 };
 
@@ -644,18 +325,113 @@ struct PassNullGuess {
   }
 };
 
+// Basis vectors one pass of a step's dots covers: 8 with the FP32 basis, 4
+// with FP64 (its registers then allow three CTAs per SM, which measured
+// faster than two CTAs with 8)
+template <typename VT>
+constexpr int del_chunk() { return sizeof(VT) == 4 ? 8 : 4; }
+
+// Delayed form, dots of one step over the owned rows: acc[2j] += (V_k, u)
+// and acc[2j+1] += (V_k, w) for k = k0 + j < kend (j < del_chunk); with
+// `norms`, nrm[0] += (u, u) and nrm[1] += (u, w).  Without W the w terms
+// are skipped (the cycle's last step has no product).
+template <typename VT, bool W>
+struct PassDotsUW {
+  static constexpr int kChunk = del_chunk<VT>();
+  const VT* V;
+  const VT* u;
+  const VT* w;
+  long long ldv;
+  int k0, kend;
+  bool norms;
+  VT acc[2 * kChunk];
+  VT nrm[2];
+  __device__ __forceinline__ void quad(int r) {
+    VT uq[4], wq[4];
+    vld4_cg(u + r, uq);
+    if constexpr (W) vld4_cg(w + r, wq);
+    if (norms) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        nrm[0] = add_rn(nrm[0], mul_rn(uq[q], uq[q]));
+        if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(uq[q], wq[q]));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kChunk; j++) {
+      if (k0 + j < kend) {
+        VT v[4];
+        vld4_cg(V + (k0 + j) * ldv + r, v);
+        VT a = acc[2 * j], c = acc[2 * j + 1];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          a = add_rn(a, mul_rn(v[q], uq[q]));
+          if constexpr (W) c = add_rn(c, mul_rn(v[q], wq[q]));
+        }
+        acc[2 * j] = a;
+        acc[2 * j + 1] = c;
+      }
+    }
+  }
+  __device__ __forceinline__ void row(int r) {
+    const VT ur = __ldcg(u + r);
+    const VT wr = W ? __ldcg(w + r) : VT(0);
+    if (norms) {
+      nrm[0] = add_rn(nrm[0], mul_rn(ur, ur));
+      if constexpr (W) nrm[1] = add_rn(nrm[1], mul_rn(ur, wr));
+    }
+#pragma unroll
+    for (int j = 0; j < kChunk; j++) {
+      if (k0 + j < kend) {
+        const VT v = __ldcg(V + (k0 + j) * ldv + r);
+        acc[2 * j] = add_rn(acc[2 * j], mul_rn(v, ur));
+        if constexpr (W) acc[2 * j + 1] = add_rn(acc[2 * j + 1], mul_rn(v, wr));
+      }
+    }
+  }
+};
+
 // Delayed form, the step's reductions into s_vals (CTA sums): [2k] = (V_k, u),
-// [2k+1] = (V_k, w) for k < i, [2i] = (u, u), [2i+1] = (u, w).
+// [2k+1] = (V_k, w) for k < i, [2i] = (u, u), [2i+1] = (u, w).  The basis
+// goes in chunks of del_chunk vectors, one pass over the owned rows each;
+// after a chunk every warp folds its lanes' sums (shuffle tree) into its own
+// row of s_part and goes on, and the CTA adds the warps' rows in warp order
+// once, at the end.  (Tried and slower: each warp of the CTA taking a share
+// of the basis over all the CTA's rows, one pass, u and w re-read through
+// L1; and lane k summing V_k over rows staged by its warp, whose loads touch
+// 32 vectors at once.)
 template <typename VT, bool W>
 __device__ __forceinline__ void delayed_dots(const Cgs2Args<VT>& a, int i, double* s_part,
                                              double* s_vals) {
-  for (int k0 = 0; k0 < max(i, 1); k0 += kDelChunk) {
+  constexpr int kChunk = del_chunk<VT>();
+  const int lane = threadIdx.x & 31;
+  double* mp = s_part + (threadIdx.x >> 5) * kWide;
+  for (int k0 = 0; k0 < max(i, 1); k0 += kChunk) {
     PassDotsUW<VT, W> f{a.V, a.u, a.w, a.ldv, k0, i, k0 == 0, {}, {}};
     own_rows(a.Ain, f);
-    const int cnt = min(kDelChunk, i - k0);
-    if (cnt > 0) block_sum_many<2 * kDelChunk>(f.acc, 2 * cnt, s_part, s_vals + 2 * k0);
-    if (k0 == 0) block_sum_many<2>(f.nrm, 2, s_part, s_vals + 2 * i);
+    const int cnt = 2 * min(kChunk, i - k0);
+#pragma unroll
+    for (int j = 0; j < 2 * kChunk; j++) {
+      if (j < cnt) {
+        const VT v = warp_sum(f.acc[j]);
+        if (lane == 0) mp[2 * k0 + j] = (double)v;
+      }
+    }
+    if (k0 == 0) {
+      const VT v0 = warp_sum(f.nrm[0]), v1 = warp_sum(f.nrm[1]);
+      if (lane == 0) {
+        mp[2 * i] = (double)v0;
+        mp[2 * i + 1] = (double)v1;
+      }
+    }
   }
+  __syncthreads();
+  if ((int)threadIdx.x < 2 * i + 2) {
+    double t = 0.0;
+    for (int w = 0; w < kWarpsG; w++) t = add_rn(t, s_part[w * kWide + threadIdx.x]);
+    s_vals[threadIdx.x] = t;
+  }
+  __syncthreads();
 }
 
 __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, double res) {
@@ -668,12 +444,12 @@ __device__ __forceinline__ void cgs2_hist(const History& h, int* len, int it, do
 
 static_assert(kWide <= NTG, "a wide barrier deposits one value per thread");
 
-template <typename VT, bool DEL>
-__global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
+template <typename VT>
+__global__ void __launch_bounds__(NTG, 3)
     gmres_cgs2_kernel(Cgs2Args<VT> a, Persist P, History H, Cgs2Out* out) {
   __shared__ double s_red[kWarpsG];
   __shared__ VT s_redv[kWarpsG];
-  __shared__ double s_part[kWarpsG * kCgs2MaxK];  // every CTA reduction uses it
+  __shared__ double s_part[kWarpsG * kWide];  // every CTA reduction uses it
   __shared__ double s_vals[kWide];
   __shared__ double s_h1[kCgs2MaxK];
   __shared__ double s_h2[kCgs2MaxK + 1];
@@ -684,16 +460,12 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
   double* sv = Hm + ld * ld;  // s(0..m)
   double* cs = sv + ld;       // rotations_cos
   double* sn = cs + ld;       // rotations_sin
-  // three-pass form, FP32 basis: per-thread dot accumulators, column tid of
-  // m rows (k <= i <= m - 1); delayed form: the Hessenberg matrix unrotated
-  VT* s_acc = reinterpret_cast<VT*>(sn + ld);
-  VT* my_acc = s_acc + threadIdx.x;
-  double* Hr = sn + ld;
+  double* Hr = sn + ld;        // the Hessenberg matrix as built, unrotated
   const int tid = threadIdx.x;
   const bool lead = (blockIdx.x == 0 && tid == 0);
   unsigned epoch = 0;
   int hlen = 0;
-  for (int k = tid; k < (DEL ? 2 : 1) * ld * ld + 3 * ld; k += NTG) s_dyn[k] = 0.0;
+  for (int k = tid; k < 2 * ld * ld + 3 * ld; k += NTG) s_dyn[k] = 0.0;
 
   // ||b||^2: the refinement form stops on ||b - A x|| / ||b||
   double nb = 1.0;
@@ -762,7 +534,7 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
     const double beta_cycle = beta;
     const int inner_max = nb_iter + m;
     int i = 0;
-    if constexpr (DEL) {
+    {
       // Delayed reorthogonalization.  Entering step i, V_0..V_{i-1} are
       // final and u is the next vector projected once, not normalized
       // (u = r at i = 0).  Step i:
@@ -842,91 +614,6 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
         }
         i++;
       }
-    } else {
-    double h = beta;
-    for (;;) {
-      VT* Vi = a.V + (long long)i * a.ldv;
-      const VT inv_h = (VT)(1.0 / h);
-      // 1. w = M^{-1} A u / h; V_i = u / h; h1_k = (V_k, w)
-      {
-        EpiArnoldi<VT> e{a.u, Vi, a.w, a.diag_in, inv_h};
-        XLoadCg<VT> xl{a.u};
-        sell_spmv<NTG, VT, VT>(a.Ain, xl, e, s_redv, blockIdx.x, gridDim.x);
-        if constexpr (sizeof(VT) == 4) {
-          for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
-          PassDots<VT> f{a.V, a.w, a.ldv, i, my_acc};
-          own_rows(a.Ain, f);
-          block_sum_columns(s_acc, i + 1, s_part, s_vals);
-        } else {
-          for (int k0 = 0; k0 <= i; k0 += kDotChunk) {
-            PassDotsReg<VT> f{a.V, a.w, a.ldv, k0, i, {}};
-#pragma unroll
-            for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
-            own_rows(a.Ain, f);
-            block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
-          }
-        }
-        if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
-        if (tid <= i) s_h1[tid] = s_vals[tid];
-        __syncthreads();
-      }
-      // 2. w -= V h1; h2_k = (V_k, w)
-      {
-        if constexpr (sizeof(VT) == 4) {
-          for (int k = 0; k <= i; k++) my_acc[k * NTG] = VT(0);
-          PassProjectDots<VT> f{a.V, a.w, s_h1, a.ldv, i, my_acc};
-          own_rows(a.Ain, f);
-          block_sum_columns(s_acc, i + 1, s_part, s_vals);
-        } else {
-          PassProjectDotsReg<VT> f{a.V, a.w, s_h1, a.ldv, i, {}};
-#pragma unroll
-          for (int j = 0; j < kDotChunk; j++) f.acc[j] = VT(0);
-          own_rows(a.Ain, f);
-          block_sum_many<kDotChunk>(f.acc, min(kDotChunk, i + 1), s_part, s_vals);
-          for (int k0 = kDotChunk; k0 <= i; k0 += kDotChunk) {
-            PassDotsReg<VT> g{a.V, a.w, a.ldv, k0, i, {}};
-#pragma unroll
-            for (int j = 0; j < kDotChunk; j++) g.acc[j] = VT(0);
-            own_rows(a.Ain, g);
-            block_sum_many<kDotChunk>(g.acc, min(kDotChunk, i + 1 - k0), s_part, s_vals + k0);
-          }
-        }
-        if (!grid_sync_wide(P, a.wide, epoch, i + 1, s_vals)) return;
-        if (tid <= i) s_h2[tid] = s_vals[tid];
-        __syncthreads();
-      }
-      // 3. u = w - V h2; ||u||^2
-      {
-        PassProjectNorm<VT> f{a.V, a.w, a.u, s_h2, a.ldv, i, VT(0)};
-        own_rows(a.Ain, f);
-        const VT t = block_sum<NTG>(f.acc, s_redv);
-        if (tid == 0) s_vals[0] = (double)t;
-        __syncthreads();
-        if (!grid_sync_wide(P, a.wide, epoch, 1, s_vals)) return;
-      }
-      double hn = sqrt(s_vals[0]);
-      // H(:, i); rotations (every CTA computes the same scalars)
-      if (tid == 0) {
-        for (int k = 0; k <= i; k++) Hm[k + i * ld] = add_rn(s_h1[k], s_h2[k]);
-        for (int k = 0; k < i; k++) apply_rot(Hm[k + i * ld], Hm[k + 1 + i * ld], cs[k], sn[k]);
-        if (hn != 0.0) {
-          double hc = hn;
-          gen_rot(Hm[i + i * ld], hc, cs[i], sn[i]);
-          apply_rot(sv[i], sv[i + 1], cs[i], sn[i]);
-        }
-      }
-      h = (hn != 0.0) ? hn : 1.0;
-      i++;
-      nb_iter++;
-      __syncthreads();
-      // inner.Finished(|s(i)|), at most m steps a cycle
-      const double rin = fabs(sv[i]);
-      reste = facteur * rin;
-      if (lead && !a.ir) cgs2_hist(H, &hlen, nb_iter, reste);
-      bool stop = (reste < a.tol) || (nb_iter >= inner_max) || (hn == 0.0);
-      if (a.ir) stop = stop || (rin <= a.inner_tol * beta_cycle) || (nb_iter >= a.max_iter);
-      if (stop) break;
-    }
     }
     // Solve(H, s): netlib DTRSV column sweep on the leading i x i block
     if (tid == 0) {
@@ -967,17 +654,10 @@ __global__ void __launch_bounds__(NTG, sizeof(VT) == 4 ? 3 : 2)
 
 // ----------------------------------------------------------------- host side
 
-#ifndef SB2_CGS2_DELAYED
-#define SB2_CGS2_DELAYED 1
-#endif
-// The Arnoldi form both precisions run: delayed reorthogonalization (two
-// basis reads and two grid barriers a step) or three passes (three and three).
-constexpr bool kDelayed = SB2_CGS2_DELAYED != 0;
-
 template <typename VT>
 static int cgs2_grid(size_t smem, const SellOp<VT>& S, int n) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_cgs2_kernel<VT, kDelayed>, NTG,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_cgs2_kernel<VT>, NTG,
                                                     smem) !=
           cudaSuccess ||
       per_sm < 1)
@@ -1001,14 +681,9 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
                       double inner_tol, int max_iter, int max_cycles, int init_guess_null, int ir,
                       Cgs2Out* o, double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
   const int n = A->m;
-  // Hessenberg matrix, rotations, s, and (FP32 basis) the threads' dot
-  // accumulators: m rows, a step projects on at most m basis vectors.  The
-  // FP64 form accumulates in registers: shared accumulators measured slower
-  // there (the L1 they take served the projection pass's second read)
-  const size_t smem =
-      sizeof(double) * ((kDelayed ? 2 : 1) * (size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
-      (!kDelayed && sizeof(VT) == 4 ? sizeof(VT) * (size_t)m * NTG : 0);
-  SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT, kDelayed>,
+  // the Hessenberg matrix rotated and as built, s and the rotations
+  const size_t smem = sizeof(double) * (2 * (size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1));
+  SB2_CUDA_TRY(cudaFuncSetAttribute(gmres_cgs2_kernel<VT>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = cgs2_grid<VT>(smem, Ain, n);
   if (grid < 1) return SB2_ERR_CUDA;
@@ -1047,7 +722,7 @@ static int cgs2_solve(const sb2_csr* A, const SellOp<VT>& Ain, const double* dia
   History H{reinterpret_cast<double*>(base + o_h), reinterpret_cast<int*>(base + o_hi), hcap};
   Cgs2Out* d_out = reinterpret_cast<Cgs2Out*>(base + o_out);
   void* kargs[4] = {&args, &P, &H, &d_out};
-  SB2_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)gmres_cgs2_kernel<VT, kDelayed>, dim3(grid),
+  SB2_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)gmres_cgs2_kernel<VT>, dim3(grid),
                                            dim3(NTG), kargs, smem, s));
   GridSync gs;
   SB2_CUDA_TRY(cudaMemcpyAsync(o, d_out, sizeof(Cgs2Out), cudaMemcpyDeviceToHost, s));
