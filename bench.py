@@ -618,18 +618,21 @@ def gmres_bytes(n, nnz, iterations, m, vw, mw, variant):
       mgs   Seldon's modified Gram-Schmidt (Gmres.cxx:127-132): pass k reads
             w, V_k and V_{k+1} and writes w (4 vectors), i+1 passes, then
             V_{i+1} = w / h (2 vectors)
-      cgs2  three passes over V_0..V_i (dots; projection and dots; projection
-            and norm), the write of V_i, and w read and written, w read and u
-            written (5 vectors); the second read of V in the projection-and-
-            dots pass comes from cache"""
+      cgs2  CGS2 with the second projection delayed a step: step i's dots
+            read V_0..V_{i-1}, u and w, its update pass reads V_0..V_{i-1},
+            u and w and writes V_i and u (2i + 6 vectors); the step that
+            ends a cycle reads V and u once more (a full cycle: dots only;
+            a converged one: with the product, which then goes unused)"""
     spmv = nnz * (mw + 4) + 4 * (n + 1) + 2 * n * vw
     spmv64 = nnz * 12 + 4 * (n + 1) + 3 * n * 8  # residual: x in, b in, r out
     total, done = 0, 0
     while done < iterations:
         steps = min(m, iterations - done)
         for i in range(steps):
-            vec = 4 * (i + 1) + 2 if variant == "mgs" else 3 * (i + 1) + 5
+            vec = 4 * (i + 1) + 2 if variant == "mgs" else 2 * i + 6
             total += spmv + vec * n * vw
+        if variant == "cgs2":
+            total += (steps + 1) * n * vw if steps == m else spmv + (steps + 2) * n * vw
         total += spmv64 + steps * n * vw + 2 * n * 8
         done += steps
     return total
