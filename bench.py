@@ -927,6 +927,7 @@ def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every
                            "est_ms_all": round(per * nsys, 1)}
     out["speedup_mixed_vs_loop"] = round(out["loop_fp64_cg"]["est_ms_all"] / out["mixed"]["ms"], 1)
     Bt.close()
+    out["few_large_systems"] = run_batch_few_large(api, matgen, torch, dev, timed)
     if jobs is not None:
         sample = list(range(0, nsys, sample_every))
         jobs.append(("batch_lap2d_4096",
@@ -934,6 +935,39 @@ def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every
                                         np.concatenate([[0], np.cumsum([s[0].size - 1 for s in systems])])),
                      True))
     return out
+
+
+def run_batch_few_large(api, matgen, torch, dev, timed, nsys=12, lo=150, hi=180):
+    """Fewer large systems than the GPU's CTA slots (12 shifted 2D Laplacians,
+    side U{150..180}): the autotuned plan, which may give each system a whole
+    thread-block cluster, against one CTA per system."""
+    rng = np.random.default_rng(9)
+    systems, rhs = [], []
+    for _ in range(nsys):
+        g = int(rng.integers(lo, hi + 1))
+        p, i, v = matgen.lap2d(g, shift=0.01)
+        systems.append((p, i, v))
+        rhs.append(matgen.matvec(p, i, v, rng.uniform(-1, 1, g * g)))
+    Bt = api.Batch(systems)
+    b = torch.as_tensor(np.concatenate(rhs), device=dev)
+    X = torch.zeros(Bt.m, dtype=torch.float64, device=dev)
+    its = torch.zeros(Bt.nsys, dtype=torch.int32, device=dev)
+    rr = torch.zeros(Bt.nsys, dtype=torch.float64, device=dev)
+    Bt.autotune(X, b, tol=1e-9)
+    plan = Bt.plan() + Bt.cluster_plan()
+    Bt.solve(X, b, its, rr, tol=1e-9)
+    ms, res = timed(lambda: Bt.solve(X, b, its, rr, tol=1e-9), reps=3)
+    Bt.set_plan(512, 0)
+    Bt.solve(X, b, its, rr, tol=1e-9)
+    ms_cta, _ = timed(lambda: Bt.solve(X, b, its, rr, tol=1e-9), reps=3)
+    Bt.close()
+    return {"systems": nsys, "rows": int(sum(s[0].size - 1 for s in systems)),
+            "plan": {"threads": plan[0], "warp_max_rows": plan[1], "cluster_ctas": plan[2],
+                     "cluster_min_rows": plan[3]},
+            "ms": round(ms, 3), "converged": res.converged,
+            "max_rel_residual": res.max_rel_residual,
+            "ms_one_cta_per_system": round(ms_cta, 3),
+            "speedup_vs_one_cta_per_system": round(ms_cta / ms, 2)}
 
 
 def _cpu_batch(systems, rhs, sample, nsys, x_gpu, offs, tol=1e-9):

@@ -580,6 +580,20 @@ int sb2_batch_get_threads(const sb2_batch* B);
 int sb2_batch_set_plan(sb2_batch* B, int threads, int warp_max);
 int sb2_batch_get_plan(const sb2_batch* B, int* threads, int* warp_max);
 
+/* Cluster part of the plan, for batches with fewer large systems than the
+ * GPU has CTA slots: the launch groups its CTAs in thread-block clusters of
+ * `cluster` CTAs (2, 4, 8 or 16; 0: none), and the systems of more than
+ * cluster_min rows are each solved by a whole cluster (rows spread over its
+ * CTAs, reductions through distributed shared memory and the cluster's
+ * barrier).  The smaller systems then go to single CTAs and warps as the
+ * rest of the plan says.  sb2_batch_set_plan clears it; the autotuner also
+ * times clusters of 4 and 16 CTAs for the systems above half or an eighth of
+ * the largest, and caches the cluster part with the rest.  A cluster plan
+ * that the GPU cannot schedule makes sb2_batch_solve return
+ * SB2_ERR_NOT_SUPPORTED. */
+int sb2_batch_set_cluster_plan(sb2_batch* B, int cluster, int cluster_min);
+int sb2_batch_get_cluster_plan(const sb2_batch* B, int* cluster, int* cluster_min);
+
 /* Size from which Cg runs as a chain of full-occupancy kernels (one per
  * pass, scalars in device memory) instead of one persistent kernel.  The
  * default, 2800000 rows, is where the two cross on 7-point Poisson matrices

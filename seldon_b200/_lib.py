@@ -219,6 +219,8 @@ _PROTOS += [
     ("sb2_batch_get_threads", ctypes.c_int, [c_void_p]),
     ("sb2_batch_set_plan", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
     ("sb2_batch_get_plan", ctypes.c_int, [c_void_p, c_int_p, c_int_p]),
+    ("sb2_batch_set_cluster_plan", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("sb2_batch_get_cluster_plan", ctypes.c_int, [c_void_p, c_int_p, c_int_p]),
 ]
 _PROTOS += [
     ("sb2_csr_set_values", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p]),

@@ -1050,8 +1050,21 @@ class Batch:
         check(_L.sb2_batch_get_plan(self._h, ctypes.byref(t), ctypes.byref(w)), "sb2_batch_get_plan")
         return t.value, w.value
 
-    def set_plan(self, threads, warp_max=0):
+    def set_plan(self, threads, warp_max=0, cluster=0, cluster_min=0):
+        """Fixes the plan: CTA size, largest system one warp solves, and the
+        cluster part (CTAs per cluster, 0: none; systems of more than
+        cluster_min rows each take a whole cluster)."""
         check(_L.sb2_batch_set_plan(self._h, int(threads), int(warp_max)), "sb2_batch_set_plan")
+        if cluster:
+            check(_L.sb2_batch_set_cluster_plan(self._h, int(cluster), int(cluster_min)),
+                  "sb2_batch_set_cluster_plan")
+
+    def cluster_plan(self):
+        """(CTAs per cluster, 0: none; systems of more rows take a whole cluster)."""
+        c, m = ctypes.c_int(0), ctypes.c_int(0)
+        check(_L.sb2_batch_get_cluster_plan(self._h, ctypes.byref(c), ctypes.byref(m)),
+              "sb2_batch_get_cluster_plan")
+        return c.value, m.value
 
     @classmethod
     def from_coordinates(cls, IndRow, IndCol, Val, index=0, m=0, n=0, validate=True):

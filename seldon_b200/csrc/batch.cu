@@ -25,6 +25,8 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "sb2_internal.cuh"
 
 struct sb2_batch {
@@ -47,6 +49,8 @@ struct sb2_batch {
   // plan (autotuned): CTA size, and the largest system a single warp solves
   int threads = 256;
   int warp_max = 0;
+  int cluster = 0;       // CTAs of a cluster plan (0: none)
+  int cluster_min = 0;   // systems of more rows are solved by a whole cluster
   int max_rows = 0;
   unsigned long long histo_key = 0;  // size histogram, for the tuned-plan cache
 };
@@ -73,6 +77,7 @@ struct BatchArgs {
   int mode;
   int init_guess_null;
   int warp_max;     // systems of at most this many rows: one warp each
+  int cluster_min;  // cluster launches: systems of more rows take the whole cluster
   int* iters;       // per system (may be null)
   double* relres;   // per system (may be null)
 };
@@ -84,10 +89,15 @@ struct BatchArgs {
 // may start while slow threads still read this one.
 template <int NT>
 struct CtaGroup {
+  // values other threads of the group wrote (the product's gathers): the
+  // SM's L1 holds the CTA's own stores
+  template <typename T>
+  static __device__ __forceinline__ T ld(const T* p) { return *p; }
   double* red;  // shared: 2 buffers x 2 values x NT/32 warps
   int ph;
   static constexpr int kSize = NT;
   __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int stride() const { return NT; }
   __device__ __forceinline__ void sync() const { __syncthreads(); }
   template <int K, typename T>
   __device__ __forceinline__ void sums(T (&v)[K]) {
@@ -118,7 +128,10 @@ struct CtaGroup {
 
 struct WarpGroup {
   static constexpr int kSize = 32;
+  template <typename T>
+  static __device__ __forceinline__ T ld(const T* p) { return *p; }
   __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+  __device__ __forceinline__ int stride() const { return 32; }
   __device__ __forceinline__ void sync() const { __syncwarp(); }
   // __syncwarp orders the lanes' memory accesses around the reduction
   // (shuffles alone do not), as __syncthreads does for the CTA form
@@ -135,16 +148,77 @@ struct WarpGroup {
   }
 };
 
+// A whole thread-block cluster of NT-thread CTAs on one system (the largest
+// systems of a cluster plan).  Rows go to threads by cluster rank.  sums():
+// a shuffle tree per warp, the warps in order into the CTA's partial (in its
+// shared memory), a cluster barrier, then the partials of ranks 0..C-1 in
+// rank order, read through distributed shared memory.  Partials alternate
+// between two buffers, so one cluster barrier per reduction suffices: no
+// CTA can write a buffer again before every CTA has passed the next
+// reduction's barrier, after its reads of this one.  The product's gathers
+// read other CTAs' rows from L2: another SM's L1 may hold an older copy.
+template <int NT>
+struct ClusterGroup {
+  double* red;    // shared: 2 buffers x 2 values x NT/32 warps
+  double* cpart;  // shared: 2 buffers x 2 values (this CTA's partials)
+  double* gath;   // shared: 2 values x 16 ranks (partials gathered)
+  int ph;
+  int nrank;
+  int crank;
+  __device__ __forceinline__ int rank() const { return crank * NT + (int)threadIdx.x; }
+  __device__ __forceinline__ int stride() const { return nrank * NT; }
+  __device__ __forceinline__ void sync() const { cooperative_groups::this_cluster().sync(); }
+  template <typename T>
+  static __device__ __forceinline__ T ld(const T* p) { return __ldcg(p); }
+  template <int K, typename T>
+  __device__ __forceinline__ void sums(T (&v)[K]) {
+    constexpr int W = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* buf = red + ph * 2 * W;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const T t = warp_sum(v[k]);
+      if (lane == 0) buf[k * W + w] = (double)t;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+      T acc = T(0);
+      for (int q = 0; q < W; q++) acc = add_rn(acc, (T)buf[threadIdx.x * W + q]);
+      cpart[ph * 2 + threadIdx.x] = (double)acc;
+    }
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    cl.sync();
+    if ((int)threadIdx.x < K * nrank) {
+      const int k = threadIdx.x / nrank, r = threadIdx.x % nrank;
+      gath[k * 16 + r] = *cl.map_shared_rank(cpart + ph * 2 + k, r);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      T acc = T(0);
+      for (int r = 0; r < nrank; r++) acc = add_rn(acc, (T)gath[k * 16 + r]);
+      v[k] = acc;
+    }
+    ph ^= 1;
+  }
+  template <typename T>
+  __device__ __forceinline__ T sum(T v) {
+    T o[1] = {v};
+    sums<1>(o);
+    return o[0];
+  }
+};
+
 // r64 = b - A x over one system (FP64, entries in stored order); returns
 // ||r64||^2 in every thread of the group.  x must be complete (synced).
 template <class G, typename IT>
 __device__ double fp64_residual(G& g, const BatchArgs& a, int r0, int n, const double* xs) {
   const IT* __restrict__ ind = static_cast<const IT*>(a.ind);
   double acc = 0.0;
-  for (int i = g.rank(); i < n; i += G::kSize) {
+  for (int i = g.rank(); i < n; i += g.stride()) {
     const int k0 = __ldg(a.ptr + r0 + i), k1 = __ldg(a.ptr + r0 + i + 1);
     double t = 0.0;
-    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(__ldg(a.val + k), xs[__ldg(ind + k)]));
+    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(__ldg(a.val + k), G::ld(xs + __ldg(ind + k))));
     const double v = add_rn(__ldg(a.b + r0 + i), -t);
     a.r64[r0 + i] = v;
     acc = add_rn(acc, mul_rn(v, v));
@@ -156,7 +230,7 @@ __device__ double fp64_residual(G& g, const BatchArgs& a, int r0, int n, const d
 template <class G, typename T>
 __device__ __forceinline__ void direction(G& g, int n, const T* __restrict__ r, T* __restrict__ p,
                                           bool first, T beta, T zc) {
-  for (int i = g.rank(); i < n; i += G::kSize)
+  for (int i = g.rank(); i < n; i += g.stride())
     p[i] = first ? r[i] : add_rn(mul_rn(p[i], beta), mul_rn(zc, r[i]));
 }
 
@@ -168,10 +242,10 @@ __device__ __forceinline__ T product_dot(G& g, const BatchArgs& a, const VT* __r
                                          T* __restrict__ q) {
   const IT* __restrict__ ind = static_cast<const IT*>(a.ind);
   T pq = T(0);
-  for (int i = g.rank(); i < n; i += G::kSize) {
+  for (int i = g.rank(); i < n; i += g.stride()) {
     const int k0 = __ldg(a.ptr + r0 + i), k1 = __ldg(a.ptr + r0 + i + 1);
     T t = T(0);
-    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(T(__ldg(val + k)), p[__ldg(ind + k)]));
+    for (int k = k0; k < k1; k++) t = add_rn(t, mul_rn(T(__ldg(val + k)), G::ld(p + __ldg(ind + k))));
     q[i] = t;
     pq = add_rn(pq, mul_rn(p[i], t));
   }
@@ -188,7 +262,7 @@ __device__ void solve_fp64(G& g, const BatchArgs& a, int s, int r0, int n, doubl
   double rr;
   if (a.init_guess_null) {
     double acc = 0.0;
-    for (int i = g.rank(); i < n; i += G::kSize) {
+    for (int i = g.rank(); i < n; i += g.stride()) {
       x[i] = 0.0;
       const double bi = __ldg(a.b + r0 + i);
       r[i] = bi;
@@ -209,7 +283,7 @@ __device__ void solve_fp64(G& g, const BatchArgs& a, int s, int r0, int n, doubl
     if (delta == 0.0) break;
     const double alpha = rho / delta;
     double acc = 0.0;
-    for (int i = g.rank(); i < n; i += G::kSize) {
+    for (int i = g.rank(); i < n; i += g.stride()) {
       x[i] = add_rn(x[i], mul_rn(alpha, p[i]));
       const double ri = add_rn(r[i], mul_rn(-alpha, q[i]));
       r[i] = ri;
@@ -237,7 +311,7 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
   float* q = a.w32 + 3 * (size_t)a.m + r0;
   float* d = a.w32 + 4 * (size_t)a.m + r0;
   if (a.init_guess_null)
-    for (int i = g.rank(); i < n; i += G::kSize) x[i] = 0.0;
+    for (int i = g.rank(); i < n; i += g.stride()) x[i] = 0.0;
   g.sync();
   double rr64 = fp64_residual<G, IT>(g, a, r0, n, x);
   double res = sqrt(rr64) / nb;
@@ -251,7 +325,7 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
   }
   const float fnb = (float)nb;
   float acc = 0.0f;
-  for (int i = g.rank(); i < n; i += G::kSize) {
+  for (int i = g.rank(); i < n; i += g.stride()) {
     const float ri = (float)a.r64[r0 + i];
     r[i] = ri;
     d[i] = 0.0f;
@@ -269,7 +343,7 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
     if (delta == 0.0f) break;
     const float alpha = rho / delta;
     acc = 0.0f;
-    for (int i = g.rank(); i < n; i += G::kSize) {
+    for (int i = g.rank(); i < n; i += g.stride()) {
       d[i] = add_rn(d[i], mul_rn(alpha, p[i]));
       const float ri = add_rn(r[i], mul_rn(-alpha, q[i]));
       r[i] = ri;
@@ -287,7 +361,7 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
       continue;
     }
     // FP64 correction: x += d, d = 0, r64 = b - A x
-    for (int i = g.rank(); i < n; i += G::kSize) {
+    for (int i = g.rank(); i < n; i += g.stride()) {
       x[i] = add_rn(x[i], (double)d[i]);
       d[i] = 0.0f;
     }
@@ -298,7 +372,7 @@ __device__ void solve_mixed(G& g, const BatchArgs& a, int s, int r0, int n, doub
     // replace the FP32 residual; keep the direction, minus its component
     // along the new residual
     float v2[2] = {0.0f, 0.0f};
-    for (int i = g.rank(); i < n; i += G::kSize) {
+    for (int i = g.rank(); i < n; i += g.stride()) {
       const float ri = (float)a.r64[r0 + i];
       r[i] = ri;
       v2[0] = add_rn(v2[0], mul_rn(ri, ri));
@@ -322,7 +396,7 @@ template <class G, typename IT>
 __device__ void solve_system(G& g, const BatchArgs& a, int s) {
   const int r0 = __ldg(a.sys_row + s), n = __ldg(a.sys_row + s + 1) - r0;
   double acc = 0.0;
-  for (int i = g.rank(); i < n; i += G::kSize) {
+  for (int i = g.rank(); i < n; i += g.stride()) {
     const double bi = __ldg(a.b + r0 + i);
     acc = add_rn(acc, mul_rn(bi, bi));
   }
@@ -344,22 +418,52 @@ __device__ void solve_system(G& g, const BatchArgs& a, int s) {
 // and solve each with all their threads; the first system of at most
 // warp_max rows that a CTA takes switches it to warps: from then on (every
 // later system is as small or smaller) each warp takes and solves systems on
-// its own, with shuffle reductions and no CTA barrier.
-template <int NT, typename IT, bool WARPS>
+// its own, with shuffle reductions and no CTA barrier.  In a cluster launch
+// (CLUSTER) the clusters first take the systems of more than cluster_min
+// rows, one system per cluster; the first smaller system a cluster takes
+// goes to its rank-0 CTA, and from then on its CTAs take systems alone.
+template <int NT, typename IT, bool WARPS, bool CLUSTER>
 __global__ void __launch_bounds__(NT, 1536 / NT) batch_kernel(BatchArgs a) {
   __shared__ int s_sys;
   __shared__ double s_red[2 * 2 * (NT / 32)];
   CtaGroup<NT> cg{s_red, 0};
+  int carry = -1;  // a system taken in the cluster phase that this CTA solves alone
+  if constexpr (CLUSTER) {
+    __shared__ double s_cpart[4];
+    __shared__ double s_gath[2 * 16];
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    ClusterGroup<NT> clg{s_red, s_cpart, s_gath, 0, (int)cl.num_blocks(), (int)cl.block_rank()};
+    for (;;) {
+      if (clg.crank == 0 && threadIdx.x == 0) {
+        const unsigned k = atomicAdd(a.queue, 1u);
+        const int t = (k < (unsigned)a.nsys) ? __ldg(a.order + k) : -1;
+        for (int r = 0; r < clg.nrank; r++) *cl.map_shared_rank(&s_sys, r) = t;
+      }
+      cl.sync();
+      const int s = s_sys;
+      cl.sync();  // every CTA has read s_sys before rank 0 writes it again
+      if (s < 0) return;
+      if (__ldg(a.sys_row + s + 1) - __ldg(a.sys_row + s) <= a.cluster_min) {
+        if (clg.crank == 0) carry = s;
+        break;
+      }
+      solve_system<ClusterGroup<NT>, IT>(clg, a, s);
+    }
+  }
   int small = -1;
   for (;;) {
-    if (threadIdx.x == 0) {
-      const unsigned k = atomicAdd(a.queue, 1u);
-      s_sys = (k < (unsigned)a.nsys) ? __ldg(a.order + k) : -1;
+    int s = carry;
+    carry = -1;
+    if (s < 0) {
+      if (threadIdx.x == 0) {
+        const unsigned k = atomicAdd(a.queue, 1u);
+        s_sys = (k < (unsigned)a.nsys) ? __ldg(a.order + k) : -1;
+      }
+      __syncthreads();
+      s = s_sys;
+      __syncthreads();
+      if (s < 0) return;
     }
-    __syncthreads();
-    const int s = s_sys;
-    __syncthreads();
-    if (s < 0) return;
     if (WARPS && __ldg(a.sys_row + s + 1) - __ldg(a.sys_row + s) <= a.warp_max) {
       small = s;
       break;
@@ -388,43 +492,90 @@ __global__ void __launch_bounds__(NT, 1536 / NT) batch_kernel(BatchArgs a) {
   }
 }
 
+// Clusters of `cluster` CTAs that one GPU holds at once for this kernel
+// (0: the launch cannot be scheduled).
 template <int NT, typename IT, bool WARPS>
-static int launch_batch(const BatchArgs& a, cudaStream_t s) {
+static int cluster_grid(int cluster) {
+  auto* k = batch_kernel<NT, IT, WARPS, true>;
+  if (cluster > 8 &&
+      cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster);
+  cfg.blockDim = dim3(NT);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+template <int NT, typename IT, bool WARPS>
+static int launch_batch(const BatchArgs& a, int cluster, cudaStream_t s) {
+  if (cluster >= 2) {
+    const int nc = cluster_grid<NT, IT, WARPS>(cluster);
+    if (nc < 1) return SB2_ERR_NOT_SUPPORTED;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nc * cluster);
+    cfg.blockDim = dim3(NT);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SB2_CUDA_TRY(cudaLaunchKernelEx(&cfg, batch_kernel<NT, IT, WARPS, true>, a));
+    return SB2_OK;
+  }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT, IT, WARPS>, NT, 0) !=
-          cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<NT, IT, WARPS, false>,
+                                                    NT, 0) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const int grid = std::min(a.nsys, per_sm * num_sms(current_device()));
-  batch_kernel<NT, IT, WARPS><<<std::max(grid, 1), NT, 0, s>>>(a);
+  batch_kernel<NT, IT, WARPS, false><<<std::max(grid, 1), NT, 0, s>>>(a);
   SB2_CUDA_TRY(cudaGetLastError());
   return SB2_OK;
 }
 
 // the kernel without the warp path (warp_max == 0) keeps fewer registers
 template <typename IT, bool WARPS>
-static int launch_batch_w(const BatchArgs& a, int threads, cudaStream_t s) {
+static int launch_batch_w(const BatchArgs& a, int threads, int cluster, cudaStream_t s) {
   switch (threads) {
-    case 128: return launch_batch<128, IT, WARPS>(a, s);
-    case 512: return launch_batch<512, IT, WARPS>(a, s);
-    default: return launch_batch<256, IT, WARPS>(a, s);
+    case 128: return launch_batch<128, IT, WARPS>(a, cluster, s);
+    case 512: return launch_batch<512, IT, WARPS>(a, cluster, s);
+    default: return launch_batch<256, IT, WARPS>(a, cluster, s);
   }
 }
 
 template <typename IT>
-static int launch_batch_t(const BatchArgs& a, int threads, cudaStream_t s) {
-  return a.warp_max > 0 ? launch_batch_w<IT, true>(a, threads, s)
-                        : launch_batch_w<IT, false>(a, threads, s);
+static int launch_batch_t(const BatchArgs& a, int threads, int cluster, cudaStream_t s) {
+  return a.warp_max > 0 ? launch_batch_w<IT, true>(a, threads, cluster, s)
+                        : launch_batch_w<IT, false>(a, threads, cluster, s);
 }
 
 static int batch_run(const sb2_batch* B, double* x, const double* b, const sb2_batch_params* prm,
-                     int* iters, double* relres, int threads, int warp_max, cudaStream_t s) {
+                     int* iters, double* relres, int threads, int warp_max, int cluster,
+                     int cluster_min, cudaStream_t s) {
   BatchArgs a{B->nsys, B->d_sys_row, B->d_order, B->d_ptr, B->d_ind, B->d_val, B->d_val32,
               b, x, B->d_r64, B->d_w32, B->m, B->d_queue, prm->tol, prm->update_ratio,
-              prm->max_iter, prm->mode, prm->init_guess_null, warp_max, iters, relres};
+              prm->max_iter, prm->mode, prm->init_guess_null, warp_max, cluster_min, iters,
+              relres};
   SB2_CUDA_TRY(cudaMemsetAsync(B->d_queue, 0, sizeof(unsigned), s));
-  return B->ind16 ? launch_batch_t<unsigned short>(a, threads, s)
-                  : launch_batch_t<int>(a, threads, s);
+  return B->ind16 ? launch_batch_t<unsigned short>(a, threads, cluster, s)
+                  : launch_batch_t<int>(a, threads, cluster, s);
 }
 
 __global__ void batch_ind16(long long n, const int* __restrict__ a, unsigned short* __restrict__ b) {
@@ -461,7 +612,7 @@ static unsigned long long size_histogram_key(int nsys, const int* sys_row) {
 }
 
 struct BatchPlan {
-  int threads, warp_max;
+  int threads, warp_max, cluster, cluster_min;
 };
 // Plans chosen by sb2_batch_autotune, per (size histogram, mode): a later
 // batch with the same histogram takes its plan without timing.
@@ -579,7 +730,8 @@ int sb2_batch_solve(const sb2_batch* B, double* x, const double* b, const sb2_ba
     if (result) *result = sb2_batch_result{};
     return SB2_OK;
   }
-  SB2_TRY(batch_run(B, x, b, prm, d_iters, d_relres, B->threads, B->warp_max, s));
+  SB2_TRY(batch_run(B, x, b, prm, d_iters, d_relres, B->threads, B->warp_max, B->cluster,
+                    B->cluster_min, s));
   if (!result) return SB2_OK;
   // host summary (synchronizes): per-system counts and residuals
   std::vector<int> it(B->nsys);
@@ -614,6 +766,24 @@ int sb2_batch_set_plan(sb2_batch* B, int threads, int warp_max) try {
     return SB2_ERR_INVALID_VALUE;
   B->threads = threads;
   B->warp_max = warp_max;
+  B->cluster = 0;
+  B->cluster_min = 0;
+  return SB2_OK;
+} SB2_CATCH
+
+int sb2_batch_set_cluster_plan(sb2_batch* B, int cluster, int cluster_min) try {
+  if (!B || (cluster != 0 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) ||
+      cluster_min < 0)
+    return SB2_ERR_INVALID_VALUE;
+  B->cluster = cluster;
+  B->cluster_min = cluster ? cluster_min : 0;
+  return SB2_OK;
+} SB2_CATCH
+
+int sb2_batch_get_cluster_plan(const sb2_batch* B, int* cluster, int* cluster_min) try {
+  if (!B || !cluster || !cluster_min) return SB2_ERR_INVALID_VALUE;
+  *cluster = B->cluster;
+  *cluster_min = B->cluster_min;
   return SB2_OK;
 } SB2_CATCH
 
@@ -637,6 +807,8 @@ extern "C" int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
     if (it != sb2::g_plans.end()) {
       B->threads = it->second.threads;
       B->warp_max = it->second.warp_max;
+      B->cluster = it->second.cluster;
+      B->cluster_min = it->second.cluster_min;
       return SB2_OK;
     }
   }
@@ -644,34 +816,51 @@ extern "C" int sb2_batch_autotune(sb2_batch* B, double* x, const double* b,
   cudaEvent_t e0, e1;
   SB2_CUDA_TRY(cudaEventCreate(&e0));
   SB2_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  sb2::BatchPlan bp{B->threads, B->warp_max, B->cluster, B->cluster_min};
+  int st = SB2_OK;
+  // one untimed run, one timed run of the same solve; a cluster plan the
+  // GPU cannot schedule is skipped
+  auto trial = [&](const sb2::BatchPlan& p) {
+    int r = sb2::batch_run(B, x, b, prm, nullptr, nullptr, p.threads, p.warp_max, p.cluster,
+                           p.cluster_min, s);
+    if (r == SB2_ERR_NOT_SUPPORTED) return SB2_OK;
+    if (r != SB2_OK) return r;
+    cudaEventRecord(e0, s);
+    r = sb2::batch_run(B, x, b, prm, nullptr, nullptr, p.threads, p.warp_max, p.cluster,
+                       p.cluster_min, s);
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) r = SB2_ERR_CUDA;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r == SB2_OK && ms < best) {
+      best = ms;
+      bp = p;
+    }
+    return r;
+  };
   // CTA sizes x the largest system one warp solves (0: none)
   const int cand_t[3] = {128, 256, 512};
   const int cand_w[3] = {0, 256, 1024};
-  float best = 1e30f;
-  sb2::BatchPlan bp{B->threads, B->warp_max};
-  int st = SB2_OK;
   for (int ci = 0; ci < 9 && st == SB2_OK; ci++) {
     const int t = cand_t[ci / 3], w = cand_w[ci % 3];
     if (w > 0 && ci % 3 > 0 && cand_w[ci % 3 - 1] >= B->max_rows) continue;  // same plan as a smaller w
-    // one untimed run, one timed run of the same solve
-    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, t, w, s);
-    if (st != SB2_OK) break;
-    cudaEventRecord(e0, s);
-    st = sb2::batch_run(B, x, b, prm, nullptr, nullptr, t, w, s);
-    cudaEventRecord(e1, s);
-    if (cudaEventSynchronize(e1) != cudaSuccess) st = SB2_ERR_CUDA;
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (st == SB2_OK && ms < best) {
-      best = ms;
-      bp = sb2::BatchPlan{t, w};
-    }
+    st = trial(sb2::BatchPlan{t, w, 0, 0});
   }
+  // then clusters of 4 or 16 CTAs for the systems above half or an eighth of
+  // the largest, on the best plan's CTA size and warp systems
+  const sb2::BatchPlan base = bp;
+  const int cand_c[2] = {4, 16};
+  const int cand_m[2] = {B->max_rows / 2, B->max_rows / 8};
+  for (int ci = 0; ci < 4 && st == SB2_OK; ci++)
+    st = trial(sb2::BatchPlan{base.threads, base.warp_max, cand_c[ci / 2], cand_m[ci % 2]});
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st == SB2_OK) {
     B->threads = bp.threads;
     B->warp_max = bp.warp_max;
+    B->cluster = bp.cluster;
+    B->cluster_min = bp.cluster_min;
     std::lock_guard<std::mutex> g(sb2::g_plan_mu);
     sb2::g_plans[key] = bp;
   }

@@ -66,4 +66,9 @@ cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(int* n, const
   *n = 1;
   return cudaSuccess;
 }
+cudaError_t cudaOccupancyMaxActiveClusters(int* n, const void*, const cudaLaunchConfig_t*) {
+  *n = 1;
+  return cudaSuccess;
+}
+cudaError_t cudaLaunchKernelExC(const cudaLaunchConfig_t*, const void*, void**) { return cudaSuccess; }
 }

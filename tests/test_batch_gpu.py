@@ -57,6 +57,81 @@ def test_batch_matches_oracle(api, oracle, mixed, plan):
             assert abs(int(its[s]) - no) <= max(2, no // 20), (s, its[s], no)
 
 
+# cluster plans: (threads, warp_max, CTAs per cluster, systems above this
+# many rows take a whole cluster)
+CLUSTER_PLANS = [(512, 256, 4, 200), (256, 0, 2, 0), (128, 64, 8, 400), (512, 0, 8, 0)]
+
+
+@pytest.mark.parametrize("mixed", [True, False])
+@pytest.mark.parametrize("plan", CLUSTER_PLANS)
+def test_batch_cluster_plans_match_oracle(api, oracle, mixed, plan):
+    """The largest systems solved by whole thread-block clusters (rows
+    spread over the CTAs, sums through distributed shared memory), the rest
+    by CTAs and warps: every system against the oracle, repeat solves bit
+    for bit."""
+    import torch
+    systems, rhs, xs = _systems(5, 40, 4, 36)
+    B = api.Batch(systems)
+    B.set_plan(*plan)
+    assert B.plan() == plan[:2] and B.cluster_plan() == plan[2:]
+    b = to_dev(np.concatenate(rhs))
+    X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    res = B.solve(X, b, it, rr, tol=1e-9, mixed=mixed)
+    assert res.converged == B.nsys and res.max_rel_residual < 1e-9
+    x = to_host(X).copy()
+    its = to_host(it)
+    for s, ((ptr, ind, val), bb) in enumerate(zip(systems, rhs)):
+        xsys = x[B.sys_row[s]:B.sys_row[s + 1]]
+        rel = np.linalg.norm(bb - matgen.matvec(ptr, ind, val, xsys)) / np.linalg.norm(bb)
+        assert rel < 1e-9, (s, rel)
+        xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, bb, tol=1e-9, max_iter=2000)
+        assert np.linalg.norm(xsys - xo) / np.linalg.norm(xo) < 1e-6
+        if not mixed:
+            assert abs(int(its[s]) - no) <= max(2, no // 20), (s, its[s], no)
+    X.zero_()
+    B.solve(X, b, it, rr, tol=1e-9, mixed=mixed)
+    assert np.array_equal(to_host(X), x)
+    # a two-number plan clears the cluster part
+    B.set_plan(256, 0)
+    assert B.cluster_plan() == (0, 0)
+
+
+def test_batch_cluster_plan_few_large_systems(api, oracle):
+    """Fewer large systems than the GPU's CTA slots: a cluster per system
+    against one CTA per system, same answers; timings printed."""
+    import time
+    import torch
+    systems, rhs, xs = _systems(9, 12, 150, 180)
+    B = api.Batch(systems)
+    b = to_dev(np.concatenate(rhs))
+    X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    out = {}
+    for plan in [(512, 0), (512, 0, 8, 0), (512, 0, 16, 0)]:
+        B.set_plan(*plan)
+        try:
+            B.solve(X, b, it, rr, tol=1e-9)
+        except Exception as e:  # a cluster size the GPU cannot schedule
+            from seldon_b200._lib import SeldonB200Error
+            assert isinstance(e, SeldonB200Error) and plan[2] == 16
+            continue
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = B.solve(X, b, it, rr, tol=1e-9)
+        out[plan] = (time.perf_counter() - t0) * 1e3
+        assert res.converged == B.nsys
+        x = to_host(X)
+        for s in (0, 5, 11):
+            ptr, ind, val = systems[s]
+            xsys = x[B.sys_row[s]:B.sys_row[s + 1]]
+            xo, _, _, _, _ = oracle.solve("cg", ptr, ind, val, rhs[s], tol=1e-9, max_iter=5000)
+            assert np.linalg.norm(xsys - xo) / np.linalg.norm(xo) < 1e-6
+    print("few large systems, ms:", {k: round(v, 2) for k, v in out.items()})
+
+
 def test_batch_edges(api):
     import torch
     systems, rhs, xs = _systems(2, 6, 3, 12, zero=(2,))
