@@ -62,7 +62,8 @@ def parse():
     p.add_argument("--batch-systems", type=int, default=4096,
                    help="systems of the batch extra (profiling captures take fewer)")
     p.add_argument("--batch-plan", default=None,
-                   help="threads,warp_max: a fixed batch plan instead of the autotuner's")
+                   help="threads,warp_max[,cluster,cluster_min]: a fixed batch plan instead of "
+                        "the autotuner's")
     p.add_argument("--no-cpu-solves", action="store_true",
                    help="skip the reference's host solves beside the solver extras")
     return p.parse_args()
@@ -870,14 +871,16 @@ def run_batch(api, matgen, torch, dev, timed, jobs=None, nsys=4096, sample_every
     its = torch.zeros(Bt.nsys, dtype=torch.int32, device=dev)
     rr = torch.zeros(Bt.nsys, dtype=torch.float64, device=dev)
     t0 = time.perf_counter()
-    if plan:
+    if plan:  # threads,warp_max[,cluster,cluster_min]
         Bt.set_plan(*(int(v) for v in plan.split(",")))
     else:
         Bt.autotune(X, b, tol=1e-9)
     tune_s = time.perf_counter() - t0
     threads, warp_max = Bt.plan()
+    cluster, cluster_min = Bt.cluster_plan()
     out = {"systems": nsys, "rows": Bt.m, "nnz": int(sum(s[1].size for s in systems)),
            "tol": 1e-9, "plan": {"threads": threads, "warp_max_rows": warp_max,
+                                 "cluster_ctas": cluster, "cluster_min_rows": cluster_min,
                                  "autotune_s": round(tune_s, 2)}}
     rows = np.array([s[0].size - 1 for s in systems], dtype=np.float64)
     nnzs = np.array([s[1].size for s in systems], dtype=np.float64)
