@@ -28,17 +28,22 @@ __device__ __forceinline__ bool chain_done(const ChainState<T>* st) {
 
 // Finished() at the current nb_iter (Iterative.cxx:299-319), run by one thread.
 template <typename T>
-__device__ __forceinline__ bool chain_finished(ChainArgs<T>& a, T rr) {
-  ChainState<T>* st = a.st;
+__device__ __forceinline__ bool chain_finished_at(ChainState<T>* st, double* hist, int* hist_it,
+                                                  T rr) {
   const T res = (T)sqrt(rr);
   const double reste = (double)((T)st->facteur * res);
   st->reste = reste;
   if (st->hist_len < st->hist_cap) {
-    a.hist[st->hist_len] = reste;
-    a.hist_it[st->hist_len] = st->nb_iter;
+    hist[st->hist_len] = reste;
+    hist_it[st->hist_len] = st->nb_iter;
   }
   st->hist_len++;
   return (reste < st->tol) || (st->nb_iter >= st->max_iter);
+}
+
+template <typename T>
+__device__ __forceinline__ bool chain_finished(ChainArgs<T>& a, T rr) {
+  return chain_finished_at(a.st, a.hist, a.hist_it, rr);
 }
 
 // ||b||: Init(b) (Iterative.cxx:235-249).
@@ -536,6 +541,201 @@ __global__ void __launch_bounds__(CT, 4) k_pc_x(ChainArgs<T> a) {
   }
 }
 
+// ----------------------------------------------------------------- BiCgStab, any preconditioner
+//
+// BiCgStab (BiCgStab.cxx:43-145) with a preconditioner applied by its own
+// launches, every scalar in device memory.  One loop (two iterations of the
+// reference's counter):
+//   K_bp (p) -> [M apply: phat] -> K_bv (v = A phat, sigma = (rt, v), alpha)
+//   -> K_bs (s = r - alpha v, ++iter, Finished(||s||)) -> [M apply: shat]
+//   -> K_bt (t = A shat, (t, s), (t, t), omega)
+//   -> K_bxr (x += alpha phat + omega shat, r = s - omega t, ++iter,
+//             Finished(||r||), rho = (rt, r), the breakdowns, beta)
+// A stop on ||s|| sets `fin`: the products after it return, K_bxr only adds
+// alpha phat to x and ends the solve.
+
+template <typename T>
+struct BicgChain {
+  int n;
+  T* x;
+  T* r;
+  T* rt;
+  T* p;
+  T* phat;
+  T* v;
+  T* s;
+  T* shat;
+  T* t;
+  ChainState<T>* st;
+  T* part;
+  double* hist;
+  int* hist_it;
+};
+
+template <typename T>
+__device__ __forceinline__ bool bicg_stopped(const ChainState<T>* st) {
+  return (*((volatile const int*)&st->done) | *((volatile const int*)&st->fin)) != 0;
+}
+
+// rt = r: the shadow residual (Copy(r, rtilde)), after the start kernels
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_b_copy(BicgChain<T> a) {
+  if (*((volatile const int*)&a.st->done)) return;
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT)
+    a.rt[i] = a.r[i];
+}
+
+// p = r (first loop) | Add(-omega, v, p); Mlt(beta, p); Add(1, r, p)
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_b_p(BicgChain<T> a) {
+  pdl_wait();
+  pdl_release();
+  if (bicg_stopped(a.st)) return;
+  const bool first = (a.st->nb_iter == 0);
+  const T beta = a.st->beta, mo = -a.st->omega;
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    if (first) {
+      a.p[i] = a.r[i];
+      continue;
+    }
+    T pi = a.p[i];
+    if (mo != T(0)) pi = add_rn(pi, mul_rn(mo, a.v[i]));
+    pi = mul_rn(beta, pi);
+    a.p[i] = add_rn(pi, a.r[i]);
+  }
+}
+
+// v = A phat with sigma = (rt, v) (MODE 0); t = A shat with (t, s), (t, t)
+// (MODE 1).
+template <typename T, int MODE>
+struct EpiBicg {
+  T* out;
+  const T* w;
+  T acc0, acc1;
+  __device__ __forceinline__ void operator()(int i, T t) {
+    out[i] = t;
+    if (MODE == 0) {
+      acc0 = add_rn(acc0, mul_rn(__ldg(w + i), t));
+    } else {
+      acc0 = add_rn(acc0, mul_rn(t, __ldg(w + i)));
+      acc1 = add_rn(acc1, mul_rn(t, t));
+    }
+  }
+};
+
+template <typename T, typename VT, int MODE, int PART>
+__global__ void __launch_bounds__(CT, PART == 1 ? 1 : chain_spmv_occ<VT>())
+    k_b_spmv(BicgChain<T> a, SellOp<VT> S, int slot0, int tot) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  pdl_wait();
+  pdl_release();
+  if (bicg_stopped(a.st)) return;
+  EpiBicg<T, MODE> epi{MODE == 0 ? a.v : a.t, MODE == 0 ? a.rt : a.s, T(0), T(0)};
+  XLoadLdg<T> xl{MODE == 0 ? a.phat : a.shat};
+  if (PART == 0)
+    sell_spmv_slices<CT, VT, T, XLoadLdg<T>, EpiBicg<T, MODE>, chain_spmv_unroll<VT>()>(
+        S, xl, epi, blockIdx.x, gridDim.x);
+  else
+    sell_spmv_long<CT, VT, T>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+  T v[2] = {block_sum<CT>(epi.acc0, s_red), block_sum<CT>(epi.acc1, s_red)};
+  if (deposit_and_finish<CT, 2>(v, a.part, &a.st->cnt, slot0 + blockIdx.x, tot, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    if (MODE == 0) {
+      if (s_out[0] == T(0)) {  // breakdown #3
+        st->fail = 3;
+        st->done = 1;
+        return;
+      }
+      st->alpha = st->rho / s_out[0];
+    } else {
+      st->omega = s_out[0] / s_out[1];
+    }
+  }
+}
+
+// Copy(r, s); Add(-alpha, v, s); ++iter; Finished(||s||)
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_b_s(BicgChain<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (bicg_stopped(a.st)) return;
+  const T ma = -a.st->alpha;
+  T ss = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    T si = a.r[i];
+    if (ma != T(0)) si = add_rn(si, mul_rn(ma, a.v[i]));
+    a.s[i] = si;
+    ss = add_rn(ss, mul_rn(si, si));
+  }
+  T v[1] = {block_sum<CT>(ss, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<T>* st = a.st;
+    st->nb_iter++;
+    if (chain_finished_at(st, a.hist, a.hist_it, s_out[0])) st->fin = 1;
+  }
+}
+
+// Add(alpha, phat, x); Add(omega, shat, x); Copy(s, r); Add(-omega, t, r);
+// rho_2 = rho_1; ++iter; then the top of the next loop: Finished(||r||),
+// rho_1 = (rt, r), breakdowns #1 and #2, beta = (rho_1/rho_2)(alpha/omega).
+// After a stop on ||s||: Add(alpha, phat, x) only, and the solve ends.
+template <typename T>
+__global__ void __launch_bounds__(CT, 4) k_b_xr(BicgChain<T> a) {
+  __shared__ T s_red[CT / 32];
+  __shared__ T s_out[2];
+  pdl_wait();
+  pdl_release();
+  ChainState<T>* st = a.st;
+  if (*((volatile const int*)&st->done)) return;
+  const bool fin = *((volatile const int*)&st->fin) != 0;
+  const T alpha = st->alpha, omega = st->omega;
+  T rr = T(0), rtr = T(0);
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    T xi = a.x[i];
+    if (alpha != T(0)) xi = add_rn(xi, mul_rn(alpha, a.phat[i]));
+    if (!fin) {
+      if (omega != T(0)) xi = add_rn(xi, mul_rn(omega, a.shat[i]));
+      T ri = a.s[i];
+      if (-omega != T(0)) ri = add_rn(ri, mul_rn(-omega, a.t[i]));
+      a.r[i] = ri;
+      rr = add_rn(rr, mul_rn(ri, ri));
+      rtr = add_rn(rtr, mul_rn(a.rt[i], ri));
+    }
+    a.x[i] = xi;
+  }
+  T v[2] = {block_sum<CT>(rr, s_red), block_sum<CT>(rtr, s_red)};
+  if (deposit_and_finish<CT, 2>(v, a.part, &st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    if (fin) {
+      st->done = 1;
+      return;
+    }
+    st->rho_1 = st->rho;
+    st->nb_iter++;
+    if (chain_finished_at(st, a.hist, a.hist_it, s_out[0])) {
+      st->done = 1;
+      return;
+    }
+    st->rho = s_out[1];
+    if (st->rho == T(0)) {
+      st->fail = 1;
+      st->done = 1;
+      return;
+    }
+    if (st->omega == T(0)) {
+      st->fail = 2;
+      st->done = 1;
+      return;
+    }
+    st->beta = mul_rn(st->rho / st->rho_1, st->alpha / st->omega);
+  }
+}
+
 // ----------------------------------------------------------------- host driver
 
 // Elementwise passes: at most one resident wave (4 CTAs per SM), threads
@@ -698,6 +898,79 @@ int chain_pcg(const SellOp<double>& S, int n, const PrecondLaunch& apply, double
     SB2_TRY(pipe.wait(&h, &at));
     if (h.done || at > max_iter + 1) break;
     chunk = plan.next(h.nb_iter, h.reste, tol, 0, std::min(chunk * 2, 16), 1, 16);
+  }
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));
+  return SB2_OK;
+}
+
+// The two kernels of a BiCgStab product (slices, long rows), one deposit array.
+template <typename VT>
+static int launch_b_spmv(int mode, const BicgChain<double>& a, const SellOp<VT>& S,
+                         cudaStream_t s) {
+  const int g1 = reducing_slice_grid(S);
+  const int g2 = (S.nwarp_rows + S.ncta_rows) > 0 ? std::max((S.nwarp_rows + 7) / 8, S.ncta_rows) : 0;
+  const int tot = g1 + g2;
+  if (tot == 0) return SB2_ERR_NOT_SUPPORTED;
+  if (mode == 0) {
+    if (g1) SB2_CUDA_TRY(launch_pdl(k_b_spmv<double, VT, 0, 0>, g1, s, a, S, 0, tot));
+    if (g2) SB2_CUDA_TRY(launch_pdl(k_b_spmv<double, VT, 0, 1>, g2, s, a, S, g1, tot));
+  } else {
+    if (g1) SB2_CUDA_TRY(launch_pdl(k_b_spmv<double, VT, 1, 0>, g1, s, a, S, 0, tot));
+    if (g2) SB2_CUDA_TRY(launch_pdl(k_b_spmv<double, VT, 1, 1>, g2, s, a, S, g1, tot));
+  }
+  return SB2_OK;
+}
+
+// BiCgStab with a preconditioner's own launches (SOR, ILUT), as a
+// device-resident chain.  work: 8n doubles (r, rt, p, phat, v, s, shat, t).
+// As in chain_pcg, no chunk is queued ahead of the one the host waits for.
+int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, double* x,
+                    const double* b, double* work, ChainState<double>* st, double* part,
+                    double* hist, int* hist_it, int hist_cap, double tol, int max_iter,
+                    int init_guess_null, cudaStream_t s, ChainState<double>* out) {
+  ChainState<double> init{};
+  init.max_iter = max_iter;
+  init.tol = tol;
+  init.hist_cap = hist_cap;
+  init.zc = 1.0;
+  SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  const size_t nn = (size_t)n;
+  BicgChain<double> bc{n, x, work, work + nn, work + 2 * nn, work + 3 * nn, work + 4 * nn,
+                       work + 5 * nn, work + 6 * nn, work + 7 * nn, st, part, hist, hist_it};
+  // the start: ||b||, r = b (- A x) with Finished(||r||) and rho = (r, r) = (rt, r)
+  ChainArgs<double> a{n, b, x, bc.r, bc.p, bc.v, nullptr, st, part, hist, hist_it};
+  const int ge = chain_elem_grid(n);
+  k_norm_b<double><<<ge, CT, 0, s>>>(a);
+  if (init_guess_null)
+    k_init_null<double><<<ge, CT, 0, s>>>(a);
+  else
+    SB2_TRY((launch_spmv_pair<double, double>(1, a, S, s)));
+  k_b_copy<double><<<ge, CT, 0, s>>>(bc);
+  SB2_CUDA_TRY(cudaGetLastError());
+  ChainPipe<double> pipe;
+  SB2_TRY(pipe.init());
+  ChunkPlanner plan;
+  int launched = 0, chunk = 2;
+  for (;;) {
+    for (int c = 0; c < chunk; c++) {
+      SB2_CUDA_TRY(launch_pdl(k_b_p<double>, ge, s, bc));
+      SB2_TRY(apply(bc.p, bc.phat, s));
+      SB2_TRY(launch_b_spmv<double>(0, bc, S, s));
+      SB2_CUDA_TRY(launch_pdl(k_b_s<double>, ge, s, bc));
+      SB2_TRY(apply(bc.s, bc.shat, s));
+      SB2_TRY(launch_b_spmv<double>(1, bc, S, s));
+      SB2_CUDA_TRY(launch_pdl(k_b_xr<double>, ge, s, bc));
+    }
+    SB2_CUDA_TRY(cudaGetLastError());
+    launched += chunk;
+    SB2_TRY(pipe.mark(st, launched, s));
+    ChainState<double> h;
+    int at = 0;
+    SB2_TRY(pipe.wait(&h, &at));
+    if (h.done || 2 * at > max_iter + 2) break;
+    // two iterations of the counter a loop
+    chunk = (plan.next(h.nb_iter, h.reste, tol, 0, std::min(chunk * 4, 16), 2, 16) + 1) / 2;
   }
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));

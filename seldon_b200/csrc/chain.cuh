@@ -41,6 +41,10 @@ struct ChainState {
   T zc;          // coefficient of z in the next p update (1 except right
                  // after a correction, where it also removes from p its
                  // component along the replaced residual)
+  // BiCgStab (chain_pbicgstab): omega, and `fin` once Finished(||s||) has
+  // stopped the solve in mid-loop (x still takes alpha * phat)
+  T omega;
+  int fin;
 };
 
 template <typename T>

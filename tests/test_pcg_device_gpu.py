@@ -1,4 +1,4 @@
-"""Cg with SOR or ILUT preconditioning as a device-resident chain.
+"""Cg and BiCgStab with SOR or ILUT preconditioning as device-resident chains.
 
 The scalars of the iteration (rho, alpha, beta, the residual, the stop flag)
 stay in device memory and the preconditioner's level-scheduled sweeps are
@@ -6,7 +6,9 @@ enqueued between the chain's passes, so no iteration waits on the host.
 Against the oracle's Cg with the same preconditioner (Cg.cxx:45-116 with
 SorPreconditioner, Precond_Ssor.cxx:62-74): same error code, iteration count
 within max(2, 5%), solutions to the accuracy the tolerance implies; and
-against the host-driven loop of library calls (sb2_krylov_set_pcg(0))."""
+against the host-driven loop of library calls (sb2_krylov_set_pcg(0)).
+BiCgStab follows BiCgStab.cxx:43-145: two iterations of the counter per
+loop, Finished() on ||r|| and on ||s||."""
 import time
 
 import numpy as np
@@ -24,11 +26,11 @@ def api(cuda):
     return api
 
 
-def _cg(api, A, b, M, tol=1e-10, max_iter=5000):
+def _cg(api, A, b, M, tol=1e-10, max_iter=5000, solver="Cg"):
     X = to_dev(np.zeros(A.m))
     it = api.Iteration(max_iter, tol)
     it.HideMessages()
-    code = api.Cg(A, X, to_dev(b), M, it)
+    code = getattr(api, solver)(A, X, to_dev(b), M, it)
     return code, it, to_host(X)
 
 
@@ -108,4 +110,68 @@ def test_device_chain_edge_cases(api, oracle):
     # repeated solves give the same bits (fixed-order reductions)
     _, _, x1 = _cg(api, A, b, S)
     _, _, x2 = _cg(api, A, b, S)
+    assert np.array_equal(x1, x2)
+
+
+# ------------------------------------------------------------------ BiCgStab
+
+@pytest.mark.parametrize("sym", [False, True])
+def test_ssor_bicgstab_convdiff(api, oracle, sym):
+    full = matgen.convdiff3d(40) if not sym else matgen.poisson3d(40)  # 64,000 rows
+    A = matgen.upper(*full) if sym else full
+    n = full[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(40).uniform(-1, 1, n))
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+    S = api.SorPreconditioner()
+    S.SetParameterRelaxation(1.2)
+    (code, it, x, t_dev), (code_h, it_h, x_h, t_host) = _both(api, M, b, S, solver="BiCgStab")
+    xo, co, no, _, _ = oracle.solve("bicgstab", *A, b, sym=sym, precond=2, omega=1.2, tol=1e-10,
+                                    max_iter=5000)
+    assert code == code_h == co == 0
+    assert abs(it.GetNumberIteration() - no) <= max(2, no // 10), (it.GetNumberIteration(), no)
+    assert abs(it.GetNumberIteration() - it_h.GetNumberIteration()) <= max(2, no // 10)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+    assert np.linalg.norm(x - x_h) / np.linalg.norm(x_h) < 1e-7
+    r = oracle.mltadd(n, n, *full, -1.0, x, 1.0, b)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-10
+    # the history is Seldon's: Finished() on ||r|| and on ||s||, the counter
+    # rising by one each time
+    hs = [h[0] for h in it.history]
+    assert hs == list(range(it.GetNumberIteration() + 1))
+    print(f"SSOR-BiCgStab 40^3 sym={sym}: {it.GetNumberIteration()} it, device chain "
+          f"{t_dev * 1e3:.1f} ms, host-driven {t_host * 1e3:.1f} ms")
+
+
+def test_ilut_bicgstab_device_chain(api, oracle):
+    ptr, ind, val = matgen.convdiff3d(30)
+    n = ptr.size - 1
+    S = api.RowSparse(n, n, ptr, ind, val)
+    M = api.IlutPreconditioning()
+    M.SetDroppingThreshold(1e-2)
+    M.FactorizeMatrix(S)
+    b = matgen.matvec(ptr, ind, val, np.random.default_rng(5).uniform(-1, 1, n))
+    (code, it, x, _), (code_h, it_h, x_h, _) = _both(api, S, b, M, solver="BiCgStab")
+    assert code == code_h == 0
+    assert abs(it.GetNumberIteration() - it_h.GetNumberIteration()) <= 2
+    assert np.linalg.norm(x - x_h) / np.linalg.norm(x_h) < 1e-8
+    r = oracle.mltadd(n, n, ptr, ind, val, -1.0, x, 1.0, b)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-10
+
+
+def test_bicgstab_device_chain_edge_cases(api, oracle):
+    full = matgen.convdiff3d(12)
+    n = full[0].size - 1
+    A = api.RowSparse(n, n, *full)
+    S = api.SorPreconditioner()
+    code, it, x = _cg(api, A, np.zeros(n), S, solver="BiCgStab")
+    assert code == 0 and it.GetNumberIteration() == 0 and not x.any()
+    b = matgen.matvec(*full, np.random.default_rng(2).uniform(-1, 1, n))
+    for max_iter in (3, 4):  # stops on ||s|| (odd) and on ||r|| (even)
+        code, it, x = _cg(api, A, b, S, solver="BiCgStab", max_iter=max_iter)
+        xo, co, no, _, _ = oracle.solve("bicgstab", *full, b, precond=2, tol=1e-10,
+                                        max_iter=max_iter)
+        assert code == co == -2 and it.GetNumberIteration() == no == max_iter
+        np.testing.assert_allclose(x, xo, rtol=1e-10, atol=1e-13)
+    _, _, x1 = _cg(api, A, b, S, solver="BiCgStab")
+    _, _, x2 = _cg(api, A, b, S, solver="BiCgStab")
     assert np.array_equal(x1, x2)
