@@ -162,12 +162,14 @@ def test_batch_autotune_and_graph(api):
     X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
     assert B.autotune(X, b, tol=1e-9) in (128, 256, 512)
     chosen = B.plan()
+    chosen_cluster = B.cluster_plan()
     assert chosen[1] in (0, 256, 1024)
-    # a batch with the same size histogram takes the cached plan
+    assert chosen_cluster[0] in (0, 4, 16)
+    # a batch with the same size histogram takes the cached plan, cluster part included
     B2 = api.Batch(systems)
-    B2.set_plan(128, 0)
+    B2.set_plan(128, 0, 2, 5)
     B2.autotune(X, b, tol=1e-9)
-    assert B2.plan() == chosen
+    assert B2.plan() == chosen and B2.cluster_plan() == chosen_cluster
     B2.close()
     # the solve enqueues only device work: capture it once, replay it
     X.zero_()
