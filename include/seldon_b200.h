@@ -611,15 +611,17 @@ int sb2_krylov_set_config(int chain_min_n);
  * cap).  No counterpart in the reference (a tuning knob of this engine). */
 int sb2_krylov_set_cluster(int on);
 
-/* Cg and BiCgStab with an SOR or ILUT preconditioner: 1 (default) runs them
- * as chains of device kernels whose scalars (rho, alpha, beta, omega, the
- * residual and the stop flags) stay in device memory, the preconditioner's
- * sweeps enqueued between them, with no host synchronization per iteration;
- * 0 runs the host-driven loop of library calls (a dot product returned to
- * the host each time, as the reference's generic driver does).  The two
- * group their reductions differently, so their iterates agree to rounding.
- * Gmres with these preconditioners is host-driven.  Returns the previous
- * setting.  No counterpart in the reference (a tuning knob of this engine). */
+/* Cg, BiCgStab and Gmres with an SOR or ILUT preconditioner: 1 (default)
+ * runs them as chains of device kernels whose scalars (rho, alpha, beta,
+ * omega, Gmres's Hessenberg matrix, rotations and s, the residual and the
+ * stop flags) stay in device memory, the preconditioner's sweeps enqueued
+ * between them, with no host synchronization per iteration (Gmres: the host
+ * reads the state once per chunk of Arnoldi steps, to place the end of each
+ * cycle); 0 runs the host-driven loop of library calls (a dot product
+ * returned to the host each time, as the reference's generic driver does).
+ * The two group their reductions differently, so their iterates agree to
+ * rounding.  Returns the previous setting.  No counterpart in the reference
+ * (a tuning knob of this engine). */
 int sb2_krylov_set_pcg(int device_resident);
 
 /* Device-side wait limit for the fused solvers' grid barriers, in

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "chain.cuh"
+#include "givens.cuh"
 #include "spmv_core.cuh"
 
 namespace sb2 {
@@ -736,6 +737,273 @@ __global__ void __launch_bounds__(CT, 4) k_b_xr(BicgChain<T> a) {
   }
 }
 
+// ----------------------------------------------------------------- Gmres, any preconditioner
+//
+// Restarted Gmres(m) (Gmres.cxx:44-183, left preconditioned, Seldon's
+// modified Gram-Schmidt) with a preconditioner applied by its own launches,
+// every scalar, the Hessenberg matrix, the rotations and s in device memory.
+// Step i of a cycle:
+//   K_gprod (u = A V_i) -> [M apply: w] -> K_gdot0 (H(0,i) = (V_0, w))
+//   -> K_gmgs(k), k = 0..i: Add(-H(k,i), V_k, w), then H(k+1,i) = (V_{k+1}, w)
+//      or, for k = i, ||w|| and the step's tail (rotations, ++iter, the inner
+//      test) -> K_gvnext (V_{i+1} = w / ||w||)
+// A step's kernels run only if the steps before it completed in this cycle
+// and no inner test has stopped it (the host enqueues steps ahead; the
+// applies cannot check, and compute from stale input).  At the end of a
+// cycle: K_gsolve (back-solve, one thread) -> K_gxupd (x += V y) -> the
+// residual product -> [M apply: r] -> K_gbeta (||r||, the outer test, the
+// next cycle's s).  The cycle-end flag is ChainState::pending, which the host
+// reads from its snapshots.
+
+struct GmresChain {
+  int n;
+  const double* b;
+  double* x;
+  double* w;
+  double* r;
+  double* u;
+  double* V;     // m+1 vectors, ldv apart
+  long long ldv;
+  ChainState<double>* st;
+  GmresChainExtra* ex;
+  double* Hm;    // (m+1) x (m+1), column-major, rotated in place
+  double* sv;    // s(0..m)
+  double* cs;
+  double* sn;
+  double* part;
+  double* hist;
+  int* hist_it;
+};
+
+__device__ __forceinline__ bool g_done(const GmresChain& a) {
+  return *((volatile const int*)&a.st->done) != 0;
+}
+// step i's kernels run after steps 0..i-1 of this cycle, until an inner stop
+__device__ __forceinline__ bool g_step_live(const GmresChain& a, int i) {
+  return !g_done(a) && !*((volatile const int*)&a.st->pending) &&
+         *((volatile const int*)&a.ex->ncol) == i;
+}
+
+// w = b - A x: Copy(b, w); MltAdd(-1, A, x, 1, w)
+struct EpiGResidual {
+  const double* b;
+  double* w;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    w[i] = add_rn(__ldg(b + i), mul_rn(-1.0, t));
+  }
+};
+// u = A v
+struct EpiGStore {
+  double* u;
+  __device__ __forceinline__ void operator()(int i, double t) { u[i] = t; }
+};
+
+template <typename VT, int PART>
+__global__ void __launch_bounds__(CT, PART == 1 ? 1 : chain_spmv_occ<VT>())
+    k_gresid(GmresChain a, SellOp<VT> S) {
+  __shared__ double s_red[CT / 32];
+  pdl_wait();
+  pdl_release();
+  if (g_done(a)) return;
+  EpiGResidual epi{a.b, a.w};
+  XLoadLdg<double> xl{a.x};
+  if (PART == 0)
+    sell_spmv_slices<CT, VT, double, XLoadLdg<double>, EpiGResidual, chain_spmv_unroll<VT>()>(
+        S, xl, epi, blockIdx.x, gridDim.x);
+  else
+    sell_spmv_long<CT, VT, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+}
+
+template <typename VT, int PART>
+__global__ void __launch_bounds__(CT, PART == 1 ? 1 : chain_spmv_occ<VT>())
+    k_gprod(GmresChain a, SellOp<VT> S, int i) {
+  __shared__ double s_red[CT / 32];
+  pdl_wait();
+  pdl_release();
+  if (!g_step_live(a, i)) return;
+  EpiGStore epi{a.u};
+  XLoadLdg<double> xl{a.V + (long long)i * a.ldv};
+  if (PART == 0)
+    sell_spmv_slices<CT, VT, double, XLoadLdg<double>, EpiGStore, chain_spmv_unroll<VT>()>(
+        S, xl, epi, blockIdx.x, gridDim.x);
+  else
+    sell_spmv_long<CT, VT, double>(S, xl, epi, s_red, blockIdx.x, gridDim.x);
+}
+
+// Null initial guess: x = 0, w = b
+__global__ void __launch_bounds__(CT, 4) k_gnull(GmresChain a) {
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    a.x[i] = 0.0;
+    a.w[i] = __ldg(a.b + i);
+  }
+}
+
+// beta = ||r||; the first time the Init test (a zero r ends the solve,
+// x untouched); then the outer test Finished(beta), and the next cycle's s
+__global__ void __launch_bounds__(CT, 4) k_gbeta(GmresChain a, int init) {
+  __shared__ double s_red[CT / 32];
+  __shared__ double s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (g_done(a)) return;
+  double rr = 0.0;
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT) {
+    const double ri = a.r[i];
+    rr = add_rn(rr, mul_rn(ri, ri));
+  }
+  double v[1] = {block_sum<CT>(rr, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    ChainState<double>* st = a.st;
+    GmresChainExtra* ex = a.ex;
+    const double beta = sqrt(s_out[0]);
+    if (init) {
+      if (beta == 0.0) {
+        st->init_failed = 1;
+        st->done = 1;
+        return;
+      }
+      st->facteur = 1.0 / beta;
+    }
+    if (chain_finished_at(st, a.hist, a.hist_it, s_out[0])) {
+      st->done = 1;
+      return;
+    }
+    ex->beta = beta;
+    for (int k = 0; k < ex->ld; k++) a.sv[k] = 0.0;
+    a.sv[0] = beta;
+    ex->ncol = 0;
+    ex->inner_max = st->nb_iter + ex->m;
+    st->pending = 0;
+  }
+}
+
+// V_0 = r / beta: Copy(r, V_0); Mlt(1/beta, V_0)
+__global__ void __launch_bounds__(CT, 4) k_gv0(GmresChain a) {
+  pdl_wait();
+  pdl_release();
+  if (g_done(a)) return;
+  const double inv = 1.0 / a.ex->beta;
+  for (long long i = (long long)blockIdx.x * CT + threadIdx.x; i < a.n; i += (long long)gridDim.x * CT)
+    a.V[i] = mul_rn(a.r[i], inv);
+}
+
+// H(0,i) = (V_0, w)
+__global__ void __launch_bounds__(CT, 4) k_gdot0(GmresChain a, int i) {
+  __shared__ double s_red[CT / 32];
+  __shared__ double s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (!g_step_live(a, i)) return;
+  double acc = 0.0;
+  for (long long e = (long long)blockIdx.x * CT + threadIdx.x; e < a.n; e += (long long)gridDim.x * CT)
+    acc = add_rn(acc, mul_rn(a.V[e], a.w[e]));
+  double v[1] = {block_sum<CT>(acc, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    a.ex->h = s_out[0];
+    a.Hm[0 + (size_t)i * a.ex->ld] = s_out[0];
+  }
+}
+
+// Add(-H(k,i), V_k, w); then H(k+1,i) = (V_{k+1}, w) (k < i) or, for k = i,
+// ||w|| and the step's tail: the rotations of column i (ApplyRot with the
+// earlier ones, GenRot, ApplyRot on s), ++iter and the inner test on |s(i+1)|
+__global__ void __launch_bounds__(CT, 4) k_gmgs(GmresChain a, int i, int k) {
+  __shared__ double s_red[CT / 32];
+  __shared__ double s_out[1];
+  pdl_wait();
+  pdl_release();
+  if (!g_step_live(a, i)) return;
+  const double mh = -a.ex->h;
+  const double* vk = a.V + (long long)k * a.ldv;
+  const double* vn = k < i ? a.V + (long long)(k + 1) * a.ldv : nullptr;
+  double acc = 0.0;
+  for (long long e = (long long)blockIdx.x * CT + threadIdx.x; e < a.n; e += (long long)gridDim.x * CT) {
+    double we = a.w[e];
+    if (mh != 0.0) {
+      we = add_rn(we, mul_rn(mh, vk[e]));
+      a.w[e] = we;
+    }
+    acc = add_rn(acc, vn ? mul_rn(vn[e], we) : mul_rn(we, we));
+  }
+  double v[1] = {block_sum<CT>(acc, s_red)};
+  if (deposit_and_finish<CT, 1>(v, a.part, &a.st->cnt, blockIdx.x, gridDim.x, s_red, s_out) &&
+      threadIdx.x == 0) {
+    GmresChainExtra* ex = a.ex;
+    const int ld = ex->ld;
+    if (k < i) {
+      ex->h = s_out[0];
+      a.Hm[k + 1 + (size_t)i * ld] = s_out[0];
+      return;
+    }
+    ChainState<double>* st = a.st;
+    double hi = sqrt(s_out[0]);
+    ex->hi = hi;
+    double* Hc = a.Hm + (size_t)i * ld;
+    for (int q = 0; q < i; q++) apply_rot(Hc[q], Hc[q + 1], a.cs[q], a.sn[q]);
+    if (hi != 0.0) {
+      gen_rot(Hc[i], hi, a.cs[i], a.sn[i]);
+      apply_rot(a.sv[i], a.sv[i + 1], a.cs[i], a.sn[i]);
+    }
+    st->nb_iter++;
+    ex->ncol = i + 1;
+    // inner.Finished(|s(i+1)|): its limit is the end of the cycle
+    const double reste = st->facteur * fabs(a.sv[i + 1]);
+    st->reste = reste;
+    if (st->hist_len < st->hist_cap) {
+      a.hist[st->hist_len] = reste;
+      a.hist_it[st->hist_len] = st->nb_iter;
+    }
+    st->hist_len++;
+    if (reste < st->tol || st->nb_iter >= ex->inner_max) st->pending = 1;
+  }
+}
+
+// V_{i+1} = w, scaled by 1/||w|| unless ||w|| = 0
+__global__ void __launch_bounds__(CT, 4) k_gvnext(GmresChain a, int i) {
+  pdl_wait();
+  pdl_release();
+  if (g_done(a) || *((volatile const int*)&a.ex->ncol) != i + 1) return;
+  const double hi = a.ex->hi;
+  const double inv = hi != 0.0 ? 1.0 / hi : 1.0;
+  double* vn = a.V + (long long)(i + 1) * a.ldv;
+  for (long long e = (long long)blockIdx.x * CT + threadIdx.x; e < a.n; e += (long long)gridDim.x * CT)
+    vn[e] = hi != 0.0 ? mul_rn(a.w[e], inv) : a.w[e];
+}
+
+// Solve(H, s) on the leading ncol x ncol block (the netlib DTRSV column
+// sweep the reference's cblas path takes), one thread
+__global__ void k_gsolve(GmresChain a) {
+  pdl_wait();
+  pdl_release();
+  if (g_done(a) || threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int nc = a.ex->ncol, ld = a.ex->ld;
+  double* sv = a.sv;
+  for (int j = nc - 1; j >= 0; j--)
+    if (sv[j] != 0.0) {
+      sv[j] = sv[j] / a.Hm[j + (size_t)j * ld];
+      const double t = sv[j];
+      for (int q = j - 1; q >= 0; q--) sv[q] = __dsub_rn(sv[q], mul_rn(t, a.Hm[q + (size_t)j * ld]));
+    }
+}
+
+// x += sum_k s(k) V_k, k in order (Add skipped for s(k) = 0)
+__global__ void __launch_bounds__(CT, 4) k_gxupd(GmresChain a) {
+  pdl_wait();
+  pdl_release();
+  if (g_done(a)) return;
+  const int nc = a.ex->ncol;
+  for (long long e = (long long)blockIdx.x * CT + threadIdx.x; e < a.n; e += (long long)gridDim.x * CT) {
+    double xe = a.x[e];
+    for (int k = 0; k < nc; k++) {
+      const double y = a.sv[k];
+      if (y != 0.0) xe = add_rn(xe, mul_rn(y, a.V[(long long)k * a.ldv + e]));
+    }
+    a.x[e] = xe;
+  }
+}
+
 // ----------------------------------------------------------------- host driver
 
 // Elementwise passes: at most one resident wave (4 CTAs per SM), threads
@@ -971,6 +1239,97 @@ int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, 
     if (h.done || 2 * at > max_iter + 2) break;
     // two iterations of the counter a loop
     chunk = (plan.next(h.nb_iter, h.reste, tol, 0, std::min(chunk * 4, 16), 2, 16) + 1) / 2;
+  }
+  SB2_CUDA_TRY(cudaStreamSynchronize(s));
+  SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));
+  return SB2_OK;
+}
+
+// The residual product w = b - A x, or step i's product u = A V_i.
+template <typename VT>
+static int launch_gspmv(bool resid, const GmresChain& a, const SellOp<VT>& S, int i,
+                        cudaStream_t s) {
+  const int g1 = reducing_slice_grid(S);
+  const int g2 = (S.nwarp_rows + S.ncta_rows) > 0 ? std::max((S.nwarp_rows + 7) / 8, S.ncta_rows) : 0;
+  if (g1 + g2 == 0) return SB2_ERR_NOT_SUPPORTED;
+  if (resid) {
+    if (g1) SB2_CUDA_TRY(launch_pdl(k_gresid<VT, 0>, g1, s, a, S));
+    if (g2) SB2_CUDA_TRY(launch_pdl(k_gresid<VT, 1>, g2, s, a, S));
+  } else {
+    if (g1) SB2_CUDA_TRY(launch_pdl(k_gprod<VT, 0>, g1, s, a, S, i));
+    if (g2) SB2_CUDA_TRY(launch_pdl(k_gprod<VT, 1>, g2, s, a, S, i));
+  }
+  return SB2_OK;
+}
+
+// Gmres(m) with a preconditioner's own launches (SOR, ILUT), as a
+// device-resident chain.  work: (m+4) vectors `ldv` apart (w, r, u, V_0..V_m);
+// hbuf: (m+1)^2 + 3(m+1) doubles (H, s, cos, sin).  The host enqueues the
+// steps of a cycle in chunks sized from the residual's decay and reads the
+// state behind each chunk; once an inner test has stopped the cycle
+// (ChainState::pending), it enqueues the cycle's end: the back-solve, the
+// update of x, the new residual and the outer test.
+int chain_pgmres(const SellOp<double>& S, int n, int m, const PrecondLaunch& apply, double* x,
+                 const double* b, double* work, long long ldv, ChainState<double>* st,
+                 GmresChainExtra* ex, double* hbuf, double* part, double* hist, int* hist_it,
+                 int hist_cap, double tol, int max_iter, int init_guess_null, cudaStream_t s,
+                 ChainState<double>* out) {
+  const int ld = m + 1;
+  ChainState<double> init{};
+  init.max_iter = max_iter;
+  init.tol = tol;
+  init.hist_cap = hist_cap;
+  GmresChainExtra ei{};
+  ei.m = m;
+  ei.ld = ld;
+  SB2_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  SB2_CUDA_TRY(cudaMemcpyAsync(ex, &ei, sizeof(ei), cudaMemcpyHostToDevice, s));
+  SB2_CUDA_TRY(cudaMemsetAsync(hbuf, 0, sizeof(double) * ((size_t)ld * ld + 3 * (size_t)ld), s));
+  GmresChain a{n, b, x, work, work + ldv, work + 2 * ldv, work + 3 * ldv, ldv, st, ex, hbuf,
+               hbuf + (size_t)ld * ld, hbuf + (size_t)ld * ld + ld, hbuf + (size_t)ld * ld + 2 * ld,
+               part, hist, hist_it};
+  const int ge = chain_elem_grid(n);
+  if (init_guess_null) {
+    k_gnull<<<ge, CT, 0, s>>>(a);
+    SB2_CUDA_TRY(cudaGetLastError());
+  } else {
+    SB2_TRY(launch_gspmv<double>(true, a, S, 0, s));
+  }
+  SB2_TRY(apply(a.w, a.r, s));
+  SB2_CUDA_TRY(launch_pdl(k_gbeta, ge, s, a, 1));
+  ChainPipe<double> pipe;
+  SB2_TRY(pipe.init());
+  int launched = 0, at = 0;
+  ChainState<double> h;
+  SB2_TRY(pipe.mark(st, ++launched, s));
+  SB2_TRY(pipe.wait(&h, &at));
+  ChunkPlanner plan;
+  int chunk = std::min(4, m);
+  for (int cycles = 0; !h.done && cycles <= max_iter; cycles++) {
+    SB2_CUDA_TRY(launch_pdl(k_gv0, ge, s, a));
+    int step = 0;
+    for (;;) {
+      for (int c = 0; c < chunk && step < m; c++, step++) {
+        SB2_TRY(launch_gspmv<double>(false, a, S, step, s));
+        SB2_TRY(apply(a.u, a.w, s));
+        SB2_CUDA_TRY(launch_pdl(k_gdot0, ge, s, a, step));
+        for (int k = 0; k <= step; k++) SB2_CUDA_TRY(launch_pdl(k_gmgs, ge, s, a, step, k));
+        SB2_CUDA_TRY(launch_pdl(k_gvnext, ge, s, a, step));
+      }
+      SB2_TRY(pipe.mark(st, ++launched, s));
+      SB2_TRY(pipe.wait(&h, &at));
+      if (h.done || h.pending || step >= m) break;
+      chunk = plan.next(h.nb_iter, h.reste, tol, 0, std::min(chunk * 2, m), 1, m - step);
+    }
+    if (h.done) break;
+    // the cycle's end: Solve(H, s), x += V s, r = M^{-1}(b - A x), Finished(||r||)
+    SB2_CUDA_TRY(launch_pdl(k_gsolve, 1, s, a));
+    SB2_CUDA_TRY(launch_pdl(k_gxupd, ge, s, a));
+    SB2_TRY(launch_gspmv<double>(true, a, S, 0, s));
+    SB2_TRY(apply(a.w, a.r, s));
+    SB2_CUDA_TRY(launch_pdl(k_gbeta, ge, s, a, 0));
+    SB2_TRY(pipe.mark(st, ++launched, s));
+    SB2_TRY(pipe.wait(&h, &at));
   }
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   SB2_CUDA_TRY(cudaMemcpy(out, st, sizeof(*out), cudaMemcpyDeviceToHost));

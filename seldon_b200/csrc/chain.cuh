@@ -62,6 +62,17 @@ struct ChainArgs {
   int* hist_it;
 };
 
+// Device-resident scalars of chain_pgmres beyond ChainState's (whose
+// `pending` flags the end of a cycle there).
+struct GmresChainExtra {
+  int m, ld;
+  int ncol;       // steps done in the current cycle
+  int inner_max;  // iteration count at which the cycle ends
+  double beta;    // ||r|| at the start of the cycle
+  double h;       // the coefficient of the next MGS pass
+  double hi;      // ||w|| of the last step
+};
+
 // A preconditioner apply z = M^{-1} r enqueued on a stream (chain_pcg).
 struct PrecondLaunch {
   const sb2_precond* M;

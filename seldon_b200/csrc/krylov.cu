@@ -1352,16 +1352,29 @@ int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, 
                     double* hist, int* hist_it, int hist_cap, double tol, int max_iter,
                     int init_guess_null, cudaStream_t s, ChainState<double>* out);
 
-// Cg (BICG = false) or BiCgStab (true) with SOR or ILUT as a device-resident
-// chain around the preconditioner's launches.
+int chain_pgmres(const SellOp<double>& S, int n, int m, const PrecondLaunch& apply, double* x,
+                 const double* b, double* work, long long ldv, ChainState<double>* st,
+                 GmresChainExtra* ex, double* hbuf, double* part, double* hist, int* hist_it,
+                 int hist_cap, double tol, int max_iter, int init_guess_null, cudaStream_t s,
+                 ChainState<double>* out);
+
+// Cg, BiCgStab or Gmres with SOR or ILUT as a device-resident chain around
+// the preconditioner's launches.
 static int pcg_solve(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                      const sb2_iter_params* prm, sb2_iter_result* res, double* hist,
-                     int* hist_it, int hist_cap, cudaStream_t s, bool bicg = false) {
+                     int* hist_it, int hist_cap, cudaStream_t s, int which = kCg) {
   const SellOp<double> S = sell_op(A->full);
   const int n = A->m;
   const long long slots = chain_part_slots(S, n);
   const int hcap = std::max(hist_cap, 1);
-  const size_t vb = sizeof(double) * (bicg ? 8 : 4) * (size_t)n;
+  const int m = std::max(prm->restart, 1);
+  const long long ldv = (long long)vector_stride(n, sizeof(double));
+  // Gmres: w, r, u, V_0..V_m, then H, s, cos, sin and the extra scalars
+  const size_t gh = sizeof(double) * ((size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1)) +
+                    sizeof(GmresChainExtra);
+  const size_t vb = which == kGmres
+                        ? sizeof(double) * (size_t)ldv * (m + 4) + (gh + 255) / 256 * 256
+                        : sizeof(double) * (which == kBicg ? 8 : 4) * (size_t)n;
   const size_t sb = 256, pb = sizeof(double) * slots, hb = sizeof(double) * hcap, ib = sizeof(int) * hcap;
   DeviceBuf buf;
   buf.s = s;
@@ -1373,12 +1386,19 @@ static int pcg_solve(const sb2_csr* A, const sb2_precond* M, double* x, const do
   double* dh = (double*)(c + vb + sb + pb);
   int* dhi = (int*)(c + vb + sb + pb + hb);
   ChainState<double> o;
-  if (bicg)
+  if (which == kGmres) {
+    double* hb = work + (size_t)ldv * (m + 4);
+    GmresChainExtra* ex = reinterpret_cast<GmresChainExtra*>(
+        hb + (size_t)(m + 1) * (m + 1) + 3 * (size_t)(m + 1));
+    SB2_TRY(chain_pgmres(S, n, m, PrecondLaunch{M, false}, x, b, work, ldv, st, ex, hb, part, dh,
+                         dhi, hcap, prm->tol, prm->max_iter, prm->init_guess_null, s, &o));
+  } else if (which == kBicg) {
     SB2_TRY(chain_pbicgstab(S, n, PrecondLaunch{M, false}, x, b, work, st, part, dh, dhi, hcap,
                             prm->tol, prm->max_iter, prm->init_guess_null, s, &o));
-  else
+  } else {
     SB2_TRY(chain_pcg(S, n, PrecondLaunch{M, false}, x, b, work, st, part, dh, dhi, hcap,
                       prm->tol, prm->max_iter, prm->init_guess_null, s, &o));
+  }
   const int nh = std::min(o.hist_len, std::max(hist_cap, 0));
   if (hist && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist, dh, sizeof(double) * nh, cudaMemcpyDeviceToHost));
   if (hist_it && nh > 0) SB2_CUDA_TRY(cudaMemcpy(hist_it, dhi, sizeof(int) * nh, cudaMemcpyDeviceToHost));
@@ -1409,9 +1429,9 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   } else if (M && precond_matrix(M) != A) {
     return SB2_ERR_INVALID_VALUE;
   }
-  if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && (which == kCg || which == kBicg) &&
-      A->full.sell.nslice >= 0 && g_pcg_device)
-    return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which == kBicg);
+  if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && A->full.sell.nslice >= 0 &&
+      g_pcg_device)
+    return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which);
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;
