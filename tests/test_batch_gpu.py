@@ -132,6 +132,31 @@ def test_batch_cluster_plan_few_large_systems(api, oracle):
     print("few large systems, ms:", {k: round(v, 2) for k, v in out.items()})
 
 
+def test_batch_cluster_plan_wide_columns(api, oracle):
+    """A system of more than 65,536 rows makes the batch keep 4-byte local
+    columns; a cluster solves it, CTAs and warps the small ones."""
+    import torch
+    big = matgen.lap2d(262, shift=0.01)  # 68,644 rows
+    systems, rhs, _ = _systems(11, 10, 4, 40)
+    xs = np.random.default_rng(12).uniform(-1, 1, 262 * 262)
+    systems.insert(3, big)
+    rhs.insert(3, matgen.matvec(*big, xs))
+    B = api.Batch(systems)
+    B.set_plan(512, 256, 8, 1000)
+    b = to_dev(np.concatenate(rhs))
+    X = torch.zeros(B.m, dtype=torch.float64, device="cuda")
+    it = torch.zeros(B.nsys, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(B.nsys, dtype=torch.float64, device="cuda")
+    res = B.solve(X, b, it, rr, tol=1e-9, max_iter=20000)
+    assert res.converged == B.nsys and res.max_rel_residual < 1e-9
+    x = to_host(X)
+    for s in (0, 3, 10):
+        ptr, ind, val = systems[s]
+        xsys = x[B.sys_row[s]:B.sys_row[s + 1]]
+        xo, _, _, _, _ = oracle.solve("cg", ptr, ind, val, rhs[s], tol=1e-9, max_iter=20000)
+        assert np.linalg.norm(xsys - xo) / np.linalg.norm(xo) < 1e-6
+
+
 def test_batch_edges(api):
     import torch
     systems, rhs, xs = _systems(2, 6, 3, 12, zero=(2,))

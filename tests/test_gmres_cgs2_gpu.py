@@ -63,7 +63,7 @@ def _gmres(api, A, b, M, restart, tol=1e-10, max_iter=5000, orth="cgs2", x0=None
 
 
 @pytest.mark.parametrize("name", ["conv7", "conv16", "zipf", "lap"])
-@pytest.mark.parametrize("restart", [5, 20, 30])
+@pytest.mark.parametrize("restart", [1, 2, 5, 20, 30, 32])
 @pytest.mark.parametrize("jacobi", [False, True])
 def test_cgs2_matches_oracle(api, oracle, name, restart, jacobi):
     ptr, ind, val, b = _system(name)

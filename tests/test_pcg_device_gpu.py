@@ -164,6 +164,24 @@ def test_ilut_bicgstab_device_chain(api, oracle):
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-10
 
 
+def test_ilut_sym_bicgstab_device_chain(api, oracle):
+    full = matgen.lap2d(200)
+    up = matgen.upper(*full)
+    n = up[0].size - 1
+    S = api.RowSymSparse(n, *up)
+    M = api.IlutPreconditioning()
+    M.SetSymmetricAlgorithm()
+    M.SetDroppingThreshold(1e-3)
+    M.FactorizeMatrix(S)
+    b = matgen.matvec(*full, np.random.default_rng(8).uniform(-1, 1, n))
+    (code, it, x, _), (code_h, it_h, x_h, _) = _both(api, S, b, M, solver="BiCgStab")
+    assert code == code_h == 0
+    assert abs(it.GetNumberIteration() - it_h.GetNumberIteration()) <= 2
+    assert np.linalg.norm(x - x_h) / np.linalg.norm(x_h) < 1e-8
+    r = oracle.mltadd(n, n, *full, -1.0, x, 1.0, b)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.05e-10
+
+
 def test_bicgstab_device_chain_edge_cases(api, oracle):
     full = matgen.convdiff3d(12)
     n = full[0].size - 1
