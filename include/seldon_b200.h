@@ -275,8 +275,8 @@ int sb2_precond_destroy(sb2_precond* M);
  * z is the reference's z bit for bit.  The arrays are copied.  A factor
  * whose rows break the layout above gives SB2_ERR_INVALID_CSR, a
  * permutation that is not one SB2_ERR_INVALID_VALUE.  The Krylov drivers
- * accept it (host-driven iterations); sb2_ir_cg does not
- * (SB2_ERR_NOT_SUPPORTED). */
+ * accept it (device-resident chains around its sweeps, sb2_krylov_set_pcg);
+ * sb2_ir_solve does not (SB2_ERR_NOT_SUPPORTED). */
 int sb2_precond_create_ilut(const sb2_csr* A, int n, const int* fptr,
                             const int* find, const double* fval,
                             const int* perm_row, const int* perm_col,
