@@ -513,15 +513,21 @@ def _cpu_solve(which, ptr, ind, val, b, x_gpu, sym=False, precond=0, restart=10,
     if fast is None:
         return {"unavailable": "oracle/_ref is not built"}
     n = ptr.size - 1
-    t0 = time.perf_counter()
-    xr, code, it = fast.solve(which, ptr, ind, val, b, sym=sym, precond=precond, tol=tol,
-                              max_iter=max_iter, restart=restart)
-    dt = time.perf_counter() - t0
+    # a solve under 0.2 s is repeated (best of up to 5): the host is shared and
+    # the other records' solves run beside it, so one short run varies by 2x
+    dt, reps = None, 0
+    while reps < 5 and (dt is None or dt < 0.2):
+        t0 = time.perf_counter()
+        xr, code, it = fast.solve(which, ptr, ind, val, b, sym=sym, precond=precond, tol=tol,
+                                  max_iter=max_iter, restart=restart)
+        d = time.perf_counter() - t0
+        dt = d if dt is None else min(dt, d)
+        reps += 1
 
     def relres(x):
         r = parity.mltadd(n, n, ptr, ind, val, -1.0, x, 1.0, b, sym=sym)
         return float(np.linalg.norm(r) / np.linalg.norm(b))
-    return {"ms": round(dt * 1e3, 1), "iterations": it, "error_code": code,
+    return {"ms": round(dt * 1e3, 1), "runs": reps, "iterations": it, "error_code": code,
             "true_rel_residual": relres(xr), "gpu_true_rel_residual": relres(x_gpu),
             "forward_diff_gpu_vs_reference": float(np.linalg.norm(x_gpu - xr) /
                                                   np.linalg.norm(xr)),
