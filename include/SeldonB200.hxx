@@ -1599,13 +1599,24 @@ namespace Seldon
       }
     };
 
-    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2 };
+    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
-      // the strings Cg.cxx:82,101 and BiCgStab.cxx:77,87,107 pass to Fail
+      // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110
+      // and TfQmr.cxx:116,138,148,186,219 pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
+      if (kind == kCgs)
+        return code == 1 ? "Cgs breakdown #1" : "Cgs breakdown #2";
+      if (kind == kTfQmr)
+        {
+          if (code == 1)
+            return "Tfqmr breakdown: sigma=0";
+          if (code == 2)
+            return "Tfqmr breakdown: alpha=0";
+          return code == 5 ? "tfqmr breakdown: beta=0" : "Tfqmr breakdown: tau=0";
+        }
       if (code == 1)
         return "Bicgstab breakdown #1";
       return code == 2 ? "Bicgstab breakdown #2" : "Bicgstab breakdown #3";
@@ -1653,11 +1664,19 @@ namespace Seldon
         st = sb2_gmres(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                        cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                        GetStream());
+      else if (kind == kCgs)
+        st = sb2_cgs(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                     cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kTfQmr)
+        st = sb2_tfqmr(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                       cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
+                       GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
-      Check(st, kind == kCg ? "Cg" : (kind == kBiCgStab ? "BiCgStab" : "Gmres"));
+      static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr"};
+      Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
         return iter.ErrorCode();
@@ -1709,6 +1728,10 @@ namespace Seldon
           return Seldon::Cg<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kBiCgStab)
           return Seldon::BiCgStab<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kCgs)
+          return Seldon::Cgs<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kTfQmr)
+          return Seldon::TfQmr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1760,6 +1783,44 @@ namespace Seldon
                Preconditioner& M, Iteration<Titer>& iter)
   {
     return b200::Solve(b200::kBiCgStab, A, x, b, M, iter);
+  }
+
+  //! Conjugate gradient squared on the GPU (Cgs.cxx:45-132).
+  template <class Titer, class Prop, class Preconditioner>
+  int Cgs(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+          Vector<double, VectFull, CudaAlloc<double> >& x,
+          const Vector<double, VectFull, CudaAlloc<double> >& b,
+          Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCgs, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int Cgs(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+          Vector<double, VectFull, CudaAlloc<double> >& x,
+          const Vector<double, VectFull, CudaAlloc<double> >& b,
+          Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCgs, A, x, b, M, iter);
+  }
+
+  //! Transpose-free QMR on the GPU (TfQmr.cxx:44-243).
+  template <class Titer, class Prop, class Preconditioner>
+  int TfQmr(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+            Vector<double, VectFull, CudaAlloc<double> >& x,
+            const Vector<double, VectFull, CudaAlloc<double> >& b,
+            Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kTfQmr, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int TfQmr(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+            Vector<double, VectFull, CudaAlloc<double> >& x,
+            const Vector<double, VectFull, CudaAlloc<double> >& b,
+            Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kTfQmr, A, x, b, M, iter);
   }
 
   //! Restarted left-preconditioned GMRES(m) on the GPU (Gmres.cxx:44-183).

@@ -378,8 +378,10 @@ typedef struct {
 /* What the solve reports back. */
 typedef struct {
   int nb_iter;          /* Iteration::GetNumberIteration() at exit */
-  int error_code;       /* Iteration::ErrorCode(): 0, -2 (max_iter), 1/2/3 */
-  int init_failed;      /* 1 when Init() found a zero right-hand side */
+  int error_code;       /* Iteration::ErrorCode(): 0, -2 (max_iter), or the
+                           driver's breakdown code (1 to 5) */
+  int init_failed;      /* 1 when Init() found a zero right-hand side (for
+                           TfQmr a zero preconditioned initial residual) */
   int hist_len;         /* entries written to the caller's history buffer */
   double facteur_reste; /* 1/||r_init|| (Iteration::GetFactor) */
   double last_residual; /* relative residual of the last Finished() test */
@@ -398,6 +400,23 @@ int sb2_bicgstab(const sb2_csr* A, const sb2_precond* M, double* x,
                  sb2_iter_result* result, double* hist, int* hist_it,
                  int hist_cap, void* stream);
 int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x,
+              const double* b, const sb2_iter_params* params,
+              sb2_iter_result* result, double* hist, int* hist_it,
+              int hist_cap, void* stream);
+
+/* Seldon's Cgs (Cgs.cxx:45-132) and TfQmr (TfQmr.cxx:44-243), with the
+ * arguments, history and error codes of sb2_cg.  Cgs preconditions on the
+ * right and tests the true residual ||b - A x|| / ||b|| twice per loop
+ * (nb_iter advances by 2, codes 1 and 2 for its two breakdowns).  TfQmr
+ * preconditions on the left and tests the quasi-residual bound
+ * tau sqrt(m + 1) / ||r0|| with r0 = M^{-1}(b - A x0) after each half step
+ * (codes 1 to 5); a zero r0 returns at once as a zero right-hand side does.
+ * The identity and Jacobi run as one persistent kernel per solve; SOR and
+ * ILUT drive the same device operations from the host, one at a time. */
+int sb2_cgs(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+            const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+            int* hist_it, int hist_cap, void* stream);
+int sb2_tfqmr(const sb2_csr* A, const sb2_precond* M, double* x,
               const double* b, const sb2_iter_params* params,
               sb2_iter_result* result, double* hist, int* hist_it,
               int hist_cap, void* stream);

@@ -16,6 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libseldon_ref.so")
+# the `which` numbers of orc_solve / ref_solve
+_SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "cgs": 3, "tfqmr": 4}
 REF_FAST_SO = os.path.join(HERE, "_ref", "libseldon_ref_fast.so")
 
 _vp = ctypes.c_void_p
@@ -134,9 +136,9 @@ class Oracle(_Base):
     def solve(self, which, ptr, ind, val, b, x0=None, sym=False, precond=0, omega=1.0,
               sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
               hist_cap=0):
-        """which: 'cg' | 'bicgstab' | 'gmres'.  precond: 0 identity, 1 Jacobi, 2 SOR.
+        """which: 'cg' | 'bicgstab' | 'gmres' | 'cgs' | 'tfqmr'.  precond: 0 identity, 1 Jacobi, 2 SOR.
         Returns (x, error_code, nb_iter, hist, hist_it)."""
-        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        w = _SOLVERS[which]
         ptr, ind, val = _csr_args(ptr, ind, val)
         m = ptr.size - 1
         b = np.ascontiguousarray(b, dtype=np.float64)
@@ -261,7 +263,7 @@ class Reference(_Base):
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
         nb = ctypes.c_int()
-        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        w = _SOLVERS[which]
         code = self.lib.ref_solve_ilut(w, ptr.size - 1, ind.size, _p(ptr), _p(ind), _p(val),
                                        int(sym), _p(x), _p(b), tol, max_iter, restart,
                                        int(x0 is None), ctypes.byref(nb))
@@ -351,7 +353,7 @@ class Reference(_Base):
               sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
               print_level=0):
         """Returns (x, error_code, nb_iter)."""
-        w = {"cg": 0, "bicgstab": 1, "gmres": 2}[which]
+        w = _SOLVERS[which]
         ptr, ind, val = _csr_args(ptr, ind, val)
         m = ptr.size - 1
         b = np.ascontiguousarray(b, dtype=np.float64)

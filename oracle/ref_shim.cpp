@@ -8,6 +8,7 @@
 //   MltAdd RowSymSparse     computation/basic_functions/Functions_MatVect.cxx:526-564
 //   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
 //   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
+//   Cgs / TfQmr             computation/solver/iterative/{Cgs,TfQmr}.cxx
 //   SOR                     matrix_sparse/Relaxation_MatVect.cxx:41-95, 176-298
 //   SorPreconditioner       computation/solver/preconditioner/Precond_Ssor.cxx:24-90
 //
@@ -122,6 +123,8 @@ namespace
       case 0: return Cg(A, x, b, M, it);
       case 1: return BiCgStab(A, x, b, M, it);
       case 2: return Gmres(A, x, b, M, it);
+      case 3: return Cgs(A, x, b, M, it);
+      case 4: return TfQmr(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -360,7 +363,8 @@ extern "C"
     return 0;
   }
 
-  // which: 0 Cg, 1 BiCgStab, 2 Gmres.  precond: 0 identity, 1 Jacobi, 2 SOR.
+  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr.  precond: 0 identity,
+  // 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
                 const double* val, int sym, int precond, double omega,

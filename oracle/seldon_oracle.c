@@ -541,7 +541,168 @@ out:
   return code;
 }
 
-/* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres.
+/* Cgs, computation/solver/iterative/Cgs.cxx:45-132.  Right preconditioning;
+ * the test is on the unpreconditioned residual and the count advances by two
+ * per loop (after each product). */
+static int orc_cgs_impl(const orc_csr* A, double* x, const double* b,
+                        const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  double rho_1, rho_2 = 0.0, alpha, beta, delta;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *p = malloc(bytes), *phat = malloc(bytes), *q = malloc(bytes),
+         *qhat = malloc(bytes), *vhat = malloc(bytes), *u = malloc(bytes),
+         *uhat = malloc(bytes), *r = malloc(bytes), *rtilde = malloc(bytes);
+  double* all[9] = {p, phat, q, qhat, vhat, u, uhat, r, rtilde};
+  for (int k = 0; k < 9; k++) memcpy(all[k], b, bytes);
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  orc_copy(N, r, rtilde);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r))) {
+    rho_1 = orc_dot(N, rtilde, r);
+    if (rho_1 == 0.0) { it_fail(it, 1); break; }
+    if (it->nb_iter == 0) {
+      orc_copy(N, r, u);
+      orc_copy(N, u, p);
+    } else {
+      /* u = r + beta q;  p = beta (beta p + q) + u */
+      beta = rho_1 / rho_2;
+      orc_copy(N, r, u);
+      orc_axpy(N, beta, q, u);
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, q, p);
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, u, p);
+    }
+    prec_solve(M, A, p, phat);
+    csr_mlt(A, phat, vhat);
+    it->nb_iter++;
+    delta = orc_dot(N, rtilde, vhat);
+    if (delta == 0.0) { it_fail(it, 2); break; }
+    alpha = rho_1 / delta;
+    orc_copy(N, u, q);
+    orc_axpy(N, -alpha, vhat, q);
+    orc_axpy(N, 1.0, q, u);
+    prec_solve(M, A, u, uhat);
+    orc_axpy(N, alpha, uhat, x);
+    csr_mlt(A, uhat, qhat);
+    orc_axpy(N, -alpha, qhat, r);
+    rho_2 = rho_1;
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 9; k++) free(all[k]);
+  return code;
+}
+
+/* TfQmr, computation/solver/iterative/TfQmr.cxx:44-243.  Left
+ * preconditioning; two half steps per loop, each ending with the scalar
+ * test Finished(kappa) (Iterative.cxx:299-319) on the quasi-residual bound
+ * kappa = tau sqrt(m + 1). */
+static int orc_tfqmr_impl(const orc_csr* A, double* x, const double* b,
+                          const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *tmp = malloc(bytes), *r0 = malloc(bytes), *v = malloc(bytes),
+         *h = malloc(bytes), *w = malloc(bytes), *y1 = malloc(bytes),
+         *g = malloc(bytes), *y0 = malloc(bytes), *rtilde = malloc(bytes),
+         *d = malloc(bytes);
+  double* all[10] = {tmp, r0, v, h, w, y1, g, y0, rtilde, d};
+  for (int k = 0; k < 10; k++) memcpy(all[k], b, bytes);
+  double sigma, alpha, beta, eta, rho, rho0, c, kappa, tau, theta;
+  int code;
+  memset(tmp, 0, bytes);
+  /* 1. r0 = M^{-1} (b - A x) */
+  orc_copy(N, b, tmp);
+  if (!it->init_guess_null)
+    csr_residual(A, x, tmp);
+  else
+    memset(x, 0, bytes);
+  prec_solve(M, A, tmp, r0);
+  if (it_init(it, N, r0) != 0) { code = it_error_code(it); goto out; }
+  /* 2.-3. w = y = r0; g = v = M^{-1} A y */
+  orc_copy(N, r0, w);
+  orc_copy(N, r0, y1);
+  orc_copy(N, y1, v);
+  csr_mlt(A, v, tmp);
+  prec_solve(M, A, tmp, v);
+  it->nb_iter++;
+  orc_copy(N, v, g);
+  /* 4.-8. */
+  memset(d, 0, bytes);
+  tau = orc_nrm2(N, r0);
+  theta = 0.0;
+  eta = 0.0;
+  orc_copy(N, r0, rtilde);
+  rho = orc_dot(N, rtilde, r0);
+  rho0 = rho;
+  it->nb_iter = 0;
+  for (;;) {
+    sigma = orc_dot(N, rtilde, v);
+    if (sigma == 0.0) { it_fail(it, 1); break; }
+    alpha = rho / sigma;
+    orc_copy(N, y1, y0);
+    orc_axpy(N, -alpha, v, y0);
+    orc_copy(N, y0, h);
+    csr_mlt(A, h, tmp);
+    prec_solve(M, A, tmp, h);
+    /* first half step (m = 2k - 1) */
+    orc_axpy(N, -alpha, g, w);
+    if (alpha == 0.0) { it_fail(it, 2); break; }
+    orc_scal(N, theta * theta * eta / alpha, d);
+    orc_axpy(N, 1.0, y1, d);
+    if (tau == 0.0) { it_fail(it, 3); break; }
+    theta = orc_nrm2(N, w) / tau;
+    c = 1.0 / sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    orc_axpy(N, eta, d, x);
+    kappa = tau * sqrt(2. * (it->nb_iter + 1));
+    if (it_finished(it, kappa)) break;
+    it->nb_iter++;
+    /* second half step (m = 2k) */
+    orc_copy(N, h, g);
+    orc_axpy(N, -alpha, g, w);
+    orc_scal(N, theta * theta * eta / alpha, d);
+    orc_axpy(N, 1.0, y0, d);
+    if (tau == 0.0) { it_fail(it, 4); break; }
+    theta = orc_nrm2(N, w) / tau;
+    c = 1.0 / sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    orc_axpy(N, eta, d, x);
+    kappa = tau * sqrt(2. * (it->nb_iter + 1) + 1.);
+    if (it_finished(it, kappa)) break;
+    /* 22.-26. */
+    rho0 = rho;
+    rho = orc_dot(N, rtilde, w);
+    if (rho0 == 0.0) { it_fail(it, 5); break; }
+    beta = rho / rho0;
+    orc_copy(N, w, y1);
+    orc_axpy(N, beta, y0, y1);
+    orc_copy(N, y1, g);
+    csr_mlt(A, g, tmp);
+    prec_solve(M, A, tmp, g);
+    orc_scal(N, beta * beta, v);
+    orc_axpy(N, beta, h, v);
+    orc_axpy(N, 1.0, g, v);
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 10; k++) free(all[k]);
+  return code;
+}
+
+/* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -570,6 +731,10 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_cg_impl(&A, x, b, &M, &it);
   else if (which == 1)
     code = orc_bicgstab_impl(&A, x, b, &M, &it);
+  else if (which == 3)
+    code = orc_cgs_impl(&A, x, b, &M, &it);
+  else if (which == 4)
+    code = orc_tfqmr_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

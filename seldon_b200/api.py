@@ -927,6 +927,19 @@ def BiCgStab(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_bicgstab, A, x, b, M, iteration, hist_cap, stream)
 
 
+def Cgs(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Conjugate gradient squared (Cgs.cxx:45-132), right preconditioned;
+    returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_cgs, A, x, b, M, iteration, hist_cap, stream)
+
+
+def TfQmr(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Transpose-free QMR (TfQmr.cxx:44-243), left preconditioned; the
+    stopping test is on the quasi-residual bound; returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_tfqmr, A, x, b, M, iteration, hist_cap, stream)
+
+
 def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None, orthogonalization="mgs"):
     """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183).
 

@@ -8,12 +8,14 @@
 // vector updates with the next residual norm; grid-wide reductions are
 // deterministic (fixed CTA order).
 //
-// SOR preconditioning (level-scheduled sweeps, many dependent launches) goes
-// through a host-driven driver over the same device kernels, one operation at
-// a time, in the reference's order.
+// SOR and ILUT preconditioning (level-scheduled sweeps, many dependent
+// launches) of Cg, BiCgStab and Gmres run as device-resident chains around the
+// sweeps (chain.cu); Cgs and TfQmr with them, and every driver when those
+// chains are switched off, go through a host-driven driver over the same
+// device kernels, one operation at a time, in the reference's order.
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
-// Iterative.cxx:235-354.
+// Cgs.cxx:45-132, TfQmr.cxx:44-243, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -410,6 +412,412 @@ __global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVec
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- CGS
+
+struct CgsVecs {
+  const double* b;
+  double *x, *r, *rt, *u, *p, *ph, *q, *vh, *uh;
+};
+
+// epilogue of qhat = A uhat: Add(-alpha, qhat, r), then ||r||^2 and
+// (rtilde, r) for the next test and rho (qhat itself is not kept)
+struct EpiResidUpdate {
+  double* r;
+  const double* rt;
+  double malpha;
+  double rr, rtr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    double ri = __ldcg(r + i);
+    if (malpha != 0.0) {
+      ri = add_rn(ri, mul_rn(malpha, t));
+      r[i] = ri;
+    }
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rtr = add_rn(rtr, mul_rn(__ldcg(rt + i), ri));
+  }
+};
+
+// Cgs (Cgs.cxx:45-132): four grid barriers per loop, two products; the
+// second product is fused with the residual update and both reductions.
+__global__ void __launch_bounds__(NT, 4) cgs_fused_kernel(OpArgs A, CgsVecs v, IterArgs it,
+                                                       Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b); rtilde = r; ||r||^2 (= (rtilde, r))
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      v.x[i] = 0.0;
+      v.r[i] = bi;
+      v.rt[i] = bi;
+      rr = add_rn(rr, mul_rn(bi, bi));
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    for (long long i = gt; i < n; i += gs) v.rt[i] = __ldcg(v.r + i);
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double rho_1 = rr, rho_2 = 0.0;
+  const bool jac = (A.diag != nullptr);
+  double* ph = jac ? v.ph : v.p;  // identity: phat aliases p, uhat aliases u
+  double* uh = jac ? v.uh : v.u;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho_1 == 0.0) { fail = 1; break; }
+    {
+      const double* __restrict__ rp = v.r;
+      const double* __restrict__ qp = v.q;
+      double* __restrict__ up = v.u;
+      double* __restrict__ pp = v.p;
+      double* __restrict__ php = ph;
+      if (nb_iter == 0) {
+        // Copy(r, u); Copy(u, p); phat = M^{-1} p
+#pragma unroll 4
+        for (long long i = gt; i < n; i += gs) {
+          const double ri = __ldcg(rp + i);
+          up[i] = ri;
+          pp[i] = ri;
+          if (jac) php[i] = precond_val(A.diag, (int)i, ri);
+        }
+      } else {
+        // Copy(r, u); Add(beta, q, u); Mlt(beta, p); Add(1, q, p); Mlt(beta, p);
+        // Add(1, u, p); phat = M^{-1} p
+        const double beta = rho_1 / rho_2;
+#pragma unroll 4
+        for (long long i = gt; i < n; i += gs) {
+          const double qi = __ldcg(qp + i);
+          double ui = __ldcg(rp + i);
+          if (beta != 0.0) ui = add_rn(ui, mul_rn(beta, qi));
+          up[i] = ui;
+          double pi = add_rn(mul_rn(__ldcg(pp + i), beta), qi);
+          pi = add_rn(mul_rn(pi, beta), ui);
+          pp[i] = pi;
+          if (jac) php[i] = precond_val(A.diag, (int)i, pi);
+        }
+      }
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // vhat = A phat fused with delta = (rtilde, vhat)
+    EpiStoreDot e1{v.vh, v.rt, 0.0};
+    spmv_phase(A, ph, e1, s_prod, s_red);
+    const double d = block_sum<NT>(e1.acc, s_red);
+    if (tid == 0) s_vals[0] = d;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    nb_iter++;
+    const double delta = s_vals[0];
+    if (delta == 0.0) { fail = 2; break; }
+    const double alpha = rho_1 / delta;
+    // Copy(u, q); Add(-alpha, vhat, q); Add(1, q, u); uhat = M^{-1} u;
+    // Add(alpha, uhat, x)
+    {
+      double* __restrict__ up = v.u;
+      double* __restrict__ qp = v.q;
+      double* __restrict__ xp = v.x;
+      double* __restrict__ uhp = uh;
+      const double* __restrict__ vhp = v.vh;
+#pragma unroll 4
+      for (long long i = gt; i < n; i += gs) {
+        double ui = __ldcg(up + i);
+        double qi = ui;
+        if (-alpha != 0.0) qi = add_rn(qi, mul_rn(-alpha, __ldcg(vhp + i)));
+        qp[i] = qi;
+        ui = add_rn(ui, qi);
+        up[i] = ui;
+        const double uhi = jac ? precond_val(A.diag, (int)i, ui) : ui;
+        if (jac) uhp[i] = uhi;
+        if (alpha != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(alpha, uhi));
+      }
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // qhat = A uhat fused with Add(-alpha, qhat, r), ||r||^2 and (rtilde, r)
+    EpiResidUpdate e2{v.r, v.rt, -alpha, 0.0, 0.0};
+    spmv_phase(A, uh, e2, s_prod, s_red);
+    rr = block_sum<NT>(e2.rr, s_red);
+    const double rtr = block_sum<NT>(e2.rtr, s_red);
+    if (tid == 0) { s_vals[0] = rr; s_vals[1] = rtr; }
+    if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    rr = s_vals[0];
+    rho_2 = rho_1;
+    rho_1 = s_vals[1];
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
+// ----------------------------------------------------------------- TFQMR
+
+struct TfqmrVecs {
+  const double* b;
+  double *x, *rt, *w, *y1, *y0, *v, *g, *h, *d;
+};
+
+// epilogue of the initial residual: r0 = M^{-1}(b - A x); w = y1 = rtilde =
+// r0; d = 0; accumulate ||r0||^2
+struct EpiTfqmrInit {
+  const double* b;
+  const double* diag;
+  double *w, *y1, *rt, *d;
+  double rr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double r0 = precond_val(diag, i, add_rn(__ldg(b + i), -t));
+    w[i] = r0;
+    y1[i] = r0;
+    rt[i] = r0;
+    d[i] = 0.0;
+    rr = add_rn(rr, mul_rn(r0, r0));
+  }
+};
+
+// epilogue of v = M^{-1} A y1 at the start: g = v; accumulate (rtilde, v)
+struct EpiTfqmrFirstV {
+  const double* diag;
+  const double* rt;
+  double *v, *g;
+  double sigma;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double vi = precond_val(diag, i, t);
+    v[i] = vi;
+    g[i] = vi;
+    sigma = add_rn(sigma, mul_rn(__ldcg(rt + i), vi));
+  }
+};
+
+// epilogue of h = M^{-1} A y0 (the end of the first half step and the start
+// of the second): Add(eta, d, x); Copy(h, g) is implied (g is overwritten
+// before its next read, so h is read in its place); Add(-alpha, h, w);
+// Mlt(c1, d); Add(1, y0, d); accumulate ||w||^2 and (rtilde, w)
+struct EpiTfqmrHalf {
+  const double* diag;
+  const double *rt, *y0;
+  double *h, *x, *w, *d;
+  double eta, malpha, c1;
+  double ww, rtw;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double hi = precond_val(diag, i, t);
+    h[i] = hi;
+    double di = __ldcg(d + i);
+    if (eta != 0.0) x[i] = add_rn(__ldcg(x + i), mul_rn(eta, di));
+    double wi = __ldcg(w + i);
+    if (malpha != 0.0) {
+      wi = add_rn(wi, mul_rn(malpha, hi));
+      w[i] = wi;
+    }
+    d[i] = add_rn(mul_rn(di, c1), __ldcg(y0 + i));
+    ww = add_rn(ww, mul_rn(wi, wi));
+    rtw = add_rn(rtw, mul_rn(__ldcg(rt + i), wi));
+  }
+};
+
+// epilogue of g = M^{-1} A y1: Mlt(beta^2, v); Add(beta, h, v); Add(1, g, v);
+// accumulate (rtilde, v) for the next loop's sigma
+struct EpiTfqmrNextV {
+  const double* diag;
+  const double *rt, *h;
+  double *g, *v;
+  double beta, bb;
+  double sigma;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double gi = precond_val(diag, i, t);
+    g[i] = gi;
+    double vi = mul_rn(__ldcg(v + i), bb);
+    if (beta != 0.0) vi = add_rn(vi, mul_rn(beta, __ldcg(h + i)));
+    vi = add_rn(vi, gi);
+    v[i] = vi;
+    sigma = add_rn(sigma, mul_rn(__ldcg(rt + i), vi));
+  }
+};
+
+// TfQmr (TfQmr.cxx:44-243), left preconditioned: four grid barriers and two
+// products per loop of two half steps.  The vector work of each half step
+// rides in the epilogue of the product that follows it.
+__global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs v, IterArgs it,
+                                                         Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  // 1.-2. r0 = M^{-1}(b - A x) (or x = 0); w = y1 = rtilde = r0; d = 0
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      const double r0 = precond_val(A.diag, (int)i, __ldg(v.b + i));
+      v.w[i] = r0;
+      v.y1[i] = r0;
+      v.rt[i] = r0;
+      v.d[i] = 0.0;
+      rr = add_rn(rr, mul_rn(r0, r0));
+    }
+  } else {
+    EpiTfqmrInit epi{v.b, A.diag, v.w, v.y1, v.rt, v.d, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  // iter.Init(r0); tau = Norm2(r0); rho = (rtilde, r0) with rtilde = r0
+  const double tau0 = sqrt(s_vals[0]);
+  if (tau0 == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / tau0;
+  double tau = tau0, rho = s_vals[0], theta = 0.0, eta = 0.0;
+  // 3. g = v = M^{-1} A y1, with the first sigma = (rtilde, v)
+  {
+    EpiTfqmrFirstV epi{A.diag, v.rt, v.v, v.g, 0.0};
+    spmv_phase(A, v.y1, epi, s_prod, s_red);
+    const double sg = block_sum<NT>(epi.sigma, s_red);
+    if (tid == 0) s_vals[0] = sg;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  }
+  double sigma = s_vals[0];
+
+  int nb_iter = 0, fail = 0;
+  double reste = 0.0;
+  bool done = false;
+  for (;;) {
+    // 9.-11. alpha = rho / sigma; y0 = y1 - alpha v; the breakdown tests of
+    // the first half step come before any vector that outlives the loop
+    if (sigma == 0.0) { fail = 1; break; }
+    const double alpha = rho / sigma;
+    if (alpha == 0.0) { fail = 2; break; }
+    if (tau == 0.0) { fail = 3; break; }
+    // first half: Add(-alpha, g, w); Mlt(theta^2 eta / alpha, d); Add(1, y1, d)
+    {
+      const double c1 = theta * theta * eta / alpha;
+      const double* __restrict__ y1p = v.y1;
+      const double* __restrict__ vp = v.v;
+      const double* __restrict__ gp = v.g;
+      double* __restrict__ y0p = v.y0;
+      double* __restrict__ wp = v.w;
+      double* __restrict__ dp = v.d;
+      double ww = 0.0;
+#pragma unroll 4
+      for (long long i = gt; i < n; i += gs) {
+        const double y1i = __ldcg(y1p + i);
+        y0p[i] = add_rn(y1i, mul_rn(-alpha, __ldcg(vp + i)));
+        const double wi = add_rn(__ldcg(wp + i), mul_rn(-alpha, __ldcg(gp + i)));
+        wp[i] = wi;
+        dp[i] = add_rn(mul_rn(__ldcg(dp + i), c1), y1i);
+        ww = add_rn(ww, mul_rn(wi, wi));
+      }
+      ww = block_sum<NT>(ww, s_red);
+      if (tid == 0) s_vals[0] = ww;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    // 14.-21. theta, c, tau, eta; x += eta d; Finished(kappa)
+    theta = sqrt(s_vals[0]) / tau;
+    double c = 1.0 / sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    double kappa = tau * sqrt(2. * (nb_iter + 1));
+    reste = facteur * kappa;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) {
+      if (eta != 0.0)
+        for (long long i = gt; i < n; i += gs)
+          v.x[i] = add_rn(__ldcg(v.x + i), mul_rn(eta, __ldcg(v.d + i)));
+      break;
+    }
+    nb_iter++;
+    // h = M^{-1} A y0 with the first half's x update and the second half's
+    // w and d updates
+    {
+      EpiTfqmrHalf epi{A.diag, v.rt, v.y0, v.h, v.x, v.w, v.d,
+                        eta, -alpha, theta * theta * eta / alpha, 0.0, 0.0};
+      spmv_phase(A, v.y0, epi, s_prod, s_red);
+      const double ww = block_sum<NT>(epi.ww, s_red);
+      const double rtw = block_sum<NT>(epi.rtw, s_red);
+      if (tid == 0) { s_vals[0] = ww; s_vals[1] = rtw; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    }
+    if (tau == 0.0) { fail = 4; break; }
+    theta = sqrt(s_vals[0]) / tau;
+    c = 1.0 / sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    kappa = tau * sqrt(2. * (nb_iter + 1) + 1.);
+    reste = facteur * kappa;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    const double rho0 = rho;
+    rho = s_vals[1];
+    // Add(eta, d, x) comes before the test and the last breakdown
+    done = (reste < it.tol || nb_iter >= it.max_iter);
+    if (!done && rho0 == 0.0) fail = 5;
+    const double beta = (done || fail) ? 0.0 : rho / rho0;
+    // x += eta d; 24. y1 = w + beta y0
+    {
+      double* __restrict__ xp = v.x;
+      double* __restrict__ y1p = v.y1;
+      const double* __restrict__ dp = v.d;
+      const double* __restrict__ wp = v.w;
+      const double* __restrict__ y0p = v.y0;
+      const bool next = !done && !fail;
+#pragma unroll 4
+      for (long long i = gt; i < n; i += gs) {
+        if (eta != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(eta, __ldcg(dp + i)));
+        if (next) {
+          double yi = __ldcg(wp + i);
+          if (beta != 0.0) yi = add_rn(yi, mul_rn(beta, __ldcg(y0p + i)));
+          y1p[i] = yi;
+        }
+      }
+    }
+    if (done || fail) break;
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // 25.-26. g = M^{-1} A y1; v = beta^2 v + beta h + g; next sigma
+    {
+      EpiTfqmrNextV epi{A.diag, v.rt, v.h, v.g, v.v, beta, beta * beta, 0.0};
+      spmv_phase(A, v.y1, epi, s_prod, s_red);
+      const double sg = block_sum<NT>(epi.sigma, s_red);
+      if (tid == 0) s_vals[0] = sg;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    sigma = s_vals[0];
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -703,7 +1111,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
                 sell_op(f)};
 }
 
-enum Solver { kCg = 0, kBicg = 1, kGmres = 2 };
+enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
@@ -715,6 +1123,8 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   int nvec = 0;
   if (which == kCg) { kern = (const void*)cg_fused_kernel; nvec = 3; }
   if (which == kBicg) { kern = (const void*)bicgstab_fused_kernel; nvec = 9; }
+  if (which == kCgs) { kern = (const void*)cgs_fused_kernel; nvec = 8; }
+  if (which == kTfqmr) { kern = (const void*)tfqmr_fused_kernel; nvec = 8; }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -740,6 +1150,8 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   CgVecs cv;
   BicgVecs bv;
   GmresVecs gv;
+  CgsVecs sv;
+  TfqmrVecs tv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -752,6 +1164,14 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     bv = BicgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                   V + 7 * nn};
     args[1] = &bv;
+  } else if (which == kCgs) {
+    sv = CgsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                 V + 7 * nn};
+    args[1] = &sv;
+  } else if (which == kTfqmr) {
+    tv = TfqmrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                   V + 7 * nn};
+    args[1] = &tv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -884,6 +1304,127 @@ static int host_bicgstab(Ops& o, double* x, const double* b, const sb2_iter_para
   return SB2_OK;
 }
 
+static int host_cgs(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                    HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *p = V, *phat = V + n, *q = V + 2 * n, *qhat = V + 3 * n, *vhat = V + 4 * n,
+         *u = V + 5 * n, *uhat = V + 6 * n, *r = V + 7 * n, *rt = V + 8 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.copy(r, rt));
+  double rho_1, rho_2 = 0.0, res;
+  for (;;) {
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    SB2_TRY(o.dot(rt, r, &rho_1));
+    if (rho_1 == 0.0) { it.fail = 1; break; }
+    if (it.nb_iter == 0) {
+      SB2_TRY(o.copy(r, u));
+      SB2_TRY(o.copy(u, p));
+    } else {
+      const double beta = rho_1 / rho_2;
+      SB2_TRY(o.copy(r, u));
+      SB2_TRY(o.axpy(beta, q, u));
+      SB2_TRY(o.scal(beta, p));
+      SB2_TRY(o.axpy(1.0, q, p));
+      SB2_TRY(o.scal(beta, p));
+      SB2_TRY(o.axpy(1.0, u, p));
+    }
+    SB2_TRY(o.prec(p, phat));
+    SB2_TRY(o.mlt(phat, vhat));
+    it.nb_iter++;
+    double delta;
+    SB2_TRY(o.dot(rt, vhat, &delta));
+    if (delta == 0.0) { it.fail = 2; break; }
+    const double alpha = rho_1 / delta;
+    SB2_TRY(o.copy(u, q));
+    SB2_TRY(o.axpy(-alpha, vhat, q));
+    SB2_TRY(o.axpy(1.0, q, u));
+    SB2_TRY(o.prec(u, uhat));
+    SB2_TRY(o.axpy(alpha, uhat, x));
+    SB2_TRY(o.mlt(uhat, qhat));
+    SB2_TRY(o.axpy(-alpha, qhat, r));
+    rho_2 = rho_1;
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
+static int host_tfqmr(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                      HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *tmp = V, *r0 = V + n, *v = V + 2 * n, *h = V + 3 * n, *w = V + 4 * n,
+         *y1 = V + 5 * n, *g = V + 6 * n, *y0 = V + 7 * n, *rt = V + 8 * n, *d = V + 9 * n;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, tmp));
+  else { SB2_TRY(o.copy(b, tmp)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.prec(tmp, r0));
+  double tau;
+  SB2_TRY(o.nrm(r0, &tau));
+  if (tau == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / tau;
+  SB2_TRY(o.copy(r0, w));
+  SB2_TRY(o.copy(r0, y1));
+  SB2_TRY(o.mlt(y1, tmp));
+  SB2_TRY(o.prec(tmp, v));
+  SB2_TRY(o.copy(v, g));
+  SB2_TRY(sb2_fill(o.n, 0.0, d, o.s));
+  SB2_TRY(o.copy(r0, rt));
+  double rho, sigma, theta = 0.0, eta = 0.0;
+  SB2_TRY(o.dot(rt, r0, &rho));
+  for (;;) {
+    SB2_TRY(o.dot(rt, v, &sigma));
+    if (sigma == 0.0) { it.fail = 1; break; }
+    const double alpha = rho / sigma;
+    SB2_TRY(o.copy(y1, y0));
+    SB2_TRY(o.axpy(-alpha, v, y0));
+    SB2_TRY(o.mlt(y0, tmp));
+    SB2_TRY(o.prec(tmp, h));
+    SB2_TRY(o.axpy(-alpha, g, w));
+    if (alpha == 0.0) { it.fail = 2; break; }
+    SB2_TRY(o.scal(theta * theta * eta / alpha, d));
+    SB2_TRY(o.axpy(1.0, y1, d));
+    if (tau == 0.0) { it.fail = 3; break; }
+    double nw;
+    SB2_TRY(o.nrm(w, &nw));
+    theta = nw / tau;
+    double c = 1.0 / std::sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    SB2_TRY(o.axpy(eta, d, x));
+    if (it.finished(tau * std::sqrt(2. * (it.nb_iter + 1)))) break;
+    it.nb_iter++;
+    SB2_TRY(o.copy(h, g));
+    SB2_TRY(o.axpy(-alpha, g, w));
+    SB2_TRY(o.scal(theta * theta * eta / alpha, d));
+    SB2_TRY(o.axpy(1.0, y0, d));
+    if (tau == 0.0) { it.fail = 4; break; }
+    SB2_TRY(o.nrm(w, &nw));
+    theta = nw / tau;
+    c = 1.0 / std::sqrt(1.0 + theta * theta);
+    tau = tau * c * theta;
+    eta = c * c * alpha;
+    SB2_TRY(o.axpy(eta, d, x));
+    if (it.finished(tau * std::sqrt(2. * (it.nb_iter + 1) + 1.))) break;
+    const double rho0 = rho;
+    SB2_TRY(o.dot(rt, w, &rho));
+    if (rho0 == 0.0) { it.fail = 5; break; }
+    const double beta = rho / rho0;
+    SB2_TRY(o.copy(w, y1));
+    SB2_TRY(o.axpy(beta, y0, y1));
+    SB2_TRY(o.mlt(y1, tmp));
+    SB2_TRY(o.prec(tmp, g));
+    SB2_TRY(o.scal(beta * beta, v));
+    SB2_TRY(o.axpy(beta, h, v));
+    SB2_TRY(o.axpy(1.0, g, v));
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -985,7 +1526,11 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                       double* hist, int* hist_it, int hist_cap, cudaStream_t s) {
   const int n = A->m;
   const int m = std::max(prm->restart, 1);
-  const int nvec = which == kCg ? 4 : (which == kBicg ? 8 : 3 + m + 1);
+  const int nvec = which == kCg ? 4
+                   : which == kBicg ? 8
+                   : which == kCgs ? 9
+                   : which == kTfqmr ? 10
+                                     : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
   SB2_CUDA_TRY(pool_malloc((void**)&buf.p, sizeof(double) * (size_t)std::max(n, 1) * nvec, s));
@@ -997,6 +1542,8 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   double* V = (double*)buf.p;
   if (which == kCg) SB2_TRY(host_cg(o, x, b, prm, it, V, &init_failed));
   else if (which == kBicg) SB2_TRY(host_bicgstab(o, x, b, prm, it, V, &init_failed));
+  else if (which == kCgs) SB2_TRY(host_cgs(o, x, b, prm, it, V, &init_failed));
+  else if (which == kTfqmr) SB2_TRY(host_tfqmr(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -1430,7 +1977,7 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
     return SB2_ERR_INVALID_VALUE;
   }
   if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && A->full.sell.nslice >= 0 &&
-      g_pcg_device)
+      g_pcg_device && which <= kGmres)
     return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which);
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
@@ -1507,6 +2054,22 @@ int sb2_gmres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b
               int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_gmres");
   return solve_entry(kGmres, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_cgs(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+            const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,
+            int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_cgs");
+  return solve_entry(kCgs, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_tfqmr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+              int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_tfqmr");
+  return solve_entry(kTfqmr, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

@@ -1,0 +1,194 @@
+"""Cgs (Cgs.cxx:45-132) and TfQmr (TfQmr.cxx:44-243) on the device against
+the oracle's restatements, which are pinned bit for bit to the reference's
+own templates (tests/test_oracle_pin.py).
+
+The identity and Jacobi run the persistent kernels; SOR and ILUT the
+host-driven loop over the device operations.  Reductions are summed in
+another order than Seldon's sequential loops, so the bar is the one the other
+drivers meet: same error code, iteration count within a few percent, both
+solutions meeting the stopping rule and agreeing to what the tolerance
+implies.  Edge cases (breakdowns, limits, zero and exact guesses, non-finite
+inputs) must give the oracle's code and count exactly."""
+import numpy as np
+import pytest
+
+from seldon_b200 import matgen
+from tests.helpers import to_dev, to_host
+from tests.test_oracle_pin import _edge_solves, _nonfinite_cases
+
+pytestmark = pytest.mark.gpu
+
+SOLVERS = ["cgs", "tfqmr"]
+
+
+@pytest.fixture(scope="module")
+def api(cuda):
+    from seldon_b200 import api
+    return api
+
+
+def _fn(api, which):
+    return {"cgs": api.Cgs, "tfqmr": api.TfQmr}[which]
+
+
+def _precond(api, pc):
+    if pc == 0:
+        return api.Preconditioner_Base()
+    if pc == 1:
+        return api.JacobiPreconditioner()
+    S = api.SorPreconditioner()
+    S.SetParameterRelaxation(1.2)
+    return S
+
+
+def _matrix(api, A, sym):
+    n = A[0].size - 1
+    return api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
+
+
+def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000):
+    n = A[0].size - 1
+    M = _matrix(api, A, sym)
+    X = to_dev(np.zeros(n) if x0 is None else x0)
+    it = api.Iteration(max_iter, tol)
+    it.HideMessages()
+    if x0 is not None:
+        it.SetInitGuess(False)
+    code = _fn(api, which)(M, X, to_dev(b), _precond(api, pc), it)
+    return code, it, to_host(X)
+
+
+CASES = [(w, m, pc) for w in SOLVERS for m in ("conv", "lap", "lap_up") for pc in (0, 1, 2)]
+
+
+@pytest.mark.parametrize("which,mname,pc", CASES)
+def test_parity(api, oracle, which, mname, pc):
+    full = matgen.convdiff3d(9) if mname == "conv" else matgen.lap2d(30)
+    sym = mname == "lap_up"
+    A = matgen.upper(*full) if sym else full
+    n = A[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(3).uniform(-1, 1, n))
+    tol = 1e-10
+    xo, co, no, ho, hio = oracle.solve(which, *A, b, sym=sym, precond=pc, omega=1.2, tol=tol,
+                                       max_iter=2000, hist_cap=10000)
+    code, it, x = _solve(api, which, A, sym, b, pc, tol=tol)
+    assert code == co == 0
+    nb = it.GetNumberIteration()
+    assert abs(nb - no) <= max(2, int(0.05 * no)), (nb, no)
+    for xx in (x, xo):
+        r = b - matgen.matvec(*full, xx)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 100 * tol
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+    # the history: Finished() at the oracle's iteration numbers, the same
+    # first relative residual, the last one below tol
+    its = [i for i, _ in it.history]
+    k = min(len(its), len(hio)) - 2
+    assert its[:k] == hio[:k].tolist()
+    h = np.array([r for _, r in it.history])
+    assert h[0] == pytest.approx(ho[0], rel=1e-12)
+    assert h[-1] < tol
+
+
+@pytest.mark.parametrize("which", SOLVERS)
+def test_initial_guess(api, oracle, which):
+    full = matgen.convdiff3d(8)
+    n = full[0].size - 1
+    rng = np.random.default_rng(9)
+    b = matgen.matvec(*full, rng.uniform(-1, 1, n))
+    x0 = rng.uniform(-1, 1, n)
+    for pc in (0, 1):
+        xo, co, no, _, _ = oracle.solve(which, *full, b, x0=x0, precond=pc, tol=1e-10,
+                                        max_iter=2000)
+        code, it, x = _solve(api, which, full, False, b, pc, x0=x0)
+        assert code == co == 0
+        assert abs(it.GetNumberIteration() - no) <= max(2, int(0.05 * no))
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+
+
+@pytest.mark.parametrize("which", SOLVERS)
+def test_edges(api, oracle, which):
+    for name, (p, i, v), b, x0, kw in _edge_solves():
+        for pc in (0, 1, 2):
+            xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, omega=1.2,
+                                            **kw)
+            code, it, x = _solve(api, which, (p, i, v), False, b, pc, x0=x0,
+                                 tol=kw.get("tol", 1e-6), max_iter=kw.get("max_iter", 100))
+            nb = it.GetNumberIteration()
+            assert code == co, (name, pc, code, co)
+            if name == "zero_b" and no > 0:
+                # TfQmr's Init sees r0 = -M^{-1} A x0, not b: an iterative
+                # solve of A x = 0 from x0, counts within the slack (Cgs's
+                # Init sees b = 0 and leaves x0 untouched, compared below)
+                assert abs(nb - no) <= 2, (name, pc, nb, no)
+                assert np.linalg.norm(x) < 1e-5
+                continue
+            assert nb == no, (name, pc, nb, no)
+            scale = max(np.linalg.norm(xo), 1e-300)
+            assert np.linalg.norm(x - xo) / scale < 1e-12, (name, pc)
+
+
+@pytest.mark.parametrize("which", SOLVERS)
+def test_nonfinite(api, oracle, which):
+    for name, (p, i, v, b, x0) in _nonfinite_cases().items():
+        for pc in (0, 1, 2):
+            xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, omega=1.2,
+                                            tol=1e-10, max_iter=25)
+            code, it, x = _solve(api, which, (p, i, v), False, b, pc, x0=x0, tol=1e-10,
+                                 max_iter=25)
+            assert (code, it.GetNumberIteration()) == (co, no), (name, pc)
+            assert np.array_equal(np.isnan(x), np.isnan(xo)), (name, pc)
+
+
+@pytest.mark.parametrize("which", SOLVERS)
+def test_deterministic_and_larger(api, oracle, which):
+    # 64,000 rows: a grid of many CTAs, every product in the binned layout
+    full = matgen.convdiff3d(40)
+    n = full[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(1).uniform(-1, 1, n))
+    outs = [_solve(api, which, full, False, b, 1) for _ in range(2)]
+    assert outs[0][0] == outs[1][0] == 0
+    assert outs[0][1].GetNumberIteration() == outs[1][1].GetNumberIteration()
+    assert np.array_equal(outs[0][2], outs[1][2])
+    xo, co, no, _, _ = oracle.solve(which, *full, b, precond=1, tol=1e-10, max_iter=2000)
+    assert co == 0
+    assert abs(outs[0][1].GetNumberIteration() - no) <= max(2, int(0.05 * no))
+    assert np.linalg.norm(outs[0][2] - xo) / np.linalg.norm(xo) < 1e-7
+
+
+@pytest.mark.parametrize("which", SOLVERS)
+def test_ilut(api, reference, which):
+    # the host-driven loop with the device ILUT apply against the reference's
+    # driver with its own factor
+    ptr, ind, val = matgen.convdiff3d(12)
+    n = ptr.size - 1
+    S = api.RowSparse(n, n, ptr, ind, val)
+    M = api.IlutPreconditioning()
+    M.SetDroppingThreshold(1e-2)
+    M.FactorizeMatrix(S)
+    b = matgen.matvec(ptr, ind, val, np.random.default_rng(5).uniform(-1, 1, n))
+    X = to_dev(np.zeros(n))
+    it = api.Iteration(2000, 1e-10)
+    it.HideMessages()
+    code = _fn(api, which)(S, X, to_dev(b), M, it)
+    reference.ilut_factor(ptr, ind, val, droptol=1e-2)
+    xr, cr, nr = reference.solve_ilut(which, ptr, ind, val, b, tol=1e-10, max_iter=2000)
+    assert code == cr == 0
+    assert abs(it.GetNumberIteration() - nr) <= max(2, int(0.05 * nr))
+    x = to_host(X)
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-7
+
+
+def test_breakdowns(api, oracle):
+    # diag(1, -1) with b = (1, 1): Cgs's (rtilde, A phat) and TfQmr's
+    # (rtilde, v) vanish exactly
+    ptr, ind, val = np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, -1.0])
+    A = api.RowSparse(2, 2, ptr, ind, val)
+    for which in SOLVERS:
+        it = api.Iteration(10, 1e-12)
+        it.HideMessages()
+        X = to_dev(np.zeros(2))
+        b = np.array([1.0, 1.0])
+        code = _fn(api, which)(A, X, to_dev(b), api.Preconditioner_Base(), it)
+        _, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, tol=1e-12, max_iter=10)
+        assert (code, it.GetNumberIteration()) == (co, no)
+        assert code == (2 if which == "cgs" else 1)

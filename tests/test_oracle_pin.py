@@ -99,7 +99,7 @@ def test_mltadd_live(reference, oracle, seed):
                           reference.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True))
 
 
-@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres"])
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
     ptr, ind, val = matgen.convdiff3d(5) if which != "cg" else matgen.lap2d(15)
@@ -137,6 +137,38 @@ def test_breakdown_and_edge_codes(reference, oracle):
     xo, co, no, _, _ = oracle.solve("cg", ptr, ind, val, b)
     xr, cr, nr = reference.solve("cg", ptr, ind, val, b)
     assert co == cr == 2
+
+
+def _edge_solves():
+    """Small cases on the edges of Cgs and TfQmr: a zero right-hand side with
+    a nonzero guess, an exact guess (TfQmr's Init sees a zero preconditioned
+    residual), iteration limits 0 to 3, and the indefinite 2 x 2 system whose
+    first projections vanish."""
+    ptr, ind, val = matgen.lap2d(4)
+    n = 16
+    rng = np.random.default_rng(5)
+    xs = rng.uniform(-1, 1, n)
+    b = matgen.matvec(ptr, ind, val, xs)
+    out = [("zero_b", (ptr, ind, val), np.zeros(n), np.arange(16.0), {}),
+           ("exact_x0", (ptr, ind, val), b, xs, {})]
+    for k in range(4):
+        out.append((f"max_iter_{k}", (ptr, ind, val), b, None, {"tol": 1e-30, "max_iter": k}))
+    ind2 = np.array([0, 1], dtype=np.int32)
+    out.append(("indefinite", (np.array([0, 1, 2], dtype=np.int32), ind2,
+                               np.array([1.0, -1.0])), np.array([1.0, 1.0]), None, {}))
+    out.append(("one_by_one", (np.array([0, 1], dtype=np.int32), ind2[:1], np.array([4.0])),
+                np.array([2.0]), None, {}))
+    return out
+
+
+@pytest.mark.parametrize("which", ["cgs", "tfqmr"])
+def test_cgs_tfqmr_edges_live(reference, oracle, which):
+    for name, (p, i, v), b, x0, kw in _edge_solves():
+        for pc in (0, 1, 2):
+            xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, **kw)
+            xr, cr, nr = reference.solve(which, p, i, v, b, x0=x0, precond=pc, **kw)
+            assert (co, no) == (cr, nr), (name, pc)
+            assert np.array_equal(xo, xr, equal_nan=True), (name, pc)
 
 
 COO_CASES = ["gen_dup_i1", "gen_min", "sym_both", "sym_i1_min", "empty_gen", "empty_sym"]
@@ -250,4 +282,14 @@ def test_nonfinite_inputs_live(oracle, reference, name):
             xr, cr, nr = reference.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                          max_iter=25, restart=5)
             assert (co, no) == (cr, nr) == (-2, 25)
+            assert np.array_equal(xo, xr, equal_nan=True)
+    # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
+    # product: the codes and counts are the reference's, whatever they are
+    for which in ("cgs", "tfqmr"):
+        for pc in (0, 1, 2):
+            xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
+                                            max_iter=25)
+            xr, cr, nr = reference.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
+                                         max_iter=25)
+            assert (co, no) == (cr, nr)
             assert np.array_equal(xo, xr, equal_nan=True)
