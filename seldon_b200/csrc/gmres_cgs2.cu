@@ -139,6 +139,7 @@ __device__ __forceinline__ bool grid_sync_wide(const Persist& P, double* wide, u
       }
       __nanosleep(32);
     }
+    __threadfence();  // as grid_sync: the next phase gathers through L1
   }
   // thread 0's acquire, then the CTA barrier, orders every thread's reads
   // of the published sums after the release
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(NTG, 3)
       vv = f.vv;
     } else {
       EpiResidualCgs2<VT> e{a.b, a.diag64, a.u, 0.0, 0.0};
-      XLoadCg<double> xl{a.x};
+      XLoadCa<double> xl{a.x};
       sell_spmv<NTG, double, double>(a.A64, xl, e, s_red, blockIdx.x, gridDim.x);
       zz = e.zz;
       vv = e.vv;
@@ -555,7 +556,7 @@ __global__ void __launch_bounds__(NTG, 3)
         const bool prod = i < m;
         if (prod) {
           EpiPrecond<VT> e{a.w, a.diag_in};
-          XLoadCg<VT> xl{a.u};
+          XLoadCa<VT> xl{a.u};
           sell_spmv<NTG, VT, VT>(a.Ain, xl, e, s_redv, blockIdx.x, gridDim.x);
           delayed_dots<VT, true>(a, i, s_part, s_vals);
         } else {

@@ -19,6 +19,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <vector>
 
@@ -64,6 +65,73 @@ __device__ __forceinline__ double precond_val(const double* diag, int i, double 
   return diag ? __ddiv_rn(r, diag[i]) : r;  // Jacobi z_i = r_i / A(i,i)
 }
 
+// W consecutive entries of a vector (W = 1, or 2 read and written as one
+// 16-byte access)
+template <int W>
+struct Ents {
+  double v[W];
+};
+
+template <int W>
+__device__ __forceinline__ Ents<W> ldw(const double* p, long long i) {
+  Ents<W> o;
+  if constexpr (W == 2) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p + i));
+    o.v[0] = a.x;
+    o.v[1] = a.y;
+  } else {
+    o.v[0] = __ldcg(p + i);
+  }
+  return o;
+}
+
+template <int W>
+__device__ __forceinline__ void stw(double* p, long long i, const Ents<W>& a) {
+  if constexpr (W == 2) *reinterpret_cast<double2*>(p + i) = make_double2(a.v[0], a.v[1]);
+  else p[i] = a.v[0];
+}
+
+// Jacobi (or identity) on W entries
+template <int W>
+__device__ __forceinline__ Ents<W> precond_w(const double* diag, long long i, Ents<W> r) {
+  if (diag) {
+    Ents<W> d;
+    if constexpr (W == 2) {
+      const double2 a = __ldg(reinterpret_cast<const double2*>(diag + i));
+      d.v[0] = a.x;
+      d.v[1] = a.y;
+    } else {
+      d.v[0] = __ldg(diag + i);
+    }
+#pragma unroll
+    for (int j = 0; j < W; j++) r.v[j] = __ddiv_rn(r.v[j], d.v[j]);
+  }
+  return r;
+}
+
+// A grid-stride vector pass over entries [0, n).  With `paired` (every vector
+// the pass touches 16-byte aligned) each step takes two consecutive entries
+// with 16-byte loads and stores, which keeps twice the bytes in flight per
+// register, and the odd last entry follows alone; otherwise one entry a step.
+// f(std::integral_constant<int, W>, i) handles entries i .. i + W - 1.
+template <class F>
+__device__ __forceinline__ void vec_pass(long long n, long long gt, long long gs, bool paired,
+                                         F&& f) {
+  if (paired) {
+    const long long n2 = n >> 1;
+#pragma unroll 2
+    for (long long k = gt; k < n2; k += gs) f(std::integral_constant<int, 2>(), 2 * k);
+    if ((n & 1) && gt == 0) f(std::integral_constant<int, 1>(), n - 1);
+  } else {
+#pragma unroll 4
+    for (long long i = gt; i < n; i += gs) f(std::integral_constant<int, 1>(), i);
+  }
+}
+
+__device__ __forceinline__ bool al16(const void* p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
 __device__ __forceinline__ void hist_push(const History& h, int* len, int it, double res) {
   if (*len < h.cap) {
     h.res[*len] = res;
@@ -92,6 +160,19 @@ struct EpiStoreDot {
     y[r] = t;
     acc = add_rn(acc, mul_rn(__ldcg(w + r), t));
   }
+  // rows r..r+3 of one lane (r % 4 == 0) with 32-byte accesses
+  __device__ __forceinline__ void quad(int r, const double* t) {
+    if (!al16(y + r) || !al16(w + r)) {
+      for (int j = 0; j < 4; j++) (*this)(r + j, t[j]);
+      return;
+    }
+    double wv[4];
+    const double tv[4] = {t[0], t[1], t[2], t[3]};
+    vld4_cg(w + r, wv);
+    vst4(y + r, tv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc = add_rn(acc, mul_rn(wv[j], t[j]));
+  }
 };
 
 // epilogue: r_r = b_r - t (MltAdd(-1, A, x, 1, r) after Copy(b, r)), then the
@@ -113,7 +194,7 @@ struct EpiResidual {
 template <class Epi>
 __device__ __forceinline__ void spmv_phase(const OpArgs& A, const double* x, Epi& epi,
                                            double* s_prod, double* s_red) {
-  XLoadCg<double> xl{x};
+  XLoadCa<double> xl{x};
   if (A.sell.nslice >= 0) {
     sell_spmv<NT, double, double>(A.sell, xl, epi, s_red, blockIdx.x, gridDim.x);
     return;
@@ -265,6 +346,21 @@ struct EpiStoreDot2 {
     y[r] = t;
     acc0 = add_rn(acc0, mul_rn(__ldcg(w0 + r), t));
     if (self) acc1 = add_rn(acc1, mul_rn(t, t));
+  }
+  __device__ __forceinline__ void quad(int r, const double* t) {
+    if (!al16(y + r) || !al16(w0 + r)) {
+      for (int j = 0; j < 4; j++) (*this)(r + j, t[j]);
+      return;
+    }
+    double wv[4];
+    const double tv[4] = {t[0], t[1], t[2], t[3]};
+    vld4_cg(w0 + r, wv);
+    vst4(y + r, tv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      acc0 = add_rn(acc0, mul_rn(wv[j], t[j]));
+      if (self) acc1 = add_rn(acc1, mul_rn(t[j], t[j]));
+    }
   }
 };
 
@@ -435,6 +531,25 @@ struct EpiResidUpdate {
     rr = add_rn(rr, mul_rn(ri, ri));
     rtr = add_rn(rtr, mul_rn(__ldcg(rt + i), ri));
   }
+  __device__ __forceinline__ void quad(int i, const double* t) {
+    if (!al16(r + i) || !al16(rt + i)) {
+      for (int j = 0; j < 4; j++) (*this)(i + j, t[j]);
+      return;
+    }
+    double rv[4], tv[4];
+    vld4_cg(r + i, rv);
+    vld4_cg(rt + i, tv);
+    if (malpha != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) rv[j] = add_rn(rv[j], mul_rn(malpha, t[j]));
+      vst4(r + i, rv);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      rr = add_rn(rr, mul_rn(rv[j], rv[j]));
+      rtr = add_rn(rtr, mul_rn(tv[j], rv[j]));
+    }
+  }
 };
 
 // Cgs (Cgs.cxx:45-132): four grid barriers per loop, two products; the
@@ -497,37 +612,32 @@ __global__ void __launch_bounds__(NT, 4) cgs_fused_kernel(OpArgs A, CgsVecs v, I
     if (lead) hist_push(H, &hlen, nb_iter, reste);
     if (reste < it.tol || nb_iter >= it.max_iter) break;
     if (rho_1 == 0.0) { fail = 1; break; }
-    {
-      const double* __restrict__ rp = v.r;
-      const double* __restrict__ qp = v.q;
-      double* __restrict__ up = v.u;
-      double* __restrict__ pp = v.p;
-      double* __restrict__ php = ph;
-      if (nb_iter == 0) {
-        // Copy(r, u); Copy(u, p); phat = M^{-1} p
-#pragma unroll 4
-        for (long long i = gt; i < n; i += gs) {
-          const double ri = __ldcg(rp + i);
-          up[i] = ri;
-          pp[i] = ri;
-          if (jac) php[i] = precond_val(A.diag, (int)i, ri);
+    if (nb_iter == 0) {
+      // Copy(r, u); Copy(u, p); phat = M^{-1} p
+      vec_pass(n, gt, gs, true, [&](auto w, long long i) {
+        constexpr int W = decltype(w)::value;
+        const Ents<W> ri = ldw<W>(v.r, i);
+        stw<W>(v.u, i, ri);
+        stw<W>(v.p, i, ri);
+        if (jac) stw<W>(ph, i, precond_w<W>(A.diag, i, ri));
+      });
+    } else {
+      // Copy(r, u); Add(beta, q, u); Mlt(beta, p); Add(1, q, p); Mlt(beta, p);
+      // Add(1, u, p); phat = M^{-1} p
+      const double beta = rho_1 / rho_2;
+      vec_pass(n, gt, gs, true, [&](auto w, long long i) {
+        constexpr int W = decltype(w)::value;
+        const Ents<W> qi = ldw<W>(v.q, i);
+        Ents<W> ui = ldw<W>(v.r, i), pi = ldw<W>(v.p, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          if (beta != 0.0) ui.v[j] = add_rn(ui.v[j], mul_rn(beta, qi.v[j]));
+          pi.v[j] = add_rn(mul_rn(add_rn(mul_rn(pi.v[j], beta), qi.v[j]), beta), ui.v[j]);
         }
-      } else {
-        // Copy(r, u); Add(beta, q, u); Mlt(beta, p); Add(1, q, p); Mlt(beta, p);
-        // Add(1, u, p); phat = M^{-1} p
-        const double beta = rho_1 / rho_2;
-#pragma unroll 4
-        for (long long i = gt; i < n; i += gs) {
-          const double qi = __ldcg(qp + i);
-          double ui = __ldcg(rp + i);
-          if (beta != 0.0) ui = add_rn(ui, mul_rn(beta, qi));
-          up[i] = ui;
-          double pi = add_rn(mul_rn(__ldcg(pp + i), beta), qi);
-          pi = add_rn(mul_rn(pi, beta), ui);
-          pp[i] = pi;
-          if (jac) php[i] = precond_val(A.diag, (int)i, pi);
-        }
-      }
+        stw<W>(v.u, i, ui);
+        stw<W>(v.p, i, pi);
+        if (jac) stw<W>(ph, i, precond_w<W>(A.diag, i, pi));
+      });
     }
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // vhat = A phat fused with delta = (rtilde, vhat)
@@ -542,25 +652,25 @@ __global__ void __launch_bounds__(NT, 4) cgs_fused_kernel(OpArgs A, CgsVecs v, I
     const double alpha = rho_1 / delta;
     // Copy(u, q); Add(-alpha, vhat, q); Add(1, q, u); uhat = M^{-1} u;
     // Add(alpha, uhat, x)
-    {
-      double* __restrict__ up = v.u;
-      double* __restrict__ qp = v.q;
-      double* __restrict__ xp = v.x;
-      double* __restrict__ uhp = uh;
-      const double* __restrict__ vhp = v.vh;
-#pragma unroll 4
-      for (long long i = gt; i < n; i += gs) {
-        double ui = __ldcg(up + i);
-        double qi = ui;
-        if (-alpha != 0.0) qi = add_rn(qi, mul_rn(-alpha, __ldcg(vhp + i)));
-        qp[i] = qi;
-        ui = add_rn(ui, qi);
-        up[i] = ui;
-        const double uhi = jac ? precond_val(A.diag, (int)i, ui) : ui;
-        if (jac) uhp[i] = uhi;
-        if (alpha != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(alpha, uhi));
+    vec_pass(n, gt, gs, al16(v.x), [&](auto w, long long i) {
+      constexpr int W = decltype(w)::value;
+      Ents<W> ui = ldw<W>(v.u, i), qi = ui, xi = ldw<W>(v.x, i);
+      const Ents<W> vhi = ldw<W>(v.vh, i);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        if (-alpha != 0.0) qi.v[j] = add_rn(qi.v[j], mul_rn(-alpha, vhi.v[j]));
+        ui.v[j] = add_rn(ui.v[j], qi.v[j]);
       }
-    }
+      stw<W>(v.q, i, qi);
+      stw<W>(v.u, i, ui);
+      const Ents<W> uhi = precond_w<W>(A.diag, i, ui);
+      if (jac) stw<W>(uh, i, uhi);
+      if (alpha != 0.0) {
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, uhi.v[j]));
+        stw<W>(v.x, i, xi);
+      }
+    });
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // qhat = A uhat fused with Add(-alpha, qhat, r), ||r||^2 and (rtilde, r)
     EpiResidUpdate e2{v.r, v.rt, -alpha, 0.0, 0.0};
@@ -639,6 +749,43 @@ struct EpiTfqmrHalf {
     ww = add_rn(ww, mul_rn(wi, wi));
     rtw = add_rn(rtw, mul_rn(__ldcg(rt + i), wi));
   }
+  __device__ __forceinline__ void quad(int i, const double* t) {
+    if (!al16(x + i) || (diag && !al16(diag + i))) {
+      for (int j = 0; j < 4; j++) (*this)(i + j, t[j]);
+      return;
+    }
+    double hv[4] = {t[0], t[1], t[2], t[3]}, dv[4], xv[4], wv[4], yv[4], rv[4];
+    if (diag) {
+      double gv[4];
+      vld4_ldg(diag + i, gv);
+#pragma unroll
+      for (int j = 0; j < 4; j++) hv[j] = __ddiv_rn(t[j], gv[j]);
+    }
+    vld4_cg(d + i, dv);
+    vld4_cg(w + i, wv);
+    vld4_cg(y0 + i, yv);
+    vld4_cg(rt + i, rv);
+    vst4(h + i, hv);
+    if (eta != 0.0) {
+      vld4_cg(x + i, xv);
+#pragma unroll
+      for (int j = 0; j < 4; j++) xv[j] = add_rn(xv[j], mul_rn(eta, dv[j]));
+      vst4(x + i, xv);
+    }
+    if (malpha != 0.0) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) wv[j] = add_rn(wv[j], mul_rn(malpha, hv[j]));
+      vst4(w + i, wv);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) dv[j] = add_rn(mul_rn(dv[j], c1), yv[j]);
+    vst4(d + i, dv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      ww = add_rn(ww, mul_rn(wv[j], wv[j]));
+      rtw = add_rn(rtw, mul_rn(rv[j], wv[j]));
+    }
+  }
 };
 
 // epilogue of g = M^{-1} A y1: Mlt(beta^2, v); Add(beta, h, v); Add(1, g, v);
@@ -657,6 +804,32 @@ struct EpiTfqmrNextV {
     vi = add_rn(vi, gi);
     v[i] = vi;
     sigma = add_rn(sigma, mul_rn(__ldcg(rt + i), vi));
+  }
+  __device__ __forceinline__ void quad(int i, const double* t) {
+    if (diag && !al16(diag + i)) {
+      for (int j = 0; j < 4; j++) (*this)(i + j, t[j]);
+      return;
+    }
+    double gv[4] = {t[0], t[1], t[2], t[3]}, vv[4], hv[4], rv[4];
+    if (diag) {
+      double dv[4];
+      vld4_ldg(diag + i, dv);
+#pragma unroll
+      for (int j = 0; j < 4; j++) gv[j] = __ddiv_rn(t[j], dv[j]);
+    }
+    vld4_cg(v + i, vv);
+    vld4_cg(h + i, hv);
+    vld4_cg(rt + i, rv);
+    vst4(g + i, gv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      vv[j] = mul_rn(vv[j], bb);
+      if (beta != 0.0) vv[j] = add_rn(vv[j], mul_rn(beta, hv[j]));
+      vv[j] = add_rn(vv[j], gv[j]);
+    }
+    vst4(v + i, vv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) sigma = add_rn(sigma, mul_rn(rv[j], vv[j]));
   }
 };
 
@@ -724,22 +897,22 @@ __global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs 
     // first half: Add(-alpha, g, w); Mlt(theta^2 eta / alpha, d); Add(1, y1, d)
     {
       const double c1 = theta * theta * eta / alpha;
-      const double* __restrict__ y1p = v.y1;
-      const double* __restrict__ vp = v.v;
-      const double* __restrict__ gp = v.g;
-      double* __restrict__ y0p = v.y0;
-      double* __restrict__ wp = v.w;
-      double* __restrict__ dp = v.d;
       double ww = 0.0;
-#pragma unroll 4
-      for (long long i = gt; i < n; i += gs) {
-        const double y1i = __ldcg(y1p + i);
-        y0p[i] = add_rn(y1i, mul_rn(-alpha, __ldcg(vp + i)));
-        const double wi = add_rn(__ldcg(wp + i), mul_rn(-alpha, __ldcg(gp + i)));
-        wp[i] = wi;
-        dp[i] = add_rn(mul_rn(__ldcg(dp + i), c1), y1i);
-        ww = add_rn(ww, mul_rn(wi, wi));
-      }
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> y1i = ldw<W>(v.y1, i), vi = ldw<W>(v.v, i), gi = ldw<W>(v.g, i);
+        Ents<W> y0i, wi = ldw<W>(v.w, i), di = ldw<W>(v.d, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          y0i.v[j] = add_rn(y1i.v[j], mul_rn(-alpha, vi.v[j]));
+          wi.v[j] = add_rn(wi.v[j], mul_rn(-alpha, gi.v[j]));
+          di.v[j] = add_rn(mul_rn(di.v[j], c1), y1i.v[j]);
+          ww = add_rn(ww, mul_rn(wi.v[j], wi.v[j]));
+        }
+        stw<W>(v.y0, i, y0i);
+        stw<W>(v.w, i, wi);
+        stw<W>(v.d, i, di);
+      });
       ww = block_sum<NT>(ww, s_red);
       if (tid == 0) s_vals[0] = ww;
       if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
@@ -785,23 +958,26 @@ __global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs 
     if (!done && rho0 == 0.0) fail = 5;
     const double beta = (done || fail) ? 0.0 : rho / rho0;
     // x += eta d; 24. y1 = w + beta y0
-    {
-      double* __restrict__ xp = v.x;
-      double* __restrict__ y1p = v.y1;
-      const double* __restrict__ dp = v.d;
-      const double* __restrict__ wp = v.w;
-      const double* __restrict__ y0p = v.y0;
-      const bool next = !done && !fail;
-#pragma unroll 4
-      for (long long i = gt; i < n; i += gs) {
-        if (eta != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(eta, __ldcg(dp + i)));
-        if (next) {
-          double yi = __ldcg(wp + i);
-          if (beta != 0.0) yi = add_rn(yi, mul_rn(beta, __ldcg(y0p + i)));
-          y1p[i] = yi;
-        }
+    const bool next = !done && !fail;
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      if (eta != 0.0) {
+        Ents<W> xi = ldw<W>(v.x, i);
+        const Ents<W> di = ldw<W>(v.d, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(eta, di.v[j]));
+        stw<W>(v.x, i, xi);
       }
-    }
+      if (next) {
+        Ents<W> yi = ldw<W>(v.w, i);
+        if (beta != 0.0) {
+          const Ents<W> y0i = ldw<W>(v.y0, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) yi.v[j] = add_rn(yi.v[j], mul_rn(beta, y0i.v[j]));
+        }
+        stw<W>(v.y1, i, yi);
+      }
+    });
     if (done || fail) break;
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // 25.-26. g = M^{-1} A y1; v = beta^2 v + beta h + g; next sigma
@@ -836,6 +1012,23 @@ struct EpiPrecDot {
     const double wr = precond_val(diag, r, t);
     w[r] = wr;
     acc = add_rn(acc, mul_rn(__ldcg(v0 + r), wr));
+  }
+  __device__ __forceinline__ void quad(int r, const double* t) {
+    if (!al16(w + r) || !al16(v0 + r) || (diag && !al16(diag + r))) {
+      for (int j = 0; j < 4; j++) (*this)(r + j, t[j]);
+      return;
+    }
+    double vv[4], wv[4] = {t[0], t[1], t[2], t[3]};
+    vld4_cg(v0 + r, vv);
+    if (diag) {
+      double dv[4];
+      vld4_ldg(diag + r, dv);
+#pragma unroll
+      for (int j = 0; j < 4; j++) wv[j] = __ddiv_rn(t[j], dv[j]);
+    }
+    vst4(w + r, wv);
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc = add_rn(acc, mul_rn(vv[j], wv[j]));
   }
 };
 

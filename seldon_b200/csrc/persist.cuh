@@ -93,6 +93,10 @@ __device__ __forceinline__ bool grid_sync(const Persist& P, unsigned& epoch, int
       }
       __nanosleep(32);
     }
+    // a gpu-scope fence after the wait, as cooperative groups' grid.sync
+    // takes: with the CTA barrier below, the L1-cached gathers of the next
+    // phase (XLoadCa) see every write made before the barrier
+    __threadfence();
   }
   if (tid == 0) {
     for (int k = 0; k < K; k++) s_vals[k] = __ldcg(P.sync->res + k);
@@ -103,19 +107,25 @@ __device__ __forceinline__ bool grid_sync(const Persist& P, unsigned& epoch, int
   return s_ok != 0;
 }
 
-// Loads of vectors written inside the same persistent kernel go to L2
-// (the coherence point); the read-only matrix uses the streaming path.
+// Gathers of the product's operand inside a persistent kernel: cached in L1
+// (ld.ca), where a stencil's neighbouring columns hit.  The operand must have
+// been written in an EARLIER phase, never in the phase that gathers it: every
+// phase ends at grid_sync / grid_sync_wide, whose gpu-scope fences (the
+// waiting thread's acquire and fence, the last CTA's fence) and CTA barrier
+// order these loads after every write released before the barrier -- the
+// guarantee ordinary loads have after cooperative groups' grid.sync.  The
+// read-only matrix uses the streaming path.
 template <typename T>
-struct XLoadCg {
+struct XLoadCa {
   const T* x;
-  __device__ __forceinline__ T operator()(int j) const { return __ldcg(x + j); }
+  __device__ __forceinline__ T operator()(int j) const { return __ldca(x + j); }
   template <typename O>
   __device__ __forceinline__ void gather4(const int4& c, O (&o)[4]) const {
     T v[4];
     if (quad_contiguous(x, c)) {
-      vld4_cg(x + c.x, v);
+      vld4_ca(x + c.x, v);
     } else {
-      v[0] = __ldcg(x + c.x); v[1] = __ldcg(x + c.y); v[2] = __ldcg(x + c.z); v[3] = __ldcg(x + c.w);
+      v[0] = __ldca(x + c.x); v[1] = __ldca(x + c.y); v[2] = __ldca(x + c.z); v[3] = __ldca(x + c.w);
     }
     o[0] = O(v[0]); o[1] = O(v[1]); o[2] = O(v[2]); o[3] = O(v[3]);
   }

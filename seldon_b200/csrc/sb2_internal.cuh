@@ -320,6 +320,18 @@ __device__ __forceinline__ void vld4_cg(const T* p, T (&o)[4]) {
 }
 
 template <typename T>
+__device__ __forceinline__ void vld4_ca(const T* p, T (&o)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 a = __ldca(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldca(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  } else {
+    const float4 a = __ldca(reinterpret_cast<const float4*>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  }
+}
+
+template <typename T>
 __device__ __forceinline__ void vst4(T* p, const T (&v)[4]) {
   if constexpr (sizeof(T) == 8) {
     reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
