@@ -52,7 +52,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true", help="skip the solver/Zipf extras")
     p.add_argument("--extras", default="all",
-                   help="comma list of extras to run: c1, c3, gmres, zipf, batch, adjoint, assemble, ilu0 "
+                   help="comma list of extras to run: c1, c3, gmres, krylov, zipf, batch, adjoint, assemble, "
+                        "ilu0 "
                         "(default all)")
     p.add_argument("--cpu-seconds", type=float, default=8.0,
                    help="bounded CPU-baseline sample (seconds of work)")
@@ -411,12 +412,12 @@ def run_ours(args, rank, world, local):
 def run_extras(api, matgen, torch, dev, which="all", cpu=True, gmres_grid=128, batch_systems=4096,
                batch_plan=None):
     """Time-to-solution figures on the other configurations (device-timed).
-    `which`: comma list of c1, c3, gmres, zipf, batch, adjoint, assemble,
-    ilu0, or all.  With `cpu`, the reference's own solvers then run on the
+    `which`: comma list of c1, c3, gmres, krylov, zipf, batch, adjoint,
+    assemble, ilu0, or all.  With `cpu`, the reference's own solvers then run on the
     host cores on the same systems (after every device measurement, so they
     do not disturb it) and each record gains a `cpu_reference` entry."""
     out = {}
-    names = {"c1", "c3", "gmres", "zipf", "batch", "adjoint", "assemble", "ilu0"}
+    names = {"c1", "c3", "gmres", "krylov", "zipf", "batch", "adjoint", "assemble", "ilu0"}
     want = names if which == "all" else set(w.strip() for w in which.split(","))
     unknown = want - names
     if unknown:
@@ -450,6 +451,8 @@ def run_extras(api, matgen, torch, dev, which="all", cpu=True, gmres_grid=128, b
         key = "batch_lap2d_4096" if batch_systems == 4096 else f"batch_lap2d_{batch_systems}"
         out[key] = run_batch(api, matgen, torch, dev, timed, jobs, nsys=batch_systems,
                              plan=batch_plan)
+    if "krylov" in want:
+        out.update(extra_krylov(api, matgen, torch, dev, timed, jobs, gmres_grid))
     if "c1" in want:
         out.update(extra_c1(api, matgen, torch, dev, timed, jobs))
     if "gmres" in want:
@@ -716,6 +719,60 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
     x = xs_gpu["mgs"]
     jobs.append((k_mgs,
                  lambda: _cpu_solve("gmres", ptr, ind, val, bh, x, precond=1, restart=30), False))
+    return out
+
+
+def krylov_loop_bytes(which, n, nnz, jacobi):
+    """Bytes one loop of the persistent BiCgStab, Cgs or TfQmr kernel reads
+    and writes (a loop advances Seldon's count by two): two products
+    (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
+    epilogues, the gathered operand counted once per product.  Per loop:
+      bicgstab  21 vectors (+4 with Jacobi: two diagonal reads, phat, shat)
+      cgs       18 vectors (+4 with Jacobi: two diagonal reads, phat, uhat)
+      tfqmr     30 vectors (+2 with Jacobi: the diagonal in both epilogues)
+    L2 serves part of the re-reads, so the figure bounds DRAM traffic from
+    above."""
+    vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi}[which]
+    return 2 * (nnz * 12 + 4 * (n + 1)) + vec * n * 8
+
+
+def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
+    """BiCgStab, Cgs and TfQmr with Jacobi on the 128^3 convection-diffusion
+    operator (BiCgStab.cxx:43-145, Cgs.cxx:45-132, TfQmr.cxx:44-243): one
+    persistent kernel per solve, against the reference's own drivers on one
+    host core."""
+    ptr, ind, val = matgen.convdiff3d(g)
+    n = ptr.size - 1
+    xs = np.random.default_rng(g + 1).uniform(-1, 1, n)
+    bh = matgen.matvec(ptr, ind, val, xs)
+    b = torch.as_tensor(bh, device=dev)
+    A = api.RowSparse(n, n, ptr, ind, val)
+    J = api.JacobiPreconditioner()
+    peak, _ = measured_peak()
+    out = {}
+    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr}
+    for which, fn in fns.items():
+        def run():
+            X = torch.zeros(n, dtype=torch.float64, device=dev)
+            it = api.Iteration(20000, 1e-10)
+            it.HideMessages()
+            code = fn(A, X, b, J, it)
+            return code, it, X
+        run()
+        ms, (code, it, X) = timed(run, reps=3)
+        x = X.cpu().numpy()
+        nit = it.GetNumberIteration()
+        nbytes = krylov_loop_bytes(which, n, ind.size, True) * nit / 2
+        key = f"{which}_jacobi_convdiff{g}"
+        out[key] = {"ms": round(ms, 2), "error_code": code, "iterations": nit,
+                    "us_per_iteration": round(ms * 1e3 / max(nit, 1), 1),
+                    "rel_residual_host_check": float(
+                        np.linalg.norm(matgen.matvec(ptr, ind, val, x) - bh) / np.linalg.norm(bh)),
+                    "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                    "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
+                    "timing": "best of 3"}
+        jobs.append((key, (lambda w, xg: lambda: _cpu_solve(w, ptr, ind, val, bh, xg, precond=1))(
+            which, x), False))
     return out
 
 

@@ -272,19 +272,20 @@ __global__ void __launch_bounds__(NT, 4) cg_fused_kernel(OpArgs A, CgVecs v, Ite
     if (rho == 0.0) { fail = 1; break; }
     // p = z (first) | p = beta*p + z: Mlt(beta, p); Add(1, z, p)
     {
-      double* __restrict__ pp = v.p;
-      const double* __restrict__ rp = v.r;
-      if (nb_iter == 0) {
-#pragma unroll 4
-        for (long long i = gt; i < n; i += gs) pp[i] = precond_val(A.diag, (int)i, __ldcg(rp + i));
-      } else {
-        const double beta = rho / rho_1;
-#pragma unroll 4
-        for (long long i = gt; i < n; i += gs) {
-          const double z = precond_val(A.diag, (int)i, __ldcg(rp + i));
-          pp[i] = add_rn(mul_rn(__ldcg(pp + i), beta), z);
+      const bool first = nb_iter == 0;
+      const double beta = first ? 0.0 : rho / rho_1;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> z = precond_w<W>(A.diag, i, ldw<W>(v.r, i));
+        if (first) {
+          stw<W>(v.p, i, z);
+        } else {
+          Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) pi.v[j] = add_rn(mul_rn(pi.v[j], beta), z.v[j]);
+          stw<W>(v.p, i, pi);
         }
-      }
+      });
     }
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // q = A p fused with delta = (p, q)
@@ -299,24 +300,29 @@ __global__ void __launch_bounds__(NT, 4) cg_fused_kernel(OpArgs A, CgVecs v, Ite
     // Add(alpha, p, x); Add(-alpha, q, r); then ||r||^2 and (r, z) for the next test
     rr = 0.0;
     rz = 0.0;
-    {
-      double* __restrict__ xp = v.x;
-      double* __restrict__ rp = v.r;
-      const double* __restrict__ pp = v.p;
-      const double* __restrict__ qp = v.q;
-#pragma unroll 4
-      for (long long i = gt; i < n; i += gs) {
-        if (alpha != 0.0) xp[i] = add_rn(__ldcg(xp + i), mul_rn(alpha, __ldcg(pp + i)));
-        double ri = __ldcg(rp + i);
-        if (-alpha != 0.0) {
-          ri = add_rn(ri, mul_rn(-alpha, __ldcg(qp + i)));
-          rp[i] = ri;
-        }
-        const double z = precond_val(A.diag, (int)i, ri);
-        rr = add_rn(rr, mul_rn(ri, ri));
-        rz = add_rn(rz, mul_rn(ri, z));
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      if (alpha != 0.0) {
+        Ents<W> xi = ldw<W>(v.x, i);
+        const Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, pi.v[j]));
+        stw<W>(v.x, i, xi);
       }
-    }
+      Ents<W> ri = ldw<W>(v.r, i);
+      if (-alpha != 0.0) {
+        const Ents<W> qi = ldw<W>(v.q, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) ri.v[j] = add_rn(ri.v[j], mul_rn(-alpha, qi.v[j]));
+        stw<W>(v.r, i, ri);
+      }
+      const Ents<W> z = precond_w<W>(A.diag, i, ri);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        rr = add_rn(rr, mul_rn(ri.v[j], ri.v[j]));
+        rz = add_rn(rz, mul_rn(ri.v[j], z.v[j]));
+      }
+    });
     rr = block_sum<NT>(rr, s_red);
     rz = block_sum<NT>(rz, s_red);
     if (tid == 0) { s_vals[0] = rr; s_vals[1] = rz; }
@@ -426,21 +432,28 @@ __global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVec
     if (rho_1 == 0.0) { fail = 1; break; }
     if (nb_iter == 0) {
       // Copy(r, p); phat = M^{-1} p
-      for (long long i = gt; i < n; i += gs) {
-        const double pi = __ldcg(v.r + i);
-        v.p[i] = pi;
-        if (jac) ph[i] = precond_val(A.diag, (int)i, pi);
-      }
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> pi = ldw<W>(v.r, i);
+        stw<W>(v.p, i, pi);
+        if (jac) stw<W>(ph, i, precond_w<W>(A.diag, i, pi));
+      });
     } else {
       if (omega == 0.0) { fail = 2; break; }
       const double beta = (rho_1 / rho_2) * (alpha / omega);
       // Add(-omega, v, p); Mlt(beta, p); Add(1, r, p); phat = M^{-1} p
-      for (long long i = gt; i < n; i += gs) {
-        double pi = add_rn(__ldcg(v.p + i), mul_rn(-omega, __ldcg(v.v + i)));
-        pi = add_rn(mul_rn(pi, beta), __ldcg(v.r + i));
-        v.p[i] = pi;
-        if (jac) ph[i] = precond_val(A.diag, (int)i, pi);
-      }
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> pi = ldw<W>(v.p, i);
+        const Ents<W> vi = ldw<W>(v.v, i), ri = ldw<W>(v.r, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          pi.v[j] = add_rn(pi.v[j], mul_rn(-omega, vi.v[j]));
+          pi.v[j] = add_rn(mul_rn(pi.v[j], beta), ri.v[j]);
+        }
+        stw<W>(v.p, i, pi);
+        if (jac) stw<W>(ph, i, precond_w<W>(A.diag, i, pi));
+      });
     }
     if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
     // v = A phat, sigma = (rtilde, v)
@@ -454,13 +467,19 @@ __global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVec
     alpha = rho_1 / sigma;
     // Copy(r, s); Add(-alpha, v, s); shat = M^{-1} s; ||s||^2
     double ss = 0.0;
-    for (long long i = gt; i < n; i += gs) {
-      double si = __ldcg(v.r + i);
-      if (-alpha != 0.0) si = add_rn(si, mul_rn(-alpha, __ldcg(v.v + i)));
-      v.s[i] = si;
-      if (jac) sh[i] = precond_val(A.diag, (int)i, si);
-      ss = add_rn(ss, mul_rn(si, si));
-    }
+    vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      Ents<W> si = ldw<W>(v.r, i);
+      if (-alpha != 0.0) {
+        const Ents<W> vi = ldw<W>(v.v, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) si.v[j] = add_rn(si.v[j], mul_rn(-alpha, vi.v[j]));
+      }
+      stw<W>(v.s, i, si);
+      if (jac) stw<W>(sh, i, precond_w<W>(A.diag, i, si));
+#pragma unroll
+      for (int j = 0; j < W; j++) ss = add_rn(ss, mul_rn(si.v[j], si.v[j]));
+    });
     ss = block_sum<NT>(ss, s_red);
     if (tid == 0) s_vals[0] = ss;
     if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
@@ -485,17 +504,34 @@ __global__ void __launch_bounds__(NT, 4) bicgstab_fused_kernel(OpArgs A, BicgVec
     // Add(alpha, phat, x); Add(omega, shat, x); Copy(s, r); Add(-omega, t, r)
     rr = 0.0;
     double rtr = 0.0;
-    for (long long i = gt; i < n; i += gs) {
-      double xi = __ldcg(v.x + i);
-      if (alpha != 0.0) xi = add_rn(xi, mul_rn(alpha, __ldcg(ph + i)));
-      if (omega != 0.0) xi = add_rn(xi, mul_rn(omega, __ldcg(sh + i)));
-      v.x[i] = xi;
-      double ri = __ldcg(v.s + i);
-      if (-omega != 0.0) ri = add_rn(ri, mul_rn(-omega, __ldcg(v.t + i)));
-      v.r[i] = ri;
-      rr = add_rn(rr, mul_rn(ri, ri));
-      rtr = add_rn(rtr, mul_rn(__ldcg(v.rt + i), ri));
-    }
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      Ents<W> xi = ldw<W>(v.x, i);
+      if (alpha != 0.0) {
+        const Ents<W> pi = ldw<W>(ph, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, pi.v[j]));
+      }
+      if (omega != 0.0) {
+        const Ents<W> si = ldw<W>(sh, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(omega, si.v[j]));
+      }
+      stw<W>(v.x, i, xi);
+      Ents<W> ri = ldw<W>(v.s, i);
+      if (-omega != 0.0) {
+        const Ents<W> ti = ldw<W>(v.t, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) ri.v[j] = add_rn(ri.v[j], mul_rn(-omega, ti.v[j]));
+      }
+      stw<W>(v.r, i, ri);
+      const Ents<W> rti = ldw<W>(v.rt, i);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        rr = add_rn(rr, mul_rn(ri.v[j], ri.v[j]));
+        rtr = add_rn(rtr, mul_rn(rti.v[j], ri.v[j]));
+      }
+    });
     rr = block_sum<NT>(rr, s_red);
     rtr = block_sum<NT>(rtr, s_red);
     if (tid == 0) { s_vals[0] = rr; s_vals[1] = rtr; }
@@ -1114,31 +1150,22 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
         if (tid == 0) Hm[k + i * ld] = h;
         const double* Vk = v.V + (size_t)k * nn;
         const double* Vn = (k < i) ? v.V + (size_t)(k + 1) * nn : nullptr;
+        // paired 16-byte passes: 169 against 188 ms for the scalar form on
+        // the 128^3 convection-diffusion operator with Jacobi and restart 30
         double acc = 0.0;
-        double* __restrict__ wp = v.w;
-        const double* __restrict__ vk = Vk;
-        const double* __restrict__ vn = Vn;
-        if (vn) {
-#pragma unroll 4
-          for (long long e = gt; e < n; e += gs) {
-            double we = __ldcg(wp + e);
-            if (-h != 0.0) {
-              we = add_rn(we, mul_rn(-h, __ldcg(vk + e)));
-              wp[e] = we;
-            }
-            acc = add_rn(acc, mul_rn(__ldcg(vn + e), we));
+        vec_pass(n, gt, gs, true, [&](auto wc, long long e) {
+          constexpr int W = decltype(wc)::value;
+          Ents<W> we = ldw<W>(v.w, e);
+          if (-h != 0.0) {
+            const Ents<W> vke = ldw<W>(Vk, e);
+#pragma unroll
+            for (int j = 0; j < W; j++) we.v[j] = add_rn(we.v[j], mul_rn(-h, vke.v[j]));
+            stw<W>(v.w, e, we);
           }
-        } else {
-#pragma unroll 4
-          for (long long e = gt; e < n; e += gs) {
-            double we = __ldcg(wp + e);
-            if (-h != 0.0) {
-              we = add_rn(we, mul_rn(-h, __ldcg(vk + e)));
-              wp[e] = we;
-            }
-            acc = add_rn(acc, mul_rn(we, we));
-          }
-        }
+          const Ents<W> vne = Vn ? ldw<W>(Vn, e) : we;
+#pragma unroll
+          for (int j = 0; j < W; j++) acc = add_rn(acc, mul_rn(vne.v[j], we.v[j]));
+        });
         acc = block_sum<NT>(acc, s_red);
         if (tid == 0) s_vals[0] = acc;
         if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
@@ -1147,10 +1174,15 @@ __global__ void __launch_bounds__(NT, 4) gmres_fused_kernel(OpArgs A, GmresVecs 
       double hi_ip1 = sqrt(s_vals[0]);
       double* Vn = v.V + (size_t)(i + 1) * nn;
       const double inv_h = (hi_ip1 != 0.0) ? 1.0 / hi_ip1 : 1.0;
-      for (long long e = gt; e < n; e += gs) {
-        const double we = __ldcg(v.w + e);
-        Vn[e] = (hi_ip1 != 0.0) ? mul_rn(we, inv_h) : we;
-      }
+      vec_pass(n, gt, gs, true, [&](auto wc, long long e) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> we = ldw<W>(v.w, e);
+        if (hi_ip1 != 0.0) {
+#pragma unroll
+          for (int j = 0; j < W; j++) we.v[j] = mul_rn(we.v[j], inv_h);
+        }
+        stw<W>(Vn, e, we);
+      });
       // rotations (every CTA computes the same scalars)
       if (tid == 0) {
         for (int k = 0; k < i; k++) apply_rot(Hm[k + i * ld], Hm[k + 1 + i * ld], cs[k], sn[k]);
