@@ -613,13 +613,15 @@ int sb2_batch_get_plan(const sb2_batch* B, int* threads, int* warp_max);
 int sb2_batch_set_cluster_plan(sb2_batch* B, int cluster, int cluster_min);
 int sb2_batch_get_cluster_plan(const sb2_batch* B, int* cluster, int* cluster_min);
 
-/* Size from which Cg and BiCgStab (identity or Jacobi) run as chains of
- * full-occupancy kernels (one per pass, scalars in device memory) instead
- * of one persistent kernel.  The default, 2800000 rows, is where the two
- * cross on 7-point Poisson and convection-diffusion matrices on a B200.  The
- * two forms group their reductions differently, so their iterates agree to
- * rounding.  Returns the previous value.  No counterpart in the reference (a
- * tuning knob of this engine). */
+/* Size from which Cg (identity or Jacobi) runs as a chain of full-occupancy
+ * kernels (one per pass, scalars in device memory) instead of one
+ * persistent kernel; BiCgStab does from three times that size.  The
+ * default, 3500000 rows, is where Cg's two forms cross on 7-point Poisson
+ * matrices on a B200; BiCgStab's persistent kernel is still the faster at
+ * 7.1M rows.  The forms group their reductions differently, so their
+ * iterates agree to rounding.  0 runs both drivers chained at every size.
+ * Returns the previous value.  No counterpart in the reference (a tuning
+ * knob of this engine). */
 int sb2_krylov_set_config(int chain_min_n);
 
 /* Cluster-resident CG (on by default): a system whose matrix and vectors fit

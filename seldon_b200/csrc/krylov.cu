@@ -1795,10 +1795,13 @@ int chain_cg(const SellOp<VT>& S, int n, const T* diag, T* x, const T* b, T* wor
 // Systems at least this large run CG as a chain of full-occupancy kernels;
 // smaller ones as one persistent kernel, where an iteration is latency-bound
 // and grid barriers cost less than launches.  On a B200 the two cross near
-// 3e6 rows (7-point Poisson: persistent 70.6 us/iteration against 87.2 at
-// 2.1e6 rows, equal at 3.0e6, chained 213 against 249 at 7.1e6).
+// 3.5e6 rows (7-point Poisson, identity, us per iteration persistent /
+// chained: 93.4 / 102.9 at 3.0e6 rows, 132.2 / 125.5 at 4.1e6, 224.6 / 211.9
+// at 7.1e6).  BiCgStab crosses over at three times that size: its
+// persistent kernel is still the faster at 7.1e6 rows (convection-diffusion,
+// identity: 126.7 / 132.6 at 4.1e6, 206.2 / 210.2 at 7.1e6).
 // sb2_krylov_set_config changes it.
-static std::atomic<int> g_chain_min_n{2800000};
+static std::atomic<int> g_chain_min_n{3500000};
 // Systems that fit one thread-block cluster's shared memory run CG there.
 static std::atomic<int> g_cluster_cg{1};
 static std::atomic<int> g_cluster_cap{16};  // most CTAs a cluster may take
@@ -2213,10 +2216,7 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   }
   if (which == kCg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
     return chain_cg_solve(A, diag, x, b, prm, res, hist, hist_it, hist_cap, s);
-  // BiCgStab crosses over where Cg does: measured on convection-diffusion and
-  // Poisson operators, the chain is 10-13% faster per iteration at 4.1M and
-  // 7.1M rows, the persistent kernel 3% faster at 2.1M
-  if (which == kBicg && A->m >= g_chain_min_n && A->full.sell.nslice >= 0)
+  if (which == kBicg && (long long)A->m >= 3LL * g_chain_min_n && A->full.sell.nslice >= 0)
     return pcg_solve(A, kind == SB2_PRECOND_IDENTITY ? nullptr : M, x, b, prm, res, hist, hist_it,
                      hist_cap, s, kBicg);
   if (which == kCg && g_cluster_cg) {

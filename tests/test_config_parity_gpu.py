@@ -144,7 +144,7 @@ def test_cg_poisson128_vs_reference(api, reference, poisson128, engine):
     ptr, ind, val, b, xr, nr = poisson128
     n = ptr.size - 1
     L = _lib.load()
-    # the chained engine takes systems from 2.8M rows by default (192^3 runs
+    # the chained engine takes systems from 3.5M rows by default (192^3 runs
     # there); lower its threshold to run this one through it
     old = L.sb2_krylov_set_config(n if engine == "chained" else 1 << 30)
     try:
