@@ -722,36 +722,45 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
     return out
 
 
-def krylov_loop_bytes(which, n, nnz, jacobi):
-    """Bytes one loop of the persistent BiCgStab, Cgs or TfQmr kernel reads
-    and writes (a loop advances Seldon's count by two): two products
+def krylov_bytes(which, n, nnz, jacobi, iterations):
+    """Bytes a persistent BiCgStab, Cgs, TfQmr or MinRes solve of
+    `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
-    epilogues, the gathered operand counted once per product.  Per loop:
-      bicgstab  21 vectors (+4 with Jacobi: two diagonal reads, phat, shat)
-      cgs       18 vectors (+4 with Jacobi: two diagonal reads, phat, uhat)
-      tfqmr     30 vectors (+2 with Jacobi: the diagonal in both epilogues)
+    epilogues, the gathered operand counted once per product.
+      bicgstab  per loop (two counted iterations): two products, 21 vectors
+                (+4 with Jacobi: two diagonal reads, phat, shat)
+      cgs       per loop: two products, 18 vectors (+4 with Jacobi)
+      tfqmr     per loop: two products, 30 vectors (+2 with Jacobi)
+      minres    per iteration: one product, 20 vectors (+1 with Jacobi)
     L2 serves part of the re-reads, so the figure bounds DRAM traffic from
     above."""
+    prod = nnz * 12 + 4 * (n + 1)
+    if which == "minres":
+        return iterations * (prod + (20 + jacobi) * n * 8)
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi}[which]
-    return 2 * (nnz * 12 + 4 * (n + 1)) + vec * n * 8
+    return iterations / 2 * (2 * prod + vec * n * 8)
 
 
 def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     """BiCgStab, Cgs and TfQmr with Jacobi on the 128^3 convection-diffusion
-    operator (BiCgStab.cxx:43-145, Cgs.cxx:45-132, TfQmr.cxx:44-243): one
-    persistent kernel per solve, against the reference's own drivers on one
-    host core."""
-    ptr, ind, val = matgen.convdiff3d(g)
-    n = ptr.size - 1
-    xs = np.random.default_rng(g + 1).uniform(-1, 1, n)
-    bh = matgen.matvec(ptr, ind, val, xs)
-    b = torch.as_tensor(bh, device=dev)
-    A = api.RowSparse(n, n, ptr, ind, val)
-    J = api.JacobiPreconditioner()
+    operator, MinRes with Jacobi on the 128^3 Poisson operator
+    (BiCgStab.cxx:43-145, Cgs.cxx:45-132, TfQmr.cxx:44-243,
+    MinRes.cxx:46-153): one persistent kernel per solve, against the
+    reference's own drivers on one host core."""
     peak, _ = measured_peak()
     out = {}
-    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr}
+    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes}
+    systems = {}
     for which, fn in fns.items():
+        op = "poisson" if which == "minres" else "convdiff"
+        if op not in systems:
+            ptr, ind, val = matgen.poisson3d(g) if op == "poisson" else matgen.convdiff3d(g)
+            n = ptr.size - 1
+            xs = np.random.default_rng(g + 1).uniform(-1, 1, n)
+            bh = matgen.matvec(ptr, ind, val, xs)
+            systems[op] = (ptr, ind, val, n, bh, torch.as_tensor(bh, device=dev),
+                           api.RowSparse(n, n, ptr, ind, val), api.JacobiPreconditioner())
+        ptr, ind, val, n, bh, b, A, J = systems[op]
         def run():
             X = torch.zeros(n, dtype=torch.float64, device=dev)
             it = api.Iteration(20000, 1e-10)
@@ -762,8 +771,8 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
         ms, (code, it, X) = timed(run, reps=3)
         x = X.cpu().numpy()
         nit = it.GetNumberIteration()
-        nbytes = krylov_loop_bytes(which, n, ind.size, True) * nit / 2
-        key = f"{which}_jacobi_convdiff{g}"
+        nbytes = krylov_bytes(which, n, ind.size, True, nit)
+        key = f"{which}_jacobi_{op}{g}"
         out[key] = {"ms": round(ms, 2), "error_code": code, "iterations": nit,
                     "us_per_iteration": round(ms * 1e3 / max(nit, 1), 1),
                     "rel_residual_host_check": float(
@@ -771,8 +780,8 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
                     "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
                     "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
                     "timing": "best of 3"}
-        jobs.append((key, (lambda w, xg: lambda: _cpu_solve(w, ptr, ind, val, bh, xg, precond=1))(
-            which, x), False))
+        jobs.append((key, (lambda w, xg, p, i, v, bb: lambda: _cpu_solve(
+            w, p, i, v, bb, xg, precond=1))(which, x, ptr, ind, val, bh), False))
     return out
 
 

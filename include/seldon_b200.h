@@ -421,6 +421,18 @@ int sb2_tfqmr(const sb2_csr* A, const sb2_precond* M, double* x,
               sb2_iter_result* result, double* hist, int* hist_it,
               int hist_cap, void* stream);
 
+/* Seldon's MinRes (MinRes.cxx:46-153) for symmetric, possibly indefinite,
+ * systems with a symmetric preconditioner; arguments, history and error
+ * codes of sb2_cg (codes 1 and 2 for its two breakdowns).  The stopping
+ * test is on the recurrence's residual estimate, ||b|| times the product
+ * of the Givens sines so far.  The identity and Jacobi run as one
+ * persistent kernel per solve; SOR and ILUT drive the device operations
+ * from the host, one at a time. */
+int sb2_minres(const sb2_csr* A, const sb2_precond* M, double* x,
+               const double* b, const sb2_iter_params* params,
+               sb2_iter_result* result, double* hist, int* hist_it,
+               int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

@@ -8,7 +8,7 @@
 //   MltAdd RowSymSparse     computation/basic_functions/Functions_MatVect.cxx:526-564
 //   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
 //   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
-//   Cgs / TfQmr             computation/solver/iterative/{Cgs,TfQmr}.cxx
+//   Cgs / TfQmr / MinRes    computation/solver/iterative/{Cgs,TfQmr,MinRes}.cxx
 //   SOR                     matrix_sparse/Relaxation_MatVect.cxx:41-95, 176-298
 //   SorPreconditioner       computation/solver/preconditioner/Precond_Ssor.cxx:24-90
 //
@@ -125,6 +125,7 @@ namespace
       case 2: return Gmres(A, x, b, M, it);
       case 3: return Cgs(A, x, b, M, it);
       case 4: return TfQmr(A, x, b, M, it);
+      case 5: return MinRes(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -363,8 +364,8 @@ extern "C"
     return 0;
   }
 
-  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr.  precond: 0 identity,
-  // 1 Jacobi, 2 SOR.
+  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes.  precond:
+  // 0 identity, 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
                 const double* val, int sym, int precond, double omega,

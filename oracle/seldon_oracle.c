@@ -702,7 +702,91 @@ out:
   return code;
 }
 
-/* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr.
+/* MinRes, computation/solver/iterative/MinRes.cxx:46-153.  Symmetric A and
+ * M; the test is on the recurrence's residual estimate np (||b|| times the
+ * product of the |s| of the rotations so far). */
+static int orc_minres_impl(const orc_csr* A, double* x, const double* b,
+                           const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *u_old = malloc(bytes), *u = malloc(bytes), *r = malloc(bytes),
+         *v_old = malloc(bytes), *v = malloc(bytes), *w_old = malloc(bytes),
+         *w = malloc(bytes), *z = malloc(bytes), *w_oold = malloc(bytes);
+  double* all[9] = {u_old, u, r, v_old, v, w_old, w, z, w_oold};
+  for (int k = 0; k < 9; k++) memcpy(all[k], b, bytes);
+  double dp, beta, ibeta, beta_old, alpha, eta, ceta;
+  double cold, coold, c, soold, sold, s, rho0, rho1, rho2, rho3, np;
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  memset(u_old, 0, bytes); memset(v_old, 0, bytes); memset(w_old, 0, bytes);
+  memset(w, 0, bytes); memset(w_oold, 0, bytes);
+  prec_solve(M, A, r, z);
+  dp = orc_dot(N, r, z);
+  dp = sqrt(dp);
+  beta = dp;
+  eta = beta;
+  orc_copy(N, r, v);
+  orc_copy(N, z, u);
+  ibeta = 1.0 / beta;
+  orc_scal(N, ibeta, v);
+  orc_scal(N, ibeta, u);
+  c = 1.0; s = 0.0; cold = 1.0; sold = 0.0;
+  np = orc_nrm2(N, b);
+  it->nb_iter = 0;
+  while (!it_finished(it, np)) {
+    csr_mlt(A, u, r);
+    alpha = orc_dot(N, r, u);
+    prec_solve(M, A, r, z);
+    orc_axpy(N, -alpha, v, r);
+    orc_axpy(N, -alpha, u, z);
+    orc_axpy(N, -beta, v_old, r);
+    orc_axpy(N, -beta, u_old, z);
+    beta_old = beta;
+    dp = orc_dot(N, r, z);
+    beta = sqrt(dp);
+    /* QR factorization */
+    coold = cold; cold = c; soold = sold; sold = s;
+    rho0 = cold * alpha - coold * sold * beta_old;
+    rho1 = sqrt(rho0 * rho0 + beta * beta);
+    rho2 = sold * alpha + coold * cold * beta_old;
+    rho3 = soold * beta_old;
+    if (rho1 == 0.0) { it_fail(it, 1); break; }
+    c = rho0 / rho1;
+    s = beta / rho1;
+    orc_copy(N, w_old, w_oold);
+    orc_copy(N, w, w_old);
+    orc_copy(N, u, w);
+    orc_axpy(N, -rho2, w_old, w);
+    orc_axpy(N, -rho3, w_oold, w);
+    orc_scal(N, 1. / rho1, w);
+    ceta = c * eta;
+    orc_axpy(N, ceta, w, x);
+    eta = -s * eta;
+    orc_copy(N, v, v_old);
+    orc_copy(N, u, u_old);
+    orc_copy(N, r, v);
+    orc_copy(N, z, u);
+    if (beta == 0.0) { it_fail(it, 2); break; }
+    ibeta = 1.0 / beta;
+    orc_scal(N, ibeta, v);
+    orc_scal(N, ibeta, u);
+    np *= fabs(s);
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 9; k++) free(all[k]);
+  return code;
+}
+
+/* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
+ * 5 MinRes.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -735,6 +819,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_cgs_impl(&A, x, b, &M, &it);
   else if (which == 4)
     code = orc_tfqmr_impl(&A, x, b, &M, &it);
+  else if (which == 5)
+    code = orc_minres_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

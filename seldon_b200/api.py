@@ -940,6 +940,13 @@ def TfQmr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_tfqmr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def MinRes(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """MINRES for symmetric (possibly indefinite) systems (MinRes.cxx:46-153);
+    the stopping test is on the recurrence's residual estimate; returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_minres, A, x, b, M, iteration, hist_cap, stream)
+
+
 def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None, orthogonalization="mgs"):
     """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183).
 

@@ -10,12 +10,12 @@
 //
 // SOR and ILUT preconditioning (level-scheduled sweeps, many dependent
 // launches) of Cg, BiCgStab and Gmres run as device-resident chains around the
-// sweeps (chain.cu); Cgs and TfQmr with them, and every driver when those
-// chains are switched off, go through a host-driven driver over the same
+// sweeps (chain.cu); Cgs, TfQmr and MinRes with them, and every driver when
+// those chains are switched off, go through a host-driven driver over the same
 // device kernels, one operation at a time, in the reference's order.
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
-// Cgs.cxx:45-132, TfQmr.cxx:44-243, Iterative.cxx:235-354.
+// Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -955,7 +955,7 @@ __global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs 
     }
     // 14.-21. theta, c, tau, eta; x += eta d; Finished(kappa)
     theta = sqrt(s_vals[0]) / tau;
-    double c = 1.0 / sqrt(1.0 + theta * theta);
+    double c = 1.0 / sqrt(add_rn(1.0, mul_rn(theta, theta)));
     tau = tau * c * theta;
     eta = c * c * alpha;
     double kappa = tau * sqrt(2. * (nb_iter + 1));
@@ -981,7 +981,7 @@ __global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs 
     }
     if (tau == 0.0) { fail = 4; break; }
     theta = sqrt(s_vals[0]) / tau;
-    c = 1.0 / sqrt(1.0 + theta * theta);
+    c = 1.0 / sqrt(add_rn(1.0, mul_rn(theta, theta)));
     tau = tau * c * theta;
     eta = c * c * alpha;
     kappa = tau * sqrt(2. * (nb_iter + 1) + 1.);
@@ -1025,6 +1025,220 @@ __global__ void __launch_bounds__(NT, 4) tfqmr_fused_kernel(OpArgs A, TfqmrVecs 
       if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
     }
     sigma = s_vals[0];
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
+// ----------------------------------------------------------------- MINRES
+
+struct MinresVecs {
+  const double* b;
+  double *x, *r, *z;
+  double *u, *u_old, *v, *v_old, *w, *w_old, *w_oold;  // initial roles
+};
+
+// MinRes (MinRes.cxx:46-153): per iteration the product fused with
+// (r, u), one pass forming r and z with (r, z), and one pass forming w, x
+// and the next v and u -- three grid barriers.  Seldon's copies between the
+// old and new vectors (Copy(w_old, w_oold), Copy(v, v_old), ...) are role
+// rotations of the buffers: every thread swaps the same register pointers.  The
+// scalar recurrences are rounded step by step (mul_rn / add_rn), as the
+// reference's separately rounded products and sums.
+__global__ void __launch_bounds__(NT, 4) minres_fused_kernel(OpArgs A, MinresVecs v, IterArgs it,
+                                                          Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  // iter.Init(b)
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b); z = M^{-1} r; dp = (r, z)
+  double dp = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      v.x[i] = 0.0;
+      v.r[i] = bi;
+      dp = add_rn(dp, mul_rn(bi, precond_val(A.diag, (int)i, bi)));
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, A.diag, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    dp = epi.rz;
+  }
+  dp = block_sum<NT>(dp, s_red);
+  if (tid == 0) s_vals[0] = dp;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  double beta = sqrt(s_vals[0]);
+  double eta = beta;
+  {
+    // v = r / beta, u = z / beta (Copy then Mlt(ibeta, .)); the old vectors
+    // and the w's start at zero
+    const double ibeta = 1.0 / beta;
+    vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      const Ents<W> ri = ldw<W>(v.r, i);
+      const Ents<W> zi = precond_w<W>(A.diag, i, ri);
+      Ents<W> a, c, zero;
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        a.v[j] = mul_rn(ri.v[j], ibeta);
+        c.v[j] = mul_rn(zi.v[j], ibeta);
+        zero.v[j] = 0.0;
+      }
+      stw<W>(v.v, i, a);
+      stw<W>(v.u, i, c);
+      stw<W>(v.u_old, i, zero);
+      stw<W>(v.v_old, i, zero);
+      stw<W>(v.w, i, zero);
+      stw<W>(v.w_old, i, zero);
+      stw<W>(v.w_oold, i, zero);
+    });
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  double c = 1.0, s = 0.0, cold = 1.0, sold = 0.0;
+  double np = normb;  // Norm2(b)
+  double *u = v.u, *u_old = v.u_old, *vv = v.v, *v_old = v.v_old;
+  double *w = v.w, *w_old = v.w_old, *w_oold = v.w_oold;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * np;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    // r = A u fused with alpha = (r, u)
+    {
+      EpiStoreDot epi{v.r, u, 0.0};
+      spmv_phase(A, u, epi, s_prod, s_red);
+      const double a = block_sum<NT>(epi.acc, s_red);
+      if (tid == 0) s_vals[0] = a;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double alpha = s_vals[0];
+    // z = M^{-1} r; Add(-alpha, v, r); Add(-alpha, u, z); Add(-beta, v_old, r);
+    // Add(-beta, u_old, z); dp = (r, z)
+    {
+      double d = 0.0;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> ri = ldw<W>(v.r, i);
+        Ents<W> zi = precond_w<W>(A.diag, i, ri);
+        if (-alpha != 0.0) {
+          const Ents<W> a = ldw<W>(vv, i), b = ldw<W>(u, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            ri.v[j] = add_rn(ri.v[j], mul_rn(-alpha, a.v[j]));
+            zi.v[j] = add_rn(zi.v[j], mul_rn(-alpha, b.v[j]));
+          }
+        }
+        if (-beta != 0.0) {
+          const Ents<W> a = ldw<W>(v_old, i), b = ldw<W>(u_old, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            ri.v[j] = add_rn(ri.v[j], mul_rn(-beta, a.v[j]));
+            zi.v[j] = add_rn(zi.v[j], mul_rn(-beta, b.v[j]));
+          }
+        }
+        stw<W>(v.r, i, ri);
+        stw<W>(v.z, i, zi);
+#pragma unroll
+        for (int j = 0; j < W; j++) d = add_rn(d, mul_rn(ri.v[j], zi.v[j]));
+      });
+      d = block_sum<NT>(d, s_red);
+      if (tid == 0) s_vals[0] = d;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double beta_old = beta;
+    beta = sqrt(s_vals[0]);
+    // QR factorization
+    const double coold = cold, soold = sold;
+    cold = c;
+    sold = s;
+    const double rho0 = add_rn(mul_rn(cold, alpha), -mul_rn(mul_rn(coold, sold), beta_old));
+    const double rho1 = sqrt(add_rn(mul_rn(rho0, rho0), mul_rn(beta, beta)));
+    const double rho2 = add_rn(mul_rn(sold, alpha), mul_rn(mul_rn(coold, cold), beta_old));
+    const double rho3 = mul_rn(soold, beta_old);
+    if (rho1 == 0.0) { fail = 1; break; }
+    c = rho0 / rho1;
+    s = beta / rho1;
+    // w_oold <- w_old, w_old <- w, w <- (u - rho2 w_old - rho3 w_oold) / rho1,
+    // written over the old w_oold; x += c eta w; then v_old <- v, u_old <- u,
+    // v <- r / beta, u <- z / beta, written over the old v_old and u_old
+    const double inv_rho1 = 1. / rho1;
+    const double ceta = mul_rn(c, eta);
+    eta = mul_rn(-s, eta);
+    const bool last = (beta == 0.0);
+    const double ibeta = last ? 0.0 : 1.0 / beta;
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      Ents<W> wn = ldw<W>(u, i);
+      if (-rho2 != 0.0) {
+        const Ents<W> a = ldw<W>(w, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) wn.v[j] = add_rn(wn.v[j], mul_rn(-rho2, a.v[j]));
+      }
+      if (-rho3 != 0.0) {
+        const Ents<W> a = ldw<W>(w_old, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) wn.v[j] = add_rn(wn.v[j], mul_rn(-rho3, a.v[j]));
+      }
+#pragma unroll
+      for (int j = 0; j < W; j++) wn.v[j] = mul_rn(wn.v[j], inv_rho1);
+      stw<W>(w_oold, i, wn);
+      if (ceta != 0.0) {
+        Ents<W> xi = ldw<W>(v.x, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(ceta, wn.v[j]));
+        stw<W>(v.x, i, xi);
+      }
+      if (!last) {
+        Ents<W> ri = ldw<W>(v.r, i), zi = ldw<W>(v.z, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          ri.v[j] = mul_rn(ri.v[j], ibeta);
+          zi.v[j] = mul_rn(zi.v[j], ibeta);
+        }
+        stw<W>(v_old, i, ri);
+        stw<W>(u_old, i, zi);
+      }
+    });
+    if (last) { fail = 2; break; }
+    {
+      double* t = w_oold;  // the new w sits where w_oold was
+      w_oold = w_old;
+      w_old = w;
+      w = t;
+    }
+    {
+      double* t = u;  // the new u and v sit where u_old and v_old were
+      u = u_old;
+      u_old = t;
+      t = vv;
+      vv = v_old;
+      v_old = t;
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    np = mul_rn(np, fabs(s));
     nb_iter++;
   }
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
@@ -1336,7 +1550,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
                 sell_op(f)};
 }
 
-enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4 };
+enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
@@ -1350,6 +1564,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kBicg) { kern = (const void*)bicgstab_fused_kernel; nvec = 9; }
   if (which == kCgs) { kern = (const void*)cgs_fused_kernel; nvec = 8; }
   if (which == kTfqmr) { kern = (const void*)tfqmr_fused_kernel; nvec = 8; }
+  if (which == kMinres) { kern = (const void*)minres_fused_kernel; nvec = 9; }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -1377,6 +1592,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   GmresVecs gv;
   CgsVecs sv;
   TfqmrVecs tv;
+  MinresVecs mv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -1397,6 +1613,10 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     tv = TfqmrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                    V + 7 * nn};
     args[1] = &tv;
+  } else if (which == kMinres) {
+    mv = MinresVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                    V + 7 * nn, V + 8 * nn};
+    args[1] = &mv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -1650,6 +1870,77 @@ static int host_tfqmr(Ops& o, double* x, const double* b, const sb2_iter_params*
   return SB2_OK;
 }
 
+static int host_minres(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                       HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *u_old = V, *u = V + n, *r = V + 2 * n, *v_old = V + 3 * n, *v = V + 4 * n,
+         *w_old = V + 5 * n, *w = V + 6 * n, *z = V + 7 * n, *w_oold = V + 8 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  for (double* p : {u_old, v_old, w_old, w, w_oold}) SB2_TRY(sb2_fill(o.n, 0.0, p, o.s));
+  SB2_TRY(o.prec(r, z));
+  double dp;
+  SB2_TRY(o.dot(r, z, &dp));
+  double beta = std::sqrt(dp), eta = beta;
+  SB2_TRY(o.copy(r, v));
+  SB2_TRY(o.copy(z, u));
+  double ibeta = 1.0 / beta;
+  SB2_TRY(o.scal(ibeta, v));
+  SB2_TRY(o.scal(ibeta, u));
+  double c = 1.0, s = 0.0, cold = 1.0, sold = 0.0, np = nb;
+  for (;;) {
+    if (it.finished(np)) break;
+    SB2_TRY(o.mlt(u, r));
+    double alpha;
+    SB2_TRY(o.dot(r, u, &alpha));
+    SB2_TRY(o.prec(r, z));
+    SB2_TRY(o.axpy(-alpha, v, r));
+    SB2_TRY(o.axpy(-alpha, u, z));
+    SB2_TRY(o.axpy(-beta, v_old, r));
+    SB2_TRY(o.axpy(-beta, u_old, z));
+    const double beta_old = beta;
+    SB2_TRY(o.dot(r, z, &dp));
+    beta = std::sqrt(dp);
+    const double coold = cold, soold = sold;
+    cold = c;
+    sold = s;
+    volatile double t0 = cold * alpha, t1 = coold * sold, t2 = t1 * beta_old;
+    const double rho0 = t0 - t2;
+    volatile double q0 = rho0 * rho0, q1 = beta * beta;
+    const double rho1 = std::sqrt(q0 + q1);
+    volatile double a0 = sold * alpha, a1 = coold * cold, a2 = a1 * beta_old;
+    const double rho2 = a0 + a2;
+    const double rho3 = soold * beta_old;
+    if (rho1 == 0.0) { it.fail = 1; break; }
+    c = rho0 / rho1;
+    s = beta / rho1;
+    SB2_TRY(o.copy(w_old, w_oold));
+    SB2_TRY(o.copy(w, w_old));
+    SB2_TRY(o.copy(u, w));
+    SB2_TRY(o.axpy(-rho2, w_old, w));
+    SB2_TRY(o.axpy(-rho3, w_oold, w));
+    SB2_TRY(o.scal(1. / rho1, w));
+    const double ceta = c * eta;
+    SB2_TRY(o.axpy(ceta, w, x));
+    eta = -s * eta;
+    SB2_TRY(o.copy(v, v_old));
+    SB2_TRY(o.copy(u, u_old));
+    SB2_TRY(o.copy(r, v));
+    SB2_TRY(o.copy(z, u));
+    if (beta == 0.0) { it.fail = 2; break; }
+    ibeta = 1.0 / beta;
+    SB2_TRY(o.scal(ibeta, v));
+    SB2_TRY(o.scal(ibeta, u));
+    np *= std::fabs(s);
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -1755,7 +2046,8 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kBicg ? 8
                    : which == kCgs ? 9
                    : which == kTfqmr ? 10
-                                     : 3 + m + 1;
+                   : which == kMinres ? 9
+                                      : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
   SB2_CUDA_TRY(pool_malloc((void**)&buf.p, sizeof(double) * (size_t)std::max(n, 1) * nvec, s));
@@ -1769,6 +2061,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kBicg) SB2_TRY(host_bicgstab(o, x, b, prm, it, V, &init_failed));
   else if (which == kCgs) SB2_TRY(host_cgs(o, x, b, prm, it, V, &init_failed));
   else if (which == kTfqmr) SB2_TRY(host_tfqmr(o, x, b, prm, it, V, &init_failed));
+  else if (which == kMinres) SB2_TRY(host_minres(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -2295,6 +2588,14 @@ int sb2_tfqmr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b
               int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_tfqmr");
   return solve_entry(kTfqmr, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_minres(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_minres");
+  return solve_entry(kMinres, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

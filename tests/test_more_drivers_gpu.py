@@ -1,6 +1,7 @@
-"""Cgs (Cgs.cxx:45-132) and TfQmr (TfQmr.cxx:44-243) on the device against
-the oracle's restatements, which are pinned bit for bit to the reference's
-own templates (tests/test_oracle_pin.py).
+"""Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243) and MinRes
+(MinRes.cxx:46-153) on the device against the oracle's restatements, which
+are pinned bit for bit to the reference's own templates
+(tests/test_oracle_pin.py).
 
 The identity and Jacobi run the persistent kernels; SOR and ILUT the
 host-driven loop over the device operations.  Reductions are summed in
@@ -14,11 +15,11 @@ import pytest
 
 from seldon_b200 import matgen
 from tests.helpers import to_dev, to_host
-from tests.test_oracle_pin import _edge_solves, _nonfinite_cases
+from tests.test_oracle_pin import _edge_solves, _nonfinite_cases, shifted_laplacian
 
 pytestmark = pytest.mark.gpu
 
-SOLVERS = ["cgs", "tfqmr"]
+SOLVERS = ["cgs", "tfqmr", "minres"]
 
 
 @pytest.fixture(scope="module")
@@ -28,7 +29,7 @@ def api(cuda):
 
 
 def _fn(api, which):
-    return {"cgs": api.Cgs, "tfqmr": api.TfQmr}[which]
+    return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes}[which]
 
 
 def _precond(api, pc):
@@ -58,13 +59,25 @@ def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000):
     return code, it, to_host(X)
 
 
-CASES = [(w, m, pc) for w in SOLVERS for m in ("conv", "lap", "lap_up") for pc in (0, 1, 2)]
+# MinRes wants symmetric systems: the Laplacian, and the Laplacian shifted
+# to be indefinite (its case), in both storages
+CASES = ([(w, m, pc) for w in ("cgs", "tfqmr") for m in ("conv", "lap", "lap_up")
+          for pc in (0, 1, 2)] +
+         [("minres", m, pc) for m in ("lap", "lap_up", "indef", "indef_up") for pc in (0, 1, 2)])
+
+
+def _case_matrix(mname):
+    if mname == "conv":
+        return matgen.convdiff3d(9)
+    if mname.startswith("indef"):
+        return shifted_laplacian(30, 0.02)
+    return matgen.lap2d(30)
 
 
 @pytest.mark.parametrize("which,mname,pc", CASES)
 def test_parity(api, oracle, which, mname, pc):
-    full = matgen.convdiff3d(9) if mname == "conv" else matgen.lap2d(30)
-    sym = mname == "lap_up"
+    full = _case_matrix(mname)
+    sym = mname.endswith("_up")
     A = matgen.upper(*full) if sym else full
     n = A[0].size - 1
     b = matgen.matvec(*full, np.random.default_rng(3).uniform(-1, 1, n))
@@ -91,7 +104,7 @@ def test_parity(api, oracle, which, mname, pc):
 
 @pytest.mark.parametrize("which", SOLVERS)
 def test_initial_guess(api, oracle, which):
-    full = matgen.convdiff3d(8)
+    full = matgen.convdiff3d(8) if which != "minres" else matgen.poisson3d(16)
     n = full[0].size - 1
     rng = np.random.default_rng(9)
     b = matgen.matvec(*full, rng.uniform(-1, 1, n))
@@ -123,8 +136,12 @@ def test_edges(api, oracle, which):
                 assert np.linalg.norm(x) < 1e-5
                 continue
             assert nb == no, (name, pc, nb, no)
-            scale = max(np.linalg.norm(xo), 1e-300)
-            assert np.linalg.norm(x - xo) / scale < 1e-12, (name, pc)
+            # MinRes from the exact guess divides by a zero (r, z): NaN where
+            # the reference has NaN
+            assert np.array_equal(np.isnan(x), np.isnan(xo)), (name, pc)
+            ok = ~np.isnan(xo)
+            scale = max(np.linalg.norm(xo[ok]), 1e-300)
+            assert np.linalg.norm(x[ok] - xo[ok]) / scale < 1e-12, (name, pc)
 
 
 @pytest.mark.parametrize("which", SOLVERS)
@@ -142,7 +159,7 @@ def test_nonfinite(api, oracle, which):
 @pytest.mark.parametrize("which", SOLVERS)
 def test_deterministic_and_larger(api, oracle, which):
     # 64,000 rows: a grid of many CTAs, every product in the binned layout
-    full = matgen.convdiff3d(40)
+    full = matgen.convdiff3d(40) if which != "minres" else matgen.poisson3d(40)
     n = full[0].size - 1
     b = matgen.matvec(*full, np.random.default_rng(1).uniform(-1, 1, n))
     outs = [_solve(api, which, full, False, b, 1) for _ in range(2)]
@@ -155,7 +172,7 @@ def test_deterministic_and_larger(api, oracle, which):
     assert np.linalg.norm(outs[0][2] - xo) / np.linalg.norm(xo) < 1e-7
 
 
-@pytest.mark.parametrize("which", SOLVERS)
+@pytest.mark.parametrize("which", ["cgs", "tfqmr"])
 def test_ilut(api, reference, which):
     # the host-driven loop with the device ILUT apply against the reference's
     # driver with its own factor
@@ -183,7 +200,7 @@ def test_breakdowns(api, oracle):
     # (rtilde, v) vanish exactly
     ptr, ind, val = np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, -1.0])
     A = api.RowSparse(2, 2, ptr, ind, val)
-    for which in SOLVERS:
+    for which in ("cgs", "tfqmr"):
         it = api.Iteration(10, 1e-12)
         it.HideMessages()
         X = to_dev(np.zeros(2))
@@ -192,3 +209,28 @@ def test_breakdowns(api, oracle):
         _, co, no, _, _ = oracle.solve(which, ptr, ind, val, b, tol=1e-12, max_iter=10)
         assert (code, it.GetNumberIteration()) == (co, no)
         assert code == (2 if which == "cgs" else 1)
+
+
+def test_minres_breakdown_and_estimate(api, oracle):
+    # a 1 x 1 system: the first step solves it and (r, z) vanishes, MinRes's
+    # breakdown #2 at iteration 0 with x exact
+    A = api.RowSparse(1, 1, np.array([0, 1]), np.array([0]), np.array([4.0]))
+    it = api.Iteration(10, 1e-12)
+    it.HideMessages()
+    X = to_dev(np.zeros(1))
+    code = api.MinRes(A, X, to_dev(np.array([2.0])), api.Preconditioner_Base(), it)
+    assert (code, it.GetNumberIteration()) == (2, 0)
+    assert to_host(X)[0] == 0.5
+    # the history is the recurrence's estimate: the oracle's to rounding,
+    # one entry per iteration from 0
+    full = shifted_laplacian(20, 0.05)
+    n = full[0].size - 1
+    b = np.random.default_rng(8).uniform(-1, 1, n)
+    _, co, no, ho, hio = oracle.solve("minres", *full, b, tol=1e-10, max_iter=2000,
+                                      hist_cap=5000)
+    code, it, x = _solve(api, "minres", full, False, b, 0)
+    assert code == co == 0
+    its = [i for i, _ in it.history]
+    assert its == list(range(it.GetNumberIteration() + 1))
+    k = min(len(its), len(hio)) - 2
+    np.testing.assert_allclose([r for _, r in it.history][:k], ho[:k], rtol=1e-6)

@@ -99,10 +99,10 @@ def test_mltadd_live(reference, oracle, seed):
                           reference.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True))
 
 
-@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr"])
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
-    ptr, ind, val = matgen.convdiff3d(5) if which != "cg" else matgen.lap2d(15)
+    ptr, ind, val = matgen.convdiff3d(5) if which not in ("cg", "minres") else matgen.lap2d(15)
     m = ptr.size - 1
     rng = np.random.default_rng(7)
     b = matgen.matvec(ptr, ind, val, rng.uniform(-1, 1, m))
@@ -161,7 +161,31 @@ def _edge_solves():
     return out
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr"])
+def shifted_laplacian(g, sigma):
+    """The g x g Laplacian minus sigma I: symmetric indefinite for sigma
+    above its smallest eigenvalue (MinRes's case)."""
+    ptr, ind, val = matgen.lap2d(g)
+    val = val.copy()
+    rows = np.repeat(np.arange(ptr.size - 1), np.diff(ptr))
+    val[ind == rows] -= sigma
+    return ptr, ind, val
+
+
+@pytest.mark.parametrize("pc", [0, 1, 2])
+@pytest.mark.parametrize("sym", [False, True])
+def test_minres_indefinite_live(reference, oracle, pc, sym):
+    full = shifted_laplacian(15, 0.5)
+    A = matgen.upper(*full) if sym else full
+    b = np.random.default_rng(4).uniform(-1, 1, full[0].size - 1)
+    xo, co, no, _, _ = oracle.solve("minres", *A, b, sym=sym, precond=pc, omega=1.1,
+                                    tol=1e-10, max_iter=500)
+    xr, cr, nr = reference.solve("minres", *A, b, sym=sym, precond=pc, omega=1.1, tol=1e-10,
+                                 max_iter=500)
+    assert (co, no) == (cr, nr)
+    assert np.array_equal(xo, xr)
+
+
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
@@ -285,7 +309,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
             assert np.array_equal(xo, xr, equal_nan=True)
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
-    for which in ("cgs", "tfqmr"):
+    for which in ("cgs", "tfqmr", "minres"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
