@@ -722,8 +722,8 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
     return out
 
 
-def krylov_bytes(which, n, nnz, jacobi, iterations):
-    """Bytes a persistent BiCgStab, Cgs, TfQmr or MinRes solve of
+def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
+    """Bytes a persistent BiCgStab, Cgs, TfQmr, MinRes or Gcr solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -732,35 +732,50 @@ def krylov_bytes(which, n, nnz, jacobi, iterations):
       cgs       per loop: two products, 18 vectors (+4 with Jacobi)
       tfqmr     per loop: two products, 30 vectors (+2 with Jacobi)
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
+      gcr       per inner step j of a cycle (two counted iterations): two
+                products, 2j + 14 vectors (the j + 1 projections and the
+                j + 1 terms of the new direction; +2 with Jacobi); per cycle
+                2 more (p_0 = r / ||r||)
     L2 serves part of the re-reads, so the figure bounds DRAM traffic from
     above."""
     prod = nnz * 12 + 4 * (n + 1)
     if which == "minres":
         return iterations * (prod + (20 + jacobi) * n * 8)
+    if which == "gcr":
+        steps, cycle, total = int(iterations // 2), max((restart + 1) // 2, 1), 0
+        for k in range(steps):
+            j = k % cycle
+            total += 2 * prod + (2 * j + 14 + 2 * jacobi + (2 if j == 0 else 0)) * n * 8
+        return total
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
 def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     """BiCgStab, Cgs and TfQmr with Jacobi on the 128^3 convection-diffusion
-    operator, MinRes with Jacobi on the 128^3 Poisson operator
-    (BiCgStab.cxx:43-145, Cgs.cxx:45-132, TfQmr.cxx:44-243,
-    MinRes.cxx:46-153): one persistent kernel per solve, against the
-    reference's own drivers on one host core."""
+    operator, MinRes with Jacobi on the 128^3 Poisson operator, Gcr(10) with
+    Jacobi on the 64^3 convection-diffusion operator (its iteration count
+    grows with the grid: 768 at 32^3, 1494 at 48^3, so the reference's host
+    solve at 128^3 would take minutes) (BiCgStab.cxx:43-145, Cgs.cxx:45-132,
+    TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141): one persistent
+    kernel per solve, against the reference's own drivers on one host
+    core."""
     peak, _ = measured_peak()
     out = {}
-    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes}
+    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "gcr": api.Gcr,
+           "minres": api.MinRes}
     systems = {}
     for which, fn in fns.items():
         op = "poisson" if which == "minres" else "convdiff"
-        if op not in systems:
-            ptr, ind, val = matgen.poisson3d(g) if op == "poisson" else matgen.convdiff3d(g)
+        gg = g // 2 if which == "gcr" else g
+        if (op, gg) not in systems:
+            ptr, ind, val = matgen.poisson3d(gg) if op == "poisson" else matgen.convdiff3d(gg)
             n = ptr.size - 1
-            xs = np.random.default_rng(g + 1).uniform(-1, 1, n)
+            xs = np.random.default_rng(gg + 1).uniform(-1, 1, n)
             bh = matgen.matvec(ptr, ind, val, xs)
-            systems[op] = (ptr, ind, val, n, bh, torch.as_tensor(bh, device=dev),
-                           api.RowSparse(n, n, ptr, ind, val), api.JacobiPreconditioner())
-        ptr, ind, val, n, bh, b, A, J = systems[op]
+            systems[(op, gg)] = (ptr, ind, val, n, bh, torch.as_tensor(bh, device=dev),
+                                 api.RowSparse(n, n, ptr, ind, val), api.JacobiPreconditioner())
+        ptr, ind, val, n, bh, b, A, J = systems[(op, gg)]
         def run():
             X = torch.zeros(n, dtype=torch.float64, device=dev)
             it = api.Iteration(20000, 1e-10)
@@ -772,7 +787,7 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
         x = X.cpu().numpy()
         nit = it.GetNumberIteration()
         nbytes = krylov_bytes(which, n, ind.size, True, nit)
-        key = f"{which}_jacobi_{op}{g}"
+        key = f"{which}_jacobi_{op}{gg}"
         out[key] = {"ms": round(ms, 2), "error_code": code, "iterations": nit,
                     "us_per_iteration": round(ms * 1e3 / max(nit, 1), 1),
                     "rel_residual_host_check": float(

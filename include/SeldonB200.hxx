@@ -1599,18 +1599,21 @@ namespace Seldon
       }
     };
 
-    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes };
+    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
       // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110,
-      // TfQmr.cxx:116,138,148,186,219 and MinRes.cxx:120,142 pass to Fail
+      // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142 and Gcr.cxx:108
+      // pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
         return code == 1 ? "Cgs breakdown #1" : "Cgs breakdown #2";
       if (kind == kMinRes)
         return code == 1 ? "Minres breakdown #1" : "MinRes breakdown #2";
+      if (kind == kGcr)
+        return "Gcr breakdown #1";
       if (kind == kTfQmr)
         {
           if (code == 1)
@@ -1677,12 +1680,15 @@ namespace Seldon
         st = sb2_minres(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                         cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                         GetStream());
+      else if (kind == kGcr)
+        st = sb2_gcr(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                     cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
-                                          "MinRes"};
+                                          "MinRes", "Gcr"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1741,6 +1747,8 @@ namespace Seldon
           return Seldon::TfQmr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kMinRes)
           return Seldon::MinRes<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kGcr)
+          return Seldon::Gcr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1849,6 +1857,25 @@ namespace Seldon
              Preconditioner& M, Iteration<Titer>& iter)
   {
     return b200::Solve(b200::kMinRes, A, x, b, M, iter);
+  }
+
+  //! Restarted generalized conjugate residuals on the GPU (Gcr.cxx:45-141).
+  template <class Titer, class Prop, class Preconditioner>
+  int Gcr(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+          Vector<double, VectFull, CudaAlloc<double> >& x,
+          const Vector<double, VectFull, CudaAlloc<double> >& b,
+          Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGcr, A, x, b, M, outer);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int Gcr(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+          Vector<double, VectFull, CudaAlloc<double> >& x,
+          const Vector<double, VectFull, CudaAlloc<double> >& b,
+          Preconditioner& M, Iteration<Titer>& outer)
+  {
+    return b200::Solve(b200::kGcr, A, x, b, M, outer);
   }
 
   //! Restarted left-preconditioned GMRES(m) on the GPU (Gmres.cxx:44-183).

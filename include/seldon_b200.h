@@ -433,6 +433,20 @@ int sb2_minres(const sb2_csr* A, const sb2_precond* M, double* x,
                sb2_iter_result* result, double* hist, int* hist_it,
                int hist_cap, void* stream);
 
+/* Seldon's Gcr (Gcr.cxx:45-141): restarted generalized conjugate residuals,
+ * left preconditioned, restart m = params->restart; arguments, history and
+ * error codes of sb2_cg (code 1 for its breakdown; like the reference, a
+ * breakdown ends only the current cycle).  Every cycle logs the outer and
+ * the inner Finished() test, as the reference's two Iteration objects do.
+ * Where the reference never returns -- a cycle that takes no step (a
+ * breakdown at its first product, or m = 0), which every later cycle then
+ * repeats -- the solve stops after that cycle.  The identity and Jacobi
+ * with m <= 16 run as one persistent kernel per solve; larger restarts, SOR
+ * and ILUT drive the device operations from the host. */
+int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+            const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+            int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it
@@ -456,7 +470,7 @@ int sb2_gmres_cgs2(const sb2_csr* A, const sb2_precond* M, double* x,
  * plugin hosts that forbid libraries to allocate.  Such a caller creates the
  * matrix beforehand and passes x and b (device memory it owns).
  * The work vectors live in a fixed array inside this library, sized for
- * n <= 131072 rows (about 3.2 MB, held on every GPU that loads the library
+ * n <= 131072 rows (about 3.3 MB, held on every GPU that loads the library
  * until the process exits); larger systems are rejected with
  * SB2_ERR_INVALID_VALUE.  The first call on a device looks up that array's
  * device address, so make it before any stream capture.  The address is

@@ -9,6 +9,8 @@
 //   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
 //   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
 //   Cgs / TfQmr / MinRes    computation/solver/iterative/{Cgs,TfQmr,MinRes}.cxx
+//   Gcr                     computation/solver/iterative/Gcr.cxx (never with an
+//                           input where it cannot return: see orc_gcr_impl)
 //   SOR                     matrix_sparse/Relaxation_MatVect.cxx:41-95, 176-298
 //   SorPreconditioner       computation/solver/preconditioner/Precond_Ssor.cxx:24-90
 //
@@ -126,6 +128,7 @@ namespace
       case 3: return Cgs(A, x, b, M, it);
       case 4: return TfQmr(A, x, b, M, it);
       case 5: return MinRes(A, x, b, M, it);
+      case 6: return Gcr(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -364,7 +367,7 @@ extern "C"
     return 0;
   }
 
-  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes.  precond:
+  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes, 6 Gcr.  precond:
   // 0 identity, 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,

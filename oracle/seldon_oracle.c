@@ -785,8 +785,74 @@ out:
   return code;
 }
 
+/* Gcr(m), computation/solver/iterative/Gcr.cxx:45-141.  Restarted
+ * generalized conjugate residuals, left preconditioned, the test on
+ * ||M^{-1}(b - A x)|| / ||b||.  Each cycle runs an inner Iteration copied
+ * from the outer one (Iterative.cxx:114-124) whose limit is the outer count
+ * plus m; both test the same residual, and both tests are logged.  Where
+ * the reference never returns -- a cycle whose inner loop takes no step (a
+ * breakdown at its first product, or m = 0), after which every cycle
+ * repeats it -- this stops after that cycle. */
+static int orc_gcr_impl(const orc_csr* A, double* x, const double* b,
+                        const orc_prec* M, orc_iter* outer, int m) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  if (it_init(outer, N, b) != 0) return it_error_code(outer);
+  size_t bytes = (size_t)N * sizeof(double);
+  const int nm = m > 0 ? m : 0;
+  double* P = calloc((size_t)(nm + 1) * N, sizeof(double));
+  double* Wv = calloc((size_t)(nm + 1) * N, sizeof(double));
+  double* beta = calloc((size_t)(nm + 1), sizeof(double));
+  double *r = malloc(bytes), *q = malloc(bytes), *u = malloc(bytes);
+  memcpy(r, b, bytes); memcpy(q, b, bytes); memcpy(u, b, bytes);
+  orc_copy(N, b, u);
+  if (!outer->init_guess_null)
+    csr_residual(A, x, u);
+  else
+    memset(x, 0, bytes);
+  prec_solve(M, A, u, r);
+  double alpha, delta, normr = orc_nrm2(N, r);
+  outer->nb_iter = 0;
+  while (!it_finished(outer, orc_nrm2(N, r))) {
+    orc_iter inner = *outer;
+    inner.max_iter = outer->nb_iter + m;
+    orc_copy(N, r, P);
+    orc_scal(N, 1.0 / normr, P);
+    int j = 0;
+    while (!it_finished(&inner, orc_nrm2(N, r))) {
+      double *pj = P + (size_t)j * N, *wj = Wv + (size_t)j * N;
+      csr_mlt(A, pj, u);
+      prec_solve(M, A, u, wj);
+      beta[j] = orc_dot(N, wj, wj);
+      if (beta[j] == 0.0) { it_fail(outer, 1); break; }
+      alpha = orc_dot(N, wj, r) / beta[j];
+      orc_axpy(N, alpha, pj, x);
+      orc_axpy(N, -alpha, wj, r);
+      inner.nb_iter++;
+      outer->nb_iter++;
+      csr_mlt(A, r, u);
+      prec_solve(M, A, u, q);
+      double* pn = P + (size_t)(j + 1) * N;
+      orc_copy(N, r, pn);
+      for (int i = 0; i <= j; i++) {
+        delta = -orc_dot(N, Wv + (size_t)i * N, q) / beta[i];
+        orc_axpy(N, delta, P + (size_t)i * N, pn);
+      }
+      inner.nb_iter++;
+      outer->nb_iter++;
+      j++;
+    }
+    outer->hist_len = inner.hist_len;
+    if (j == 0) break; /* the reference would repeat this cycle for ever */
+    normr = orc_nrm2(N, r);
+  }
+  int code = it_error_code(outer);
+  free(P); free(Wv); free(beta); free(r); free(q); free(u);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes.
+ * 5 MinRes, 6 Gcr.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -821,6 +887,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_tfqmr_impl(&A, x, b, &M, &it);
   else if (which == 5)
     code = orc_minres_impl(&A, x, b, &M, &it);
+  else if (which == 6)
+    code = orc_gcr_impl(&A, x, b, &M, &it, restart);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

@@ -947,6 +947,13 @@ def MinRes(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_minres, A, x, b, M, iteration, hist_cap, stream)
 
 
+def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Restarted generalized conjugate residuals (Gcr.cxx:45-141), left
+    preconditioned, restart iteration.GetRestart(); returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
+
+
 def Gmres(A, x, b, M, iteration, hist_cap=None, stream=None, orthogonalization="mgs"):
     """Restarted left-preconditioned GMRES(m) (Gmres.cxx:44-183).
 

@@ -10,12 +10,13 @@
 //
 // SOR and ILUT preconditioning (level-scheduled sweeps, many dependent
 // launches) of Cg, BiCgStab and Gmres run as device-resident chains around the
-// sweeps (chain.cu); Cgs, TfQmr and MinRes with them, and every driver when
-// those chains are switched off, go through a host-driven driver over the same
-// device kernels, one operation at a time, in the reference's order.
+// sweeps (chain.cu); Cgs, TfQmr, MinRes and Gcr with them, and every driver
+// when those chains are switched off, go through a host-driven driver over the
+// same device kernels, one operation at a time, in the reference's order.
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
-// Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Iterative.cxx:235-354.
+// Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
+// Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -1244,6 +1245,232 @@ __global__ void __launch_bounds__(NT, 4) minres_fused_kernel(OpArgs A, MinresVec
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- GCR
+
+// Largest restart the persistent Gcr takes: a step reduces ceil(m / 2)
+// projections in one barrier, at most kMaxRed.
+constexpr int kGcrMaxRestart = 2 * kMaxRed;
+
+struct GcrVecs {
+  const double* b;
+  double *x, *r;
+  double* P;  // p_0 .. p_m, `ld` apart
+  double* W;  // w_0 .. w_m
+  long long ld;
+};
+
+// epilogue of the initial residual: r = M^{-1}(b - A x), with ||r||^2
+struct EpiPrecResidual {
+  const double* b;
+  double* r;
+  const double* diag;
+  double rr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double ri = precond_val(diag, i, add_rn(__ldg(b + i), -t));
+    r[i] = ri;
+    rr = add_rn(rr, mul_rn(ri, ri));
+  }
+};
+
+// epilogue of w_j = M^{-1} A p_j: (w_j, w_j) and (w_j, r)
+struct EpiGcrW {
+  double* w;
+  const double* r;
+  const double* diag;
+  double ww, wr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double wi = precond_val(diag, i, t);
+    w[i] = wi;
+    ww = add_rn(ww, mul_rn(wi, wi));
+    wr = add_rn(wr, mul_rn(wi, __ldcg(r + i)));
+  }
+};
+
+// epilogue of q = M^{-1} A r: the projections (w_k, q), k < nd; q itself is
+// never stored
+struct EpiGcrQ {
+  const double* W;
+  long long ld;
+  const double* diag;
+  int nd;
+  double acc[kMaxRed];
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double qi = precond_val(diag, i, t);
+#pragma unroll
+    for (int k = 0; k < kMaxRed; k++)
+      if (k < nd) acc[k] = add_rn(acc[k], mul_rn(__ldcg(W + k * ld + i), qi));
+  }
+};
+
+// Gcr(m) (Gcr.cxx:45-141), left preconditioned.  An inner step takes two
+// products and four grid barriers: w_j = M^{-1} A p_j with (w_j, w_j) and
+// (w_j, r); the x and r updates with ||r||^2; q = M^{-1} A r with the j + 1
+// projections (w_i, q); then p_{j+1} = r + sum_i delta_i p_i.  The outer and
+// the inner Iteration test the same residual, and both tests are logged, as
+// the reference's two Finished() calls are.  Where the reference never
+// returns -- a cycle whose inner loop takes no step, which every later cycle
+// then repeats -- the solve stops after that cycle.
+__global__ void __launch_bounds__(NT, 4) gcr_fused_kernel(OpArgs A, GcrVecs v, IterArgs it,
+                                                       Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  __shared__ double s_beta[kGcrMaxRestart + 1];
+  __shared__ double s_delta[kMaxRed];
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const int m = it.restart;
+  const long long ld = v.ld;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  // outer.Init(b)
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // u = b - A x (or x = 0, u = b); r = M^{-1} u; ||r||^2
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      const double ri = precond_val(A.diag, (int)i, __ldg(v.b + i));
+      v.r[i] = ri;
+      rr = add_rn(rr, mul_rn(ri, ri));
+    }
+  } else {
+    EpiPrecResidual epi{v.b, v.r, A.diag, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double normr = sqrt(rr);
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    // outer.Finished(r)
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    const int inner_max = nb_iter + m;
+    // Copy(r, p_0); Mlt(1 / normr, p_0)
+    {
+      const double inv = 1.0 / normr;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int Wd = decltype(wc)::value;
+        Ents<Wd> ri = ldw<Wd>(v.r, i);
+#pragma unroll
+        for (int k = 0; k < Wd; k++) ri.v[k] = mul_rn(ri.v[k], inv);
+        stw<Wd>(v.P, i, ri);
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    int j = 0;
+    for (;;) {
+      // inner.Finished(r)
+      reste = facteur * sqrt(rr);
+      if (lead) hist_push(H, &hlen, nb_iter, reste);
+      if (reste < it.tol || nb_iter >= inner_max) break;
+      double* pj = v.P + (long long)j * ld;
+      double* wj = v.W + (long long)j * ld;
+      // w_j = M^{-1} A p_j; beta_j = (w_j, w_j); (w_j, r)
+      {
+        EpiGcrW epi{wj, v.r, A.diag, 0.0, 0.0};
+        spmv_phase(A, pj, epi, s_prod, s_red);
+        const double ww = block_sum<NT>(epi.ww, s_red);
+        const double wr = block_sum<NT>(epi.wr, s_red);
+        if (tid == 0) { s_vals[0] = ww; s_vals[1] = wr; }
+        if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      }
+      const double beta_j = s_vals[0];
+      if (beta_j == 0.0) { fail = 1; break; }
+      if (tid == 0) s_beta[j] = beta_j;
+      const double alpha = s_vals[1] / beta_j;
+      // Add(alpha, p_j, x); Add(-alpha, w_j, r); ||r||^2
+      {
+        double a = 0.0;
+        vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+          constexpr int Wd = decltype(wc)::value;
+          if (alpha != 0.0) {
+            Ents<Wd> xi = ldw<Wd>(v.x, i);
+            const Ents<Wd> pi = ldw<Wd>(pj, i);
+#pragma unroll
+            for (int k = 0; k < Wd; k++) xi.v[k] = add_rn(xi.v[k], mul_rn(alpha, pi.v[k]));
+            stw<Wd>(v.x, i, xi);
+          }
+          Ents<Wd> ri = ldw<Wd>(v.r, i);
+          if (-alpha != 0.0) {
+            const Ents<Wd> wi = ldw<Wd>(wj, i);
+#pragma unroll
+            for (int k = 0; k < Wd; k++) ri.v[k] = add_rn(ri.v[k], mul_rn(-alpha, wi.v[k]));
+            stw<Wd>(v.r, i, ri);
+          }
+#pragma unroll
+          for (int k = 0; k < Wd; k++) a = add_rn(a, mul_rn(ri.v[k], ri.v[k]));
+        });
+        a = block_sum<NT>(a, s_red);
+        if (tid == 0) s_vals[0] = a;
+        if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+        rr = s_vals[0];
+      }
+      nb_iter++;
+      // q = M^{-1} A r; delta_i = -(w_i, q) / beta_i
+      const int nd = j + 1;
+      {
+        EpiGcrQ epi{v.W, ld, A.diag, nd, {}};
+        spmv_phase(A, v.r, epi, s_prod, s_red);
+#pragma unroll
+        for (int k = 0; k < kMaxRed; k++)
+          if (k < nd) {
+            const double d = block_sum<NT>(epi.acc[k], s_red);
+            if (tid == 0) s_vals[k] = d;
+          }
+        if (!grid_sync<NT>(P, epoch, nd, s_vals, s_red)) return;
+      }
+      if (tid < nd) s_delta[tid] = -s_vals[tid] / s_beta[tid];
+      __syncthreads();
+      // Copy(r, p_{j+1}); Add(delta_i, p_i, p_{j+1}) for i = 0..j
+      {
+        double* pn = v.P + (long long)(j + 1) * ld;
+        vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+          constexpr int Wd = decltype(wc)::value;
+          Ents<Wd> pv = ldw<Wd>(v.r, i);
+          for (int k = 0; k < nd; k++) {
+            const double dk = s_delta[k];
+            if (dk != 0.0) {
+              const Ents<Wd> pk = ldw<Wd>(v.P + (long long)k * ld, i);
+#pragma unroll
+              for (int q = 0; q < Wd; q++) pv.v[q] = add_rn(pv.v[q], mul_rn(dk, pk.v[q]));
+            }
+          }
+          stw<Wd>(pn, i, pv);
+        });
+        if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+      }
+      nb_iter++;
+      j++;
+    }
+    if (j == 0) break;  // the reference would repeat this cycle for ever
+    normr = sqrt(rr);
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -1550,7 +1777,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
                 sell_op(f)};
 }
 
-enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5 };
+enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
@@ -1565,6 +1792,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kCgs) { kern = (const void*)cgs_fused_kernel; nvec = 8; }
   if (which == kTfqmr) { kern = (const void*)tfqmr_fused_kernel; nvec = 8; }
   if (which == kMinres) { kern = (const void*)minres_fused_kernel; nvec = 9; }
+  if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -1582,7 +1810,8 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   SB2_TRY(alloc_scratch(s, n, nvec, grid, hcap, &S));
   Persist P{S.sync, S.partials, barrier_wait_ns()};
   History H{S.hist, S.hist_it, hcap};
-  IterArgs it{prm->tol, prm->max_iter, m, prm->init_guess_null};
+  IterArgs it{prm->tol, prm->max_iter, which == kGcr ? std::max(prm->restart, 0) : m,
+              prm->init_guess_null};
   OpArgs op = op_args(A, diag);
   const size_t nn = vector_stride(n, sizeof(double));
   double* V = S.vec;
@@ -1593,6 +1822,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   CgsVecs sv;
   TfqmrVecs tv;
   MinresVecs mv;
+  GcrVecs rv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -1617,6 +1847,10 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     mv = MinresVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                     V + 7 * nn, V + 8 * nn};
     args[1] = &mv;
+  } else if (which == kGcr) {
+    const int mg = std::max(prm->restart, 0);
+    rv = GcrVecs{b, x, V, V + nn, V + (size_t)(mg + 2) * nn, (long long)nn};
+    args[1] = &rv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -1655,7 +1889,11 @@ struct Ops {
     SB2_TRY(copy(b, r));
     return sb2_spmv(A, 0, -1.0, x, 1.0, r, s);
   }
-  int prec(const double* r, double* z) { return precond_apply(M, false, r, z, s); }
+  // no handle is the identity (Preconditioner_Base::Solve is a Copy): Gcr
+  // with a restart above the persistent kernel's reaches this loop with it
+  int prec(const double* r, double* z) {
+    return M ? precond_apply(M, false, r, z, s) : copy(r, z);
+  }
 };
 
 static int host_cg(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
@@ -1941,6 +2179,64 @@ static int host_minres(Ops& o, double* x, const double* b, const sb2_iter_params
   return SB2_OK;
 }
 
+static int host_gcr(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                    HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  const int m = std::max(prm->restart, 0);
+  double *r = V, *q = V + n, *u = V + 2 * n, *Pv = V + 3 * n, *Wv = V + (size_t)(m + 4) * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, u));
+  else { SB2_TRY(o.copy(b, u)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.prec(u, r));
+  std::vector<double> beta(m + 1, 0.0);
+  double normr, res;
+  SB2_TRY(o.nrm(r, &normr));
+  for (;;) {
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    HostIter inner = it;
+    inner.max_iter = it.nb_iter + m;
+    SB2_TRY(o.copy(r, Pv));
+    SB2_TRY(o.scal(1.0 / normr, Pv));
+    int j = 0;
+    for (;;) {
+      SB2_TRY(o.nrm(r, &res));
+      if (inner.finished(res)) break;
+      double *pj = Pv + (size_t)j * n, *wj = Wv + (size_t)j * n;
+      SB2_TRY(o.mlt(pj, u));
+      SB2_TRY(o.prec(u, wj));
+      SB2_TRY(o.dot(wj, wj, &beta[j]));
+      if (beta[j] == 0.0) { it.fail = 1; break; }
+      double wr;
+      SB2_TRY(o.dot(wj, r, &wr));
+      const double alpha = wr / beta[j];
+      SB2_TRY(o.axpy(alpha, pj, x));
+      SB2_TRY(o.axpy(-alpha, wj, r));
+      inner.nb_iter++;
+      it.nb_iter++;
+      SB2_TRY(o.mlt(r, u));
+      SB2_TRY(o.prec(u, q));
+      double* pn = Pv + (size_t)(j + 1) * n;
+      SB2_TRY(o.copy(r, pn));
+      for (int i = 0; i <= j; i++) {
+        double d;
+        SB2_TRY(o.dot(Wv + (size_t)i * n, q, &d));
+        SB2_TRY(o.axpy(-d / beta[i], Pv + (size_t)i * n, pn));
+      }
+      inner.nb_iter++;
+      it.nb_iter++;
+      j++;
+    }
+    it.hist = inner.hist;
+    if (j == 0) break;  // the reference would repeat this cycle for ever
+    SB2_TRY(o.nrm(r, &normr));
+  }
+  return SB2_OK;
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -2047,6 +2343,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kCgs ? 9
                    : which == kTfqmr ? 10
                    : which == kMinres ? 9
+                   : which == kGcr ? 3 + 2 * (std::max(prm->restart, 0) + 1)
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -2062,6 +2359,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kCgs) SB2_TRY(host_cgs(o, x, b, prm, it, V, &init_failed));
   else if (which == kTfqmr) SB2_TRY(host_tfqmr(o, x, b, prm, it, V, &init_failed));
   else if (which == kMinres) SB2_TRY(host_minres(o, x, b, prm, it, V, &init_failed));
+  else if (which == kGcr) SB2_TRY(host_gcr(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -2502,6 +2800,9 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
     return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which);
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
+  // a Gcr step reduces ceil(m / 2) projections in one barrier
+  if (which == kGcr && prm->restart > kGcrMaxRestart)
+    return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;
   if (kind == SB2_PRECOND_JACOBI) {
     SB2_TRY(ensure_diag(A));
@@ -2596,6 +2897,14 @@ int sb2_minres(const sb2_csr* A, const sb2_precond* M, double* x, const double* 
                int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_minres");
   return solve_entry(kMinres, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+            const sb2_iter_params* params, sb2_iter_result* result, double* hist, int* hist_it,
+            int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_gcr");
+  return solve_entry(kGcr, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

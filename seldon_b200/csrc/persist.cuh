@@ -11,7 +11,7 @@
 
 namespace sb2 {
 
-constexpr int kMaxRed = 4;  // scalars reduced by one barrier at most
+constexpr int kMaxRed = 8;  // scalars reduced by one barrier at most
 
 struct GridSync {
   unsigned count;  // arrivals at the current barrier

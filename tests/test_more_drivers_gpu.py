@@ -1,7 +1,7 @@
-"""Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243) and MinRes
-(MinRes.cxx:46-153) on the device against the oracle's restatements, which
-are pinned bit for bit to the reference's own templates
-(tests/test_oracle_pin.py).
+"""Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243), MinRes
+(MinRes.cxx:46-153) and Gcr (Gcr.cxx:45-141) on the device against the
+oracle's restatements, which are pinned bit for bit to the reference's own
+templates (tests/test_oracle_pin.py).
 
 The identity and Jacobi run the persistent kernels; SOR and ILUT the
 host-driven loop over the device operations.  Reductions are summed in
@@ -19,7 +19,7 @@ from tests.test_oracle_pin import _edge_solves, _nonfinite_cases, shifted_laplac
 
 pytestmark = pytest.mark.gpu
 
-SOLVERS = ["cgs", "tfqmr", "minres"]
+SOLVERS = ["cgs", "tfqmr", "minres", "gcr"]
 
 
 @pytest.fixture(scope="module")
@@ -29,7 +29,7 @@ def api(cuda):
 
 
 def _fn(api, which):
-    return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes}[which]
+    return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes, "gcr": api.Gcr}[which]
 
 
 def _precond(api, pc):
@@ -47,11 +47,12 @@ def _matrix(api, A, sym):
     return api.RowSymSparse(n, *A) if sym else api.RowSparse(n, n, *A)
 
 
-def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000):
+def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000, restart=10):
     n = A[0].size - 1
     M = _matrix(api, A, sym)
     X = to_dev(np.zeros(n) if x0 is None else x0)
     it = api.Iteration(max_iter, tol)
+    it.SetRestart(restart)
     it.HideMessages()
     if x0 is not None:
         it.SetInitGuess(False)
@@ -61,7 +62,7 @@ def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000):
 
 # MinRes wants symmetric systems: the Laplacian, and the Laplacian shifted
 # to be indefinite (its case), in both storages
-CASES = ([(w, m, pc) for w in ("cgs", "tfqmr") for m in ("conv", "lap", "lap_up")
+CASES = ([(w, m, pc) for w in ("cgs", "tfqmr", "gcr") for m in ("conv", "lap", "lap_up")
           for pc in (0, 1, 2)] +
          [("minres", m, pc) for m in ("lap", "lap_up", "indef", "indef_up") for pc in (0, 1, 2)])
 
@@ -172,7 +173,7 @@ def test_deterministic_and_larger(api, oracle, which):
     assert np.linalg.norm(outs[0][2] - xo) / np.linalg.norm(xo) < 1e-7
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr"])
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "gcr"])
 def test_ilut(api, reference, which):
     # the host-driven loop with the device ILUT apply against the reference's
     # driver with its own factor
@@ -234,3 +235,44 @@ def test_minres_breakdown_and_estimate(api, oracle):
     assert its == list(range(it.GetNumberIteration() + 1))
     k = min(len(its), len(hio)) - 2
     np.testing.assert_allclose([r for _, r in it.history][:k], ho[:k], rtol=1e-6)
+
+
+# Gcr: restarts the persistent kernel takes (a step reduces ceil(m / 2)
+# projections in one barrier, m <= 16) and one it hands to the host loop
+@pytest.mark.parametrize("restart", [1, 4, 16, 24])
+@pytest.mark.parametrize("pc", [0, 1])
+def test_gcr_restarts(api, oracle, restart, pc):
+    full = matgen.convdiff3d(9)
+    n = full[0].size - 1
+    b = matgen.matvec(*full, np.random.default_rng(6).uniform(-1, 1, n))
+    xo, co, no, ho, hio = oracle.solve("gcr", *full, b, precond=pc, tol=1e-10, max_iter=3000,
+                                       restart=restart, hist_cap=20000)
+    code, it, x = _solve(api, "gcr", full, False, b, pc, max_iter=3000, restart=restart)
+    assert code == co == 0
+    nb = it.GetNumberIteration()
+    assert abs(nb - no) <= max(2, int(0.05 * no)), (nb, no)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7
+    # both Finished() tests of every cycle are logged
+    its = [i for i, _ in it.history]
+    k = min(len(its), len(hio)) - 4
+    assert its[:k] == hio[:k].tolist()
+
+
+def test_gcr_no_step_stops(api, oracle):
+    """Where the reference never returns (a cycle that takes no step), the
+    device stops after that cycle, as the oracle does: a singular 1 x 1
+    system breaks down at the first product (code 1); restart 0 takes no
+    step (code 0, x left as it started)."""
+    A = api.RowSparse(1, 1, np.array([0, 1]), np.array([0]), np.array([0.0]))
+    it = api.Iteration(50, 1e-10)
+    it.HideMessages()
+    X = to_dev(np.zeros(1))
+    assert api.Gcr(A, X, to_dev(np.array([1.0])), api.Preconditioner_Base(), it) == 1
+    assert it.GetNumberIteration() == 0
+    ptr, ind, val = matgen.lap2d(4)
+    code, it, x = _solve(api, "gcr", (ptr, ind, val), False, np.ones(16), 0, max_iter=50,
+                         restart=0)
+    _, co, no, ho, _ = oracle.solve("gcr", ptr, ind, val, np.ones(16), tol=1e-10, max_iter=50,
+                                    restart=0, hist_cap=10)
+    assert (code, it.GetNumberIteration()) == (co, no) == (0, 0)
+    assert not x.any() and len(it.history) == len(ho) == 2

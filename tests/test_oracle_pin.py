@@ -99,7 +99,7 @@ def test_mltadd_live(reference, oracle, seed):
                           reference.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True))
 
 
-@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres"])
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
     ptr, ind, val = matgen.convdiff3d(5) if which not in ("cg", "minres") else matgen.lap2d(15)
@@ -161,6 +161,32 @@ def _edge_solves():
     return out
 
 
+@pytest.mark.parametrize("restart", [1, 2, 5, 16, 24])
+def test_gcr_restarts_live(reference, oracle, restart):
+    ptr, ind, val = matgen.convdiff3d(6)
+    b = np.random.default_rng(5).uniform(-1, 1, ptr.size - 1)
+    for pc in (0, 1):
+        xo, co, no, _, _ = oracle.solve("gcr", ptr, ind, val, b, precond=pc, tol=1e-10,
+                                        max_iter=600, restart=restart)
+        xr, cr, nr = reference.solve("gcr", ptr, ind, val, b, precond=pc, tol=1e-10,
+                                     max_iter=600, restart=restart)
+        assert (co, no) == (cr, nr)
+        assert np.array_equal(xo, xr)
+
+
+def test_gcr_no_step_stops(oracle):
+    """Where the reference's Gcr never returns (a cycle that takes no step:
+    a breakdown at its first product, or restart 0), the restatement stops
+    after that cycle.  Never run on the reference."""
+    one = (np.array([0, 1], dtype=np.int32), np.array([0], dtype=np.int32), np.array([0.0]))
+    _, code, nb, _, _ = oracle.solve("gcr", *one, np.array([1.0]), tol=1e-10, max_iter=50)
+    assert (code, nb) == (1, 0)
+    ptr, ind, val = matgen.lap2d(4)
+    x, code, nb, h, _ = oracle.solve("gcr", ptr, ind, val, np.ones(16), tol=1e-10, max_iter=50,
+                                     restart=0, hist_cap=10)
+    assert (code, nb) == (0, 0) and not x.any() and len(h) == 2
+
+
 def shifted_laplacian(g, sigma):
     """The g x g Laplacian minus sigma I: symmetric indefinite for sigma
     above its smallest eigenvalue (MinRes's case)."""
@@ -185,7 +211,7 @@ def test_minres_indefinite_live(reference, oracle, pc, sym):
     assert np.array_equal(xo, xr)
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres"])
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
@@ -309,7 +335,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
             assert np.array_equal(xo, xr, equal_nan=True)
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
-    for which in ("cgs", "tfqmr", "minres"):
+    for which in ("cgs", "tfqmr", "minres", "gcr"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
