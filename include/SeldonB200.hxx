@@ -1599,13 +1599,16 @@ namespace Seldon
       }
     };
 
-    enum SolverKind { kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr };
+    enum SolverKind
+    {
+      kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl
+    };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
       // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110,
-      // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142 and Gcr.cxx:108
-      // pass to Fail
+      // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108 and
+      // BiCgStabl.cxx:99,115 pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
@@ -1614,6 +1617,8 @@ namespace Seldon
         return code == 1 ? "Minres breakdown #1" : "MinRes breakdown #2";
       if (kind == kGcr)
         return "Gcr breakdown #1";
+      if (kind == kBiCgStabl)
+        return code == 1 ? "Bicgstabl breakdown #1" : "Bicgstabl Breakdown #2";
       if (kind == kTfQmr)
         {
           if (code == 1)
@@ -1683,12 +1688,16 @@ namespace Seldon
       else if (kind == kGcr)
         st = sb2_gcr(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                      cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kBiCgStabl)
+        st = sb2_bicgstabl(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                           cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
+                           GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
-                                          "MinRes", "Gcr"};
+                                          "MinRes", "Gcr", "BiCgStabl"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1749,6 +1758,8 @@ namespace Seldon
           return Seldon::MinRes<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kGcr)
           return Seldon::Gcr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kBiCgStabl)
+          return Seldon::BiCgStabl<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1876,6 +1887,25 @@ namespace Seldon
           Preconditioner& M, Iteration<Titer>& outer)
   {
     return b200::Solve(b200::kGcr, A, x, b, M, outer);
+  }
+
+  //! BiCGSTAB(l) on the GPU, l = iter.GetRestart() (BiCgStabl.cxx:43-180).
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCgStabl(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+                Vector<double, VectFull, CudaAlloc<double> >& x,
+                const Vector<double, VectFull, CudaAlloc<double> >& b,
+                Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCgStabl, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCgStabl(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+                Vector<double, VectFull, CudaAlloc<double> >& x,
+                const Vector<double, VectFull, CudaAlloc<double> >& b,
+                Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCgStabl, A, x, b, M, iter);
   }
 
   //! Restarted left-preconditioned GMRES(m) on the GPU (Gmres.cxx:44-183).

@@ -447,6 +447,21 @@ int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
             int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's BiCgStabl (BiCgStabl.cxx:43-180): BiCGSTAB(l) with l =
+ * params->restart >= 1 (l = 0 gives SB2_ERR_INVALID_VALUE: the reference
+ * reads past its gamma vector there), right preconditioning (x is mapped
+ * back by M^{-1} at the end, as the reference does); arguments, history and
+ * error codes of sb2_cg (codes 1 and 2; like the reference, a breakdown
+ * ends only the BiCG part of the cycle).  Where the reference can repeat a
+ * cycle for ever (one that counts no iteration) the solve stops after it.
+ * The identity and Jacobi with l <= 16 run as one persistent kernel per
+ * solve; larger l, SOR and ILUT drive the device operations from the
+ * host. */
+int sb2_bicgstabl(const sb2_csr* A, const sb2_precond* M, double* x,
+                  const double* b, const sb2_iter_params* params,
+                  sb2_iter_result* result, double* hist, int* hist_it,
+                  int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

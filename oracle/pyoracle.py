@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libseldon_ref.so")
 # the `which` numbers of orc_solve / ref_solve
-_SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "cgs": 3, "tfqmr": 4, "minres": 5, "gcr": 6}
+_SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "cgs": 3, "tfqmr": 4, "minres": 5, "gcr": 6,
+            "bicgstabl": 7}
 REF_FAST_SO = os.path.join(HERE, "_ref", "libseldon_ref_fast.so")
 
 _vp = ctypes.c_void_p
@@ -136,7 +137,8 @@ class Oracle(_Base):
     def solve(self, which, ptr, ind, val, b, x0=None, sym=False, precond=0, omega=1.0,
               sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
               hist_cap=0):
-        """which: 'cg' | 'bicgstab' | 'gmres' | 'cgs' | 'tfqmr' | 'minres' | 'gcr'.  precond: 0 identity, 1 Jacobi, 2 SOR.
+        """which: 'cg' | 'bicgstab' | 'gmres' | 'cgs' | 'tfqmr' | 'minres' | 'gcr' |
+        'bicgstabl'.  precond: 0 identity, 1 Jacobi, 2 SOR.
         Returns (x, error_code, nb_iter, hist, hist_it)."""
         w = _SOLVERS[which]
         ptr, ind, val = _csr_args(ptr, ind, val)

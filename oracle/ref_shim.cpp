@@ -9,8 +9,9 @@
 //   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
 //   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
 //   Cgs / TfQmr / MinRes    computation/solver/iterative/{Cgs,TfQmr,MinRes}.cxx
-//   Gcr                     computation/solver/iterative/Gcr.cxx (never with an
-//                           input where it cannot return: see orc_gcr_impl)
+//   Gcr, BiCgStabl          computation/solver/iterative/{Gcr,BiCgStabl}.cxx
+//                           (never with an input where they cannot return:
+//                           see orc_gcr_impl, orc_bicgstabl_impl)
 //   SOR                     matrix_sparse/Relaxation_MatVect.cxx:41-95, 176-298
 //   SorPreconditioner       computation/solver/preconditioner/Precond_Ssor.cxx:24-90
 //
@@ -129,6 +130,7 @@ namespace
       case 4: return TfQmr(A, x, b, M, it);
       case 5: return MinRes(A, x, b, M, it);
       case 6: return Gcr(A, x, b, M, it);
+      case 7: return BiCgStabl(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -367,8 +369,8 @@ extern "C"
     return 0;
   }
 
-  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes, 6 Gcr.  precond:
-  // 0 identity, 1 Jacobi, 2 SOR.
+  // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes, 6 Gcr,
+  // 7 BiCgStabl.  precond: 0 identity, 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
                 const double* val, int sym, int precond, double omega,

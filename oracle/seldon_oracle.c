@@ -851,8 +851,120 @@ static int orc_gcr_impl(const orc_csr* A, double* x, const double* b,
   return code;
 }
 
+/* BiCgStabl(l), computation/solver/iterative/BiCgStabl.cxx:43-180, with
+ * l = the restart parameter.  Right preconditioning: x gathers u's in the
+ * preconditioned coordinates and is mapped back by M^{-1} at the end; the
+ * test is on ||r_0|| / ||b||, the count advances by two per BiCG step.  A
+ * breakdown ends the BiCG part only; the MR part and the loop go on.  tau
+ * and the gammas carry over from cycle to cycle, as the reference's do.
+ * Where the reference can repeat a cycle for ever -- one that counts no
+ * iteration (a breakdown at the first step) -- this stops after it. */
+static int orc_bicgstabl_impl(const orc_csr* A, double* x, const double* b,
+                              const orc_prec* M, orc_iter* it, int m) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  /* l = 0 reads gamma(1) past the end of a one-entry vector in the
+   * reference: no result to restate */
+  if (m < 1) return -100;
+  const int l = m;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *q = malloc(bytes), *r0 = malloc(bytes);
+  memcpy(q, b, bytes); memcpy(r0, b, bytes);
+  double* R = calloc((size_t)(l + 1) * N, sizeof(double));
+  double* U = calloc((size_t)(l + 1) * N, sizeof(double));
+  double* gamma = calloc((size_t)(l + 1), sizeof(double));
+  double* gamma_p = calloc((size_t)(l + 1), sizeof(double));
+  double* gamma_t = calloc((size_t)(l + 1), sizeof(double));
+  double* tau = calloc((size_t)(l + 1) * (l + 1), sizeof(double));
+#define TAU(i, j) tau[(size_t)(i) * (l + 1) + (j)]
+#define RV(i) (R + (size_t)(i) * N)
+#define UV(i) (U + (size_t)(i) * N)
+  double rho_0, rho_1, alpha, beta, omega, sigma;
+  int code;
+  orc_copy(N, b, RV(0));
+  if (!it->init_guess_null)
+    csr_residual(A, x, RV(0));
+  else
+    memset(x, 0, bytes);
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, RV(0), r0);
+  rho_0 = 1.0; alpha = 0.0; omega = 1.0;
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, RV(0)))) {
+    const int start = it->nb_iter;
+    rho_0 *= -omega;
+    /* Bi-CG part */
+    for (int j = 0; j < l; j++) {
+      rho_1 = orc_dot(N, RV(j), r0);
+      if (rho_0 == 0.0) { it_fail(it, 1); break; }
+      beta = alpha * (rho_1 / rho_0);
+      rho_0 = rho_1;
+      for (int i = 0; i <= j; i++) {
+        orc_scal(N, -beta, UV(i));
+        orc_axpy(N, 1.0, RV(i), UV(i));
+      }
+      prec_solve(M, A, UV(j), q);
+      csr_mlt(A, q, UV(j + 1));
+      it->nb_iter++;
+      sigma = orc_dot(N, UV(j + 1), r0);
+      if (sigma == 0.0) { it_fail(it, 2); break; }
+      alpha = rho_1 / sigma;
+      orc_axpy(N, alpha, UV(0), x);
+      for (int i = 0; i <= j; i++) orc_axpy(N, -alpha, UV(i + 1), RV(i));
+      prec_solve(M, A, RV(j), q);
+      csr_mlt(A, q, RV(j + 1));
+      it->nb_iter++;
+    }
+    /* MR part, modified Gram-Schmidt */
+    for (int j = 1; j <= l; j++) {
+      for (int i = 1; i < j; i++) {
+        if (gamma[i] != 0.0) {
+          TAU(i, j) = orc_dot(N, RV(j), RV(i)) / gamma[i];
+          orc_axpy(N, -TAU(i, j), RV(i), RV(j));
+        }
+      }
+      gamma[j] = orc_dot(N, RV(j), RV(j));
+      if (gamma[j] != 0.0) gamma_p[j] = orc_dot(N, RV(0), RV(j)) / gamma[j];
+    }
+    /* gamma = tau^{-1} gamma' */
+    gamma[l] = gamma_p[l];
+    omega = gamma[l];
+    for (int j = l - 1; j >= 1; j--) {
+      sigma = 0.0;
+      for (int i = j + 1; i <= l; i++) sigma += TAU(j, i) * gamma[i];
+      gamma[j] = gamma_p[j] - sigma;
+    }
+    /* gamma'' = T S gamma */
+    for (int j = 1; j <= l - 1; j++) {
+      sigma = 0.0;
+      for (int i = j + 1; i <= l - 1; i++) sigma += TAU(j, i) * gamma[i + 1];
+      gamma_t[j] = gamma[j + 1] + sigma;
+    }
+    /* update */
+    orc_axpy(N, gamma[1], RV(0), x);
+    orc_axpy(N, -gamma_p[l], RV(l), RV(0));
+    orc_axpy(N, -gamma[l], UV(l), UV(0));
+    for (int j = 1; j <= l - 1; j++) {
+      orc_axpy(N, -gamma[j], UV(j), UV(0));
+      orc_axpy(N, gamma_t[j], RV(j), x);
+      orc_axpy(N, -gamma_p[j], RV(j), RV(0));
+    }
+    if (it->nb_iter == start) break; /* the reference may repeat this for ever */
+  }
+  /* change of coordinates (right preconditioning) */
+  orc_copy(N, x, q);
+  prec_solve(M, A, q, x);
+  code = it_error_code(it);
+out:
+#undef TAU
+#undef RV
+#undef UV
+  free(q); free(r0); free(R); free(U); free(gamma); free(gamma_p); free(gamma_t); free(tau);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -889,6 +1001,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_minres_impl(&A, x, b, &M, &it);
   else if (which == 6)
     code = orc_gcr_impl(&A, x, b, &M, &it, restart);
+  else if (which == 7)
+    code = orc_bicgstabl_impl(&A, x, b, &M, &it, restart);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

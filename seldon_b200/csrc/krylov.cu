@@ -10,13 +10,13 @@
 //
 // SOR and ILUT preconditioning (level-scheduled sweeps, many dependent
 // launches) of Cg, BiCgStab and Gmres run as device-resident chains around the
-// sweeps (chain.cu); Cgs, TfQmr, MinRes and Gcr with them, and every driver
-// when those chains are switched off, go through a host-driven driver over the
-// same device kernels, one operation at a time, in the reference's order.
+// sweeps (chain.cu); the other drivers with them, and every driver when those
+// chains are switched off, go through a host-driven driver over the same
+// device kernels, one operation at a time, in the reference's order.
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
-// Iterative.cxx:235-354.
+// BiCgStabl.cxx:43-180, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -1471,6 +1471,315 @@ __global__ void __launch_bounds__(NT, 4) gcr_fused_kernel(OpArgs A, GcrVecs v, I
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- BICGSTAB(L)
+
+// Largest l of the persistent BiCgStabl: tau and the gammas live in shared
+// memory, (l + 1)^2 + 3(l + 1) doubles.
+constexpr int kBicglMax = 16;
+
+struct BicglVecs {
+  const double* b;
+  double *x, *rt, *q;  // r0 (the shadow residual), M^{-1} of a product's operand
+  double *R, *U;       // r_0 .. r_l and u_0 .. u_l, `ld` apart
+  long long ld;
+};
+
+// epilogue of the initial residual: r_0 = b - A x, r0 = r_0, ||r_0||^2
+struct EpiBiclInit {
+  const double* b;
+  double *r, *rt;
+  double rr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double v = add_rn(__ldg(b + i), -t);
+    r[i] = v;
+    rt[i] = v;
+    rr = add_rn(rr, mul_rn(v, v));
+  }
+};
+
+// BiCgStabl(l) (BiCgStabl.cxx:43-180), l = the restart parameter, right
+// preconditioning.  A cycle: l BiCG steps of two products and four grid
+// barriers each (the u and r updates ride the passes between products,
+// (u_{j+1}, r0) and (r_{j+1}, r0) the products' epilogues), then the MR
+// part's modified Gram-Schmidt over r_1 .. r_l (each axpy fused with the
+// next dot), the small triangular solves for the gammas (every CTA the same,
+// thread 0 into shared memory), and one update pass that also reduces the
+// next test's ||r_0||^2 and (r_0, r0).  A breakdown ends the BiCG part only,
+// as in the reference; tau and the gammas carry over between cycles.  x is
+// mapped back by M^{-1} at the end.  Where the reference can repeat a cycle
+// for ever (one that counts no iteration) the solve stops after it.
+__global__ void __launch_bounds__(NT, 4) bicgstabl_fused_kernel(OpArgs A, BicglVecs v,
+                                                             IterArgs it, Persist P, History H,
+                                                             SolveOut* out) {
+  SB2_SHARED_DECL;
+  __shared__ double s_tau[(kBicglMax + 1) * (kBicglMax + 1)];
+  __shared__ double s_g[kBicglMax + 1], s_gp[kBicglMax + 1], s_gt[kBicglMax + 1];
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const int l = it.restart;
+  const int L1 = l + 1;
+  const long long ld = v.ld;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  const bool jac = (A.diag != nullptr);
+  unsigned epoch = 0;
+  int hlen = 0;
+  auto Rv = [&](int i) { return v.R + (long long)i * ld; };
+  auto Uv = [&](int i) { return v.U + (long long)i * ld; };
+
+  for (int k = tid; k < L1 * L1; k += NT) s_tau[k] = 0.0;
+  for (int k = tid; k < L1; k += NT) s_g[k] = s_gp[k] = s_gt[k] = 0.0;
+  // r_1..r_l and u_0..u_l start at zero; x = 0 for a null guess; ||b||
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+    if (it.init_guess_null) v.x[i] = 0.0;
+    for (int k = 0; k <= l; k++) {
+      if (k > 0) Rv(k)[i] = 0.0;
+      Uv(k)[i] = 0.0;
+    }
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  // iter.Init(b) comes after r_0 in the reference; r_0 is not observable
+  // when it fails, x (zeroed for a null guess) is
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+  // r_0 = b - A x (or b); r0 = r_0
+  double rr = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double bi = __ldg(v.b + i);
+      Rv(0)[i] = bi;
+      v.rt[i] = bi;
+      rr = add_rn(rr, mul_rn(bi, bi));
+    }
+  } else {
+    EpiBiclInit epi{v.b, Rv(0), v.rt, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    rr = epi.rr;
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double rho_next = rr;  // (r_0, r0) with r0 = r_0
+  double rho_0 = 1.0, alpha = 0.0, omega = 1.0;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    const int start = nb_iter;
+    rho_0 = mul_rn(rho_0, -omega);
+    // Bi-CG part
+    for (int j = 0; j < l; j++) {
+      const double rho_1 = rho_next;  // (r_j, r0)
+      if (rho_0 == 0.0) { fail = 1; break; }
+      const double beta = mul_rn(alpha, rho_1 / rho_0);
+      rho_0 = rho_1;
+      // u_i = r_i - beta u_i (Mlt(-beta, u_i); Add(1, r_i, u_i)), i <= j;
+      // q = M^{-1} u_j
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        for (int k = 0; k <= j; k++) {
+          Ents<W> u = ldw<W>(Uv(k), i);
+          const Ents<W> r = ldw<W>(Rv(k), i);
+#pragma unroll
+          for (int e = 0; e < W; e++) u.v[e] = add_rn(mul_rn(u.v[e], -beta), r.v[e]);
+          stw<W>(Uv(k), i, u);
+          if (jac && k == j) stw<W>(v.q, i, precond_w<W>(A.diag, i, u));
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+      // u_{j+1} = A q; sigma = (u_{j+1}, r0)
+      {
+        EpiStoreDot epi{Uv(j + 1), v.rt, 0.0};
+        spmv_phase(A, jac ? v.q : Uv(j), epi, s_prod, s_red);
+        const double d = block_sum<NT>(epi.acc, s_red);
+        if (tid == 0) s_vals[0] = d;
+        if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+      }
+      nb_iter++;
+      const double sigma = s_vals[0];
+      if (sigma == 0.0) { fail = 2; break; }
+      alpha = rho_1 / sigma;
+      // Add(alpha, u_0, x); Add(-alpha, u_{i+1}, r_i), i <= j; q = M^{-1} r_j
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        if (alpha != 0.0) {
+          Ents<W> xi = ldw<W>(v.x, i);
+          const Ents<W> u0 = ldw<W>(Uv(0), i);
+#pragma unroll
+          for (int e = 0; e < W; e++) xi.v[e] = add_rn(xi.v[e], mul_rn(alpha, u0.v[e]));
+          stw<W>(v.x, i, xi);
+        }
+        for (int k = 0; k <= j; k++) {
+          Ents<W> r = ldw<W>(Rv(k), i);
+          if (-alpha != 0.0) {
+            const Ents<W> u = ldw<W>(Uv(k + 1), i);
+#pragma unroll
+            for (int e = 0; e < W; e++) r.v[e] = add_rn(r.v[e], mul_rn(-alpha, u.v[e]));
+            stw<W>(Rv(k), i, r);
+          }
+          if (jac && k == j) stw<W>(v.q, i, precond_w<W>(A.diag, i, r));
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+      // r_{j+1} = A q; the next step's rho = (r_{j+1}, r0)
+      {
+        EpiStoreDot epi{Rv(j + 1), v.rt, 0.0};
+        spmv_phase(A, jac ? v.q : Rv(j), epi, s_prod, s_red);
+        const double d = block_sum<NT>(epi.acc, s_red);
+        if (tid == 0) s_vals[0] = d;
+        if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+      }
+      rho_next = s_vals[0];
+      nb_iter++;
+    }
+    // MR part: for j = 1..l, tau(i, j) = (r_j, r_i) / gamma_i and
+    // r_j -= tau(i, j) r_i for i < j with gamma_i != 0, each axpy fused with
+    // the next dot; gamma_j = (r_j, r_j), gamma'_j = (r_0, r_j) / gamma_j
+    for (int j = 1; j <= l; j++) {
+      int pi = 0;          // pending axpy: r_j -= ptau r_pi (pi = 0: none)
+      double ptau = 0.0;
+      for (int i = 1; i <= j; i++) {
+        const bool last = (i == j);
+        if (!last && s_g[i] == 0.0) continue;
+        double d0 = 0.0, d1 = 0.0;
+        double* rj = Rv(j);
+        const double* ri = Rv(last ? 0 : i);
+        const double* rp = Rv(pi);
+        vec_pass(n, gt, gs, true, [&](auto wc, long long e) {
+          constexpr int W = decltype(wc)::value;
+          Ents<W> a = ldw<W>(rj, e);
+          if (pi > 0 && -ptau != 0.0) {
+            const Ents<W> p = ldw<W>(rp, e);
+#pragma unroll
+            for (int k = 0; k < W; k++) a.v[k] = add_rn(a.v[k], mul_rn(-ptau, p.v[k]));
+            stw<W>(rj, e, a);
+          }
+          const Ents<W> c = ldw<W>(ri, e);
+#pragma unroll
+          for (int k = 0; k < W; k++) {
+            if (last) {
+              d0 = add_rn(d0, mul_rn(a.v[k], a.v[k]));
+              d1 = add_rn(d1, mul_rn(c.v[k], a.v[k]));
+            } else {
+              d0 = add_rn(d0, mul_rn(a.v[k], c.v[k]));
+            }
+          }
+        });
+        d0 = block_sum<NT>(d0, s_red);
+        if (last) d1 = block_sum<NT>(d1, s_red);
+        if (tid == 0) { s_vals[0] = d0; s_vals[1] = d1; }
+        if (!grid_sync<NT>(P, epoch, last ? 2 : 1, s_vals, s_red)) return;
+        if (!last) {
+          ptau = s_vals[0] / s_g[i];
+          if (tid == 0) s_tau[i * L1 + j] = ptau;
+          pi = i;
+        } else {
+          const double gj = s_vals[0];
+          const double gpj = s_vals[1];
+          __syncthreads();  // every thread has read s_g before thread 0 writes
+          if (tid == 0) {
+            s_g[j] = gj;
+            if (gj != 0.0) s_gp[j] = gpj / gj;
+          }
+          __syncthreads();
+        }
+      }
+    }
+    // gamma = tau^{-1} gamma'; gamma'' = T S gamma (thread 0, in order)
+    if (tid == 0) {
+      s_g[l] = s_gp[l];
+      for (int j = l - 1; j >= 1; j--) {
+        double sg = 0.0;
+        for (int i = j + 1; i <= l; i++) sg = add_rn(sg, mul_rn(s_tau[j * L1 + i], s_g[i]));
+        s_g[j] = add_rn(s_gp[j], -sg);
+      }
+      for (int j = 1; j <= l - 1; j++) {
+        double sg = 0.0;
+        for (int i = j + 1; i <= l - 1; i++)
+          sg = add_rn(sg, mul_rn(s_tau[j * L1 + i], s_g[i + 1]));
+        s_gt[j] = add_rn(s_g[j + 1], sg);
+      }
+    }
+    __syncthreads();
+    omega = s_g[l];
+    // the update, with the next test's ||r_0||^2 and (r_0, r0)
+    {
+      double a0 = 0.0, a1 = 0.0;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long e) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> xi = ldw<W>(v.x, e), r0e = ldw<W>(Rv(0), e), u0e = ldw<W>(Uv(0), e);
+        const double g1 = s_g[1];
+        if (g1 != 0.0)
+#pragma unroll
+          for (int k = 0; k < W; k++) xi.v[k] = add_rn(xi.v[k], mul_rn(g1, r0e.v[k]));
+        {
+          const double c = -s_gp[l];
+          if (c != 0.0) {
+            const Ents<W> t = ldw<W>(Rv(l), e);
+#pragma unroll
+            for (int k = 0; k < W; k++) r0e.v[k] = add_rn(r0e.v[k], mul_rn(c, t.v[k]));
+          }
+          const double cu = -s_g[l];
+          if (cu != 0.0) {
+            const Ents<W> t = ldw<W>(Uv(l), e);
+#pragma unroll
+            for (int k = 0; k < W; k++) u0e.v[k] = add_rn(u0e.v[k], mul_rn(cu, t.v[k]));
+          }
+        }
+        for (int j = 1; j <= l - 1; j++) {
+          const double cu = -s_g[j], cx = s_gt[j], cr = -s_gp[j];
+          if (cu != 0.0) {
+            const Ents<W> t = ldw<W>(Uv(j), e);
+#pragma unroll
+            for (int k = 0; k < W; k++) u0e.v[k] = add_rn(u0e.v[k], mul_rn(cu, t.v[k]));
+          }
+          if (cx != 0.0 || cr != 0.0) {
+            const Ents<W> t = ldw<W>(Rv(j), e);
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+              if (cx != 0.0) xi.v[k] = add_rn(xi.v[k], mul_rn(cx, t.v[k]));
+              if (cr != 0.0) r0e.v[k] = add_rn(r0e.v[k], mul_rn(cr, t.v[k]));
+            }
+          }
+        }
+        stw<W>(v.x, e, xi);
+        stw<W>(Rv(0), e, r0e);
+        stw<W>(Uv(0), e, u0e);
+        const Ents<W> rte = ldw<W>(v.rt, e);
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+          a0 = add_rn(a0, mul_rn(r0e.v[k], r0e.v[k]));
+          a1 = add_rn(a1, mul_rn(r0e.v[k], rte.v[k]));
+        }
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      rr = s_vals[0];
+      rho_next = s_vals[1];
+    }
+    if (nb_iter == start) break;  // the reference may repeat this cycle for ever
+  }
+  // change of coordinates (right preconditioning): x = M^{-1} x
+  if (jac)
+    for (long long i = gt; i < n; i += gs) v.x[i] = precond_val(A.diag, (int)i, __ldcg(v.x + i));
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -1777,7 +2086,9 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
                 sell_op(f)};
 }
 
-enum Solver { kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6 };
+enum Solver {
+  kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7
+};
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
                        const double* b, const sb2_iter_params* prm, sb2_iter_result* res,
@@ -1793,6 +2104,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kTfqmr) { kern = (const void*)tfqmr_fused_kernel; nvec = 8; }
   if (which == kMinres) { kern = (const void*)minres_fused_kernel; nvec = 9; }
   if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
+  if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -1810,7 +2122,8 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   SB2_TRY(alloc_scratch(s, n, nvec, grid, hcap, &S));
   Persist P{S.sync, S.partials, barrier_wait_ns()};
   History H{S.hist, S.hist_it, hcap};
-  IterArgs it{prm->tol, prm->max_iter, which == kGcr ? std::max(prm->restart, 0) : m,
+  IterArgs it{prm->tol, prm->max_iter,
+              which == kGcr ? std::max(prm->restart, 0) : which == kBicgl ? prm->restart : m,
               prm->init_guess_null};
   OpArgs op = op_args(A, diag);
   const size_t nn = vector_stride(n, sizeof(double));
@@ -1823,6 +2136,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   TfqmrVecs tv;
   MinresVecs mv;
   GcrVecs rv;
+  BicglVecs lv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -1851,6 +2165,9 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     const int mg = std::max(prm->restart, 0);
     rv = GcrVecs{b, x, V, V + nn, V + (size_t)(mg + 2) * nn, (long long)nn};
     args[1] = &rv;
+  } else if (which == kBicgl) {
+    lv = BicglVecs{b, x, V, V + nn, V + 2 * nn, V + (size_t)(prm->restart + 3) * nn, (long long)nn};
+    args[1] = &lv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -2237,6 +2554,100 @@ static int host_gcr(Ops& o, double* x, const double* b, const sb2_iter_params* p
   return SB2_OK;
 }
 
+static int host_bicgstabl(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                          HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  const int l = prm->restart;
+  double *q = V, *r0 = V + n, *Rb = V + 2 * n, *Ub = V + (size_t)(l + 3) * n;
+  auto R = [&](int i) { return Rb + (size_t)i * n; };
+  auto U = [&](int i) { return Ub + (size_t)i * n; };
+  const int L1 = l + 1;
+  std::vector<double> tau((size_t)L1 * L1, 0.0), g(L1, 0.0), gp(L1, 0.0), gt(L1, 0.0);
+  for (int i = 0; i <= l; i++) {
+    SB2_TRY(sb2_fill(o.n, 0.0, R(i), o.s));
+    SB2_TRY(sb2_fill(o.n, 0.0, U(i), o.s));
+  }
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, R(0)));
+  else { SB2_TRY(o.copy(b, R(0))); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  SB2_TRY(o.copy(R(0), r0));
+  double rho_0 = 1.0, rho_1, alpha = 0.0, omega = 1.0, sigma, res;
+  for (;;) {
+    SB2_TRY(o.nrm(R(0), &res));
+    if (it.finished(res)) break;
+    const int start = it.nb_iter;
+    rho_0 *= -omega;
+    for (int j = 0; j < l; j++) {
+      SB2_TRY(o.dot(R(j), r0, &rho_1));
+      if (rho_0 == 0.0) { it.fail = 1; break; }
+      const double beta = alpha * (rho_1 / rho_0);
+      rho_0 = rho_1;
+      for (int i = 0; i <= j; i++) {
+        SB2_TRY(o.scal(-beta, U(i)));
+        SB2_TRY(o.axpy(1.0, R(i), U(i)));
+      }
+      SB2_TRY(o.prec(U(j), q));
+      SB2_TRY(o.mlt(q, U(j + 1)));
+      it.nb_iter++;
+      SB2_TRY(o.dot(U(j + 1), r0, &sigma));
+      if (sigma == 0.0) { it.fail = 2; break; }
+      alpha = rho_1 / sigma;
+      SB2_TRY(o.axpy(alpha, U(0), x));
+      for (int i = 0; i <= j; i++) SB2_TRY(o.axpy(-alpha, U(i + 1), R(i)));
+      SB2_TRY(o.prec(R(j), q));
+      SB2_TRY(o.mlt(q, R(j + 1)));
+      it.nb_iter++;
+    }
+    for (int j = 1; j <= l; j++) {
+      for (int i = 1; i < j; i++)
+        if (g[i] != 0.0) {
+          double d;
+          SB2_TRY(o.dot(R(j), R(i), &d));
+          tau[(size_t)i * L1 + j] = d / g[i];
+          SB2_TRY(o.axpy(-tau[(size_t)i * L1 + j], R(i), R(j)));
+        }
+      SB2_TRY(o.dot(R(j), R(j), &g[j]));
+      if (g[j] != 0.0) {
+        double d;
+        SB2_TRY(o.dot(R(0), R(j), &d));
+        gp[j] = d / g[j];
+      }
+    }
+    g[l] = gp[l];
+    omega = g[l];
+    for (int j = l - 1; j >= 1; j--) {
+      double sg = 0.0;
+      for (int i = j + 1; i <= l; i++) {
+        volatile double t = tau[(size_t)j * L1 + i] * g[i];
+        sg += t;
+      }
+      g[j] = gp[j] - sg;
+    }
+    for (int j = 1; j <= l - 1; j++) {
+      double sg = 0.0;
+      for (int i = j + 1; i <= l - 1; i++) {
+        volatile double t = tau[(size_t)j * L1 + i] * g[i + 1];
+        sg += t;
+      }
+      gt[j] = g[j + 1] + sg;
+    }
+    SB2_TRY(o.axpy(g[1], R(0), x));
+    SB2_TRY(o.axpy(-gp[l], R(l), R(0)));
+    SB2_TRY(o.axpy(-g[l], U(l), U(0)));
+    for (int j = 1; j <= l - 1; j++) {
+      SB2_TRY(o.axpy(-g[j], U(j), U(0)));
+      SB2_TRY(o.axpy(gt[j], R(j), x));
+      SB2_TRY(o.axpy(-gp[j], R(j), R(0)));
+    }
+    if (it.nb_iter == start) break;  // the reference may repeat this cycle for ever
+  }
+  SB2_TRY(o.copy(x, q));
+  return o.prec(q, x);
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -2344,6 +2755,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kTfqmr ? 10
                    : which == kMinres ? 9
                    : which == kGcr ? 3 + 2 * (std::max(prm->restart, 0) + 1)
+                   : which == kBicgl ? 2 + 2 * (std::max(prm->restart, 0) + 1)
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -2360,6 +2772,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kTfqmr) SB2_TRY(host_tfqmr(o, x, b, prm, it, V, &init_failed));
   else if (which == kMinres) SB2_TRY(host_minres(o, x, b, prm, it, V, &init_failed));
   else if (which == kGcr) SB2_TRY(host_gcr(o, x, b, prm, it, V, &init_failed));
+  else if (which == kBicgl) SB2_TRY(host_bicgstabl(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -2798,10 +3211,14 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && A->full.sell.nslice >= 0 &&
       g_pcg_device && which <= kGmres)
     return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which);
+  // l = 0 reads past the reference's one-entry gamma vector (BiCgStabl.cxx:167)
+  if (which == kBicgl && prm->restart < 1) return SB2_ERR_INVALID_VALUE;
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
-  // a Gcr step reduces ceil(m / 2) projections in one barrier
-  if (which == kGcr && prm->restart > kGcrMaxRestart)
+  // a Gcr step reduces ceil(m / 2) projections in one barrier; BiCgStabl's
+  // tau lives in shared memory
+  if ((which == kGcr && prm->restart > kGcrMaxRestart) ||
+      (which == kBicgl && prm->restart > kBicglMax))
     return host_solve(which, A, M, x, b, prm, res, hist, hist_it, hist_cap, s);
   const double* diag = nullptr;
   if (kind == SB2_PRECOND_JACOBI) {
@@ -2905,6 +3322,14 @@ int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
             int hist_cap, void* stream) try {
   SB2_TRACE("sb2_gcr");
   return solve_entry(kGcr, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_bicgstabl(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+                  const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+                  int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_bicgstabl");
+  return solve_entry(kBicgl, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

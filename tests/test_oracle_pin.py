@@ -99,7 +99,8 @@ def test_mltadd_live(reference, oracle, seed):
                           reference.mltadd(m, n, ptr, ind, val, a, xt, b, yt, trans=True))
 
 
-@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr"])
+@pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr",
+                                   "bicgstabl"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
     ptr, ind, val = matgen.convdiff3d(5) if which not in ("cg", "minres") else matgen.lap2d(15)
@@ -174,6 +175,32 @@ def test_gcr_restarts_live(reference, oracle, restart):
         assert np.array_equal(xo, xr)
 
 
+@pytest.mark.parametrize("l", [1, 2, 4, 10, 16, 20])
+def test_bicgstabl_live(reference, oracle, l):
+    ptr, ind, val = matgen.convdiff3d(6)
+    b = np.random.default_rng(7).uniform(-1, 1, ptr.size - 1)
+    for pc in (0, 1, 2):
+        xo, co, no, _, _ = oracle.solve("bicgstabl", ptr, ind, val, b, precond=pc, omega=1.1,
+                                        tol=1e-10, max_iter=600, restart=l)
+        assert co == 0
+        xr, cr, nr = reference.solve("bicgstabl", ptr, ind, val, b, precond=pc, omega=1.1,
+                                     tol=1e-10, max_iter=600, restart=l)
+        assert (co, no) == (cr, nr)
+        assert np.array_equal(xo, xr)
+
+
+def test_bicgstabl_no_progress_stops(oracle):
+    """diag(1, -1), b = (1, 1): sigma = (A r, r) vanishes at the first step,
+    then rho_0 = 0 at every later cycle, and the reference repeats that
+    cycle for ever; the restatement stops after it.  Never run on the
+    reference."""
+    p, i, v = (np.array([0, 1, 2], dtype=np.int32), np.array([0, 1], dtype=np.int32),
+               np.array([1.0, -1.0]))
+    _, code, nb, h, _ = oracle.solve("bicgstabl", p, i, v, np.array([1.0, 1.0]), tol=1e-10,
+                                     max_iter=100, hist_cap=10)
+    assert (code, nb) == (1, 1) and len(h) == 2
+
+
 def test_gcr_no_step_stops(oracle):
     """Where the reference's Gcr never returns (a cycle that takes no step:
     a breakdown at its first product, or restart 0), the restatement stops
@@ -211,11 +238,15 @@ def test_minres_indefinite_live(reference, oracle, pc, sym):
     assert np.array_equal(xo, xr)
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr"])
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr", "bicgstabl"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, **kw)
+            if which == "bicgstabl" and co in (1, 2):
+                # after a breakdown the reference's BiCgStabl may repeat a
+                # cycle that counts nothing for ever: never run it there
+                continue
             xr, cr, nr = reference.solve(which, p, i, v, b, x0=x0, precond=pc, **kw)
             assert (co, no) == (cr, nr), (name, pc)
             assert np.array_equal(xo, xr, equal_nan=True), (name, pc)
@@ -335,7 +366,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
             assert np.array_equal(xo, xr, equal_nan=True)
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
-    for which in ("cgs", "tfqmr", "minres", "gcr"):
+    for which in ("cgs", "tfqmr", "minres", "gcr", "bicgstabl"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
