@@ -723,7 +723,7 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
-    """Bytes a persistent BiCgStab, Cgs, TfQmr, MinRes or Gcr solve of
+    """Bytes a persistent BiCgStab, Cgs, TfQmr, MinRes, Gcr or BiCgStabl solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -736,6 +736,11 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 products, 2j + 14 vectors (the j + 1 projections and the
                 j + 1 terms of the new direction; +2 with Jacobi); per cycle
                 2 more (p_0 = r / ||r||)
+      bicgstabl per BiCG step j of a cycle (two counted iterations): two
+                products and 6j + 15 vectors (the j + 1 u and r updates of
+                both passes; +4 with Jacobi); per cycle of l steps the MR
+                part's Gram-Schmidt, 3 l(l + 1) / 2, and the update pass,
+                2l + 7
     L2 serves part of the re-reads, so the figure bounds DRAM traffic from
     above."""
     prod = nnz * 12 + 4 * (n + 1)
@@ -747,23 +752,33 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
             j = k % cycle
             total += 2 * prod + (2 * j + 14 + 2 * jacobi + (2 if j == 0 else 0)) * n * 8
         return total
+    if which == "bicgstabl":
+        l, steps, total = max(restart, 1), int(iterations // 2), 0
+        for k in range(steps):
+            j = k % l
+            total += 2 * prod + (6 * j + 15 + 4 * jacobi) * n * 8
+            if j == l - 1:
+                total += (3 * l * (l + 1) // 2 + 2 * l + 7) * n * 8
+        return total
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
 def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
-    """BiCgStab, Cgs and TfQmr with Jacobi on the 128^3 convection-diffusion
-    operator, MinRes with Jacobi on the 128^3 Poisson operator, Gcr(10) with
+    """BiCgStab, Cgs, TfQmr and BiCgStabl(4) with Jacobi on the 128^3
+    convection-diffusion operator, MinRes with Jacobi on the 128^3 Poisson
+    operator, Gcr(10) with
     Jacobi on the 64^3 convection-diffusion operator (its iteration count
     grows with the grid: 768 at 32^3, 1494 at 48^3, so the reference's host
     solve at 128^3 would take minutes) (BiCgStab.cxx:43-145, Cgs.cxx:45-132,
-    TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141): one persistent
-    kernel per solve, against the reference's own drivers on one host
-    core."""
+    TfQmr.cxx:44-243, BiCgStabl.cxx:43-180, MinRes.cxx:46-153,
+    Gcr.cxx:45-141): one persistent kernel per solve, against the
+    reference's own drivers on one host core."""
     peak, _ = measured_peak()
     out = {}
-    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "gcr": api.Gcr,
-           "minres": api.MinRes}
+    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl,
+           "gcr": api.Gcr, "minres": api.MinRes}
+    restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():
         op = "poisson" if which == "minres" else "convdiff"
@@ -776,9 +791,12 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
             systems[(op, gg)] = (ptr, ind, val, n, bh, torch.as_tensor(bh, device=dev),
                                  api.RowSparse(n, n, ptr, ind, val), api.JacobiPreconditioner())
         ptr, ind, val, n, bh, b, A, J = systems[(op, gg)]
+        rs = restarts.get(which, 10)
+
         def run():
             X = torch.zeros(n, dtype=torch.float64, device=dev)
             it = api.Iteration(20000, 1e-10)
+            it.SetRestart(rs)
             it.HideMessages()
             code = fn(A, X, b, J, it)
             return code, it, X
@@ -786,8 +804,8 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
         ms, (code, it, X) = timed(run, reps=3)
         x = X.cpu().numpy()
         nit = it.GetNumberIteration()
-        nbytes = krylov_bytes(which, n, ind.size, True, nit)
-        key = f"{which}_jacobi_{op}{gg}"
+        nbytes = krylov_bytes(which, n, ind.size, True, nit, rs)
+        key = f"{which}{rs if which in restarts else ''}_jacobi_{op}{gg}"
         out[key] = {"ms": round(ms, 2), "error_code": code, "iterations": nit,
                     "us_per_iteration": round(ms * 1e3 / max(nit, 1), 1),
                     "rel_residual_host_check": float(
@@ -795,8 +813,8 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
                     "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
                     "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
                     "timing": "best of 3"}
-        jobs.append((key, (lambda w, xg, p, i, v, bb: lambda: _cpu_solve(
-            w, p, i, v, bb, xg, precond=1))(which, x, ptr, ind, val, bh), False))
+        jobs.append((key, (lambda w, xg, p, i, v, bb, m: lambda: _cpu_solve(
+            w, p, i, v, bb, xg, precond=1, restart=m))(which, x, ptr, ind, val, bh, rs), False))
     return out
 
 
