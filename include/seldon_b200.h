@@ -488,9 +488,10 @@ int sb2_gmres_cgs2(const sb2_csr* A, const sb2_precond* M, double* x,
  * n <= 131072 rows (about 3.3 MB, held on every GPU that loads the library
  * until the process exits); larger systems are rejected with
  * SB2_ERR_INVALID_VALUE.  The first call on a device looks up that array's
- * device address, which is kept for the life of the process: cudaDeviceReset destroys the array with
- * the context, and this entry point must not be called on that device
- * afterwards (matrix handles made before the reset are gone too).  All
+ * device address, which is kept for the life of the process:
+ * cudaDeviceReset destroys the array with the context, and this entry point
+ * must not be called on that device afterwards (matrix handles made before
+ * the reset are gone too).  All
  * calls on a device share the one array: calls that overlap on the GPU
  * (other streams, other host threads) race and must be serialized by the
  * caller.  The call returns after the solve has finished: it reads the
