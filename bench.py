@@ -723,7 +723,8 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
-    """Bytes a persistent BiCgStab, Cgs, TfQmr, MinRes, Gcr or BiCgStabl solve of
+    """Bytes a persistent BiCgStab, Cgs, TfQmr, QCgs, MinRes, Gcr or BiCgStabl
+    solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -731,6 +732,7 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 (+4 with Jacobi: two diagonal reads, phat, shat)
       cgs       per loop: two products, 18 vectors (+4 with Jacobi)
       tfqmr     per loop: two products, 30 vectors (+2 with Jacobi)
+      qcgs      per loop: two products, 29 vectors (+4 with Jacobi)
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
       gcr       per inner step j of a cycle (two counted iterations): two
                 products, 2j + 14 vectors (the j + 1 projections and the
@@ -760,24 +762,25 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
             if j == l - 1:
                 total += (3 * l * (l + 1) // 2 + 2 * l + 7) * n * 8
         return total
-    vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi}[which]
+    vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi,
+           "qcgs": 29 + 4 * jacobi}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
 def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
-    """BiCgStab, Cgs, TfQmr and BiCgStabl(4) with Jacobi on the 128^3
+    """BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) with Jacobi on the 128^3
     convection-diffusion operator, MinRes with Jacobi on the 128^3 Poisson
     operator, Gcr(10) with
     Jacobi on the 64^3 convection-diffusion operator (its iteration count
     grows with the grid: 768 at 32^3, 1494 at 48^3, so the reference's host
     solve at 128^3 would take minutes) (BiCgStab.cxx:43-145, Cgs.cxx:45-132,
-    TfQmr.cxx:44-243, BiCgStabl.cxx:43-180, MinRes.cxx:46-153,
+    QCgs.cxx:46-165, TfQmr.cxx:44-243, BiCgStabl.cxx:43-180, MinRes.cxx:46-153,
     Gcr.cxx:45-141): one persistent kernel per solve, against the
     reference's own drivers on one host core."""
     peak, _ = measured_peak()
     out = {}
-    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl,
-           "gcr": api.Gcr, "minres": api.MinRes}
+    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs, "tfqmr": api.TfQmr,
+           "bicgstabl": api.BiCgStabl, "gcr": api.Gcr, "minres": api.MinRes}
     restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():

@@ -1601,14 +1601,14 @@ namespace Seldon
 
     enum SolverKind
     {
-      kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl
+      kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs
     };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
       // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110,
-      // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108 and
-      // BiCgStabl.cxx:99,115 pass to Fail
+      // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108,
+      // BiCgStabl.cxx:99,115 and QCgs.cxx:86,108,138 pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
@@ -1619,6 +1619,9 @@ namespace Seldon
         return "Gcr breakdown #1";
       if (kind == kBiCgStabl)
         return code == 1 ? "Bicgstabl breakdown #1" : "Bicgstabl Breakdown #2";
+      if (kind == kQCgs)
+        return code == 1 ? "QCgs breakdown #1"
+                         : (code == 2 ? "Qcgs breakdown #2" : "Qcgs breakdown #3");
       if (kind == kTfQmr)
         {
           if (code == 1)
@@ -1692,12 +1695,15 @@ namespace Seldon
         st = sb2_bicgstabl(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                            cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                            GetStream());
+      else if (kind == kQCgs)
+        st = sb2_qcgs(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                      cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
-                                          "MinRes", "Gcr", "BiCgStabl"};
+                                          "MinRes", "Gcr", "BiCgStabl", "QCgs"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1760,6 +1766,8 @@ namespace Seldon
           return Seldon::Gcr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kBiCgStabl)
           return Seldon::BiCgStabl<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kQCgs)
+          return Seldon::QCgs<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1887,6 +1895,25 @@ namespace Seldon
           Preconditioner& M, Iteration<Titer>& outer)
   {
     return b200::Solve(b200::kGcr, A, x, b, M, outer);
+  }
+
+  //! Cgs with quasi-minimal smoothing on the GPU (QCgs.cxx:46-165).
+  template <class Titer, class Prop, class Preconditioner>
+  int QCgs(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kQCgs, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int QCgs(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kQCgs, A, x, b, M, iter);
   }
 
   //! BiCGSTAB(l) on the GPU, l = iter.GetRestart() (BiCgStabl.cxx:43-180).

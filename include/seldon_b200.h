@@ -462,6 +462,16 @@ int sb2_bicgstabl(const sb2_csr* A, const sb2_precond* M, double* x,
                   sb2_iter_result* result, double* hist, int* hist_it,
                   int hist_cap, void* stream);
 
+/* Seldon's QCgs (QCgs.cxx:46-165): Cgs with a quasi-minimal smoothing
+ * step, right preconditioning; arguments, history and error codes of
+ * sb2_cg (codes 1 to 3).  The test is on the smoothed residual, and x is
+ * replaced by M^{-1} x_qcgs at the end, breakdown or not, as in the
+ * reference.  The identity and Jacobi run as one persistent kernel per
+ * solve; SOR and ILUT drive the device operations from the host. */
+int sb2_qcgs(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

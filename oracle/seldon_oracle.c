@@ -963,8 +963,93 @@ out:
   return code;
 }
 
+/* QCgs, computation/solver/iterative/QCgs.cxx:46-165: Cgs with a
+ * quasi-minimal smoothing step (a 2 x 2 least-squares fit on
+ * r_qcgs - r and v per loop).  The test is on ||r_qcgs|| / ||b||; x is
+ * replaced by M^{-1} x_qcgs at the end, breakdown or not. */
+static int orc_qcgs_impl(const orc_csr* A, double* x, const double* b,
+                         const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *p = malloc(bytes), *q = malloc(bytes), *r = malloc(bytes),
+         *rtilde = malloc(bytes), *u = malloc(bytes), *phat = malloc(bytes),
+         *r_q = malloc(bytes), *x_q = malloc(bytes), *v = malloc(bytes);
+  double* all[9] = {p, q, r, rtilde, u, phat, r_q, x_q, v};
+  for (int k = 0; k < 9; k++) memcpy(all[k], b, bytes);
+  double rho_1, rho_2, mu, nu, alpha, beta, sigma, delta;
+  double b00, b11, b10, m00, m11, m10, rn0, rn1;
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  orc_copy(N, r, rtilde);
+  rho_1 = 1.0;
+  memset(q, 0, bytes);
+  memset(p, 0, bytes);
+  orc_copy(N, r, r_q);
+  orc_copy(N, x, x_q);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r_q))) {
+    rho_2 = orc_dot(N, rtilde, r);
+    if (rho_1 == 0.0) { it_fail(it, 1); break; }
+    beta = rho_2 / rho_1;
+    orc_copy(N, r, u);
+    orc_axpy(N, beta, q, u);
+    orc_scal(N, beta, p);
+    orc_axpy(N, 1.0, q, p);
+    orc_scal(N, beta, p);
+    orc_axpy(N, 1.0, u, p);
+    prec_solve(M, A, p, phat);
+    csr_mlt(A, phat, v);
+    it->nb_iter++;
+    sigma = orc_dot(N, rtilde, v);
+    if (sigma == 0.0) { it_fail(it, 2); break; }
+    alpha = rho_2 / sigma;
+    orc_copy(N, u, q);
+    orc_axpy(N, -alpha, v, q);
+    orc_axpy(N, 1.0, q, u);
+    orc_axpy(N, alpha, u, x);
+    prec_solve(M, A, u, phat);
+    csr_mlt(A, phat, u);
+    orc_axpy(N, -alpha, u, r);
+    orc_copy(N, r_q, u);
+    orc_axpy(N, -1.0, r, u);
+    b00 = orc_dot(N, u, u);
+    b11 = orc_dot(N, v, v);
+    b10 = orc_dot(N, u, v);
+    /* inverse of the symmetric 2 x 2 matrix (b(0,1) is b(1,0)) */
+    delta = b00 * b11 - b10 * b10;
+    if (delta == 0.0) { it_fail(it, 3); break; }
+    m00 = b11 / delta;
+    m11 = b00 / delta;
+    m10 = -b10 / delta;
+    rn0 = -orc_dot(N, u, r);
+    rn1 = -orc_dot(N, v, r);
+    mu = m00 * rn0 + m10 * rn1;
+    nu = m10 * rn0 + m11 * rn1;
+    /* smoothing step */
+    orc_copy(N, r, r_q);
+    orc_axpy(N, mu, u, r_q);
+    orc_axpy(N, nu, v, r_q);
+    orc_scal(N, mu, x_q);
+    orc_axpy(N, 1.0 - mu, x, x_q);
+    orc_axpy(N, -nu, p, x_q);
+    rho_1 = rho_2;
+    it->nb_iter++;
+  }
+  prec_solve(M, A, x_q, x);
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 9; k++) free(all[k]);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr, 7 BiCgStabl.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1003,6 +1088,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_gcr_impl(&A, x, b, &M, &it, restart);
   else if (which == 7)
     code = orc_bicgstabl_impl(&A, x, b, &M, &it, restart);
+  else if (which == 8)
+    code = orc_qcgs_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

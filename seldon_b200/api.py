@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def QCgs(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Cgs with a quasi-minimal smoothing step (QCgs.cxx:46-165), right
+    preconditioned; returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_qcgs, A, x, b, M, iteration, hist_cap, stream)
+
+
 def BiCgStabl(A, x, b, M, iteration, hist_cap=None, stream=None):
     """BiCGSTAB(l) with l = iteration.GetRestart() >= 1 (BiCgStabl.cxx:43-180),
     right preconditioned; returns Iteration::ErrorCode()."""

@@ -16,7 +16,7 @@
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
-// BiCgStabl.cxx:43-180, Iterative.cxx:235-354.
+// BiCgStabl.cxx:43-180, QCgs.cxx:46-165, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -1780,6 +1780,233 @@ __global__ void __launch_bounds__(NT, 4) bicgstabl_fused_kernel(OpArgs A, BicglV
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- QCGS
+
+struct QcgsVecs {
+  const double* b;
+  double *x, *r, *rt, *u, *p, *ph, *q, *v, *rq, *xq;
+  double* uf;  // u = r_qcgs - r after the second product (its operand is u)
+};
+
+// epilogue of the product that follows Add(-alpha, ., r): r -= alpha t
+// (A M^{-1} u, never stored), u = r_qcgs - r, and the projections (u, u),
+// (u, v), (u, r), (v, r).  The new u goes to its own buffer: the product
+// gathers the old one.
+struct EpiQcgsFit {
+  double *r, *u;
+  const double *rq, *v;
+  double malpha;
+  double uu, uv, ur, vr;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    double ri = __ldcg(r + i);
+    if (malpha != 0.0) {
+      ri = add_rn(ri, mul_rn(malpha, t));
+      r[i] = ri;
+    }
+    const double ui = add_rn(__ldcg(rq + i), -ri);
+    u[i] = ui;
+    const double vi = __ldcg(v + i);
+    uu = add_rn(uu, mul_rn(ui, ui));
+    uv = add_rn(uv, mul_rn(ui, vi));
+    ur = add_rn(ur, mul_rn(ui, ri));
+    vr = add_rn(vr, mul_rn(vi, ri));
+  }
+};
+
+// QCgs (QCgs.cxx:46-165): Cgs with a quasi-minimal smoothing step.  Five
+// grid barriers per loop: the u, p, phat pass; v = A phat with (rtilde, v)
+// and (v, v); the q, u, x pass; the second product with the r update, the
+// new u = r_qcgs - r and four projections; the smoothing pass with
+// ||r_qcgs||^2 and the next (rtilde, r).  x becomes M^{-1} x_qcgs at the
+// end, breakdown or not, as in the reference.
+__global__ void __launch_bounds__(NT, 4) qcgs_fused_kernel(OpArgs A, QcgsVecs v, IterArgs it,
+                                                        Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  const bool jac = (A.diag != nullptr);
+  double* ph = jac ? v.ph : v.p;  // identity: phat aliases its operand
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b)
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      v.r[i] = __ldg(v.b + i);
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // rtilde = r_qcgs = r; x_qcgs = x; q = p = 0; ||r||^2 (= (rtilde, r))
+  double rr = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double ri = __ldcg(v.r + i);
+    v.rt[i] = ri;
+    v.rq[i] = ri;
+    v.xq[i] = __ldcg(v.x + i);
+    v.q[i] = 0.0;
+    v.p[i] = 0.0;
+    rr = add_rn(rr, mul_rn(ri, ri));
+  }
+  rr = block_sum<NT>(rr, s_red);
+  if (tid == 0) s_vals[0] = rr;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  double rqq = s_vals[0], rho_2 = s_vals[0], rho_1 = 1.0;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rqq);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho_1 == 0.0) { fail = 1; break; }
+    const double beta = rho_2 / rho_1;
+    // Copy(r, u); Add(beta, q, u); Mlt(beta, p); Add(1, q, p); Mlt(beta, p);
+    // Add(1, u, p); phat = M^{-1} p
+    vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      const Ents<W> qi = ldw<W>(v.q, i);
+      Ents<W> ui = ldw<W>(v.r, i), pi = ldw<W>(v.p, i);
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        if (beta != 0.0) ui.v[j] = add_rn(ui.v[j], mul_rn(beta, qi.v[j]));
+        pi.v[j] = add_rn(mul_rn(add_rn(mul_rn(pi.v[j], beta), qi.v[j]), beta), ui.v[j]);
+      }
+      stw<W>(v.u, i, ui);
+      stw<W>(v.p, i, pi);
+      if (jac) stw<W>(ph, i, precond_w<W>(A.diag, i, pi));
+    });
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // v = A phat with sigma = (rtilde, v) and (v, v)
+    {
+      EpiStoreDot2 epi{v.v, v.rt, true, 0.0, 0.0};
+      spmv_phase(A, ph, epi, s_prod, s_red);
+      const double sg = block_sum<NT>(epi.acc0, s_red);
+      const double vv = block_sum<NT>(epi.acc1, s_red);
+      if (tid == 0) { s_vals[0] = sg; s_vals[1] = vv; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    }
+    nb_iter++;
+    const double sigma = s_vals[0];
+    const double b11 = s_vals[1];
+    if (sigma == 0.0) { fail = 2; break; }
+    const double alpha = rho_2 / sigma;
+    // Copy(u, q); Add(-alpha, v, q); Add(1, q, u); Add(alpha, u, x);
+    // phat = M^{-1} u
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      Ents<W> ui = ldw<W>(v.u, i), qi = ui;
+      if (-alpha != 0.0) {
+        const Ents<W> vi = ldw<W>(v.v, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) qi.v[j] = add_rn(qi.v[j], mul_rn(-alpha, vi.v[j]));
+      }
+#pragma unroll
+      for (int j = 0; j < W; j++) ui.v[j] = add_rn(ui.v[j], qi.v[j]);
+      stw<W>(v.q, i, qi);
+      stw<W>(v.u, i, ui);
+      if (alpha != 0.0) {
+        Ents<W> xi = ldw<W>(v.x, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, ui.v[j]));
+        stw<W>(v.x, i, xi);
+      }
+      if (jac) stw<W>(v.ph, i, precond_w<W>(A.diag, i, ui));
+    });
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // u = A phat; Add(-alpha, u, r); u = r_qcgs - r; the four projections
+    {
+      EpiQcgsFit epi{v.r, v.uf, v.rq, v.v, -alpha, 0.0, 0.0, 0.0, 0.0};
+      spmv_phase(A, jac ? v.ph : v.u, epi, s_prod, s_red);
+      const double uu = block_sum<NT>(epi.uu, s_red);
+      const double uv = block_sum<NT>(epi.uv, s_red);
+      const double ur = block_sum<NT>(epi.ur, s_red);
+      const double vr = block_sum<NT>(epi.vr, s_red);
+      if (tid == 0) { s_vals[0] = uu; s_vals[1] = uv; s_vals[2] = ur; s_vals[3] = vr; }
+      if (!grid_sync<NT>(P, epoch, 4, s_vals, s_red)) return;
+    }
+    const double b00 = s_vals[0], b10 = s_vals[1];
+    // the symmetric 2 x 2 inverse (b(0,1) is b(1,0))
+    const double delta = add_rn(mul_rn(b00, b11), -mul_rn(b10, b10));
+    if (delta == 0.0) { fail = 3; break; }
+    const double m00 = b11 / delta, m11 = b00 / delta, m10 = -b10 / delta;
+    const double rn0 = -s_vals[2], rn1 = -s_vals[3];
+    const double mu = add_rn(mul_rn(m00, rn0), mul_rn(m10, rn1));
+    const double nu = add_rn(mul_rn(m10, rn0), mul_rn(m11, rn1));
+    const double omu = 1.0 - mu;
+    // r_qcgs = r + mu u + nu v; x_qcgs = mu x_qcgs + (1 - mu) x - nu p;
+    // ||r_qcgs||^2 and the next (rtilde, r)
+    {
+      double a0 = 0.0, a1 = 0.0;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> ri = ldw<W>(v.r, i), rti = ldw<W>(v.rt, i);
+        Ents<W> rqi = ri, xqi = ldw<W>(v.xq, i);
+        if (mu != 0.0) {
+          const Ents<W> ui = ldw<W>(v.uf, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) rqi.v[j] = add_rn(rqi.v[j], mul_rn(mu, ui.v[j]));
+        }
+        if (nu != 0.0) {
+          const Ents<W> vi = ldw<W>(v.v, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) rqi.v[j] = add_rn(rqi.v[j], mul_rn(nu, vi.v[j]));
+        }
+#pragma unroll
+        for (int j = 0; j < W; j++) xqi.v[j] = mul_rn(xqi.v[j], mu);
+        if (omu != 0.0) {
+          const Ents<W> xi = ldw<W>(v.x, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xqi.v[j] = add_rn(xqi.v[j], mul_rn(omu, xi.v[j]));
+        }
+        if (-nu != 0.0) {
+          const Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xqi.v[j] = add_rn(xqi.v[j], mul_rn(-nu, pi.v[j]));
+        }
+        stw<W>(v.rq, i, rqi);
+        stw<W>(v.xq, i, xqi);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          a0 = add_rn(a0, mul_rn(rqi.v[j], rqi.v[j]));
+          a1 = add_rn(a1, mul_rn(rti.v[j], ri.v[j]));
+        }
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      rqq = s_vals[0];
+      rho_1 = rho_2;
+      rho_2 = s_vals[1];
+    }
+    nb_iter++;
+  }
+  // x = M^{-1} x_qcgs (a Copy for the identity)
+  for (long long i = gt; i < n; i += gs) v.x[i] = precond_val(A.diag, (int)i, __ldcg(v.xq + i));
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -2087,7 +2314,8 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 }
 
 enum Solver {
-  kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7
+  kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
+  kQcgs = 8
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -2105,6 +2333,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kMinres) { kern = (const void*)minres_fused_kernel; nvec = 9; }
   if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
+  if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -2137,6 +2366,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   MinresVecs mv;
   GcrVecs rv;
   BicglVecs lv;
+  QcgsVecs qv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -2168,6 +2398,10 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   } else if (which == kBicgl) {
     lv = BicglVecs{b, x, V, V + nn, V + 2 * nn, V + (size_t)(prm->restart + 3) * nn, (long long)nn};
     args[1] = &lv;
+  } else if (which == kQcgs) {
+    qv = QcgsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                  V + 7 * nn, V + 8 * nn, V + 9 * nn};
+    args[1] = &qv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -2648,6 +2882,76 @@ static int host_bicgstabl(Ops& o, double* x, const double* b, const sb2_iter_par
   return o.prec(q, x);
 }
 
+static int host_qcgs(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                     HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *p = V, *q = V + n, *r = V + 2 * n, *rt = V + 3 * n, *u = V + 4 * n,
+         *ph = V + 5 * n, *rq = V + 6 * n, *xq = V + 7 * n, *v = V + 8 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.copy(r, rt));
+  SB2_TRY(sb2_fill(o.n, 0.0, q, o.s));
+  SB2_TRY(sb2_fill(o.n, 0.0, p, o.s));
+  SB2_TRY(o.copy(r, rq));
+  SB2_TRY(o.copy(x, xq));
+  double rho_1 = 1.0, rho_2, res;
+  for (;;) {
+    SB2_TRY(o.nrm(rq, &res));
+    if (it.finished(res)) break;
+    SB2_TRY(o.dot(rt, r, &rho_2));
+    if (rho_1 == 0.0) { it.fail = 1; break; }
+    const double beta = rho_2 / rho_1;
+    SB2_TRY(o.copy(r, u));
+    SB2_TRY(o.axpy(beta, q, u));
+    SB2_TRY(o.scal(beta, p));
+    SB2_TRY(o.axpy(1.0, q, p));
+    SB2_TRY(o.scal(beta, p));
+    SB2_TRY(o.axpy(1.0, u, p));
+    SB2_TRY(o.prec(p, ph));
+    SB2_TRY(o.mlt(ph, v));
+    it.nb_iter++;
+    double sigma;
+    SB2_TRY(o.dot(rt, v, &sigma));
+    if (sigma == 0.0) { it.fail = 2; break; }
+    const double alpha = rho_2 / sigma;
+    SB2_TRY(o.copy(u, q));
+    SB2_TRY(o.axpy(-alpha, v, q));
+    SB2_TRY(o.axpy(1.0, q, u));
+    SB2_TRY(o.axpy(alpha, u, x));
+    SB2_TRY(o.prec(u, ph));
+    SB2_TRY(o.mlt(ph, u));
+    SB2_TRY(o.axpy(-alpha, u, r));
+    SB2_TRY(o.copy(rq, u));
+    SB2_TRY(o.axpy(-1.0, r, u));
+    double b00, b11, b10, ur, vr;
+    SB2_TRY(o.dot(u, u, &b00));
+    SB2_TRY(o.dot(v, v, &b11));
+    SB2_TRY(o.dot(u, v, &b10));
+    volatile double d0 = b00 * b11, d1 = b10 * b10;
+    const double delta = d0 - d1;
+    if (delta == 0.0) { it.fail = 3; break; }
+    const double m00 = b11 / delta, m11 = b00 / delta, m10 = -b10 / delta;
+    SB2_TRY(o.dot(u, r, &ur));
+    SB2_TRY(o.dot(v, r, &vr));
+    const double rn0 = -ur, rn1 = -vr;
+    volatile double e0 = m00 * rn0, e1 = m10 * rn1, f0 = m10 * rn0, f1 = m11 * rn1;
+    const double mu = e0 + e1, nu = f0 + f1;
+    SB2_TRY(o.copy(r, rq));
+    SB2_TRY(o.axpy(mu, u, rq));
+    SB2_TRY(o.axpy(nu, v, rq));
+    SB2_TRY(o.scal(mu, xq));
+    SB2_TRY(o.axpy(1.0 - mu, x, xq));
+    SB2_TRY(o.axpy(-nu, p, xq));
+    rho_1 = rho_2;
+    it.nb_iter++;
+  }
+  return o.prec(xq, x);
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -2756,6 +3060,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kMinres ? 9
                    : which == kGcr ? 3 + 2 * (std::max(prm->restart, 0) + 1)
                    : which == kBicgl ? 2 + 2 * (std::max(prm->restart, 0) + 1)
+                   : which == kQcgs ? 9
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -2773,6 +3078,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kMinres) SB2_TRY(host_minres(o, x, b, prm, it, V, &init_failed));
   else if (which == kGcr) SB2_TRY(host_gcr(o, x, b, prm, it, V, &init_failed));
   else if (which == kBicgl) SB2_TRY(host_bicgstabl(o, x, b, prm, it, V, &init_failed));
+  else if (which == kQcgs) SB2_TRY(host_qcgs(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -3322,6 +3628,14 @@ int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
             int hist_cap, void* stream) try {
   SB2_TRACE("sb2_gcr");
   return solve_entry(kGcr, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_qcgs(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_qcgs");
+  return solve_entry(kQcgs, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 
