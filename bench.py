@@ -723,8 +723,8 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
-    """Bytes a persistent BiCgStab, Cgs, TfQmr, QCgs, MinRes, Gcr or BiCgStabl
-    solve of
+    """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, MinRes, Gcr or
+    BiCgStabl solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -733,6 +733,8 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
       cgs       per loop: two products, 18 vectors (+4 with Jacobi)
       tfqmr     per loop: two products, 30 vectors (+2 with Jacobi)
       qcgs      per loop: two products, 29 vectors (+4 with Jacobi)
+      bicg      per loop: a product by A and one by A^T, 19 vectors (+4 with
+                Jacobi)
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
       gcr       per inner step j of a cycle (two counted iterations): two
                 products, 2j + 14 vectors (the j + 1 projections and the
@@ -763,24 +765,25 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 total += (3 * l * (l + 1) // 2 + 2 * l + 7) * n * 8
         return total
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi,
-           "qcgs": 29 + 4 * jacobi}[which]
+           "qcgs": 29 + 4 * jacobi, "bicg": 19 + 4 * jacobi}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
 def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
-    """BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) with Jacobi on the 128^3
-    convection-diffusion operator, MinRes with Jacobi on the 128^3 Poisson
-    operator, Gcr(10) with
-    Jacobi on the 64^3 convection-diffusion operator (its iteration count
+    """Seldon's other drivers, each one persistent kernel per solve, against
+    the reference's own drivers on one host core, all with Jacobi:
+    BiCg, BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) on the 128^3
+    convection-diffusion operator, MinRes on the 128^3 Poisson operator,
+    Gcr(10) on the 64^3 convection-diffusion operator (its iteration count
     grows with the grid: 768 at 32^3, 1494 at 48^3, so the reference's host
-    solve at 128^3 would take minutes) (BiCgStab.cxx:43-145, Cgs.cxx:45-132,
-    QCgs.cxx:46-165, TfQmr.cxx:44-243, BiCgStabl.cxx:43-180, MinRes.cxx:46-153,
-    Gcr.cxx:45-141): one persistent kernel per solve, against the
-    reference's own drivers on one host core."""
+    solve at 128^3 would take minutes).  BiCg.cxx:46-134,
+    BiCgStab.cxx:43-145, Cgs.cxx:45-132, QCgs.cxx:46-165, TfQmr.cxx:44-243,
+    BiCgStabl.cxx:43-180, MinRes.cxx:46-153, Gcr.cxx:45-141."""
     peak, _ = measured_peak()
     out = {}
-    fns = {"bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs, "tfqmr": api.TfQmr,
-           "bicgstabl": api.BiCgStabl, "gcr": api.Gcr, "minres": api.MinRes}
+    fns = {"bicg": api.BiCg, "bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs,
+           "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl, "gcr": api.Gcr,
+           "minres": api.MinRes}
     restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():

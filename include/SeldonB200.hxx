@@ -1601,14 +1601,16 @@ namespace Seldon
 
     enum SolverKind
     {
-      kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs
+      kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs,
+      kBiCg
     };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
       // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110,
       // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108,
-      // BiCgStabl.cxx:99,115 and QCgs.cxx:86,108,138 pass to Fail
+      // BiCgStabl.cxx:99,115, QCgs.cxx:86,108,138 and BiCg.cxx:86,115 pass
+      // to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
@@ -1619,6 +1621,8 @@ namespace Seldon
         return "Gcr breakdown #1";
       if (kind == kBiCgStabl)
         return code == 1 ? "Bicgstabl breakdown #1" : "Bicgstabl Breakdown #2";
+      if (kind == kBiCg)
+        return code == 1 ? "Bicg breakdown #1" : "Bicg breakdown #2";
       if (kind == kQCgs)
         return code == 1 ? "QCgs breakdown #1"
                          : (code == 2 ? "Qcgs breakdown #2" : "Qcgs breakdown #3");
@@ -1698,12 +1702,15 @@ namespace Seldon
       else if (kind == kQCgs)
         st = sb2_qcgs(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                       cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kBiCg)
+        st = sb2_bicg(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                      cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
-                                          "MinRes", "Gcr", "BiCgStabl", "QCgs"};
+                                          "MinRes", "Gcr", "BiCgStabl", "QCgs", "BiCg"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1768,6 +1775,8 @@ namespace Seldon
           return Seldon::BiCgStabl<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kQCgs)
           return Seldon::QCgs<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kBiCg)
+          return Seldon::BiCg<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1895,6 +1904,25 @@ namespace Seldon
           Preconditioner& M, Iteration<Titer>& outer)
   {
     return b200::Solve(b200::kGcr, A, x, b, M, outer);
+  }
+
+  //! Biconjugate gradients on the GPU (BiCg.cxx:46-134).
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCg(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCg, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int BiCg(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kBiCg, A, x, b, M, iter);
   }
 
   //! Cgs with quasi-minimal smoothing on the GPU (QCgs.cxx:46-165).

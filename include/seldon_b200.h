@@ -472,6 +472,17 @@ int sb2_qcgs(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's BiCg (BiCg.cxx:46-134): biconjugate gradients with one product
+ * by A and one by A^T per loop (for a general matrix the transpose is built
+ * once per handle, as for sb2_spmv with trans; symmetric storage is its own
+ * transpose) and M^{-1}, M^{-T} on the two residuals; arguments, history and
+ * error codes of sb2_cg (codes 1 and 2).  The identity and Jacobi run as
+ * one persistent kernel per solve; SOR and ILUT drive the device
+ * operations from the host. */
+int sb2_bicg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

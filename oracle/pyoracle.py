@@ -18,7 +18,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libseldon_ref.so")
 # the `which` numbers of orc_solve / ref_solve
 _SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "cgs": 3, "tfqmr": 4, "minres": 5, "gcr": 6,
-            "bicgstabl": 7, "qcgs": 8}
+            "bicgstabl": 7, "qcgs": 8, "bicg": 9}
 REF_FAST_SO = os.path.join(HERE, "_ref", "libseldon_ref_fast.so")
 
 _vp = ctypes.c_void_p
@@ -138,7 +138,7 @@ class Oracle(_Base):
               sor_iter=1, sor_sym=True, tol=1e-6, max_iter=100, restart=10,
               hist_cap=0):
         """which: 'cg' | 'bicgstab' | 'gmres' | 'cgs' | 'tfqmr' | 'minres' | 'gcr' |
-        'bicgstabl' | 'qcgs'.  precond: 0 identity, 1 Jacobi, 2 SOR.
+        'bicgstabl' | 'qcgs' | 'bicg'.  precond: 0 identity, 1 Jacobi, 2 SOR.
         Returns (x, error_code, nb_iter, hist, hist_it)."""
         w = _SOLVERS[which]
         ptr, ind, val = _csr_args(ptr, ind, val)

@@ -9,7 +9,7 @@
 //   MltAdd Trans RowSparse  computation/basic_functions/Functions_MatVect.cxx:729-758
 //   Cg / BiCgStab / Gmres   computation/solver/iterative/{Cg,BiCgStab,Gmres}.cxx
 //   Cgs / TfQmr / MinRes    computation/solver/iterative/{Cgs,TfQmr,MinRes}.cxx
-//   QCgs                    computation/solver/iterative/QCgs.cxx
+//   QCgs, BiCg              computation/solver/iterative/{QCgs,BiCg}.cxx
 //   Gcr, BiCgStabl          computation/solver/iterative/{Gcr,BiCgStabl}.cxx
 //                           (never with an input where they cannot return:
 //                           see orc_gcr_impl, orc_bicgstabl_impl)
@@ -133,6 +133,7 @@ namespace
       case 6: return Gcr(A, x, b, M, it);
       case 7: return BiCgStabl(A, x, b, M, it);
       case 8: return QCgs(A, x, b, M, it);
+      case 9: return BiCg(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -372,7 +373,7 @@ extern "C"
   }
 
   // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes, 6 Gcr,
-  // 7 BiCgStabl, 8 QCgs.  precond: 0 identity, 1 Jacobi, 2 SOR.
+  // 7 BiCgStabl, 8 QCgs, 9 BiCg.  precond: 0 identity, 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
                 const double* val, int sym, int precond, double omega,

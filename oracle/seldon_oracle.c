@@ -1048,8 +1048,125 @@ out:
   return code;
 }
 
+/* Mlt(SeldonTrans, M, X, Y) (Functions_MatVect.cxx:122-130) passes its
+ * flag as the base type SeldonTranspose, so the generic MltAdd runs
+ * (:1279-1317): Y(i) = 0 + 1 * sum_j M(j, i) X(j), j increasing, over every
+ * j (the absent entries add zeros, which change no sum).  For RowSparse
+ * that is column i's entries in increasing row order, as the column
+ * scatter below adds them; for RowSymSparse, M(j, i) = M(i, j), so row i of
+ * the full symmetric matrix in increasing column order: the strict lower
+ * part (`lp/li/lv`, the upper part transposed, built once by the caller)
+ * then the stored upper row. */
+static void csr_mlt_trans(const orc_csr* A, const int* lp, const int* li,
+                          const double* lv, const double* x, double* y) {
+  memset(y, 0, (size_t)A->n * sizeof(double));
+  if (!A->sym) {
+    orc_mltadd(A->m, A->n, A->ptr, A->ind, A->val, 0, 1, 1.0, x, 0.0, y);
+    return;
+  }
+  for (int i = 0; i < A->m; i++) {
+    double t = 0.0;
+    for (int k = lp[i]; k < lp[i + 1]; k++) t += lv[k] * x[li[k]];
+    for (int k = A->ptr[i]; k < A->ptr[i + 1]; k++) t += A->val[k] * x[A->ind[k]];
+    y[i] += 1.0 * t;
+  }
+}
+
+/* The strict lower part of a RowSymSparse matrix as CSR (the strict upper
+ * part transposed), columns increasing within each row. */
+static void sym_lower(const orc_csr* A, int** lp, int** li, double** lv) {
+  const int n = A->m;
+  int* p = calloc((size_t)n + 1, sizeof(int));
+  for (int i = 0; i < n; i++)
+    for (int k = A->ptr[i]; k < A->ptr[i + 1]; k++)
+      if (A->ind[k] > i) p[A->ind[k] + 1]++;
+  for (int i = 0; i < n; i++) p[i + 1] += p[i];
+  int* fill = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) fill[i] = p[i];
+  int* c = malloc(sizeof(int) * (size_t)(p[n] > 0 ? p[n] : 1));
+  double* v = malloc(sizeof(double) * (size_t)(p[n] > 0 ? p[n] : 1));
+  for (int i = 0; i < n; i++)
+    for (int k = A->ptr[i]; k < A->ptr[i + 1]; k++)
+      if (A->ind[k] > i) {
+        const int q = fill[A->ind[k]]++;
+        c[q] = i;
+        v[q] = A->val[k];
+      }
+  free(fill);
+  *lp = p;
+  *li = c;
+  *lv = v;
+}
+
+/* BiCg, computation/solver/iterative/BiCg.cxx:46-134: biconjugate
+ * gradients, M^{-1} on the residual and M^{-T} on the shadow residual, one
+ * product with A and one with A^T per loop. */
+static int orc_bicg_impl(const orc_csr* A, double* x, const double* b,
+                         const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *r = malloc(bytes), *z = malloc(bytes), *p = malloc(bytes),
+         *q = malloc(bytes), *rt = malloc(bytes), *zt = malloc(bytes),
+         *pt = malloc(bytes), *qt = malloc(bytes);
+  double* all[8] = {r, z, p, q, rt, zt, pt, qt};
+  for (int k = 0; k < 8; k++) memcpy(all[k], b, bytes);
+  double rho_1, rho_2 = 0.0, alpha, beta, delta;
+  int code;
+  int *lp = NULL, *li = NULL;
+  double* lv = NULL;
+  if (A->sym) sym_lower(A, &lp, &li, &lv);
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  orc_copy(N, r, rt);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r))) {
+    /* z = M^{-1} r, zt = M^{-T} rt (SOR's TransSolve sweeps backward) */
+    prec_solve(M, A, r, z);
+    if (M->kind == 2) {
+      memset(zt, 0, bytes);
+      orc_sor(N, A->ptr, A->ind, A->val, A->sym, zt, rt, M->omega, M->nb_iter,
+              M->symmetric ? 0 : 3);
+    } else {
+      prec_solve(M, A, rt, zt);
+    }
+    rho_1 = orc_dot(N, z, rt);
+    if (rho_1 == 0.0) { it_fail(it, 1); break; }
+    if (it->nb_iter == 0) {
+      orc_copy(N, z, p);
+      orc_copy(N, zt, pt);
+    } else {
+      beta = rho_1 / rho_2;
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, z, p);
+      orc_scal(N, beta, pt);
+      orc_axpy(N, 1.0, zt, pt);
+    }
+    csr_mlt(A, p, q);
+    it->nb_iter++;
+    csr_mlt_trans(A, lp, li, lv, pt, qt);
+    delta = orc_dot(N, pt, q);
+    if (delta == 0.0) { it_fail(it, 2); break; }
+    alpha = rho_1 / delta;
+    orc_axpy(N, alpha, p, x);
+    orc_axpy(N, -alpha, q, r);
+    orc_axpy(N, -alpha, qt, rt);
+    rho_2 = rho_1;
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  for (int k = 0; k < 8; k++) free(all[k]);
+  free(lp); free(li); free(lv);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1090,6 +1207,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_bicgstabl_impl(&A, x, b, &M, &it, restart);
   else if (which == 8)
     code = orc_qcgs_impl(&A, x, b, &M, &it);
+  else if (which == 9)
+    code = orc_bicg_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def BiCg(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Biconjugate gradients (BiCg.cxx:46-134), one product by A and one by
+    A^T per loop; returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_bicg, A, x, b, M, iteration, hist_cap, stream)
+
+
 def QCgs(A, x, b, M, iteration, hist_cap=None, stream=None):
     """Cgs with a quasi-minimal smoothing step (QCgs.cxx:46-165), right
     preconditioned; returns Iteration::ErrorCode()."""

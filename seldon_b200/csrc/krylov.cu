@@ -16,7 +16,8 @@
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
-// BiCgStabl.cxx:43-180, QCgs.cxx:46-165, Iterative.cxx:235-354.
+// BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134,
+// Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2007,6 +2008,176 @@ __global__ void __launch_bounds__(NT, 4) qcgs_fused_kernel(OpArgs A, QcgsVecs v,
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- BICG
+
+struct BcgVecs {
+  const double* b;
+  double *x, *r, *rt, *p, *pt, *q, *qt;
+  OpArgs AT;  // the transposed product: A itself for symmetric storage
+};
+
+// epilogue that only stores the product
+struct EpiStore {
+  double* y;
+  __device__ __forceinline__ void operator()(int r, double t) { y[r] = t; }
+  __device__ __forceinline__ void quad(int r, const double* t) {
+    if (!al16(y + r)) {
+      for (int j = 0; j < 4; j++) y[r + j] = t[j];
+      return;
+    }
+    const double tv[4] = {t[0], t[1], t[2], t[3]};
+    vst4(y + r, tv);
+  }
+};
+
+// BiCg (BiCg.cxx:46-134): three grid barriers per loop -- the p and p~
+// pass; the products q = A p (fused with (p~, q)) and q~ = A^T p~ in one
+// phase, since neither reads what the other writes; the update pass with
+// ||r||^2 and the next rho = (M^{-1} r, r~).  z and z~ are never stored:
+// with the identity or Jacobi they are recomputed where they are read.
+// Seldon's Mlt(SeldonTrans, ...) sums row i of the transpose in increasing
+// index order (Functions_MatVect.cxx:1279-1317), which is what the product
+// over the explicit transpose (or the expanded symmetric pattern) does.
+__global__ void __launch_bounds__(NT, 4) bicg_fused_kernel(OpArgs A, BcgVecs v, IterArgs it,
+                                                        Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b)
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      v.r[i] = __ldg(v.b + i);
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // r~ = r; ||r||^2 and rho = (M^{-1} r, r~)
+  double rr = 0.0, rz = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double ri = __ldcg(v.r + i);
+    v.rt[i] = ri;
+    rr = add_rn(rr, mul_rn(ri, ri));
+    rz = add_rn(rz, mul_rn(precond_val(A.diag, (int)i, ri), ri));
+  }
+  rr = block_sum<NT>(rr, s_red);
+  rz = block_sum<NT>(rz, s_red);
+  if (tid == 0) { s_vals[0] = rr; s_vals[1] = rz; }
+  if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+  rr = s_vals[0];
+  double rho_1 = s_vals[1], rho_2 = 0.0;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho_1 == 0.0) { fail = 1; break; }
+    // p = z, p~ = z~ (first) | Mlt(beta, p); Add(1, z, p); the same for p~
+    {
+      const bool first = nb_iter == 0;
+      const double beta = first ? 0.0 : rho_1 / rho_2;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> z = precond_w<W>(A.diag, i, ldw<W>(v.r, i));
+        const Ents<W> zt = precond_w<W>(A.diag, i, ldw<W>(v.rt, i));
+        if (first) {
+          stw<W>(v.p, i, z);
+          stw<W>(v.pt, i, zt);
+        } else {
+          Ents<W> pi = ldw<W>(v.p, i), pti = ldw<W>(v.pt, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            pi.v[j] = add_rn(mul_rn(pi.v[j], beta), z.v[j]);
+            pti.v[j] = add_rn(mul_rn(pti.v[j], beta), zt.v[j]);
+          }
+          stw<W>(v.p, i, pi);
+          stw<W>(v.pt, i, pti);
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    // q = A p with delta = (p~, q); q~ = A^T p~
+    {
+      EpiStoreDot e1{v.q, v.pt, 0.0};
+      spmv_phase(A, v.p, e1, s_prod, s_red);
+      EpiStore e2{v.qt};
+      spmv_phase(v.AT, v.pt, e2, s_prod, s_red);
+      const double d = block_sum<NT>(e1.acc, s_red);
+      if (tid == 0) s_vals[0] = d;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    nb_iter++;
+    const double delta = s_vals[0];
+    if (delta == 0.0) { fail = 2; break; }
+    const double alpha = rho_1 / delta;
+    // Add(alpha, p, x); Add(-alpha, q, r); Add(-alpha, q~, r~); the next
+    // ||r||^2 and rho
+    {
+      double a0 = 0.0, a1 = 0.0;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        if (alpha != 0.0) {
+          Ents<W> xi = ldw<W>(v.x, i);
+          const Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, pi.v[j]));
+          stw<W>(v.x, i, xi);
+        }
+        Ents<W> ri = ldw<W>(v.r, i), rti = ldw<W>(v.rt, i);
+        if (-alpha != 0.0) {
+          const Ents<W> qi = ldw<W>(v.q, i), qti = ldw<W>(v.qt, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            ri.v[j] = add_rn(ri.v[j], mul_rn(-alpha, qi.v[j]));
+            rti.v[j] = add_rn(rti.v[j], mul_rn(-alpha, qti.v[j]));
+          }
+          stw<W>(v.r, i, ri);
+          stw<W>(v.rt, i, rti);
+        }
+        const Ents<W> zi = precond_w<W>(A.diag, i, ri);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          a0 = add_rn(a0, mul_rn(ri.v[j], ri.v[j]));
+          a1 = add_rn(a1, mul_rn(zi.v[j], rti.v[j]));
+        }
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      rr = s_vals[0];
+      rho_2 = rho_1;
+      rho_1 = s_vals[1];
+    }
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -2315,7 +2486,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
-  kQcgs = 8
+  kQcgs = 8, kBcg = 9  // kBicg is BiCgStab, kBcg BiCg
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -2334,6 +2505,11 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
+  if (which == kBcg) {
+    kern = (const void*)bicg_fused_kernel;
+    nvec = 6;
+    if (!A->sym) SB2_TRY(ensure_transpose(A));
+  }
   if (which == kGmres) {
     kern = (const void*)gmres_fused_kernel;
     nvec = 2 + (m + 1);
@@ -2367,6 +2543,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   GcrVecs rv;
   BicglVecs lv;
   QcgsVecs qv;
+  BcgVecs gcv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -2402,6 +2579,13 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     qv = QcgsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                   V + 7 * nn, V + 8 * nn, V + 9 * nn};
     args[1] = &qv;
+  } else if (which == kBcg) {
+    // Seldon's transpose of RowSymSparse storage is the matrix itself
+    const CsrArrays& t = A->sym ? A->full : A->trans;
+    const OpArgs at{t.d_ptr, t.d_ind, t.d_val, t.part.d_blk, t.part.d_kind, t.part.nblk, A->m,
+                    diag, sell_op(t)};
+    gcv = BcgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, at};
+    args[1] = &gcv;
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -2445,6 +2629,10 @@ struct Ops {
   int prec(const double* r, double* z) {
     return M ? precond_apply(M, false, r, z, s) : copy(r, z);
   }
+  int prect(const double* r, double* z) {  // TransSolve
+    return M ? precond_apply(M, true, r, z, s) : copy(r, z);
+  }
+  int mltt(const double* x, double* y) { return sb2_mlt(A, 1, 1.0, x, y, s); }
 };
 
 static int host_cg(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
@@ -2952,6 +3140,52 @@ static int host_qcgs(Ops& o, double* x, const double* b, const sb2_iter_params* 
   return o.prec(xq, x);
 }
 
+static int host_bicg(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                     HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *r = V, *z = V + n, *p = V + 2 * n, *q = V + 3 * n, *rt = V + 4 * n, *zt = V + 5 * n,
+         *pt = V + 6 * n, *qt = V + 7 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.copy(r, rt));
+  double rho_1, rho_2 = 0.0, res;
+  for (;;) {
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    SB2_TRY(o.prec(r, z));
+    SB2_TRY(o.prect(rt, zt));
+    SB2_TRY(o.dot(z, rt, &rho_1));
+    if (rho_1 == 0.0) { it.fail = 1; break; }
+    if (it.nb_iter == 0) {
+      SB2_TRY(o.copy(z, p));
+      SB2_TRY(o.copy(zt, pt));
+    } else {
+      const double beta = rho_1 / rho_2;
+      SB2_TRY(o.scal(beta, p));
+      SB2_TRY(o.axpy(1.0, z, p));
+      SB2_TRY(o.scal(beta, pt));
+      SB2_TRY(o.axpy(1.0, zt, pt));
+    }
+    SB2_TRY(o.mlt(p, q));
+    it.nb_iter++;
+    SB2_TRY(o.mltt(pt, qt));
+    double delta;
+    SB2_TRY(o.dot(pt, q, &delta));
+    if (delta == 0.0) { it.fail = 2; break; }
+    const double alpha = rho_1 / delta;
+    SB2_TRY(o.axpy(alpha, p, x));
+    SB2_TRY(o.axpy(-alpha, q, r));
+    SB2_TRY(o.axpy(-alpha, qt, rt));
+    rho_2 = rho_1;
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -3061,6 +3295,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kGcr ? 3 + 2 * (std::max(prm->restart, 0) + 1)
                    : which == kBicgl ? 2 + 2 * (std::max(prm->restart, 0) + 1)
                    : which == kQcgs ? 9
+                   : which == kBcg ? 8
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -3079,6 +3314,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kGcr) SB2_TRY(host_gcr(o, x, b, prm, it, V, &init_failed));
   else if (which == kBicgl) SB2_TRY(host_bicgstabl(o, x, b, prm, it, V, &init_failed));
   else if (which == kQcgs) SB2_TRY(host_qcgs(o, x, b, prm, it, V, &init_failed));
+  else if (which == kBcg) SB2_TRY(host_bicg(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -3628,6 +3864,14 @@ int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
             int hist_cap, void* stream) try {
   SB2_TRACE("sb2_gcr");
   return solve_entry(kGcr, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_bicg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_bicg");
+  return solve_entry(kBcg, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 
