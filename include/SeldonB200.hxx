@@ -1602,15 +1602,15 @@ namespace Seldon
     enum SolverKind
     {
       kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs,
-      kBiCg
+      kBiCg, kCoCg
     };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
     {
       // the strings Cg.cxx:82,101, BiCgStab.cxx:77,87,107, Cgs.cxx:80,110,
       // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108,
-      // BiCgStabl.cxx:99,115, QCgs.cxx:86,108,138 and BiCg.cxx:86,115 pass
-      // to Fail
+      // BiCgStabl.cxx:99,115, QCgs.cxx:86,108,138, BiCg.cxx:86,115 and
+      // CoCg.cxx:84,102 pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
@@ -1623,6 +1623,8 @@ namespace Seldon
         return code == 1 ? "Bicgstabl breakdown #1" : "Bicgstabl Breakdown #2";
       if (kind == kBiCg)
         return code == 1 ? "Bicg breakdown #1" : "Bicg breakdown #2";
+      if (kind == kCoCg)
+        return code == 1 ? "Cocg breakdown #1" : "Cocg breakdown #2";
       if (kind == kQCgs)
         return code == 1 ? "QCgs breakdown #1"
                          : (code == 2 ? "Qcgs breakdown #2" : "Qcgs breakdown #3");
@@ -1705,12 +1707,16 @@ namespace Seldon
       else if (kind == kBiCg)
         st = sb2_bicg(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                       cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kCoCg)
+        st = sb2_cocg(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                      cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
-                                          "MinRes", "Gcr", "BiCgStabl", "QCgs", "BiCg"};
+                                          "MinRes", "Gcr", "BiCgStabl", "QCgs", "BiCg",
+                                          "CoCg"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1777,6 +1783,8 @@ namespace Seldon
           return Seldon::QCgs<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kBiCg)
           return Seldon::BiCg<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kCoCg)
+          return Seldon::CoCg<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1904,6 +1912,25 @@ namespace Seldon
           Preconditioner& M, Iteration<Titer>& outer)
   {
     return b200::Solve(b200::kGcr, A, x, b, M, outer);
+  }
+
+  //! CoCg on the GPU (CoCg.cxx:45-116): Cg's steps in real arithmetic.
+  template <class Titer, class Prop, class Preconditioner>
+  int CoCg(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCoCg, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int CoCg(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+           Vector<double, VectFull, CudaAlloc<double> >& x,
+           const Vector<double, VectFull, CudaAlloc<double> >& b,
+           Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kCoCg, A, x, b, M, iter);
   }
 
   //! Biconjugate gradients on the GPU (BiCg.cxx:46-134).

@@ -483,6 +483,14 @@ int sb2_bicg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's CoCg (CoCg.cxx:45-116), conjugate orthogonal CG for complex
+ * symmetric systems.  In real arithmetic its steps are Cg's, so it runs
+ * sb2_cg's engines and returns sb2_cg's results (the reference's CoCg and
+ * Cg agree bit for bit as well). */
+int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def CoCg(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """CoCg (CoCg.cxx:45-116): in real arithmetic Cg's steps and results;
+    returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_cocg, A, x, b, M, iteration, hist_cap, stream)
+
+
 def BiCg(A, x, b, M, iteration, hist_cap=None, stream=None):
     """Biconjugate gradients (BiCg.cxx:46-134), one product by A and one by
     A^T per loop; returns Iteration::ErrorCode()."""

@@ -3867,6 +3867,17 @@ int sb2_gcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
                      (cudaStream_t)stream);
 } SB2_CATCH
 
+// CoCg (CoCg.cxx:45-116) in real arithmetic is Cg step for step (the same
+// dots without conjugation, the same updates and tests), so it runs Cg's
+// engines; the two give the same bits in the reference too.
+int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_cocg");
+  return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
 int sb2_bicg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream) try {

@@ -326,3 +326,21 @@ def test_bicgstabl_refusals_and_stop(api, oracle):
     code, it, _ = _solve(api, "bicgstabl", (p, i, v), False, np.array([1.0, 1.0]), 0,
                          max_iter=100)
     assert (code, it.GetNumberIteration()) == (co, no) == (1, 1)
+
+
+def test_cocg_runs_cg(api):
+    # sb2_cocg runs Cg's engines: the same bits as Cg, cluster-resident,
+    # persistent or with SSOR
+    for A, pc in ((matgen.lap2d(30), 0), (matgen.poisson3d(40), 1), (matgen.lap2d(30), 2)):
+        n = A[0].size - 1
+        b = matgen.matvec(*A, np.random.default_rng(4).uniform(-1, 1, n))
+        outs = []
+        for fn in (api.Cg, api.CoCg):
+            M = api.RowSparse(n, n, *A)
+            X = to_dev(np.zeros(n))
+            it = api.Iteration(2000, 1e-10)
+            it.HideMessages()
+            code = fn(M, X, to_dev(b), _precond(api, pc), it)
+            outs.append((code, it.GetNumberIteration(), to_host(X)))
+        assert outs[0][:2] == outs[1][:2] and outs[0][0] == 0
+        assert np.array_equal(outs[0][2], outs[1][2])

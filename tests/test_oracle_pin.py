@@ -220,6 +220,28 @@ def test_bicg_transpose_live(reference, oracle, sor_sym):
             assert np.array_equal(xo, xr)
 
 
+def test_cocg_is_cg_live(reference):
+    """The reference's CoCg in real arithmetic gives its Cg's bits (the same
+    steps without conjugation), which is why sb2_cocg runs Cg's engines."""
+    cases = [(matgen.lap2d(15), False), (matgen.upper(*matgen.lap2d(15)), True),
+             (matgen.convdiff3d(6), False)]
+    for A, sym in cases:
+        b = np.random.default_rng(3).uniform(-1, 1, A[0].size - 1)
+        for pc in (0, 1, 2):
+            x1, c1, n1 = reference.solve("cg", *A, b, sym=sym, precond=pc, omega=1.1,
+                                         tol=1e-10, max_iter=500)
+            x2, c2, n2 = reference.solve("cocg", *A, b, sym=sym, precond=pc, omega=1.1,
+                                         tol=1e-10, max_iter=500)
+            assert (c1, n1) == (c2, n2)
+            assert np.array_equal(x1, x2, equal_nan=True)
+    for name, (p, i, v), b, x0, kw in _edge_solves():
+        for pc in (0, 1, 2):
+            x1, c1, n1 = reference.solve("cg", p, i, v, b, x0=x0, precond=pc, **kw)
+            x2, c2, n2 = reference.solve("cocg", p, i, v, b, x0=x0, precond=pc, **kw)
+            assert (c1, n1) == (c2, n2), name
+            assert np.array_equal(x1, x2, equal_nan=True), name
+
+
 def test_gcr_no_step_stops(oracle):
     """Where the reference's Gcr never returns (a cycle that takes no step:
     a breakdown at its first product, or restart 0), the restatement stops
