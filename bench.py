@@ -723,7 +723,7 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
-    """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, MinRes, Gcr or
+    """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, Cgne, MinRes, Gcr or
     BiCgStabl solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
@@ -734,6 +734,8 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
       tfqmr     per loop: two products, 30 vectors (+2 with Jacobi)
       qcgs      per loop: two products, 29 vectors (+4 with Jacobi)
       bicg      per loop: a product by A and one by A^T, 19 vectors (+4 with
+                Jacobi)
+      cgne      per loop: a product by A and one by A^T, 12 vectors (+2 with
                 Jacobi)
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
       gcr       per inner step j of a cycle (two counted iterations): two
@@ -765,7 +767,7 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 total += (3 * l * (l + 1) // 2 + 2 * l + 7) * n * 8
         return total
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi,
-           "qcgs": 29 + 4 * jacobi, "bicg": 19 + 4 * jacobi}[which]
+           "qcgs": 29 + 4 * jacobi, "bicg": 19 + 4 * jacobi, "cgne": 12 + 2 * jacobi}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
@@ -774,21 +776,28 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     the reference's own drivers on one host core, all with Jacobi:
     BiCg, BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) on the 128^3
     convection-diffusion operator, MinRes on the 128^3 Poisson operator,
-    Gcr(10) on the 64^3 convection-diffusion operator (its iteration count
-    grows with the grid: 768 at 32^3, 1494 at 48^3, so the reference's host
-    solve at 128^3 would take minutes).  BiCg.cxx:46-134,
-    BiCgStab.cxx:43-145, Cgs.cxx:45-132, QCgs.cxx:46-165, TfQmr.cxx:44-243,
-    BiCgStabl.cxx:43-180, MinRes.cxx:46-153, Gcr.cxx:45-141."""
+    Gcr(10) and Cgne on the 64^3 convection-diffusion operator (their
+    iteration counts grow with the grid: Gcr's 768 at 32^3, 1494 at 48^3;
+    Cgne's 6080 at 48^3, 10072 at 64^3, the normal equations squaring the
+    condition number).  BiCg.cxx:46-134, BiCgStab.cxx:43-145,
+    Cgs.cxx:45-132, QCgs.cxx:46-165, TfQmr.cxx:44-243, BiCgStabl.cxx:43-180,
+    MinRes.cxx:46-153, Gcr.cxx:45-141, Cgne.cxx:40-127.
+
+    BiCg's and Cgne's products by A^T are, in the reference,
+    MltAdd(alpha, SeldonTrans, M, X, beta, Y)'s generic loop over every
+    (j, i) pair with the element access M(j, i) (Functions_MatVect.cxx:
+    1274-1317): n^2 row searches a product, so their host solves are not
+    run at these sizes."""
     peak, _ = measured_peak()
     out = {}
     fns = {"bicg": api.BiCg, "bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs,
            "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl, "gcr": api.Gcr,
-           "minres": api.MinRes}
+           "cgne": api.Cgne, "minres": api.MinRes}
     restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():
         op = "poisson" if which == "minres" else "convdiff"
-        gg = g // 2 if which == "gcr" else g
+        gg = g // 2 if which in ("gcr", "cgne") else g
         if (op, gg) not in systems:
             ptr, ind, val = matgen.poisson3d(gg) if op == "poisson" else matgen.convdiff3d(gg)
             n = ptr.size - 1
@@ -801,7 +810,7 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
 
         def run():
             X = torch.zeros(n, dtype=torch.float64, device=dev)
-            it = api.Iteration(20000, 1e-10)
+            it = api.Iteration(40000, 1e-10)
             it.SetRestart(rs)
             it.HideMessages()
             code = fn(A, X, b, J, it)
@@ -819,6 +828,11 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
                     "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
                     "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
                     "timing": "best of 3"}
+        if which in ("bicg", "cgne"):
+            out[key]["cpu_reference"] = {
+                "unavailable": f"the reference's product by A^T is its generic M(j, i) loop "
+                               f"(Functions_MatVect.cxx:1274-1317): {n}^2 row searches a product"}
+            continue
         jobs.append((key, (lambda w, xg, p, i, v, bb, m: lambda: _cpu_solve(
             w, p, i, v, bb, xg, precond=1, restart=m))(which, x, ptr, ind, val, bh, rs), False))
     return out

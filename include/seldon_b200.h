@@ -491,6 +491,17 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's Cgne (Cgne.cxx:40-127): CG on the normal equations
+ * A^T A x = A^T b, with M^{-T} then M^{-1} applied to the residual;
+ * arguments, history and error codes of sb2_cg (codes 1 and 2).  The test
+ * is on ||r|| / ||A^T b||, the first one on ||A^T b|| even from an initial
+ * guess, and the count advances by two per loop, as in the reference.  The
+ * identity and Jacobi run as one persistent kernel per solve; SOR and ILUT
+ * drive the device operations from the host. */
+int sb2_cgne(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

@@ -135,6 +135,7 @@ namespace
       case 8: return QCgs(A, x, b, M, it);
       case 9: return BiCg(A, x, b, M, it);
       case 10: return CoCg(A, x, b, M, it);
+      case 11: return Cgne(A, x, b, M, it);
       default: return -100;
       }
   }
@@ -374,8 +375,8 @@ extern "C"
   }
 
   // which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr, 5 MinRes, 6 Gcr,
-  // 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg.  precond: 0 identity, 1 Jacobi,
-  // 2 SOR.
+  // 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne.  precond: 0 identity,
+  // 1 Jacobi, 2 SOR.
   // Returns Seldon's Iteration::ErrorCode(); *nb_iter the iteration count.
   int ref_solve(int which, int m, int nnz, const int* ptr, const int* ind,
                 const double* val, int sym, int precond, double omega,

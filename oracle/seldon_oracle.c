@@ -1048,6 +1048,20 @@ out:
   return code;
 }
 
+/* M^{-T} r: SorPreconditioner::TransSolve sweeps backward (type 3) when
+ * the preconditioner is not symmetric (Precond_Ssor.cxx:78-90); the
+ * identity and Jacobi are their own transposes. */
+static void prec_trans_solve(const orc_prec* M, const orc_csr* A, const double* r,
+                             double* z) {
+  if (M->kind != 2) {
+    prec_solve(M, A, r, z);
+    return;
+  }
+  memset(z, 0, (size_t)A->m * sizeof(double));
+  orc_sor(A->m, A->ptr, A->ind, A->val, A->sym, z, r, M->omega, M->nb_iter,
+          M->symmetric ? 0 : 3);
+}
+
 /* Mlt(SeldonTrans, M, X, Y) (Functions_MatVect.cxx:122-130) passes its
  * flag as the base type SeldonTranspose, so the generic MltAdd runs
  * (:1279-1317): Y(i) = 0 + 1 * sum_j M(j, i) X(j), j increasing, over every
@@ -1127,13 +1141,7 @@ static int orc_bicg_impl(const orc_csr* A, double* x, const double* b,
   while (!it_finished(it, orc_nrm2(N, r))) {
     /* z = M^{-1} r, zt = M^{-T} rt (SOR's TransSolve sweeps backward) */
     prec_solve(M, A, r, z);
-    if (M->kind == 2) {
-      memset(zt, 0, bytes);
-      orc_sor(N, A->ptr, A->ind, A->val, A->sym, zt, rt, M->omega, M->nb_iter,
-              M->symmetric ? 0 : 3);
-    } else {
-      prec_solve(M, A, rt, zt);
-    }
+    prec_trans_solve(M, A, rt, zt);
     rho_1 = orc_dot(N, z, rt);
     if (rho_1 == 0.0) { it_fail(it, 1); break; }
     if (it->nb_iter == 0) {
@@ -1165,8 +1173,66 @@ out:
   return code;
 }
 
+/* Cgne, computation/solver/iterative/Cgne.cxx:40-127: CG on the normal
+ * equations A^T A x = A^T b, M^{-T} then M^{-1} on r.  The test is on
+ * ||r|| / ||A^T b||, and the first one on ||A^T b|| itself even from an
+ * initial guess; the count advances by two per loop. */
+static int orc_cgne_impl(const orc_csr* A, double* x, const double* b,
+                         const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *p = malloc(bytes), *q = malloc(bytes), *r = malloc(bytes), *z = malloc(bytes);
+  memcpy(p, b, bytes); memcpy(q, b, bytes); memcpy(r, b, bytes); memcpy(z, b, bytes);
+  int *lp = NULL, *li = NULL;
+  double* lv = NULL;
+  if (A->sym) sym_lower(A, &lp, &li, &lv);
+  double rho = 1.0, rho_1 = 0.0, alpha, beta, delta, dp;
+  int code;
+  csr_mlt_trans(A, lp, li, lv, b, q);
+  if (it_init(it, N, q) != 0) { code = it_error_code(it); goto out; }
+  if (!it->init_guess_null) {
+    csr_mlt(A, x, p);
+    csr_mlt_trans(A, lp, li, lv, p, r);
+    orc_scal(N, -1.0, r);
+    orc_axpy(N, 1.0, q, r);
+  } else {
+    orc_copy(N, q, r);
+    memset(x, 0, bytes);
+  }
+  dp = orc_nrm2(N, q);
+  it->nb_iter = 0;
+  while (!it_finished(it, dp)) {
+    prec_trans_solve(M, A, r, q);
+    prec_solve(M, A, q, z);
+    rho = orc_dot(N, r, z);
+    if (rho == 0.0) { it_fail(it, 1); break; }
+    if (it->nb_iter == 0)
+      orc_copy(N, z, p);
+    else {
+      beta = rho / rho_1;
+      orc_scal(N, beta, p);
+      orc_axpy(N, 1.0, z, p);
+    }
+    csr_mlt(A, p, q);
+    csr_mlt_trans(A, lp, li, lv, q, z);
+    delta = orc_dot(N, p, z);
+    if (delta == 0.0) { it_fail(it, 2); break; }
+    alpha = rho / delta;
+    orc_axpy(N, alpha, p, x);
+    orc_axpy(N, -alpha, z, r);
+    rho_1 = rho;
+    dp = orc_nrm2(N, r);
+    it->nb_iter += 2;
+  }
+  code = it_error_code(it);
+out:
+  free(p); free(q); free(r); free(z); free(lp); free(li); free(lv);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1209,6 +1275,10 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_qcgs_impl(&A, x, b, &M, &it);
   else if (which == 9)
     code = orc_bicg_impl(&A, x, b, &M, &it);
+  else if (which == 10)
+    code = orc_cg_impl(&A, x, b, &M, &it); /* CoCg: Cg's steps in real arithmetic */
+  else if (which == 11)
+    code = orc_cgne_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

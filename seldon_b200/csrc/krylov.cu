@@ -16,8 +16,8 @@
 //
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
-// BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134,
-// Iterative.cxx:235-354.
+// BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134, CoCg.cxx:45-116,
+// Cgne.cxx:40-127, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2178,6 +2178,176 @@ __global__ void __launch_bounds__(NT, 4) bicg_fused_kernel(OpArgs A, BcgVecs v, 
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- CGNE
+
+struct CgneVecs {
+  const double* b;
+  double *x, *r, *p, *q, *z;
+  OpArgs AT;  // the transposed product: A itself for symmetric storage
+};
+
+// z = M^{-1} M^{-T} r (TransSolve then Solve; Jacobi divides twice)
+__device__ __forceinline__ double cgne_z(const double* diag, int i, double r) {
+  return precond_val(diag, i, precond_val(diag, i, r));
+}
+
+// epilogue of r = A^T (A x): Mlt(-1, r); Add(1, q, r); with (r, z)
+struct EpiCgneInit {
+  double* r;
+  const double* q;
+  const double* diag;
+  double rz;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double ri = add_rn(-t, __ldcg(q + i));
+    r[i] = ri;
+    rz = add_rn(rz, mul_rn(ri, cgne_z(diag, i, ri)));
+  }
+};
+
+// epilogue of q = A^T b: store q, with ||q||^2
+struct EpiStoreNorm {
+  double* y;
+  double acc;
+  __device__ __forceinline__ void operator()(int r, double t) {
+    y[r] = t;
+    acc = add_rn(acc, mul_rn(t, t));
+  }
+};
+
+// Cgne (Cgne.cxx:40-127): CG on A^T A x = A^T b.  Four grid barriers per
+// loop (two counted iterations): the p pass, with z = M^{-1} M^{-T} r
+// recomputed where it is read; q = A p; z = A^T q fused with (p, z); the
+// update pass with ||r||^2 and the next rho = (r, M^{-1} M^{-T} r).  The
+// first test is on ||A^T b|| even from an initial guess, as in the
+// reference.
+__global__ void __launch_bounds__(NT, 4) cgne_fused_kernel(OpArgs A, CgneVecs v, IterArgs it,
+                                                        Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  // q = A^T b; iter.Init(q)
+  {
+    EpiStoreNorm epi{v.q, 0.0};
+    spmv_phase(v.AT, v.b, epi, s_prod, s_red);
+    const double a = block_sum<NT>(epi.acc, s_red);
+    if (tid == 0) s_vals[0] = a;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  }
+  const double dq = sqrt(s_vals[0]);
+  if (dq == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / dq;
+  // r = q - A^T A x (or r = q, x = 0), with rho = (r, z)
+  double rz = 0.0;
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      const double ri = __ldcg(v.q + i);
+      v.r[i] = ri;
+      v.x[i] = 0.0;
+      rz = add_rn(rz, mul_rn(ri, cgne_z(A.diag, (int)i, ri)));
+    }
+  } else {
+    EpiStore e1{v.p};
+    spmv_phase(A, v.x, e1, s_prod, s_red);
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    EpiCgneInit e2{v.r, v.q, A.diag, 0.0};
+    spmv_phase(v.AT, v.p, e2, s_prod, s_red);
+    rz = e2.rz;
+  }
+  rz = block_sum<NT>(rz, s_red);
+  if (tid == 0) s_vals[0] = rz;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  double rho = s_vals[0], rho_1 = 0.0;
+  double dp = dq;  // Norm2(q)
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * dp;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho == 0.0) { fail = 1; break; }
+    // p = z (first) | Mlt(beta, p); Add(1, z, p)
+    {
+      const bool first = nb_iter == 0;
+      const double beta = first ? 0.0 : rho / rho_1;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> z = precond_w<W>(A.diag, i, precond_w<W>(A.diag, i, ldw<W>(v.r, i)));
+        if (first) {
+          stw<W>(v.p, i, z);
+        } else {
+          Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) pi.v[j] = add_rn(mul_rn(pi.v[j], beta), z.v[j]);
+          stw<W>(v.p, i, pi);
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    // q = A p
+    {
+      EpiStore e{v.q};
+      spmv_phase(A, v.p, e, s_prod, s_red);
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    // z = A^T q with delta = (p, z)
+    {
+      EpiStoreDot e{v.z, v.p, 0.0};
+      spmv_phase(v.AT, v.q, e, s_prod, s_red);
+      const double d = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = d;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double delta = s_vals[0];
+    if (delta == 0.0) { fail = 2; break; }
+    const double alpha = rho / delta;
+    // Add(alpha, p, x); Add(-alpha, z, r); ||r||^2 and the next rho
+    {
+      double a0 = 0.0, a1 = 0.0;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        if (alpha != 0.0) {
+          Ents<W> xi = ldw<W>(v.x, i);
+          const Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, pi.v[j]));
+          stw<W>(v.x, i, xi);
+        }
+        Ents<W> ri = ldw<W>(v.r, i);
+        if (-alpha != 0.0) {
+          const Ents<W> zi = ldw<W>(v.z, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) ri.v[j] = add_rn(ri.v[j], mul_rn(-alpha, zi.v[j]));
+          stw<W>(v.r, i, ri);
+        }
+        const Ents<W> zn = precond_w<W>(A.diag, i, precond_w<W>(A.diag, i, ri));
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          a0 = add_rn(a0, mul_rn(ri.v[j], ri.v[j]));
+          a1 = add_rn(a1, mul_rn(ri.v[j], zn.v[j]));
+        }
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      rho_1 = rho;
+      rho = s_vals[1];
+      dp = sqrt(s_vals[0]);
+    }
+    nb_iter += 2;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -2486,7 +2656,8 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
-  kQcgs = 8, kBcg = 9  // kBicg is BiCgStab, kBcg BiCg
+  kQcgs = 8, kBcg = 9,  // kBicg is BiCgStab, kBcg BiCg
+  kCgne = 10
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -2505,9 +2676,9 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
-  if (which == kBcg) {
-    kern = (const void*)bicg_fused_kernel;
-    nvec = 6;
+  if (which == kBcg || which == kCgne) {
+    kern = which == kBcg ? (const void*)bicg_fused_kernel : (const void*)cgne_fused_kernel;
+    nvec = which == kBcg ? 6 : 4;
     if (!A->sym) SB2_TRY(ensure_transpose(A));
   }
   if (which == kGmres) {
@@ -2544,6 +2715,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   BicglVecs lv;
   QcgsVecs qv;
   BcgVecs gcv;
+  CgneVecs nev;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -2579,13 +2751,18 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     qv = QcgsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                   V + 7 * nn, V + 8 * nn, V + 9 * nn};
     args[1] = &qv;
-  } else if (which == kBcg) {
+  } else if (which == kBcg || which == kCgne) {
     // Seldon's transpose of RowSymSparse storage is the matrix itself
     const CsrArrays& t = A->sym ? A->full : A->trans;
     const OpArgs at{t.d_ptr, t.d_ind, t.d_val, t.part.d_blk, t.part.d_kind, t.part.nblk, A->m,
                     diag, sell_op(t)};
-    gcv = BcgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, at};
-    args[1] = &gcv;
+    if (which == kBcg) {
+      gcv = BcgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, at};
+      args[1] = &gcv;
+    } else {
+      nev = CgneVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, at};
+      args[1] = &nev;
+    }
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
     args[1] = &gv;
@@ -3186,6 +3363,51 @@ static int host_bicg(Ops& o, double* x, const double* b, const sb2_iter_params* 
   return SB2_OK;
 }
 
+static int host_cgne(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                     HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *p = V, *q = V + n, *r = V + 2 * n, *z = V + 3 * n;
+  SB2_TRY(o.mltt(b, q));
+  double dp;
+  SB2_TRY(o.nrm(q, &dp));
+  if (dp == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / dp;
+  if (!prm->init_guess_null) {
+    SB2_TRY(o.mlt(x, p));
+    SB2_TRY(o.mltt(p, r));
+    SB2_TRY(o.scal(-1.0, r));
+    SB2_TRY(o.axpy(1.0, q, r));
+  } else {
+    SB2_TRY(o.copy(q, r));
+    SB2_TRY(sb2_fill(o.n, 0.0, x, o.s));
+  }
+  double rho = 1.0, rho_1 = 0.0;
+  for (;;) {
+    if (it.finished(dp)) break;
+    SB2_TRY(o.prect(r, q));
+    SB2_TRY(o.prec(q, z));
+    SB2_TRY(o.dot(r, z, &rho));
+    if (rho == 0.0) { it.fail = 1; break; }
+    if (it.nb_iter == 0) SB2_TRY(o.copy(z, p));
+    else {
+      SB2_TRY(o.scal(rho / rho_1, p));
+      SB2_TRY(o.axpy(1.0, z, p));
+    }
+    SB2_TRY(o.mlt(p, q));
+    SB2_TRY(o.mltt(q, z));
+    double delta;
+    SB2_TRY(o.dot(p, z, &delta));
+    if (delta == 0.0) { it.fail = 2; break; }
+    const double alpha = rho / delta;
+    SB2_TRY(o.axpy(alpha, p, x));
+    SB2_TRY(o.axpy(-alpha, z, r));
+    rho_1 = rho;
+    SB2_TRY(o.nrm(r, &dp));
+    it.nb_iter += 2;
+  }
+  return SB2_OK;
+}
+
 static void host_genrot(double& a_in, double& b_in, double& c_, double& s_) {
   const double a = a_in, b = b_in;
   const double roe = (std::fabs(a) > std::fabs(b)) ? a : b;
@@ -3296,6 +3518,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kBicgl ? 2 + 2 * (std::max(prm->restart, 0) + 1)
                    : which == kQcgs ? 9
                    : which == kBcg ? 8
+                   : which == kCgne ? 4
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -3315,6 +3538,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kBicgl) SB2_TRY(host_bicgstabl(o, x, b, prm, it, V, &init_failed));
   else if (which == kQcgs) SB2_TRY(host_qcgs(o, x, b, prm, it, V, &init_failed));
   else if (which == kBcg) SB2_TRY(host_bicg(o, x, b, prm, it, V, &init_failed));
+  else if (which == kCgne) SB2_TRY(host_cgne(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -3875,6 +4099,14 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cocg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_cgne(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_cgne");
+  return solve_entry(kCgne, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

@@ -100,7 +100,7 @@ def test_mltadd_live(reference, oracle, seed):
 
 
 @pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr",
-                                   "bicgstabl", "qcgs", "bicg"])
+                                   "bicgstabl", "qcgs", "bicg", "cgne"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
     ptr, ind, val = matgen.convdiff3d(5) if which not in ("cg", "minres") else matgen.lap2d(15)
@@ -201,20 +201,22 @@ def test_bicgstabl_no_progress_stops(oracle):
     assert (code, nb) == (1, 1) and len(h) == 2
 
 
+@pytest.mark.parametrize("which", ["bicg", "cgne"])
 @pytest.mark.parametrize("sor_sym", [True, False])
-def test_bicg_transpose_live(reference, oracle, sor_sym):
-    """BiCg's product by A^T: the reference's Mlt(SeldonTrans, ...) runs the
-    generic loop over M(j, i) (Functions_MatVect.cxx:1279-1317) -- column
-    sums for RowSparse, full symmetric rows for RowSymSparse -- and SOR's
-    TransSolve sweeps backward when the preconditioner is not symmetric."""
+def test_bicg_transpose_live(reference, oracle, sor_sym, which):
+    """BiCg's and Cgne's product by A^T: the reference's Mlt(SeldonTrans, ...)
+    runs the generic loop over M(j, i) (Functions_MatVect.cxx:1279-1317) --
+    column sums for RowSparse, full symmetric rows for RowSymSparse -- and
+    SOR's TransSolve sweeps backward when the preconditioner is not
+    symmetric."""
     cases = [(matgen.convdiff3d(5), False), (matgen.upper(*matgen.poisson3d(6)), True),
              (matgen.upper(*matgen.lap2d(12)), True)]
     for A, sym in cases:
         b = np.random.default_rng(9).uniform(-1, 1, A[0].size - 1)
         for pc in (0, 1, 2):
-            xo, co, no, _, _ = oracle.solve("bicg", *A, b, sym=sym, precond=pc, omega=1.1,
+            xo, co, no, _, _ = oracle.solve(which, *A, b, sym=sym, precond=pc, omega=1.1,
                                             sor_sym=sor_sym, tol=1e-10, max_iter=400)
-            xr, cr, nr = reference.solve("bicg", *A, b, sym=sym, precond=pc, omega=1.1,
+            xr, cr, nr = reference.solve(which, *A, b, sym=sym, precond=pc, omega=1.1,
                                          sor_sym=sor_sym, tol=1e-10, max_iter=400)
             assert (co, no) == (cr, nr)
             assert np.array_equal(xo, xr)
@@ -279,7 +281,8 @@ def test_minres_indefinite_live(reference, oracle, pc, sym):
     assert np.array_equal(xo, xr)
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg"])
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg",
+                                   "cgne"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
@@ -407,7 +410,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
             assert np.array_equal(xo, xr, equal_nan=True)
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
-    for which in ("cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg"):
+    for which in ("cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
