@@ -502,6 +502,16 @@ int sb2_cgne(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's BiCgcr (BiCgcr.cxx:44-118): biconjugate conjugate residuals, one
+ * product a step; arguments, history and error codes of sb2_cg (codes 1 and
+ * 2).  The count starts at 1, as in the reference, which counts the first
+ * product before its first test; the test is on the unpreconditioned
+ * residual.  The identity and Jacobi run as one persistent kernel per
+ * solve; SOR and ILUT drive the device operations from the host. */
+int sb2_bicgcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

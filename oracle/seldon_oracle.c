@@ -1231,8 +1231,56 @@ out:
   return code;
 }
 
+/* BiCgcr.cxx:44-118: biconjugate conjugate residuals.  One product a step;
+ * the count starts at 1 (the initial product a = A p is counted) and the
+ * test is on the unpreconditioned residual v. */
+static int orc_bicgcr_impl(const orc_csr* A, double* x, const double* b,
+                           const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *v = calloc(N, sizeof(double)), *w = calloc(N, sizeof(double)),
+         *s = calloc(N, sizeof(double)), *z = calloc(N, sizeof(double)),
+         *p = calloc(N, sizeof(double)), *a = calloc(N, sizeof(double));
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  memcpy(v, b, bytes);
+  if (!it->init_guess_null)
+    csr_residual(A, x, v);
+  else
+    memset(x, 0, bytes);
+  it->nb_iter = 0;
+  prec_solve(M, A, v, s);
+  orc_copy(N, s, p);
+  csr_mlt(A, p, a);
+  prec_solve(M, A, a, w);
+  it->nb_iter++;
+  while (!it_finished(it, orc_nrm2(N, v))) {
+    double rho = orc_dot(N, w, v), mu = orc_dot(N, w, a);
+    if (mu == 0.0) { it_fail(it, 1); break; }
+    double alpha = rho / mu;
+    orc_axpy(N, alpha, p, x);
+    orc_axpy(N, -alpha, a, v);
+    orc_axpy(N, -alpha, w, s);
+    csr_mlt(A, s, z);
+    double tau = orc_dot(N, w, z);
+    if (tau == 0.0) { it_fail(it, 2); break; }
+    double beta = tau / mu;
+    orc_scal(N, -beta, p);
+    orc_axpy(N, 1.0, s, p);
+    orc_scal(N, -beta, a);
+    orc_axpy(N, 1.0, z, a);
+    prec_solve(M, A, a, w);
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  free(v); free(w); free(s); free(z); free(p); free(a);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne, 12 BiCgcr.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1279,6 +1327,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_cg_impl(&A, x, b, &M, &it); /* CoCg: Cg's steps in real arithmetic */
   else if (which == 11)
     code = orc_cgne_impl(&A, x, b, &M, &it);
+  else if (which == 12)
+    code = orc_bicgcr_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def BiCgcr(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Biconjugate conjugate residuals (BiCgcr.cxx:44-118); returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_bicgcr, A, x, b, M, iteration, hist_cap, stream)
+
+
 def Cgne(A, x, b, M, iteration, hist_cap=None, stream=None):
     """CG on the normal equations A^T A x = A^T b (Cgne.cxx:40-127);
     returns Iteration::ErrorCode()."""

@@ -17,7 +17,7 @@
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
 // BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134, CoCg.cxx:45-116,
-// Cgne.cxx:40-127, Iterative.cxx:235-354.
+// Cgne.cxx:40-127, BiCgcr.cxx:44-118, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2348,6 +2348,165 @@ __global__ void __launch_bounds__(NT, 4) cgne_fused_kernel(OpArgs A, CgneVecs v,
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- BiCgcr
+
+struct BcrVecs {
+  const double* b;
+  double *x, *v, *w, *s, *z, *p, *a;
+};
+
+// epilogue of a = A p: a stored, w = M^{-1} a, with ||v||^2, (w, v), (w, a)
+struct EpiBcrA {
+  double *a, *w;
+  const double* v;
+  const double* diag;
+  double vv, wv, wa;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    a[i] = t;
+    const double wi = precond_val(diag, i, t);
+    w[i] = wi;
+    const double vi = __ldcg(v + i);
+    vv = add_rn(vv, mul_rn(vi, vi));
+    wv = add_rn(wv, mul_rn(wi, vi));
+    wa = add_rn(wa, mul_rn(wi, t));
+  }
+};
+
+// BiCgcr (BiCgcr.cxx:44-118): biconjugate conjugate residuals.  Three grid
+// barriers a step: the x, v, s update pass; z = A s fused with tau = (w, z);
+// the p, a, w pass with ||v||^2 and the next step's rho = (w, v) and
+// mu = (w, a).  The count starts at 1: the reference counts the first
+// product a = A p before its first test.
+__global__ void __launch_bounds__(NT, 4) bicgcr_fused_kernel(OpArgs A, BcrVecs v, IterArgs it,
+                                                          Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // v = b - A x (or x = 0, v = b)
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      v.v[i] = __ldg(v.b + i);
+    }
+  } else {
+    EpiResidual epi{v.b, v.v, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // s = M^{-1} v; p = s
+  for (long long i = gt; i < n; i += gs) {
+    const double si = precond_val(A.diag, (int)i, __ldcg(v.v + i));
+    v.s[i] = si;
+    v.p[i] = si;
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // a = A p; w = M^{-1} a; ++iter
+  double vv, wv, wa;
+  {
+    EpiBcrA e{v.a, v.w, v.v, A.diag, 0.0, 0.0, 0.0};
+    spmv_phase(A, v.p, e, s_prod, s_red);
+    vv = block_sum<NT>(e.vv, s_red);
+    wv = block_sum<NT>(e.wv, s_red);
+    wa = block_sum<NT>(e.wa, s_red);
+    if (tid == 0) { s_vals[0] = vv; s_vals[1] = wv; s_vals[2] = wa; }
+    if (!grid_sync<NT>(P, epoch, 3, s_vals, s_red)) return;
+    vv = s_vals[0]; wv = s_vals[1]; wa = s_vals[2];
+  }
+
+  int nb_iter = 1, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(vv);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    const double mu = wa;
+    if (mu == 0.0) { fail = 1; break; }
+    const double alpha = wv / mu;
+    // Add(alpha, p, x); Add(-alpha, a, v); Add(-alpha, w, s)
+    if (alpha != 0.0) {
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> xi = ldw<W>(v.x, i), vi = ldw<W>(v.v, i), si = ldw<W>(v.s, i);
+        const Ents<W> pi = ldw<W>(v.p, i), ai = ldw<W>(v.a, i), wi = ldw<W>(v.w, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          xi.v[j] = add_rn(xi.v[j], mul_rn(alpha, pi.v[j]));
+          vi.v[j] = add_rn(vi.v[j], mul_rn(-alpha, ai.v[j]));
+          si.v[j] = add_rn(si.v[j], mul_rn(-alpha, wi.v[j]));
+        }
+        stw<W>(v.x, i, xi);
+        stw<W>(v.v, i, vi);
+        stw<W>(v.s, i, si);
+      });
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    // z = A s with tau = (w, z)
+    {
+      EpiStoreDot e{v.z, v.w, 0.0};
+      spmv_phase(A, v.s, e, s_prod, s_red);
+      const double d = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = d;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double tau = s_vals[0];
+    if (tau == 0.0) { fail = 2; break; }
+    const double nbeta = -(tau / mu);
+    // Mlt(-beta, p); Add(1, s, p); Mlt(-beta, a); Add(1, z, a); w = M^{-1} a,
+    // with ||v||^2, (w, v), (w, a)
+    {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> pi = ldw<W>(v.p, i), ai = ldw<W>(v.a, i);
+        const Ents<W> si = ldw<W>(v.s, i), zi = ldw<W>(v.z, i), vi = ldw<W>(v.v, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          pi.v[j] = add_rn(mul_rn(nbeta, pi.v[j]), si.v[j]);
+          ai.v[j] = add_rn(mul_rn(nbeta, ai.v[j]), zi.v[j]);
+        }
+        const Ents<W> wi = precond_w<W>(A.diag, i, ai);
+        stw<W>(v.p, i, pi);
+        stw<W>(v.a, i, ai);
+        stw<W>(v.w, i, wi);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          a0 = add_rn(a0, mul_rn(vi.v[j], vi.v[j]));
+          a1 = add_rn(a1, mul_rn(wi.v[j], vi.v[j]));
+          a2 = add_rn(a2, mul_rn(wi.v[j], ai.v[j]));
+        }
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      a2 = block_sum<NT>(a2, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; s_vals[2] = a2; }
+      if (!grid_sync<NT>(P, epoch, 3, s_vals, s_red)) return;
+      vv = s_vals[0]; wv = s_vals[1]; wa = s_vals[2];
+    }
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- GMRES
 
 struct GmresVecs {
@@ -2657,7 +2816,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
   kQcgs = 8, kBcg = 9,  // kBicg is BiCgStab, kBcg BiCg
-  kCgne = 10
+  kCgne = 10, kBcr = 11  // kBcr BiCgcr
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -2676,6 +2835,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kGcr) { kern = (const void*)gcr_fused_kernel; nvec = 1 + 2 * (std::max(prm->restart, 0) + 1); }
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
+  if (which == kBcr) { kern = (const void*)bicgcr_fused_kernel; nvec = 6; }
   if (which == kBcg || which == kCgne) {
     kern = which == kBcg ? (const void*)bicg_fused_kernel : (const void*)cgne_fused_kernel;
     nvec = which == kBcg ? 6 : 4;
@@ -2716,6 +2876,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   QcgsVecs qv;
   BcgVecs gcv;
   CgneVecs nev;
+  BcrVecs crv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -2751,6 +2912,9 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     qv = QcgsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
                   V + 7 * nn, V + 8 * nn, V + 9 * nn};
     args[1] = &qv;
+  } else if (which == kBcr) {
+    crv = BcrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn};
+    args[1] = &crv;
   } else if (which == kBcg || which == kCgne) {
     // Seldon's transpose of RowSymSparse storage is the matrix itself
     const CsrArrays& t = A->sym ? A->full : A->trans;
@@ -3363,6 +3527,48 @@ static int host_bicg(Ops& o, double* x, const double* b, const sb2_iter_params* 
   return SB2_OK;
 }
 
+static int host_bicgcr(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                       HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *v = V, *w = V + n, *s = V + 2 * n, *z = V + 3 * n, *p = V + 4 * n, *a = V + 5 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, v));
+  else { SB2_TRY(o.copy(b, v)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.prec(v, s));
+  SB2_TRY(o.copy(s, p));
+  SB2_TRY(o.mlt(p, a));
+  SB2_TRY(o.prec(a, w));
+  it.nb_iter = 1;
+  for (;;) {
+    double res;
+    SB2_TRY(o.nrm(v, &res));
+    if (it.finished(res)) break;
+    double rho, mu;
+    SB2_TRY(o.dot(w, v, &rho));
+    SB2_TRY(o.dot(w, a, &mu));
+    if (mu == 0.0) { it.fail = 1; break; }
+    const double alpha = rho / mu;
+    SB2_TRY(o.axpy(alpha, p, x));
+    SB2_TRY(o.axpy(-alpha, a, v));
+    SB2_TRY(o.axpy(-alpha, w, s));
+    SB2_TRY(o.mlt(s, z));
+    double tau;
+    SB2_TRY(o.dot(w, z, &tau));
+    if (tau == 0.0) { it.fail = 2; break; }
+    const double beta = tau / mu;
+    SB2_TRY(o.scal(-beta, p));
+    SB2_TRY(o.axpy(1.0, s, p));
+    SB2_TRY(o.scal(-beta, a));
+    SB2_TRY(o.axpy(1.0, z, a));
+    SB2_TRY(o.prec(a, w));
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
 static int host_cgne(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
                      HostIter& it, double* V, int* init_failed) {
   const size_t n = o.n;
@@ -3519,6 +3725,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kQcgs ? 9
                    : which == kBcg ? 8
                    : which == kCgne ? 4
+                   : which == kBcr ? 6
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -3539,6 +3746,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kQcgs) SB2_TRY(host_qcgs(o, x, b, prm, it, V, &init_failed));
   else if (which == kBcg) SB2_TRY(host_bicg(o, x, b, prm, it, V, &init_failed));
   else if (which == kCgne) SB2_TRY(host_cgne(o, x, b, prm, it, V, &init_failed));
+  else if (which == kBcr) SB2_TRY(host_bicgcr(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -4099,6 +4307,14 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cocg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_bicgcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_bicgcr");
+  return solve_entry(kBcr, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

@@ -1,7 +1,7 @@
 """Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243), MinRes
 (MinRes.cxx:46-153), Gcr (Gcr.cxx:45-141), BiCgStabl (BiCgStabl.cxx:43-180)
-QCgs (QCgs.cxx:46-165), BiCg (BiCg.cxx:46-134) and Cgne (Cgne.cxx:40-127)
-on the device against the
+QCgs (QCgs.cxx:46-165), BiCg (BiCg.cxx:46-134), Cgne (Cgne.cxx:40-127) and
+BiCgcr (BiCgcr.cxx:44-118) on the device against the
 oracle's restatements, which are pinned bit for bit to the reference's own
 templates (tests/test_oracle_pin.py).
 
@@ -21,7 +21,7 @@ from tests.test_oracle_pin import _edge_solves, _nonfinite_cases, shifted_laplac
 
 pytestmark = pytest.mark.gpu
 
-SOLVERS = ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne"]
+SOLVERS = ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr"]
 
 
 @pytest.fixture(scope="module")
@@ -33,7 +33,7 @@ def api(cuda):
 def _fn(api, which):
     return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes, "gcr": api.Gcr,
             "bicgstabl": api.BiCgStabl, "qcgs": api.QCgs, "bicg": api.BiCg,
-            "cgne": api.Cgne}[which]
+            "cgne": api.Cgne, "bicgcr": api.BiCgcr}[which]
 
 
 def _precond(api, pc):
@@ -66,7 +66,7 @@ def _solve(api, which, A, sym, b, pc, x0=None, tol=1e-10, max_iter=2000, restart
 
 # MinRes wants symmetric systems: the Laplacian, and the Laplacian shifted
 # to be indefinite (its case), in both storages
-CASES = ([(w, m, pc) for w in ("cgs", "tfqmr", "gcr", "bicgstabl", "qcgs")
+CASES = ([(w, m, pc) for w in ("cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicgcr")
           for m in ("conv", "lap", "lap_up") for pc in (0, 1, 2)] +
          [("minres", m, pc) for m in ("lap", "lap_up", "indef", "indef_up") for pc in (0, 1, 2)] +
          # BiCg and Cgne with SSOR do not converge on the
@@ -187,7 +187,8 @@ def test_deterministic_and_larger(api, oracle, which):
     assert np.linalg.norm(outs[0][2] - xo) / np.linalg.norm(xo) < 1e-7
 
 
-@pytest.mark.parametrize("which", ["cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicg", "cgne"])
+@pytest.mark.parametrize("which", ["cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicg", "cgne",
+                                   "bicgcr"])
 def test_ilut(api, reference, which):
     # the host-driven loop with the device ILUT apply against the reference's
     # driver with its own factor
