@@ -723,8 +723,8 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
-    """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, Cgne, BiCgcr, MinRes,
-    Gcr or BiCgStabl solve of
+    """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, Cgne, Lsqr, BiCgcr,
+    MinRes, Gcr or BiCgStabl solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -737,6 +737,8 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 Jacobi)
       cgne      per loop: a product by A and one by A^T, 12 vectors (+2 with
                 Jacobi)
+      lsqr      per loop: a product by A and one by A^T, 12 vectors (no
+                preconditioner)
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
       bicgcr    per iteration: one product, 19 vectors (+1 with Jacobi)
       gcr       per inner step j of a cycle (two counted iterations): two
@@ -770,7 +772,8 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
                 total += (3 * l * (l + 1) // 2 + 2 * l + 7) * n * 8
         return total
     vec = {"bicgstab": 21 + 4 * jacobi, "cgs": 18 + 4 * jacobi, "tfqmr": 30 + 2 * jacobi,
-           "qcgs": 29 + 4 * jacobi, "bicg": 19 + 4 * jacobi, "cgne": 12 + 2 * jacobi}[which]
+           "qcgs": 29 + 4 * jacobi, "bicg": 19 + 4 * jacobi, "cgne": 12 + 2 * jacobi,
+           "lsqr": 12}[which]
     return iterations / 2 * (2 * prod + vec * n * 8)
 
 
@@ -779,14 +782,16 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     the reference's own drivers on one host core, all with Jacobi:
     BiCg, BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) on the 128^3
     convection-diffusion operator, MinRes on the 128^3 Poisson operator,
-    Gcr(10), Cgne and BiCgcr on the 64^3 convection-diffusion operator
+    Gcr(10), Cgne, Lsqr and BiCgcr on the 64^3 convection-diffusion operator
     (their iteration counts grow with the grid: Gcr's 768 at 32^3, 1494 at
     48^3; Cgne's 6080 at 48^3, 10072 at 64^3, the normal equations squaring
-    the condition number; BiCgcr's 180 at 40^3, 1113 at 64^3).  BiCg.cxx:46-134, BiCgStab.cxx:43-145,
+    the condition number, Lsqr's 7020 at 48^3; BiCgcr's 180 at 40^3, 1113 at
+    64^3).  Lsqr uses no preconditioner.  BiCg.cxx:46-134, BiCgStab.cxx:43-145,
     Cgs.cxx:45-132, QCgs.cxx:46-165, TfQmr.cxx:44-243, BiCgStabl.cxx:43-180,
-    MinRes.cxx:46-153, Gcr.cxx:45-141, Cgne.cxx:40-127, BiCgcr.cxx:44-118.
+    MinRes.cxx:46-153, Gcr.cxx:45-141, Cgne.cxx:40-127, BiCgcr.cxx:44-118,
+    Lsqr.cxx:40-135.
 
-    BiCg's and Cgne's products by A^T are, in the reference,
+    BiCg's, Cgne's and Lsqr's products by A^T are, in the reference,
     MltAdd(alpha, SeldonTrans, M, X, beta, Y)'s generic loop over every
     (j, i) pair with the element access M(j, i) (Functions_MatVect.cxx:
     1274-1317): n^2 row searches a product, so their host solves are not
@@ -795,12 +800,12 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     out = {}
     fns = {"bicg": api.BiCg, "bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs,
            "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl, "gcr": api.Gcr,
-           "cgne": api.Cgne, "bicgcr": api.BiCgcr, "minres": api.MinRes}
+           "cgne": api.Cgne, "lsqr": api.Lsqr, "bicgcr": api.BiCgcr, "minres": api.MinRes}
     restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():
         op = "poisson" if which == "minres" else "convdiff"
-        gg = g // 2 if which in ("gcr", "cgne", "bicgcr") else g
+        gg = g // 2 if which in ("gcr", "cgne", "lsqr", "bicgcr") else g
         if (op, gg) not in systems:
             ptr, ind, val = matgen.poisson3d(gg) if op == "poisson" else matgen.convdiff3d(gg)
             n = ptr.size - 1
@@ -822,7 +827,7 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
         ms, (code, it, X) = timed(run, reps=3)
         x = X.cpu().numpy()
         nit = it.GetNumberIteration()
-        nbytes = krylov_bytes(which, n, ind.size, True, nit, rs)
+        nbytes = krylov_bytes(which, n, ind.size, which != "lsqr", nit, rs)
         key = f"{which}{rs if which in restarts else ''}_jacobi_{op}{gg}"
         out[key] = {"ms": round(ms, 2), "error_code": code, "iterations": nit,
                     "us_per_iteration": round(ms * 1e3 / max(nit, 1), 1),
@@ -831,7 +836,7 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
                     "gbs_model": round(nbytes / (ms * 1e-3) / 1e9, 1),
                     "frac_of_measured_peak": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
                     "timing": "best of 3"}
-        if which in ("bicg", "cgne"):
+        if which in ("bicg", "cgne", "lsqr"):
             out[key]["cpu_reference"] = {
                 "unavailable": f"the reference's product by A^T is its generic M(j, i) loop "
                                f"(Functions_MatVect.cxx:1274-1317): {n}^2 row searches a product"}

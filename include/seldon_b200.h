@@ -512,6 +512,17 @@ int sb2_bicgcr(const sb2_csr* A, const sb2_precond* M, double* x, const double* 
                const sb2_iter_params* params, sb2_iter_result* result, double* hist,
                int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's Lsqr (Lsqr.cxx:40-135): Golub-Kahan bidiagonalisation with the
+ * products by A and A^T; arguments, history and error codes of sb2_cg
+ * (codes 1 to 3).  The preconditioner is not used (any valid handle, or
+ * NULL).  As in the reference, an initial guess enters only the first test
+ * (on ||b - A x0|| / ||b||): x is zeroed and the iteration starts from b.
+ * The later tests are on |phi_bar| / ||b|| and the count advances by two a
+ * step.  One persistent kernel per solve. */
+int sb2_lsqr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

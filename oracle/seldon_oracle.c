@@ -1279,8 +1279,75 @@ out:
   return code;
 }
 
+/* Lsqr.cxx:40-135: Golub-Kahan bidiagonalisation on A and A^T.  The
+ * preconditioner is not used.  The initial guess enters only the first test
+ * (rnorm = ||b - A x0||): x is zeroed and u starts from b either way.  The
+ * test is on |phi_bar| after the first, and the count advances by two a
+ * loop. */
+static int orc_lsqr_impl(const orc_csr* A, double* x, const double* b, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *v = malloc(bytes), *v1 = malloc(bytes), *u = malloc(bytes),
+         *u1 = malloc(bytes), *w = malloc(bytes);
+  memcpy(v, b, bytes); memcpy(v1, b, bytes); memcpy(u, b, bytes);
+  memcpy(u1, b, bytes); memcpy(w, b, bytes);
+  int *lp = NULL, *li = NULL;
+  double* lv = NULL;
+  if (A->sym) sym_lower(A, &lp, &li, &lv);
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, u);
+  if (!it->init_guess_null)
+    csr_residual(A, x, u);
+  else
+    memset(x, 0, bytes);
+  double rnorm = orc_nrm2(N, u);
+  orc_copy(N, b, u);
+  double beta = orc_nrm2(N, u);
+  orc_scal(N, 1.0 / beta, u);
+  csr_mlt_trans(A, lp, li, lv, u, v);
+  double alpha = orc_nrm2(N, v);
+  orc_scal(N, 1.0 / alpha, v);
+  orc_copy(N, v, w);
+  memset(x, 0, bytes);
+  double phi_bar = beta, rho_bar = alpha;
+  it->nb_iter = 0;
+  while (!it_finished(it, rnorm)) {
+    csr_mlt(A, v, u1);
+    orc_axpy(N, -alpha, u, u1);
+    beta = orc_nrm2(N, u1);
+    if (beta == 0.0) { it_fail(it, 1); break; }
+    orc_scal(N, 1.0 / beta, u1);
+    csr_mlt_trans(A, lp, li, lv, u1, v1);
+    orc_axpy(N, -beta, v, v1);
+    alpha = orc_nrm2(N, v1);
+    if (alpha == 0.0) { it_fail(it, 2); break; }
+    orc_scal(N, 1.0 / alpha, v1);
+    double rho = sqrt(rho_bar * rho_bar + beta * beta);
+    if (rho == 0.0) { it_fail(it, 3); break; }
+    double c = rho_bar / rho, s = beta / rho;
+    double theta = s * alpha;
+    rho_bar = -c * alpha;
+    double phi = c * phi_bar;
+    phi_bar = s * phi_bar;
+    orc_axpy(N, phi / rho, w, x);
+    orc_scal(N, -theta / rho, w);
+    orc_axpy(N, 1.0, v1, w);
+    rnorm = fabs(phi_bar);
+    double* t = u1; u1 = u; u = t;
+    t = v1; v1 = v; v = t;
+    it->nb_iter += 2;
+  }
+  code = it_error_code(it);
+out:
+  free(v); free(v1); free(u); free(u1); free(w); free(lp); free(li); free(lv);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
- * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne, 12 BiCgcr.
+ * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne, 12 BiCgcr,
+ * 13 Lsqr.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1329,6 +1396,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_cgne_impl(&A, x, b, &M, &it);
   else if (which == 12)
     code = orc_bicgcr_impl(&A, x, b, &M, &it);
+  else if (which == 13)
+    code = orc_lsqr_impl(&A, x, b, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

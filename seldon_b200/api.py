@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def Lsqr(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Lsqr (Lsqr.cxx:40-135); M is not used, as in the reference; returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_lsqr, A, x, b, M, iteration, hist_cap, stream)
+
+
 def BiCgcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     """Biconjugate conjugate residuals (BiCgcr.cxx:44-118); returns
     Iteration::ErrorCode()."""

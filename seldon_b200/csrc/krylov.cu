@@ -17,7 +17,7 @@
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
 // BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134, CoCg.cxx:45-116,
-// Cgne.cxx:40-127, BiCgcr.cxx:44-118, Iterative.cxx:235-354.
+// Cgne.cxx:40-127, BiCgcr.cxx:44-118, Lsqr.cxx:40-135, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2348,6 +2348,171 @@ __global__ void __launch_bounds__(NT, 4) cgne_fused_kernel(OpArgs A, CgneVecs v,
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- Lsqr
+
+struct LsqrVecs {
+  const double* b;
+  double *x, *u, *u1, *v, *v1, *w;
+  OpArgs AT;  // the transposed product: A itself for symmetric storage
+};
+
+// epilogue of y = A x; Add(na, u, y) (skipped when na == 0, as Seldon's Add
+// is); with ||y||^2
+struct EpiAxpyNorm {
+  double* y;
+  const double* u;
+  double na;
+  double acc;
+  __device__ __forceinline__ void operator()(int i, double t) {
+    const double yi = na != 0.0 ? add_rn(t, mul_rn(na, __ldcg(u + i))) : t;
+    y[i] = yi;
+    acc = add_rn(acc, mul_rn(yi, yi));
+  }
+};
+
+// Lsqr (Lsqr.cxx:40-135): Golub-Kahan bidiagonalisation; the preconditioner
+// is not used.  The initial guess enters only the first test: x is zeroed
+// and u starts from b either way, as in the reference.  Four grid barriers a
+// loop (two counted iterations): u1 = A v - alpha u with ||u1||^2; u1 /=
+// beta; v1 = A^T u1 - beta v with ||v1||^2; the pass that scales v1 and
+// updates x and w.  u, u1 and v, v1 swap by pointer.
+__global__ void __launch_bounds__(NT, 4) lsqr_fused_kernel(OpArgs A, LsqrVecs v, IterArgs it,
+                                                        Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+  // rnorm = ||b - A x|| (||b|| from a zero guess)
+  double rnorm = normb;
+  if (!it.init_guess_null) {
+    EpiResidual epi{v.b, v.u, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+    const double r2 = block_sum<NT>(epi.rr, s_red);
+    if (tid == 0) s_vals[0] = r2;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    rnorm = sqrt(s_vals[0]);
+  }
+  // u = b / ||b||; x = 0
+  {
+    const double tb = 1.0 / normb;
+    for (long long i = gt; i < n; i += gs) {
+      v.u[i] = mul_rn(__ldg(v.b + i), tb);
+      v.x[i] = 0.0;
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  }
+  // v = A^T u, alpha = ||v||; v /= alpha; w = v
+  double alpha;
+  {
+    EpiStoreNorm e{v.v, 0.0};
+    spmv_phase(v.AT, v.u, e, s_prod, s_red);
+    const double a = block_sum<NT>(e.acc, s_red);
+    if (tid == 0) s_vals[0] = a;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    alpha = sqrt(s_vals[0]);
+    const double ta = 1.0 / alpha;
+    for (long long i = gt; i < n; i += gs) {
+      const double vi = mul_rn(__ldcg(v.v + i), ta);
+      v.v[i] = vi;
+      v.w[i] = vi;
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  }
+  double phi_bar = normb, rho_bar = alpha;
+  double *u = v.u, *u1 = v.u1, *vv = v.v, *v1 = v.v1;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * rnorm;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    // u1 = A v; Add(-alpha, u, u1); beta = ||u1||
+    {
+      EpiAxpyNorm e{u1, u, -alpha, 0.0};
+      spmv_phase(A, vv, e, s_prod, s_red);
+      const double a = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = a;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double beta = sqrt(s_vals[0]);
+    if (beta == 0.0) { fail = 1; break; }
+    // Mlt(1 / beta, u1)
+    {
+      const double tb = 1.0 / beta;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> ui = ldw<W>(u1, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) ui.v[j] = mul_rn(ui.v[j], tb);
+        stw<W>(u1, i, ui);
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    // v1 = A^T u1; Add(-beta, v, v1); alpha = ||v1||
+    {
+      EpiAxpyNorm e{v1, vv, -beta, 0.0};
+      spmv_phase(v.AT, u1, e, s_prod, s_red);
+      const double a = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = a;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    alpha = sqrt(s_vals[0]);
+    if (alpha == 0.0) { fail = 2; break; }
+    const double rho = sqrt(add_rn(mul_rn(rho_bar, rho_bar), mul_rn(beta, beta)));
+    if (rho == 0.0) { fail = 3; break; }
+    const double c = rho_bar / rho, s = beta / rho;
+    const double theta = mul_rn(s, alpha);
+    rho_bar = mul_rn(-c, alpha);
+    const double phi = mul_rn(c, phi_bar);
+    phi_bar = mul_rn(s, phi_bar);
+    // Mlt(1 / alpha, v1); Add(phi / rho, w, x); Mlt(-theta / rho, w); Add(1, v1, w)
+    {
+      const double ta = 1.0 / alpha, tx = phi / rho, tw = -theta / rho;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> vi = ldw<W>(v1, i), wi = ldw<W>(v.w, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) vi.v[j] = mul_rn(vi.v[j], ta);
+        stw<W>(v1, i, vi);
+        if (tx != 0.0) {
+          Ents<W> xi = ldw<W>(v.x, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(tx, wi.v[j]));
+          stw<W>(v.x, i, xi);
+        }
+#pragma unroll
+        for (int j = 0; j < W; j++) wi.v[j] = add_rn(mul_rn(wi.v[j], tw), vi.v[j]);
+        stw<W>(v.w, i, wi);
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    rnorm = fabs(phi_bar);
+    double* t = u1; u1 = u; u = t;
+    t = v1; v1 = vv; vv = t;
+    nb_iter += 2;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- BiCgcr
 
 struct BcrVecs {
@@ -2816,7 +2981,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
   kQcgs = 8, kBcg = 9,  // kBicg is BiCgStab, kBcg BiCg
-  kCgne = 10, kBcr = 11  // kBcr BiCgcr
+  kCgne = 10, kBcr = 11, kLsqr = 12  // kBcr BiCgcr
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -2836,9 +3001,11 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
   if (which == kBcr) { kern = (const void*)bicgcr_fused_kernel; nvec = 6; }
-  if (which == kBcg || which == kCgne) {
-    kern = which == kBcg ? (const void*)bicg_fused_kernel : (const void*)cgne_fused_kernel;
-    nvec = which == kBcg ? 6 : 4;
+  if (which == kBcg || which == kCgne || which == kLsqr) {
+    kern = which == kBcg    ? (const void*)bicg_fused_kernel
+           : which == kCgne ? (const void*)cgne_fused_kernel
+                            : (const void*)lsqr_fused_kernel;
+    nvec = which == kBcg ? 6 : which == kCgne ? 4 : 5;
     if (!A->sym) SB2_TRY(ensure_transpose(A));
   }
   if (which == kGmres) {
@@ -2877,6 +3044,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   BcgVecs gcv;
   CgneVecs nev;
   BcrVecs crv;
+  LsqrVecs lsv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -2915,7 +3083,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   } else if (which == kBcr) {
     crv = BcrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn};
     args[1] = &crv;
-  } else if (which == kBcg || which == kCgne) {
+  } else if (which == kBcg || which == kCgne || which == kLsqr) {
     // Seldon's transpose of RowSymSparse storage is the matrix itself
     const CsrArrays& t = A->sym ? A->full : A->trans;
     const OpArgs at{t.d_ptr, t.d_ind, t.d_val, t.part.d_blk, t.part.d_kind, t.part.nblk, A->m,
@@ -2923,9 +3091,12 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
     if (which == kBcg) {
       gcv = BcgVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, at};
       args[1] = &gcv;
-    } else {
+    } else if (which == kCgne) {
       nev = CgneVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, at};
       args[1] = &nev;
+    } else {
+      lsv = LsqrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, at};
+      args[1] = &lsv;
     }
   } else {
     gv = GmresVecs{b, x, V, V + nn, V + 2 * nn, (long long)nn};
@@ -4185,6 +4356,9 @@ static int solve_entry(int which, const sb2_csr* A, const sb2_precond* M, double
   if ((kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT) && A->full.sell.nslice >= 0 &&
       g_pcg_device && which <= kGmres)
     return pcg_solve(A, M, x, b, prm, res, hist, hist_it, hist_cap, s, which);
+  // Lsqr uses no preconditioner (Lsqr.cxx:40-135): one kernel for every kind
+  if (which == kLsqr)
+    return fused_solve(which, A, nullptr, x, b, prm, res, hist, hist_it, hist_cap, s);
   // l = 0 reads past the reference's one-entry gamma vector (BiCgStabl.cxx:167)
   if (which == kBicgl && prm->restart < 1) return SB2_ERR_INVALID_VALUE;
   if (kind == SB2_PRECOND_SOR || kind == SB2_PRECOND_ILUT)
@@ -4307,6 +4481,14 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cocg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_lsqr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+             const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+             int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_lsqr");
+  return solve_entry(kLsqr, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

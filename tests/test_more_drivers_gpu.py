@@ -1,7 +1,7 @@
 """Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243), MinRes
 (MinRes.cxx:46-153), Gcr (Gcr.cxx:45-141), BiCgStabl (BiCgStabl.cxx:43-180)
-QCgs (QCgs.cxx:46-165), BiCg (BiCg.cxx:46-134), Cgne (Cgne.cxx:40-127) and
-BiCgcr (BiCgcr.cxx:44-118) on the device against the
+QCgs (QCgs.cxx:46-165), BiCg (BiCg.cxx:46-134), Cgne (Cgne.cxx:40-127),
+BiCgcr (BiCgcr.cxx:44-118) and Lsqr (Lsqr.cxx:40-135) on the device against the
 oracle's restatements, which are pinned bit for bit to the reference's own
 templates (tests/test_oracle_pin.py).
 
@@ -21,7 +21,8 @@ from tests.test_oracle_pin import _edge_solves, _nonfinite_cases, shifted_laplac
 
 pytestmark = pytest.mark.gpu
 
-SOLVERS = ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr"]
+SOLVERS = ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr",
+           "lsqr"]
 
 
 @pytest.fixture(scope="module")
@@ -33,7 +34,7 @@ def api(cuda):
 def _fn(api, which):
     return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes, "gcr": api.Gcr,
             "bicgstabl": api.BiCgStabl, "qcgs": api.QCgs, "bicg": api.BiCg,
-            "cgne": api.Cgne, "bicgcr": api.BiCgcr}[which]
+            "cgne": api.Cgne, "bicgcr": api.BiCgcr, "lsqr": api.Lsqr}[which]
 
 
 def _precond(api, pc):
@@ -72,7 +73,9 @@ CASES = ([(w, m, pc) for w in ("cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicg
          # BiCg and Cgne with SSOR do not converge on the
          # convection-diffusion operator, for the reference either
          [(w, m, pc) for w in ("bicg", "cgne") for m in ("conv", "lap", "lap_up")
-          for pc in (0, 1, 2) if (m, pc) != ("conv", 2)])
+          for pc in (0, 1, 2) if (m, pc) != ("conv", 2)] +
+         # Lsqr uses no preconditioner: one case a matrix
+         [("lsqr", m, 1) for m in ("conv", "lap", "lap_up")])
 
 
 def _case_matrix(mname):
@@ -175,8 +178,9 @@ def test_deterministic_and_larger(api, oracle, which):
     full = matgen.convdiff3d(40) if which != "minres" else matgen.poisson3d(40)
     n = full[0].size - 1
     b = matgen.matvec(*full, np.random.default_rng(1).uniform(-1, 1, n))
-    # Cgne squares the condition number: 4,710 counted iterations here
-    mi = 8000 if which == "cgne" else 2000
+    # Cgne and Lsqr square the condition number: 4,710 and 5,072 counted
+    # iterations here
+    mi = 8000 if which in ("cgne", "lsqr") else 2000
     outs = [_solve(api, which, full, False, b, 1, max_iter=mi) for _ in range(2)]
     assert outs[0][0] == outs[1][0] == 0
     assert outs[0][1].GetNumberIteration() == outs[1][1].GetNumberIteration()
@@ -188,7 +192,7 @@ def test_deterministic_and_larger(api, oracle, which):
 
 
 @pytest.mark.parametrize("which", ["cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicg", "cgne",
-                                   "bicgcr"])
+                                   "bicgcr", "lsqr"])
 def test_ilut(api, reference, which):
     # the host-driven loop with the device ILUT apply against the reference's
     # driver with its own factor
@@ -351,7 +355,8 @@ def test_cocg_runs_cg(api):
         assert np.array_equal(outs[0][2], outs[1][2])
 
 
-def test_cgne_transpose_storages(api, oracle):
+@pytest.mark.parametrize("which", ["cgne", "lsqr"])
+def test_cgne_transpose_storages(api, oracle, which):
     # the product by A^T over the explicit transpose (RowSparse) and over the
     # matrix itself (RowSymSparse), from an initial guess, with the identity,
     # Jacobi (M^{-1} M^{-T} in the passes) and SSOR (the host-driven loop)
@@ -362,9 +367,9 @@ def test_cgne_transpose_storages(api, oracle):
     x0 = rng.uniform(-1, 1, n)
     for A, sym in ((full, False), (matgen.upper(*full), True)):
         for pc in (0, 1, 2):
-            xo, co, no, _, _ = oracle.solve("cgne", *A, b, sym=sym, x0=x0, precond=pc,
+            xo, co, no, _, _ = oracle.solve(which, *A, b, sym=sym, x0=x0, precond=pc,
                                             omega=1.2, tol=1e-10, max_iter=2000)
-            code, it, x = _solve(api, "cgne", A, sym, b, pc, x0=x0)
+            code, it, x = _solve(api, which, A, sym, b, pc, x0=x0)
             assert code == co == 0, (sym, pc)
             assert abs(it.GetNumberIteration() - no) <= max(2, int(0.05 * no)), (sym, pc)
             assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-7, (sym, pc)

@@ -100,7 +100,7 @@ def test_mltadd_live(reference, oracle, seed):
 
 
 @pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr",
-                                   "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr"])
+                                   "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr", "lsqr"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
     ptr, ind, val = matgen.convdiff3d(5) if which not in ("cg", "minres") else matgen.lap2d(15)
@@ -201,7 +201,7 @@ def test_bicgstabl_no_progress_stops(oracle):
     assert (code, nb) == (1, 1) and len(h) == 2
 
 
-@pytest.mark.parametrize("which", ["bicg", "cgne"])
+@pytest.mark.parametrize("which", ["bicg", "cgne", "lsqr"])
 @pytest.mark.parametrize("sor_sym", [True, False])
 def test_bicg_transpose_live(reference, oracle, sor_sym, which):
     """BiCg's and Cgne's product by A^T: the reference's Mlt(SeldonTrans, ...)
@@ -282,7 +282,7 @@ def test_minres_indefinite_live(reference, oracle, pc, sym):
 
 
 @pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg",
-                                   "cgne", "bicgcr"])
+                                   "cgne", "bicgcr", "lsqr"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
@@ -411,7 +411,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
     for which in ("cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne",
-                  "bicgcr"):
+                  "bicgcr", "lsqr"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
