@@ -37,13 +37,14 @@
 //   JacobiPreconditioner<T>                   (absent from Seldon) z_i = r_i / A(i,i)
 //
 //   BiCg, BiCgcr, BiCgStabl, Cgne, Cgs,       BiCg.cxx:46-134, BiCgStabl.cxx:43-180,
-//   CoCg, Gcr, Lsqr, MinRes, QCgs, TfQmr      BiCgcr.cxx:44-118, Lsqr.cxx:40-135,
+//   CoCg, Gcr, Lsqr, MinRes, QCgs, QmrSym,    BiCgcr.cxx:44-118, Lsqr.cxx:40-135,
+//   TfQmr                                     QmrSym.cxx:41-165,
 //                                             Cgne.cxx:40-127, Cgs.cxx:45-132,
 //                                             CoCg.cxx:45-116, Gcr.cxx:45-141,
 //                                             MinRes.cxx:46-153, QCgs.cxx:46-165,
 //                                             TfQmr.cxx:44-243
 //
-// Seldon's other Krylov drivers (Qmr, QmrSym, Symmlq) need no
+// Seldon's other Krylov drivers (Qmr, Symmlq) need no
 // overload: their generic templates, instantiated on the device types, call
 // only the operations above, so every vector operation runs on the GPU.
 //
@@ -1608,7 +1609,7 @@ namespace Seldon
     enum SolverKind
     {
       kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs,
-      kBiCg, kCoCg, kCgne, kBiCgcr, kLsqr
+      kBiCg, kCoCg, kCgne, kBiCgcr, kLsqr, kQmrSym
     };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
@@ -1617,7 +1618,7 @@ namespace Seldon
       // TfQmr.cxx:116,138,148,186,219, MinRes.cxx:120,142, Gcr.cxx:108,
       // BiCgStabl.cxx:99,115, QCgs.cxx:86,108,138, BiCg.cxx:86,115 and
       // CoCg.cxx:84,102, Cgne.cxx:90,110, BiCgcr.cxx:85,101 and
-      // Lsqr.cxx:88,100,108 pass to Fail
+      // Lsqr.cxx:88,100,108 and QmrSym.cxx:83,95,114,121,140 pass to Fail
       if (kind == kCg)
         return code == 1 ? "Cg breakdown #1" : "Cg breakdown #2";
       if (kind == kCgs)
@@ -1639,6 +1640,13 @@ namespace Seldon
       if (kind == kLsqr)
         return code == 1 ? "Lsqr breakdown #1"
                          : (code == 2 ? "Lsqr breakdown #2" : "Lsqr breakdown #3");
+      if (kind == kQmrSym)
+        {
+          static const char* const qmr[] = {"Qmr breakdown #1", "Qmr breakdown #2",
+                                            "Qmr breakdown #3", "Qmr breakdown #4",
+                                            "Qmr breakdown #5"};
+          return qmr[code == 1 ? 0 : (code >= 3 && code <= 6 ? code - 2 : 4)];
+        }
       if (kind == kQCgs)
         return code == 1 ? "QCgs breakdown #1"
                          : (code == 2 ? "Qcgs breakdown #2" : "Qcgs breakdown #3");
@@ -1733,13 +1741,16 @@ namespace Seldon
       else if (kind == kLsqr)
         st = sb2_lsqr(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                       cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kQmrSym)
+        st = sb2_qmrsym(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                        cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
                                           "MinRes", "Gcr", "BiCgStabl", "QCgs", "BiCg",
-                                          "CoCg", "Cgne", "BiCgcr", "Lsqr"};
+                                          "CoCg", "Cgne", "BiCgcr", "Lsqr", "QmrSym"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1814,6 +1825,8 @@ namespace Seldon
           return Seldon::BiCgcr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kLsqr)
           return Seldon::Lsqr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kQmrSym)
+          return Seldon::QmrSym<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1960,6 +1973,25 @@ namespace Seldon
            Preconditioner& M, Iteration<Titer>& iter)
   {
     return b200::Solve(b200::kCoCg, A, x, b, M, iter);
+  }
+
+  //! QMR for symmetric systems on the GPU (QmrSym.cxx:41-165).
+  template <class Titer, class Prop, class Preconditioner>
+  int QmrSym(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+             Vector<double, VectFull, CudaAlloc<double> >& x,
+             const Vector<double, VectFull, CudaAlloc<double> >& b,
+             Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kQmrSym, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int QmrSym(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+             Vector<double, VectFull, CudaAlloc<double> >& x,
+             const Vector<double, VectFull, CudaAlloc<double> >& b,
+             Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kQmrSym, A, x, b, M, iter);
   }
 
   //! Lsqr on the GPU (Lsqr.cxx:40-135); the preconditioner is not used.

@@ -523,6 +523,15 @@ int sb2_lsqr(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              const sb2_iter_params* params, sb2_iter_result* result, double* hist,
              int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's QmrSym (QmrSym.cxx:41-165): QMR for symmetric systems, one
+ * product a step; arguments and history of sb2_cg.  Error codes are the
+ * reference's Fail codes 1, 3, 4, 5 and 6 (its messages number them #1 to
+ * #5).  The identity and Jacobi run as one persistent kernel per solve; SOR
+ * and ILUT drive the device operations from the host. */
+int sb2_qmrsym(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

@@ -138,6 +138,7 @@ namespace
       case 11: return Cgne(A, x, b, M, it);
       case 12: return BiCgcr(A, x, b, M, it);
       case 13: return Lsqr(A, x, b, M, it);
+      case 14: return QmrSym(A, x, b, M, it);
       default: return -100;
       }
   }

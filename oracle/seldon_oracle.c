@@ -1345,9 +1345,83 @@ out:
   return code;
 }
 
+/* QmrSym.cxx:41-165: QMR for symmetric systems, one product a step.  Its
+ * Fail codes are 1, 3, 4, 5 and 6 (the messages number them #1 to #5). */
+static int orc_qmrsym_impl(const orc_csr* A, double* x, const double* b,
+                           const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *r = malloc(bytes), *y = malloc(bytes), *v = malloc(bytes),
+         *pt = malloc(bytes), *p = malloc(bytes), *d = malloc(bytes), *s = malloc(bytes);
+  memcpy(r, b, bytes); memcpy(y, b, bytes); memcpy(v, b, bytes); memcpy(pt, b, bytes);
+  memcpy(p, b, bytes); memcpy(d, b, bytes); memcpy(s, b, bytes);
+  double delta, ep = 0.0, beta, rho, rho_1, theta_1, gamma_1;
+  double theta = 0.0, gamma = 1.0, eta = -1.0;
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  orc_copy(N, r, v);
+  prec_solve(M, A, v, y);
+  rho = orc_nrm2(N, y);
+  it->nb_iter = 0;
+  while (!it_finished(it, orc_nrm2(N, r))) {
+    if (rho == 0.0) { it_fail(it, 1); break; }
+    orc_scal(N, 1. / rho, v);
+    orc_scal(N, 1. / rho, y);
+    delta = orc_dot(N, v, y);
+    if (delta == 0.0) { it_fail(it, 3); break; }
+    if (it->nb_iter == 0)
+      orc_copy(N, y, p);
+    else {
+      orc_scal(N, -(rho * delta / ep), p);
+      orc_axpy(N, 1.0, y, p);
+    }
+    csr_mlt(A, p, pt);
+    ep = orc_dot(N, p, pt);
+    if (ep == 0.0) { it_fail(it, 4); break; }
+    beta = ep / delta;
+    if (beta == 0.0) { it_fail(it, 5); break; }
+    orc_scal(N, -beta, v);
+    orc_axpy(N, 1.0, pt, v);
+    prec_solve(M, A, v, y);
+    rho_1 = rho;
+    rho = orc_nrm2(N, y);
+    gamma_1 = gamma;
+    theta_1 = theta;
+    theta = rho / (gamma_1 * beta);
+    gamma = 1.0 / sqrt(1.0 + theta * theta);
+    if (gamma == 0.0) { it_fail(it, 6); break; }
+    eta = -eta * rho_1 * gamma * gamma / (beta * gamma_1 * gamma_1);
+    if (it->nb_iter == 0) {
+      orc_copy(N, p, d);
+      orc_scal(N, eta, d);
+      orc_copy(N, pt, s);
+      orc_scal(N, eta, s);
+    } else {
+      double tmp = theta_1 * theta_1 * gamma * gamma;
+      orc_scal(N, tmp, d);
+      orc_axpy(N, eta, p, d);
+      orc_scal(N, tmp, s);
+      orc_axpy(N, eta, pt, s);
+    }
+    orc_axpy(N, 1.0, d, x);
+    orc_axpy(N, -1.0, s, r);
+    it->nb_iter++;
+  }
+  code = it_error_code(it);
+out:
+  free(r); free(y); free(v); free(pt); free(p); free(d); free(s);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
  * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne, 12 BiCgcr,
- * 13 Lsqr.
+ * 13 Lsqr, 14 QmrSym.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1398,6 +1472,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_bicgcr_impl(&A, x, b, &M, &it);
   else if (which == 13)
     code = orc_lsqr_impl(&A, x, b, &it);
+  else if (which == 14)
+    code = orc_qmrsym_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

@@ -954,6 +954,12 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def QmrSym(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """QMR for symmetric systems (QmrSym.cxx:41-165); returns
+    Iteration::ErrorCode()."""
+    return _solve(_L.sb2_qmrsym, A, x, b, M, iteration, hist_cap, stream)
+
+
 def Lsqr(A, x, b, M, iteration, hist_cap=None, stream=None):
     """Lsqr (Lsqr.cxx:40-135); M is not used, as in the reference; returns
     Iteration::ErrorCode()."""

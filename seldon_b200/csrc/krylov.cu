@@ -17,7 +17,8 @@
 // References: Cg.cxx:45-116, BiCgStab.cxx:43-145, Gmres.cxx:44-183,
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
 // BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134, CoCg.cxx:45-116,
-// Cgne.cxx:40-127, BiCgcr.cxx:44-118, Lsqr.cxx:40-135, Iterative.cxx:235-354.
+// Cgne.cxx:40-127, BiCgcr.cxx:44-118, Lsqr.cxx:40-135, QmrSym.cxx:41-165,
+// Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2348,6 +2349,217 @@ __global__ void __launch_bounds__(NT, 4) cgne_fused_kernel(OpArgs A, CgneVecs v,
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- QmrSym
+
+struct QmrsVecs {
+  const double* b;
+  double *x, *r, *y, *v, *p, *pt, *d, *s;
+};
+
+// QmrSym (QmrSym.cxx:41-165): QMR for symmetric systems, one product a step.
+// Four grid barriers a step: the p pass; pt = A p fused with ep = (p, pt);
+// the v, y pass with ||y||^2; the d, s, x, r pass with ||r||^2, which also
+// scales v and y by the new 1 / rho and reduces the next step's
+// delta = (v, y) (the reference scales them at the top of its next step,
+// after the test, which reads neither).  Fail codes 1, 3, 4, 5, 6 as in the
+// reference.
+__global__ void __launch_bounds__(NT, 4) qmrsym_fused_kernel(OpArgs A, QmrsVecs v, IterArgs it,
+                                                          Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b)
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      v.r[i] = __ldg(v.b + i);
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // v = r; y = M^{-1} v; rho = ||y||; ||r||^2
+  double rr, rho;
+  {
+    double a0 = 0.0, a1 = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      const double ri = __ldcg(v.r + i);
+      const double yi = precond_val(A.diag, (int)i, ri);
+      v.v[i] = ri;
+      v.y[i] = yi;
+      a0 = add_rn(a0, mul_rn(yi, yi));
+      a1 = add_rn(a1, mul_rn(ri, ri));
+    }
+    a0 = block_sum<NT>(a0, s_red);
+    a1 = block_sum<NT>(a1, s_red);
+    if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+    if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+    rho = sqrt(s_vals[0]);
+    rr = s_vals[1];
+  }
+  // Mlt(1 / rho, v); Mlt(1 / rho, y); delta = (v, y)
+  double delta;
+  {
+    const double ir = 1. / rho;
+    double a0 = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      const double vi = mul_rn(__ldcg(v.v + i), ir), yi = mul_rn(__ldcg(v.y + i), ir);
+      v.v[i] = vi;
+      v.y[i] = yi;
+      a0 = add_rn(a0, mul_rn(vi, yi));
+    }
+    a0 = block_sum<NT>(a0, s_red);
+    if (tid == 0) s_vals[0] = a0;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    delta = s_vals[0];
+  }
+  double ep = 0.0, theta = 0.0, gamma = 1.0, eta = -1.0;
+
+  int nb_iter = 0, fail = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * sqrt(rr);
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (rho == 0.0) { fail = 1; break; }
+    if (delta == 0.0) { fail = 3; break; }
+    const bool first = nb_iter == 0;
+    // p = y (first) | Mlt(-(rho delta / ep), p); Add(1, y, p)
+    {
+      const double c = first ? 0.0 : -(mul_rn(rho, delta) / ep);
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> yi = ldw<W>(v.y, i);
+        if (first) {
+          stw<W>(v.p, i, yi);
+        } else {
+          Ents<W> pi = ldw<W>(v.p, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) pi.v[j] = add_rn(mul_rn(pi.v[j], c), yi.v[j]);
+          stw<W>(v.p, i, pi);
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+    }
+    // pt = A p with ep = (p, pt)
+    {
+      EpiStoreDot e{v.pt, v.p, 0.0};
+      spmv_phase(A, v.p, e, s_prod, s_red);
+      const double a = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = a;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    ep = s_vals[0];
+    if (ep == 0.0) { fail = 4; break; }
+    const double beta = ep / delta;
+    if (beta == 0.0) { fail = 5; break; }
+    // Mlt(-beta, v); Add(1, pt, v); y = M^{-1} v; rho = ||y||
+    {
+      double a0 = 0.0;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> vi = ldw<W>(v.v, i);
+        const Ents<W> pti = ldw<W>(v.pt, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) vi.v[j] = add_rn(mul_rn(vi.v[j], -beta), pti.v[j]);
+        const Ents<W> yi = precond_w<W>(A.diag, i, vi);
+        stw<W>(v.v, i, vi);
+        stw<W>(v.y, i, yi);
+#pragma unroll
+        for (int j = 0; j < W; j++) a0 = add_rn(a0, mul_rn(yi.v[j], yi.v[j]));
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      if (tid == 0) s_vals[0] = a0;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double rho_1 = rho;
+    rho = sqrt(s_vals[0]);
+    const double gamma_1 = gamma, theta_1 = theta;
+    theta = rho / mul_rn(gamma_1, beta);
+    gamma = 1.0 / sqrt(add_rn(1.0, mul_rn(theta, theta)));
+    if (gamma == 0.0) { fail = 6; break; }
+    eta = mul_rn(mul_rn(mul_rn(-eta, rho_1), gamma), gamma) /
+          mul_rn(mul_rn(beta, gamma_1), gamma_1);
+    // d, s; Add(1, d, x); Add(-1, s, r) with ||r||^2; then the next step's
+    // Mlt(1 / rho, v), Mlt(1 / rho, y) and delta = (v, y)
+    {
+      const double tmp = first ? 0.0 : mul_rn(mul_rn(mul_rn(theta_1, theta_1), gamma), gamma);
+      const double ir = 1. / rho;
+      const double et = eta;
+      double a0 = 0.0, a1 = 0.0;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> pi = ldw<W>(v.p, i), pti = ldw<W>(v.pt, i);
+        Ents<W> di, si;
+        if (first) {
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            di.v[j] = mul_rn(pi.v[j], et);
+            si.v[j] = mul_rn(pti.v[j], et);
+          }
+        } else {
+          di = ldw<W>(v.d, i);
+          si = ldw<W>(v.s, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            di.v[j] = mul_rn(di.v[j], tmp);
+            si.v[j] = mul_rn(si.v[j], tmp);
+            if (et != 0.0) {
+              di.v[j] = add_rn(di.v[j], mul_rn(et, pi.v[j]));
+              si.v[j] = add_rn(si.v[j], mul_rn(et, pti.v[j]));
+            }
+          }
+        }
+        stw<W>(v.d, i, di);
+        stw<W>(v.s, i, si);
+        Ents<W> xi = ldw<W>(v.x, i), ri = ldw<W>(v.r, i), vi = ldw<W>(v.v, i), yi = ldw<W>(v.y, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          xi.v[j] = add_rn(xi.v[j], di.v[j]);
+          ri.v[j] = add_rn(ri.v[j], -si.v[j]);
+          vi.v[j] = mul_rn(vi.v[j], ir);
+          yi.v[j] = mul_rn(yi.v[j], ir);
+          a0 = add_rn(a0, mul_rn(ri.v[j], ri.v[j]));
+          a1 = add_rn(a1, mul_rn(vi.v[j], yi.v[j]));
+        }
+        stw<W>(v.x, i, xi);
+        stw<W>(v.r, i, ri);
+        stw<W>(v.v, i, vi);
+        stw<W>(v.y, i, yi);
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      a1 = block_sum<NT>(a1, s_red);
+      if (tid == 0) { s_vals[0] = a0; s_vals[1] = a1; }
+      if (!grid_sync<NT>(P, epoch, 2, s_vals, s_red)) return;
+      rr = s_vals[0];
+      delta = s_vals[1];
+    }
+    nb_iter++;
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- Lsqr
 
 struct LsqrVecs {
@@ -2981,7 +3193,7 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
   kQcgs = 8, kBcg = 9,  // kBicg is BiCgStab, kBcg BiCg
-  kCgne = 10, kBcr = 11, kLsqr = 12  // kBcr BiCgcr
+  kCgne = 10, kBcr = 11, kLsqr = 12, kQmrs = 13  // kBcr BiCgcr, kQmrs QmrSym
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -3001,6 +3213,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kBicgl) { kern = (const void*)bicgstabl_fused_kernel; nvec = 2 + 2 * (prm->restart + 1); }
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
   if (which == kBcr) { kern = (const void*)bicgcr_fused_kernel; nvec = 6; }
+  if (which == kQmrs) { kern = (const void*)qmrsym_fused_kernel; nvec = 7; }
   if (which == kBcg || which == kCgne || which == kLsqr) {
     kern = which == kBcg    ? (const void*)bicg_fused_kernel
            : which == kCgne ? (const void*)cgne_fused_kernel
@@ -3045,6 +3258,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   CgneVecs nev;
   BcrVecs crv;
   LsqrVecs lsv;
+  QmrsVecs qsv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -3083,6 +3297,9 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   } else if (which == kBcr) {
     crv = BcrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn};
     args[1] = &crv;
+  } else if (which == kQmrs) {
+    qsv = QmrsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn};
+    args[1] = &qsv;
   } else if (which == kBcg || which == kCgne || which == kLsqr) {
     // Seldon's transpose of RowSymSparse storage is the matrix itself
     const CsrArrays& t = A->sym ? A->full : A->trans;
@@ -3698,6 +3915,72 @@ static int host_bicg(Ops& o, double* x, const double* b, const sb2_iter_params* 
   return SB2_OK;
 }
 
+static int host_qmrsym(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                       HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *r = V, *y = V + n, *v = V + 2 * n, *p = V + 3 * n, *pt = V + 4 * n, *d = V + 5 * n,
+         *s = V + 6 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(o.copy(r, v));
+  SB2_TRY(o.prec(v, y));
+  double rho, ep = 0.0, theta = 0.0, gamma = 1.0, eta = -1.0;
+  SB2_TRY(o.nrm(y, &rho));
+  it.nb_iter = 0;
+  for (;;) {
+    double res;
+    SB2_TRY(o.nrm(r, &res));
+    if (it.finished(res)) break;
+    if (rho == 0.0) { it.fail = 1; break; }
+    SB2_TRY(o.scal(1. / rho, v));
+    SB2_TRY(o.scal(1. / rho, y));
+    double delta;
+    SB2_TRY(o.dot(v, y, &delta));
+    if (delta == 0.0) { it.fail = 3; break; }
+    const bool first = it.nb_iter == 0;
+    if (first) SB2_TRY(o.copy(y, p));
+    else {
+      SB2_TRY(o.scal(-(rho * delta / ep), p));
+      SB2_TRY(o.axpy(1.0, y, p));
+    }
+    SB2_TRY(o.mlt(p, pt));
+    SB2_TRY(o.dot(p, pt, &ep));
+    if (ep == 0.0) { it.fail = 4; break; }
+    const double beta = ep / delta;
+    if (beta == 0.0) { it.fail = 5; break; }
+    SB2_TRY(o.scal(-beta, v));
+    SB2_TRY(o.axpy(1.0, pt, v));
+    SB2_TRY(o.prec(v, y));
+    const double rho_1 = rho;
+    SB2_TRY(o.nrm(y, &rho));
+    const double gamma_1 = gamma, theta_1 = theta;
+    theta = rho / (gamma_1 * beta);
+    gamma = 1.0 / std::sqrt(1.0 + theta * theta);
+    if (gamma == 0.0) { it.fail = 6; break; }
+    eta = -eta * rho_1 * gamma * gamma / (beta * gamma_1 * gamma_1);
+    if (first) {
+      SB2_TRY(o.copy(p, d));
+      SB2_TRY(o.scal(eta, d));
+      SB2_TRY(o.copy(pt, s));
+      SB2_TRY(o.scal(eta, s));
+    } else {
+      const double tmp = theta_1 * theta_1 * gamma * gamma;
+      SB2_TRY(o.scal(tmp, d));
+      SB2_TRY(o.axpy(eta, p, d));
+      SB2_TRY(o.scal(tmp, s));
+      SB2_TRY(o.axpy(eta, pt, s));
+    }
+    SB2_TRY(o.axpy(1.0, d, x));
+    SB2_TRY(o.axpy(-1.0, s, r));
+    it.nb_iter++;
+  }
+  return SB2_OK;
+}
+
 static int host_bicgcr(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
                        HostIter& it, double* V, int* init_failed) {
   const size_t n = o.n;
@@ -3897,6 +4180,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kBcg ? 8
                    : which == kCgne ? 4
                    : which == kBcr ? 6
+                   : which == kQmrs ? 7
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -3918,6 +4202,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kBcg) SB2_TRY(host_bicg(o, x, b, prm, it, V, &init_failed));
   else if (which == kCgne) SB2_TRY(host_cgne(o, x, b, prm, it, V, &init_failed));
   else if (which == kBcr) SB2_TRY(host_bicgcr(o, x, b, prm, it, V, &init_failed));
+  else if (which == kQmrs) SB2_TRY(host_qmrsym(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -4481,6 +4766,14 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cocg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_qmrsym(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_qmrsym");
+  return solve_entry(kQmrs, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 
