@@ -19,7 +19,7 @@ REF_SO = os.path.join(HERE, "_ref", "libseldon_ref.so")
 # the `which` numbers of orc_solve / ref_solve
 _SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "cgs": 3, "tfqmr": 4, "minres": 5, "gcr": 6,
             "bicgstabl": 7, "qcgs": 8, "bicg": 9, "cocg": 10, "cgne": 11,
-            "bicgcr": 12, "lsqr": 13, "qmrsym": 14}
+            "bicgcr": 12, "lsqr": 13, "qmrsym": 14, "symmlq": 15}
 REF_FAST_SO = os.path.join(HERE, "_ref", "libseldon_ref_fast.so")
 
 _vp = ctypes.c_void_p

@@ -139,6 +139,7 @@ namespace
       case 12: return BiCgcr(A, x, b, M, it);
       case 13: return Lsqr(A, x, b, M, it);
       case 14: return QmrSym(A, x, b, M, it);
+      case 15: return Symmlq(A, x, b, M, it);
       default: return -100;
       }
   }

@@ -1419,9 +1419,93 @@ out:
   return code;
 }
 
+/* Symmlq.cxx:45-161: SYMMLQ (Lanczos with an LQ factorisation).  The first
+ * test is on ||b|| even from an initial guess; later ones on the estimate
+ * s_prod / |c|.  x takes its last correction ceta_bar * w_bar after the
+ * loop, whichever way the loop ended.  No Fail code. */
+static int orc_symmlq_impl(const orc_csr* A, double* x, const double* b,
+                           const orc_prec* M, orc_iter* it) {
+  const int N = A->m;
+  if (N <= 0) return 0;
+  size_t bytes = (size_t)N * sizeof(double);
+  double *r = malloc(bytes), *z = malloc(bytes), *u = malloc(bytes), *v = malloc(bytes),
+         *w = calloc(N, sizeof(double)), *u_old = calloc(N, sizeof(double)),
+         *v_old = calloc(N, sizeof(double)), *w_bar = calloc(N, sizeof(double));
+  memcpy(r, b, bytes); memcpy(z, b, bytes); memcpy(u, b, bytes); memcpy(v, b, bytes);
+  double alpha, beta, ibeta, beta_old, beta1, ceta = 0.0, ceta_oold, ceta_old, ceta_bar;
+  double c, cold, s, sold, coold, soold, rho0, rho1, rho2, rho3, dp, np, s_prod;
+  int code;
+  if (it_init(it, N, b) != 0) { code = it_error_code(it); goto out; }
+  orc_copy(N, b, r);
+  if (!it->init_guess_null)
+    csr_residual(A, x, r);
+  else
+    memset(x, 0, bytes);
+  ceta_oold = 0.0; ceta_old = 0.0;
+  c = 1.0; cold = 1.0; s = 0.0; sold = 0.0;
+  prec_solve(M, A, r, z);
+  dp = orc_dot(N, r, z);
+  dp = sqrt(dp); beta = dp; beta1 = beta;
+  s_prod = fabs(beta1);
+  orc_copy(N, r, v); orc_copy(N, z, u);
+  ibeta = 1.0 / beta;
+  orc_scal(N, ibeta, v); orc_scal(N, ibeta, u);
+  orc_copy(N, u, w_bar);
+  np = orc_nrm2(N, b);
+  it->nb_iter = 0;
+  while (!it_finished(it, np)) {
+    if (it->nb_iter != 0) {
+      orc_copy(N, v, v_old); orc_copy(N, u, u_old);
+      ibeta = 1.0 / beta;
+      orc_copy(N, r, v); orc_scal(N, ibeta, v);
+      orc_copy(N, z, u); orc_scal(N, ibeta, u);
+      orc_copy(N, w_bar, w); orc_scal(N, c, w); orc_axpy(N, s, u, w);
+      orc_scal(N, -s, w_bar); orc_axpy(N, c, u, w_bar);
+      orc_axpy(N, ceta, w, x);
+      ceta_oold = ceta_old;
+      ceta_old = ceta;
+    }
+    csr_mlt(A, u, r);
+    alpha = orc_dot(N, u, r);
+    prec_solve(M, A, r, z);
+    orc_axpy(N, -alpha, v, r);
+    orc_axpy(N, -alpha, u, z);
+    orc_axpy(N, -beta, v_old, r);
+    orc_axpy(N, -beta, u_old, z);
+    beta_old = beta;
+    dp = orc_dot(N, r, z);
+    beta = sqrt(dp);
+    coold = cold; cold = c; soold = sold; sold = s;
+    rho0 = cold * alpha - coold * sold * beta_old;
+    rho1 = sqrt(rho0 * rho0 + beta * beta);
+    rho2 = sold * alpha + coold * cold * beta_old;
+    rho3 = soold * beta_old;
+    c = rho0 / rho1; s = beta / rho1;
+    if (it->nb_iter == 0)
+      ceta = beta1 / rho1;
+    else
+      ceta = -(rho2 * ceta_old + rho3 * ceta_oold) / rho1;
+    s_prod *= fabs(s);
+    if (c == 0.0)
+      np = s_prod * 1e16;
+    else
+      np = s_prod / fabs(c);
+    it->nb_iter++;
+  }
+  if (c == 0.0)
+    ceta_bar = ceta * 1e15;
+  else
+    ceta_bar = ceta / c;
+  orc_axpy(N, ceta_bar, w_bar, x);
+  code = it_error_code(it);
+out:
+  free(r); free(z); free(u); free(v); free(w); free(u_old); free(v_old); free(w_bar);
+  return code;
+}
+
 /* C entry used by tests.  which: 0 Cg, 1 BiCgStab, 2 Gmres, 3 Cgs, 4 TfQmr,
  * 5 MinRes, 6 Gcr, 7 BiCgStabl, 8 QCgs, 9 BiCg, 10 CoCg, 11 Cgne, 12 BiCgcr,
- * 13 Lsqr, 14 QmrSym.
+ * 13 Lsqr, 14 QmrSym, 15 Symmlq.
  * precond: 0 identity, 1 Jacobi, 2 SOR (omega, sor_iter, sor_sym).
  * hist/hist_it (may be NULL) receive the relative residual and iteration
  * number of every Finished() test, hist_len their count.
@@ -1474,6 +1558,8 @@ int orc_solve(int which, int m, int nnz, const int* ptr, const int* ind,
     code = orc_lsqr_impl(&A, x, b, &it);
   else if (which == 14)
     code = orc_qmrsym_impl(&A, x, b, &M, &it);
+  else if (which == 15)
+    code = orc_symmlq_impl(&A, x, b, &M, &it);
   else
     code = orc_gmres_impl(&A, x, b, &M, &it, restart);
   free(M.diag);

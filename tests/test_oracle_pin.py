@@ -101,10 +101,10 @@ def test_mltadd_live(reference, oracle, seed):
 
 @pytest.mark.parametrize("which", ["cg", "bicgstab", "gmres", "cgs", "tfqmr", "minres", "gcr",
                                    "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr", "lsqr",
-                                   "qmrsym"])
+                                   "qmrsym", "symmlq"])
 @pytest.mark.parametrize("pc", [0, 1, 2])
 def test_solvers_live(reference, oracle, which, pc):
-    ptr, ind, val = (matgen.convdiff3d(5) if which not in ("cg", "minres", "qmrsym")
+    ptr, ind, val = (matgen.convdiff3d(5) if which not in ("cg", "minres", "qmrsym", "symmlq")
                      else matgen.lap2d(15))
     m = ptr.size - 1
     rng = np.random.default_rng(7)
@@ -284,7 +284,7 @@ def test_minres_indefinite_live(reference, oracle, pc, sym):
 
 
 @pytest.mark.parametrize("which", ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg",
-                                   "cgne", "bicgcr", "lsqr", "qmrsym"])
+                                   "cgne", "bicgcr", "lsqr", "qmrsym", "symmlq"])
 def test_cgs_tfqmr_edges_live(reference, oracle, which):
     for name, (p, i, v), b, x0, kw in _edge_solves():
         for pc in (0, 1, 2):
@@ -413,7 +413,7 @@ def test_nonfinite_inputs_live(oracle, reference, name):
     # Cgs counts two per loop and TfQmr's scalars may vanish on an infinite
     # product: the codes and counts are the reference's, whatever they are
     for which in ("cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne",
-                  "bicgcr", "lsqr", "qmrsym"):
+                  "bicgcr", "lsqr", "qmrsym", "symmlq"):
         for pc in (0, 1, 2):
             xo, co, no, _, _ = oracle.solve(which, p, i, v, b, x0=x0, precond=pc, tol=1e-10,
                                             max_iter=25)
