@@ -724,7 +724,7 @@ def extra_gmres(api, matgen, torch, dev, timed, jobs, g=GRID):
 
 def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
     """Bytes a persistent BiCg, BiCgStab, Cgs, TfQmr, QCgs, Cgne, Lsqr, BiCgcr,
-    QmrSym, MinRes, Gcr or BiCgStabl solve of
+    QmrSym, Symmlq, MinRes, Gcr or BiCgStabl solve of
     `iterations` (Seldon's count) reads and writes: its products
     (nnz*12 + 4(n+1) each) plus the vector streams of its passes and product
     epilogues, the gathered operand counted once per product.
@@ -742,6 +742,7 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
       minres    per iteration: one product, 20 vectors (+1 with Jacobi)
       bicgcr    per iteration: one product, 19 vectors (+1 with Jacobi)
       qmrsym    per iteration: one product, 23 vectors (+1 with Jacobi)
+      symmlq    per iteration: one product, 18 vectors (+1 with Jacobi)
       gcr       per inner step j of a cycle (two counted iterations): two
                 products, 2j + 14 vectors (the j + 1 projections and the
                 j + 1 terms of the new direction; +2 with Jacobi); per cycle
@@ -760,6 +761,8 @@ def krylov_bytes(which, n, nnz, jacobi, iterations, restart=10):
         return iterations * (prod + (19 + jacobi) * n * 8)
     if which == "qmrsym":
         return iterations * (prod + (23 + jacobi) * n * 8)
+    if which == "symmlq":
+        return iterations * (prod + (18 + jacobi) * n * 8)
     if which == "gcr":
         steps, cycle, total = int(iterations // 2), max((restart + 1) // 2, 1), 0
         for k in range(steps):
@@ -784,8 +787,8 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     """Seldon's other drivers, each one persistent kernel per solve, against
     the reference's own drivers on one host core, all with Jacobi:
     BiCg, BiCgStab, Cgs, QCgs, TfQmr and BiCgStabl(4) on the 128^3
-    convection-diffusion operator, MinRes and QmrSym on the 128^3 Poisson
-    operator,
+    convection-diffusion operator, MinRes, QmrSym and Symmlq on the 128^3
+    Poisson operator,
     Gcr(10), Cgne, Lsqr and BiCgcr on the 64^3 convection-diffusion operator
     (their iteration counts grow with the grid: Gcr's 768 at 32^3, 1494 at
     48^3; Cgne's 6080 at 48^3, 10072 at 64^3, the normal equations squaring
@@ -793,7 +796,7 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     64^3).  Lsqr uses no preconditioner.  BiCg.cxx:46-134, BiCgStab.cxx:43-145,
     Cgs.cxx:45-132, QCgs.cxx:46-165, TfQmr.cxx:44-243, BiCgStabl.cxx:43-180,
     MinRes.cxx:46-153, Gcr.cxx:45-141, Cgne.cxx:40-127, BiCgcr.cxx:44-118,
-    Lsqr.cxx:40-135, QmrSym.cxx:41-165.
+    Lsqr.cxx:40-135, QmrSym.cxx:41-165, Symmlq.cxx:45-161.
 
     BiCg's, Cgne's and Lsqr's products by A^T are, in the reference,
     MltAdd(alpha, SeldonTrans, M, X, beta, Y)'s generic loop over every
@@ -805,11 +808,11 @@ def extra_krylov(api, matgen, torch, dev, timed, jobs, g=GRID):
     fns = {"bicg": api.BiCg, "bicgstab": api.BiCgStab, "cgs": api.Cgs, "qcgs": api.QCgs,
            "tfqmr": api.TfQmr, "bicgstabl": api.BiCgStabl, "gcr": api.Gcr,
            "cgne": api.Cgne, "lsqr": api.Lsqr, "bicgcr": api.BiCgcr, "minres": api.MinRes,
-           "qmrsym": api.QmrSym}
+           "qmrsym": api.QmrSym, "symmlq": api.Symmlq}
     restarts = {"bicgstabl": 4, "gcr": 10}
     systems = {}
     for which, fn in fns.items():
-        op = "poisson" if which in ("minres", "qmrsym") else "convdiff"
+        op = "poisson" if which in ("minres", "qmrsym", "symmlq") else "convdiff"
         gg = g // 2 if which in ("gcr", "cgne", "lsqr", "bicgcr") else g
         if (op, gg) not in systems:
             ptr, ind, val = matgen.poisson3d(gg) if op == "poisson" else matgen.convdiff3d(gg)

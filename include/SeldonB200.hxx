@@ -38,15 +38,15 @@
 //
 //   BiCg, BiCgcr, BiCgStabl, Cgne, Cgs,       BiCg.cxx:46-134, BiCgStabl.cxx:43-180,
 //   CoCg, Gcr, Lsqr, MinRes, QCgs, QmrSym,    BiCgcr.cxx:44-118, Lsqr.cxx:40-135,
-//   TfQmr                                     QmrSym.cxx:41-165,
+//   Symmlq, TfQmr                             QmrSym.cxx:41-165, Symmlq.cxx:45-161,
 //                                             Cgne.cxx:40-127, Cgs.cxx:45-132,
 //                                             CoCg.cxx:45-116, Gcr.cxx:45-141,
 //                                             MinRes.cxx:46-153, QCgs.cxx:46-165,
 //                                             TfQmr.cxx:44-243
 //
-// Seldon's other Krylov drivers (Qmr, Symmlq) need no
-// overload: their generic templates, instantiated on the device types, call
-// only the operations above, so every vector operation runs on the GPU.
+// Seldon's other Krylov driver (Qmr) needs no overload: its generic
+// template, instantiated on the device types, calls only the operations
+// above, so every vector operation runs on the GPU.
 //
 // The solver overloads run the library's fused kernels when the
 // preconditioner is Preconditioner_Base, JacobiPreconditioner or
@@ -1609,7 +1609,7 @@ namespace Seldon
     enum SolverKind
     {
       kCg, kBiCgStab, kGmres, kGmresCgs2, kCgs, kTfQmr, kMinRes, kGcr, kBiCgStabl, kQCgs,
-      kBiCg, kCoCg, kCgne, kBiCgcr, kLsqr, kQmrSym
+      kBiCg, kCoCg, kCgne, kBiCgcr, kLsqr, kQmrSym, kSymmlq
     };
 
     inline const char* BreakdownMessage(SolverKind kind, int code)
@@ -1744,13 +1744,17 @@ namespace Seldon
       else if (kind == kQmrSym)
         st = sb2_qmrsym(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                         cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
+      else if (kind == kSymmlq)
+        st = sb2_symmlq(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
+                        cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap, GetStream());
       else
         st = sb2_gmres_cgs2(A.GetHandle(), ph.use, x.GetData(), b.GetData(), &prm, &res,
                             cap ? &hist[0] : NULL, cap ? &hist_it[0] : NULL, cap,
                             GetStream());
       static const char* const names[] = {"Cg", "BiCgStab", "Gmres", "Gmres", "Cgs", "TfQmr",
                                           "MinRes", "Gcr", "BiCgStabl", "QCgs", "BiCg",
-                                          "CoCg", "Cgne", "BiCgcr", "Lsqr", "QmrSym"};
+                                          "CoCg", "Cgne", "BiCgcr", "Lsqr", "QmrSym",
+                                          "Symmlq"};
       Check(st, names[kind]);
       // Init() found a zero right-hand side: Seldon returns at once
       if (res.init_failed)
@@ -1827,6 +1831,8 @@ namespace Seldon
           return Seldon::Lsqr<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         if (kind == kQmrSym)
           return Seldon::QmrSym<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
+        if (kind == kSymmlq)
+          return Seldon::Symmlq<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
         return Seldon::Gmres<Titer, MatrixD, VectorD, P>(A, x, b, M, iter);
       }
     };
@@ -1973,6 +1979,25 @@ namespace Seldon
            Preconditioner& M, Iteration<Titer>& iter)
   {
     return b200::Solve(b200::kCoCg, A, x, b, M, iter);
+  }
+
+  //! Symmlq on the GPU (Symmlq.cxx:45-161).
+  template <class Titer, class Prop, class Preconditioner>
+  int Symmlq(Matrix<double, Prop, RowSparse, CudaAlloc<double> >& A,
+             Vector<double, VectFull, CudaAlloc<double> >& x,
+             const Vector<double, VectFull, CudaAlloc<double> >& b,
+             Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kSymmlq, A, x, b, M, iter);
+  }
+
+  template <class Titer, class Prop, class Preconditioner>
+  int Symmlq(Matrix<double, Prop, RowSymSparse, CudaAlloc<double> >& A,
+             Vector<double, VectFull, CudaAlloc<double> >& x,
+             const Vector<double, VectFull, CudaAlloc<double> >& b,
+             Preconditioner& M, Iteration<Titer>& iter)
+  {
+    return b200::Solve(b200::kSymmlq, A, x, b, M, iter);
   }
 
   //! QMR for symmetric systems on the GPU (QmrSym.cxx:41-165).

@@ -532,6 +532,17 @@ int sb2_qmrsym(const sb2_csr* A, const sb2_precond* M, double* x, const double* 
                const sb2_iter_params* params, sb2_iter_result* result, double* hist,
                int* hist_it, int hist_cap, void* stream);
 
+/* Seldon's Symmlq (Symmlq.cxx:45-161): Lanczos with an LQ factorisation, one
+ * product a step; arguments and history of sb2_cg, no breakdown code.  The
+ * first test is on ||b|| even from an initial guess, the later ones on the
+ * recurrence's estimate; x takes its last correction after the loop however
+ * it ended, as in the reference.  The identity and Jacobi run as one
+ * persistent kernel per solve; SOR and ILUT drive the device operations
+ * from the host. */
+int sb2_symmlq(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream);
+
 /* Gmres(m) with classical Gram-Schmidt applied twice (CGS2) in place of the
  * reference's modified Gram-Schmidt loop (Gmres.cxx:127-132): each Arnoldi
  * step projects the new vector on the whole basis at once, twice, so it

@@ -203,7 +203,7 @@ _SOLVER_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IterParam
                 ctypes.POINTER(IterResult), c_void_p, c_void_p, ctypes.c_int, c_void_p]
 for _name in ("sb2_cg", "sb2_bicgstab", "sb2_gmres", "sb2_gmres_cgs2", "sb2_cgs", "sb2_tfqmr",
               "sb2_minres", "sb2_gcr", "sb2_bicgstabl", "sb2_qcgs", "sb2_bicg", "sb2_cocg",
-              "sb2_cgne", "sb2_bicgcr", "sb2_lsqr", "sb2_qmrsym"):
+              "sb2_cgne", "sb2_bicgcr", "sb2_lsqr", "sb2_qmrsym", "sb2_symmlq"):
     _PROTOS.append((_name, ctypes.c_int, _SOLVER_ARGS))
 _PROTOS.append(("sb2_ir_solve", ctypes.c_int,
                 [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.POINTER(IrParams),

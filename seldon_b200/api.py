@@ -954,6 +954,11 @@ def Gcr(A, x, b, M, iteration, hist_cap=None, stream=None):
     return _solve(_L.sb2_gcr, A, x, b, M, iteration, hist_cap, stream)
 
 
+def Symmlq(A, x, b, M, iteration, hist_cap=None, stream=None):
+    """Symmlq (Symmlq.cxx:45-161); returns Iteration::ErrorCode()."""
+    return _solve(_L.sb2_symmlq, A, x, b, M, iteration, hist_cap, stream)
+
+
 def QmrSym(A, x, b, M, iteration, hist_cap=None, stream=None):
     """QMR for symmetric systems (QmrSym.cxx:41-165); returns
     Iteration::ErrorCode()."""

@@ -18,7 +18,7 @@
 // Cgs.cxx:45-132, TfQmr.cxx:44-243, MinRes.cxx:46-153, Gcr.cxx:45-141,
 // BiCgStabl.cxx:43-180, QCgs.cxx:46-165, BiCg.cxx:46-134, CoCg.cxx:45-116,
 // Cgne.cxx:40-127, BiCgcr.cxx:44-118, Lsqr.cxx:40-135, QmrSym.cxx:41-165,
-// Iterative.cxx:235-354.
+// Symmlq.cxx:45-161, Iterative.cxx:235-354.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -2349,6 +2349,208 @@ __global__ void __launch_bounds__(NT, 4) cgne_fused_kernel(OpArgs A, CgneVecs v,
   if (lead) write_out(out, nb_iter, it.max_iter, fail, facteur, reste, hlen);
 }
 
+// ----------------------------------------------------------------- Symmlq
+
+struct SymmlqVecs {
+  const double* b;
+  double *x, *r, *z, *w, *w_bar, *u0, *u1, *v0, *v1;  // u, u_old and v, v_old by rotation
+};
+
+// Symmlq (Symmlq.cxx:45-161): Lanczos with an LQ factorisation, one product
+// a step.  Three grid barriers a step: the update pass (v = r / beta,
+// u = z / beta, w, w_bar, x += ceta w; the old u and v kept by pointer
+// rotation); r = A u fused with alpha = (u, r); the pass z = M^{-1} r,
+// r -= alpha v + beta v_old, z -= alpha u + beta u_old with (r, z).  The
+// first test is on ||b|| even from an initial guess; x takes
+// ceta_bar * w_bar after the loop, as in the reference.
+__global__ void __launch_bounds__(NT, 4) symmlq_fused_kernel(OpArgs A, SymmlqVecs v, IterArgs it,
+                                                          Persist P, History H, SolveOut* out) {
+  SB2_SHARED_DECL;
+  const int tid = threadIdx.x;
+  const long long gt = (long long)blockIdx.x * NT + tid, gs = (long long)gridDim.x * NT;
+  const int n = A.n;
+  const bool lead = (blockIdx.x == 0 && tid == 0);
+  unsigned epoch = 0;
+  int hlen = 0;
+
+  double acc = 0.0;
+  for (long long i = gt; i < n; i += gs) {
+    const double bi = __ldg(v.b + i);
+    acc = add_rn(acc, mul_rn(bi, bi));
+  }
+  acc = block_sum<NT>(acc, s_red);
+  if (tid == 0) s_vals[0] = acc;
+  if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  const double normb = sqrt(s_vals[0]);
+  if (normb == 0.0) {
+    if (lead) { out->init_failed = 1; out->hist_len = 0; }
+    return;
+  }
+  const double facteur = 1.0 / normb;
+
+  // r = b - A x (or x = 0, r = b)
+  if (it.init_guess_null) {
+    for (long long i = gt; i < n; i += gs) {
+      v.x[i] = 0.0;
+      v.r[i] = __ldg(v.b + i);
+    }
+  } else {
+    EpiResidual epi{v.b, v.r, nullptr, 0.0, 0.0};
+    spmv_phase(A, v.x, epi, s_prod, s_red);
+  }
+  if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  // z = M^{-1} r; dp = (r, z)
+  {
+    double a0 = 0.0;
+    for (long long i = gt; i < n; i += gs) {
+      const double ri = __ldcg(v.r + i);
+      const double zi = precond_val(A.diag, (int)i, ri);
+      v.z[i] = zi;
+      a0 = add_rn(a0, mul_rn(ri, zi));
+    }
+    a0 = block_sum<NT>(a0, s_red);
+    if (tid == 0) s_vals[0] = a0;
+    if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+  }
+  double beta = sqrt(s_vals[0]);
+  const double beta1 = beta;
+  double sprod = fabs(beta1);
+  double *u = v.u0, *u_old = v.u1, *vv = v.v0, *v_old = v.v1;
+  // v = r / beta; u = z / beta; w_bar = u; u_old = v_old = 0
+  {
+    const double ib = 1.0 / beta;
+    for (long long i = gt; i < n; i += gs) {
+      const double ui = mul_rn(__ldcg(v.z + i), ib);
+      vv[i] = mul_rn(__ldcg(v.r + i), ib);
+      u[i] = ui;
+      v.w_bar[i] = ui;
+      u_old[i] = 0.0;
+      v_old[i] = 0.0;
+    }
+    if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+  }
+  double ceta = 0.0, ceta_old = 0.0, ceta_oold = 0.0;
+  double c = 1.0, cold = 1.0, s = 0.0, sold = 0.0;
+  double np = normb;
+
+  int nb_iter = 0;
+  double reste;
+  for (;;) {
+    reste = facteur * np;
+    if (lead) hist_push(H, &hlen, nb_iter, reste);
+    if (reste < it.tol || nb_iter >= it.max_iter) break;
+    if (nb_iter != 0) {
+      // v_old = v; u_old = u (rotation); v = r / beta; u = z / beta;
+      // w = c w_bar + s u; w_bar = -s w_bar + c u; x += ceta w
+      double* t = v_old; v_old = vv; vv = t;
+      t = u_old; u_old = u; u = t;
+      const double ib = 1.0 / beta, cc = c, ss = s, ce = ceta;
+      vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        const Ents<W> ri = ldw<W>(v.r, i), zi = ldw<W>(v.z, i);
+        Ents<W> vi, ui, wi, wb = ldw<W>(v.w_bar, i);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+          vi.v[j] = mul_rn(ri.v[j], ib);
+          ui.v[j] = mul_rn(zi.v[j], ib);
+          wi.v[j] = mul_rn(wb.v[j], cc);
+          if (ss != 0.0) wi.v[j] = add_rn(wi.v[j], mul_rn(ss, ui.v[j]));
+          wb.v[j] = mul_rn(wb.v[j], -ss);
+          if (cc != 0.0) wb.v[j] = add_rn(wb.v[j], mul_rn(cc, ui.v[j]));
+        }
+        stw<W>(vv, i, vi);
+        stw<W>(u, i, ui);
+        stw<W>(v.w, i, wi);
+        stw<W>(v.w_bar, i, wb);
+        if (ce != 0.0) {
+          Ents<W> xi = ldw<W>(v.x, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(ce, wi.v[j]));
+          stw<W>(v.x, i, xi);
+        }
+      });
+      if (!grid_sync<NT>(P, epoch, 0, s_vals, s_red)) return;
+      ceta_oold = ceta_old;
+      ceta_old = ceta;
+    }
+    // r = A u with alpha = (u, r)
+    {
+      EpiStoreDot e{v.r, u, 0.0};
+      spmv_phase(A, u, e, s_prod, s_red);
+      const double a = block_sum<NT>(e.acc, s_red);
+      if (tid == 0) s_vals[0] = a;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double alpha = s_vals[0];
+    // z = M^{-1} r; Add(-alpha, v, r); Add(-alpha, u, z); Add(-beta, v_old, r);
+    // Add(-beta, u_old, z); dp = (r, z)
+    {
+      double a0 = 0.0;
+      const double na = -alpha, nbt = -beta;
+      vec_pass(n, gt, gs, true, [&](auto wc, long long i) {
+        constexpr int W = decltype(wc)::value;
+        Ents<W> ri = ldw<W>(v.r, i);
+        Ents<W> zi = precond_w<W>(A.diag, i, ri);
+        if (na != 0.0) {
+          const Ents<W> vi = ldw<W>(vv, i), ui = ldw<W>(u, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            ri.v[j] = add_rn(ri.v[j], mul_rn(na, vi.v[j]));
+            zi.v[j] = add_rn(zi.v[j], mul_rn(na, ui.v[j]));
+          }
+        }
+        if (nbt != 0.0) {
+          const Ents<W> vo = ldw<W>(v_old, i), uo = ldw<W>(u_old, i);
+#pragma unroll
+          for (int j = 0; j < W; j++) {
+            ri.v[j] = add_rn(ri.v[j], mul_rn(nbt, vo.v[j]));
+            zi.v[j] = add_rn(zi.v[j], mul_rn(nbt, uo.v[j]));
+          }
+        }
+        stw<W>(v.r, i, ri);
+        stw<W>(v.z, i, zi);
+#pragma unroll
+        for (int j = 0; j < W; j++) a0 = add_rn(a0, mul_rn(ri.v[j], zi.v[j]));
+      });
+      a0 = block_sum<NT>(a0, s_red);
+      if (tid == 0) s_vals[0] = a0;
+      if (!grid_sync<NT>(P, epoch, 1, s_vals, s_red)) return;
+    }
+    const double beta_old = beta;
+    beta = sqrt(s_vals[0]);
+    // the QR factorisation and the Givens rotation
+    const double coold = cold, soold = sold;
+    cold = c;
+    sold = s;
+    const double rho0 = add_rn(mul_rn(cold, alpha), -mul_rn(mul_rn(coold, sold), beta_old));
+    const double rho1 = sqrt(add_rn(mul_rn(rho0, rho0), mul_rn(beta, beta)));
+    const double rho2 = add_rn(mul_rn(sold, alpha), mul_rn(mul_rn(coold, cold), beta_old));
+    const double rho3 = mul_rn(soold, beta_old);
+    c = rho0 / rho1;
+    s = beta / rho1;
+    if (nb_iter == 0)
+      ceta = beta1 / rho1;
+    else
+      ceta = -add_rn(mul_rn(rho2, ceta_old), mul_rn(rho3, ceta_oold)) / rho1;
+    sprod = mul_rn(sprod, fabs(s));
+    np = c == 0.0 ? mul_rn(sprod, 1e16) : sprod / fabs(c);
+    nb_iter++;
+  }
+  // Add(ceta_bar, w_bar, x)
+  const double ceta_bar = c == 0.0 ? mul_rn(ceta, 1e15) : ceta / c;
+  if (ceta_bar != 0.0) {
+    vec_pass(n, gt, gs, al16(v.x), [&](auto wc, long long i) {
+      constexpr int W = decltype(wc)::value;
+      Ents<W> xi = ldw<W>(v.x, i);
+      const Ents<W> wb = ldw<W>(v.w_bar, i);
+#pragma unroll
+      for (int j = 0; j < W; j++) xi.v[j] = add_rn(xi.v[j], mul_rn(ceta_bar, wb.v[j]));
+      stw<W>(v.x, i, xi);
+    });
+  }
+  if (lead) write_out(out, nb_iter, it.max_iter, 0, facteur, reste, hlen);
+}
+
 // ----------------------------------------------------------------- QmrSym
 
 struct QmrsVecs {
@@ -3193,7 +3395,8 @@ static OpArgs op_args(const sb2_csr* A, const double* diag) {
 enum Solver {
   kCg = 0, kBicg = 1, kGmres = 2, kCgs = 3, kTfqmr = 4, kMinres = 5, kGcr = 6, kBicgl = 7,
   kQcgs = 8, kBcg = 9,  // kBicg is BiCgStab, kBcg BiCg
-  kCgne = 10, kBcr = 11, kLsqr = 12, kQmrs = 13  // kBcr BiCgcr, kQmrs QmrSym
+  kCgne = 10, kBcr = 11, kLsqr = 12, kQmrs = 13,  // kBcr BiCgcr, kQmrs QmrSym
+  kSymm = 14                                     // Symmlq
 };
 
 static int fused_solve(int which, const sb2_csr* A, const double* diag, double* x,
@@ -3214,6 +3417,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   if (which == kQcgs) { kern = (const void*)qcgs_fused_kernel; nvec = 10; }
   if (which == kBcr) { kern = (const void*)bicgcr_fused_kernel; nvec = 6; }
   if (which == kQmrs) { kern = (const void*)qmrsym_fused_kernel; nvec = 7; }
+  if (which == kSymm) { kern = (const void*)symmlq_fused_kernel; nvec = 8; }
   if (which == kBcg || which == kCgne || which == kLsqr) {
     kern = which == kBcg    ? (const void*)bicg_fused_kernel
            : which == kCgne ? (const void*)cgne_fused_kernel
@@ -3259,6 +3463,7 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   BcrVecs crv;
   LsqrVecs lsv;
   QmrsVecs qsv;
+  SymmlqVecs syv;
   args[0] = &op;
   args[2] = &it;
   args[3] = &P;
@@ -3297,6 +3502,10 @@ static int fused_solve(int which, const sb2_csr* A, const double* diag, double* 
   } else if (which == kBcr) {
     crv = BcrVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn};
     args[1] = &crv;
+  } else if (which == kSymm) {
+    syv = SymmlqVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn,
+                     V + 7 * nn};
+    args[1] = &syv;
   } else if (which == kQmrs) {
     qsv = QmrsVecs{b, x, V, V + nn, V + 2 * nn, V + 3 * nn, V + 4 * nn, V + 5 * nn, V + 6 * nn};
     args[1] = &qsv;
@@ -3915,6 +4124,83 @@ static int host_bicg(Ops& o, double* x, const double* b, const sb2_iter_params* 
   return SB2_OK;
 }
 
+static int host_symmlq(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
+                       HostIter& it, double* V, int* init_failed) {
+  const size_t n = o.n;
+  double *r = V, *z = V + n, *w = V + 2 * n, *w_bar = V + 3 * n, *u = V + 4 * n,
+         *u_old = V + 5 * n, *v = V + 6 * n, *v_old = V + 7 * n;
+  double nb;
+  SB2_TRY(o.nrm(b, &nb));
+  if (nb == 0.0) { *init_failed = 1; return SB2_OK; }
+  it.facteur = 1.0 / nb;
+  if (!prm->init_guess_null) SB2_TRY(o.residual(b, x, r));
+  else { SB2_TRY(o.copy(b, r)); SB2_TRY(sb2_fill(o.n, 0.0, x, o.s)); }
+  SB2_TRY(sb2_fill(o.n, 0.0, u_old, o.s));
+  SB2_TRY(sb2_fill(o.n, 0.0, v_old, o.s));
+  double ceta = 0.0, ceta_old = 0.0, ceta_oold = 0.0, c = 1.0, cold = 1.0, s = 0.0, sold = 0.0;
+  SB2_TRY(o.prec(r, z));
+  double dp;
+  SB2_TRY(o.dot(r, z, &dp));
+  double beta = std::sqrt(dp);
+  const double beta1 = beta;
+  double s_prod = std::fabs(beta1);
+  SB2_TRY(o.copy(r, v));
+  SB2_TRY(o.copy(z, u));
+  SB2_TRY(o.scal(1.0 / beta, v));
+  SB2_TRY(o.scal(1.0 / beta, u));
+  SB2_TRY(o.copy(u, w_bar));
+  double np = nb;
+  it.nb_iter = 0;
+  for (;;) {
+    if (it.finished(np)) break;
+    if (it.nb_iter != 0) {
+      SB2_TRY(o.copy(v, v_old));
+      SB2_TRY(o.copy(u, u_old));
+      const double ib = 1.0 / beta;
+      SB2_TRY(o.copy(r, v));
+      SB2_TRY(o.scal(ib, v));
+      SB2_TRY(o.copy(z, u));
+      SB2_TRY(o.scal(ib, u));
+      SB2_TRY(o.copy(w_bar, w));
+      SB2_TRY(o.scal(c, w));
+      SB2_TRY(o.axpy(s, u, w));
+      SB2_TRY(o.scal(-s, w_bar));
+      SB2_TRY(o.axpy(c, u, w_bar));
+      SB2_TRY(o.axpy(ceta, w, x));
+      ceta_oold = ceta_old;
+      ceta_old = ceta;
+    }
+    SB2_TRY(o.mlt(u, r));
+    double alpha;
+    SB2_TRY(o.dot(u, r, &alpha));
+    SB2_TRY(o.prec(r, z));
+    SB2_TRY(o.axpy(-alpha, v, r));
+    SB2_TRY(o.axpy(-alpha, u, z));
+    SB2_TRY(o.axpy(-beta, v_old, r));
+    SB2_TRY(o.axpy(-beta, u_old, z));
+    const double beta_old = beta;
+    SB2_TRY(o.dot(r, z, &dp));
+    beta = std::sqrt(dp);
+    const double coold = cold, soold = sold;
+    cold = c;
+    sold = s;
+    const double rho0 = cold * alpha - coold * sold * beta_old;
+    const double rho1 = std::sqrt(rho0 * rho0 + beta * beta);
+    const double rho2 = sold * alpha + coold * cold * beta_old;
+    const double rho3 = soold * beta_old;
+    c = rho0 / rho1;
+    s = beta / rho1;
+    if (it.nb_iter == 0) ceta = beta1 / rho1;
+    else ceta = -(rho2 * ceta_old + rho3 * ceta_oold) / rho1;
+    s_prod *= std::fabs(s);
+    np = c == 0.0 ? s_prod * 1e16 : s_prod / std::fabs(c);
+    it.nb_iter++;
+  }
+  const double ceta_bar = c == 0.0 ? ceta * 1e15 : ceta / c;
+  SB2_TRY(o.axpy(ceta_bar, w_bar, x));
+  return SB2_OK;
+}
+
 static int host_qmrsym(Ops& o, double* x, const double* b, const sb2_iter_params* prm,
                        HostIter& it, double* V, int* init_failed) {
   const size_t n = o.n;
@@ -4181,6 +4467,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
                    : which == kCgne ? 4
                    : which == kBcr ? 6
                    : which == kQmrs ? 7
+                   : which == kSymm ? 8
                                       : 3 + m + 1;
   DeviceBuf buf;
   buf.s = s;
@@ -4203,6 +4490,7 @@ static int host_solve(int which, const sb2_csr* A, const sb2_precond* M, double*
   else if (which == kCgne) SB2_TRY(host_cgne(o, x, b, prm, it, V, &init_failed));
   else if (which == kBcr) SB2_TRY(host_bicgcr(o, x, b, prm, it, V, &init_failed));
   else if (which == kQmrs) SB2_TRY(host_qmrsym(o, x, b, prm, it, V, &init_failed));
+  else if (which == kSymm) SB2_TRY(host_symmlq(o, x, b, prm, it, V, &init_failed));
   else SB2_TRY(host_gmres(o, x, b, prm, it, V, &init_failed));
   SB2_CUDA_TRY(cudaStreamSynchronize(s));
   res->init_failed = init_failed;
@@ -4766,6 +5054,14 @@ int sb2_cocg(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
              int* hist_it, int hist_cap, void* stream) try {
   SB2_TRACE("sb2_cocg");
   return solve_entry(kCg, A, M, x, b, params, result, hist, hist_it, hist_cap,
+                     (cudaStream_t)stream);
+} SB2_CATCH
+
+int sb2_symmlq(const sb2_csr* A, const sb2_precond* M, double* x, const double* b,
+               const sb2_iter_params* params, sb2_iter_result* result, double* hist,
+               int* hist_it, int hist_cap, void* stream) try {
+  SB2_TRACE("sb2_symmlq");
+  return solve_entry(kSymm, A, M, x, b, params, result, hist, hist_it, hist_cap,
                      (cudaStream_t)stream);
 } SB2_CATCH
 

@@ -1,8 +1,8 @@
 """Cgs (Cgs.cxx:45-132), TfQmr (TfQmr.cxx:44-243), MinRes
 (MinRes.cxx:46-153), Gcr (Gcr.cxx:45-141), BiCgStabl (BiCgStabl.cxx:43-180)
 QCgs (QCgs.cxx:46-165), BiCg (BiCg.cxx:46-134), Cgne (Cgne.cxx:40-127),
-BiCgcr (BiCgcr.cxx:44-118), Lsqr (Lsqr.cxx:40-135) and QmrSym
-(QmrSym.cxx:41-165) on the device against the
+BiCgcr (BiCgcr.cxx:44-118), Lsqr (Lsqr.cxx:40-135), QmrSym
+(QmrSym.cxx:41-165) and Symmlq (Symmlq.cxx:45-161) on the device against the
 oracle's restatements, which are pinned bit for bit to the reference's own
 templates (tests/test_oracle_pin.py).
 
@@ -23,7 +23,7 @@ from tests.test_oracle_pin import _edge_solves, _nonfinite_cases, shifted_laplac
 pytestmark = pytest.mark.gpu
 
 SOLVERS = ["cgs", "tfqmr", "minres", "gcr", "bicgstabl", "qcgs", "bicg", "cgne", "bicgcr",
-           "lsqr", "qmrsym"]
+           "lsqr", "qmrsym", "symmlq"]
 
 
 @pytest.fixture(scope="module")
@@ -36,7 +36,7 @@ def _fn(api, which):
     return {"cgs": api.Cgs, "tfqmr": api.TfQmr, "minres": api.MinRes, "gcr": api.Gcr,
             "bicgstabl": api.BiCgStabl, "qcgs": api.QCgs, "bicg": api.BiCg,
             "cgne": api.Cgne, "bicgcr": api.BiCgcr, "lsqr": api.Lsqr,
-            "qmrsym": api.QmrSym}[which]
+            "qmrsym": api.QmrSym, "symmlq": api.Symmlq}[which]
 
 
 def _precond(api, pc):
@@ -78,8 +78,9 @@ CASES = ([(w, m, pc) for w in ("cgs", "tfqmr", "gcr", "bicgstabl", "qcgs", "bicg
           for pc in (0, 1, 2) if (m, pc) != ("conv", 2)] +
          # Lsqr uses no preconditioner: one case a matrix
          [("lsqr", m, 1) for m in ("conv", "lap", "lap_up")] +
-         # QmrSym wants symmetric systems
-         [("qmrsym", m, pc) for m in ("lap", "lap_up") for pc in (0, 1, 2)])
+         # QmrSym and Symmlq want symmetric systems
+         [(w, m, pc) for w in ("qmrsym", "symmlq") for m in ("lap", "lap_up")
+          for pc in (0, 1, 2)])
 
 
 def _case_matrix(mname):
@@ -120,7 +121,7 @@ def test_parity(api, oracle, which, mname, pc):
 
 @pytest.mark.parametrize("which", SOLVERS)
 def test_initial_guess(api, oracle, which):
-    full = matgen.convdiff3d(8) if which not in ("minres", "qmrsym") else matgen.poisson3d(16)
+    full = matgen.convdiff3d(8) if which not in ("minres", "qmrsym", "symmlq") else matgen.poisson3d(16)
     n = full[0].size - 1
     rng = np.random.default_rng(9)
     b = matgen.matvec(*full, rng.uniform(-1, 1, n))
@@ -179,7 +180,7 @@ def test_nonfinite(api, oracle, which):
 @pytest.mark.parametrize("which", SOLVERS)
 def test_deterministic_and_larger(api, oracle, which):
     # 64,000 rows: a grid of many CTAs, every product in the binned layout
-    full = matgen.convdiff3d(40) if which not in ("minres", "qmrsym") else matgen.poisson3d(40)
+    full = matgen.convdiff3d(40) if which not in ("minres", "qmrsym", "symmlq") else matgen.poisson3d(40)
     n = full[0].size - 1
     b = matgen.matvec(*full, np.random.default_rng(1).uniform(-1, 1, n))
     # Cgne and Lsqr square the condition number: 4,710 and 5,072 counted
